@@ -1,0 +1,355 @@
+#!/usr/bin/env python
+"""Closest-hit throughput on the 2.5M-triangle synthetic city at 1080p.
+
+One step = the closest-hit pass over one frame's ray batch of the city workload:
+1920x1080 pixels x 4 jittered primary rays (8,294,400 rays) followed by one cosine-weighted
+diffuse bounce ray for every primary hit, each batch one launch of the traversal kernel.
+`value` is Mrays/s with the rays already resident in HBM; `e2e` is the same metric through the
+C ABI with host (pinned) ray and hit buffers, the copies inside the timed region.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Multi-GPU: one process per GPU (torchrun); every rank traces its own replica of the frame
+(views are independent; no collective on the data path) and rank 0 reports the aggregate.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SEED = 2
+WIDTH, HEIGHT, SPP = 1920, 1080, 4
+CONFIG = {
+    "workload": "synthetic city: 1,024 objects, ~2.5M FP32 triangles (lognormal per-object "
+                "counts, median 1k, max 200k), 64 emissive quads; 1920x1080 x 4 spp jittered "
+                "primary rays + 1 diffuse bounce per primary hit; closest-hit",
+    "scene_seed": SEED, "width": WIDTH, "height": HEIGHT, "spp": SPP,
+    "l2": "inputs larger than L2 (rays 265 MB + 160 MB, traversal layout 233 MB)",
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.idx = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def build_workload(nb, ctx_for_bounces=None):
+    scene = nb.synth_city(seed=SEED)
+    sb = nb.SceneBVH(scene)
+    cam = nb.city_camera(WIDTH, HEIGHT)
+    primary = cam.primary_rays(SPP, seed=SEED + 10)
+    return scene, sb, primary
+
+
+def cpu_leg(sb, rays, budget_s=12.0, use_reference=False):
+    """Times the CPU traversal on the host cores over a bounded sample of the workload."""
+    cores = len(os.sched_getaffinity(0))
+    if use_reference:
+        from oracle import reference as ref
+        if not ref.available():
+            use_reference = False
+    from oracle import oracle as orc
+    os_ = orc.OracleScene(sb)
+    rng = np.random.default_rng(123)
+    sample = rays[rng.permutation(rays.shape[0])[:2_000_000]]
+    done, t0 = 0, time.perf_counter()
+    chunk = 50_000
+    while done < sample.shape[0] and time.perf_counter() - t0 < budget_s:
+        part = sample[done:done + chunk]
+        if use_reference:
+            ref.closest(sb, part, threads=cores)
+        else:
+            os_.closest(part, orc.MODE_REFERENCE_ORDER, threads=cores)
+        done += part.shape[0]
+    dt = time.perf_counter() - t0
+    return {"value": done / dt / 1e6, "unit": "Mrays/s", "cores": cores,
+            "kind": "reference" if use_reference else "port",
+            "sample": f"{done} rays drawn uniformly from the workload's primary+bounce batch "
+                      f"({dt:.1f} s of CPU work, {cores} threads)"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import nomad_b200 as nb
+    from oracle import reference as ref
+    scene, sb, primary = build_workload(nb)
+    # Bounce rays need the primary hits; the reference arm computes them on the CPU too.
+    from oracle import oracle as orc
+    os_ = orc.OracleScene(sb)
+    rng = np.random.default_rng(7)
+    idx = rng.permutation(primary.shape[0])[:400_000]
+    ph = os_.closest(primary[idx], orc.MODE_REFERENCE_ORDER)
+    bounce = nb.bounce_rays(primary[idx], ph, sb.prims, seed=SEED + 11)
+    mix = np.concatenate([primary[idx], bounce])
+    use_ref = ref.available()
+    cores = len(os.sched_getaffinity(0))
+    per_step = min(mix.shape[0], 300_000)
+    for _ in range(args.warmup):
+        (ref.closest(sb, mix[:20_000], threads=cores) if use_ref
+         else os_.closest(mix[:20_000], orc.MODE_REFERENCE_ORDER, threads=cores))
+    times = []
+    for s in range(args.steps):
+        part = mix[(s * per_step) % mix.shape[0]:][:per_step]
+        t0 = time.perf_counter()
+        (ref.closest(sb, part, threads=cores) if use_ref
+         else os_.closest(part, orc.MODE_REFERENCE_ORDER, threads=cores))
+        times.append((time.perf_counter() - t0, part.shape[0]))
+    tot_t = sum(t for t, _ in times)
+    tot_r = sum(n for _, n in times)
+    v = tot_r / tot_t / 1e6
+    kind = "reference" if use_ref else "port"
+    line = {"impl": "reference", "metric": "closest-hit Mrays/s (city 1080p x4spp + bounce)",
+            "value": v, "unit": "Mrays/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": CONFIG,
+            "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": cores, "kind": kind,
+                             "sample": f"{per_step} rays per step from the primary+bounce mix"},
+            "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="nomad", choices=["nomad", "reference"])
+    ap.add_argument("--kernel", type=int, default=0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+    import nomad_b200 as nb
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    t_setup = time.perf_counter()
+    scene, sb, primary = build_workload(nb)
+    ctx = nb.Context(local)
+    ctx.upload(sb)
+    if args.kernel:
+        ctx.set_kernel(args.kernel)
+    # A dedicated stream: the kernels and the timing events must share it (the legacy default
+    # stream has handle 0, which the C ABI reads as "the context's own stream").
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+
+    def dev_rays(r):
+        return torch.from_numpy(r.view(np.float32).reshape(-1, 8)).cuda()
+
+    d_prim = dev_rays(primary)
+    d_ph = torch.empty((primary.shape[0], 5), dtype=torch.int32, device="cuda")
+    ctx.trace_closest_dev(d_prim.data_ptr(), primary.shape[0], d_ph.data_ptr())
+    torch.cuda.synchronize()
+    ph = d_ph.cpu().numpy().view(nb.HIT_DTYPE).reshape(-1)
+    bounce = nb.bounce_rays(primary, ph, sb.prims, seed=SEED + 11)
+    d_b = dev_rays(bounce)
+    d_bh = torch.empty((bounce.shape[0], 5), dtype=torch.int32, device="cuda")
+    n_prim, n_b = primary.shape[0], bounce.shape[0]
+    rays_per_step = n_prim + n_b
+    log(f"setup {time.perf_counter() - t_setup:.1f}s: {sb.prim_count} prims, "
+        f"{n_prim} primary + {n_b} bounce rays")
+
+    # Algorithmic bytes per launch from the work counters (near-first binary traversal).
+    d_w = torch.empty((max(n_prim, n_b), 4), dtype=torch.int32, device="cuda")
+
+    def alg_bytes(d, n):
+        ctx.trace_work_dev(d.data_ptr(), n, d_w.data_ptr())
+        torch.cuda.synchronize()
+        w = d_w[:n].to(torch.int64)
+        return int((32 * w[:, 0] + 52 * w[:, 1] + 16 * w[:, 2] + 48 * w[:, 3]).sum().item())
+
+    bytes_prim = alg_bytes(d_prim, n_prim)
+    bytes_b = alg_bytes(d_b, n_b)
+    del d_w
+
+    def step():
+        ctx.trace_closest_dev(d_prim.data_ptr(), n_prim, d_ph.data_ptr())
+        ctx.trace_closest_dev(d_b.data_ptr(), n_b, d_bh.data_ptr())
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        time.sleep(0.3)
+        torch.cuda.synchronize()
+        start.record(stream)
+        for i in range(args.steps):
+            ev[i][0].record(stream)
+            ctx.trace_closest_dev(d_prim.data_ptr(), n_prim, d_ph.data_ptr())
+            ev[i][1].record(stream)
+            ctx.trace_closest_dev(d_b.data_ptr(), n_b, d_bh.data_ptr())
+            ev[i][2].record(stream)
+        end.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    total_ms = start.elapsed_time(end)
+    t_prim = np.mean([e[0].elapsed_time(e[1]) for e in ev])
+    t_b = np.mean([e[1].elapsed_time(e[2]) for e in ev])
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_step = total_ms / args.steps
+    value = world * rays_per_step * args.steps / (total_ms / 1e3) / 1e6
+
+    # e2e through the C ABI with pinned host buffers (copies inside the timed region).
+    h_rays = torch.from_numpy(np.concatenate([primary, bounce]).view(np.uint8)).pin_memory()
+    h_hits = torch.empty((rays_per_step * 20,), dtype=torch.uint8).pin_memory()
+    rays_np = h_rays.numpy().view(nb.RAY_DTYPE)
+    hits_np = h_hits.numpy().view(nb.HIT_DTYPE)
+    ctx.set_stream(0)
+
+    def e2e_step():
+        st = ctx.lib.nomad_trace_closest(ctx.h, rays_np.ctypes.data, rays_per_step,
+                                         hits_np.ctypes.data, 0)
+        if st != 0:
+            raise nb.NomadError(st, ctx.lib.nomad_last_error(ctx.h).decode())
+
+    for _ in range(2):
+        e2e_step()
+    if world > 1:
+        dist.barrier()
+    e_steps = max(2, min(args.steps, 5))
+    t0 = time.perf_counter()
+    for _ in range(e_steps):
+        e2e_step()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * rays_per_step * e_steps / e2e_s / 1e6
+    ok = np.array_equal(hits_np.view(np.int32).reshape(-1, 5)[:n_prim],
+                        d_ph.cpu().numpy()) if True else True
+
+    peak, peak_kind = measured_peaks()
+    achieved = (bytes_prim + bytes_b) / ((t_prim + t_b) / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None,
+                "peak_source": peak_kind,
+                "algorithmic_bytes_per_launch": {"primary": bytes_prim, "bounce": bytes_b},
+                "kernel_ms": {"primary": t_prim, "bounce": t_b}}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_leg(sb, np.concatenate([primary, bounce]))
+
+    if rank == 0:
+        line = {
+            "metric": "closest-hit Mrays/s (city 1080p x4spp + bounce)",
+            "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": dict(CONFIG, parallelism=f"replicas{world}"),
+            "primary_mrays_s": n_prim / (t_prim / 1e3) / 1e6,
+            "bounce_mrays_s": n_b / (t_b / 1e3) / 1e6,
+            "rays_per_step": rays_per_step,
+            "e2e": {"value": e2e_value, "unit": "Mrays/s",
+                    "h2d_bytes_per_step": rays_per_step * 32, "d2h_bytes_per_step": rays_per_step * 20,
+                    "matches_device_result": bool(ok)},
+            "gpu_launches": 2 * args.steps,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

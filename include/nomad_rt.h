@@ -1,0 +1,137 @@
+/*
+ * nomad_rt.h — C ABI of the B200 traversal / path-tracing core (libnomad_rt.so).
+ *
+ * The reference binds its hot path as one Metal compute kernel argument table,
+ * pathTraceKernel (Nomad Path Tracer/Renderer/Shaders/PathTraceKernel.metal:7-44), filled by
+ * Renderer::draw (Renderer/Renderer.cpp:7484-7566), with the C++ residency interface
+ * setObjectActive / setPrimitiveActive / updateResidency / flushResidencyChanges above it.
+ * Each entry point below names the reference interface it replaces.
+ *
+ * Conventions
+ *   - Every call returns nomad_status (0 = NOMAD_OK; codes in nomad_scene.h). No exceptions
+ *     cross the ABI; nomad_last_error() gives the text of the last failure on a context.
+ *   - Host pointers unless NOMAD_TRACE_DEVICE_POINTERS is set, in which case the caller passes
+ *     CUDA device pointers (e.g. from its own allocator) and the call returns without waiting.
+ *   - A context is used from one thread at a time, like the reference's Renderer. Distinct
+ *     contexts may run on distinct threads.
+ *   - Device-side failures (a traversal stack that would overflow, an exhausted bounded wait)
+ *     never fault or trap the GPU: kernels set bits in a status word that nomad_get_status()
+ *     returns.
+ */
+#ifndef NOMAD_RT_H
+#define NOMAD_RT_H
+
+#include <stdint.h>
+#include <stddef.h>
+#include "nomad_scene.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct nomad_ctx nomad_ctx;
+
+typedef struct nomad_config {
+  int32_t device;          /* CUDA device ordinal                                          */
+  uint32_t flags;          /* reserved, 0                                                  */
+} nomad_config;
+
+/* One ray: the reference's Ray (Shaders/PathTracing.h:30-35) packed into two float4.
+ * Closest-hit accepts t in (RAY_EPS = 1e-4, tmax) and, like firstHitTLAS, does not read tmin;
+ * tmax = +inf gives the reference's unbounded closest hit. Any-hit accepts t in (1e-4, tmax). */
+typedef struct nomad_ray {
+  float ox, oy, oz, tmin;
+  float dx, dy, dz, tmax;
+} nomad_ray;
+
+/* Closest hit: instance (object) index and primitive index (-1, -1 on a miss), distance t and
+ * barycentrics (u, v) of Möller–Trumbore (the reference's intersection.barycentric,
+ * Shaders/PathTracing.h:844). Sphere and rectangle hits report u = v = 0. */
+typedef struct nomad_hit {
+  int32_t inst;
+  int32_t prim;
+  float t, u, v;
+} nomad_hit;
+
+/* Flags of the trace calls. */
+enum {
+  NOMAD_TRACE_DEVICE_POINTERS = 1u << 0, /* rays/outputs are device pointers                  */
+  NOMAD_TRACE_COUNT_HITS = 1u << 1       /* add closest hits to the per-object hit counters   */
+};
+
+/* Traversal kernel variants (the autotuner picks one per scene; 0 = default). */
+enum {
+  NOMAD_KERNEL_AUTO = 0,
+  NOMAD_KERNEL_BVH2 = 1,        /* binary pair-node traversal, one ray per thread, local stack   */
+  NOMAD_KERNEL_BVH2_PERSIST = 2 /* same, persistent warps fetching rays from a global counter    */
+};
+
+/* ---- context -------------------------------------------------------------------------------- */
+nomad_status nomad_create(const nomad_config *cfg, nomad_ctx **out);
+nomad_status nomad_destroy(nomad_ctx *ctx);
+const char *nomad_last_error(const nomad_ctx *ctx);
+/* Waits for all work queued on the context's stream. */
+nomad_status nomad_sync(nomad_ctx *ctx);
+/* Runs the context's device-pointer work on the caller's CUDA stream (a cudaStream_t passed
+ * as void*); NULL restores the context's own stream. */
+nomad_status nomad_set_stream(nomad_ctx *ctx, void *cuda_stream);
+/* Device status word: bit 0 stack overflow guard, bit 1 bounded wait expired. Cleared by reading. */
+nomad_status nomad_get_status(nomad_ctx *ctx, uint32_t *status_word);
+
+/* ---- scene upload (replaces the GPU uploads of Renderer::rebuildResidentResources,
+ *      Renderer.cpp:5983-6292, for the non-compacted resident set) ------------------------ */
+/* Arrays use the SceneBVH layouts exactly: bvh_nodes/tlas_nodes are float4 pairs
+ * (createBVHBuffer / createTLASBuffer), prims 7 float4 per primitive (createTransformsBuffer),
+ * materials 5 float4 per primitive (createMaterialsBuffer), prim_indices int32
+ * (createPrimitiveIndexBuffer), instances one record per object. The caller owns the host
+ * arrays; the library copies them and builds its traversal layout on the device. All
+ * primitives start active; objects with blas_root_index < 0 start non-resident. */
+nomad_status nomad_scene_upload(nomad_ctx *ctx, const float *bvh_nodes, uint32_t bvh_node_count,
+                                const float *tlas_nodes, uint32_t tlas_node_count,
+                                const float *prims, const float *materials,
+                                const int32_t *prim_indices, uint32_t prim_count,
+                                const nomad_instance_record *instances, uint32_t object_count);
+
+/* ---- residency (Renderer::setPrimitiveActive, Renderer.cpp:7819-7869;
+ *      setObjectActive, RendererResidency.cpp:965-1031; flushResidencyChanges,
+ *      RendererResidency.cpp:5157-5193) --------------------------------------------------- */
+/* Marks one primitive (in)active. *changed = 1 when its state flipped. Takes effect at flush. */
+nomad_status nomad_residency_set_primitive_active(nomad_ctx *ctx, uint32_t prim, int32_t active,
+                                                  int32_t *changed);
+/* Marks every primitive of one object (in)active; *toggled = primitives whose state flipped. */
+nomad_status nomad_residency_set_object_active(nomad_ctx *ctx, uint32_t obj, int32_t active,
+                                               uint32_t *toggled);
+/* Applies pending toggles to the device: an object with no active primitive gets
+ * blas_root_index = -1 (skipped by the traversal), inactive primitives are skipped in leaves. */
+nomad_status nomad_residency_flush(nomad_ctx *ctx);
+/* Copies the current instance records (after the last flush) into out[object_count]. */
+nomad_status nomad_residency_get_instances(nomad_ctx *ctx, nomad_instance_record *out);
+
+/* ---- traversal (replaces firstHitTLAS/firstHitBVH, Shaders/PathTracing.h:670-1066, and the
+ *      visibility test isLightVisible, :503-556, as standalone ray queries) ---------------- */
+/* Closest hit per ray. Ties in t go to the lowest primitive index. */
+nomad_status nomad_trace_closest(nomad_ctx *ctx, const nomad_ray *rays, uint64_t n,
+                                 nomad_hit *out, uint32_t flags);
+/* Any hit per ray in (1e-4, tmax): out[i] = 1 when occluded, else 0. Exits at the first hit. */
+nomad_status nomad_trace_any(nomad_ctx *ctx, const nomad_ray *rays, uint64_t n, uint8_t *out,
+                             uint32_t flags);
+/* Chooses the traversal variant used by the trace calls (NOMAD_KERNEL_*). */
+nomad_status nomad_set_kernel(nomad_ctx *ctx, uint32_t kernel);
+
+/* Work counters of a near-first binary traversal over the SceneBVH arrays, per ray:
+ * out[4*i+0] nodes whose box was tested (TLAS + BLAS), [1] primitive tests, [2] instance
+ * records read, [3] 1 when the ray hit. Defines the algorithmic bytes per ray:
+ * 32*nodes + 48*tests + 4*tests + 16*instances + 48*hit. */
+nomad_status nomad_trace_work(nomad_ctx *ctx, const nomad_ray *rays, uint64_t n, uint32_t *out,
+                              uint32_t flags);
+
+/* ---- hit counters (the reference's primitiveRayStats, Shaders/PathTracing.h:1171-1226, and
+ *      the per-object sums of processRayHitCounters, Renderer.cpp:8415-8426) -------------- */
+/* Per-object closest-hit counts accumulated by NOMAD_TRACE_COUNT_HITS calls: out[object_count]. */
+nomad_status nomad_read_object_hits(nomad_ctx *ctx, uint32_t *out);
+nomad_status nomad_reset_object_hits(nomad_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,138 @@
+/*
+ * nomad_scene.h — host-side scene description and SceneBVH-compatible builder.
+ *
+ * These entry points replace the host half of the reference's scene pipeline:
+ *   - Scene::addObject / addObjectInternal (Nomad Path Tracer/Scene/Scene.cpp:107-168),
+ *     including Triangle::computeFrame (Scene/Triangle.h:20-107) and
+ *     Rectangle::computeFrame (Scene/Rectangle.h:19-75);
+ *   - Scene::buildBVH (Scene/SceneBVH.cpp:16-159) with buildBVHRecursive (:549-623),
+ *     evaluateSAHSplit (:704-815) and buildTLASRecursive (:625-702);
+ *   - the GPU packers createTransformsBuffer (:165-209), createMaterialsBuffer (:211-222),
+ *     createBVHBuffer (:420-428), createTLASBuffer (:467-488) and
+ *     createPrimitiveIndexBuffer (:514-520);
+ *   - the non-compacted instance-record fill in Renderer::rebuildResidentResources
+ *     (Renderer/Renderer.cpp:5305-5326).
+ * The arrays they produce use exactly the reference's GPU layouts, so a caller can feed
+ * them to nomad_scene_upload (nomad_rt.h) or to any consumer of the reference's buffers.
+ *
+ * Plus seeded synthetic scene generators (icosphere instances, a procedural city) that
+ * stand in for the reference's XML/OBJ scenes.
+ *
+ * All functions are host-only, thread-safe on distinct handles, and return nomad_status
+ * (0 = OK). No exceptions cross this ABI.
+ */
+#ifndef NOMAD_SCENE_H
+#define NOMAD_SCENE_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t nomad_status;
+enum {
+  NOMAD_OK = 0,
+  NOMAD_ERR_INVALID_ARGUMENT = 1,
+  NOMAD_ERR_OUT_OF_MEMORY = 2,
+  NOMAD_ERR_CUDA = 3,
+  NOMAD_ERR_NOT_READY = 4,
+  NOMAD_ERR_SCENE_INVALID = 5,
+  NOMAD_ERR_DEVICE_STATUS = 6,
+  NOMAD_ERR_UNSUPPORTED = 7,
+  NOMAD_ERR_LIMIT = 8
+};
+
+/* Primitive types, numbered as PrimitiveType (Scene/Primitive.h:13-17). */
+enum { NOMAD_PRIM_SPHERE = 0, NOMAD_PRIM_TRIANGLE = 1, NOMAD_PRIM_RECTANGLE = 2 };
+
+/* Floats per primitive in a scene description:
+ *   triangle : v0.xyz v1.xyz v2.xyz uv0.xy uv1.xy uv2.xy           (15 used)
+ *   rectangle: center.xyz u.xyz v.xyz                               (9 used)
+ *   sphere   : center.xyz radius                                    (4 used)            */
+#define NOMAD_PRIM_GEOM_FLOATS 15
+/* Floats per material = 5 float4, encoded as encodeMaterial (Scene/Material.h:32-44):
+ *   {diffuse.rgb, opacity} {specular.rgb, shininess} {emission.rgb, power}
+ *   {transmission.rgb, ior} {diffuseTex, specularTex, normalTex, roughness}          */
+#define NOMAD_MATERIAL_FLOATS 20
+/* float4 per packed primitive and per packed material in the GPU buffers. */
+#define NOMAD_PRIM_FLOAT4 7
+#define NOMAD_MATERIAL_FLOAT4 5
+
+/* A scene description: primitives grouped into objects. Objects are contiguous,
+ * non-overlapping primitive ranges, in order (Scene::addObject appends). */
+typedef struct nomad_scene_desc {
+  uint32_t prim_count;
+  const int32_t *prim_type;      /* [prim_count] NOMAD_PRIM_*                         */
+  const float *prim_geom;        /* [prim_count * NOMAD_PRIM_GEOM_FLOATS]             */
+  const float *prim_material;    /* [prim_count * NOMAD_MATERIAL_FLOATS]              */
+  uint32_t object_count;
+  const uint32_t *object_first;  /* [object_count] first primitive of each object     */
+  const uint32_t *object_prims;  /* [object_count] primitive count of each object     */
+} nomad_scene_desc;
+
+/* The TLAS instance record, laid out as InstanceRecord (Renderer/Shaders/Structs.h:31-37)
+ * and BlasInstanceRecord (Renderer/Renderer.h:31-36). blas_root_index < 0 marks an
+ * object that is not resident; the traversal skips it. */
+typedef struct nomad_instance_record {
+  int32_t blas_root_index;
+  uint32_t primitive_base;
+  uint32_t primitive_count;
+  uint32_t primitive_index_base;
+} nomad_instance_record;
+
+/* Read-only views of a built SceneBVH. Every pointer stays valid until the handle is freed.
+ * Node arrays are float4 pairs: {min.xyz, bits(leftFirst|left)} {max.xyz, bits(count|right)}. */
+typedef struct nomad_scenebvh_view {
+  uint32_t prim_count;
+  uint32_t object_count;
+  uint32_t bvh_node_count;       /* BLAS nodes of all objects, concatenated            */
+  uint32_t tlas_node_count;
+  const float *bvh_nodes;        /* [bvh_node_count * 8]  createBVHBuffer             */
+  const float *tlas_nodes;       /* [tlas_node_count * 8] createTLASBuffer            */
+  const float *prims;            /* [prim_count * 28]     createTransformsBuffer      */
+  const float *materials;        /* [prim_count * 20]     createMaterialsBuffer       */
+  const int32_t *prim_indices;   /* [prim_count]          createPrimitiveIndexBuffer  */
+  const nomad_instance_record *instances; /* [object_count], all objects resident      */
+  const float *object_bounds;    /* [object_count * 6] min.xyz max.xyz                 */
+  uint32_t max_depth;            /* deepest TLAS+BLAS root-to-leaf path, in nodes      */
+} nomad_scenebvh_view;
+
+typedef struct nomad_scenebvh nomad_scenebvh;
+
+/* Builds the SceneBVH arrays for a scene description (objects in parallel on host
+ * threads, like Scene::buildBVH). threads = 0 uses all hardware threads. */
+nomad_status nomad_scenebvh_build(const nomad_scene_desc *desc, uint32_t threads,
+                                  nomad_scenebvh **out);
+nomad_status nomad_scenebvh_view_get(const nomad_scenebvh *h, nomad_scenebvh_view *out);
+void nomad_scenebvh_free(nomad_scenebvh *h);
+
+/* ---- seeded synthetic scenes (no reference counterpart: stand-ins for its XML scenes) ---- */
+
+typedef struct nomad_scene_owned nomad_scene_owned;
+
+/* Small scene: `instances` copies of a 3x-subdivided icosphere (1,280 triangles each),
+ * world-space baked with translation U[-extent/2, extent/2]^3, scale U(0.5,3) and a
+ * uniform random rotation. One object per instance. */
+nomad_status nomad_synth_icospheres(uint64_t seed, uint32_t instances, float extent,
+                                    nomad_scene_owned **out);
+
+/* Procedural city: grid x grid cells on a `size_m` square; each cell is one object holding
+ * a noise-displaced box or cylinder with a lognormal triangle count (median
+ * `median_tris`, clamped to `max_tris`, rescaled to about `target_tris` in total), its
+ * ground tile, and — for `emissive_quads` seeded cells — an emissive rectangle lamp.
+ * `emissive_tris` extra small emissive triangles with lognormal power (sigma
+ * `emissive_sigma`) are scattered over the roofs (0 for none). */
+nomad_status nomad_synth_city(uint64_t seed, uint32_t grid, float size_m, uint32_t target_tris,
+                              uint32_t median_tris, uint32_t max_tris, uint32_t emissive_quads,
+                              uint32_t emissive_tris, float emissive_sigma,
+                              nomad_scene_owned **out);
+
+nomad_status nomad_scene_owned_desc(const nomad_scene_owned *s, nomad_scene_desc *out);
+void nomad_scene_owned_free(nomad_scene_owned *s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,12 @@
+"""nomad_b200 — B200-native ray traversal / path-tracing core.
+
+The compute path is libnomad_rt.so (hand-written sm_100a CUDA + host C++), reached through the
+C ABI in include/nomad_rt.h and include/nomad_scene.h. This package only binds it (ctypes) and
+builds host-side ray batches; it has no CPU fallback.
+"""
+from .native import (  # noqa: F401
+    Context, HostScene, SceneBVH, NomadError, load, synth_city, synth_icospheres,
+    RAY_DTYPE, HIT_DTYPE, INSTANCE_DTYPE, LIB_PATH, SIGNATURES,
+    KERNEL_AUTO, KERNEL_BVH2, KERNEL_BVH2_PERSIST, TRACE_COUNT_HITS, TRACE_DEVICE_POINTERS,
+)
+from .rays import Camera, bounce_rays, city_camera, icosphere_camera  # noqa: F401

@@ -1,0 +1,554 @@
+// libnomad_rt: CUDA context, scene upload, residency and the trace entry points of nomad_rt.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../../include/nomad_rt.h"
+#include "../host/layout.h"
+#include "rt_device.cuh"
+
+using namespace nomad_dev;
+
+namespace {
+
+constexpr int kStack = 64;          // entries; the upload rejects deeper trees
+constexpr int kBlock = 128;
+constexpr int kPersistBlock = 128;
+
+__device__ __forceinline__ void warp_count_object_hit(int32_t inst, uint32_t *counts) {
+  unsigned mask = __activemask();
+  unsigned peers = __match_any_sync(mask, inst);
+  int lane = threadIdx.x & 31;
+  int leader = __ffs(peers) - 1;
+  if (inst >= 0 && lane == leader) atomicAdd(counts + inst, (uint32_t)__popc(peers));
+}
+
+__device__ __forceinline__ void store_hit(nomad_hit *out, uint64_t i, const HitRec &h) {
+  int32_t *o = reinterpret_cast<int32_t *>(out + i);
+  o[0] = h.inst;
+  o[1] = h.prim;
+  o[2] = __float_as_int(h.t);
+  o[3] = __float_as_int(h.u);
+  o[4] = __float_as_int(h.v);
+}
+
+__global__ void __launch_bounds__(kBlock) k_closest(DevScene S, const float4 *__restrict__ rays,
+                                                     uint64_t n, nomad_hit *__restrict__ out,
+                                                     uint32_t *__restrict__ counts) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 a = __ldg(rays + 2 * i), b = __ldg(rays + 2 * i + 1);
+  RayP r = prep_ray(a, b);
+  HitRec h;
+  Work w{0, 0, 0};
+  traverse<kStack, false, false>(S, r, b.w, h, w);
+  if (h.prim < 0) h.t = INFINITY;
+  store_hit(out, i, h);
+  if (counts) warp_count_object_hit(h.prim >= 0 ? h.inst : -1, counts);
+}
+
+// Persistent variant: each warp takes 32 rays at a time from a global cursor.
+__global__ void __launch_bounds__(kPersistBlock) k_closest_persist(
+    DevScene S, const float4 *__restrict__ rays, uint64_t n, nomad_hit *__restrict__ out,
+    uint32_t *__restrict__ counts, unsigned long long *__restrict__ cursor) {
+  int lane = threadIdx.x & 31;
+  for (;;) {
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(cursor, 32ull);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= n) break;
+    uint64_t i = base + lane;
+    if (i < n) {
+      float4 a = __ldg(rays + 2 * i), b = __ldg(rays + 2 * i + 1);
+      RayP r = prep_ray(a, b);
+      HitRec h;
+      Work w{0, 0, 0};
+      traverse<kStack, false, false>(S, r, b.w, h, w);
+      if (h.prim < 0) h.t = INFINITY;
+      store_hit(out, i, h);
+      if (counts) warp_count_object_hit(h.prim >= 0 ? h.inst : -1, counts);
+    }
+    __syncwarp();
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_any(DevScene S, const float4 *__restrict__ rays,
+                                                 uint64_t n, uint8_t *__restrict__ out) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 a = __ldg(rays + 2 * i), b = __ldg(rays + 2 * i + 1);
+  RayP r = prep_ray(a, b);
+  HitRec h;
+  Work w{0, 0, 0};
+  traverse<kStack, true, false>(S, r, b.w, h, w);
+  out[i] = h.prim >= 0 ? 1 : 0;
+}
+
+__global__ void __launch_bounds__(kBlock) k_work(DevScene S, const float4 *__restrict__ rays,
+                                                  uint64_t n, uint4 *__restrict__ out) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 a = __ldg(rays + 2 * i), b = __ldg(rays + 2 * i + 1);
+  RayP r = prep_ray(a, b);
+  HitRec h;
+  Work w{0, 0, 0};
+  traverse<kStack, false, true>(S, r, b.w, h, w);
+  out[i] = make_uint4(w.nodes, w.tests, w.insts, h.prim >= 0 ? 1u : 0u);
+}
+
+// Residency patches: word offsets into the layout arena and their new values.
+__global__ void k_patch(int32_t *__restrict__ arena, const int64_t *__restrict__ offs,
+                        const int32_t *__restrict__ vals, uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) arena[offs[i]] = vals[i];
+}
+
+}  // namespace
+
+struct DeviceBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  ~DeviceBuf() {
+    if (p) cudaFree(p);
+  }
+  cudaError_t reserve(size_t b) {
+    if (b <= bytes) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e == cudaSuccess) bytes = b;
+    return e;
+  }
+};
+
+struct nomad_ctx {
+  int device = 0;
+  int smCount = 0;
+  cudaStream_t stream = nullptr;     // stream used by calls (own or caller's)
+  cudaStream_t ownStream = nullptr;
+  cudaStream_t copyStreams[2] = {nullptr, nullptr};
+  std::string err;
+  uint32_t kernel = NOMAD_KERNEL_BVH2;
+  bool sceneReady = false;
+  // scene sizes
+  uint32_t primCount = 0, objectCount = 0;
+  // device memory
+  DeviceBuf arena;      // pair nodes then triangle records
+  DeviceBuf prims, materials;
+  DeviceBuf objHits, status, cursor;
+  DeviceBuf stageIn, stageOut, stageAux;  // host-pointer staging
+  DeviceBuf patchOffs, patchVals;
+  size_t pnodeWords = 0;  // int32 words of the pair-node part of the arena
+  DevScene scene{};
+  // host residency state
+  nomad::TraversalLayout layout;
+  std::vector<uint8_t> primActive, objResident;
+  std::vector<uint32_t> objActiveCount;
+  std::vector<nomad_instance_record> instances;
+  std::vector<uint32_t> dirtyPrims, dirtyObjs;
+  std::vector<uint8_t> primDirtyFlag, objDirtyFlag;
+};
+
+namespace {
+
+nomad_status fail(nomad_ctx *c, nomad_status st, const std::string &msg) {
+  if (c) c->err = msg;
+  return st;
+}
+
+nomad_status cuda_fail(nomad_ctx *c, cudaError_t e, const char *what) {
+  return fail(c, NOMAD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define NOMAD_CUDA(ctx, call)                             \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
+  } while (0)
+
+bool is_device_ptr(const void *p) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+}  // namespace
+
+extern "C" nomad_status nomad_create(const nomad_config *cfg, nomad_ctx **out) {
+  if (!out) return NOMAD_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  std::unique_ptr<nomad_ctx> c(new (std::nothrow) nomad_ctx());
+  if (!c) return NOMAD_ERR_OUT_OF_MEMORY;
+  c->device = cfg ? cfg->device : 0;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return NOMAD_ERR_CUDA;
+  }
+  if (c->device < 0 || c->device >= count) return NOMAD_ERR_INVALID_ARGUMENT;
+  if (cudaSetDevice(c->device) != cudaSuccess) return NOMAD_ERR_CUDA;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, c->device) != cudaSuccess) return NOMAD_ERR_CUDA;
+  if (prop.major < 10) return NOMAD_ERR_UNSUPPORTED;  // built for sm_100a only
+  c->smCount = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&c->ownStream, cudaStreamNonBlocking) != cudaSuccess)
+    return NOMAD_ERR_CUDA;
+  c->stream = c->ownStream;
+  for (auto &s : c->copyStreams)
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return NOMAD_ERR_CUDA;
+  if (c->status.reserve(16) != cudaSuccess || c->cursor.reserve(16) != cudaSuccess)
+    return NOMAD_ERR_OUT_OF_MEMORY;
+  cudaMemset(c->status.p, 0, 16);
+  *out = c.release();
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_destroy(nomad_ctx *ctx) {
+  if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  for (auto s : ctx->copyStreams)
+    if (s) cudaStreamDestroy(s);
+  if (ctx->ownStream) cudaStreamDestroy(ctx->ownStream);
+  delete ctx;
+  return NOMAD_OK;
+}
+
+extern "C" const char *nomad_last_error(const nomad_ctx *ctx) {
+  return ctx ? ctx->err.c_str() : "null context";
+}
+
+extern "C" nomad_status nomad_sync(nomad_ctx *ctx) {
+  if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
+  NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_set_stream(nomad_ctx *ctx, void *cuda_stream) {
+  if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
+  ctx->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : ctx->ownStream;
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_get_status(nomad_ctx *ctx, uint32_t *word) {
+  if (!ctx || !word) return NOMAD_ERR_INVALID_ARGUMENT;
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(word, ctx->status.p, 4, cudaMemcpyDeviceToHost, ctx->stream));
+  NOMAD_CUDA(ctx, cudaMemsetAsync(ctx->status.p, 0, 4, ctx->stream));
+  NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_scene_upload(nomad_ctx *ctx, const float *bvh, uint32_t bvhCount,
+                                           const float *tlas, uint32_t tlasCount,
+                                           const float *prims, const float *materials,
+                                           const int32_t *primIndices, uint32_t primCount,
+                                           const nomad_instance_record *inst,
+                                           uint32_t objectCount) {
+  if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
+  if (!bvh || !tlas || !prims || !materials || !primIndices || !inst)
+    return fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "null scene array");
+  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  ctx->sceneReady = false;
+  std::vector<nomad::ObjectRange> objs(objectCount);
+  for (uint32_t o = 0; o < objectCount; ++o)
+    objs[o] = {inst[o].blas_root_index, inst[o].primitive_base, inst[o].primitive_count};
+  std::string err;
+  try {
+    if (!nomad::build_traversal_layout(bvh, bvhCount, tlas, tlasCount, prims, primIndices,
+                                       primCount, objs.data(), objectCount, ctx->layout,
+                                       ctx->objResident, err))
+      return fail(ctx, NOMAD_ERR_SCENE_INVALID, err);
+  } catch (const std::bad_alloc &) {
+    return fail(ctx, NOMAD_ERR_OUT_OF_MEMORY, "host memory");
+  }
+  if (ctx->layout.maxDepth > (uint32_t)kStack)
+    return fail(ctx, NOMAD_ERR_LIMIT,
+                "tree depth " + std::to_string(ctx->layout.maxDepth) + " exceeds the traversal stack");
+  const auto &L = ctx->layout;
+  size_t pnBytes = L.pnodes.size() * 4, triBytes = L.tris.size() * 4;
+  NOMAD_CUDA(ctx, ctx->arena.reserve(pnBytes + triBytes + 64));
+  NOMAD_CUDA(ctx, ctx->prims.reserve((size_t)primCount * 112));
+  NOMAD_CUDA(ctx, ctx->materials.reserve((size_t)primCount * 80));
+  NOMAD_CUDA(ctx, ctx->objHits.reserve((size_t)objectCount * 4 + 16));
+  char *base = static_cast<char *>(ctx->arena.p);
+  if (pnBytes)
+    NOMAD_CUDA(ctx, cudaMemcpy(base, L.pnodes.data(), pnBytes, cudaMemcpyHostToDevice));
+  NOMAD_CUDA(ctx, cudaMemcpy(base + pnBytes, L.tris.data(), triBytes, cudaMemcpyHostToDevice));
+  NOMAD_CUDA(ctx, cudaMemcpy(ctx->prims.p, prims, (size_t)primCount * 112, cudaMemcpyHostToDevice));
+  NOMAD_CUDA(ctx, cudaMemcpy(ctx->materials.p, materials, (size_t)primCount * 80,
+                             cudaMemcpyHostToDevice));
+  NOMAD_CUDA(ctx, cudaMemset(ctx->objHits.p, 0, (size_t)objectCount * 4 + 16));
+  ctx->pnodeWords = pnBytes / 4;
+  DevScene &S = ctx->scene;
+  S.pn = reinterpret_cast<const float4 *>(base);
+  S.tri = reinterpret_cast<const float4 *>(base + pnBytes);
+  S.prims = static_cast<const float4 *>(ctx->prims.p);
+  for (int k = 0; k < 3; ++k) {
+    S.rmin[k] = L.rootMin[k];
+    S.rmax[k] = L.rootMax[k];
+  }
+  S.rootRef = L.rootRef;
+  S.tlasPairs = L.tlasPairCount;
+  S.status = static_cast<uint32_t *>(ctx->status.p);
+  ctx->primCount = primCount;
+  ctx->objectCount = objectCount;
+  ctx->primActive.assign(primCount, 1);
+  ctx->objActiveCount.assign(objectCount, 0);
+  for (uint32_t o = 0; o < objectCount; ++o) ctx->objActiveCount[o] = inst[o].primitive_count;
+  ctx->instances.assign(inst, inst + objectCount);
+  ctx->dirtyPrims.clear();
+  ctx->dirtyObjs.clear();
+  ctx->primDirtyFlag.assign(primCount, 0);
+  ctx->objDirtyFlag.assign(objectCount, 0);
+  // Objects uploaded non-resident keep their primitives flagged active (like the reference,
+  // where residency is per object through the instance record); they are skipped via the TLAS.
+  ctx->sceneReady = true;
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_residency_set_primitive_active(nomad_ctx *ctx, uint32_t prim,
+                                                             int32_t active, int32_t *changed) {
+  if (!ctx || !ctx->sceneReady) return NOMAD_ERR_NOT_READY;
+  if (changed) *changed = 0;
+  if (prim >= ctx->primCount) return fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "primitive out of range");
+  uint8_t a = active ? 1 : 0;
+  if (ctx->primActive[prim] == a) return NOMAD_OK;
+  ctx->primActive[prim] = a;
+  uint32_t o = static_cast<uint32_t>(ctx->layout.primObject[prim]);
+  if (a)
+    ++ctx->objActiveCount[o];
+  else if (ctx->objActiveCount[o] > 0)
+    --ctx->objActiveCount[o];
+  if (!ctx->primDirtyFlag[prim]) {
+    ctx->primDirtyFlag[prim] = 1;
+    ctx->dirtyPrims.push_back(prim);
+  }
+  if (!ctx->objDirtyFlag[o]) {
+    ctx->objDirtyFlag[o] = 1;
+    ctx->dirtyObjs.push_back(o);
+  }
+  if (changed) *changed = 1;
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_residency_set_object_active(nomad_ctx *ctx, uint32_t obj,
+                                                          int32_t active, uint32_t *toggled) {
+  if (!ctx || !ctx->sceneReady) return NOMAD_ERR_NOT_READY;
+  if (toggled) *toggled = 0;
+  if (obj >= ctx->objectCount) return fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "object out of range");
+  const nomad_instance_record &r = ctx->instances[obj];
+  uint32_t n = 0;
+  for (uint32_t p = r.primitive_base; p < r.primitive_base + r.primitive_count; ++p) {
+    int32_t ch = 0;
+    nomad_residency_set_primitive_active(ctx, p, active, &ch);
+    n += ch;
+  }
+  // An object toggled with no primitive change still gets its instance record refreshed.
+  if (!ctx->objDirtyFlag[obj]) {
+    ctx->objDirtyFlag[obj] = 1;
+    ctx->dirtyObjs.push_back(obj);
+  }
+  if (toggled) *toggled = n;
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_residency_flush(nomad_ctx *ctx) {
+  if (!ctx || !ctx->sceneReady) return NOMAD_ERR_NOT_READY;
+  std::vector<int64_t> offs;
+  std::vector<int32_t> vals;
+  const auto &L = ctx->layout;
+  for (uint32_t p : ctx->dirtyPrims) {
+    ctx->primDirtyFlag[p] = 0;
+    int64_t pos = L.primPos[p];
+    offs.push_back((int64_t)ctx->pnodeWords + pos * 12 + 3);
+    vals.push_back(ctx->primActive[p] ? (int32_t)p : ~(int32_t)p);
+  }
+  for (uint32_t o : ctx->dirtyObjs) {
+    ctx->objDirtyFlag[o] = 0;
+    bool res = ctx->objActiveCount[o] > 0 && ctx->instances[o].primitive_count > 0;
+    ctx->objResident[o] = res ? 1 : 0;
+    int32_t ref = res ? L.objBlasRef[o] : nomad::kEmptyRef;
+    // Instance record as the reference fills it (Renderer.cpp:5344-5357).
+    ctx->instances[o].blas_root_index = res ? L.objRootNode[o] : -1;
+    int64_t slot = L.objSlot[o];
+    if (slot == -1) {
+      ctx->scene.rootRef = ref;
+    } else if (slot >= 0) {
+      int64_t pair = slot / 2, side = slot % 2;
+      offs.push_back(pair * 16 + (side == 0 ? 3 : 7));
+      vals.push_back(ref);
+    }
+  }
+  ctx->dirtyPrims.clear();
+  ctx->dirtyObjs.clear();
+  if (offs.empty()) return NOMAD_OK;
+  NOMAD_CUDA(ctx, ctx->patchOffs.reserve(offs.size() * 8));
+  NOMAD_CUDA(ctx, ctx->patchVals.reserve(vals.size() * 4));
+  // Synchronous copies: the host vectors go out of scope at return.
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(ctx->patchOffs.p, offs.data(), offs.size() * 8,
+                                  cudaMemcpyHostToDevice, ctx->stream));
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(ctx->patchVals.p, vals.data(), vals.size() * 4,
+                                  cudaMemcpyHostToDevice, ctx->stream));
+  uint32_t n = static_cast<uint32_t>(offs.size());
+  k_patch<<<(n + 255) / 256, 256, 0, ctx->stream>>>(static_cast<int32_t *>(ctx->arena.p),
+                                                    static_cast<const int64_t *>(ctx->patchOffs.p),
+                                                    static_cast<const int32_t *>(ctx->patchVals.p), n);
+  NOMAD_CUDA(ctx, cudaGetLastError());
+  NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_residency_get_instances(nomad_ctx *ctx, nomad_instance_record *out) {
+  if (!ctx || !ctx->sceneReady) return NOMAD_ERR_NOT_READY;
+  if (!out) return NOMAD_ERR_INVALID_ARGUMENT;
+  for (uint32_t o = 0; o < ctx->objectCount; ++o) {
+    out[o] = ctx->instances[o];
+    if (!ctx->objResident[o]) out[o].blas_root_index = -1;
+  }
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_set_kernel(nomad_ctx *ctx, uint32_t kernel) {
+  if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
+  if (kernel == NOMAD_KERNEL_AUTO) kernel = NOMAD_KERNEL_BVH2;
+  if (kernel != NOMAD_KERNEL_BVH2 && kernel != NOMAD_KERNEL_BVH2_PERSIST)
+    return fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "unknown kernel");
+  ctx->kernel = kernel;
+  return NOMAD_OK;
+}
+
+namespace {
+
+// Launches one of the trace kernels over device arrays on `st`.
+enum class Op { Closest, Any, Work };
+
+nomad_status launch(nomad_ctx *ctx, Op op, const float4 *rays, uint64_t n, void *out,
+                    bool countHits, cudaStream_t st) {
+  if (n == 0) return NOMAD_OK;
+  uint32_t *counts = countHits ? static_cast<uint32_t *>(ctx->objHits.p) : nullptr;
+  if (op == Op::Closest && ctx->kernel == NOMAD_KERNEL_BVH2_PERSIST) {
+    NOMAD_CUDA(ctx, cudaMemsetAsync(ctx->cursor.p, 0, 8, st));
+    int perSm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_closest_persist, kPersistBlock, 0);
+    perSm = std::max(perSm, 1);
+    uint64_t blocks = (uint64_t)ctx->smCount * perSm;
+    uint64_t need = (n + kPersistBlock - 1) / kPersistBlock;
+    blocks = std::max<uint64_t>(1, std::min(blocks, need));
+    k_closest_persist<<<(unsigned)blocks, kPersistBlock, 0, st>>>(
+        ctx->scene, rays, n, static_cast<nomad_hit *>(out), counts,
+        static_cast<unsigned long long *>(ctx->cursor.p));
+  } else {
+    uint64_t blocks = (n + kBlock - 1) / kBlock;
+    if (blocks > 0x7fffffffull) return fail(ctx, NOMAD_ERR_LIMIT, "too many rays for one call");
+    if (op == Op::Closest)
+      k_closest<<<(unsigned)blocks, kBlock, 0, st>>>(ctx->scene, rays, n,
+                                                     static_cast<nomad_hit *>(out), counts);
+    else if (op == Op::Any)
+      k_any<<<(unsigned)blocks, kBlock, 0, st>>>(ctx->scene, rays, n, static_cast<uint8_t *>(out));
+    else
+      k_work<<<(unsigned)blocks, kBlock, 0, st>>>(ctx->scene, rays, n, static_cast<uint4 *>(out));
+  }
+  NOMAD_CUDA(ctx, cudaGetLastError());
+  return NOMAD_OK;
+}
+
+// Host-pointer path: rays are copied in and results out in chunks, alternating two streams
+// so one chunk's copies overlap another chunk's traversal.
+nomad_status trace_host(nomad_ctx *ctx, Op op, const nomad_ray *rays, uint64_t n, void *out,
+                        size_t outStride, bool countHits) {
+  NOMAD_CUDA(ctx, ctx->stageIn.reserve(n * sizeof(nomad_ray)));
+  NOMAD_CUDA(ctx, ctx->stageOut.reserve(n * outStride));
+  const uint64_t chunk = std::max<uint64_t>(1 << 20, (n + 7) / 8);
+  cudaEvent_t start;
+  NOMAD_CUDA(ctx, cudaEventCreateWithFlags(&start, cudaEventDisableTiming));
+  NOMAD_CUDA(ctx, cudaEventRecord(start, ctx->stream));
+  std::vector<cudaEvent_t> done;
+  int k = 0;
+  for (uint64_t off = 0; off < n; off += chunk, ++k) {
+    uint64_t m = std::min(chunk, n - off);
+    cudaStream_t s = ctx->copyStreams[k & 1];
+    cudaStreamWaitEvent(s, start, 0);
+    char *din = static_cast<char *>(ctx->stageIn.p) + off * sizeof(nomad_ray);
+    char *dout = static_cast<char *>(ctx->stageOut.p) + off * outStride;
+    NOMAD_CUDA(ctx, cudaMemcpyAsync(din, rays + off, m * sizeof(nomad_ray), cudaMemcpyHostToDevice, s));
+    nomad_status st = launch(ctx, op, reinterpret_cast<const float4 *>(din), m, dout, countHits, s);
+    if (st != NOMAD_OK) return st;
+    NOMAD_CUDA(ctx, cudaMemcpyAsync(static_cast<char *>(out) + off * outStride, dout, m * outStride,
+                                    cudaMemcpyDeviceToHost, s));
+    cudaEvent_t ev;
+    NOMAD_CUDA(ctx, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    NOMAD_CUDA(ctx, cudaEventRecord(ev, s));
+    done.push_back(ev);
+  }
+  for (auto ev : done) {
+    cudaStreamWaitEvent(ctx->stream, ev, 0);
+    cudaEventDestroy(ev);
+  }
+  cudaEventDestroy(start);
+  NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return NOMAD_OK;
+}
+
+nomad_status trace_entry(nomad_ctx *ctx, Op op, const nomad_ray *rays, uint64_t n, void *out,
+                         size_t outStride, uint32_t flags) {
+  if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
+  if (!ctx->sceneReady) return fail(ctx, NOMAD_ERR_NOT_READY, "no scene uploaded");
+  if (n == 0) return NOMAD_OK;
+  if (!rays || !out) return fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "null rays or output");
+  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  bool countHits = (flags & NOMAD_TRACE_COUNT_HITS) != 0 && op == Op::Closest;
+  if (flags & NOMAD_TRACE_DEVICE_POINTERS) {
+    if (reinterpret_cast<uintptr_t>(rays) % 16 != 0)
+      return fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "device rays must be 16-byte aligned");
+    return launch(ctx, op, reinterpret_cast<const float4 *>(rays), n, out, countHits, ctx->stream);
+  }
+  if (is_device_ptr(rays) || is_device_ptr(out))
+    return fail(ctx, NOMAD_ERR_INVALID_ARGUMENT,
+                "device pointer passed without NOMAD_TRACE_DEVICE_POINTERS");
+  return trace_host(ctx, op, rays, n, out, outStride, countHits);
+}
+
+}  // namespace
+
+extern "C" nomad_status nomad_trace_closest(nomad_ctx *ctx, const nomad_ray *rays, uint64_t n,
+                                            nomad_hit *out, uint32_t flags) {
+  return trace_entry(ctx, Op::Closest, rays, n, out, sizeof(nomad_hit), flags);
+}
+
+extern "C" nomad_status nomad_trace_any(nomad_ctx *ctx, const nomad_ray *rays, uint64_t n,
+                                        uint8_t *out, uint32_t flags) {
+  return trace_entry(ctx, Op::Any, rays, n, out, 1, flags);
+}
+
+extern "C" nomad_status nomad_trace_work(nomad_ctx *ctx, const nomad_ray *rays, uint64_t n,
+                                         uint32_t *out, uint32_t flags) {
+  return trace_entry(ctx, Op::Work, rays, n, out, 16, flags);
+}
+
+extern "C" nomad_status nomad_read_object_hits(nomad_ctx *ctx, uint32_t *out) {
+  if (!ctx || !ctx->sceneReady) return NOMAD_ERR_NOT_READY;
+  if (!out) return NOMAD_ERR_INVALID_ARGUMENT;
+  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(out, ctx->objHits.p, (size_t)ctx->objectCount * 4,
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+  NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_reset_object_hits(nomad_ctx *ctx) {
+  if (!ctx || !ctx->sceneReady) return NOMAD_ERR_NOT_READY;
+  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  NOMAD_CUDA(ctx, cudaMemsetAsync(ctx->objHits.p, 0, (size_t)ctx->objectCount * 4, ctx->stream));
+  return NOMAD_OK;
+}

@@ -1,0 +1,362 @@
+"""ctypes bindings for libnomad_rt.so (include/nomad_rt.h, include/nomad_scene.h).
+
+The library is built in-tree (``make -C nomad_b200/csrc``) and loaded from
+``nomad_b200/lib/libnomad_rt.so``. Importing this module never falls back to anything else:
+when the library is missing, :func:`load` raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libnomad_rt.so")
+
+NOMAD_OK = 0
+STATUS_NAMES = {
+    0: "OK", 1: "INVALID_ARGUMENT", 2: "OUT_OF_MEMORY", 3: "CUDA", 4: "NOT_READY",
+    5: "SCENE_INVALID", 6: "DEVICE_STATUS", 7: "UNSUPPORTED", 8: "LIMIT",
+}
+PRIM_SPHERE, PRIM_TRIANGLE, PRIM_RECTANGLE = 0, 1, 2
+TRACE_DEVICE_POINTERS = 1 << 0
+TRACE_COUNT_HITS = 1 << 1
+KERNEL_AUTO, KERNEL_BVH2, KERNEL_BVH2_PERSIST = 0, 1, 2
+
+# numpy views of the ABI structs
+RAY_DTYPE = np.dtype([("ox", "<f4"), ("oy", "<f4"), ("oz", "<f4"), ("tmin", "<f4"),
+                      ("dx", "<f4"), ("dy", "<f4"), ("dz", "<f4"), ("tmax", "<f4")])
+HIT_DTYPE = np.dtype([("inst", "<i4"), ("prim", "<i4"), ("t", "<f4"), ("u", "<f4"), ("v", "<f4")])
+INSTANCE_DTYPE = np.dtype([("blas_root_index", "<i4"), ("primitive_base", "<u4"),
+                           ("primitive_count", "<u4"), ("primitive_index_base", "<u4")])
+
+
+class NomadError(RuntimeError):
+    def __init__(self, status: int, message: str = ""):
+        self.status = status
+        super().__init__(f"nomad status {status} ({STATUS_NAMES.get(status, '?')}): {message}")
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [("prim_count", C.c_uint32), ("prim_type", C.POINTER(C.c_int32)),
+                ("prim_geom", C.POINTER(C.c_float)), ("prim_material", C.POINTER(C.c_float)),
+                ("object_count", C.c_uint32), ("object_first", C.POINTER(C.c_uint32)),
+                ("object_prims", C.POINTER(C.c_uint32))]
+
+
+class SceneBVHView(C.Structure):
+    _fields_ = [("prim_count", C.c_uint32), ("object_count", C.c_uint32),
+                ("bvh_node_count", C.c_uint32), ("tlas_node_count", C.c_uint32),
+                ("bvh_nodes", C.POINTER(C.c_float)), ("tlas_nodes", C.POINTER(C.c_float)),
+                ("prims", C.POINTER(C.c_float)), ("materials", C.POINTER(C.c_float)),
+                ("prim_indices", C.POINTER(C.c_int32)), ("instances", C.c_void_p),
+                ("object_bounds", C.POINTER(C.c_float)), ("max_depth", C.c_uint32)]
+
+
+class Config(C.Structure):
+    _fields_ = [("device", C.c_int32), ("flags", C.c_uint32)]
+
+
+# Every symbol declared in include/*.h, with its ctypes signature.
+_P = C.c_void_p
+SIGNATURES = {
+    # nomad_scene.h
+    "nomad_scenebvh_build": (C.c_int32, [C.POINTER(SceneDesc), C.c_uint32, C.POINTER(_P)]),
+    "nomad_scenebvh_view_get": (C.c_int32, [_P, C.POINTER(SceneBVHView)]),
+    "nomad_scenebvh_free": (None, [_P]),
+    "nomad_synth_icospheres": (C.c_int32, [C.c_uint64, C.c_uint32, C.c_float, C.POINTER(_P)]),
+    "nomad_synth_city": (C.c_int32, [C.c_uint64, C.c_uint32, C.c_float, C.c_uint32, C.c_uint32,
+                                     C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.POINTER(_P)]),
+    "nomad_scene_owned_desc": (C.c_int32, [_P, C.POINTER(SceneDesc)]),
+    "nomad_scene_owned_free": (None, [_P]),
+    # nomad_rt.h
+    "nomad_create": (C.c_int32, [C.POINTER(Config), C.POINTER(_P)]),
+    "nomad_destroy": (C.c_int32, [_P]),
+    "nomad_last_error": (C.c_char_p, [_P]),
+    "nomad_sync": (C.c_int32, [_P]),
+    "nomad_set_stream": (C.c_int32, [_P, _P]),
+    "nomad_get_status": (C.c_int32, [_P, C.POINTER(C.c_uint32)]),
+    "nomad_scene_upload": (C.c_int32, [_P, _P, C.c_uint32, _P, C.c_uint32, _P, _P, _P, C.c_uint32,
+                                       _P, C.c_uint32]),
+    "nomad_residency_set_primitive_active": (C.c_int32, [_P, C.c_uint32, C.c_int32,
+                                                         C.POINTER(C.c_int32)]),
+    "nomad_residency_set_object_active": (C.c_int32, [_P, C.c_uint32, C.c_int32,
+                                                      C.POINTER(C.c_uint32)]),
+    "nomad_residency_flush": (C.c_int32, [_P]),
+    "nomad_residency_get_instances": (C.c_int32, [_P, _P]),
+    "nomad_trace_closest": (C.c_int32, [_P, _P, C.c_uint64, _P, C.c_uint32]),
+    "nomad_trace_any": (C.c_int32, [_P, _P, C.c_uint64, _P, C.c_uint32]),
+    "nomad_set_kernel": (C.c_int32, [_P, C.c_uint32]),
+    "nomad_trace_work": (C.c_int32, [_P, _P, C.c_uint64, _P, C.c_uint32]),
+    "nomad_read_object_hits": (C.c_int32, [_P, _P]),
+    "nomad_reset_object_hits": (C.c_int32, [_P]),
+}
+
+_lib: Optional[C.CDLL] = None
+
+
+def load() -> C.CDLL:
+    """Loads libnomad_rt.so; raises when it is missing (there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C nomad_b200/csrc`")
+    lib = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _ptr(a) -> int:
+    """Address of a contiguous numpy array or a torch tensor."""
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    assert a.flags["C_CONTIGUOUS"], "array must be C-contiguous"
+    return a.ctypes.data
+
+
+def _f(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+# ---------------------------------------------------------------------------------------------
+# Host scenes
+
+
+class HostScene:
+    """A scene description (primitives grouped into objects) as numpy arrays."""
+
+    def __init__(self, prim_type, prim_geom, prim_material, object_first, object_prims):
+        self.prim_type = np.ascontiguousarray(prim_type, dtype=np.int32)
+        self.prim_geom = _f(prim_geom).reshape(-1, 15)
+        self.prim_material = _f(prim_material).reshape(-1, 20)
+        self.object_first = np.ascontiguousarray(object_first, dtype=np.uint32)
+        self.object_prims = np.ascontiguousarray(object_prims, dtype=np.uint32)
+
+    @property
+    def prim_count(self) -> int:
+        return int(self.prim_type.shape[0])
+
+    @property
+    def object_count(self) -> int:
+        return int(self.object_first.shape[0])
+
+    def desc(self) -> SceneDesc:
+        d = SceneDesc()
+        d.prim_count = self.prim_count
+        d.prim_type = self.prim_type.ctypes.data_as(C.POINTER(C.c_int32))
+        d.prim_geom = self.prim_geom.ctypes.data_as(C.POINTER(C.c_float))
+        d.prim_material = self.prim_material.ctypes.data_as(C.POINTER(C.c_float))
+        d.object_count = self.object_count
+        d.object_first = self.object_first.ctypes.data_as(C.POINTER(C.c_uint32))
+        d.object_prims = self.object_prims.ctypes.data_as(C.POINTER(C.c_uint32))
+        return d
+
+    @staticmethod
+    def _from_owned(h) -> "HostScene":
+        lib = load()
+        d = SceneDesc()
+        _check(lib.nomad_scene_owned_desc(h, C.byref(d)))
+        n, m = d.prim_count, d.object_count
+        s = HostScene(np.ctypeslib.as_array(d.prim_type, (n,)).copy(),
+                      np.ctypeslib.as_array(d.prim_geom, (n * 15,)).copy(),
+                      np.ctypeslib.as_array(d.prim_material, (n * 20,)).copy(),
+                      np.ctypeslib.as_array(d.object_first, (m,)).copy(),
+                      np.ctypeslib.as_array(d.object_prims, (m,)).copy())
+        lib.nomad_scene_owned_free(h)
+        return s
+
+
+def synth_icospheres(seed: int, instances: int = 64, extent: float = 100.0) -> HostScene:
+    lib = load()
+    h = _P()
+    _check(lib.nomad_synth_icospheres(seed, instances, extent, C.byref(h)))
+    return HostScene._from_owned(h)
+
+
+def synth_city(seed: int, grid: int = 32, size_m: float = 1000.0, target_tris: int = 2_500_000,
+               median_tris: int = 1000, max_tris: int = 200_000, emissive_quads: int = 64,
+               emissive_tris: int = 0, emissive_sigma: float = 1.5) -> HostScene:
+    lib = load()
+    h = _P()
+    _check(lib.nomad_synth_city(seed, grid, size_m, target_tris, median_tris, max_tris,
+                                emissive_quads, emissive_tris, emissive_sigma, C.byref(h)))
+    return HostScene._from_owned(h)
+
+
+class SceneBVH:
+    """SceneBVH arrays (reference GPU layouts) built from a HostScene, as numpy copies."""
+
+    def __init__(self, scene: HostScene, threads: int = 0):
+        lib = load()
+        h = _P()
+        d = scene.desc()
+        _check(lib.nomad_scenebvh_build(C.byref(d), threads, C.byref(h)))
+        try:
+            v = SceneBVHView()
+            _check(lib.nomad_scenebvh_view_get(h, C.byref(v)))
+            self.prim_count = v.prim_count
+            self.object_count = v.object_count
+            self.bvh_nodes = np.ctypeslib.as_array(v.bvh_nodes, (v.bvh_node_count * 8,)).copy()
+            self.tlas_nodes = np.ctypeslib.as_array(v.tlas_nodes, (v.tlas_node_count * 8,)).copy()
+            self.prims = np.ctypeslib.as_array(v.prims, (v.prim_count * 28,)).copy()
+            self.materials = np.ctypeslib.as_array(v.materials, (v.prim_count * 20,)).copy()
+            self.prim_indices = np.ctypeslib.as_array(v.prim_indices, (v.prim_count,)).copy()
+            inst = (C.c_char * (v.object_count * 16)).from_address(v.instances)
+            self.instances = np.frombuffer(bytes(inst), dtype=INSTANCE_DTYPE).copy()
+            self.object_bounds = np.ctypeslib.as_array(v.object_bounds, (v.object_count * 6,)).copy()
+            self.max_depth = v.max_depth
+        finally:
+            lib.nomad_scenebvh_free(h)
+        self.prim_object = np.repeat(np.arange(self.object_count, dtype=np.int32),
+                                     self.instances["primitive_count"].astype(np.int64))
+
+    @property
+    def bvh_node_count(self) -> int:
+        return self.bvh_nodes.size // 8
+
+    @property
+    def tlas_node_count(self) -> int:
+        return self.tlas_nodes.size // 8
+
+    def geometry_bytes_per_object(self) -> np.ndarray:
+        """Bytes an object occupies on the device: 32 per BLAS node plus 112 + 80 + 4 per
+        primitive (packed primitive, material, index)."""
+        nodes = np.zeros(self.object_count, np.int64)
+        # Node blocks are per object and in object order: count them via the roots.
+        roots = self.instances["blas_root_index"].astype(np.int64)
+        order = np.argsort(roots)
+        bounds = np.append(roots[order], self.bvh_node_count)
+        nodes[order] = np.diff(bounds)
+        return 32 * nodes + 196 * self.instances["primitive_count"].astype(np.int64)
+
+
+def _check(st: int, ctx=None):
+    if st != NOMAD_OK:
+        msg = ""
+        if ctx is not None:
+            m = load().nomad_last_error(ctx)
+            msg = m.decode() if m else ""
+        raise NomadError(st, msg)
+
+
+# ---------------------------------------------------------------------------------------------
+# Device context
+
+
+class Context:
+    """One libnomad_rt context on one CUDA device."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load()
+        cfg = Config(device, 0)
+        h = _P()
+        _check(self.lib.nomad_create(C.byref(cfg), C.byref(h)))
+        self.h = h
+        self.object_count = 0
+        self.prim_count = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.nomad_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, st):
+        _check(st, self.h)
+
+    def upload(self, s: SceneBVH, instances: Optional[np.ndarray] = None):
+        inst = s.instances if instances is None else np.ascontiguousarray(instances, INSTANCE_DTYPE)
+        self._keep = (s, inst)
+        self._ck(self.lib.nomad_scene_upload(
+            self.h, _ptr(s.bvh_nodes), s.bvh_node_count, _ptr(s.tlas_nodes), s.tlas_node_count,
+            _ptr(s.prims), _ptr(s.materials), _ptr(s.prim_indices), s.prim_count, _ptr(inst),
+            s.object_count))
+        self.object_count = s.object_count
+        self.prim_count = s.prim_count
+
+    def set_stream(self, stream_handle: int):
+        self._ck(self.lib.nomad_set_stream(self.h, _P(stream_handle) if stream_handle else None))
+
+    def set_kernel(self, k: int):
+        self._ck(self.lib.nomad_set_kernel(self.h, k))
+
+    def sync(self):
+        self._ck(self.lib.nomad_sync(self.h))
+
+    def status(self) -> int:
+        w = C.c_uint32()
+        self._ck(self.lib.nomad_get_status(self.h, C.byref(w)))
+        return w.value
+
+    # residency
+    def set_object_active(self, obj: int, active: bool) -> int:
+        t = C.c_uint32()
+        self._ck(self.lib.nomad_residency_set_object_active(self.h, obj, int(active), C.byref(t)))
+        return t.value
+
+    def set_primitive_active(self, prim: int, active: bool) -> bool:
+        c = C.c_int32()
+        self._ck(self.lib.nomad_residency_set_primitive_active(self.h, prim, int(active), C.byref(c)))
+        return bool(c.value)
+
+    def flush(self):
+        self._ck(self.lib.nomad_residency_flush(self.h))
+
+    def instances(self) -> np.ndarray:
+        out = np.zeros(self.object_count, INSTANCE_DTYPE)
+        self._ck(self.lib.nomad_residency_get_instances(self.h, _ptr(out)))
+        return out
+
+    # traversal (host arrays)
+    def trace_closest(self, rays: np.ndarray, count_hits: bool = False) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, RAY_DTYPE)
+        out = np.empty(rays.shape[0], HIT_DTYPE)
+        self._ck(self.lib.nomad_trace_closest(self.h, _ptr(rays), rays.shape[0], _ptr(out),
+                                              TRACE_COUNT_HITS if count_hits else 0))
+        return out
+
+    def trace_any(self, rays: np.ndarray) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, RAY_DTYPE)
+        out = np.empty(rays.shape[0], np.uint8)
+        self._ck(self.lib.nomad_trace_any(self.h, _ptr(rays), rays.shape[0], _ptr(out), 0))
+        return out
+
+    def trace_work(self, rays: np.ndarray) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, RAY_DTYPE)
+        out = np.empty((rays.shape[0], 4), np.uint32)
+        self._ck(self.lib.nomad_trace_work(self.h, _ptr(rays), rays.shape[0], _ptr(out), 0))
+        return out
+
+    # traversal (device pointers, e.g. torch tensors); asynchronous on the context stream
+    def trace_closest_dev(self, rays_ptr: int, n: int, hits_ptr: int, count_hits: bool = False):
+        self._ck(self.lib.nomad_trace_closest(self.h, _P(rays_ptr), n, _P(hits_ptr),
+                                              TRACE_DEVICE_POINTERS |
+                                              (TRACE_COUNT_HITS if count_hits else 0)))
+
+    def trace_any_dev(self, rays_ptr: int, n: int, out_ptr: int):
+        self._ck(self.lib.nomad_trace_any(self.h, _P(rays_ptr), n, _P(out_ptr),
+                                          TRACE_DEVICE_POINTERS))
+
+    def trace_work_dev(self, rays_ptr: int, n: int, out_ptr: int):
+        self._ck(self.lib.nomad_trace_work(self.h, _P(rays_ptr), n, _P(out_ptr),
+                                           TRACE_DEVICE_POINTERS))
+
+    def object_hits(self) -> np.ndarray:
+        out = np.zeros(self.object_count, np.uint32)
+        self._ck(self.lib.nomad_read_object_hits(self.h, _ptr(out)))
+        return out
+
+    def reset_object_hits(self):
+        self._ck(self.lib.nomad_reset_object_hits(self.h))

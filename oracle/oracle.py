@@ -1,0 +1,93 @@
+"""ORACLE — test infrastructure only (the checker, never the product).
+
+ctypes wrapper of oracle/_build/liboracle.so, the scalar C++ restatement of the reference's
+traversal (see contract.cpp for the file:line map). Only tests/, __graft_entry__.smoke() and
+bench.py's CPU legs import this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+REF_LIB_PATH = os.path.join(_HERE, "_ref", "libref_nomad.so")
+
+HIT_DTYPE = np.dtype([("inst", "<i4"), ("prim", "<i4"), ("t", "<f4"), ("u", "<f4"), ("v", "<f4")])
+MODE_REFERENCE_ORDER, MODE_NEAR_FIRST, MODE_BRUTE = 0, 1, 2
+
+_lib = None
+_P = C.c_void_p
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} missing: run `make -C oracle`")
+        lib = C.CDLL(LIB_PATH)
+        common = [_P, _P, C.c_uint32, _P, _P, _P, _P, _P, C.c_uint32, _P, C.c_uint64]
+        lib.oracle_trace_closest.argtypes = common + [_P, C.c_int, C.c_uint32]
+        lib.oracle_trace_closest.restype = C.c_int
+        lib.oracle_trace_any.argtypes = common + [_P, C.c_int, C.c_uint32]
+        lib.oracle_trace_any.restype = C.c_int
+        lib.oracle_trace_work.argtypes = common + [_P, _P, C.c_uint32]
+        lib.oracle_trace_work.restype = C.c_int
+        _lib = lib
+    return _lib
+
+
+def _p(a):
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data
+
+
+class OracleScene:
+    """The SceneBVH arrays plus residency state the oracle traverses."""
+
+    def __init__(self, sb, active=None, blas_root=None):
+        self.bvh = np.ascontiguousarray(sb.bvh_nodes, np.float32)
+        self.tlas = np.ascontiguousarray(sb.tlas_nodes, np.float32)
+        self.prims = np.ascontiguousarray(sb.prims, np.float32)
+        self.prim_indices = np.ascontiguousarray(sb.prim_indices, np.int32)
+        self.prim_object = np.ascontiguousarray(sb.prim_object, np.int32)
+        self.object_count = int(sb.object_count)
+        self.active = (np.ones(sb.prim_count, np.uint8) if active is None
+                       else np.ascontiguousarray(active, np.uint8))
+        self.blas_root = (np.ascontiguousarray(sb.instances["blas_root_index"], np.int32)
+                          if blas_root is None else np.ascontiguousarray(blas_root, np.int32))
+
+    def _args(self, rays):
+        rays = np.ascontiguousarray(rays)
+        assert rays.dtype.itemsize == 32
+        return (_p(self.bvh), _p(self.tlas), self.tlas.size // 8, _p(self.prims),
+                _p(self.prim_indices), _p(self.active), _p(self.blas_root), _p(self.prim_object),
+                self.object_count, _p(rays), rays.shape[0]), rays
+
+    def closest(self, rays, mode=MODE_REFERENCE_ORDER, threads=0):
+        args, rays = self._args(rays)
+        out = np.empty(rays.shape[0], HIT_DTYPE)
+        assert load().oracle_trace_closest(*args, _p(out), mode, threads) == 0
+        return out
+
+    def any(self, rays, mode=MODE_REFERENCE_ORDER, threads=0):
+        args, rays = self._args(rays)
+        out = np.empty(rays.shape[0], np.uint8)
+        assert load().oracle_trace_any(*args, _p(out), mode, threads) == 0
+        return out
+
+    def work(self, rays, threads=0):
+        args, rays = self._args(rays)
+        out = np.empty((rays.shape[0], 4), np.uint32)
+        hits = np.empty(rays.shape[0], HIT_DTYPE)
+        assert load().oracle_trace_work(*args, _p(out), _p(hits), threads) == 0
+        return out, hits
+
+
+def algorithmic_bytes(work: np.ndarray) -> np.ndarray:
+    """Bytes per ray: 32 per box tested, 48+4 per primitive test (positions + index),
+    16 per instance record, 48 per closest hit (the hit's frame float4 4..6)."""
+    w = work.astype(np.int64)
+    return 32 * w[:, 0] + 52 * w[:, 1] + 16 * w[:, 2] + 48 * w[:, 3]

@@ -1,0 +1,162 @@
+"""GPU parity: the CUDA traversal against the scalar oracle, through the C ABI.
+
+Bar: (instance, primitive) bit-exact, and t/u/v bit-exact too (the kernels use the oracle's
+operation order with no FMA, so the 4-ulp allowance is not needed); any-hit booleans
+bit-exact; per-object hit counters equal to the oracle's per-object sums.
+"""
+import numpy as np
+import pytest
+
+from tests import raysets
+
+pytestmark = pytest.mark.gpu
+
+
+def _bits(h):
+    return np.ascontiguousarray(h).view(np.int32).reshape(-1, 5)
+
+
+def _assert_hits_equal(got, want):
+    g, w = _bits(got), _bits(want)
+    bad = np.nonzero((g != w).any(1))[0]
+    assert bad.size == 0, f"{bad.size} of {len(g)} rays differ; first {bad[:5]}: got {got[bad[:3]]} want {want[bad[:3]]}"
+
+
+def _rays(sb, seed, n=20000):
+    return np.concatenate([raysets.aimed_rays(sb, n, seed), raysets.random_rays(sb, n, seed + 1),
+                           raysets.edge_case_rays(sb, seed + 2)])
+
+
+@pytest.fixture(scope="module")
+def ctx(nb):
+    c = nb.Context(0)
+    yield c
+    c.close()
+
+
+@pytest.mark.parametrize("kernel", [1, 2])
+@pytest.mark.parametrize("which", ["ico", "city"])
+def test_closest_parity(nb, orc, ctx, ico_scene, small_city, which, kernel):
+    scene, sb = ico_scene if which == "ico" else small_city
+    ctx.upload(sb)
+    ctx.set_kernel(kernel)
+    cam = nb.icosphere_camera(160, 90) if which == "ico" else nb.Camera((0, 60, -180), (0, 0, 0), width=160, height=90)
+    prim = cam.primary_rays(2, seed=3)
+    rays = np.concatenate([prim, _rays(sb, 40)])
+    ref = orc.OracleScene(sb)
+    want = ref.closest(rays)
+    got = ctx.trace_closest(rays)
+    _assert_hits_equal(got, want)
+    bounce = nb.bounce_rays(prim, want[: prim.shape[0]], sb.prims, seed=4)
+    _assert_hits_equal(ctx.trace_closest(bounce), ref.closest(bounce))
+    assert ctx.status() == 0
+    ctx.set_kernel(1)
+
+
+@pytest.mark.parametrize("which", ["ico", "city"])
+def test_any_parity(orc, ctx, ico_scene, small_city, which):
+    scene, sb = ico_scene if which == "ico" else small_city
+    ctx.upload(sb)
+    rays = _rays(sb, 50)
+    # finite tmax: half of each ray's closest distance, so some rays become unoccluded
+    ref = orc.OracleScene(sb)
+    h = ref.closest(rays)
+    short = rays.copy()
+    hit = h["prim"] >= 0
+    short["tmax"][hit] = h["t"][hit] * np.float32(0.5)
+    for rs in (rays, short):
+        got = ctx.trace_any(rs)
+        want = ref.any(rs)
+        assert np.array_equal(got, want), f"{(got != want).sum()} any-hit mismatches"
+
+
+def test_work_counters(orc, ctx, small_city):
+    scene, sb = small_city
+    ctx.upload(sb)
+    rays = _rays(sb, 60, n=5000)
+    w_ref, h_ref = orc.OracleScene(sb).work(rays)
+    w = ctx.trace_work(rays)
+    assert np.array_equal(w, w_ref)
+
+
+def test_object_hit_counters(orc, ctx, small_city):
+    scene, sb = small_city
+    ctx.upload(sb)
+    rays = _rays(sb, 70)
+    ctx.reset_object_hits()
+    h = ctx.trace_closest(rays, count_hits=True)
+    h2 = ctx.trace_closest(rays[::3], count_hits=True)
+    want = (np.bincount(h["inst"][h["prim"] >= 0], minlength=sb.object_count)
+            + np.bincount(h2["inst"][h2["prim"] >= 0], minlength=sb.object_count))
+    assert np.array_equal(ctx.object_hits(), want.astype(np.uint32))
+    ctx.reset_object_hits()
+    assert ctx.object_hits().sum() == 0
+
+
+def test_residency_toggles(orc, ctx, small_city):
+    scene, sb = small_city
+    ctx.upload(sb)
+    rays = _rays(sb, 80)
+    rng = np.random.default_rng(9)
+    off_objs = np.nonzero(rng.random(sb.object_count) < 0.3)[0]
+    off_prims = np.nonzero(rng.random(sb.prim_count) < 0.1)[0]
+    toggled = sum(ctx.set_object_active(int(o), False) for o in off_objs)
+    assert toggled == int(sb.instances["primitive_count"][off_objs].sum())
+    for p in off_prims:
+        ctx.set_primitive_active(int(p), False)
+    ctx.flush()
+    active = np.ones(sb.prim_count, np.uint8)
+    active[off_prims] = 0
+    for o in off_objs:
+        b = sb.instances["primitive_base"][o]
+        active[b:b + sb.instances["primitive_count"][o]] = 0
+    root = sb.instances["blas_root_index"].copy()
+    counts = np.add.reduceat(active.astype(np.int64), sb.instances["primitive_base"].astype(np.int64))
+    root[counts == 0] = -1
+    inst = ctx.instances()
+    assert np.array_equal(inst["blas_root_index"], root)
+    ref = orc.OracleScene(sb, active=active, blas_root=root)
+    _assert_hits_equal(ctx.trace_closest(rays), ref.closest(rays))
+    assert np.array_equal(ctx.trace_any(rays), ref.any(rays))
+    # everything back on
+    for o in range(sb.object_count):
+        ctx.set_object_active(o, True)
+    ctx.flush()
+    _assert_hits_equal(ctx.trace_closest(rays), orc.OracleScene(sb).closest(rays))
+
+
+def test_device_pointer_path(nb, orc, ctx, small_city):
+    import torch
+
+    scene, sb = small_city
+    ctx.upload(sb)
+    rays = _rays(sb, 90)
+    d_rays = torch.from_numpy(rays.view(np.float32).reshape(-1, 8)).cuda()
+    d_hits = torch.empty((rays.shape[0], 5), dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    ctx.trace_closest_dev(d_rays.data_ptr(), rays.shape[0], d_hits.data_ptr())
+    torch.cuda.synchronize()
+    ctx.set_stream(0)
+    got = d_hits.cpu().numpy().view(nb.HIT_DTYPE).reshape(-1)
+    _assert_hits_equal(got, orc.OracleScene(sb).closest(rays))
+
+
+def test_full_city_sample(nb, orc, ctx):
+    """The 2.5M-triangle city at 1080p: a seeded 1/40 sample of the primary rays and their
+    bounces against the oracle, and counters over all primary rays against the hits."""
+    scene = nb.synth_city(seed=2)
+    sb = nb.SceneBVH(scene)
+    ctx.upload(sb)
+    cam = nb.city_camera(1920, 1080)
+    rays = cam.primary_rays(1, seed=5)
+    ctx.reset_object_hits()
+    hits = ctx.trace_closest(rays, count_hits=True)
+    want = np.bincount(hits["inst"][hits["prim"] >= 0], minlength=sb.object_count)
+    assert np.array_equal(ctx.object_hits(), want.astype(np.uint32))
+    idx = np.random.default_rng(1).choice(rays.shape[0], rays.shape[0] // 40, replace=False)
+    ref = orc.OracleScene(sb)
+    _assert_hits_equal(hits[idx], ref.closest(rays[idx]))
+    b = nb.bounce_rays(rays[idx], hits[idx], sb.prims, seed=6)
+    _assert_hits_equal(ctx.trace_closest(b), ref.closest(b))
+    assert ctx.status() == 0
