@@ -64,7 +64,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -74,7 +74,7 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
 
     def __exit__(self, *exc):
         if self.proc:
@@ -84,10 +84,19 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
 
-    def summary(self):
+    def summary(self, t_begin=None, t_end=None):
+        """Median SM clock and active throttle reasons over the samples taken inside
+        [t_begin, t_end] (host wall time; all samples when no window is given, the first
+        sample after t_begin when the window is shorter than the sampling period)."""
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        rows = self.lines
+        if t_begin is not None:
+            inside = [r for r in rows if t_begin - 0.02 <= r[0] <= t_end + 0.02]
+            if not inside:
+                inside = [r for r in rows if r[0] >= t_begin][:1]
+            rows = inside
+        for _, ln in rows:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -105,11 +114,11 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def build_workload(nb, ctx_for_bounces=None):
+def build_workload(nb, spp=SPP):
     scene = nb.synth_city(seed=SEED)
     sb = nb.SceneBVH(scene)
     cam = nb.city_camera(WIDTH, HEIGHT)
-    primary = cam.primary_rays(SPP, seed=SEED + 10)
+    primary = cam.primary_rays(spp, seed=SEED + 10)
     return scene, sb, primary
 
 
@@ -123,11 +132,13 @@ def cpu_leg(sb, rays, budget_s=12.0, use_reference=False):
     from oracle import oracle as orc
     os_ = orc.OracleScene(sb)
     rng = np.random.default_rng(123)
-    sample = rays[rng.permutation(rays.shape[0])[:2_000_000]]
+    sample = rays[rng.permutation(rays.shape[0])]
     done, t0 = 0, time.perf_counter()
-    chunk = 50_000
-    while done < sample.shape[0] and time.perf_counter() - t0 < budget_s:
-        part = sample[done:done + chunk]
+    chunk = 200_000
+    # Cycle through the shuffled batch until the time budget is spent.
+    while time.perf_counter() - t0 < budget_s and done < 20 * sample.shape[0]:
+        off = done % sample.shape[0]
+        part = sample[off:off + chunk]
         if use_reference:
             ref.closest(sb, part, threads=cores)
         else:
@@ -190,8 +201,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="nomad", choices=["nomad", "reference"])
     ap.add_argument("--kernel", type=int, default=0)
-    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--spp", type=int, default=SPP,
+                    help="primary rays per pixel (smaller values give the profiling case)")
     args = ap.parse_args()
+    CONFIG["spp"] = args.spp
     if args.impl == "reference":
         return run_reference(args)
 
@@ -209,7 +223,7 @@ def main():
                                 device_id=torch.device("cuda", local))
 
     t_setup = time.perf_counter()
-    scene, sb, primary = build_workload(nb)
+    scene, sb, primary = build_workload(nb, args.spp)
     ctx = nb.Context(local)
     ctx.upload(sb)
     if args.kernel:
@@ -262,8 +276,9 @@ def main():
            torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
-        time.sleep(0.3)
+        time.sleep(0.5)
         torch.cuda.synchronize()
+        t_begin = time.time()
         start.record(stream)
         for i in range(args.steps):
             ev[i][0].record(stream)
@@ -273,6 +288,8 @@ def main():
             ev[i][2].record(stream)
         end.record(stream)
         torch.cuda.synchronize()
+        t_end = time.time()
+        time.sleep(0.1)
     if world > 1:
         dist.barrier()
     total_ms = start.elapsed_time(end)
@@ -343,7 +360,7 @@ def main():
             "gpu_launches": 2 * args.steps,
             "roofline": roofline,
             "cpu_baseline": cpu,
-            "clocks": clk.summary(),
+            "clocks": clk.summary(t_begin, t_end),
         }
         print(json.dumps(line), flush=True)
     ctx.close()
