@@ -131,6 +131,21 @@ nomad_status nomad_trace_work(nomad_ctx *ctx, const nomad_ray *rays, uint64_t n,
 nomad_status nomad_read_object_hits(nomad_ctx *ctx, uint32_t *out);
 nomad_status nomad_reset_object_hits(nomad_ctx *ctx);
 
+/* ---- allocation-free closest hit (no counterpart in the reference) ----------------------
+ * For callers that cannot allocate GPU memory while tracing: a frame loop whose memory budget
+ * is fully committed to resident geometry, or one that cannot take the implicit device
+ * synchronisation cudaMalloc/cudaFree may cause mid-frame. Same result as nomad_trace_closest
+ * with NOMAD_TRACE_COUNT_HITS on device pointers, but its scratch (work cursor + per-object hit
+ * accumulators) is a fixed static device array, so the call allocates nothing:
+ *   - d_rays[n] in, d_hits[n] and d_object_hits[object_count] (hits of this call only) out,
+ *     all device pointers; asynchronous on the context's stream;
+ *   - scenes with more than 16,384 objects are rejected (NOMAD_ERR_LIMIT);
+ *   - the first call on a device looks up the static array's address; make it before any
+ *     stream capture. The array stays allocated on every GPU that loads the library;
+ *   - all calls share the array: calls that overlap on the GPU race. Serialise them. */
+nomad_status nomad_trace_closest_noalloc(nomad_ctx *ctx, const nomad_ray *d_rays, uint64_t n,
+                                         nomad_hit *d_hits, uint32_t *d_object_hits);
+
 #ifdef __cplusplus
 }
 #endif

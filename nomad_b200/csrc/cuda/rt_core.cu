@@ -552,3 +552,103 @@ extern "C" nomad_status nomad_reset_object_hits(nomad_ctx *ctx) {
   NOMAD_CUDA(ctx, cudaMemsetAsync(ctx->objHits.p, 0, (size_t)ctx->objectCount * 4, ctx->stream));
   return NOMAD_OK;
 }
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free closest hit with per-object hit counts.
+//
+// For callers that cannot allocate GPU memory at trace time: a frame loop that has committed
+// its whole geometry budget to resident objects (every byte is accounted by the residency
+// manager), or one that cannot afford the implicit device synchronisation that cudaMalloc and
+// cudaFree may cause in the middle of a frame. The persistent closest-hit kernel needs scratch
+// memory (a work cursor and per-object hit accumulators); here that scratch is a fixed
+// file-scope device array instead of memory allocated per context or per call.
+//
+// Limits and behaviour:
+//   * at most kNoAllocMaxObjects objects (64 KiB of accumulators + one 256-byte cursor line);
+//     larger scenes are rejected with NOMAD_ERR_LIMIT;
+//   * the array lives in every GPU that loads this library, until the process exits;
+//   * the first call on a device looks up the array's device address (cudaGetSymbolAddress,
+//     with that device current) and caches it; make that first call before any stream capture;
+//   * every call shares the one array: calls on the same device that overlap on the GPU (two
+//     streams, or two contexts) race on it. Serialise them;
+//   * each call clears the cursor and the accumulators it uses before the launch.
+namespace {
+
+constexpr uint32_t kNoAllocMaxObjects = 16384;
+constexpr uint32_t kNoAllocCursorWords = 64;  // one 256-byte line holding the 64-bit cursor
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocCursorWords + kNoAllocMaxObjects];
+
+uint32_t *g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+__global__ void __launch_bounds__(kPersistBlock) k_closest_persist_noalloc(
+    DevScene S, const float4 *__restrict__ rays, uint64_t n, nomad_hit *__restrict__ out,
+    uint32_t *__restrict__ scratch) {
+  unsigned long long *cursor = reinterpret_cast<unsigned long long *>(scratch);
+  uint32_t *counts = scratch + kNoAllocCursorWords;
+  int lane = threadIdx.x & 31;
+  for (;;) {
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(cursor, 32ull);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= n) break;
+    uint64_t i = base + lane;
+    if (i < n) {
+      float4 a = __ldg(rays + 2 * i), b = __ldg(rays + 2 * i + 1);
+      RayP r = prep_ray(a, b);
+      HitRec h;
+      Work w{0, 0, 0};
+      traverse<kStack, false, false>(S, r, b.w, h, w);
+      if (h.prim < 0) h.t = INFINITY;
+      store_hit(out, i, h);
+      warp_count_object_hit(h.prim >= 0 ? h.inst : -1, counts);
+    }
+    __syncwarp();
+  }
+}
+
+}  // namespace
+
+extern "C" nomad_status nomad_trace_closest_noalloc(nomad_ctx *ctx, const nomad_ray *d_rays,
+                                                    uint64_t n, nomad_hit *d_hits,
+                                                    uint32_t *d_object_hits) {
+  if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
+  if (!ctx->sceneReady) return fail(ctx, NOMAD_ERR_NOT_READY, "no scene uploaded");
+  if (ctx->objectCount > kNoAllocMaxObjects)
+    return fail(ctx, NOMAD_ERR_LIMIT,
+                "nomad_trace_closest_noalloc supports at most " +
+                    std::to_string(kNoAllocMaxObjects) + " objects; the scene has " +
+                    std::to_string(ctx->objectCount));
+  if (!d_rays || !d_hits || !d_object_hits)
+    return fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "null device pointer");
+  if (reinterpret_cast<uintptr_t>(d_rays) % 16 != 0)
+    return fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "device rays must be 16-byte aligned");
+  if (ctx->device < 0 || ctx->device >= kNoAllocMaxDevices)
+    return fail(ctx, NOMAD_ERR_LIMIT, "device ordinal too large for the static scratch table");
+  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  uint32_t *scratch = g_noalloc_addr[ctx->device];
+  if (!scratch) {
+    void *p = nullptr;
+    NOMAD_CUDA(ctx, cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    scratch = static_cast<uint32_t *>(p);
+    g_noalloc_addr[ctx->device] = scratch;
+  }
+  size_t clearBytes = (kNoAllocCursorWords + (size_t)ctx->objectCount) * 4;
+  NOMAD_CUDA(ctx, cudaMemsetAsync(scratch, 0, clearBytes, ctx->stream));
+  if (n > 0) {
+    int perSm = 0;
+    NOMAD_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_closest_persist_noalloc,
+                                                                  kPersistBlock, 0));
+    perSm = std::max(perSm, 1);
+    uint64_t blocks = (uint64_t)ctx->smCount * perSm;
+    blocks = std::max<uint64_t>(1, std::min(blocks, (n + kPersistBlock - 1) / kPersistBlock));
+    k_closest_persist_noalloc<<<(unsigned)blocks, kPersistBlock, 0, ctx->stream>>>(
+        ctx->scene, reinterpret_cast<const float4 *>(d_rays), n, d_hits, scratch);
+    NOMAD_CUDA(ctx, cudaGetLastError());
+  }
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(d_object_hits, scratch + kNoAllocCursorWords,
+                                  (size_t)ctx->objectCount * 4, cudaMemcpyDeviceToDevice,
+                                  ctx->stream));
+  return NOMAD_OK;
+}

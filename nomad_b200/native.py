@@ -92,6 +92,7 @@ SIGNATURES = {
     "nomad_trace_work": (C.c_int32, [_P, _P, C.c_uint64, _P, C.c_uint32]),
     "nomad_read_object_hits": (C.c_int32, [_P, _P]),
     "nomad_reset_object_hits": (C.c_int32, [_P]),
+    "nomad_trace_closest_noalloc": (C.c_int32, [_P, _P, C.c_uint64, _P, _P]),
 }
 
 _lib: Optional[C.CDLL] = None
