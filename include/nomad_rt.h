@@ -131,6 +131,51 @@ nomad_status nomad_trace_work(nomad_ctx *ctx, const nomad_ray *rays, uint64_t n,
 nomad_status nomad_read_object_hits(nomad_ctx *ctx, uint32_t *out);
 nomad_status nomad_reset_object_hits(nomad_ctx *ctx);
 
+/* ---- path tracing (replaces pathTraceKernel + rayColor, PathTraceKernel.metal:7-162 and
+ *      PathTracing.h:1069-1881, as a wavefront loop; the reference's per-pixel seed hash is
+ *      replaced by Philox4x32-10 streams) ---------------------------------------------------- */
+/* A pinhole view with the reference's uniforms (populateViewportUniforms, Renderer.cpp:1237-1259)
+ * plus the frame's sampling parameters. */
+typedef struct nomad_view {
+  float camera_pos[3];
+  float viewport_u[3];
+  float viewport_v[3];
+  float first_pixel[3];
+  uint32_t width, height;
+  uint32_t spp;        /* samples (paths) per pixel                                         */
+  uint32_t max_depth;  /* closest-hit segments per path (maxRayDepth)                       */
+  uint32_t seed_lo, seed_hi; /* Philox key                                                  */
+  uint32_t frame;      /* frame index, added to the key's high word                          */
+  uint32_t flags;      /* NOMAD_VIEW_*                                                       */
+} nomad_view;
+
+enum {
+  /* Clamp each sample and each pixel average to [0, 1] like pathTraceKernel (:143) and rayColor
+   * (:1879). Without it the output is HDR radiance. */
+  NOMAD_VIEW_CLAMP = 1u << 0,
+  /* Direct lighting at the first bounce by ReSTIR DI (nomad_set_restir) instead of one-sample NEE. */
+  NOMAD_VIEW_RESTIR = 1u << 1
+};
+
+/* Fills a view from a camera, as populateViewportUniforms does (vertical fov in degrees);
+ * spp = 1, max_depth = 1, seeds 0, flags 0. */
+nomad_status nomad_view_pinhole(const float position[3], const float look_at[3], const float up[3],
+                                float vfov_degrees, uint32_t width, uint32_t height,
+                                nomad_view *out);
+
+/* Renders every view in one batched wavefront launch sequence (paths of all views share the
+ * ray queues). radiance_out receives RGB floats per pixel, views concatenated
+ * (sum of width*height*3 floats); host memory unless NOMAD_TRACE_DEVICE_POINTERS. With
+ * NOMAD_TRACE_COUNT_HITS the per-object counters also count the closest hits of every bounce. */
+nomad_status nomad_render_frame(nomad_ctx *ctx, const nomad_view *views, uint32_t nviews,
+                                float *radiance_out, uint32_t flags);
+
+/* Ray statistics accumulated by nomad_render_frame since the last reset:
+ * out[0] closest-hit rays traced, [1] environment escapes (the reference's stats[2N]),
+ * [2] shadow rays traced, [3] closest hits. */
+nomad_status nomad_render_stats(nomad_ctx *ctx, uint64_t out[4]);
+nomad_status nomad_reset_render_stats(nomad_ctx *ctx);
+
 /* ---- allocation-free closest hit (no counterpart in the reference) ----------------------
  * For callers that cannot allocate GPU memory while tracing: a frame loop whose memory budget
  * is fully committed to resident geometry, or one that cannot take the implicit device

@@ -5,6 +5,7 @@ C ABI in include/nomad_rt.h and include/nomad_scene.h. This package only binds i
 builds host-side ray batches; it has no CPU fallback.
 """
 from .native import (  # noqa: F401
+    VIEW_DTYPE, VIEW_CLAMP, VIEW_RESTIR, view_pinhole,
     Context, HostScene, SceneBVH, NomadError, load, synth_city, synth_icospheres,
     RAY_DTYPE, HIT_DTYPE, INSTANCE_DTYPE, LIB_PATH, SIGNATURES,
     KERNEL_AUTO, KERNEL_BVH2, KERNEL_BVH2_PERSIST, TRACE_COUNT_HITS, TRACE_DEVICE_POINTERS,

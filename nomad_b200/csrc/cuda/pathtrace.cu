@@ -1,0 +1,850 @@
+// Wavefront path tracer: the reference's per-pixel rayColor loop (PathTracing.h:1069-1881,
+// PathTraceKernel.metal:67-162) reorganised as stages over ray queues.
+//
+//   raygen  -> queue A (all paths of all views)
+//   for each bounce:
+//     trace closest (persistent warps over queue A)
+//     shade: miss -> sky; hit -> counters, emission, one-sample NEE (shadow ray appended to
+//            queue S with its unoccluded contribution), BSDF sample (ray appended to queue B)
+//     trace any (persistent warps over queue S)
+//     resolve: add the contribution of every unoccluded shadow ray
+//     swap A and B
+//   finalize: average the samples of each pixel (clamped to [0,1] per sample and per pixel when
+//             NOMAD_VIEW_CLAMP, like pathTraceKernel)
+//
+// Queue appends are warp-aggregated (ballot + one atomic per warp). Every path owns fixed slots
+// (throughput, radiance), so the order of a queue does not change any result, and the
+// contributions of a path are added in the reference's order: emission, then direct light, per
+// bounce. Random numbers come from Philox4x32-10 with key (seed_lo, seed_hi + frame) and counter
+// (pixel, sample, 4*bounce + block, view): block 0 = (light choice, light u1, light u2, lobe
+// choice), block 1 = (direction u1, direction u2, roulette, Fresnel choice); raygen uses bounce 255.
+#include <algorithm>
+#include <cstring>
+
+#include "pt_math.cuh"
+#include "rt_context.h"
+
+using namespace nomad_dev;
+using namespace nomad_pt;
+
+namespace {
+
+constexpr int kPtBlock = 256;
+constexpr int kTraceBlock = 128;
+constexpr int kStackPT = 64;
+constexpr float kPi = 3.14159265358979323846f;
+
+struct ViewDev {
+  float cam[3], vu[3], vv[3], fp[3];
+  float lod;
+  uint32_t w, h, spp, maxDepth, k0, k1, flags, index;
+  unsigned long long pathOffset, pixelOffset;
+};
+
+struct Counters {
+  uint32_t qlen[4];                 // 0, 1: bounce queues; 2: shadow queue
+  unsigned long long cursor[2];     // persistent-trace cursors (closest, any)
+  unsigned long long stats[4];      // segments, escapes, shadow rays, hits
+};
+
+struct Lights {
+  const uint32_t *idx;
+  const float *cdf;
+  uint32_t count;
+  float total;
+};
+
+__device__ __forceinline__ const ViewDev &find_view(const ViewDev *views, uint32_t nviews,
+                                                    unsigned long long pid) {
+  uint32_t lo = 0, hi = nviews - 1;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi + 1) / 2;
+    if (views[mid].pathOffset <= pid) lo = mid;
+    else hi = mid - 1;
+  }
+  return views[lo];
+}
+
+__device__ __forceinline__ void warp_add64(unsigned long long *p, bool pred) {
+  unsigned m = __ballot_sync(__activemask(), pred);
+  int lane = threadIdx.x & 31;
+  if (m && lane == __ffs(__activemask()) - 1) atomicAdd(p, (unsigned long long)__popc(m));
+}
+
+// Warp-aggregated append: returns the slot of this lane (only meaningful when want).
+__device__ __forceinline__ uint32_t warp_append(uint32_t *len, bool want) {
+  unsigned act = __activemask();
+  unsigned m = __ballot_sync(act, want);
+  int lane = threadIdx.x & 31;
+  int leader = __ffs(act) - 1;
+  uint32_t base = 0;
+  if (lane == leader && m) base = atomicAdd(len, (uint32_t)__popc(m));
+  base = __shfl_sync(act, base, leader);
+  return base + __popc(m & ((1u << lane) - 1u));
+}
+
+__device__ __forceinline__ V3 ld3(const float4 &f) { return v3(f.x, f.y, f.z); }
+
+__global__ void __launch_bounds__(kPtBlock) k_raygen(const ViewDev *__restrict__ views, uint32_t nviews,
+                                                      unsigned long long P, float4 *__restrict__ rays,
+                                                      uint32_t *__restrict__ ids, float4 *__restrict__ thr,
+                                                      float4 *__restrict__ rad, Counters *cnt) {
+  unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  for (unsigned long long pid = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; pid < P; pid += stride) {
+    const ViewDev &v = find_view(views, nviews, pid);
+    unsigned long long local = pid - v.pathOffset;
+    uint32_t pixel = (uint32_t)(local / v.spp), sample = (uint32_t)(local % v.spp);
+    uint32_t px = pixel % v.w, py = pixel / v.w;
+    U4 r = philox(U4{pixel, sample, 255u * 4u, v.index}, v.k0, v.k1);
+    float ux = ((float)px + 0.5f) / (float)v.w;
+    float uy = ((float)py + 0.5f) / (float)v.h;
+    float xo = (u01(r.x) - 0.5f) / (float)v.w;
+    float yo = (u01(r.y) - 0.5f) / (float)v.h;
+    float s = ux + xo, t = uy + yo;
+    V3 d = v3(v.fp[0] + s * v.vu[0] + t * v.vv[0] - v.cam[0], v.fp[1] + s * v.vu[1] + t * v.vv[1] - v.cam[1],
+              v.fp[2] + s * v.vu[2] + t * v.vv[2] - v.cam[2]);
+    V3 dir = normalize(d);
+    rays[2 * pid] = make_float4(v.cam[0], v.cam[1], v.cam[2], kRayEps);
+    rays[2 * pid + 1] = make_float4(dir.x, dir.y, dir.z, INFINITY);
+    ids[pid] = (uint32_t)pid;
+    thr[pid] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    rad[pid] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) cnt->qlen[0] = (uint32_t)P;
+}
+
+// Persistent trace over a queue whose length lives on the device.
+template <bool ANY>
+__global__ void __launch_bounds__(kTraceBlock) k_trace_queue(DevScene S, const float4 *__restrict__ rays,
+                                                              const uint32_t *__restrict__ len,
+                                                              unsigned long long *__restrict__ cursor,
+                                                              int32_t *__restrict__ hits, uint8_t *__restrict__ occ) {
+  const uint64_t n = *len;
+  int lane = threadIdx.x & 31;
+  for (;;) {
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(cursor, 32ull);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= n) break;
+    uint64_t i = base + lane;
+    if (i < n) {
+      float4 a = __ldg(rays + 2 * i), b = __ldg(rays + 2 * i + 1);
+      RayP r = prep_ray(a, b);
+      HitRec h;
+      Work w{0, 0, 0};
+      traverse<kStackPT, ANY, false>(S, r, b.w, h, w);
+      if (ANY) {
+        occ[i] = h.prim >= 0 ? 1 : 0;
+      } else {
+        int32_t *o = hits + 5 * i;
+        o[0] = h.inst;
+        o[1] = h.prim;
+        o[2] = __float_as_int(h.prim >= 0 ? h.t : INFINITY);
+        o[3] = __float_as_int(h.u);
+        o[4] = __float_as_int(h.v);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+struct Material {
+  V3 diffuse;
+  float opacity;
+  V3 specular;
+  float shininess;
+  V3 emission;
+  float power;
+  V3 transmission;
+  float ior;
+  float roughness;
+};
+
+// decodeMaterial (PathTracing.h:165-196), untextured.
+__device__ __forceinline__ Material decode_material(const float4 *__restrict__ mats, int32_t prim, float lod) {
+  const float4 *m = mats + 5ll * prim;
+  float4 m0 = __ldg(m), m1 = __ldg(m + 1), m2 = __ldg(m + 2), m3 = __ldg(m + 3), m4 = __ldg(m + 4);
+  Material o;
+  o.diffuse = vmax0(ld3(m0) * lod);
+  o.opacity = clamp01(m0.w);
+  o.specular = vmax0(ld3(m1));
+  o.shininess = fmax_ref(m1.w, 1.0f);
+  o.emission = vmax0(ld3(m2));
+  o.power = fmax_ref(m2.w, 0.0f);
+  o.transmission = vmax0(ld3(m3));
+  o.ior = fmax_ref(m3.w, 1e-3f);
+  o.roughness = clamp01(m4.w);
+  if (o.opacity < 1.0f && luminance(o.transmission) <= 0.0f) {
+    float tr = 1.0f - o.opacity;
+    o.transmission = v3(tr, tr, tr);
+  }
+  return o;
+}
+
+// Geometric normal at a hit, as firstHitBVH sets intersection.normal before the front-face flip
+// (triangle :779-806, rectangle :853-863, sphere :766).
+__device__ __forceinline__ V3 hit_normal(const float4 *__restrict__ prims, int32_t prim, V3 p) {
+  const float4 *g = prims + 7ll * prim;
+  float4 p0 = __ldg(g), p1 = __ldg(g + 1), p2 = __ldg(g + 2), p6 = __ldg(g + 6);
+  int type = (int)p0.w;
+  V3 sn = ld3(p6);
+  if (type == 1) {
+    V3 e1 = ld3(p1) - ld3(p0), e2 = ld3(p2) - ld3(p0);
+    V3 fb = cross(e1, e2);
+    float fl = dot(fb, fb);
+    fb = fl > 0.0f ? normalize(fb) : v3(0.0f, 1.0f, 0.0f);
+    V3 n;
+    float sl = dot(sn, sn);
+    if (sl > kRayEps && finite3(sn)) n = normalize(sn);
+    else n = fb;
+    if (!finite3(n) || dot(n, n) <= kRayEps) n = fb;
+    return n;
+  } else if (type == 2) {
+    V3 fb = cross(ld3(p1), ld3(p2));
+    float fl = dot(fb, fb);
+    fb = (fl > kRayEps && finite3(fb)) ? normalize(fb) : v3(0.0f, 1.0f, 0.0f);
+    float sl = dot(sn, sn);
+    return (sl > kRayEps && finite3(sn)) ? normalize(sn) : fb;
+  }
+  return normalize(p - ld3(p0));
+}
+
+// evaluateDirectLightingBsdf (PathTracing.h:249-293): Lambert + GGX D, Schlick-GGX G, Schlick F.
+__device__ __forceinline__ V3 eval_bsdf(const Material &m, V3 normal, V3 viewDir, V3 lightDir) {
+  V3 n = normalize(normal), v = normalize(viewDir), l = normalize(lightDir);
+  if (!finite3(n) || !finite3(v) || !finite3(l)) return v3(0.0f, 0.0f, 0.0f);
+  float nDotL = fmax_ref(dot(n, l), 0.0f), nDotV = fmax_ref(dot(n, v), 0.0f);
+  if (nDotL <= 0.0f || nDotV <= 0.0f) return v3(0.0f, 0.0f, 0.0f);
+  V3 diffuseColor = vmax0(m.diffuse) * m.opacity;
+  V3 sc = m.specular * m.opacity;
+  V3 specularColor = v3(clamp01(sc.x), clamp01(sc.y), clamp01(sc.z));
+  float rough = clamp01(m.roughness);
+  float alpha = fmax_ref(rough * rough, 0.001f);
+  float alpha2 = alpha * alpha;
+  V3 h = normalize(v + l);
+  float nDotH = fmax_ref(dot(n, h), 0.0f), vDotH = fmax_ref(dot(v, h), 0.0f);
+  float denom = nDotH * nDotH * (alpha2 - 1.0f) + 1.0f;
+  float D = alpha2 / fmax_ref(kPi * denom * denom, kRayEps);
+  float k = alpha + 1.0f;
+  k = (k * k) / 8.0f;
+  float Gv = nDotV / (nDotV * (1.0f - k) + k);
+  float Gl = nDotL / (nDotL * (1.0f - k) + k);
+  float G = Gv * Gl;
+  float Fc = pow5(fmax_ref(1.0f - vDotH, 0.0f));
+  V3 F = specularColor + (v3(1.0f, 1.0f, 1.0f) - specularColor) * Fc;
+  V3 spec = F * (D * G) / fmax_ref(4.0f * nDotL * nDotV, kRayEps);
+  V3 diff = diffuseColor / kPi;
+  return diff + spec;
+}
+
+// buildOrthonormalBasis (Scatter.h:46-52).
+__device__ __forceinline__ void onb(V3 n, V3 &t, V3 &b) {
+  V3 up = fabsf(n.z) < 0.999f ? v3(0.0f, 0.0f, 1.0f) : v3(0.0f, 1.0f, 0.0f);
+  t = normalize(cross(up, n));
+  b = normalize(cross(n, t));
+}
+
+// scatter (Scatter.h:73-152). Returns the weight; writes the new direction.
+__device__ __forceinline__ V3 scatter(V3 inDir, V3 normal, bool frontFace, const Material &m,
+                                      float xiLobe, float u1, float u2, float xiFresnel, V3 &outDir) {
+  float dw = fmax_ref(luminance(m.diffuse) * m.opacity, 0.0f);
+  float sw = fmax_ref(luminance(m.specular) * m.opacity, 0.0f);
+  float tw = fmax_ref(luminance(m.transmission) * (1.0f - m.opacity), 0.0f);
+  if (tw > 0.0f) sw = 0.0f;
+  float total = dw + sw + tw;
+  if (total <= 0.0f) {
+    outDir = normal;
+    return v3(0.0f, 0.0f, 0.0f);
+  }
+  float xi = xiLobe * total;
+  if (xi < dw) {
+    // sampleCosineHemisphere (Scatter.h:54-71)
+    float r = sqrtf(fmax_ref(0.0f, u1));
+    float s, c;
+    sincos_turns(u2, s, c);
+    float x = r * c, y = r * s, z = sqrtf(fmax_ref(0.0f, 1.0f - u1));
+    V3 t, b;
+    onb(normal, t, b);
+    outDir = normalize(t * x + b * y + normal * z);
+    float prob = fmax_ref(dw / total, 1e-4f);
+    return m.diffuse * m.opacity / prob;
+  }
+  xi = xi - dw;
+  if (xi < sw) {
+    V3 refl = reflect(inDir, normal);
+    float exponent = fmax_ref(m.shininess, 1.0f);
+    if (m.roughness > 0.0f) {
+      float smooth = clamp01(1.0f - m.roughness);
+      float re = fmax_ref(1.0f, smooth * smooth * 256.0f);
+      exponent = fmax_ref(exponent, re);
+    }
+    float cosT = pow_pos(u1, 1.0f / (exponent + 1.0f));
+    float sinT = sqrtf(fmax_ref(0.0f, 1.0f - cosT * cosT));
+    float s, c;
+    sincos_turns(u2, s, c);
+    V3 t, b;
+    onb(refl, t, b);
+    outDir = normalize(t * (sinT * c) + b * (sinT * s) + refl * cosT);
+    float prob = fmax_ref(sw / total, 1e-4f);
+    return m.specular / prob;
+  }
+  float prob = fmax_ref(tw / total, 1e-4f);
+  float eta = fmax_ref(m.ior, 1e-3f);
+  float ratio = frontFace ? (1.0f / eta) : eta;
+  // mirrorAngle (Scatter.h:31-44)
+  float cosTheta = dot(-inDir, normal);
+  float sinTheta = sqrtf(fmax_ref(0.0f, 1.0f - cosTheta * cosTheta));
+  float r0 = (1.0f - ratio) / (1.0f + ratio);
+  r0 = r0 * r0;
+  float reflectance = r0 + (1.0f - r0) * pow5(1.0f - cosTheta);
+  if ((ratio * sinTheta > 1.0f) || (reflectance > xiFresnel)) {
+    outDir = reflect(inDir, normal);
+    return m.specular / prob;
+  }
+  // refract (MSL definition): k = 1 - eta^2 (1 - dot(n,i)^2)
+  float d = dot(normal, inDir);
+  float k = 1.0f - ratio * ratio * (1.0f - d * d);
+  if (k < 0.0f) {
+    outDir = reflect(inDir, normal);
+    return m.specular / prob;
+  }
+  V3 refr = inDir * ratio - normal * (ratio * d + sqrtf(k));
+  if (!finite3(refr)) {
+    outDir = reflect(inDir, normal);
+    return m.specular / prob;
+  }
+  outDir = normalize(refr);
+  return m.transmission / prob;
+}
+
+// sampleLightPoint (PathTracing.h:582-643).
+__device__ __forceinline__ bool sample_light(const float4 *__restrict__ prims, uint32_t lp, float u1, float u2,
+                                             V3 &pos, V3 &nrm, float &area) {
+  const float4 *g = prims + 7ll * lp;
+  float4 p0 = __ldg(g), p1 = __ldg(g + 1), p2 = __ldg(g + 2);
+  int type = (int)p0.w;
+  if (type == 0) {
+    float radius = p1.x;
+    if (radius <= 0.0f) return false;
+    float z = 2.0f * u1 - 1.0f;
+    float s, c;
+    sincos_turns(u2, s, c);
+    float r = sqrtf(fmax_ref(0.0f, 1.0f - z * z));
+    V3 dir = v3(r * c, r * s, z);
+    pos = ld3(p0) + dir * radius;
+    nrm = dir;
+    area = 4.0f * kPi * radius * radius;
+    return area > 0.0f;
+  } else if (type == 1) {
+    float su1 = sqrtf(u1);
+    float b0 = 1.0f - su1, b1 = su1 * (1.0f - u2), b2 = su1 * u2;
+    V3 v0 = ld3(p0), v1 = ld3(p1), v2 = ld3(p2);
+    pos = v0 * b0 + v1 * b1 + v2 * b2;
+    V3 n = cross(v1 - v0, v2 - v0);
+    float ln = length(n);
+    if (ln <= 0.0f) return false;
+    nrm = n / ln;
+    area = 0.5f * ln;
+    return area > 0.0f;
+  } else if (type == 2) {
+    float su = u1 * 2.0f - 1.0f, sv = u2 * 2.0f - 1.0f;
+    V3 c = ld3(p0), e1 = ld3(p1), e2 = ld3(p2);
+    pos = c + e1 * su + e2 * sv;
+    V3 n = cross(e1, e2);
+    float ln = length(n);
+    if (ln <= 0.0f) return false;
+    nrm = n / ln;
+    area = 4.0f * ln;
+    return area > 0.0f;
+  }
+  return false;
+}
+
+// selectLightOffset (PathTracing.h:219-235).
+__device__ __forceinline__ uint32_t select_light(float xi, const Lights &L) {
+  float target = xi * L.total;
+  uint32_t lo = 0, hi = L.count;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) / 2;
+    if (__ldg(L.cdf + mid) < target) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo < L.count - 1 ? lo : L.count - 1;
+}
+
+__global__ void __launch_bounds__(kPtBlock) k_shade(
+    uint32_t depth, const ViewDev *__restrict__ views, uint32_t nviews, const float4 *__restrict__ qRays,
+    const uint32_t *__restrict__ qIds, const int32_t *__restrict__ hits, float4 *__restrict__ nRays,
+    uint32_t *__restrict__ nIds, float4 *__restrict__ sRays, uint32_t *__restrict__ sIds,
+    float4 *__restrict__ sContrib, float4 *__restrict__ thr, float4 *__restrict__ rad,
+    const float4 *__restrict__ prims, const float4 *__restrict__ mats, Lights L, Counters *cnt, int cur,
+    uint32_t *__restrict__ objHits, int restirDepth0) {
+  const uint32_t n = cnt->qlen[cur];
+  uint32_t *nextLen = &cnt->qlen[cur ^ 1];
+  uint32_t *shadowLen = &cnt->qlen[2];
+  uint32_t stride = gridDim.x * blockDim.x;
+  uint32_t iters = (n + stride - 1) / stride;
+  for (uint32_t it = 0; it < iters; ++it) {
+    uint32_t i = it * stride + blockIdx.x * blockDim.x + threadIdx.x;
+    bool live = i < n;
+    bool hit = false, wantShadow = false, wantNext = false;
+    uint32_t pid = 0;
+    float4 sA = make_float4(0, 0, 0, 0), sB = sA, sC = sA, nA = sA, nB = sA;
+    int32_t inst = -1;
+    if (live) {
+      pid = qIds[i];
+      float4 ra = qRays[2 * i], rb = qRays[2 * i + 1];
+      V3 o = ld3(ra), d = ld3(rb);
+      const int32_t *h = hits + 5 * i;
+      int32_t prim = h[1];
+      float t = __int_as_float(h[2]);
+      float4 T = thr[pid];
+      V3 tp = ld3(T);
+      const ViewDev &v = find_view(views, nviews, pid);
+      if (prim < 0) {
+        // Sky (PathTracing.h:1211-1213): mix(1, (0.6, 0.7, 1.0), 0.5 (d.y + 1)).
+        V3 ud = normalize(d);
+        float s = 0.5f * (ud.y + 1.0f);
+        V3 sky = v3(1.0f + (0.6f - 1.0f) * s, 1.0f + (0.7f - 1.0f) * s, 1.0f + (1.0f - 1.0f) * s);
+        float4 R = rad[pid];
+        rad[pid] = make_float4(R.x + tp.x * sky.x, R.y + tp.y * sky.y, R.z + tp.z * sky.z, R.w);
+      } else {
+        hit = true;
+        inst = h[0];
+        unsigned long long local = pid - v.pathOffset;
+        uint32_t pixel = (uint32_t)(local / v.spp), sample = (uint32_t)(local % v.spp);
+        U4 b0 = philox(U4{pixel, sample, depth * 4u + 0u, v.index}, v.k0, v.k1);
+        U4 b1 = philox(U4{pixel, sample, depth * 4u + 1u, v.index}, v.k0, v.k1);
+        V3 p = v3(o.x + t * d.x, o.y + t * d.y, o.z + t * d.z);
+        V3 nrm = hit_normal(prims, prim, p);
+        bool front = dot(nrm, d) < 0.0f;
+        if (!front) nrm = -nrm;
+        Material m = decode_material(mats, prim, v.lod);
+        float4 R = rad[pid];
+        if (m.power * luminance(m.emission) > 0.0f) {
+          R.x = R.x + tp.x * m.emission.x * m.power;
+          R.y = R.y + tp.y * m.emission.y * m.power;
+          R.z = R.z + tp.z * m.emission.z * m.power;
+          rad[pid] = R;
+        }
+        V3 dc = m.diffuse * m.opacity;
+        bool restirHere = restirDepth0 && depth == 0 && (v.flags & NOMAD_VIEW_RESTIR);
+        if (!restirHere && luminance(dc) > 0.0f && L.count > 0 && L.total > 0.0f) {
+          uint32_t off = select_light(u01(b0.x), L);
+          uint32_t lp = __ldg(L.idx + off);
+          if ((int32_t)lp != prim) {
+            V3 lpos, lnrm;
+            float area = 0.0f;
+            if (sample_light(prims, lp, u01(b0.y), u01(b0.z), lpos, lnrm, area) && area > 0.0f) {
+              V3 toL = lpos - p;
+              float dist2 = dot(toL, toL);
+              if (dist2 > kRayEps) {
+                float dist = sqrtf(dist2);
+                V3 wi = toL / dist;
+                float cosT = fmax_ref(dot(nrm, wi), 0.0f);
+                float cosL = fmax_ref(dot(lnrm, -wi), 0.0f);
+                if (cosT > 0.0f && cosL > 0.0f) {
+                  float cur_ = __ldg(L.cdf + off);
+                  float prev = off > 0 ? __ldg(L.cdf + off - 1) : 0.0f;
+                  float wgt = cur_ - prev;
+                  float lpdf = (L.total > 0.0f && wgt > 0.0f) ? wgt / L.total : 0.0f;
+                  if (lpdf > 0.0f) {
+                    float pdfArea = 1.0f / area;
+                    float pdfSolid = pdfArea * dist2 / cosL;
+                    float totalPdf = lpdf * pdfSolid;
+                    if (totalPdf > 0.0f) {
+                      Material lm = decode_material(mats, (int32_t)lp, 1.0f);
+                      V3 lrad = lm.emission * lm.power;
+                      V3 view = normalize(-d);
+                      V3 bsdf = eval_bsdf(m, nrm, view, wi);
+                      V3 c = tp * bsdf * lrad * (cosT / totalPdf);
+                      float tmax = dist - kRayEps;
+                      if (tmax < kRayEps) tmax = kRayEps;
+                      V3 so = p + nrm * 0.0005f;
+                      sA = make_float4(so.x, so.y, so.z, kRayEps);
+                      sB = make_float4(wi.x, wi.y, wi.z, tmax);
+                      sC = make_float4(c.x, c.y, c.z, 0.0f);
+                      wantShadow = true;
+                    }
+                  }
+                }
+              }
+            }
+          }
+        }
+        V3 nd;
+        V3 wgt = scatter(d, nrm, front, m, u01(b0.w), u01(b1.x), u01(b1.y), u01(b1.w), nd);
+        V3 bias = dot(nd, nrm) < 0.0f ? -nrm : nrm;
+        V3 no = p + bias * kRayEps;
+        V3 nt = tp * wgt;
+        bool alive = true;
+        if (depth >= 5) {
+          float pm = fmax_ref(nt.x, fmax_ref(nt.y, nt.z));
+          if (u01(b1.z) >= pm) alive = false;
+          else nt = nt / pm;
+        }
+        thr[pid] = make_float4(nt.x, nt.y, nt.z, T.w);
+        bool zero = nt.x == 0.0f && nt.y == 0.0f && nt.z == 0.0f;
+        if (alive && !zero && depth + 1 < v.maxDepth) {
+          nA = make_float4(no.x, no.y, no.z, kRayEps);
+          nB = make_float4(nd.x, nd.y, nd.z, INFINITY);
+          wantNext = true;
+        }
+      }
+    }
+    // Counters (warp-aggregated): segments, escapes, hits, per-object hits.
+    warp_add64(&cnt->stats[0], live);
+    warp_add64(&cnt->stats[1], live && !hit);
+    warp_add64(&cnt->stats[3], hit);
+    if (objHits) {
+      unsigned act = __activemask();
+      int key = hit ? inst : -1;
+      unsigned peers = __match_any_sync(act, key);
+      if (hit && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(objHits + inst, (uint32_t)__popc(peers));
+    }
+    uint32_t ss = warp_append(shadowLen, wantShadow);
+    if (wantShadow) {
+      sRays[2 * ss] = sA;
+      sRays[2 * ss + 1] = sB;
+      sIds[ss] = pid;
+      sContrib[ss] = sC;
+    }
+    uint32_t ns = warp_append(nextLen, wantNext);
+    if (wantNext) {
+      nRays[2 * ns] = nA;
+      nRays[2 * ns + 1] = nB;
+      nIds[ns] = pid;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kPtBlock) k_resolve(const uint32_t *__restrict__ sIds,
+                                                       const float4 *__restrict__ sContrib,
+                                                       const uint8_t *__restrict__ occ, float4 *__restrict__ rad,
+                                                       Counters *cnt) {
+  uint32_t n = cnt->qlen[2];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (occ[i]) continue;
+    uint32_t pid = sIds[i];
+    float4 c = sContrib[i], R = rad[pid];
+    rad[pid] = make_float4(R.x + c.x, R.y + c.y, R.z + c.z, R.w);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) cnt->stats[2] += n;
+}
+
+// Clears the next-bounce and shadow queue lengths and the trace cursors before a bounce.
+__global__ void k_bounce_reset(Counters *cnt, int cur) {
+  cnt->qlen[cur ^ 1] = 0;
+  cnt->qlen[2] = 0;
+  cnt->cursor[0] = 0;
+  cnt->cursor[1] = 0;
+}
+
+__global__ void __launch_bounds__(kPtBlock) k_finalize(const ViewDev *__restrict__ views, uint32_t nviews,
+                                                        unsigned long long totalPixels,
+                                                        const float4 *__restrict__ rad, float *__restrict__ out) {
+  for (unsigned long long q = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; q < totalPixels;
+       q += (unsigned long long)gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = nviews - 1;
+    while (lo < hi) {
+      uint32_t mid = (lo + hi + 1) / 2;
+      if (views[mid].pixelOffset <= q) lo = mid;
+      else hi = mid - 1;
+    }
+    const ViewDev &v = views[lo];
+    unsigned long long pixel = q - v.pixelOffset;
+    bool clampOn = (v.flags & NOMAD_VIEW_CLAMP) != 0;
+    float ax = 0.0f, ay = 0.0f, az = 0.0f;
+    for (uint32_t s = 0; s < v.spp; ++s) {
+      float4 R = rad[v.pathOffset + pixel * v.spp + s];
+      float x = R.x, y = R.y, z = R.z;
+      if (clampOn) {
+        x = clamp01(x);
+        y = clamp01(y);
+        z = clamp01(z);
+      }
+      ax = ax + x;
+      ay = ay + y;
+      az = az + z;
+    }
+    float ns = (float)v.spp;
+    ax = ax / ns;
+    ay = ay / ns;
+    az = az / ns;
+    if (clampOn) {
+      ax = clamp01(ax);
+      ay = clamp01(ay);
+      az = clamp01(az);
+    }
+    out[3 * q + 0] = ax;
+    out[3 * q + 1] = ay;
+    out[3 * q + 2] = az;
+  }
+}
+
+}  // namespace
+
+// Light CDF over active emissive primitives (Renderer.cpp:5161-5211; primitiveArea :1462-1480).
+void nomad_build_lights(const nomad_ctx *ctx, LightTables &out) {
+  out = LightTables();
+  const float *P = ctx->hostPrims.data();
+  const float *M = ctx->hostMaterials.data();
+  out.pdfLookup.assign(ctx->primCount, 0.0f);
+  float total = 0.0f;
+  for (uint32_t i = 0; i < ctx->primCount; ++i) {
+    if (!ctx->primActive[i]) continue;
+    if (!ctx->objResident[ctx->layout.primObject[i]]) continue;
+    const float *m = M + 20ull * i;
+    float strength = m[11] * (m[8] * 0.2126f + m[9] * 0.7152f + m[10] * 0.0722f);
+    if (!(strength > 0.0f)) continue;
+    const float *g = P + 28ull * i;
+    int type = (int)g[3];
+    float area = 0.0f;
+    if (type == 0) {
+      float r = g[4];
+      area = 4.0f * 3.14159265358979323846f * r * r;
+    } else {
+      float ax, ay, az, bx, by, bz;
+      if (type == 1) {
+        ax = g[4] - g[0]; ay = g[5] - g[1]; az = g[6] - g[2];
+        bx = g[8] - g[0]; by = g[9] - g[1]; bz = g[10] - g[2];
+      } else {
+        ax = g[4]; ay = g[5]; az = g[6];
+        bx = g[8]; by = g[9]; bz = g[10];
+      }
+      float cx = ay * bz - az * by, cy = az * bx - ax * bz, cz = ax * by - ay * bx;
+      float len = std::sqrt(cx * cx + cy * cy + cz * cz);
+      area = type == 1 ? 0.5f * len : 4.0f * len;
+    }
+    if (!(area > 0.0f)) continue;
+    float w = area * strength;
+    if (!(w > 0.0f)) continue;
+    total += w;
+    out.indices.push_back(i);
+    out.cdf.push_back(total);
+  }
+  out.total = total;
+  if (total > 0.0f) {
+    float prev = 0.0f;
+    for (size_t k = 0; k < out.cdf.size(); ++k) {
+      float w = out.cdf[k] - prev;
+      prev = out.cdf[k];
+      if (w <= 0.0f) continue;
+      out.pdfLookup[out.indices[k]] = w / total;
+    }
+  }
+}
+
+namespace {
+
+nomad_status upload_lights(nomad_ctx *ctx) {
+  FrameState &F = ctx->frame;
+  if (!F.lightsDirty) return NOMAD_OK;
+  LightTables L;
+  nomad_build_lights(ctx, L);
+  size_t n = std::max<size_t>(1, L.indices.size());
+  NOMAD_CUDA(ctx, F.lightIdx.reserve(n * 4));
+  NOMAD_CUDA(ctx, F.lightCdf.reserve(n * 4));
+  NOMAD_CUDA(ctx, F.lightPdf.reserve((size_t)ctx->primCount * 4));
+  if (!L.indices.empty()) {
+    NOMAD_CUDA(ctx, cudaMemcpy(F.lightIdx.p, L.indices.data(), L.indices.size() * 4, cudaMemcpyHostToDevice));
+    NOMAD_CUDA(ctx, cudaMemcpy(F.lightCdf.p, L.cdf.data(), L.cdf.size() * 4, cudaMemcpyHostToDevice));
+  }
+  NOMAD_CUDA(ctx, cudaMemcpy(F.lightPdf.p, L.pdfLookup.data(), (size_t)ctx->primCount * 4, cudaMemcpyHostToDevice));
+  F.lightCount = static_cast<uint32_t>(L.indices.size());
+  F.lightTotal = L.total;
+  F.lightsDirty = false;
+  return NOMAD_OK;
+}
+
+int persist_blocks(nomad_ctx *ctx, const void *fn, int block) {
+  int perSm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, fn, block, 0);
+  return ctx->smCount * std::max(perSm, 1);
+}
+
+}  // namespace
+
+extern "C" nomad_status nomad_view_pinhole(const float pos[3], const float look[3], const float up[3],
+                                           float vfov, uint32_t width, uint32_t height, nomad_view *out) {
+  if (!pos || !look || !up || !out || width == 0 || height == 0 || !(vfov > 0.0f) || !(vfov < 180.0f))
+    return NOMAD_ERR_INVALID_ARGUMENT;
+  // populateViewportUniforms (Renderer.cpp:1237-1259).
+  auto norm = [](float v[3]) {
+    float l = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    v[0] /= l; v[1] /= l; v[2] /= l;
+  };
+  auto cross = [](const float a[3], const float b[3], float o[3]) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+  };
+  float aspect = (float)width / (float)height;
+  float fovRad = vfov * (3.14159265358979323846f / 180.0f);
+  float halfH = std::tan(fovRad * 0.5f);
+  float halfW = aspect * halfH;
+  float fwd[3] = {look[0] - pos[0], look[1] - pos[1], look[2] - pos[2]};
+  norm(fwd);
+  float w[3] = {-fwd[0], -fwd[1], -fwd[2]};
+  norm(w);
+  float u[3], v[3];
+  cross(up, w, u);
+  norm(u);
+  cross(w, u, v);
+  std::memset(out, 0, sizeof(*out));
+  for (int k = 0; k < 3; ++k) {
+    out->camera_pos[k] = pos[k];
+    out->viewport_u[k] = u[k] * (2.0f * halfW);
+    out->viewport_v[k] = -v[k] * (2.0f * halfH);
+  }
+  for (int k = 0; k < 3; ++k)
+    out->first_pixel[k] = pos[k] - w[k] - out->viewport_u[k] * 0.5f - out->viewport_v[k] * 0.5f;
+  out->width = width;
+  out->height = height;
+  out->spp = 1;
+  out->max_depth = 1;
+  return NOMAD_OK;
+}
+
+nomad_status nomad_restir_pass(nomad_ctx *ctx, const void *viewsDev, uint32_t nviews, const nomad_view *views);
+
+extern "C" nomad_status nomad_render_frame(nomad_ctx *ctx, const nomad_view *views, uint32_t nviews,
+                                           float *out, uint32_t flags) {
+  if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
+  if (!ctx->sceneReady) return nomad_fail(ctx, NOMAD_ERR_NOT_READY, "no scene uploaded");
+  if (!views || nviews == 0 || !out) return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "no views or output");
+  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  std::vector<ViewDev> vd(nviews);
+  unsigned long long P = 0, pixels = 0;
+  uint32_t maxDepth = 0;
+  for (uint32_t i = 0; i < nviews; ++i) {
+    const nomad_view &v = views[i];
+    if (v.width == 0 || v.height == 0 || v.spp == 0 || v.max_depth == 0 || v.max_depth > 64)
+      return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "view " + std::to_string(i) + " has a zero size, spp or depth");
+    ViewDev &d = vd[i];
+    for (int k = 0; k < 3; ++k) {
+      d.cam[k] = v.camera_pos[k];
+      d.vu[k] = v.viewport_u[k];
+      d.vv[k] = v.viewport_v[k];
+      d.fp[k] = v.first_pixel[k];
+    }
+    // Level-of-detail attenuation of the diffuse colour (PathTraceKernel.metal:78-81).
+    float dx[3] = {v.viewport_u[0] / (float)v.width, v.viewport_u[1] / (float)v.width, v.viewport_u[2] / (float)v.width};
+    float dy[3] = {v.viewport_v[0] / (float)v.height, v.viewport_v[1] / (float)v.height, v.viewport_v[2] / (float)v.height};
+    float cx = dx[1] * dy[2] - dx[2] * dy[1], cy = dx[2] * dy[0] - dx[0] * dy[2], cz = dx[0] * dy[1] - dx[1] * dy[0];
+    float fp = std::sqrt(cx * cx + cy * cy + cz * cz);
+    d.lod = 1.0f / (1.0f + fp);
+    d.w = v.width;
+    d.h = v.height;
+    d.spp = v.spp;
+    d.maxDepth = v.max_depth;
+    d.k0 = v.seed_lo;
+    d.k1 = v.seed_hi + v.frame;
+    d.flags = v.flags;
+    d.index = i;
+    d.pathOffset = P;
+    d.pixelOffset = pixels;
+    P += (unsigned long long)v.width * v.height * v.spp;
+    pixels += (unsigned long long)v.width * v.height;
+    maxDepth = std::max(maxDepth, v.max_depth);
+  }
+  if (P > 0xffffffffull) return nomad_fail(ctx, NOMAD_ERR_LIMIT, "more than 2^32 paths in one frame");
+  FrameState &F = ctx->frame;
+  nomad_status st = upload_lights(ctx);
+  if (st != NOMAD_OK) return st;
+  if (F.capacity < P) {
+    NOMAD_CUDA(ctx, F.thr.reserve(P * 16));
+    NOMAD_CUDA(ctx, F.rad.reserve(P * 16));
+    for (int k = 0; k < 2; ++k) {
+      NOMAD_CUDA(ctx, F.qRays[k].reserve(P * 32));
+      NOMAD_CUDA(ctx, F.qIds[k].reserve(P * 4));
+    }
+    NOMAD_CUDA(ctx, F.hits.reserve(P * 20));
+    NOMAD_CUDA(ctx, F.sRays.reserve(P * 32));
+    NOMAD_CUDA(ctx, F.sIds.reserve(P * 4));
+    NOMAD_CUDA(ctx, F.sContrib.reserve(P * 16));
+    NOMAD_CUDA(ctx, F.sOcc.reserve(P));
+    F.capacity = P;
+  }
+  if (F.counters.bytes == 0) {
+    NOMAD_CUDA(ctx, F.counters.reserve(sizeof(Counters)));
+    NOMAD_CUDA(ctx, cudaMemset(F.counters.p, 0, sizeof(Counters)));
+  }
+  NOMAD_CUDA(ctx, F.views.reserve(nviews * sizeof(ViewDev)));
+  cudaStream_t s = ctx->stream;
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(F.views.p, vd.data(), nviews * sizeof(ViewDev), cudaMemcpyHostToDevice, s));
+  // The view table is read by the kernels below; keep the host copy alive until they ran.
+  NOMAD_CUDA(ctx, cudaStreamSynchronize(s));
+
+  const ViewDev *V = F.views.as<const ViewDev>();
+  Counters *C = F.counters.as<Counters>();
+  int gridPT = ctx->smCount * 8;
+  k_raygen<<<gridPT, kPtBlock, 0, s>>>(V, nviews, P, F.qRays[0].as<float4>(), F.qIds[0].as<uint32_t>(),
+                                      F.thr.as<float4>(), F.rad.as<float4>(), C);
+  NOMAD_CUDA(ctx, cudaGetLastError());
+  Lights L{F.lightIdx.as<const uint32_t>(), F.lightCdf.as<const float>(), F.lightCount, F.lightTotal};
+  uint32_t *objHits = (flags & NOMAD_TRACE_COUNT_HITS) ? ctx->objHits.as<uint32_t>() : nullptr;
+  int gClosest = persist_blocks(ctx, (const void *)k_trace_queue<false>, kTraceBlock);
+  int gAny = persist_blocks(ctx, (const void *)k_trace_queue<true>, kTraceBlock);
+  bool anyRestir = false;
+  for (uint32_t i = 0; i < nviews; ++i) anyRestir |= (views[i].flags & NOMAD_VIEW_RESTIR) != 0;
+  int cur = 0;
+  for (uint32_t depth = 0; depth < maxDepth; ++depth) {
+    k_bounce_reset<<<1, 1, 0, s>>>(C, cur);
+    k_trace_queue<false><<<gClosest, kTraceBlock, 0, s>>>(ctx->scene, F.qRays[cur].as<const float4>(), &C->qlen[cur],
+                                                         &C->cursor[0], F.hits.as<int32_t>(), nullptr);
+    if (depth == 0 && anyRestir) {
+      st = nomad_restir_pass(ctx, F.views.p, nviews, views);
+      if (st != NOMAD_OK) return st;
+    }
+    k_shade<<<gridPT, kPtBlock, 0, s>>>(depth, V, nviews, F.qRays[cur].as<const float4>(), F.qIds[cur].as<const uint32_t>(),
+                                       F.hits.as<const int32_t>(), F.qRays[cur ^ 1].as<float4>(),
+                                       F.qIds[cur ^ 1].as<uint32_t>(), F.sRays.as<float4>(), F.sIds.as<uint32_t>(),
+                                       F.sContrib.as<float4>(), F.thr.as<float4>(), F.rad.as<float4>(),
+                                       ctx->prims.as<const float4>(), ctx->materials.as<const float4>(), L, C, cur,
+                                       objHits, anyRestir ? 1 : 0);
+    k_trace_queue<true><<<gAny, kTraceBlock, 0, s>>>(ctx->scene, F.sRays.as<const float4>(), &C->qlen[2], &C->cursor[1],
+                                                    nullptr, F.sOcc.as<uint8_t>());
+    k_resolve<<<gridPT, kPtBlock, 0, s>>>(F.sIds.as<const uint32_t>(), F.sContrib.as<const float4>(),
+                                         F.sOcc.as<const uint8_t>(), F.rad.as<float4>(), C);
+    NOMAD_CUDA(ctx, cudaGetLastError());
+    cur ^= 1;
+  }
+  float *dOut = out;
+  bool hostOut = !(flags & NOMAD_TRACE_DEVICE_POINTERS);
+  if (hostOut) {
+    NOMAD_CUDA(ctx, ctx->stageAux.reserve(pixels * 12));
+    dOut = ctx->stageAux.as<float>();
+  }
+  k_finalize<<<gridPT, kPtBlock, 0, s>>>(V, nviews, pixels, F.rad.as<const float4>(), dOut);
+  NOMAD_CUDA(ctx, cudaGetLastError());
+  if (hostOut) {
+    NOMAD_CUDA(ctx, cudaMemcpyAsync(out, dOut, pixels * 12, cudaMemcpyDeviceToHost, s));
+    NOMAD_CUDA(ctx, cudaStreamSynchronize(s));
+  }
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_render_stats(nomad_ctx *ctx, uint64_t out[4]) {
+  if (!ctx || !out) return NOMAD_ERR_INVALID_ARGUMENT;
+  std::memset(out, 0, 32);
+  if (ctx->frame.counters.bytes == 0) return NOMAD_OK;
+  Counters c;
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(&c, ctx->frame.counters.p, sizeof(Counters), cudaMemcpyDeviceToHost, ctx->stream));
+  NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int k = 0; k < 4; ++k) out[k] = c.stats[k];
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_reset_render_stats(nomad_ctx *ctx) {
+  if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
+  if (ctx->frame.counters.bytes == 0) return NOMAD_OK;
+  NOMAD_CUDA(ctx, cudaMemsetAsync(ctx->frame.counters.p, 0, sizeof(Counters), ctx->stream));
+  NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return NOMAD_OK;
+}
+
+// ReSTIR DI is compiled in restir.cu; until it is configured this pass is a no-op.
+__attribute__((weak)) nomad_status nomad_restir_pass(nomad_ctx *, const void *, uint32_t, const nomad_view *) {
+  return NOMAD_OK;
+}

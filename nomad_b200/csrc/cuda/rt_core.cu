@@ -9,9 +9,7 @@
 #include <string>
 #include <vector>
 
-#include "../../../include/nomad_rt.h"
-#include "../host/layout.h"
-#include "rt_device.cuh"
+#include "rt_context.h"
 
 using namespace nomad_dev;
 
@@ -111,67 +109,11 @@ __global__ void k_patch(int32_t *__restrict__ arena, const int64_t *__restrict__
 
 }  // namespace
 
-struct DeviceBuf {
-  void *p = nullptr;
-  size_t bytes = 0;
-  ~DeviceBuf() {
-    if (p) cudaFree(p);
-  }
-  cudaError_t reserve(size_t b) {
-    if (b <= bytes) return cudaSuccess;
-    if (p) cudaFree(p);
-    p = nullptr;
-    bytes = 0;
-    cudaError_t e = cudaMalloc(&p, b);
-    if (e == cudaSuccess) bytes = b;
-    return e;
-  }
-};
-
-struct nomad_ctx {
-  int device = 0;
-  int smCount = 0;
-  cudaStream_t stream = nullptr;     // stream used by calls (own or caller's)
-  cudaStream_t ownStream = nullptr;
-  cudaStream_t copyStreams[2] = {nullptr, nullptr};
-  std::string err;
-  uint32_t kernel = NOMAD_KERNEL_BVH2;
-  bool sceneReady = false;
-  // scene sizes
-  uint32_t primCount = 0, objectCount = 0;
-  // device memory
-  DeviceBuf arena;      // pair nodes then triangle records
-  DeviceBuf prims, materials;
-  DeviceBuf objHits, status, cursor;
-  DeviceBuf stageIn, stageOut, stageAux;  // host-pointer staging
-  DeviceBuf patchOffs, patchVals;
-  size_t pnodeWords = 0;  // int32 words of the pair-node part of the arena
-  DevScene scene{};
-  // host residency state
-  nomad::TraversalLayout layout;
-  std::vector<uint8_t> primActive, objResident;
-  std::vector<uint32_t> objActiveCount;
-  std::vector<nomad_instance_record> instances;
-  std::vector<uint32_t> dirtyPrims, dirtyObjs;
-  std::vector<uint8_t> primDirtyFlag, objDirtyFlag;
-};
-
 namespace {
 
 nomad_status fail(nomad_ctx *c, nomad_status st, const std::string &msg) {
-  if (c) c->err = msg;
-  return st;
+  return nomad_fail(c, st, msg);
 }
-
-nomad_status cuda_fail(nomad_ctx *c, cudaError_t e, const char *what) {
-  return fail(c, NOMAD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
-}
-
-#define NOMAD_CUDA(ctx, call)                             \
-  do {                                                    \
-    cudaError_t e_ = (call);                              \
-    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
-  } while (0)
 
 bool is_device_ptr(const void *p) {
   cudaPointerAttributes at;
@@ -307,6 +249,10 @@ extern "C" nomad_status nomad_scene_upload(nomad_ctx *ctx, const float *bvh, uin
   ctx->objActiveCount.assign(objectCount, 0);
   for (uint32_t o = 0; o < objectCount; ++o) ctx->objActiveCount[o] = inst[o].primitive_count;
   ctx->instances.assign(inst, inst + objectCount);
+  ctx->hostPrims.assign(prims, prims + (size_t)primCount * 28);
+  ctx->hostMaterials.assign(materials, materials + (size_t)primCount * 20);
+  ctx->frame.lightsDirty = true;
+  ctx->frame.restirValid = false;
   ctx->dirtyPrims.clear();
   ctx->dirtyObjs.clear();
   ctx->primDirtyFlag.assign(primCount, 0);
@@ -390,6 +336,7 @@ extern "C" nomad_status nomad_residency_flush(nomad_ctx *ctx) {
       vals.push_back(ref);
     }
   }
+  if (!ctx->dirtyPrims.empty()) ctx->frame.lightsDirty = true;
   ctx->dirtyPrims.clear();
   ctx->dirtyObjs.clear();
   if (offs.empty()) return NOMAD_OK;

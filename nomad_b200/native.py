@@ -93,7 +93,34 @@ SIGNATURES = {
     "nomad_read_object_hits": (C.c_int32, [_P, _P]),
     "nomad_reset_object_hits": (C.c_int32, [_P]),
     "nomad_trace_closest_noalloc": (C.c_int32, [_P, _P, C.c_uint64, _P, _P]),
+    "nomad_view_pinhole": (C.c_int32, [_P, _P, _P, C.c_float, C.c_uint32, C.c_uint32, _P]),
+    "nomad_render_frame": (C.c_int32, [_P, _P, C.c_uint32, _P, C.c_uint32]),
+    "nomad_render_stats": (C.c_int32, [_P, _P]),
+    "nomad_reset_render_stats": (C.c_int32, [_P]),
 }
+
+VIEW_DTYPE = np.dtype([("camera_pos", "<f4", 3), ("viewport_u", "<f4", 3), ("viewport_v", "<f4", 3),
+                       ("first_pixel", "<f4", 3), ("width", "<u4"), ("height", "<u4"), ("spp", "<u4"),
+                       ("max_depth", "<u4"), ("seed_lo", "<u4"), ("seed_hi", "<u4"), ("frame", "<u4"),
+                       ("flags", "<u4")])
+VIEW_CLAMP = 1 << 0
+VIEW_RESTIR = 1 << 1
+
+
+def view_pinhole(position, look_at, up=(0.0, 1.0, 0.0), vfov=60.0, width=640, height=360, spp=1,
+                 max_depth=1, seed=0, frame=0, flags=0) -> np.ndarray:
+    """A nomad_view (numpy record) for a pinhole camera, filled by the library
+    (populateViewportUniforms semantics)."""
+    lib = load()
+    out = np.zeros(1, VIEW_DTYPE)
+    pos = np.asarray(position, np.float32)
+    look = np.asarray(look_at, np.float32)
+    upv = np.asarray(up, np.float32)
+    _check(lib.nomad_view_pinhole(pos.ctypes.data, look.ctypes.data, upv.ctypes.data, vfov, width,
+                                  height, out.ctypes.data))
+    out["spp"], out["max_depth"], out["frame"], out["flags"] = spp, max_depth, frame, flags
+    out["seed_lo"], out["seed_hi"] = seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF
+    return out
 
 _lib: Optional[C.CDLL] = None
 
@@ -353,6 +380,37 @@ class Context:
     def trace_work_dev(self, rays_ptr: int, n: int, out_ptr: int):
         self._ck(self.lib.nomad_trace_work(self.h, _P(rays_ptr), n, _P(out_ptr),
                                            TRACE_DEVICE_POINTERS))
+
+    # path tracing
+    def render(self, views: np.ndarray, count_hits: bool = False) -> list:
+        """Renders the views in one batched frame; returns one (height, width, 3) float32 image
+        per view."""
+        views = np.ascontiguousarray(views, VIEW_DTYPE).reshape(-1)
+        total = int((views["width"].astype(np.int64) * views["height"]).sum())
+        out = np.empty(total * 3, np.float32)
+        self._ck(self.lib.nomad_render_frame(self.h, _ptr(views), views.shape[0], _ptr(out),
+                                             TRACE_COUNT_HITS if count_hits else 0))
+        imgs, off = [], 0
+        for v in views:
+            n = int(v["width"]) * int(v["height"])
+            imgs.append(out[3 * off:3 * (off + n)].reshape(int(v["height"]), int(v["width"]), 3))
+            off += n
+        return imgs
+
+    def render_dev(self, views: np.ndarray, out_ptr: int, count_hits: bool = False):
+        views = np.ascontiguousarray(views, VIEW_DTYPE).reshape(-1)
+        self._keep_views = views
+        self._ck(self.lib.nomad_render_frame(self.h, _ptr(views), views.shape[0], _P(out_ptr),
+                                             TRACE_DEVICE_POINTERS |
+                                             (TRACE_COUNT_HITS if count_hits else 0)))
+
+    def render_stats(self) -> np.ndarray:
+        out = np.zeros(4, np.uint64)
+        self._ck(self.lib.nomad_render_stats(self.h, _ptr(out)))
+        return out
+
+    def reset_render_stats(self):
+        self._ck(self.lib.nomad_reset_render_stats(self.h))
 
     def object_hits(self) -> np.ndarray:
         out = np.zeros(self.object_count, np.uint32)

@@ -91,3 +91,31 @@ def algorithmic_bytes(work: np.ndarray) -> np.ndarray:
     16 per instance record, 48 per closest hit (the hit's frame float4 4..6)."""
     w = work.astype(np.int64)
     return 32 * w[:, 0] + 52 * w[:, 1] + 16 * w[:, 2] + 48 * w[:, 3]
+
+
+def render(os_: "OracleScene", materials, views, pixels=None, obj_hits=False, threads=0):
+    """Scalar path tracer (pathtrace.cpp) on the listed global pixel indices of the views
+    (all pixels when None). Returns (rgb[n,3], obj_hits or None, stats[4])."""
+    lib = load()
+    if not hasattr(lib, "_render_bound"):
+        lib.oracle_render.argtypes = [_P, _P, C.c_uint32, _P, _P, _P, _P, _P, _P, C.c_uint32,
+                                      C.c_uint32, _P, C.c_uint32, _P, C.c_uint64, _P, _P, _P,
+                                      C.c_uint32]
+        lib.oracle_render.restype = C.c_int
+        lib._render_bound = True
+    views = np.ascontiguousarray(views).reshape(-1)
+    if pixels is None:
+        total = int((views["width"].astype(np.int64) * views["height"]).sum())
+        pixels = np.arange(total, dtype=np.uint64)
+    pixels = np.ascontiguousarray(pixels, np.uint64)
+    mats = np.ascontiguousarray(materials, np.float32)
+    out = np.zeros((pixels.size, 3), np.float32)
+    hits = np.zeros(os_.object_count, np.uint32) if obj_hits else None
+    stats = np.zeros(4, np.uint64)
+    rc = lib.oracle_render(_p(os_.bvh), _p(os_.tlas), os_.tlas.size // 8, _p(os_.prims), _p(mats),
+                           _p(os_.prim_indices), _p(os_.active), _p(os_.blas_root),
+                           _p(os_.prim_object), os_.object_count, os_.prims.size // 28,
+                           _p(views), views.shape[0], _p(pixels), pixels.size, _p(out),
+                           _p(hits) if hits is not None else None, _p(stats), threads)
+    assert rc == 0
+    return out, hits, stats

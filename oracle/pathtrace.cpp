@@ -1,0 +1,561 @@
+// ORACLE — test infrastructure only (the checker of the wavefront path tracer).
+//
+// Scalar restatement of the reference's per-pixel path tracer:
+//   pathTraceKernel raygen and averaging   Renderer/Shaders/PathTraceKernel.metal:67-162
+//   rayColor bounce loop                   Renderer/Shaders/PathTracing.h:1168-1881
+//     sky on miss :1211-1213, emission :1312-1317, one-sample NEE :1744-1848,
+//     scatter + offset :1851-1861, Russian roulette :1863-1870, clamp :1879
+//   decodeMaterial :165-196, evaluateDirectLightingBsdf :249-293, sampleLightPoint :582-643,
+//   selectLightOffset :219-235, scatter / sampleCosineHemisphere / mirrorAngle Scatter.h:31-152
+//   light CDF over active emissive primitives Renderer/Renderer.cpp:5161-5211, primitiveArea :1462-1480
+// Contract changes (shared with the CUDA path tracer):
+//   * random numbers: Philox4x32-10 (Salmon et al., SC'11) with key (seed_lo, seed_hi + frame)
+//     and counter (pixel, sample, 4*bounce + block, view) instead of the reference's hash of the
+//     pixel uv; block 0 = (light choice, light u1, light u2, lobe choice), block 1 = (direction
+//     u1, direction u2, roulette, Fresnel choice), raygen = bounce 255 block 0;
+//   * sin/cos(2 pi u), log2, exp2 and x^5 are defined by fixed polynomials/products (below) so
+//     that host and device round identically;
+//   * traversal and shadow visibility follow the contract (contract_core.h): lowest-index tie
+//     rule, true any-hit shadow rays over (1e-4, dist - 1e-4);
+//   * a path whose throughput becomes exactly zero stops (the reference keeps tracing it with no
+//     effect on radiance);
+//   * clamping to [0, 1] is optional (NOMAD_VIEW_CLAMP) so HDR radiance can be compared.
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "contract_core.h"
+
+using namespace oracle_core;
+
+namespace {
+
+struct View {
+  float cam[3], vu[3], vv[3], fp[3];
+  uint32_t w, h, spp, maxDepth, seedLo, seedHi, frame, flags;
+};
+const uint32_t VIEW_CLAMP = 1u;
+const float PI_F = 3.14159265358979323846f;
+
+struct V {
+  float x, y, z;
+};
+inline V v(float x, float y, float z) { return V{x, y, z}; }
+inline V add(V a, V b) { return v(a.x + b.x, a.y + b.y, a.z + b.z); }
+inline V vsub(V a, V b) { return v(a.x - b.x, a.y - b.y, a.z - b.z); }
+inline V mul(V a, V b) { return v(a.x * b.x, a.y * b.y, a.z * b.z); }
+inline V scl(V a, float s) { return v(a.x * s, a.y * s, a.z * s); }
+inline V dvs(V a, float s) { return v(a.x / s, a.y / s, a.z / s); }
+inline V neg(V a) { return v(-a.x, -a.y, -a.z); }
+inline float dt(V a, V b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline V crs(V a, V b) { return v(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+inline V nrmz(V a) {
+  float l = std::sqrt(dt(a, a));
+  return dvs(a, l);
+}
+inline bool fin(V a) { return std::isfinite(a.x) && std::isfinite(a.y) && std::isfinite(a.z); }
+inline float mx(float a, float b) { return a < b ? b : a; }
+inline float mn(float a, float b) { return b < a ? b : a; }
+inline float c01(float x) { return mn(mx(x, 0.0f), 1.0f); }
+inline V max0(V a) { return v(mx(a.x, 0.0f), mx(a.y, 0.0f), mx(a.z, 0.0f)); }
+inline float lum(V c) { return c.x * 0.2126f + c.y * 0.7152f + c.z * 0.0722f; }
+inline V refl(V i, V n) { return vsub(i, scl(n, 2.0f * dt(n, i))); }
+inline float p5(float x) {
+  float x2 = x * x;
+  return x2 * x2 * x;
+}
+
+// Philox4x32-10 from the paper: per round (hi0,lo0) = M0*c0, (hi1,lo1) = M1*c2,
+// c = (hi1^c1^k0, lo1, hi0^c3^k1, lo0); keys bumped by the Weyl constants.
+struct U4 {
+  uint32_t x, y, z, w;
+};
+U4 philox(U4 c, uint32_t k0, uint32_t k1) {
+  for (int r = 0; r < 10; ++r) {
+    uint64_t p0 = (uint64_t)0xD2511F53u * c.x, p1 = (uint64_t)0xCD9E8D57u * c.z;
+    c = U4{(uint32_t)(p1 >> 32) ^ c.y ^ k0, (uint32_t)p1, (uint32_t)(p0 >> 32) ^ c.w ^ k1, (uint32_t)p0};
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return c;
+}
+inline float u01(uint32_t x) { return (float)(x >> 8) * (1.0f / 16777216.0f); }
+
+void sincos_turns(float u, float &s, float &c) {
+  float t = u * 8.0f;
+  float fo = std::floor(t);
+  int o = (int)fo & 7;
+  float x = (t - fo - 0.5f) * 0.785398163397448f;
+  float x2 = x * x;
+  float sx = x * (1.0f - x2 * (0.16666666666666667f - x2 * (0.008333333333333333f - x2 * 0.0001984126984126984f)));
+  float cx = 1.0f - x2 * (0.5f - x2 * (0.041666666666666667f - x2 * (0.001388888888888889f - x2 * 2.48015873015873e-05f)));
+  static const float kc[8] = {0.923879532511287f, 0.382683432365090f, -0.382683432365090f, -0.923879532511287f,
+                              -0.923879532511287f, -0.382683432365090f, 0.382683432365090f, 0.923879532511287f};
+  static const float ks[8] = {0.382683432365090f, 0.923879532511287f, 0.923879532511287f, 0.382683432365090f,
+                              -0.382683432365090f, -0.923879532511287f, -0.923879532511287f, -0.382683432365090f};
+  c = kc[o] * cx - ks[o] * sx;
+  s = ks[o] * cx + kc[o] * sx;
+}
+float log2_series(float a) {
+  int e;
+  float m = std::frexp(a, &e);
+  if (m < 0.70710678118654752f) {
+    m = m * 2.0f;
+    e -= 1;
+  }
+  float s = (m - 1.0f) / (m + 1.0f);
+  float s2 = s * s;
+  float ln = 2.0f * s * (1.0f + s2 * (0.3333333333333333f + s2 * (0.2f + s2 * (0.14285714285714285f + s2 * 0.1111111111111111f))));
+  return (float)e + ln * 1.4426950408889634f;
+}
+float exp2_series(float y) {
+  if (y < -126.0f) return 0.0f;
+  if (y > 127.0f) return INFINITY;
+  float fi = std::floor(y);
+  float f = (y - fi) * 0.6931471805599453f;
+  float p = 1.0f + f * (1.0f + f * (0.5f + f * (0.16666666666666667f + f * (0.041666666666666667f +
+            f * (0.008333333333333333f + f * (0.001388888888888889f + f * (0.0001984126984126984f +
+            f * 2.48015873015873e-05f)))))));
+  return std::ldexp(p, (int)fi);
+}
+float pow_pos(float a, float b) {
+  if (!(a > 0.0f)) return 0.0f;
+  return exp2_series(b * log2_series(a));
+}
+
+struct Mat {
+  V diffuse;
+  float opacity;
+  V specular;
+  float shininess;
+  V emission;
+  float power;
+  V transmission;
+  float ior, roughness;
+};
+
+Mat decode(const float *mats, int32_t prim, float lod) {
+  const float *m = mats + 20ll * prim;
+  Mat o;
+  o.diffuse = max0(scl(v(m[0], m[1], m[2]), lod));
+  o.opacity = c01(m[3]);
+  o.specular = max0(v(m[4], m[5], m[6]));
+  o.shininess = mx(m[7], 1.0f);
+  o.emission = max0(v(m[8], m[9], m[10]));
+  o.power = mx(m[11], 0.0f);
+  o.transmission = max0(v(m[12], m[13], m[14]));
+  o.ior = mx(m[15], 1e-3f);
+  o.roughness = c01(m[19]);
+  if (o.opacity < 1.0f && lum(o.transmission) <= 0.0f) {
+    float t = 1.0f - o.opacity;
+    o.transmission = v(t, t, t);
+  }
+  return o;
+}
+
+V geom_normal(const float *prims, int32_t prim, V p) {
+  const float *g = prims + 28ll * prim;
+  int type = (int)g[3];
+  V sn = v(g[24], g[25], g[26]);
+  if (type == 1) {
+    V v0 = v(g[0], g[1], g[2]);
+    V fb = crs(vsub(v(g[4], g[5], g[6]), v0), vsub(v(g[8], g[9], g[10]), v0));
+    fb = dt(fb, fb) > 0.0f ? nrmz(fb) : v(0.0f, 1.0f, 0.0f);
+    V n = (dt(sn, sn) > RAY_EPS && fin(sn)) ? nrmz(sn) : fb;
+    if (!fin(n) || dt(n, n) <= RAY_EPS) n = fb;
+    return n;
+  }
+  if (type == 2) {
+    V fb = crs(v(g[4], g[5], g[6]), v(g[8], g[9], g[10]));
+    fb = (dt(fb, fb) > RAY_EPS && fin(fb)) ? nrmz(fb) : v(0.0f, 1.0f, 0.0f);
+    return (dt(sn, sn) > RAY_EPS && fin(sn)) ? nrmz(sn) : fb;
+  }
+  return nrmz(vsub(p, v(g[0], g[1], g[2])));
+}
+
+V bsdf(const Mat &m, V normal, V viewDir, V lightDir) {
+  V n = nrmz(normal), vv = nrmz(viewDir), l = nrmz(lightDir);
+  if (!fin(n) || !fin(vv) || !fin(l)) return v(0, 0, 0);
+  float nl = mx(dt(n, l), 0.0f), nv = mx(dt(n, vv), 0.0f);
+  if (nl <= 0.0f || nv <= 0.0f) return v(0, 0, 0);
+  V dc = scl(max0(m.diffuse), m.opacity);
+  V sc0 = scl(m.specular, m.opacity);
+  V sc = v(c01(sc0.x), c01(sc0.y), c01(sc0.z));
+  float rough = c01(m.roughness);
+  float alpha = mx(rough * rough, 0.001f);
+  float a2 = alpha * alpha;
+  V h = nrmz(add(vv, l));
+  float nh = mx(dt(n, h), 0.0f), vh = mx(dt(vv, h), 0.0f);
+  float den = nh * nh * (a2 - 1.0f) + 1.0f;
+  float D = a2 / mx(PI_F * den * den, RAY_EPS);
+  float k = alpha + 1.0f;
+  k = (k * k) / 8.0f;
+  float G = (nv / (nv * (1.0f - k) + k)) * (nl / (nl * (1.0f - k) + k));
+  float Fc = p5(mx(1.0f - vh, 0.0f));
+  V F = add(sc, scl(vsub(v(1, 1, 1), sc), Fc));
+  V spec = dvs(scl(F, D * G), mx(4.0f * nl * nv, RAY_EPS));
+  return add(dvs(dc, PI_F), spec);
+}
+
+void onb(V n, V &t, V &b) {
+  V up = std::fabs(n.z) < 0.999f ? v(0, 0, 1) : v(0, 1, 0);
+  t = nrmz(crs(up, n));
+  b = nrmz(crs(n, t));
+}
+
+V scatter(V inDir, V normal, bool front, const Mat &m, float xiLobe, float u1, float u2, float xiF, V &out) {
+  float dw = mx(lum(m.diffuse) * m.opacity, 0.0f);
+  float sw = mx(lum(m.specular) * m.opacity, 0.0f);
+  float tw = mx(lum(m.transmission) * (1.0f - m.opacity), 0.0f);
+  if (tw > 0.0f) sw = 0.0f;
+  float total = dw + sw + tw;
+  if (total <= 0.0f) {
+    out = normal;
+    return v(0, 0, 0);
+  }
+  float xi = xiLobe * total;
+  if (xi < dw) {
+    float r = std::sqrt(mx(0.0f, u1));
+    float s, c;
+    sincos_turns(u2, s, c);
+    float x = r * c, y = r * s, z = std::sqrt(mx(0.0f, 1.0f - u1));
+    V t, b;
+    onb(normal, t, b);
+    out = nrmz(add(add(scl(t, x), scl(b, y)), scl(normal, z)));
+    return dvs(scl(m.diffuse, m.opacity), mx(dw / total, 1e-4f));
+  }
+  xi = xi - dw;
+  if (xi < sw) {
+    V rd = refl(inDir, normal);
+    float ex = mx(m.shininess, 1.0f);
+    if (m.roughness > 0.0f) {
+      float sm = c01(1.0f - m.roughness);
+      ex = mx(ex, mx(1.0f, sm * sm * 256.0f));
+    }
+    float ct = pow_pos(u1, 1.0f / (ex + 1.0f));
+    float st = std::sqrt(mx(0.0f, 1.0f - ct * ct));
+    float s, c;
+    sincos_turns(u2, s, c);
+    V t, b;
+    onb(rd, t, b);
+    out = nrmz(add(add(scl(t, st * c), scl(b, st * s)), scl(rd, ct)));
+    return dvs(m.specular, mx(sw / total, 1e-4f));
+  }
+  float prob = mx(tw / total, 1e-4f);
+  float eta = mx(m.ior, 1e-3f);
+  float ratio = front ? (1.0f / eta) : eta;
+  float cosT = dt(neg(inDir), normal);
+  float sinT = std::sqrt(mx(0.0f, 1.0f - cosT * cosT));
+  float r0 = (1.0f - ratio) / (1.0f + ratio);
+  r0 = r0 * r0;
+  float refl_ = r0 + (1.0f - r0) * p5(1.0f - cosT);
+  if ((ratio * sinT > 1.0f) || (refl_ > xiF)) {
+    out = refl(inDir, normal);
+    return dvs(m.specular, prob);
+  }
+  float d = dt(normal, inDir);
+  float k = 1.0f - ratio * ratio * (1.0f - d * d);
+  if (k < 0.0f) {
+    out = refl(inDir, normal);
+    return dvs(m.specular, prob);
+  }
+  V rr = vsub(scl(inDir, ratio), scl(normal, ratio * d + std::sqrt(k)));
+  if (!fin(rr)) {
+    out = refl(inDir, normal);
+    return dvs(m.specular, prob);
+  }
+  out = nrmz(rr);
+  return dvs(m.transmission, prob);
+}
+
+bool light_point(const float *prims, uint32_t lp, float u1, float u2, V &pos, V &nrm, float &area) {
+  const float *g = prims + 28ll * lp;
+  int type = (int)g[3];
+  if (type == 0) {
+    float radius = g[4];
+    if (radius <= 0.0f) return false;
+    float z = 2.0f * u1 - 1.0f;
+    float s, c;
+    sincos_turns(u2, s, c);
+    float r = std::sqrt(mx(0.0f, 1.0f - z * z));
+    V dir = v(r * c, r * s, z);
+    pos = add(v(g[0], g[1], g[2]), scl(dir, radius));
+    nrm = dir;
+    area = 4.0f * PI_F * radius * radius;
+    return area > 0.0f;
+  }
+  if (type == 1) {
+    float su1 = std::sqrt(u1);
+    float b0 = 1.0f - su1, b1 = su1 * (1.0f - u2), b2 = su1 * u2;
+    V v0 = v(g[0], g[1], g[2]), v1 = v(g[4], g[5], g[6]), v2 = v(g[8], g[9], g[10]);
+    pos = add(add(scl(v0, b0), scl(v1, b1)), scl(v2, b2));
+    V n = crs(vsub(v1, v0), vsub(v2, v0));
+    float ln = std::sqrt(dt(n, n));
+    if (ln <= 0.0f) return false;
+    nrm = dvs(n, ln);
+    area = 0.5f * ln;
+    return area > 0.0f;
+  }
+  if (type == 2) {
+    float su = u1 * 2.0f - 1.0f, sv = u2 * 2.0f - 1.0f;
+    V c = v(g[0], g[1], g[2]), e1 = v(g[4], g[5], g[6]), e2 = v(g[8], g[9], g[10]);
+    pos = add(add(c, scl(e1, su)), scl(e2, sv));
+    V n = crs(e1, e2);
+    float ln = std::sqrt(dt(n, n));
+    if (ln <= 0.0f) return false;
+    nrm = dvs(n, ln);
+    area = 4.0f * ln;
+    return area > 0.0f;
+  }
+  return false;
+}
+
+struct LightsH {
+  std::vector<uint32_t> idx;
+  std::vector<float> cdf;
+  float total = 0.0f;
+};
+
+LightsH build_lights(const float *prims, const float *mats, const uint8_t *active, const int32_t *blasRoot,
+                     const int32_t *primObject, uint32_t primCount) {
+  LightsH L;
+  float total = 0.0f;
+  for (uint32_t i = 0; i < primCount; ++i) {
+    if (!active[i] || blasRoot[primObject[i]] < 0) continue;
+    const float *m = mats + 20ull * i;
+    float strength = m[11] * (m[8] * 0.2126f + m[9] * 0.7152f + m[10] * 0.0722f);
+    if (!(strength > 0.0f)) continue;
+    const float *g = prims + 28ull * i;
+    int type = (int)g[3];
+    float area;
+    if (type == 0) {
+      area = 4.0f * PI_F * g[4] * g[4];
+    } else {
+      V a = type == 1 ? vsub(v(g[4], g[5], g[6]), v(g[0], g[1], g[2])) : v(g[4], g[5], g[6]);
+      V b = type == 1 ? vsub(v(g[8], g[9], g[10]), v(g[0], g[1], g[2])) : v(g[8], g[9], g[10]);
+      V c = crs(a, b);
+      float len = std::sqrt(c.x * c.x + c.y * c.y + c.z * c.z);
+      area = type == 1 ? 0.5f * len : 4.0f * len;
+    }
+    if (!(area > 0.0f)) continue;
+    float w = area * strength;
+    if (!(w > 0.0f)) continue;
+    total += w;
+    L.idx.push_back(i);
+    L.cdf.push_back(total);
+  }
+  L.total = total;
+  return L;
+}
+
+uint32_t select_light(float xi, const LightsH &L) {
+  uint32_t n = (uint32_t)L.idx.size();
+  float target = xi * L.total;
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) / 2;
+    if (L.cdf[mid] < target) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo < n - 1 ? lo : n - 1;
+}
+
+struct Ctx {
+  Scene s;
+  const float *mats;
+  LightsH L;
+  uint32_t objectCount;
+};
+
+Ray mkray(V o, V d, float tmax) { return Ray{mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), tmax}; }
+
+Hit closest(const Ctx &c, const Ray &r) {
+  Hit h{r.tmax, 0.0f, 0.0f, -1, -1};
+  trace_near_first<false>(c.s, r, h, nullptr);
+  if (h.prim < 0) h.t = INFINITY;
+  return h;
+}
+bool occluded(const Ctx &c, const Ray &r) {
+  Hit h{r.tmax, 0.0f, 0.0f, -1, -1};
+  trace_near_first<true>(c.s, r, h, nullptr);
+  return h.prim >= 0;
+}
+
+// One path; returns its radiance (unclamped) and counts closest hits per object.
+V path(const Ctx &c, const View &vw, uint32_t vi, uint32_t pixel, uint32_t sample, uint32_t *objHits,
+       uint64_t *stats) {
+  uint32_t k0 = vw.seedLo, k1 = vw.seedHi + vw.frame;
+  uint32_t px = pixel % vw.w, py = pixel / vw.w;
+  U4 r0 = philox(U4{pixel, sample, 255u * 4u, vi}, k0, k1);
+  float ux = ((float)px + 0.5f) / (float)vw.w, uy = ((float)py + 0.5f) / (float)vw.h;
+  float s = ux + (u01(r0.x) - 0.5f) / (float)vw.w, t = uy + (u01(r0.y) - 0.5f) / (float)vw.h;
+  V d = v(vw.fp[0] + s * vw.vu[0] + t * vw.vv[0] - vw.cam[0], vw.fp[1] + s * vw.vu[1] + t * vw.vv[1] - vw.cam[1],
+          vw.fp[2] + s * vw.vu[2] + t * vw.vv[2] - vw.cam[2]);
+  V dir = nrmz(d);
+  V org = v(vw.cam[0], vw.cam[1], vw.cam[2]);
+  float dx[3] = {vw.vu[0] / (float)vw.w, vw.vu[1] / (float)vw.w, vw.vu[2] / (float)vw.w};
+  float dy[3] = {vw.vv[0] / (float)vw.h, vw.vv[1] / (float)vw.h, vw.vv[2] / (float)vw.h};
+  float cx = dx[1] * dy[2] - dx[2] * dy[1], cy = dx[2] * dy[0] - dx[0] * dy[2], cz = dx[0] * dy[1] - dx[1] * dy[0];
+  float lod = 1.0f / (1.0f + std::sqrt(cx * cx + cy * cy + cz * cz));
+  V thr = v(1, 1, 1), rad = v(0, 0, 0);
+  for (uint32_t depth = 0; depth < vw.maxDepth; ++depth) {
+    stats[0]++;
+    Ray ray = mkray(org, dir, INFINITY);
+    Hit h = closest(c, ray);
+    if (h.prim < 0) {
+      stats[1]++;
+      V ud = nrmz(dir);
+      float sk = 0.5f * (ud.y + 1.0f);
+      V sky = v(1.0f + (0.6f - 1.0f) * sk, 1.0f + (0.7f - 1.0f) * sk, 1.0f + (1.0f - 1.0f) * sk);
+      rad = add(rad, mul(thr, sky));
+      break;
+    }
+    stats[3]++;
+    if (objHits) objHits[h.inst]++;
+    U4 b0 = philox(U4{pixel, sample, depth * 4u + 0u, vi}, k0, k1);
+    U4 b1 = philox(U4{pixel, sample, depth * 4u + 1u, vi}, k0, k1);
+    V p = v(org.x + h.t * dir.x, org.y + h.t * dir.y, org.z + h.t * dir.z);
+    V n = geom_normal(c.s.prims, h.prim, p);
+    bool front = dt(n, dir) < 0.0f;
+    if (!front) n = neg(n);
+    Mat m = decode(c.mats, h.prim, lod);
+    if (m.power * lum(m.emission) > 0.0f) rad = add(rad, scl(mul(thr, m.emission), m.power));
+    V dc = scl(m.diffuse, m.opacity);
+    if (lum(dc) > 0.0f && !c.L.idx.empty() && c.L.total > 0.0f) {
+      uint32_t off = select_light(u01(b0.x), c.L);
+      uint32_t lp = c.L.idx[off];
+      V lpos, lnrm;
+      float area = 0.0f;
+      if ((int32_t)lp != h.prim && light_point(c.s.prims, lp, u01(b0.y), u01(b0.z), lpos, lnrm, area) && area > 0.0f) {
+        V toL = vsub(lpos, p);
+        float d2 = dt(toL, toL);
+        if (d2 > RAY_EPS) {
+          float dist = std::sqrt(d2);
+          V wi = dvs(toL, dist);
+          float cosT = mx(dt(n, wi), 0.0f), cosL = mx(dt(lnrm, neg(wi)), 0.0f);
+          if (cosT > 0.0f && cosL > 0.0f) {
+            float prev = off > 0 ? c.L.cdf[off - 1] : 0.0f;
+            float w = c.L.cdf[off] - prev;
+            float lpdf = (c.L.total > 0.0f && w > 0.0f) ? w / c.L.total : 0.0f;
+            if (lpdf > 0.0f) {
+              float totalPdf = lpdf * ((1.0f / area) * d2 / cosL);
+              if (totalPdf > 0.0f) {
+                float tmax = dist - RAY_EPS;
+                if (tmax < RAY_EPS) tmax = RAY_EPS;
+                stats[2]++;
+                Ray sr = mkray(add(p, scl(n, 0.0005f)), wi, tmax);
+                if (!occluded(c, sr)) {
+                  Mat lm = decode(c.mats, (int32_t)lp, 1.0f);
+                  V lrad = scl(lm.emission, lm.power);
+                  V b = bsdf(m, n, nrmz(neg(dir)), wi);
+                  rad = add(rad, scl(mul(mul(thr, b), lrad), cosT / totalPdf));
+                }
+              }
+            }
+          }
+        }
+      }
+    }
+    V nd;
+    V wgt = scatter(dir, n, front, m, u01(b0.w), u01(b1.x), u01(b1.y), u01(b1.w), nd);
+    V bias = dt(nd, n) < 0.0f ? neg(n) : n;
+    org = add(p, scl(bias, RAY_EPS));
+    dir = nd;
+    thr = mul(thr, wgt);
+    if (depth >= 5) {
+      float pm = mx(thr.x, mx(thr.y, thr.z));
+      if (u01(b1.z) >= pm) break;
+      thr = dvs(thr, pm);
+    }
+    if (thr.x == 0.0f && thr.y == 0.0f && thr.z == 0.0f) break;
+  }
+  return rad;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Renders the listed pixels (global pixel indices over the concatenated views) into out
+// (3 floats per listed pixel). views: nomad_view structs. obj_hits (object_count counters) and
+// stats (4 counters: rays, escapes, shadow rays, hits) may be null; they accumulate over the
+// listed pixels only.
+int oracle_render(const float *bvh, const float *tlas, uint32_t tlas_count, const float *prims,
+                  const float *materials, const int32_t *prim_indices, const uint8_t *active,
+                  const int32_t *blas_root, const int32_t *prim_object, uint32_t object_count,
+                  uint32_t prim_count, const void *views, uint32_t nviews, const uint64_t *pixels,
+                  uint64_t npix, float *out, uint32_t *obj_hits, uint64_t *stats, uint32_t threads) {
+  if (!bvh || !tlas || !prims || !materials || !views || !out || !pixels) return 1;
+  Ctx c{{bvh, tlas, tlas_count, prims, prim_indices, active, blas_root, prim_object}, materials, {}, object_count};
+  c.L = build_lights(prims, materials, active, blas_root, prim_object, prim_count);
+  const View *vs = static_cast<const View *>(views);
+  std::vector<uint64_t> voff(nviews + 1, 0);
+  for (uint32_t i = 0; i < nviews; ++i) voff[i + 1] = voff[i] + (uint64_t)vs[i].w * vs[i].h;
+  if (threads == 0) threads = std::max(1u, std::thread::hardware_concurrency());
+  std::vector<std::vector<uint32_t>> hits(threads, std::vector<uint32_t>(obj_hits ? object_count : 0, 0));
+  std::vector<std::vector<uint64_t>> st(threads, std::vector<uint64_t>(4, 0));
+  std::atomic<uint64_t> next{0};
+  auto work = [&](uint32_t tid) {
+    for (;;) {
+      uint64_t b = next.fetch_add(64);
+      if (b >= npix) break;
+      uint64_t e = std::min<uint64_t>(npix, b + 64);
+      for (uint64_t q = b; q < e; ++q) {
+        uint64_t g = pixels[q];
+        uint32_t vi = 0;
+        while (vi + 1 < nviews && voff[vi + 1] <= g) ++vi;
+        const View &vw = vs[vi];
+        uint32_t pixel = (uint32_t)(g - voff[vi]);
+        bool cl = (vw.flags & VIEW_CLAMP) != 0;
+        float ax = 0.0f, ay = 0.0f, az = 0.0f;
+        for (uint32_t s = 0; s < vw.spp; ++s) {
+          V r = path(c, vw, vi, pixel, s, obj_hits ? hits[tid].data() : nullptr, st[tid].data());
+          if (cl) r = v(c01(r.x), c01(r.y), c01(r.z));
+          ax = ax + r.x;
+          ay = ay + r.y;
+          az = az + r.z;
+        }
+        float ns = (float)vw.spp;
+        ax = ax / ns;
+        ay = ay / ns;
+        az = az / ns;
+        if (cl) {
+          ax = c01(ax);
+          ay = c01(ay);
+          az = c01(az);
+        }
+        out[3 * q] = ax;
+        out[3 * q + 1] = ay;
+        out[3 * q + 2] = az;
+      }
+    }
+  };
+  std::vector<std::thread> pool;
+  for (uint32_t t = 0; t < threads; ++t) pool.emplace_back(work, t);
+  for (auto &t : pool) t.join();
+  if (obj_hits)
+    for (auto &hh : hits)
+      for (uint32_t o = 0; o < object_count; ++o) obj_hits[o] += hh[o];
+  if (stats)
+    for (auto &s : st)
+      for (int k = 0; k < 4; ++k) stats[k] += s[k];
+  return 0;
+}
+
+}  // extern "C"
+
+extern "C" void oracle_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+  U4 r = philox(U4{ctr[0], ctr[1], ctr[2], ctr[3]}, key[0], key[1]);
+  out[0] = r.x;
+  out[1] = r.y;
+  out[2] = r.z;
+  out[3] = r.w;
+}
+
+extern "C" void oracle_math(float u, float out[4]) {
+  sincos_turns(u, out[0], out[1]);
+  out[2] = log2_series(u > 0.0f ? u : 1.0f);
+  out[3] = exp2_series(-u * 4.0f);
+}
