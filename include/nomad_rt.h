@@ -176,6 +176,65 @@ nomad_status nomad_render_frame(nomad_ctx *ctx, const nomad_view *views, uint32_
 nomad_status nomad_render_stats(nomad_ctx *ctx, uint64_t out[4]);
 nomad_status nomad_reset_render_stats(nomad_ctx *ctx);
 
+/* ---- residency policies on the device (updateResidency, RendererResidency.cpp:165-287, with
+ *      updateAlwaysResident :656-728, updateRayHitBudget :2755-2964 and the learned scorer that
+ *      replaces updateUnifiedResidency/UnifiedNeural :2331-2753) ---------------------------- */
+enum {
+  NOMAD_POLICY_ALWAYS = 0,        /* every object resident (the image judge)                  */
+  NOMAD_POLICY_RAYHIT_BUDGET = 1, /* decayed per-object closest-hit score (the fallback)       */
+  NOMAD_POLICY_LEARNED = 2        /* BF16 MLP score over NOMAD_FEATURES per-object features    */
+};
+#define NOMAD_FEATURES 24
+
+typedef struct nomad_residency_params {
+  uint32_t policy;
+  uint32_t max_toggles;     /* residency changes applied per step; 0 = unlimited             */
+  uint64_t budget_bytes;    /* geometry bytes allowed resident; 0 = no limit                 */
+  float hit_decay;          /* score = score * hit_decay + hits (rayHitDecay, 0.85)          */
+  float camera_motion;      /* [0,1]: widens the visibility reserve                          */
+  float memory_pressure;    /* [0,1]: off-screen objects with hits keep lerp(0.5,0.2,p)      */
+  float reserve_base;       /* visibility reserve = ceil(N * (base + motion * reserve_motion)) */
+  float reserve_motion;
+  uint32_t min_active;      /* objects always kept (highest scores first)                     */
+} nomad_residency_params;
+
+/* One residency step, all on the device: consumes the per-object closest-hit counts gathered
+ * since the previous step (render or trace calls with NOMAD_TRACE_COUNT_HITS), updates the
+ * per-object history and the NOMAD_FEATURES features for `camera`, scores every object with the
+ * policy, selects the resident set greedily by score under budget_bytes (visible objects first
+ * up to the visibility reserve, ties to the lower object index), and patches the TLAS so
+ * non-resident objects are skipped (blas_root_index = -1). The light CDF follows the resident
+ * set. *toggled receives the number of objects whose residency changed. Object geometry bytes =
+ * 32 per BLAS node + 196 per primitive (packed primitive, material and index). */
+nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residency_params *params,
+                                  const nomad_view *camera, uint32_t *toggled);
+/* Per-object geometry bytes (object_count uint64). */
+nomad_status nomad_object_bytes(nomad_ctx *ctx, uint64_t *out);
+/* Features and policy scores of the last step: features[object_count * NOMAD_FEATURES],
+ * scores[object_count] (either may be NULL). */
+nomad_status nomad_residency_last(nomad_ctx *ctx, float *features, float *scores);
+/* Current residency of each object (object_count bytes, 1 = resident). */
+nomad_status nomad_residency_flags(nomad_ctx *ctx, uint8_t *out);
+
+/* ---- learned scorer: 24 -> 128 -> 128 -> 1 MLP, ReLU, BF16 weights, FP32 accumulation on the
+ *      tensor cores, trained on device (no reference counterpart for the kernels; the reference
+ *      trains a tiny FP32 MLP offline in PyTorch, Benchmarks/train_unified_neural_mlp.py) ---- */
+#define NOMAD_MLP_PARAMS (128 * 32 + 128 + 128 * 128 + 128 + 128 + 1 + 2 * NOMAD_FEATURES)
+/* Initialises the weights (He-uniform) from a seed. */
+nomad_status nomad_mlp_init(nomad_ctx *ctx, uint64_t seed);
+/* Trains on n samples (features n*NOMAD_FEATURES, targets n, host arrays): standardises the
+ * features, then `steps` AdamW steps of mean-squared error on mini-batches of `batch` samples
+ * drawn with a seeded permutation. loss_out[steps] (may be NULL) receives each step's loss. */
+nomad_status nomad_mlp_train(nomad_ctx *ctx, const float *features, const float *targets, uint64_t n,
+                             uint32_t steps, uint32_t batch, float lr, float weight_decay, uint64_t seed,
+                             float *loss_out);
+/* Inference on n samples (host arrays unless NOMAD_TRACE_DEVICE_POINTERS). */
+nomad_status nomad_mlp_infer(nomad_ctx *ctx, const float *features, uint64_t n, float *out, uint32_t flags);
+/* Model blob (NOMAD_MLP_PARAMS floats): W1[128][32] (inputs padded to 32), b1, W2[128][128],
+ * b2, w3[128], b3, feature mean[24], feature inverse std[24]. Checkpoint and restore. */
+nomad_status nomad_mlp_get(nomad_ctx *ctx, float *out);
+nomad_status nomad_mlp_set(nomad_ctx *ctx, const float *in);
+
 /* ---- allocation-free closest hit (no counterpart in the reference) ----------------------
  * For callers that cannot allocate GPU memory while tracing: a frame loop whose memory budget
  * is fully committed to resident geometry, or one that cannot take the implicit device

@@ -118,13 +118,15 @@ typedef struct nomad_scene_owned nomad_scene_owned;
 nomad_status nomad_synth_icospheres(uint64_t seed, uint32_t instances, float extent,
                                     nomad_scene_owned **out);
 
-/* Procedural city: grid x grid cells on a `size_m` square; each cell is one object holding
+/* Procedural city: grid x grid_z cells of size_m / grid metres (x spans size_m); each cell is
+ * one object holding
  * a noise-displaced box or cylinder with a lognormal triangle count (median
  * `median_tris`, clamped to `max_tris`, rescaled to about `target_tris` in total), its
  * ground tile, and — for `emissive_quads` seeded cells — an emissive rectangle lamp.
  * `emissive_tris` extra small emissive triangles with lognormal power (sigma
  * `emissive_sigma`) are scattered over the roofs (0 for none). */
-nomad_status nomad_synth_city(uint64_t seed, uint32_t grid, float size_m, uint32_t target_tris,
+nomad_status nomad_synth_city(uint64_t seed, uint32_t grid, uint32_t grid_z, float size_m,
+                              uint32_t target_tris,
                               uint32_t median_tris, uint32_t max_tris, uint32_t emissive_quads,
                               uint32_t emissive_tris, float emissive_sigma,
                               nomad_scene_owned **out);

@@ -1,0 +1,611 @@
+// Learned residency scorer: MLP 24 -> 128 -> 128 -> 1 (ReLU), BF16 weights and activations,
+// FP32 accumulation on the tensor cores (mma.sync m16n8k16), trained on the device with AdamW.
+//
+// The GEMMs are tiny (2,048 objects x 128 x 128 per frame), so the kernels are built for
+// latency: the forward pass is one fused kernel (both hidden layers and the output dot product
+// with the weights resident in shared memory); training uses one generic BF16 GEMM kernel for
+// the backward products, with split-K partial sums reduced in a fixed order so training is
+// bit-reproducible for a given seed.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <random>
+#include <vector>
+
+#include "rt_context.h"
+
+namespace {
+
+constexpr int kIn = NOMAD_FEATURES;  // 24
+constexpr int kInPad = 32;
+constexpr int kHid = 128;
+// offsets in the fp32 parameter blob
+constexpr int oW1 = 0;
+constexpr int oB1 = oW1 + kHid * kInPad;
+constexpr int oW2 = oB1 + kHid;
+constexpr int oB2 = oW2 + kHid * kHid;
+constexpr int oW3 = oB2 + kHid;
+constexpr int oB3 = oW3 + kHid;
+constexpr int oMean = oB3 + 1;
+constexpr int oIstd = oMean + kIn;
+constexpr int kParams = oIstd + kIn;
+static_assert(kParams == NOMAD_MLP_PARAMS, "parameter blob layout");
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+  __nv_bfloat162 h = __floats2bfloat162_rn(a, b);  // a -> low half
+  return *reinterpret_cast<uint32_t *>(&h);
+}
+
+__device__ __forceinline__ void mma_bf16(float c[4], const uint32_t a[4], const uint32_t b[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// ---- fused forward ------------------------------------------------------------------------
+// Block: 4 warps, 64 rows (16 per warp). Shared: W1 [128][32], W2 [128][128], X [64][32],
+// H1 [64][128] in bf16 (row stride padded by 8 halves against bank conflicts).
+constexpr int kFwdRows = 64;
+constexpr int kS32 = kInPad + 8;   // row stride (halves) for 32-wide rows
+constexpr int kS128 = kHid + 8;    // row stride for 128-wide rows
+constexpr size_t kFwdSmem =
+    sizeof(__nv_bfloat16) * (kHid * kS32 + kHid * kS128 + kFwdRows * kS32 + kFwdRows * kS128) +
+    sizeof(float) * (3 * kHid + 1 + 2 * kIn);
+
+// X rows are raw features (fp32, n x 24); standardised with the blob's mean/istd on load.
+// Outputs: y[n]; when saving for backward also Z1 (pre-ReLU) and H2 (post-ReLU) as fp32 and
+// H1 (post-ReLU) and the standardised X as bf16.
+__global__ void __launch_bounds__(128) k_mlp_forward(const float *__restrict__ X, uint64_t n,
+                                                     const float *__restrict__ P,
+                                                     const __nv_bfloat16 *__restrict__ W1b,
+                                                     const __nv_bfloat16 *__restrict__ W2b,
+                                                     float *__restrict__ y, float *__restrict__ z1,
+                                                     __nv_bfloat16 *__restrict__ h1out,
+                                                     float *__restrict__ z2,
+                                                     __nv_bfloat16 *__restrict__ xout) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __nv_bfloat16 *sW1 = reinterpret_cast<__nv_bfloat16 *>(smem);
+  __nv_bfloat16 *sW2 = sW1 + kHid * kS32;
+  __nv_bfloat16 *sX = sW2 + kHid * kS128;
+  __nv_bfloat16 *sH1 = sX + kFwdRows * kS32;
+  float *sB1 = reinterpret_cast<float *>(sH1 + kFwdRows * kS128);
+  float *sB2 = sB1 + kHid;
+  float *sW3 = sB2 + kHid;
+  float *sB3 = sW3 + kHid;
+  float *sMean = sB3 + 1;
+  float *sIstd = sMean + kIn;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < kHid * kInPad; i += 128) sW1[(i / kInPad) * kS32 + i % kInPad] = W1b[i];
+  for (int i = tid; i < kHid * kHid; i += 128) sW2[(i / kHid) * kS128 + i % kHid] = W2b[i];
+  for (int i = tid; i < kHid; i += 128) {
+    sB1[i] = P[oB1 + i];
+    sB2[i] = P[oB2 + i];
+    sW3[i] = P[oW3 + i];
+  }
+  if (tid == 0) sB3[0] = P[oB3];
+  for (int i = tid; i < kIn; i += 128) {
+    sMean[i] = P[oMean + i];
+    sIstd[i] = P[oIstd + i];
+  }
+  __syncthreads();
+  const uint64_t row0 = (uint64_t)blockIdx.x * kFwdRows;
+  for (int i = tid; i < kFwdRows * kInPad; i += 128) {
+    int r = i / kInPad, f = i % kInPad;
+    float v = 0.0f;
+    if (f < kIn && row0 + r < n) v = (X[(row0 + r) * kIn + f] - sMean[f]) * sIstd[f];
+    __nv_bfloat16 b = __float2bfloat16_rn(v);
+    sX[r * kS32 + f] = b;
+    if (xout && row0 + r < n) xout[(row0 + r) * kInPad + f] = b;
+  }
+  __syncthreads();
+  const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, t4 = lane & 3;
+  const int wr = warp * 16;
+  // layer 1: [16 x 32] x [32 x 128]
+  float acc[16][4];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
+#pragma unroll
+  for (int ks = 0; ks < kInPad; ks += 16) {
+    uint32_t a[4];
+    a[0] = *reinterpret_cast<const uint32_t *>(sX + (wr + g) * kS32 + ks + t4 * 2);
+    a[1] = *reinterpret_cast<const uint32_t *>(sX + (wr + g + 8) * kS32 + ks + t4 * 2);
+    a[2] = *reinterpret_cast<const uint32_t *>(sX + (wr + g) * kS32 + ks + 8 + t4 * 2);
+    a[3] = *reinterpret_cast<const uint32_t *>(sX + (wr + g + 8) * kS32 + ks + 8 + t4 * 2);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      uint32_t b[2];
+      b[0] = *reinterpret_cast<const uint32_t *>(sW1 + (j * 8 + g) * kS32 + ks + t4 * 2);
+      b[1] = *reinterpret_cast<const uint32_t *>(sW1 + (j * 8 + g) * kS32 + ks + 8 + t4 * 2);
+      mma_bf16(acc[j], a, b);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    int c0 = j * 8 + t4 * 2;
+    float v0 = acc[j][0] + sB1[c0], v1 = acc[j][1] + sB1[c0 + 1];
+    float v2 = acc[j][2] + sB1[c0], v3 = acc[j][3] + sB1[c0 + 1];
+    uint64_t ra = row0 + wr + g, rb = ra + 8;
+    if (z1) {
+      if (ra < n) { z1[ra * kHid + c0] = v0; z1[ra * kHid + c0 + 1] = v1; }
+      if (rb < n) { z1[rb * kHid + c0] = v2; z1[rb * kHid + c0 + 1] = v3; }
+    }
+    uint32_t pa = pack_bf16(fmaxf(v0, 0.0f), fmaxf(v1, 0.0f));
+    uint32_t pb = pack_bf16(fmaxf(v2, 0.0f), fmaxf(v3, 0.0f));
+    *reinterpret_cast<uint32_t *>(sH1 + (wr + g) * kS128 + c0) = pa;
+    *reinterpret_cast<uint32_t *>(sH1 + (wr + g + 8) * kS128 + c0) = pb;
+    if (h1out) {
+      if (ra < n) *reinterpret_cast<uint32_t *>(h1out + ra * kHid + c0) = pa;
+      if (rb < n) *reinterpret_cast<uint32_t *>(h1out + rb * kHid + c0) = pb;
+    }
+  }
+  __syncwarp();
+  // layer 2: [16 x 128] x [128 x 128]
+#pragma unroll
+  for (int j = 0; j < 16; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
+#pragma unroll 2
+  for (int ks = 0; ks < kHid; ks += 16) {
+    uint32_t a[4];
+    a[0] = *reinterpret_cast<const uint32_t *>(sH1 + (wr + g) * kS128 + ks + t4 * 2);
+    a[1] = *reinterpret_cast<const uint32_t *>(sH1 + (wr + g + 8) * kS128 + ks + t4 * 2);
+    a[2] = *reinterpret_cast<const uint32_t *>(sH1 + (wr + g) * kS128 + ks + 8 + t4 * 2);
+    a[3] = *reinterpret_cast<const uint32_t *>(sH1 + (wr + g + 8) * kS128 + ks + 8 + t4 * 2);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      uint32_t b[2];
+      b[0] = *reinterpret_cast<const uint32_t *>(sW2 + (j * 8 + g) * kS128 + ks + t4 * 2);
+      b[1] = *reinterpret_cast<const uint32_t *>(sW2 + (j * 8 + g) * kS128 + ks + 8 + t4 * 2);
+      mma_bf16(acc[j], a, b);
+    }
+  }
+  // layer 3: relu(acc + b2) . w3 + b3
+  float sa = 0.0f, sb = 0.0f;
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    int c0 = j * 8 + t4 * 2;
+    float v0 = acc[j][0] + sB2[c0], v1 = acc[j][1] + sB2[c0 + 1];
+    float v2 = acc[j][2] + sB2[c0], v3 = acc[j][3] + sB2[c0 + 1];
+    uint64_t ra = row0 + wr + g, rb = ra + 8;
+    if (z2) {
+      if (ra < n) { z2[ra * kHid + c0] = v0; z2[ra * kHid + c0 + 1] = v1; }
+      if (rb < n) { z2[rb * kHid + c0] = v2; z2[rb * kHid + c0 + 1] = v3; }
+    }
+    sa += fmaxf(v0, 0.0f) * sW3[c0] + fmaxf(v1, 0.0f) * sW3[c0 + 1];
+    sb += fmaxf(v2, 0.0f) * sW3[c0] + fmaxf(v3, 0.0f) * sW3[c0 + 1];
+  }
+  sa += __shfl_xor_sync(0xffffffffu, sa, 1);
+  sa += __shfl_xor_sync(0xffffffffu, sa, 2);
+  sb += __shfl_xor_sync(0xffffffffu, sb, 1);
+  sb += __shfl_xor_sync(0xffffffffu, sb, 2);
+  if (t4 == 0) {
+    uint64_t ra = row0 + wr + g, rb = ra + 8;
+    if (ra < n) y[ra] = sa + sB3[0];
+    if (rb < n) y[rb] = sb + sB3[0];
+  }
+}
+
+// ---- generic BF16 GEMM for the backward pass ------------------------------------------------
+// C[z][M][N] (fp32) = sum over this split's K range of op(A)[M][K] * op(B)[K][N].
+// A is stored [M][K] (transA = 0) or [K][M] (transA = 1); B is stored [K][N] (transB = 0) or
+// [N][K] (transB = 1). Block tile 64 x 64, 4 warps of 32 x 32, K step 16.
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(128) k_gemm_bf16(const __nv_bfloat16 *__restrict__ A,
+                                                   const __nv_bfloat16 *__restrict__ B,
+                                                   float *__restrict__ C, int M, int N, int K,
+                                                   int lda, int ldb, int kPerSplit) {
+  __shared__ __align__(16) __nv_bfloat16 As[64][24];
+  __shared__ __align__(16) __nv_bfloat16 Bs[64][24];  // [n][k]
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t4 = lane & 3;
+  const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
+  const int kBeg = blockIdx.z * kPerSplit, kEnd = min(K, kBeg + kPerSplit);
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+  float acc[2][4][4];
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = acc[a][b][2] = acc[a][b][3] = 0.0f;
+  const __nv_bfloat16 zero = __float2bfloat16_rn(0.0f);
+  for (int k0 = kBeg; k0 < kEnd; k0 += 16) {
+    for (int i = tid; i < 64 * 16; i += 128) {
+      int r = i / 16, c = i % 16;
+      int m = m0 + r, k = k0 + c;
+      __nv_bfloat16 v = zero;
+      if (m < M && k < kEnd) v = TA ? A[(size_t)k * lda + m] : A[(size_t)m * lda + k];
+      As[r][c] = v;
+      int nn = n0 + r;
+      __nv_bfloat16 w = zero;
+      if (nn < N && k < kEnd) w = TB ? B[(size_t)nn * ldb + k] : B[(size_t)k * ldb + nn];
+      Bs[r][c] = w;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+      uint32_t af[4];
+      int r = wm + a * 16;
+      af[0] = *reinterpret_cast<const uint32_t *>(&As[r + g][t4 * 2]);
+      af[1] = *reinterpret_cast<const uint32_t *>(&As[r + g + 8][t4 * 2]);
+      af[2] = *reinterpret_cast<const uint32_t *>(&As[r + g][8 + t4 * 2]);
+      af[3] = *reinterpret_cast<const uint32_t *>(&As[r + g + 8][8 + t4 * 2]);
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        uint32_t bf[2];
+        int c = wn + b * 8;
+        bf[0] = *reinterpret_cast<const uint32_t *>(&Bs[c + g][t4 * 2]);
+        bf[1] = *reinterpret_cast<const uint32_t *>(&Bs[c + g][8 + t4 * 2]);
+        mma_bf16(acc[a][b], af, bf);
+      }
+    }
+    __syncthreads();
+  }
+  float *Cz = C + (size_t)blockIdx.z * M * N;
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      int r = m0 + wm + a * 16 + g, c = n0 + wn + b * 8 + t4 * 2;
+      if (r < M && c < N) Cz[(size_t)r * N + c] = acc[a][b][0];
+      if (r < M && c + 1 < N) Cz[(size_t)r * N + c + 1] = acc[a][b][1];
+      if (r + 8 < M && c < N) Cz[(size_t)(r + 8) * N + c] = acc[a][b][2];
+      if (r + 8 < M && c + 1 < N) Cz[(size_t)(r + 8) * N + c + 1] = acc[a][b][3];
+    }
+}
+
+// Sums split-K partials in fixed order: out[i] = sum_z part[z][i].
+__global__ void k_reduce_splits(const float *__restrict__ part, int splits, size_t count,
+                                float *__restrict__ out) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x) {
+    float s = 0.0f;
+    for (int z = 0; z < splits; ++z) s += part[(size_t)z * count + i];
+    out[i] = s;
+  }
+}
+
+// dy = 2 (y - t) / B; per-row squared errors for the loss.
+__global__ void k_mse_grad(const float *__restrict__ y, const float *__restrict__ t, int B,
+                           float *__restrict__ dy, float *__restrict__ se) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < B) {
+    float d = y[i] - t[i];
+    dy[i] = 2.0f * d / (float)B;
+    se[i] = d * d;
+  }
+}
+
+// dZ2 = dy * w3 * (Z2 > 0) (bf16 for the GEMMs, fp32 kept for the bias gradient).
+__global__ void k_dz2(const float *__restrict__ dy, const float *__restrict__ z2, const float *__restrict__ P,
+                      int B, __nv_bfloat16 *__restrict__ dz2b, float *__restrict__ dz2f) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < B * kHid) {
+    int r = i / kHid, c = i % kHid;
+    float v = z2[i] > 0.0f ? dy[r] * P[oW3 + c] : 0.0f;
+    dz2f[i] = v;
+    dz2b[i] = __float2bfloat16_rn(v);
+  }
+}
+
+// dZ1 = dH1 * (Z1 > 0).
+__global__ void k_dz1(const float *__restrict__ dh1, const float *__restrict__ z1, int B,
+                      __nv_bfloat16 *__restrict__ dz1b, float *__restrict__ dz1f) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < B * kHid) {
+    float v = z1[i] > 0.0f ? dh1[i] : 0.0f;
+    dz1f[i] = v;
+    dz1b[i] = __float2bfloat16_rn(v);
+  }
+}
+
+// Column sums in fixed row order: out[c] = sum_r M[r][c] * (w ? w[r] : 1); one thread per column.
+__global__ void k_colsum(const float *__restrict__ M, const float *__restrict__ w, int rows, int cols,
+                         float *__restrict__ out) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < cols) {
+    float s = 0.0f;
+    for (int r = 0; r < rows; ++r) s += M[(size_t)r * cols + c] * (w ? w[r] : 1.0f);
+    out[c] = s;
+  }
+}
+
+// AdamW over the trainable part of the blob (everything before the feature statistics).
+__global__ void k_adamw(float *__restrict__ P, const float *__restrict__ G, float *__restrict__ m,
+                        float *__restrict__ v, int count, float lr, float b1, float b2, float eps,
+                        float wd, float bc1, float bc2) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < count) {
+    float g = G[i];
+    float mi = b1 * m[i] + (1.0f - b1) * g;
+    float vi = b2 * v[i] + (1.0f - b2) * g * g;
+    m[i] = mi;
+    v[i] = vi;
+    float mh = mi / bc1, vh = vi / bc2;
+    bool isWeight = (i < oB1) || (i >= oW2 && i < oB2) || (i >= oW3 && i < oB3);
+    float p = P[i];
+    if (isWeight) p = p - lr * wd * p;
+    P[i] = p - lr * mh / (sqrtf(vh) + eps);
+  }
+}
+
+// bf16 copies of W1 and W2 (W1's padded input columns stay zero).
+__global__ void k_refresh_bf16(const float *__restrict__ P, __nv_bfloat16 *__restrict__ W1b,
+                               __nv_bfloat16 *__restrict__ W2b) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < kHid * kInPad) W1b[i] = __float2bfloat16_rn((i % kInPad) < kIn ? P[oW1 + i] : 0.0f);
+  if (i < kHid * kHid) W2b[i] = __float2bfloat16_rn(P[oW2 + i]);
+}
+
+// Gathers a mini-batch of raw features and targets.
+__global__ void k_gather(const float *__restrict__ X, const float *__restrict__ T, const uint32_t *__restrict__ idx,
+                         int B, float *__restrict__ xb, float *__restrict__ tb) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < B * kIn) xb[i] = X[(size_t)idx[i / kIn] * kIn + i % kIn];
+  if (i < B) tb[i] = T[idx[i]];
+}
+
+}  // namespace
+
+// ---- host side ------------------------------------------------------------------------------
+
+struct MlpState {
+  bool ready = false;
+  DeviceBuf P, W1b, W2b, M, V, G;
+  DeviceBuf X, T, idx, xb, tb, y, z1, h1, z2, xbf, dy, se, dz2b, dz2f, dh1, dz1b, dz1f, part;
+  uint64_t trainCap = 0;
+  int batchCap = 0;
+  DeviceBuf inX, inY;
+};
+
+namespace {
+MlpState &mlp(nomad_ctx *ctx) {
+  static_assert(sizeof(MlpState) > 0, "");
+  if (!ctx->mlp) ctx->mlp = new MlpState();
+  return *static_cast<MlpState *>(ctx->mlp);
+}
+
+nomad_status refresh(nomad_ctx *ctx, MlpState &S) {
+  int n = kHid * kHid;
+  k_refresh_bf16<<<(n + 255) / 256, 256, 0, ctx->stream>>>(S.P.as<const float>(), S.W1b.as<__nv_bfloat16>(),
+                                                            S.W2b.as<__nv_bfloat16>());
+  NOMAD_CUDA(ctx, cudaGetLastError());
+  return NOMAD_OK;
+}
+
+nomad_status ensure(nomad_ctx *ctx, MlpState &S) {
+  NOMAD_CUDA(ctx, S.P.reserve(kParams * 4));
+  NOMAD_CUDA(ctx, S.W1b.reserve(kHid * kInPad * 2));
+  NOMAD_CUDA(ctx, S.W2b.reserve(kHid * kHid * 2));
+  NOMAD_CUDA(ctx, S.M.reserve(kParams * 4));
+  NOMAD_CUDA(ctx, S.V.reserve(kParams * 4));
+  NOMAD_CUDA(ctx, S.G.reserve(kParams * 4));
+  static bool attr = false;
+  if (!attr) {
+    NOMAD_CUDA(ctx, cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwdSmem));
+    attr = true;
+  }
+  return NOMAD_OK;
+}
+}  // namespace
+
+void nomad_mlp_free(void *p) { delete static_cast<MlpState *>(p); }
+
+// Inference on device features (n x 24 fp32) into y (n fp32), on the context stream.
+nomad_status nomad_mlp_infer_device(nomad_ctx *ctx, const float *X, uint64_t n, float *y) {
+  MlpState &S = mlp(ctx);
+  if (!S.ready) return nomad_fail(ctx, NOMAD_ERR_NOT_READY, "MLP not initialised or trained");
+  if (n == 0) return NOMAD_OK;
+  unsigned blocks = (unsigned)((n + kFwdRows - 1) / kFwdRows);
+  k_mlp_forward<<<blocks, 128, kFwdSmem, ctx->stream>>>(X, n, S.P.as<const float>(), S.W1b.as<const __nv_bfloat16>(),
+                                                        S.W2b.as<const __nv_bfloat16>(), y, nullptr, nullptr,
+                                                        nullptr, nullptr);
+  NOMAD_CUDA(ctx, cudaGetLastError());
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_mlp_init(nomad_ctx *ctx, uint64_t seed) {
+  if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
+  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  MlpState &S = mlp(ctx);
+  nomad_status st = ensure(ctx, S);
+  if (st != NOMAD_OK) return st;
+  std::vector<float> p(kParams, 0.0f);
+  std::mt19937_64 rng(seed);
+  auto uni = [&](float lim) { return (float)(((rng() >> 11) * (1.0 / 9007199254740992.0)) * 2.0 - 1.0) * lim; };
+  float l1 = std::sqrt(6.0f / kIn), l2 = std::sqrt(6.0f / kHid), l3 = std::sqrt(3.0f / kHid);
+  for (int o = 0; o < kHid; ++o)
+    for (int i = 0; i < kIn; ++i) p[oW1 + o * kInPad + i] = uni(l1);
+  for (int i = 0; i < kHid * kHid; ++i) p[oW2 + i] = uni(l2);
+  for (int i = 0; i < kHid; ++i) p[oW3 + i] = uni(l3);
+  for (int i = 0; i < kIn; ++i) p[oIstd + i] = 1.0f;
+  NOMAD_CUDA(ctx, cudaMemcpy(S.P.p, p.data(), kParams * 4, cudaMemcpyHostToDevice));
+  NOMAD_CUDA(ctx, cudaMemset(S.M.p, 0, kParams * 4));
+  NOMAD_CUDA(ctx, cudaMemset(S.V.p, 0, kParams * 4));
+  st = refresh(ctx, S);
+  if (st != NOMAD_OK) return st;
+  S.ready = true;
+  NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_mlp_get(nomad_ctx *ctx, float *out) {
+  if (!ctx || !out) return NOMAD_ERR_INVALID_ARGUMENT;
+  MlpState &S = mlp(ctx);
+  if (!S.ready) return nomad_fail(ctx, NOMAD_ERR_NOT_READY, "MLP not initialised");
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(out, S.P.p, kParams * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_mlp_set(nomad_ctx *ctx, const float *in) {
+  if (!ctx || !in) return NOMAD_ERR_INVALID_ARGUMENT;
+  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  MlpState &S = mlp(ctx);
+  nomad_status st = ensure(ctx, S);
+  if (st != NOMAD_OK) return st;
+  NOMAD_CUDA(ctx, cudaMemcpy(S.P.p, in, kParams * 4, cudaMemcpyHostToDevice));
+  NOMAD_CUDA(ctx, cudaMemset(S.M.p, 0, kParams * 4));
+  NOMAD_CUDA(ctx, cudaMemset(S.V.p, 0, kParams * 4));
+  st = refresh(ctx, S);
+  if (st != NOMAD_OK) return st;
+  S.ready = true;
+  NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_mlp_infer(nomad_ctx *ctx, const float *features, uint64_t n, float *out,
+                                        uint32_t flags) {
+  if (!ctx || (!features && n) || (!out && n)) return NOMAD_ERR_INVALID_ARGUMENT;
+  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  MlpState &S = mlp(ctx);
+  if (flags & NOMAD_TRACE_DEVICE_POINTERS) return nomad_mlp_infer_device(ctx, features, n, out);
+  NOMAD_CUDA(ctx, S.inX.reserve(std::max<uint64_t>(1, n) * kIn * 4));
+  NOMAD_CUDA(ctx, S.inY.reserve(std::max<uint64_t>(1, n) * 4));
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(S.inX.p, features, n * kIn * 4, cudaMemcpyHostToDevice, ctx->stream));
+  nomad_status st = nomad_mlp_infer_device(ctx, S.inX.as<const float>(), n, S.inY.as<float>());
+  if (st != NOMAD_OK) return st;
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(out, S.inY.p, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_mlp_train(nomad_ctx *ctx, const float *features, const float *targets, uint64_t n,
+                                        uint32_t steps, uint32_t batch, float lr, float wd, uint64_t seed,
+                                        float *loss_out) {
+  if (!ctx || !features || !targets || n == 0 || batch == 0 || batch % 64 != 0 || batch > 65536)
+    return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "training needs samples and a batch that is a multiple of 64");
+  if (n > 0xffffffffull) return nomad_fail(ctx, NOMAD_ERR_LIMIT, "too many samples");
+  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  MlpState &S = mlp(ctx);
+  if (!S.ready) {
+    nomad_status st = nomad_mlp_init(ctx, seed);
+    if (st != NOMAD_OK) return st;
+  }
+  cudaStream_t s = ctx->stream;
+  // Feature statistics (double accumulation on the host), stored in the blob.
+  std::vector<double> mean(kIn, 0.0), sq(kIn, 0.0);
+  for (uint64_t i = 0; i < n; ++i)
+    for (int f = 0; f < kIn; ++f) {
+      double v = features[i * kIn + f];
+      mean[f] += v;
+      sq[f] += v * v;
+    }
+  float stats[2 * kIn];
+  for (int f = 0; f < kIn; ++f) {
+    double m = mean[f] / n;
+    double var = std::max(0.0, sq[f] / n - m * m);
+    stats[f] = (float)m;
+    stats[kIn + f] = (float)(1.0 / std::max(std::sqrt(var), 1e-6));
+  }
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(S.P.as<float>() + oMean, stats, sizeof(stats), cudaMemcpyHostToDevice, s));
+  const int B = (int)batch;
+  if (S.trainCap < n) {
+    NOMAD_CUDA(ctx, S.X.reserve(n * kIn * 4));
+    NOMAD_CUDA(ctx, S.T.reserve(n * 4));
+    S.trainCap = n;
+  }
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(S.X.p, features, n * kIn * 4, cudaMemcpyHostToDevice, s));
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(S.T.p, targets, n * 4, cudaMemcpyHostToDevice, s));
+  const int splits = std::max(1, std::min(32, B / 256));
+  if (S.batchCap < B) {
+    NOMAD_CUDA(ctx, S.idx.reserve((size_t)B * 4));
+    NOMAD_CUDA(ctx, S.xb.reserve((size_t)B * kIn * 4));
+    NOMAD_CUDA(ctx, S.tb.reserve((size_t)B * 4));
+    NOMAD_CUDA(ctx, S.y.reserve((size_t)B * 4));
+    NOMAD_CUDA(ctx, S.z1.reserve((size_t)B * kHid * 4));
+    NOMAD_CUDA(ctx, S.h1.reserve((size_t)B * kHid * 2));
+    NOMAD_CUDA(ctx, S.z2.reserve((size_t)B * kHid * 4));
+    NOMAD_CUDA(ctx, S.xbf.reserve((size_t)B * kInPad * 2));
+    NOMAD_CUDA(ctx, S.dy.reserve((size_t)B * 4));
+    NOMAD_CUDA(ctx, S.se.reserve((size_t)B * 4));
+    NOMAD_CUDA(ctx, S.dz2b.reserve((size_t)B * kHid * 2));
+    NOMAD_CUDA(ctx, S.dz2f.reserve((size_t)B * kHid * 4));
+    NOMAD_CUDA(ctx, S.dh1.reserve((size_t)B * kHid * 4));
+    NOMAD_CUDA(ctx, S.dz1b.reserve((size_t)B * kHid * 2));
+    NOMAD_CUDA(ctx, S.dz1f.reserve((size_t)B * kHid * 4));
+    S.batchCap = B;
+  }
+  NOMAD_CUDA(ctx, S.part.reserve((size_t)std::max(splits, 1) * kHid * kHid * 4));
+  std::mt19937_64 rng(seed ^ 0x5EEDull);
+  std::vector<uint32_t> perm(n);
+  std::iota(perm.begin(), perm.end(), 0u);
+  uint64_t cursor = n;
+  std::vector<float> se(B);
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  float *Pm = S.P.as<float>(), *G = S.G.as<float>();
+  for (uint32_t step = 0; step < steps; ++step) {
+    if (cursor + B > n) {
+      std::shuffle(perm.begin(), perm.end(), rng);
+      cursor = 0;
+    }
+    std::vector<uint32_t> bidx(B);
+    for (int i = 0; i < B; ++i) bidx[i] = perm[(cursor + i) % n];
+    cursor += B;
+    NOMAD_CUDA(ctx, cudaMemcpyAsync(S.idx.p, bidx.data(), (size_t)B * 4, cudaMemcpyHostToDevice, s));
+    k_gather<<<(B * kIn + 255) / 256, 256, 0, s>>>(S.X.as<const float>(), S.T.as<const float>(),
+                                                   S.idx.as<const uint32_t>(), B, S.xb.as<float>(), S.tb.as<float>());
+    k_mlp_forward<<<B / kFwdRows, 128, kFwdSmem, s>>>(S.xb.as<const float>(), B, Pm, S.W1b.as<const __nv_bfloat16>(),
+                                                      S.W2b.as<const __nv_bfloat16>(), S.y.as<float>(), S.z1.as<float>(),
+                                                      S.h1.as<__nv_bfloat16>(), S.z2.as<float>(),
+                                                      S.xbf.as<__nv_bfloat16>());
+    k_mse_grad<<<(B + 255) / 256, 256, 0, s>>>(S.y.as<const float>(), S.tb.as<const float>(), B, S.dy.as<float>(),
+                                               S.se.as<float>());
+    // H2 = relu(Z2) is needed for dw3: recompute on the fly in a column sum over z2 via a mask.
+    k_dz2<<<(B * kHid + 255) / 256, 256, 0, s>>>(S.dy.as<const float>(), S.z2.as<const float>(), Pm, B,
+                                                 S.dz2b.as<__nv_bfloat16>(), S.dz2f.as<float>());
+    // dw3[c] = sum_r relu(z2[r][c]) * dy[r]; db3 = sum_r dy[r]
+    {
+      // relu in place is not allowed (z2 feeds dz2 above, already consumed): use dh1 as scratch.
+      float *h2 = S.dh1.as<float>();
+      size_t cnt = (size_t)B * kHid;
+      // h2 = max(z2, 0)
+      k_dz1<<<(unsigned)((cnt + 255) / 256), 256, 0, s>>>(S.z2.as<const float>(), S.z2.as<const float>(), B,
+                                                         S.dz1b.as<__nv_bfloat16>(), h2);
+      k_colsum<<<1, kHid, 0, s>>>(h2, S.dy.as<const float>(), B, kHid, G + oW3);
+      k_colsum<<<1, 1, 0, s>>>(S.dy.as<const float>(), nullptr, B, 1, G + oB3);
+    }
+    k_colsum<<<1, kHid, 0, s>>>(S.dz2f.as<const float>(), nullptr, B, kHid, G + oB2);
+    // dW2[n][k] = sum_i dZ2[i][n] H1[i][k]: A = dZ2^T (stored [B][128]), B = H1 [B][128]
+    {
+      int kPer = ((B / splits) + 15) / 16 * 16;
+      int sp = (B + kPer - 1) / kPer;
+      dim3 grid(kHid / 64, kHid / 64, sp);
+      k_gemm_bf16<true, false><<<grid, 128, 0, s>>>(S.dz2b.as<const __nv_bfloat16>(), S.h1.as<const __nv_bfloat16>(),
+                                                    S.part.as<float>(), kHid, kHid, B, kHid, kHid, kPer);
+      k_reduce_splits<<<64, 256, 0, s>>>(S.part.as<const float>(), sp, (size_t)kHid * kHid, G + oW2);
+    }
+    // dH1[i][k] = sum_n dZ2[i][n] W2[n][k]: A = dZ2 [B][128], B = W2 [128(n)][128(k)] row-major = [K][N]
+    {
+      dim3 grid(kHid / 64, (B + 63) / 64, 1);
+      k_gemm_bf16<false, false><<<grid, 128, 0, s>>>(S.dz2b.as<const __nv_bfloat16>(), S.W2b.as<const __nv_bfloat16>(),
+                                                     S.dh1.as<float>(), B, kHid, kHid, kHid, kHid, kHid);
+    }
+    k_dz1<<<(B * kHid + 255) / 256, 256, 0, s>>>(S.dh1.as<const float>(), S.z1.as<const float>(), B,
+                                                 S.dz1b.as<__nv_bfloat16>(), S.dz1f.as<float>());
+    k_colsum<<<1, kHid, 0, s>>>(S.dz1f.as<const float>(), nullptr, B, kHid, G + oB1);
+    // dW1[n][k] = sum_i dZ1[i][n] X[i][k]: A = dZ1^T, B = Xbf [B][32]
+    {
+      int kPer = ((B / splits) + 15) / 16 * 16;
+      int sp = (B + kPer - 1) / kPer;
+      dim3 grid(1, kHid / 64, sp);
+      k_gemm_bf16<true, false><<<grid, 128, 0, s>>>(S.dz1b.as<const __nv_bfloat16>(), S.xbf.as<const __nv_bfloat16>(),
+                                                    S.part.as<float>(), kHid, kInPad, B, kHid, kInPad, kPer);
+      k_reduce_splits<<<16, 256, 0, s>>>(S.part.as<const float>(), sp, (size_t)kHid * kInPad, G + oW1);
+    }
+    float bc1 = 1.0f - std::pow(b1, (float)(step + 1)), bc2 = 1.0f - std::pow(b2, (float)(step + 1));
+    k_adamw<<<(oMean + 255) / 256, 256, 0, s>>>(Pm, G, S.M.as<float>(), S.V.as<float>(), oMean, lr, b1, b2, eps, wd,
+                                                bc1, bc2);
+    nomad_status st = refresh(ctx, S);
+    if (st != NOMAD_OK) return st;
+    NOMAD_CUDA(ctx, cudaGetLastError());
+    if (loss_out) {
+      NOMAD_CUDA(ctx, cudaMemcpyAsync(se.data(), S.se.p, (size_t)B * 4, cudaMemcpyDeviceToHost, s));
+      NOMAD_CUDA(ctx, cudaStreamSynchronize(s));
+      double acc = 0.0;
+      for (int i = 0; i < B; ++i) acc += se[i];
+      loss_out[step] = (float)(acc / B);
+    }
+  }
+  NOMAD_CUDA(ctx, cudaStreamSynchronize(s));
+  return NOMAD_OK;
+}

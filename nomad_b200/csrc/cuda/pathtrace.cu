@@ -50,8 +50,7 @@ struct Counters {
 struct Lights {
   const uint32_t *idx;
   const float *cdf;
-  uint32_t count;
-  float total;
+  const LightMeta *meta;
 };
 
 __device__ __forceinline__ const ViewDev &find_view(const ViewDev *views, uint32_t nviews,
@@ -361,15 +360,15 @@ __device__ __forceinline__ bool sample_light(const float4 *__restrict__ prims, u
 }
 
 // selectLightOffset (PathTracing.h:219-235).
-__device__ __forceinline__ uint32_t select_light(float xi, const Lights &L) {
-  float target = xi * L.total;
-  uint32_t lo = 0, hi = L.count;
+__device__ __forceinline__ uint32_t select_light(float xi, const Lights &L, uint32_t count, float total) {
+  float target = xi * total;
+  uint32_t lo = 0, hi = count;
   while (lo < hi) {
     uint32_t mid = (lo + hi) / 2;
     if (__ldg(L.cdf + mid) < target) lo = mid + 1;
     else hi = mid;
   }
-  return lo < L.count - 1 ? lo : L.count - 1;
+  return lo < count - 1 ? lo : count - 1;
 }
 
 __global__ void __launch_bounds__(kPtBlock) k_shade(
@@ -380,6 +379,8 @@ __global__ void __launch_bounds__(kPtBlock) k_shade(
     const float4 *__restrict__ prims, const float4 *__restrict__ mats, Lights L, Counters *cnt, int cur,
     uint32_t *__restrict__ objHits, int restirDepth0) {
   const uint32_t n = cnt->qlen[cur];
+  const uint32_t lightCount = L.meta->count;
+  const float lightTotal = L.meta->total;
   uint32_t *nextLen = &cnt->qlen[cur ^ 1];
   uint32_t *shadowLen = &cnt->qlen[2];
   uint32_t stride = gridDim.x * blockDim.x;
@@ -429,8 +430,8 @@ __global__ void __launch_bounds__(kPtBlock) k_shade(
         }
         V3 dc = m.diffuse * m.opacity;
         bool restirHere = restirDepth0 && depth == 0 && (v.flags & NOMAD_VIEW_RESTIR);
-        if (!restirHere && luminance(dc) > 0.0f && L.count > 0 && L.total > 0.0f) {
-          uint32_t off = select_light(u01(b0.x), L);
+        if (!restirHere && luminance(dc) > 0.0f && lightCount > 0 && lightTotal > 0.0f) {
+          uint32_t off = select_light(u01(b0.x), L, lightCount, lightTotal);
           uint32_t lp = __ldg(L.idx + off);
           if ((int32_t)lp != prim) {
             V3 lpos, lnrm;
@@ -447,7 +448,7 @@ __global__ void __launch_bounds__(kPtBlock) k_shade(
                   float cur_ = __ldg(L.cdf + off);
                   float prev = off > 0 ? __ldg(L.cdf + off - 1) : 0.0f;
                   float wgt = cur_ - prev;
-                  float lpdf = (L.total > 0.0f && wgt > 0.0f) ? wgt / L.total : 0.0f;
+                  float lpdf = (lightTotal > 0.0f && wgt > 0.0f) ? wgt / lightTotal : 0.0f;
                   if (lpdf > 0.0f) {
                     float pdfArea = 1.0f / area;
                     float pdfSolid = pdfArea * dist2 / cosL;
@@ -584,78 +585,7 @@ __global__ void __launch_bounds__(kPtBlock) k_finalize(const ViewDev *__restrict
 
 }  // namespace
 
-// Light CDF over active emissive primitives (Renderer.cpp:5161-5211; primitiveArea :1462-1480).
-void nomad_build_lights(const nomad_ctx *ctx, LightTables &out) {
-  out = LightTables();
-  const float *P = ctx->hostPrims.data();
-  const float *M = ctx->hostMaterials.data();
-  out.pdfLookup.assign(ctx->primCount, 0.0f);
-  float total = 0.0f;
-  for (uint32_t i = 0; i < ctx->primCount; ++i) {
-    if (!ctx->primActive[i]) continue;
-    if (!ctx->objResident[ctx->layout.primObject[i]]) continue;
-    const float *m = M + 20ull * i;
-    float strength = m[11] * (m[8] * 0.2126f + m[9] * 0.7152f + m[10] * 0.0722f);
-    if (!(strength > 0.0f)) continue;
-    const float *g = P + 28ull * i;
-    int type = (int)g[3];
-    float area = 0.0f;
-    if (type == 0) {
-      float r = g[4];
-      area = 4.0f * 3.14159265358979323846f * r * r;
-    } else {
-      float ax, ay, az, bx, by, bz;
-      if (type == 1) {
-        ax = g[4] - g[0]; ay = g[5] - g[1]; az = g[6] - g[2];
-        bx = g[8] - g[0]; by = g[9] - g[1]; bz = g[10] - g[2];
-      } else {
-        ax = g[4]; ay = g[5]; az = g[6];
-        bx = g[8]; by = g[9]; bz = g[10];
-      }
-      float cx = ay * bz - az * by, cy = az * bx - ax * bz, cz = ax * by - ay * bx;
-      float len = std::sqrt(cx * cx + cy * cy + cz * cz);
-      area = type == 1 ? 0.5f * len : 4.0f * len;
-    }
-    if (!(area > 0.0f)) continue;
-    float w = area * strength;
-    if (!(w > 0.0f)) continue;
-    total += w;
-    out.indices.push_back(i);
-    out.cdf.push_back(total);
-  }
-  out.total = total;
-  if (total > 0.0f) {
-    float prev = 0.0f;
-    for (size_t k = 0; k < out.cdf.size(); ++k) {
-      float w = out.cdf[k] - prev;
-      prev = out.cdf[k];
-      if (w <= 0.0f) continue;
-      out.pdfLookup[out.indices[k]] = w / total;
-    }
-  }
-}
-
 namespace {
-
-nomad_status upload_lights(nomad_ctx *ctx) {
-  FrameState &F = ctx->frame;
-  if (!F.lightsDirty) return NOMAD_OK;
-  LightTables L;
-  nomad_build_lights(ctx, L);
-  size_t n = std::max<size_t>(1, L.indices.size());
-  NOMAD_CUDA(ctx, F.lightIdx.reserve(n * 4));
-  NOMAD_CUDA(ctx, F.lightCdf.reserve(n * 4));
-  NOMAD_CUDA(ctx, F.lightPdf.reserve((size_t)ctx->primCount * 4));
-  if (!L.indices.empty()) {
-    NOMAD_CUDA(ctx, cudaMemcpy(F.lightIdx.p, L.indices.data(), L.indices.size() * 4, cudaMemcpyHostToDevice));
-    NOMAD_CUDA(ctx, cudaMemcpy(F.lightCdf.p, L.cdf.data(), L.cdf.size() * 4, cudaMemcpyHostToDevice));
-  }
-  NOMAD_CUDA(ctx, cudaMemcpy(F.lightPdf.p, L.pdfLookup.data(), (size_t)ctx->primCount * 4, cudaMemcpyHostToDevice));
-  F.lightCount = static_cast<uint32_t>(L.indices.size());
-  F.lightTotal = L.total;
-  F.lightsDirty = false;
-  return NOMAD_OK;
-}
 
 int persist_blocks(nomad_ctx *ctx, const void *fn, int block) {
   int perSm = 0;
@@ -750,7 +680,7 @@ extern "C" nomad_status nomad_render_frame(nomad_ctx *ctx, const nomad_view *vie
   }
   if (P > 0xffffffffull) return nomad_fail(ctx, NOMAD_ERR_LIMIT, "more than 2^32 paths in one frame");
   FrameState &F = ctx->frame;
-  nomad_status st = upload_lights(ctx);
+  nomad_status st = nomad_lights_update(ctx);
   if (st != NOMAD_OK) return st;
   if (F.capacity < P) {
     NOMAD_CUDA(ctx, F.thr.reserve(P * 16));
@@ -782,7 +712,7 @@ extern "C" nomad_status nomad_render_frame(nomad_ctx *ctx, const nomad_view *vie
   k_raygen<<<gridPT, kPtBlock, 0, s>>>(V, nviews, P, F.qRays[0].as<float4>(), F.qIds[0].as<uint32_t>(),
                                       F.thr.as<float4>(), F.rad.as<float4>(), C);
   NOMAD_CUDA(ctx, cudaGetLastError());
-  Lights L{F.lightIdx.as<const uint32_t>(), F.lightCdf.as<const float>(), F.lightCount, F.lightTotal};
+  Lights L{F.lightIdx.as<const uint32_t>(), F.lightCdf.as<const float>(), F.lightMeta.as<const LightMeta>()};
   uint32_t *objHits = (flags & NOMAD_TRACE_COUNT_HITS) ? ctx->objHits.as<uint32_t>() : nullptr;
   int gClosest = persist_blocks(ctx, (const void *)k_trace_queue<false>, kTraceBlock);
   int gAny = persist_blocks(ctx, (const void *)k_trace_queue<true>, kTraceBlock);

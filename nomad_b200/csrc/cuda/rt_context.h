@@ -31,13 +31,10 @@ struct DeviceBuf {
   template <typename T> T *as() const { return static_cast<T *>(p); }
 };
 
-// Light-sampling tables over the active emissive primitives, restated from the light CDF build
-// of Renderer::rebuildResidentResources (Renderer.cpp:5161-5211).
-struct LightTables {
-  std::vector<uint32_t> indices;  // primitive index of each light
-  std::vector<float> cdf;         // running sum of area * emission strength
-  std::vector<float> pdfLookup;   // per primitive: weight / total (0 for non-lights)
-  float total = 0.0f;
+// Light tables on the device: rebuilt by one kernel whenever residency changes.
+struct LightMeta {
+  uint32_t count;
+  float total;
 };
 
 // Device buffers of the wavefront path tracer (one slot per path; see pathtrace.cu).
@@ -50,9 +47,7 @@ struct FrameState {
   DeviceBuf sOcc;                     // 1 byte per shadow entry
   DeviceBuf counters;                 // queue lengths, cursors, statistics
   DeviceBuf views;                    // view table
-  DeviceBuf lightIdx, lightCdf, lightPdf;
-  uint32_t lightCount = 0;
-  float lightTotal = 0.0f;
+  DeviceBuf lightIdx, lightCdf, lightPdf, lightMeta;
   bool lightsDirty = true;
   // ReSTIR DI reservoirs (current and previous frame) and surface records
   DeviceBuf resv[2], surf[2];
@@ -91,7 +86,31 @@ struct nomad_ctx {
   std::vector<uint8_t> primDirtyFlag, objDirtyFlag;
   // path tracer
   FrameState frame;
+  // device residency state (residency.cu)
+  struct Residency {
+    bool ready = false;
+    uint32_t bvhNodeCount = 0;
+    DeviceBuf objSlot, objBlasRef, objRes, primAct;   // int64, int32, u8, u8
+    DeviceBuf bounds, bytes, tris, emit;               // float4 (centre, radius), u64, u32, f32
+    DeviceBuf score, hist, lastHit, prevDist, visible; // f32, u32[8], u32, f32, u8
+    DeviceBuf features, keys, desired, misc;           // f32[24], f32, u8, misc words
+    DeviceBuf emissive;                                // {prim, weight bits, object} per emissive primitive
+    uint32_t emissiveCount = 0;
+    uint32_t frame = 0;
+    float prevCam[3] = {0, 0, 0};
+    bool havePrevCam = false;
+    std::vector<uint64_t> hostBytes;
+  } res;
+  void *mlp = nullptr;  // MlpState (mlp.cu)
 };
+
+void nomad_mlp_free(void *p);
+nomad_status nomad_mlp_infer_device(nomad_ctx *ctx, const float *X, uint64_t n, float *y);
+// Residency device state: created at upload, mirrored after host-side flushes.
+nomad_status nomad_residency_init(nomad_ctx *ctx);
+nomad_status nomad_residency_mirror(nomad_ctx *ctx);
+// Rebuilds the light CDF on the device if residency changed since the last build.
+nomad_status nomad_lights_update(nomad_ctx *ctx);
 
 inline nomad_status nomad_fail(nomad_ctx *c, nomad_status st, const std::string &msg) {
   if (c) c->err = msg;
@@ -108,5 +127,3 @@ inline nomad_status nomad_cuda_fail(nomad_ctx *c, cudaError_t e, const char *wha
     if (e_ != cudaSuccess) return nomad_cuda_fail(ctx, e_, #call);    \
   } while (0)
 
-// Rebuilds the light tables from the host copies of the scene and the active set.
-void nomad_build_lights(const nomad_ctx *ctx, LightTables &out);

@@ -163,6 +163,7 @@ extern "C" nomad_status nomad_destroy(nomad_ctx *ctx) {
   for (auto s : ctx->copyStreams)
     if (s) cudaStreamDestroy(s);
   if (ctx->ownStream) cudaStreamDestroy(ctx->ownStream);
+  if (ctx->mlp) nomad_mlp_free(ctx->mlp);
   delete ctx;
   return NOMAD_OK;
 }
@@ -253,12 +254,15 @@ extern "C" nomad_status nomad_scene_upload(nomad_ctx *ctx, const float *bvh, uin
   ctx->hostMaterials.assign(materials, materials + (size_t)primCount * 20);
   ctx->frame.lightsDirty = true;
   ctx->frame.restirValid = false;
+  ctx->res.bvhNodeCount = bvhCount;
   ctx->dirtyPrims.clear();
   ctx->dirtyObjs.clear();
   ctx->primDirtyFlag.assign(primCount, 0);
   ctx->objDirtyFlag.assign(objectCount, 0);
   // Objects uploaded non-resident keep their primitives flagged active (like the reference,
   // where residency is per object through the instance record); they are skipped via the TLAS.
+  nomad_status rst = nomad_residency_init(ctx);
+  if (rst != NOMAD_OK) return rst;
   ctx->sceneReady = true;
   return NOMAD_OK;
 }
@@ -336,9 +340,13 @@ extern "C" nomad_status nomad_residency_flush(nomad_ctx *ctx) {
       vals.push_back(ref);
     }
   }
-  if (!ctx->dirtyPrims.empty()) ctx->frame.lightsDirty = true;
+  bool mirror = !ctx->dirtyPrims.empty() || !ctx->dirtyObjs.empty();
   ctx->dirtyPrims.clear();
   ctx->dirtyObjs.clear();
+  if (mirror) {
+    nomad_status mst = nomad_residency_mirror(ctx);
+    if (mst != NOMAD_OK) return mst;
+  }
   if (offs.empty()) return NOMAD_OK;
   NOMAD_CUDA(ctx, ctx->patchOffs.reserve(offs.size() * 8));
   NOMAD_CUDA(ctx, ctx->patchVals.reserve(vals.size() * 4));

@@ -267,18 +267,18 @@ extern "C" nomad_status nomad_synth_icospheres(uint64_t seed, uint32_t instances
   }
 }
 
-extern "C" nomad_status nomad_synth_city(uint64_t seed, uint32_t grid, float size_m,
+extern "C" nomad_status nomad_synth_city(uint64_t seed, uint32_t grid, uint32_t grid_z, float size_m,
                                          uint32_t target_tris, uint32_t median_tris,
                                          uint32_t max_tris, uint32_t emissive_quads,
                                          uint32_t emissive_tris, float emissive_sigma,
                                          nomad_scene_owned **out) {
-  if (!out || grid == 0 || !(size_m > 0) || median_tris == 0 || max_tris < 16)
+  if (!out || grid == 0 || grid_z == 0 || !(size_m > 0) || median_tris == 0 || max_tris < 16)
     return NOMAD_ERR_INVALID_ARGUMENT;
   *out = nullptr;
   try {
     std::unique_ptr<nomad_scene_owned> s(new nomad_scene_owned());
     nomad::Rng r(seed);
-    const uint32_t cells = grid * grid;
+    const uint32_t cells = grid * grid_z;
     // Lognormal triangle budgets (median `median_tris`), clamped, then rescaled so the
     // total lands near `target_tris`.
     const double sigma = 1.336;
@@ -301,10 +301,11 @@ extern "C" nomad_status nomad_synth_city(uint64_t seed, uint32_t grid, float siz
     }
     const double pitch = size_m / grid;
     const double half = size_m * 0.5;
+    const double halfZ = pitch * grid_z * 0.5;
     uint32_t emissive_left = emissive_tris;
     for (uint32_t c = 0; c < cells; ++c) {
       uint32_t gx = c % grid, gz = c / grid;
-      D3 center = {-half + (gx + 0.5) * pitch, 0.0, -half + (gz + 0.5) * pitch};
+      D3 center = {-half + (gx + 0.5) * pitch, 0.0, -halfZ + (gz + 0.5) * pitch};
       float m[20];
       bool glossy = r.uniform() < 0.35;
       D3 alb = {r.uniform(0.2, 0.8), r.uniform(0.2, 0.8), r.uniform(0.2, 0.8)};

@@ -67,7 +67,7 @@ SIGNATURES = {
     "nomad_scenebvh_view_get": (C.c_int32, [_P, C.POINTER(SceneBVHView)]),
     "nomad_scenebvh_free": (None, [_P]),
     "nomad_synth_icospheres": (C.c_int32, [C.c_uint64, C.c_uint32, C.c_float, C.POINTER(_P)]),
-    "nomad_synth_city": (C.c_int32, [C.c_uint64, C.c_uint32, C.c_float, C.c_uint32, C.c_uint32,
+    "nomad_synth_city": (C.c_int32, [C.c_uint64, C.c_uint32, C.c_uint32, C.c_float, C.c_uint32, C.c_uint32,
                                      C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.POINTER(_P)]),
     "nomad_scene_owned_desc": (C.c_int32, [_P, C.POINTER(SceneDesc)]),
     "nomad_scene_owned_free": (None, [_P]),
@@ -97,7 +97,34 @@ SIGNATURES = {
     "nomad_render_frame": (C.c_int32, [_P, _P, C.c_uint32, _P, C.c_uint32]),
     "nomad_render_stats": (C.c_int32, [_P, _P]),
     "nomad_reset_render_stats": (C.c_int32, [_P]),
+    "nomad_residency_step": (C.c_int32, [_P, _P, _P, C.POINTER(C.c_uint32)]),
+    "nomad_object_bytes": (C.c_int32, [_P, _P]),
+    "nomad_residency_last": (C.c_int32, [_P, _P, _P]),
+    "nomad_residency_flags": (C.c_int32, [_P, _P]),
+    "nomad_mlp_init": (C.c_int32, [_P, C.c_uint64]),
+    "nomad_mlp_train": (C.c_int32, [_P, _P, _P, C.c_uint64, C.c_uint32, C.c_uint32, C.c_float,
+                                    C.c_float, C.c_uint64, _P]),
+    "nomad_mlp_infer": (C.c_int32, [_P, _P, C.c_uint64, _P, C.c_uint32]),
+    "nomad_mlp_get": (C.c_int32, [_P, _P]),
+    "nomad_mlp_set": (C.c_int32, [_P, _P]),
 }
+
+POLICY_ALWAYS, POLICY_RAYHIT_BUDGET, POLICY_LEARNED = 0, 1, 2
+N_FEATURES = 24
+MLP_PARAMS = 128 * 32 + 128 + 128 * 128 + 128 + 128 + 1 + 2 * N_FEATURES
+
+
+class ResidencyParams(C.Structure):
+    _fields_ = [("policy", C.c_uint32), ("max_toggles", C.c_uint32), ("budget_bytes", C.c_uint64),
+                ("hit_decay", C.c_float), ("camera_motion", C.c_float),
+                ("memory_pressure", C.c_float), ("reserve_base", C.c_float),
+                ("reserve_motion", C.c_float), ("min_active", C.c_uint32)]
+
+    @staticmethod
+    def make(policy, budget_bytes=0, max_toggles=0, hit_decay=0.85, camera_motion=0.0,
+             memory_pressure=0.0, reserve_base=0.02, reserve_motion=0.06, min_active=0):
+        return ResidencyParams(policy, max_toggles, budget_bytes, hit_decay, camera_motion,
+                               memory_pressure, reserve_base, reserve_motion, min_active)
 
 VIEW_DTYPE = np.dtype([("camera_pos", "<f4", 3), ("viewport_u", "<f4", 3), ("viewport_v", "<f4", 3),
                        ("first_pixel", "<f4", 3), ("width", "<u4"), ("height", "<u4"), ("spp", "<u4"),
@@ -210,10 +237,10 @@ def synth_icospheres(seed: int, instances: int = 64, extent: float = 100.0) -> H
 
 def synth_city(seed: int, grid: int = 32, size_m: float = 1000.0, target_tris: int = 2_500_000,
                median_tris: int = 1000, max_tris: int = 200_000, emissive_quads: int = 64,
-               emissive_tris: int = 0, emissive_sigma: float = 1.5) -> HostScene:
+               emissive_tris: int = 0, emissive_sigma: float = 1.5, grid_z: int = 0) -> HostScene:
     lib = load()
     h = _P()
-    _check(lib.nomad_synth_city(seed, grid, size_m, target_tris, median_tris, max_tris,
+    _check(lib.nomad_synth_city(seed, grid, grid_z or grid, size_m, target_tris, median_tris, max_tris,
                                 emissive_quads, emissive_tris, emissive_sigma, C.byref(h)))
     return HostScene._from_owned(h)
 
@@ -411,6 +438,58 @@ class Context:
 
     def reset_render_stats(self):
         self._ck(self.lib.nomad_reset_render_stats(self.h))
+
+    # residency policies
+    def residency_step(self, params: "ResidencyParams", camera_view: np.ndarray) -> int:
+        v = np.ascontiguousarray(camera_view, VIEW_DTYPE).reshape(-1)[:1]
+        t = C.c_uint32()
+        self._ck(self.lib.nomad_residency_step(self.h, C.byref(params), _ptr(v), C.byref(t)))
+        return t.value
+
+    def object_bytes(self) -> np.ndarray:
+        out = np.zeros(self.object_count, np.uint64)
+        self._ck(self.lib.nomad_object_bytes(self.h, _ptr(out)))
+        return out
+
+    def residency_last(self):
+        f = np.zeros((self.object_count, N_FEATURES), np.float32)
+        s = np.zeros(self.object_count, np.float32)
+        self._ck(self.lib.nomad_residency_last(self.h, _ptr(f), _ptr(s)))
+        return f, s
+
+    def residency_flags(self) -> np.ndarray:
+        out = np.zeros(self.object_count, np.uint8)
+        self._ck(self.lib.nomad_residency_flags(self.h, _ptr(out)))
+        return out
+
+    # learned scorer
+    def mlp_init(self, seed: int = 0):
+        self._ck(self.lib.nomad_mlp_init(self.h, seed))
+
+    def mlp_train(self, features, targets, steps=500, batch=1024, lr=1e-3, weight_decay=1e-4,
+                  seed=0) -> np.ndarray:
+        x = np.ascontiguousarray(features, np.float32)
+        t = np.ascontiguousarray(targets, np.float32)
+        loss = np.zeros(steps, np.float32)
+        self._ck(self.lib.nomad_mlp_train(self.h, _ptr(x), _ptr(t), t.shape[0], steps, batch, lr,
+                                          weight_decay, seed, _ptr(loss)))
+        return loss
+
+    def mlp_infer(self, features) -> np.ndarray:
+        x = np.ascontiguousarray(features, np.float32)
+        out = np.zeros(x.shape[0], np.float32)
+        self._ck(self.lib.nomad_mlp_infer(self.h, _ptr(x), x.shape[0], _ptr(out), 0))
+        return out
+
+    def mlp_get(self) -> np.ndarray:
+        out = np.zeros(MLP_PARAMS, np.float32)
+        self._ck(self.lib.nomad_mlp_get(self.h, _ptr(out)))
+        return out
+
+    def mlp_set(self, blob):
+        b = np.ascontiguousarray(blob, np.float32)
+        assert b.size == MLP_PARAMS
+        self._ck(self.lib.nomad_mlp_set(self.h, _ptr(b)))
 
     def object_hits(self) -> np.ndarray:
         out = np.zeros(self.object_count, np.uint32)

@@ -1,0 +1,121 @@
+"""GPU tests of the device residency step and the learned BF16 MLP scorer.
+
+* MLP inference against a float64 restatement with the device's bf16 roundings
+  (tolerance 1e-3 relative: only the fp32 accumulation order differs);
+* training lowers the loss and is bit-reproducible for a seed; the weight blob round-trips;
+* the residency step's keys, selection under a byte budget and TLAS patching against the
+  oracle restatement; traversal and rendering after eviction against the oracle.
+"""
+import numpy as np
+import pytest
+
+from tests import raysets
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx(nb):
+    c = nb.Context(0)
+    yield c
+    c.close()
+
+
+def _features(n, seed):
+    rng = np.random.default_rng(seed)
+    f = rng.normal(size=(n, 24)).astype(np.float32) * 2.0 + 1.0
+    return f
+
+
+def test_mlp_forward_matches_restatement(nb, ctx, small_city):
+    from oracle import residency as ores
+
+    ctx.upload(small_city[1])
+    ctx.mlp_init(123)
+    x = _features(1000, 1)
+    got = ctx.mlp_infer(x)
+    want = ores.mlp_forward(ctx.mlp_get(), x)
+    err = np.abs(got - want) / (1.0 + np.abs(want))
+    assert err.max() < 1e-3, err.max()
+
+
+def test_mlp_training(nb, ctx, small_city):
+    from oracle import residency as ores
+
+    ctx.upload(small_city[1])
+    rng = np.random.default_rng(2)
+    x = _features(16384, 3)
+    t = np.log1p(np.abs(x[:, 0] * 2 + x[:, 5] - 0.5 * x[:, 11] ** 2)).astype(np.float32)
+    ctx.mlp_init(7)
+    loss = ctx.mlp_train(x, t, steps=300, batch=1024, lr=2e-3, seed=11)
+    assert np.isfinite(loss).all()
+    assert loss[-20:].mean() < 0.25 * loss[:5].mean(), (loss[:5], loss[-20:])
+    blob = ctx.mlp_get()
+    # reproducible: same seed, same weights
+    ctx.mlp_init(7)
+    ctx.mlp_train(x, t, steps=300, batch=1024, lr=2e-3, seed=11)
+    assert np.array_equal(ctx.mlp_get(), blob)
+    # checkpoint round trip
+    pred = ctx.mlp_infer(x[:500])
+    ctx.mlp_init(99)
+    ctx.mlp_set(blob)
+    assert np.array_equal(ctx.mlp_infer(x[:500]), pred)
+    err = np.abs(pred - ores.mlp_forward(blob, x[:500])) / (1.0 + np.abs(pred))
+    assert err.max() < 1e-3
+
+
+def _residency_frame(nb, ctx, view):
+    ctx.reset_object_hits()
+    ctx.render(view, count_hits=True)
+    return ctx.object_hits().astype(np.int64)
+
+
+@pytest.mark.parametrize("policy", [0, 1, 2])
+def test_residency_step_against_oracle(nb, orc, ctx, small_city, policy):
+    from oracle import residency as ores
+
+    scene, sb = small_city
+    ctx.upload(sb)
+    if policy == nb.POLICY_LEARNED:
+        ctx.mlp_init(5)
+    nbytes = ctx.object_bytes()
+    budget = int(0.4 * nbytes.sum())
+    prm = nb.ResidencyParams.make(policy, budget_bytes=budget, camera_motion=0.5, memory_pressure=0.25,
+                                  min_active=2)
+    score = np.zeros(sb.object_count, np.float64)
+    flags = np.ones(sb.object_count, np.uint8)
+    for frame, pos in enumerate([(0, 60, -180), (20, 50, -150), (40, 45, -120)]):
+        view = nb.view_pinhole(pos, (0, 0, 0), width=96, height=54, spp=2, max_depth=2, seed=frame)
+        hits = _residency_frame(nb, ctx, view)
+        toggles = ctx.residency_step(prm, view)
+        feats, keys = ctx.residency_last()
+        score = (score.astype(np.float32) * np.float32(0.85) + hits.astype(np.float32)).astype(np.float32)
+        visible = feats[:, 2] > 0.5
+        if policy == nb.POLICY_RAYHIT_BUDGET:
+            want_keys = ores.rayhit_keys(score, hits, visible, 0.25)
+            assert np.array_equal(keys, want_keys)
+        if policy == nb.POLICY_LEARNED:
+            want_keys = ctx.mlp_infer(feats)
+            assert np.array_equal(keys, want_keys)
+        reserve = ores.reserve_count(sb.object_count, 0.02, 0.06, 0.5)
+        want, want_t = ores.select(keys, visible, nbytes, budget, reserve, 2, flags,
+                                   always=(policy == nb.POLICY_ALWAYS))
+        got = ctx.residency_flags()
+        assert np.array_equal(got, want), (frame, np.nonzero(got != want)[0][:10])
+        assert toggles == want_t
+        flags = got
+        if policy != nb.POLICY_ALWAYS:
+            assert int(nbytes[flags.astype(bool)].sum()) <= budget + int(np.sort(nbytes)[-2:].sum())
+    inst = ctx.instances()
+    root = sb.instances["blas_root_index"].copy()
+    root[flags == 0] = -1
+    assert np.array_equal(inst["blas_root_index"], root)
+    # traversal and shading see exactly the resident set
+    rays = np.concatenate([raysets.aimed_rays(sb, 8000, 1), raysets.random_rays(sb, 4000, 2)])
+    ref = orc.OracleScene(sb, blas_root=root)
+    got = ctx.trace_closest(rays)
+    assert np.array_equal(np.ascontiguousarray(got).view(np.int32), np.ascontiguousarray(ref.closest(rays)).view(np.int32))
+    v = nb.view_pinhole((0, 60, -180), (0, 0, 0), width=48, height=27, spp=2, max_depth=3, seed=9)
+    img = ctx.render(v)[0].reshape(-1, 3)
+    want_img, _, _ = orc.render(ref, sb.materials, v)
+    assert (img == want_img).all(1).mean() > 0.99
