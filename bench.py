@@ -151,6 +151,117 @@ def cpu_leg(sb, rays, budget_s=12.0, use_reference=False):
                       f"({dt:.1f} s of CPU work, {cores} threads)"}
 
 
+def frame_leg(nb, ctx, sb, frames=3):
+    """Path-traced city frame (1920x1080 x 4 spp, 3 bounces, NEE): ms/frame and ray rates."""
+    import torch
+
+    v = nb.view_pinhole((0.0, 220.0, -620.0), (0.0, 0.0, 60.0), width=WIDTH, height=HEIGHT, spp=SPP,
+                        max_depth=3, seed=SEED)
+    out = torch.empty(WIDTH * HEIGHT * 3, dtype=torch.float32, device="cuda")
+    ctx.render_dev(v, out.data_ptr())
+    ctx.sync()
+    ctx.reset_render_stats()
+    t0 = time.perf_counter()
+    for f in range(frames):
+        v["frame"] = f
+        ctx.render_dev(v, out.data_ptr())
+    ctx.sync()
+    dt = (time.perf_counter() - t0) / frames
+    st = ctx.render_stats() / frames
+    return {"config": "city 1920x1080 x 4 spp, 3 bounces, one-sample NEE", "ms_per_frame": dt * 1e3,
+            "closest_rays_per_frame": int(st[0]), "shadow_rays_per_frame": int(st[2]),
+            "mrays_per_s_incl_shadow": (st[0] + st[2]) / dt / 1e6}
+
+
+def multiview_views(nb, n=16, seed=404):
+    rng = np.random.default_rng(seed)
+    views = []
+    for i in range(n):
+        w = int(rng.integers(256, 1921))
+        h = int(np.clip(rng.integers(256, 1081), 256, 1080))
+        ang = rng.uniform(0, 2 * np.pi)
+        pos = (float(450 * np.cos(ang)), float(rng.uniform(40, 250)), float(450 * np.sin(ang)))
+        views.append(nb.view_pinhole(pos, (0.0, 0.0, 0.0), width=w, height=h, spp=int(rng.integers(1, 17)),
+                                     max_depth=2, seed=SEED + i))
+    return np.concatenate(views)
+
+
+def multiview_leg(nb, ctx, frames=3):
+    """16 views of the city at seeded uneven sizes (256..1920 x 256..1080) and spp (1..16),
+    2 bounces, all paths in one batched launch sequence per frame."""
+    import torch
+
+    views = multiview_views(nb)
+    px = int((views["width"].astype(np.int64) * views["height"]).sum())
+    paths = int((views["width"].astype(np.int64) * views["height"] * views["spp"]).sum())
+    out = torch.empty(px * 3, dtype=torch.float32, device="cuda")
+    ctx.render_dev(views, out.data_ptr())
+    ctx.sync()
+    ctx.reset_render_stats()
+    t0 = time.perf_counter()
+    for f in range(frames):
+        views["frame"] = f
+        ctx.render_dev(views, out.data_ptr())
+    ctx.sync()
+    dt = (time.perf_counter() - t0) / frames
+    st = ctx.render_stats() / frames
+    return {"views": int(views.shape[0]), "pixels": px, "paths": paths, "ms_per_frame": dt * 1e3,
+            "mpaths_per_s": paths / dt / 1e6, "mrays_per_s_incl_shadow": (st[0] + st[2]) / dt / 1e6}
+
+
+def restir_leg(nb, ctx, frames=8):
+    """ReSTIR DI on the city with 4,096 emissive triangles (lognormal power, sigma 1.5): per frame
+    of an 8-frame spline move, rel-MSE of 1-spp direct lighting against a 1024-spp reference
+    (pixel centres, 480x270), for ReSTIR (32 candidates, 1 temporal + 3 spatial within 30 px,
+    M-cap 20) and for one-sample NEE; and ReSTIR ms/frame at 1920x1080 x 1 spp."""
+    import torch
+
+    from nomad_b200.residency_eval import catmull_rom
+
+    scene = nb.synth_city(seed=SEED, emissive_tris=4096, emissive_sigma=1.5)
+    sb2 = nb.SceneBVH(scene)
+    c2 = nb.Context(0)
+    try:
+        c2.upload(sb2)
+        c2.set_restir(candidates=32, temporal=True, spatial=3, radius_px=30.0, m_cap=20.0)
+        rng = np.random.default_rng(SEED + 3)
+        ctrl = np.stack([rng.uniform(-150, 150, 5), rng.uniform(120, 220, 5), rng.uniform(-650, -500, 5)], 1)
+        path = catmull_rom(ctrl, frames)
+        W, H = 480, 270
+        errs = {"restir": [], "nee": []}
+        for f in range(frames):
+            pos = tuple(float(x) for x in path[f])
+            ref = c2.render(nb.view_pinhole(pos, (0.0, 0.0, 60.0), width=W, height=H, spp=1024, max_depth=1,
+                                            seed=9000 + f, flags=nb.VIEW_CENTER))[0]
+            den = float((ref.astype(np.float64) ** 2).mean())
+            for name, fl in (("restir", nb.VIEW_RESTIR), ("nee", 0)):
+                img = c2.render(nb.view_pinhole(pos, (0.0, 0.0, 60.0), width=W, height=H, spp=1, max_depth=1,
+                                                seed=7, frame=f, flags=fl | nb.VIEW_CENTER))[0]
+                errs[name].append(float(((img.astype(np.float64) - ref) ** 2).mean() / den))
+        out = torch.empty(WIDTH * HEIGHT * 3, dtype=torch.float32, device="cuda")
+        v = nb.view_pinhole((0.0, 220.0, -620.0), (0.0, 0.0, 60.0), width=WIDTH, height=HEIGHT, spp=1,
+                            max_depth=1, seed=SEED, flags=nb.VIEW_RESTIR)
+        c2.render_dev(v, out.data_ptr())
+        c2.sync()
+        t0 = time.perf_counter()
+        for f in range(4):
+            v["frame"] = f + 1
+            c2.render_dev(v, out.data_ptr())
+        c2.sync()
+        ms = (time.perf_counter() - t0) / 4 * 1e3
+        return {"config": "city + 4,096 emissive tris, 8-frame spline, 480x270 error / 1080p timing",
+                "rel_mse_per_frame": errs, "rel_mse_mean": {k: float(np.mean(v)) for k, v in errs.items()},
+                "restir_ms_per_frame_1080p_1spp": ms}
+    finally:
+        c2.close()
+
+
+def residency_leg():
+    from nomad_b200 import residency_eval
+
+    return residency_eval.run(log=log)
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -202,6 +313,8 @@ def main():
     ap.add_argument("--impl", default="nomad", choices=["nomad", "reference"])
     ap.add_argument("--kernel", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the path-tracing, multi-view, ReSTIR and residency legs")
     ap.add_argument("--spp", type=int, default=SPP,
                     help="primary rays per pixel (smaller values give the profiling case)")
     args = ap.parse_args()
@@ -262,6 +375,15 @@ def main():
     bytes_prim = alg_bytes(d_prim, n_prim)
     bytes_b = alg_bytes(d_b, n_b)
     del d_w
+
+    # Autotune the traversal variant on a sample of this frame's rays (1M primary + 1M bounce).
+    tune = None
+    if args.kernel == 0:
+        sample = torch.cat([d_prim[:1_000_000], d_b[:1_000_000]]).contiguous()
+        torch.cuda.synchronize()
+        tune = ctx.autotune((sample.data_ptr(), sample.shape[0]), repeats=3, device=True)
+        del sample
+        log(f"autotune: {tune}")
 
     def step():
         ctx.trace_closest_dev(d_prim.data_ptr(), n_prim, d_ph.data_ptr())
@@ -344,6 +466,20 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_leg(sb, np.concatenate([primary, bounce]))
 
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        ctx.set_stream(0)
+        for name, fn in (("city_frame", lambda: frame_leg(nb, ctx, sb)),
+                         ("multiview", lambda: multiview_leg(nb, ctx)),
+                         ("restir", lambda: restir_leg(nb, ctx)),
+                         ("residency", lambda: residency_leg())):
+            try:
+                t0 = time.perf_counter()
+                extras[name] = fn()
+                log(f"{name}: {time.perf_counter() - t0:.1f}s {extras[name]}")
+            except Exception as exc:  # an extra leg never hides the headline line
+                extras[name] = {"error": repr(exc)}
+
     if rank == 0:
         line = {
             "metric": "closest-hit Mrays/s (city 1080p x4spp + bounce)",
@@ -361,7 +497,10 @@ def main():
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clk.summary(t_begin, t_end),
+            "kernel_variant": tune["best"] if tune else nb.KERNEL_NAMES.get(args.kernel),
+            "autotune": tune,
         }
+        line.update(extras)
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:

@@ -59,11 +59,18 @@ enum {
   NOMAD_TRACE_COUNT_HITS = 1u << 1       /* add closest hits to the per-object hit counters   */
 };
 
-/* Traversal kernel variants (the autotuner picks one per scene; 0 = default). */
+/* Traversal kernel variants (nomad_autotune picks one per scene; 0 = the tuned or default one).
+ * Widths: binary pair nodes (2), 4- and 8-wide nodes collapsed from them. PERSIST: persistent
+ * warps take rays 32 at a time from a global cursor. */
 enum {
   NOMAD_KERNEL_AUTO = 0,
-  NOMAD_KERNEL_BVH2 = 1,        /* binary pair-node traversal, one ray per thread, local stack   */
-  NOMAD_KERNEL_BVH2_PERSIST = 2 /* same, persistent warps fetching rays from a global counter    */
+  NOMAD_KERNEL_BVH2 = 1,
+  NOMAD_KERNEL_BVH2_PERSIST = 2,
+  NOMAD_KERNEL_BVH4 = 3,
+  NOMAD_KERNEL_BVH4_PERSIST = 4,
+  NOMAD_KERNEL_BVH8 = 5,
+  NOMAD_KERNEL_BVH8_PERSIST = 6,
+  NOMAD_KERNEL_COUNT = 7
 };
 
 /* ---- context -------------------------------------------------------------------------------- */
@@ -115,6 +122,22 @@ nomad_status nomad_trace_closest(nomad_ctx *ctx, const nomad_ray *rays, uint64_t
 /* Any hit per ray in (1e-4, tmax): out[i] = 1 when occluded, else 0. Exits at the first hit. */
 nomad_status nomad_trace_any(nomad_ctx *ctx, const nomad_ray *rays, uint64_t n, uint8_t *out,
                              uint32_t flags);
+/* Autotuner result: per variant the best of `repeats` closest-hit timings on the sample (ms,
+ * negative when the variant is not available for this scene: its stack would be too shallow),
+ * the number of sample rays whose hit differs from the binary variant's (must be 0), and the
+ * stack entries each width can need on this scene. */
+typedef struct nomad_tune_result {
+  uint32_t best;                        /* NOMAD_KERNEL_* now used by the context            */
+  float ms[NOMAD_KERNEL_COUNT];
+  uint32_t mismatches[NOMAD_KERNEL_COUNT];
+  uint32_t stack_need[3];               /* binary, 4-wide, 8-wide                            */
+} nomad_tune_result;
+/* Times every traversal variant on n sample rays (device pointers when
+ * NOMAD_TRACE_DEVICE_POINTERS), checks they agree bit for bit, and selects the fastest for the
+ * trace calls and the path tracer's queues. */
+nomad_status nomad_autotune(nomad_ctx *ctx, const nomad_ray *rays, uint64_t n, uint32_t repeats,
+                            uint32_t flags, nomad_tune_result *out);
+
 /* Chooses the traversal variant used by the trace calls (NOMAD_KERNEL_*). */
 nomad_status nomad_set_kernel(nomad_ctx *ctx, uint32_t kernel);
 
@@ -154,7 +177,9 @@ enum {
    * (:1879). Without it the output is HDR radiance. */
   NOMAD_VIEW_CLAMP = 1u << 0,
   /* Direct lighting at the first bounce by ReSTIR DI (nomad_set_restir) instead of one-sample NEE. */
-  NOMAD_VIEW_RESTIR = 1u << 1
+  NOMAD_VIEW_RESTIR = 1u << 1,
+  /* Primary rays through pixel centres (no sub-pixel jitter). */
+  NOMAD_VIEW_CENTER = 1u << 2
 };
 
 /* Fills a view from a camera, as populateViewportUniforms does (vertical fov in degrees);
@@ -169,6 +194,25 @@ nomad_status nomad_view_pinhole(const float position[3], const float look_at[3],
  * NOMAD_TRACE_COUNT_HITS the per-object counters also count the closest hits of every bounce. */
 nomad_status nomad_render_frame(nomad_ctx *ctx, const nomad_view *views, uint32_t nviews,
                                 float *radiance_out, uint32_t flags);
+
+/* ReSTIR DI at the first bounce of views flagged NOMAD_VIEW_RESTIR (replaces the reference's
+ * inline reservoir block, PathTracing.h:1363-1742, by separate passes over FP32 reservoirs kept
+ * per path (pixel, sample)): `candidates` light samples by RIS (no visibility), temporal reuse
+ * of the previous frame's reservoir at the reprojected pixel, `spatial` neighbours drawn within
+ * `radius_px` from this frame's temporally resampled reservoirs, each reused reservoir's sample
+ * count capped at m_cap * candidates, surface-similarity gates of the reference (position
+ * max(1% depth, 0.02), depth max(2% depth, 0.05), normal dot >= 0.9), one visibility ray for the
+ * final sample. Temporal reuse needs the same views (sizes, spp) as the previous frame. */
+typedef struct nomad_restir_config {
+  uint32_t candidates;   /* 32                                                             */
+  uint32_t temporal;     /* 1 = reuse the previous frame                                   */
+  uint32_t spatial;      /* 3 neighbours                                                   */
+  float radius_px;       /* 30                                                             */
+  float m_cap;           /* 20                                                             */
+} nomad_restir_config;
+nomad_status nomad_set_restir(nomad_ctx *ctx, const nomad_restir_config *cfg);
+/* Forgets the previous frame's reservoirs (next frame starts without temporal reuse). */
+nomad_status nomad_reset_restir(nomad_ctx *ctx);
 
 /* Ray statistics accumulated by nomad_render_frame since the last reset:
  * out[0] closest-hit rays traced, [1] environment escapes (the reference's stats[2N]),

@@ -5,10 +5,11 @@ C ABI in include/nomad_rt.h and include/nomad_scene.h. This package only binds i
 builds host-side ray batches; it has no CPU fallback.
 """
 from .native import (  # noqa: F401
-    VIEW_DTYPE, VIEW_CLAMP, VIEW_RESTIR, view_pinhole, ResidencyParams, N_FEATURES, MLP_PARAMS,
-    POLICY_ALWAYS, POLICY_RAYHIT_BUDGET, POLICY_LEARNED,
+    VIEW_DTYPE, VIEW_CLAMP, VIEW_RESTIR, VIEW_CENTER, view_pinhole, ResidencyParams, N_FEATURES, MLP_PARAMS,
+    POLICY_ALWAYS, POLICY_RAYHIT_BUDGET, POLICY_LEARNED, RestirConfig,
     Context, HostScene, SceneBVH, NomadError, load, synth_city, synth_icospheres,
     RAY_DTYPE, HIT_DTYPE, INSTANCE_DTYPE, LIB_PATH, SIGNATURES,
-    KERNEL_AUTO, KERNEL_BVH2, KERNEL_BVH2_PERSIST, TRACE_COUNT_HITS, TRACE_DEVICE_POINTERS,
+    KERNEL_AUTO, KERNEL_BVH2, KERNEL_BVH2_PERSIST, KERNEL_BVH4, KERNEL_BVH4_PERSIST, KERNEL_BVH8,
+    KERNEL_BVH8_PERSIST, KERNEL_NAMES, TRACE_COUNT_HITS, TRACE_DEVICE_POINTERS,
 )
 from .rays import Camera, bounce_rays, city_camera, icosphere_camera  # noqa: F401

@@ -30,8 +30,6 @@ using namespace nomad_pt;
 namespace {
 
 constexpr int kPtBlock = 256;
-constexpr int kTraceBlock = 128;
-constexpr int kStackPT = 64;
 constexpr float kPi = 3.14159265358979323846f;
 
 struct ViewDev {
@@ -97,8 +95,9 @@ __global__ void __launch_bounds__(kPtBlock) k_raygen(const ViewDev *__restrict__
     U4 r = philox(U4{pixel, sample, 255u * 4u, v.index}, v.k0, v.k1);
     float ux = ((float)px + 0.5f) / (float)v.w;
     float uy = ((float)py + 0.5f) / (float)v.h;
-    float xo = (u01(r.x) - 0.5f) / (float)v.w;
-    float yo = (u01(r.y) - 0.5f) / (float)v.h;
+    bool center = (v.flags & NOMAD_VIEW_CENTER) != 0;
+    float xo = center ? 0.0f : (u01(r.x) - 0.5f) / (float)v.w;
+    float yo = center ? 0.0f : (u01(r.y) - 0.5f) / (float)v.h;
     float s = ux + xo, t = uy + yo;
     V3 d = v3(v.fp[0] + s * v.vu[0] + t * v.vv[0] - v.cam[0], v.fp[1] + s * v.vu[1] + t * v.vv[1] - v.cam[1],
               v.fp[2] + s * v.vu[2] + t * v.vv[2] - v.cam[2]);
@@ -110,41 +109,6 @@ __global__ void __launch_bounds__(kPtBlock) k_raygen(const ViewDev *__restrict__
     rad[pid] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) cnt->qlen[0] = (uint32_t)P;
-}
-
-// Persistent trace over a queue whose length lives on the device.
-template <bool ANY>
-__global__ void __launch_bounds__(kTraceBlock) k_trace_queue(DevScene S, const float4 *__restrict__ rays,
-                                                              const uint32_t *__restrict__ len,
-                                                              unsigned long long *__restrict__ cursor,
-                                                              int32_t *__restrict__ hits, uint8_t *__restrict__ occ) {
-  const uint64_t n = *len;
-  int lane = threadIdx.x & 31;
-  for (;;) {
-    unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(cursor, 32ull);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= n) break;
-    uint64_t i = base + lane;
-    if (i < n) {
-      float4 a = __ldg(rays + 2 * i), b = __ldg(rays + 2 * i + 1);
-      RayP r = prep_ray(a, b);
-      HitRec h;
-      Work w{0, 0, 0};
-      traverse<kStackPT, ANY, false>(S, r, b.w, h, w);
-      if (ANY) {
-        occ[i] = h.prim >= 0 ? 1 : 0;
-      } else {
-        int32_t *o = hits + 5 * i;
-        o[0] = h.inst;
-        o[1] = h.prim;
-        o[2] = __float_as_int(h.prim >= 0 ? h.t : INFINITY);
-        o[3] = __float_as_int(h.u);
-        o[4] = __float_as_int(h.v);
-      }
-    }
-    __syncwarp();
-  }
 }
 
 struct Material {
@@ -587,11 +551,6 @@ __global__ void __launch_bounds__(kPtBlock) k_finalize(const ViewDev *__restrict
 
 namespace {
 
-int persist_blocks(nomad_ctx *ctx, const void *fn, int block) {
-  int perSm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, fn, block, 0);
-  return ctx->smCount * std::max(perSm, 1);
-}
 
 }  // namespace
 
@@ -636,7 +595,11 @@ extern "C" nomad_status nomad_view_pinhole(const float pos[3], const float look[
   return NOMAD_OK;
 }
 
-nomad_status nomad_restir_pass(nomad_ctx *ctx, const void *viewsDev, uint32_t nviews, const nomad_view *views);
+namespace {
+struct RestirArgs;
+nomad_status restir_pass(nomad_ctx *ctx, uint32_t nviews, const nomad_view *views, unsigned long long P,
+                         const Lights &L, Counters *C);
+}  // namespace
 
 extern "C" nomad_status nomad_render_frame(nomad_ctx *ctx, const nomad_view *views, uint32_t nviews,
                                            float *out, uint32_t flags) {
@@ -714,17 +677,16 @@ extern "C" nomad_status nomad_render_frame(nomad_ctx *ctx, const nomad_view *vie
   NOMAD_CUDA(ctx, cudaGetLastError());
   Lights L{F.lightIdx.as<const uint32_t>(), F.lightCdf.as<const float>(), F.lightMeta.as<const LightMeta>()};
   uint32_t *objHits = (flags & NOMAD_TRACE_COUNT_HITS) ? ctx->objHits.as<uint32_t>() : nullptr;
-  int gClosest = persist_blocks(ctx, (const void *)k_trace_queue<false>, kTraceBlock);
-  int gAny = persist_blocks(ctx, (const void *)k_trace_queue<true>, kTraceBlock);
   bool anyRestir = false;
   for (uint32_t i = 0; i < nviews; ++i) anyRestir |= (views[i].flags & NOMAD_VIEW_RESTIR) != 0;
   int cur = 0;
   for (uint32_t depth = 0; depth < maxDepth; ++depth) {
     k_bounce_reset<<<1, 1, 0, s>>>(C, cur);
-    k_trace_queue<false><<<gClosest, kTraceBlock, 0, s>>>(ctx->scene, F.qRays[cur].as<const float4>(), &C->qlen[cur],
-                                                         &C->cursor[0], F.hits.as<int32_t>(), nullptr);
+    st = nomad_trace_variant(ctx, ctx->kernel, false, F.qRays[cur].as<const float4>(), P, &C->qlen[cur], &C->cursor[0],
+                             F.hits.as<int32_t>(), nullptr, nullptr, s);
+    if (st != NOMAD_OK) return st;
     if (depth == 0 && anyRestir) {
-      st = nomad_restir_pass(ctx, F.views.p, nviews, views);
+      st = restir_pass(ctx, nviews, views, P, L, C);
       if (st != NOMAD_OK) return st;
     }
     k_shade<<<gridPT, kPtBlock, 0, s>>>(depth, V, nviews, F.qRays[cur].as<const float4>(), F.qIds[cur].as<const uint32_t>(),
@@ -733,8 +695,9 @@ extern "C" nomad_status nomad_render_frame(nomad_ctx *ctx, const nomad_view *vie
                                        F.sContrib.as<float4>(), F.thr.as<float4>(), F.rad.as<float4>(),
                                        ctx->prims.as<const float4>(), ctx->materials.as<const float4>(), L, C, cur,
                                        objHits, anyRestir ? 1 : 0);
-    k_trace_queue<true><<<gAny, kTraceBlock, 0, s>>>(ctx->scene, F.sRays.as<const float4>(), &C->qlen[2], &C->cursor[1],
-                                                    nullptr, F.sOcc.as<uint8_t>());
+    st = nomad_trace_variant(ctx, ctx->kernel, true, F.sRays.as<const float4>(), P, &C->qlen[2], &C->cursor[1],
+                             nullptr, F.sOcc.as<uint8_t>(), nullptr, s);
+    if (st != NOMAD_OK) return st;
     k_resolve<<<gridPT, kPtBlock, 0, s>>>(F.sIds.as<const uint32_t>(), F.sContrib.as<const float4>(),
                                          F.sOcc.as<const uint8_t>(), F.rad.as<float4>(), C);
     NOMAD_CUDA(ctx, cudaGetLastError());
@@ -774,7 +737,339 @@ extern "C" nomad_status nomad_reset_render_stats(nomad_ctx *ctx) {
   return NOMAD_OK;
 }
 
-// ReSTIR DI is compiled in restir.cu; until it is configured this pass is a no-op.
-__attribute__((weak)) nomad_status nomad_restir_pass(nomad_ctx *, const void *, uint32_t, const nomad_view *) {
+
+// ---------------------------------------------------------------------------------------------
+// ReSTIR DI at the first bounce (views flagged NOMAD_VIEW_RESTIR).
+//
+// Per path (pixel, sample) the passes are:
+//   initial  : RIS over `candidates` light samples (area measure: q(y) = lightPdf / area,
+//              target p(y) = luminance(bsdf * Le * cos_theta * cos_light / dist^2), the
+//              reference's luminance(radiance * geometryFactor), PathTracing.h:93-96, 383-394);
+//   temporal : the previous frame's final reservoir at the reprojected pixel, gated by the
+//              reference's surface tests (:1455-1473), its sample count capped at
+//              m_cap * candidates, weight p_cur(y) * W_prev * M_prev;
+//   spatial  : `spatial` neighbours within radius_px (Philox offsets) from this frame's temporal
+//              reservoirs, same gates and weights;
+//   shade    : W = wSum / (M * p(y)); the unoccluded contribution bsdf * Le * cos_theta *
+//              cos_light / dist^2 * W is queued with one shadow ray (origin offset 5e-4 along the
+//              normal, kVisibilityRayOffset :28), resolved with the other shadow rays.
+// The reference weights candidates by target / (solid-angle pdf), which leaves a stray
+// cos_light / dist^2 factor in its estimate; here the candidate pdf is in area measure, the
+// measure the target is written in, so the estimate converges to the path-traced result and
+// reuse across pixels needs no Jacobian.
+namespace {
+
+struct Resv {
+  float4 a;  // light position, bits(light primitive) (-1: empty)
+  float4 b;  // light normal, 0
+  float4 c;  // 0, wSum, M, p(y) at the owner
+};
+struct Surf {
+  float4 p;  // position, depth
+  float4 n;  // shading normal, bits(primitive)
+  float4 v;  // view direction, valid
+};
+
+struct RestirDev {
+  uint32_t candidates, temporal, spatial;
+  float radius, capM;
+};
+
+__device__ __forceinline__ Resv resv_empty() {
+  Resv r;
+  r.a = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
+  r.b = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  r.c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  return r;
+}
+
+// Unoccluded area-measure integrand at surface s for light point y; returns the target.
+__device__ __forceinline__ float restir_target(const float4 *__restrict__ mats, const Material &m, const Surf &s,
+                                               V3 lpos, V3 lnrm, int32_t lp, V3 &fa, V3 &wi, float &dist) {
+  fa = v3(0.0f, 0.0f, 0.0f);
+  if (lp < 0 || lp == __float_as_int(s.n.w)) return 0.0f;
+  V3 p = ld3(s.p), n = ld3(s.n);
+  V3 toL = lpos - p;
+  float dist2 = dot(toL, toL);
+  if (dist2 <= kRayEps) return 0.0f;
+  dist = sqrtf(dist2);
+  wi = toL / dist;
+  float cosT = fmax_ref(dot(n, wi), 0.0f), cosL = fmax_ref(dot(lnrm, -wi), 0.0f);
+  if (cosT <= 0.0f || cosL <= 0.0f) return 0.0f;
+  Material lm = decode_material(mats, lp, 1.0f);
+  V3 lrad = lm.emission * lm.power;
+  V3 f = eval_bsdf(m, n, ld3(s.v), wi) * lrad * cosT;
+  float g = cosL / fmax_ref(dist2, kRayEps);
+  fa = f * g;
+  return fmax_ref(luminance(fa), 0.0f);
+}
+
+__device__ __forceinline__ bool restir_gate(const Surf &s, const Surf &q) {
+  if (q.v.w <= 0.0f) return false;
+  float depth = s.p.w;
+  V3 dp = ld3(q.p) - ld3(s.p);
+  float posTh = fmax_ref(0.01f * depth, 0.02f), depTh = fmax_ref(0.02f * depth, 0.05f);
+  if (!(length(dp) <= posTh)) return false;
+  if (!(fabsf(q.p.w - depth) <= depTh)) return false;
+  V3 qn = ld3(q.n);
+  float qn2 = dot(qn, qn);
+  if (!(qn2 > kRayEps)) return false;
+  return dot(normalize(qn), normalize(ld3(s.n))) >= 0.9f;
+}
+
+// Adds a reused reservoir to `out` (the owner surface s, material m).
+__device__ __forceinline__ void restir_merge(Resv &out, const Resv &src, const Surf &s, const Material &m,
+                                             const float4 *__restrict__ mats, float capM, float u) {
+  int32_t lp = __float_as_int(src.a.w);
+  if (lp < 0 || !(src.c.z > 0.0f) || !(src.c.y > 0.0f) || !(src.c.w > 0.0f)) return;
+  float Mp = fmin_ref(src.c.z, capM);
+  float Wp = src.c.y / (src.c.z * src.c.w);
+  V3 fa, wi;
+  float dist;
+  float ph = restir_target(mats, m, s, ld3(src.a), ld3(src.b), lp, fa, wi, dist);
+  float w = ph * Wp * Mp;
+  out.c.y = out.c.y + w;
+  out.c.z = out.c.z + Mp;
+  if (w > 0.0f && u * out.c.y < w) {
+    out.a = src.a;
+    out.b = src.b;
+    out.c.w = ph;
+  }
+}
+
+__global__ void __launch_bounds__(kPtBlock) k_restir_initial(
+    const ViewDev *__restrict__ views, uint32_t nviews, unsigned long long P, RestirDev cfg,
+    const float4 *__restrict__ rays, const int32_t *__restrict__ hits, const float4 *__restrict__ prims,
+    const float4 *__restrict__ mats, Lights L, Resv *__restrict__ rOut, Surf *__restrict__ sOut) {
+  const uint32_t lightCount = L.meta->count;
+  const float lightTotal = L.meta->total;
+  for (unsigned long long pid = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; pid < P;
+       pid += (unsigned long long)gridDim.x * blockDim.x) {
+    const ViewDev &v = find_view(views, nviews, pid);
+    Resv r = resv_empty();
+    Surf s;
+    s.p = s.n = s.v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const int32_t *h = hits + 5 * pid;
+    int32_t prim = h[1];
+    if ((v.flags & NOMAD_VIEW_RESTIR) && prim >= 0 && lightCount > 0 && lightTotal > 0.0f) {
+      float t = __int_as_float(h[2]);
+      V3 o = ld3(rays[2 * pid]), d = ld3(rays[2 * pid + 1]);
+      V3 p = v3(o.x + t * d.x, o.y + t * d.y, o.z + t * d.z);
+      V3 n = hit_normal(prims, prim, p);
+      if (!(dot(n, d) < 0.0f)) n = -n;
+      Material m = decode_material(mats, prim, v.lod);
+      if (luminance(m.diffuse * m.opacity) > 0.0f) {
+        V3 vd = normalize(-d);
+        s.p = make_float4(p.x, p.y, p.z, length(p - o));
+        s.n = make_float4(n.x, n.y, n.z, __int_as_float(prim));
+        s.v = make_float4(vd.x, vd.y, vd.z, 1.0f);
+        unsigned long long local = pid - v.pathOffset;
+        uint32_t pixel = (uint32_t)(local / v.spp), sample = (uint32_t)(local % v.spp);
+        for (uint32_t c = 0; c < cfg.candidates; ++c) {
+          U4 u = philox(U4{pixel, sample, 0x10000u + c, v.index}, v.k0, v.k1);
+          uint32_t off = select_light(u01(u.x), L, lightCount, lightTotal);
+          int32_t lp = (int32_t)__ldg(L.idx + off);
+          V3 lpos, lnrm;
+          float area = 0.0f, w = 0.0f, ph = 0.0f;
+          if (lp != prim && sample_light(prims, (uint32_t)lp, u01(u.y), u01(u.z), lpos, lnrm, area) && area > 0.0f) {
+            float prev = off > 0 ? __ldg(L.cdf + off - 1) : 0.0f;
+            float wgt = __ldg(L.cdf + off) - prev;
+            float lpdf = wgt > 0.0f ? wgt / lightTotal : 0.0f;
+            float q = lpdf * (1.0f / area);
+            V3 fa, wi;
+            float dist;
+            ph = restir_target(mats, m, s, lpos, lnrm, lp, fa, wi, dist);
+            w = q > 0.0f ? ph / q : 0.0f;
+          }
+          r.c.z = r.c.z + 1.0f;
+          r.c.y = r.c.y + w;
+          if (w > 0.0f && u01(u.w) * r.c.y < w) {
+            r.a = make_float4(lpos.x, lpos.y, lpos.z, __int_as_float(lp));
+            r.b = make_float4(lnrm.x, lnrm.y, lnrm.z, 0.0f);
+            r.c.w = ph;
+          }
+        }
+      }
+    }
+    rOut[pid] = r;
+    sOut[pid] = s;
+  }
+}
+
+__global__ void __launch_bounds__(kPtBlock) k_restir_temporal(
+    const ViewDev *__restrict__ views, const ViewDev *__restrict__ prevViews, uint32_t nviews,
+    unsigned long long P, RestirDev cfg, const float4 *__restrict__ mats, const Resv *__restrict__ rIn,
+    const Surf *__restrict__ sCur, const Resv *__restrict__ rPrev, const Surf *__restrict__ sPrev,
+    Resv *__restrict__ rOut, int usePrev) {
+  for (unsigned long long pid = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; pid < P;
+       pid += (unsigned long long)gridDim.x * blockDim.x) {
+    Resv out = rIn[pid];
+    const Surf s = sCur[pid];
+    if (usePrev && s.v.w > 0.0f) {
+      const ViewDev &v = find_view(views, nviews, pid);
+      const ViewDev &pv = prevViews[v.index];
+      V3 cam = v3(pv.cam[0], pv.cam[1], pv.cam[2]), U = v3(pv.vu[0], pv.vu[1], pv.vu[2]);
+      V3 Vv = v3(pv.vv[0], pv.vv[1], pv.vv[2]), fp = v3(pv.fp[0], pv.fp[1], pv.fp[2]);
+      V3 pn = cross(U, Vv);
+      V3 dd = ld3(s.p) - cam;
+      float den = dot(dd, pn);
+      float num = dot(fp - cam, pn);
+      if (den != 0.0f) {
+        float lam = num / den;
+        if (lam > 0.0f) {
+          V3 q = cam + dd * lam;
+          V3 rel = q - fp;
+          float u = dot(rel, U) / dot(U, U), w = dot(rel, Vv) / dot(Vv, Vv);
+          if (u >= 0.0f && u < 1.0f && w >= 0.0f && w < 1.0f) {
+            uint32_t px = min((uint32_t)(u * (float)pv.w), pv.w - 1), py = min((uint32_t)(w * (float)pv.h), pv.h - 1);
+            unsigned long long local = pid - v.pathOffset;
+            uint32_t pixel = (uint32_t)(local / v.spp), sample = (uint32_t)(local % v.spp);
+            unsigned long long ppid = pv.pathOffset + ((unsigned long long)py * pv.w + px) * pv.spp + sample;
+            if (restir_gate(s, sPrev[ppid])) {
+              Material m = decode_material(mats, __float_as_int(s.n.w), v.lod);
+              U4 rr = philox(U4{pixel, sample, 0x20000u, v.index}, v.k0, v.k1);
+              restir_merge(out, rPrev[ppid], s, m, mats, cfg.capM * (float)cfg.candidates, u01(rr.x));
+            }
+          }
+        }
+      }
+    }
+    rOut[pid] = out;
+  }
+}
+
+__global__ void __launch_bounds__(kPtBlock) k_restir_spatial(
+    const ViewDev *__restrict__ views, uint32_t nviews, unsigned long long P, RestirDev cfg,
+    const float4 *__restrict__ mats, const Resv *__restrict__ rIn, const Surf *__restrict__ sCur,
+    Resv *__restrict__ rOut) {
+  for (unsigned long long pid = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; pid < P;
+       pid += (unsigned long long)gridDim.x * blockDim.x) {
+    Resv out = rIn[pid];
+    const Surf s = sCur[pid];
+    if (s.v.w > 0.0f && cfg.spatial > 0) {
+      const ViewDev &v = find_view(views, nviews, pid);
+      unsigned long long local = pid - v.pathOffset;
+      uint32_t pixel = (uint32_t)(local / v.spp), sample = (uint32_t)(local % v.spp);
+      int px = (int)(pixel % v.w), py = (int)(pixel / v.w);
+      Material m = decode_material(mats, __float_as_int(s.n.w), v.lod);
+      for (uint32_t k = 0; k < cfg.spatial; ++k) {
+        U4 rr = philox(U4{pixel, sample, 0x30000u + k, v.index}, v.k0, v.k1);
+        float rad = cfg.radius * sqrtf(u01(rr.x));
+        float sn, cs;
+        sincos_turns(u01(rr.y), sn, cs);
+        int nx = px + (int)floorf(rad * cs + 0.5f), ny = py + (int)floorf(rad * sn + 0.5f);
+        if ((nx == px && ny == py) || nx < 0 || ny < 0 || nx >= (int)v.w || ny >= (int)v.h) continue;
+        unsigned long long npid = v.pathOffset + ((unsigned long long)ny * v.w + nx) * v.spp + sample;
+        if (!restir_gate(s, sCur[npid])) continue;
+        restir_merge(out, rIn[npid], s, m, mats, cfg.capM * (float)cfg.candidates, u01(rr.z));
+      }
+    }
+    rOut[pid] = out;
+  }
+}
+
+__global__ void __launch_bounds__(kPtBlock) k_restir_shade(
+    const ViewDev *__restrict__ views, uint32_t nviews, unsigned long long P, const float4 *__restrict__ mats,
+    const Resv *__restrict__ rIn, const Surf *__restrict__ sCur, float4 *__restrict__ sRays,
+    uint32_t *__restrict__ sIds, float4 *__restrict__ sContrib, Counters *cnt) {
+  unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  unsigned long long iters = (P + stride - 1) / stride;
+  for (unsigned long long it = 0; it < iters; ++it) {
+    unsigned long long pid = it * stride + (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    bool want = false;
+    float4 A = make_float4(0, 0, 0, 0), B = A, Cc = A;
+    if (pid < P) {
+      const Resv r = rIn[pid];
+      const Surf s = sCur[pid];
+      int32_t lp = __float_as_int(r.a.w);
+      if (s.v.w > 0.0f && lp >= 0 && r.c.z > 0.0f && r.c.y > 0.0f && r.c.w > 0.0f) {
+        const ViewDev &v = find_view(views, nviews, pid);
+        Material m = decode_material(mats, __float_as_int(s.n.w), v.lod);
+        V3 fa, wi;
+        float dist = 0.0f;
+        float ph = restir_target(mats, m, s, ld3(r.a), ld3(r.b), lp, fa, wi, dist);
+        if (ph > 0.0f) {
+          float W = r.c.y / (r.c.z * r.c.w);
+          V3 c = fa * W;
+          float tmax = dist - kRayEps;
+          if (tmax < kRayEps) tmax = kRayEps;
+          V3 o = ld3(s.p) + ld3(s.n) * (5.0f * kRayEps);
+          A = make_float4(o.x, o.y, o.z, kRayEps);
+          B = make_float4(wi.x, wi.y, wi.z, tmax);
+          Cc = make_float4(c.x, c.y, c.z, 0.0f);
+          want = true;
+        }
+      }
+    }
+    uint32_t slot = warp_append(&cnt->qlen[2], want);
+    if (want) {
+      sRays[2 * slot] = A;
+      sRays[2 * slot + 1] = B;
+      sIds[slot] = (uint32_t)pid;
+      sContrib[slot] = Cc;
+    }
+  }
+}
+
+nomad_status restir_pass(nomad_ctx *ctx, uint32_t nviews, const nomad_view *views, unsigned long long P,
+                         const Lights &L, Counters *C) {
+  FrameState &F = ctx->frame;
+  cudaStream_t s = ctx->stream;
+  if (F.restirPaths < P) {
+    NOMAD_CUDA(ctx, F.rInit.reserve(P * sizeof(Resv)));
+    NOMAD_CUDA(ctx, F.rTemp.reserve(P * sizeof(Resv)));
+    for (int k = 0; k < 2; ++k) {
+      NOMAD_CUDA(ctx, F.resv[k].reserve(P * sizeof(Resv)));
+      NOMAD_CUDA(ctx, F.surf[k].reserve(P * sizeof(Surf)));
+    }
+    F.restirPaths = P;
+    F.restirValid = false;
+  }
+  NOMAD_CUDA(ctx, F.prevViews.reserve(nviews * sizeof(ViewDev)));
+  bool compatible = F.restirValid && F.prevHostViews.size() == nviews;
+  for (uint32_t i = 0; compatible && i < nviews; ++i) {
+    const nomad_view &a = views[i], &b = F.prevHostViews[i];
+    compatible = a.width == b.width && a.height == b.height && a.spp == b.spp;
+  }
+  const nomad_restir_config &cf = F.restir;
+  RestirDev cfg{cf.candidates, cf.temporal, cf.spatial, cf.radius_px, cf.m_cap};
+  const ViewDev *V = F.views.as<const ViewDev>();
+  int cur = F.restirCur;
+  int grid = ctx->smCount * 8;
+  Surf *sCur = F.surf[cur].as<Surf>();
+  k_restir_initial<<<grid, kPtBlock, 0, s>>>(V, nviews, P, cfg, F.qRays[0].as<const float4>(), F.hits.as<const int32_t>(),
+                                            ctx->prims.as<const float4>(), ctx->materials.as<const float4>(), L,
+                                            F.rInit.as<Resv>(), sCur);
+  k_restir_temporal<<<grid, kPtBlock, 0, s>>>(V, F.prevViews.as<const ViewDev>(), nviews, P, cfg,
+                                             ctx->materials.as<const float4>(), F.rInit.as<const Resv>(), sCur,
+                                             F.resv[cur ^ 1].as<const Resv>(), F.surf[cur ^ 1].as<const Surf>(),
+                                             F.rTemp.as<Resv>(), (compatible && cf.temporal) ? 1 : 0);
+  k_restir_spatial<<<grid, kPtBlock, 0, s>>>(V, nviews, P, cfg, ctx->materials.as<const float4>(),
+                                            F.rTemp.as<const Resv>(), sCur, F.resv[cur].as<Resv>());
+  k_restir_shade<<<grid, kPtBlock, 0, s>>>(V, nviews, P, ctx->materials.as<const float4>(), F.resv[cur].as<const Resv>(),
+                                          sCur, F.sRays.as<float4>(), F.sIds.as<uint32_t>(), F.sContrib.as<float4>(), C);
+  NOMAD_CUDA(ctx, cudaGetLastError());
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(F.prevViews.p, F.views.p, nviews * sizeof(ViewDev), cudaMemcpyDeviceToDevice, s));
+  F.prevHostViews.assign(views, views + nviews);
+  F.restirCur ^= 1;
+  F.restirValid = true;
+  return NOMAD_OK;
+}
+
+}  // namespace
+
+extern "C" nomad_status nomad_set_restir(nomad_ctx *ctx, const nomad_restir_config *cfg) {
+  if (!ctx || !cfg) return NOMAD_ERR_INVALID_ARGUMENT;
+  if (cfg->candidates == 0 || cfg->candidates > 1024 || cfg->spatial > 16 || !(cfg->radius_px >= 0.0f) ||
+      !(cfg->m_cap > 0.0f))
+    return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "ReSTIR config out of range");
+  ctx->frame.restir = *cfg;
+  ctx->frame.restirValid = false;
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_reset_restir(nomad_ctx *ctx) {
+  if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
+  ctx->frame.restirValid = false;
   return NOMAD_OK;
 }

@@ -448,6 +448,7 @@ extern "C" nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residen
   nomad_status st = nomad_lights_update(ctx);
   if (st != NOMAD_OK) return st;
   ++R.frame;
+  // wide layouts follow the device flags (their root refs are fixed below with the host mirror)
   // host mirror of the object residency
   uint32_t misc[3];
   NOMAD_CUDA(ctx, cudaMemcpyAsync(misc, R.misc.p, 12, cudaMemcpyDeviceToHost, s));
@@ -459,6 +460,8 @@ extern "C" nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residen
   }
   for (uint32_t o = 0; o < N; ++o)
     ctx->instances[o].blas_root_index = ctx->objResident[o] ? ctx->layout.objRootNode[o] : -1;
+  st = nomad_patch_wide(ctx);
+  if (st != NOMAD_OK) return st;
   ctx->frame.restirValid = false;
   if (toggled) *toggled = misc[0];
   return NOMAD_OK;

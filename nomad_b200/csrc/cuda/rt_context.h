@@ -9,6 +9,7 @@
 #include "../../../include/nomad_rt.h"
 #include "../host/layout.h"
 #include "rt_device.cuh"
+#include "rt_wide.cuh"
 
 struct DeviceBuf {
   void *p = nullptr;
@@ -49,11 +50,14 @@ struct FrameState {
   DeviceBuf views;                    // view table
   DeviceBuf lightIdx, lightCdf, lightPdf, lightMeta;
   bool lightsDirty = true;
-  // ReSTIR DI reservoirs (current and previous frame) and surface records
-  DeviceBuf resv[2], surf[2];
-  uint64_t restirPixels = 0;
+  // ReSTIR DI: per-path reservoirs (initial, temporal, final of this and the previous frame),
+  // surface records (this and the previous frame) and the previous frame's view table
+  DeviceBuf rInit, rTemp, resv[2], surf[2], prevViews;
+  uint64_t restirPaths = 0;
   int restirCur = 0;
   bool restirValid = false;
+  nomad_restir_config restir{32, 1, 3, 30.0f, 20.0f};
+  std::vector<nomad_view> prevHostViews;
 };
 
 struct nomad_ctx {
@@ -75,6 +79,12 @@ struct nomad_ctx {
   DeviceBuf patchOffs, patchVals;
   size_t pnodeWords = 0;  // int32 words of the pair-node part of the arena
   nomad_dev::DevScene scene{};
+  // wide layouts (4 and 8 children) in the same arena
+  nomad::WideLayout wide[2];
+  size_t wideWordBase[2] = {0, 0};
+  nomad_dev::WideScene ws[2] = {};
+  uint32_t stackNeed[3] = {0, 0, 0};  // stack entries a walk can need: binary, 4-wide, 8-wide
+  DeviceBuf wideSlot[2], wideRef[2];
   // host copies needed by the light tables
   std::vector<float> hostPrims, hostMaterials;
   // host residency state
@@ -111,6 +121,13 @@ nomad_status nomad_residency_init(nomad_ctx *ctx);
 nomad_status nomad_residency_mirror(nomad_ctx *ctx);
 // Rebuilds the light CDF on the device if residency changed since the last build.
 nomad_status nomad_lights_update(nomad_ctx *ctx);
+// Rewrites every object's instance slot in the wide layouts from the device residency flags.
+nomad_status nomad_patch_wide(nomad_ctx *ctx);
+// Launches a closest- or any-hit trace of n device rays with the context's chosen variant
+// (queue length read from the device when lenDev is set).
+nomad_status nomad_trace_variant(nomad_ctx *ctx, uint32_t kernel, bool any, const float4 *rays, uint64_t n,
+                                 const uint32_t *lenDev, unsigned long long *cursor, int32_t *hits5,
+                                 uint8_t *occ, uint32_t *counts, cudaStream_t st);
 
 inline nomad_status nomad_fail(nomad_ctx *c, nomad_status st, const std::string &msg) {
   if (c) c->err = msg;

@@ -36,56 +36,64 @@ __device__ __forceinline__ void store_hit(nomad_hit *out, uint64_t i, const HitR
   o[4] = __float_as_int(h.v);
 }
 
-__global__ void __launch_bounds__(kBlock) k_closest(DevScene S, const float4 *__restrict__ rays,
-                                                     uint64_t n, nomad_hit *__restrict__ out,
-                                                     uint32_t *__restrict__ counts) {
-  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+// One kernel template for every traversal variant: width W (2 = pair nodes, 4, 8), stack size,
+// closest or any hit, one ray per thread or persistent warps. Closest hits are written as
+// (instance, primitive, t, u, v) words; lenDev, when set, holds the ray count on the device
+// (ray queues of the path tracer).
+template <int W, int STACK, bool ANY>
+__device__ __forceinline__ void trace_one(const DevScene &S, const WideScene &WS, const RayP &r, float tmax,
+                                          HitRec &h) {
+  if (W == 2) {
+    Work w{0, 0, 0};
+    traverse<STACK, ANY, false>(S, r, tmax, h, w);
+  } else {
+    traverse_wide<W, STACK, ANY>(S, WS, r, tmax, h);
+  }
+}
+
+template <int W, int STACK, bool ANY>
+__device__ __forceinline__ void trace_ray(const DevScene &S, const WideScene &WS, const float4 *__restrict__ rays,
+                                          uint64_t i, int32_t *__restrict__ hits5, uint8_t *__restrict__ occ,
+                                          uint32_t *__restrict__ counts) {
   float4 a = __ldg(rays + 2 * i), b = __ldg(rays + 2 * i + 1);
   RayP r = prep_ray(a, b);
   HitRec h;
-  Work w{0, 0, 0};
-  traverse<kStack, false, false>(S, r, b.w, h, w);
-  if (h.prim < 0) h.t = INFINITY;
-  store_hit(out, i, h);
-  if (counts) warp_count_object_hit(h.prim >= 0 ? h.inst : -1, counts);
+  trace_one<W, STACK, ANY>(S, WS, r, b.w, h);
+  if (ANY) {
+    occ[i] = h.prim >= 0 ? 1 : 0;
+  } else {
+    int32_t *o = hits5 + 5 * i;
+    o[0] = h.inst;
+    o[1] = h.prim;
+    o[2] = __float_as_int(h.prim >= 0 ? h.t : INFINITY);
+    o[3] = __float_as_int(h.u);
+    o[4] = __float_as_int(h.v);
+    if (counts) warp_count_object_hit(h.prim >= 0 ? h.inst : -1, counts);
+  }
 }
 
-// Persistent variant: each warp takes 32 rays at a time from a global cursor.
-__global__ void __launch_bounds__(kPersistBlock) k_closest_persist(
-    DevScene S, const float4 *__restrict__ rays, uint64_t n, nomad_hit *__restrict__ out,
-    uint32_t *__restrict__ counts, unsigned long long *__restrict__ cursor) {
+template <int W, int STACK, bool ANY, bool PERSIST>
+__global__ void __launch_bounds__(kBlock) k_trace(DevScene S, WideScene WS, const float4 *__restrict__ rays,
+                                                  uint64_t n, const uint32_t *__restrict__ lenDev,
+                                                  unsigned long long *__restrict__ cursor,
+                                                  int32_t *__restrict__ hits5, uint8_t *__restrict__ occ,
+                                                  uint32_t *__restrict__ counts) {
+  const uint64_t N = lenDev ? (uint64_t)*lenDev : n;
+  if (!PERSIST) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) trace_ray<W, STACK, ANY>(S, WS, rays, i, hits5, occ, counts);
+    return;
+  }
   int lane = threadIdx.x & 31;
   for (;;) {
     unsigned long long base = 0;
     if (lane == 0) base = atomicAdd(cursor, 32ull);
     base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= n) break;
+    if (base >= N) break;
     uint64_t i = base + lane;
-    if (i < n) {
-      float4 a = __ldg(rays + 2 * i), b = __ldg(rays + 2 * i + 1);
-      RayP r = prep_ray(a, b);
-      HitRec h;
-      Work w{0, 0, 0};
-      traverse<kStack, false, false>(S, r, b.w, h, w);
-      if (h.prim < 0) h.t = INFINITY;
-      store_hit(out, i, h);
-      if (counts) warp_count_object_hit(h.prim >= 0 ? h.inst : -1, counts);
-    }
+    if (i < N) trace_ray<W, STACK, ANY>(S, WS, rays, i, hits5, occ, counts);
     __syncwarp();
   }
-}
-
-__global__ void __launch_bounds__(kBlock) k_any(DevScene S, const float4 *__restrict__ rays,
-                                                 uint64_t n, uint8_t *__restrict__ out) {
-  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  float4 a = __ldg(rays + 2 * i), b = __ldg(rays + 2 * i + 1);
-  RayP r = prep_ray(a, b);
-  HitRec h;
-  Work w{0, 0, 0};
-  traverse<kStack, true, false>(S, r, b.w, h, w);
-  out[i] = h.prim >= 0 ? 1 : 0;
 }
 
 __global__ void __launch_bounds__(kBlock) k_work(DevScene S, const float4 *__restrict__ rays,
@@ -98,6 +106,17 @@ __global__ void __launch_bounds__(kBlock) k_work(DevScene S, const float4 *__res
   Work w{0, 0, 0};
   traverse<kStack, false, true>(S, r, b.w, h, w);
   out[i] = make_uint4(w.nodes, w.tests, w.insts, h.prim >= 0 ? 1u : 0u);
+}
+
+// Instance slots of the wide layouts from the device residency flags.
+__global__ void k_patch_wide(int32_t *__restrict__ arena, size_t base, uint32_t fpn, uint32_t width,
+                             const long long *__restrict__ slot, const int32_t *__restrict__ ref,
+                             const uint8_t *__restrict__ res, uint32_t n) {
+  uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= n) return;
+  long long s = slot[o];
+  if (s < 0) return;
+  arena[base + (size_t)(s / width) * fpn + 6 * width + (size_t)(s % width)] = res[o] ? ref[o] : kEmptyRef;
 }
 
 // Residency patches: word offsets into the layout arena and their new values.
@@ -149,7 +168,7 @@ extern "C" nomad_status nomad_create(const nomad_config *cfg, nomad_ctx **out) {
   c->stream = c->ownStream;
   for (auto &s : c->copyStreams)
     if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return NOMAD_ERR_CUDA;
-  if (c->status.reserve(16) != cudaSuccess || c->cursor.reserve(16) != cudaSuccess)
+  if (c->status.reserve(16) != cudaSuccess || c->cursor.reserve(64) != cudaSuccess)
     return NOMAD_ERR_OUT_OF_MEMORY;
   cudaMemset(c->status.p, 0, 16);
   *out = c.release();
@@ -219,8 +238,18 @@ extern "C" nomad_status nomad_scene_upload(nomad_ctx *ctx, const float *bvh, uin
     return fail(ctx, NOMAD_ERR_LIMIT,
                 "tree depth " + std::to_string(ctx->layout.maxDepth) + " exceeds the traversal stack");
   const auto &L = ctx->layout;
+  ctx->stackNeed[0] = L.maxDepth;
+  try {
+    for (int w = 0; w < 2; ++w) {
+      nomad::build_wide_layout(L, w == 0 ? 4 : 8, ctx->objResident, ctx->wide[w]);
+      ctx->stackNeed[1 + w] = (ctx->wide[w].width - 1) * ctx->wide[w].maxDepth;
+    }
+  } catch (const std::bad_alloc &) {
+    return fail(ctx, NOMAD_ERR_OUT_OF_MEMORY, "host memory");
+  }
   size_t pnBytes = L.pnodes.size() * 4, triBytes = L.tris.size() * 4;
-  NOMAD_CUDA(ctx, ctx->arena.reserve(pnBytes + triBytes + 64));
+  size_t wBytes[2] = {ctx->wide[0].nodes.size() * 4, ctx->wide[1].nodes.size() * 4};
+  NOMAD_CUDA(ctx, ctx->arena.reserve(pnBytes + triBytes + wBytes[0] + wBytes[1] + 256));
   NOMAD_CUDA(ctx, ctx->prims.reserve((size_t)primCount * 112));
   NOMAD_CUDA(ctx, ctx->materials.reserve((size_t)primCount * 80));
   NOMAD_CUDA(ctx, ctx->objHits.reserve((size_t)objectCount * 4 + 16));
@@ -228,6 +257,21 @@ extern "C" nomad_status nomad_scene_upload(nomad_ctx *ctx, const float *bvh, uin
   if (pnBytes)
     NOMAD_CUDA(ctx, cudaMemcpy(base, L.pnodes.data(), pnBytes, cudaMemcpyHostToDevice));
   NOMAD_CUDA(ctx, cudaMemcpy(base + pnBytes, L.tris.data(), triBytes, cudaMemcpyHostToDevice));
+  {
+    size_t off = pnBytes + triBytes;
+    for (int w = 0; w < 2; ++w) {
+      const nomad::WideLayout &WL = ctx->wide[w];
+      if (wBytes[w]) NOMAD_CUDA(ctx, cudaMemcpy(base + off, WL.nodes.data(), wBytes[w], cudaMemcpyHostToDevice));
+      ctx->wideWordBase[w] = off / 4;
+      ctx->ws[w].wn = reinterpret_cast<const float4 *>(base + off);
+      ctx->ws[w].root = WL.rootRef;
+      NOMAD_CUDA(ctx, ctx->wideSlot[w].reserve((size_t)objectCount * 8 + 8));
+      NOMAD_CUDA(ctx, ctx->wideRef[w].reserve((size_t)objectCount * 4 + 4));
+      NOMAD_CUDA(ctx, cudaMemcpy(ctx->wideSlot[w].p, WL.objSlot.data(), (size_t)objectCount * 8, cudaMemcpyHostToDevice));
+      NOMAD_CUDA(ctx, cudaMemcpy(ctx->wideRef[w].p, WL.objBlasRef.data(), (size_t)objectCount * 4, cudaMemcpyHostToDevice));
+      off += wBytes[w];
+    }
+  }
   NOMAD_CUDA(ctx, cudaMemcpy(ctx->prims.p, prims, (size_t)primCount * 112, cudaMemcpyHostToDevice));
   NOMAD_CUDA(ctx, cudaMemcpy(ctx->materials.p, materials, (size_t)primCount * 80,
                              cudaMemcpyHostToDevice));
@@ -346,6 +390,8 @@ extern "C" nomad_status nomad_residency_flush(nomad_ctx *ctx) {
   if (mirror) {
     nomad_status mst = nomad_residency_mirror(ctx);
     if (mst != NOMAD_OK) return mst;
+    mst = nomad_patch_wide(ctx);
+    if (mst != NOMAD_OK) return mst;
   }
   if (offs.empty()) return NOMAD_OK;
   NOMAD_CUDA(ctx, ctx->patchOffs.reserve(offs.size() * 8));
@@ -374,48 +420,102 @@ extern "C" nomad_status nomad_residency_get_instances(nomad_ctx *ctx, nomad_inst
   return NOMAD_OK;
 }
 
+namespace {
+
+// Stack entries of each variant: pair nodes 64; 4-wide 64; 8-wide 96.
+constexpr int kStackW4 = 64, kStackW8 = 96;
+
+bool variant_ok(const nomad_ctx *ctx, uint32_t k) {
+  switch (k) {
+    case NOMAD_KERNEL_BVH2:
+    case NOMAD_KERNEL_BVH2_PERSIST: return ctx->stackNeed[0] <= (uint32_t)kStack;
+    case NOMAD_KERNEL_BVH4:
+    case NOMAD_KERNEL_BVH4_PERSIST: return ctx->wide[0].width == 4 && ctx->stackNeed[1] <= (uint32_t)kStackW4;
+    case NOMAD_KERNEL_BVH8:
+    case NOMAD_KERNEL_BVH8_PERSIST: return ctx->wide[1].width == 8 && ctx->stackNeed[2] <= (uint32_t)kStackW8;
+    default: return false;
+  }
+}
+
+template <int W, int STACK, bool ANY, bool PERSIST>
+nomad_status launch_one(nomad_ctx *ctx, const WideScene &WS, const float4 *rays, uint64_t n, const uint32_t *lenDev,
+                        unsigned long long *cursor, int32_t *hits5, uint8_t *occ, uint32_t *counts, cudaStream_t st) {
+  auto kern = k_trace<W, STACK, ANY, PERSIST>;
+  uint64_t blocks;
+  if (PERSIST) {
+    int perSm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kern, kBlock, 0);
+    blocks = (uint64_t)ctx->smCount * std::max(perSm, 1);
+    blocks = std::max<uint64_t>(1, std::min(blocks, (n + kBlock - 1) / kBlock));
+    NOMAD_CUDA(ctx, cudaMemsetAsync(cursor, 0, 8, st));
+  } else {
+    blocks = (n + kBlock - 1) / kBlock;
+    if (blocks > 0x7fffffffull) return nomad_fail(ctx, NOMAD_ERR_LIMIT, "too many rays for one call");
+  }
+  kern<<<(unsigned)blocks, kBlock, 0, st>>>(ctx->scene, WS, rays, n, lenDev, cursor, hits5, occ, counts);
+  NOMAD_CUDA(ctx, cudaGetLastError());
+  return NOMAD_OK;
+}
+
+template <bool ANY>
+nomad_status dispatch(nomad_ctx *ctx, uint32_t k, const float4 *rays, uint64_t n, const uint32_t *lenDev,
+                      unsigned long long *cursor, int32_t *hits5, uint8_t *occ, uint32_t *counts, cudaStream_t st) {
+  const WideScene none{nullptr, kEmptyRef};
+  switch (k) {
+    case NOMAD_KERNEL_BVH2: return launch_one<2, kStack, ANY, false>(ctx, none, rays, n, lenDev, cursor, hits5, occ, counts, st);
+    case NOMAD_KERNEL_BVH2_PERSIST: return launch_one<2, kStack, ANY, true>(ctx, none, rays, n, lenDev, cursor, hits5, occ, counts, st);
+    case NOMAD_KERNEL_BVH4: return launch_one<4, kStackW4, ANY, false>(ctx, ctx->ws[0], rays, n, lenDev, cursor, hits5, occ, counts, st);
+    case NOMAD_KERNEL_BVH4_PERSIST: return launch_one<4, kStackW4, ANY, true>(ctx, ctx->ws[0], rays, n, lenDev, cursor, hits5, occ, counts, st);
+    case NOMAD_KERNEL_BVH8: return launch_one<8, kStackW8, ANY, false>(ctx, ctx->ws[1], rays, n, lenDev, cursor, hits5, occ, counts, st);
+    case NOMAD_KERNEL_BVH8_PERSIST: return launch_one<8, kStackW8, ANY, true>(ctx, ctx->ws[1], rays, n, lenDev, cursor, hits5, occ, counts, st);
+    default: return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "unknown kernel variant");
+  }
+}
+
+}  // namespace
+
+nomad_status nomad_trace_variant(nomad_ctx *ctx, uint32_t kernel, bool any, const float4 *rays, uint64_t n,
+                                 const uint32_t *lenDev, unsigned long long *cursor, int32_t *hits5,
+                                 uint8_t *occ, uint32_t *counts, cudaStream_t st) {
+  if (n == 0) return NOMAD_OK;
+  if (!variant_ok(ctx, kernel)) return nomad_fail(ctx, NOMAD_ERR_UNSUPPORTED, "kernel variant not available for this scene");
+  return any ? dispatch<true>(ctx, kernel, rays, n, lenDev, cursor, hits5, occ, counts, st)
+             : dispatch<false>(ctx, kernel, rays, n, lenDev, cursor, hits5, occ, counts, st);
+}
+
 extern "C" nomad_status nomad_set_kernel(nomad_ctx *ctx, uint32_t kernel) {
   if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
   if (kernel == NOMAD_KERNEL_AUTO) kernel = NOMAD_KERNEL_BVH2;
-  if (kernel != NOMAD_KERNEL_BVH2 && kernel != NOMAD_KERNEL_BVH2_PERSIST)
-    return fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "unknown kernel");
+  if (kernel >= NOMAD_KERNEL_COUNT) return fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "unknown kernel");
+  if (ctx->sceneReady && !variant_ok(ctx, kernel))
+    return fail(ctx, NOMAD_ERR_UNSUPPORTED, "kernel variant needs a deeper stack than it has for this scene");
   ctx->kernel = kernel;
   return NOMAD_OK;
 }
 
 namespace {
 
-// Launches one of the trace kernels over device arrays on `st`.
+// Launches one of the trace kernels over device arrays on `st`; `slot` picks the cursor word
+// (one per stream that may run a persistent kernel concurrently).
 enum class Op { Closest, Any, Work };
 
 nomad_status launch(nomad_ctx *ctx, Op op, const float4 *rays, uint64_t n, void *out,
-                    bool countHits, cudaStream_t st) {
+                    bool countHits, cudaStream_t st, int slot = 0) {
   if (n == 0) return NOMAD_OK;
   uint32_t *counts = countHits ? static_cast<uint32_t *>(ctx->objHits.p) : nullptr;
-  if (op == Op::Closest && ctx->kernel == NOMAD_KERNEL_BVH2_PERSIST) {
-    NOMAD_CUDA(ctx, cudaMemsetAsync(ctx->cursor.p, 0, 8, st));
-    int perSm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_closest_persist, kPersistBlock, 0);
-    perSm = std::max(perSm, 1);
-    uint64_t blocks = (uint64_t)ctx->smCount * perSm;
-    uint64_t need = (n + kPersistBlock - 1) / kPersistBlock;
-    blocks = std::max<uint64_t>(1, std::min(blocks, need));
-    k_closest_persist<<<(unsigned)blocks, kPersistBlock, 0, st>>>(
-        ctx->scene, rays, n, static_cast<nomad_hit *>(out), counts,
-        static_cast<unsigned long long *>(ctx->cursor.p));
-  } else {
+  unsigned long long *cursor = static_cast<unsigned long long *>(ctx->cursor.p) + slot;
+  if (op == Op::Work) {
     uint64_t blocks = (n + kBlock - 1) / kBlock;
     if (blocks > 0x7fffffffull) return fail(ctx, NOMAD_ERR_LIMIT, "too many rays for one call");
-    if (op == Op::Closest)
-      k_closest<<<(unsigned)blocks, kBlock, 0, st>>>(ctx->scene, rays, n,
-                                                     static_cast<nomad_hit *>(out), counts);
-    else if (op == Op::Any)
-      k_any<<<(unsigned)blocks, kBlock, 0, st>>>(ctx->scene, rays, n, static_cast<uint8_t *>(out));
-    else
-      k_work<<<(unsigned)blocks, kBlock, 0, st>>>(ctx->scene, rays, n, static_cast<uint4 *>(out));
+    k_work<<<(unsigned)blocks, kBlock, 0, st>>>(ctx->scene, rays, n, static_cast<uint4 *>(out));
+    NOMAD_CUDA(ctx, cudaGetLastError());
+    return NOMAD_OK;
   }
-  NOMAD_CUDA(ctx, cudaGetLastError());
-  return NOMAD_OK;
+  if (op == Op::Any)
+    return nomad_trace_variant(ctx, ctx->kernel, true, rays, n, nullptr, cursor, nullptr, static_cast<uint8_t *>(out),
+                               nullptr, st);
+  return nomad_trace_variant(ctx, ctx->kernel, false, rays, n, nullptr, cursor, static_cast<int32_t *>(out), nullptr,
+                             counts, st);
 }
 
 // Host-pointer path: rays are copied in and results out in chunks, alternating two streams
@@ -437,7 +537,7 @@ nomad_status trace_host(nomad_ctx *ctx, Op op, const nomad_ray *rays, uint64_t n
     char *din = static_cast<char *>(ctx->stageIn.p) + off * sizeof(nomad_ray);
     char *dout = static_cast<char *>(ctx->stageOut.p) + off * outStride;
     NOMAD_CUDA(ctx, cudaMemcpyAsync(din, rays + off, m * sizeof(nomad_ray), cudaMemcpyHostToDevice, s));
-    nomad_status st = launch(ctx, op, reinterpret_cast<const float4 *>(din), m, dout, countHits, s);
+    nomad_status st = launch(ctx, op, reinterpret_cast<const float4 *>(din), m, dout, countHits, s, 1 + (k & 1));
     if (st != NOMAD_OK) return st;
     NOMAD_CUDA(ctx, cudaMemcpyAsync(static_cast<char *>(out) + off * outStride, dout, m * outStride,
                                     cudaMemcpyDeviceToHost, s));
@@ -605,5 +705,85 @@ extern "C" nomad_status nomad_trace_closest_noalloc(nomad_ctx *ctx, const nomad_
   NOMAD_CUDA(ctx, cudaMemcpyAsync(d_object_hits, scratch + kNoAllocCursorWords,
                                   (size_t)ctx->objectCount * 4, cudaMemcpyDeviceToDevice,
                                   ctx->stream));
+  return NOMAD_OK;
+}
+
+nomad_status nomad_patch_wide(nomad_ctx *ctx) {
+  const uint32_t n = ctx->objectCount;
+  for (int w = 0; w < 2; ++w) {
+    const nomad::WideLayout &WL = ctx->wide[w];
+    if (!WL.width) continue;
+    k_patch_wide<<<(n + 255) / 256, 256, 0, ctx->stream>>>(static_cast<int32_t *>(ctx->arena.p), ctx->wideWordBase[w],
+                                                          WL.floatsPerNode, WL.width, ctx->wideSlot[w].as<const long long>(),
+                                                          ctx->wideRef[w].as<const int32_t>(),
+                                                          ctx->res.objRes.as<const uint8_t>(), n);
+    NOMAD_CUDA(ctx, cudaGetLastError());
+    for (uint32_t o = 0; o < n; ++o)
+      if (WL.objSlot[o] == -1) ctx->ws[w].root = ctx->objResident[o] ? WL.objBlasRef[o] : kEmptyRef;
+  }
+  NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_autotune(nomad_ctx *ctx, const nomad_ray *rays, uint64_t n, uint32_t repeats,
+                                       uint32_t flags, nomad_tune_result *out) {
+  if (!ctx || !out) return NOMAD_ERR_INVALID_ARGUMENT;
+  if (!ctx->sceneReady) return fail(ctx, NOMAD_ERR_NOT_READY, "no scene uploaded");
+  if (!rays || n == 0) return fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "no sample rays");
+  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  const float4 *d = reinterpret_cast<const float4 *>(rays);
+  if (!(flags & NOMAD_TRACE_DEVICE_POINTERS)) {
+    NOMAD_CUDA(ctx, ctx->stageIn.reserve(n * sizeof(nomad_ray)));
+    NOMAD_CUDA(ctx, cudaMemcpyAsync(ctx->stageIn.p, rays, n * sizeof(nomad_ray), cudaMemcpyHostToDevice, s));
+    d = ctx->stageIn.as<const float4>();
+  }
+  DeviceBuf ref, cur;
+  NOMAD_CUDA(ctx, ref.reserve(n * 20));
+  NOMAD_CUDA(ctx, cur.reserve(n * 20));
+  std::vector<int32_t> hRef(n * 5), hCur(n * 5);
+  cudaEvent_t e0, e1;
+  NOMAD_CUDA(ctx, cudaEventCreate(&e0));
+  NOMAD_CUDA(ctx, cudaEventCreate(&e1));
+  std::memset(out, 0, sizeof(*out));
+  for (int w = 0; w < 3; ++w) out->stack_need[w] = ctx->stackNeed[w];
+  float bestMs = 1e30f;
+  uint32_t best = NOMAD_KERNEL_BVH2;
+  unsigned long long *cursor = static_cast<unsigned long long *>(ctx->cursor.p);
+  for (uint32_t k = NOMAD_KERNEL_BVH2; k < NOMAD_KERNEL_COUNT; ++k) {
+    out->ms[k] = -1.0f;
+    if (!variant_ok(ctx, k)) continue;
+    DeviceBuf &dst = (k == NOMAD_KERNEL_BVH2) ? ref : cur;
+    float t = 1e30f;
+    for (uint32_t rep = 0; rep < std::max(1u, repeats) + 1; ++rep) {
+      NOMAD_CUDA(ctx, cudaEventRecord(e0, s));
+      nomad_status st = nomad_trace_variant(ctx, k, false, d, n, nullptr, cursor, dst.as<int32_t>(), nullptr, nullptr, s);
+      if (st != NOMAD_OK) return st;
+      NOMAD_CUDA(ctx, cudaEventRecord(e1, s));
+      NOMAD_CUDA(ctx, cudaEventSynchronize(e1));
+      float ms = 0.0f;
+      NOMAD_CUDA(ctx, cudaEventElapsedTime(&ms, e0, e1));
+      if (rep > 0) t = std::min(t, ms);  // first launch is a warm-up
+    }
+    out->ms[k] = t;
+    if (k == NOMAD_KERNEL_BVH2) {
+      NOMAD_CUDA(ctx, cudaMemcpy(hRef.data(), ref.p, n * 20, cudaMemcpyDeviceToHost));
+    } else {
+      NOMAD_CUDA(ctx, cudaMemcpy(hCur.data(), cur.p, n * 20, cudaMemcpyDeviceToHost));
+      uint32_t bad = 0;
+      for (uint64_t i = 0; i < n; ++i)
+        if (std::memcmp(&hRef[5 * i], &hCur[5 * i], 20) != 0) ++bad;
+      out->mismatches[k] = bad;
+      if (bad) continue;  // a variant that disagrees is never chosen
+    }
+    if (t < bestMs) {
+      bestMs = t;
+      best = k;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  ctx->kernel = best;
+  out->best = best;
   return NOMAD_OK;
 }

@@ -45,6 +45,20 @@ struct TraversalLayout {
   std::vector<int32_t> primPos;     // position of every primitive in leaf order
 };
 
+// 4- or 8-wide layout collapsed from the pair nodes (see wide.cpp). Leaves use the same
+// triangle records; refs are encoded as in the pair layout.
+struct WideLayout {
+  uint32_t width = 0;
+  uint32_t floatsPerNode = 0;        // 32 (W = 4) or 64 (W = 8)
+  std::vector<float> nodes;
+  int32_t rootRef = kEmptyRef;
+  std::vector<int32_t> objBlasRef;   // wide ref of each object's BLAS root
+  std::vector<int64_t> objSlot;      // node * W + k of each instance link, -1 root, -2 none
+  uint32_t maxDepth = 0;             // wide nodes on the longest path (+1 for the leaf)
+};
+
+void build_wide_layout(const TraversalLayout &L, int width, const std::vector<uint8_t> &resident, WideLayout &W);
+
 struct ObjectRange {
   int32_t blasRoot;  // SceneObject::blasRootIndex, or -1 when the caller marks it non-resident
   uint32_t first, count;

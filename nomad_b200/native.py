@@ -107,7 +107,23 @@ SIGNATURES = {
     "nomad_mlp_infer": (C.c_int32, [_P, _P, C.c_uint64, _P, C.c_uint32]),
     "nomad_mlp_get": (C.c_int32, [_P, _P]),
     "nomad_mlp_set": (C.c_int32, [_P, _P]),
+    "nomad_set_restir": (C.c_int32, [_P, _P]),
+    "nomad_reset_restir": (C.c_int32, [_P]),
+    "nomad_autotune": (C.c_int32, [_P, _P, C.c_uint64, C.c_uint32, C.c_uint32, _P]),
 }
+
+KERNEL_BVH4, KERNEL_BVH4_PERSIST, KERNEL_BVH8, KERNEL_BVH8_PERSIST, KERNEL_COUNT = 3, 4, 5, 6, 7
+KERNEL_NAMES = {1: "bvh2", 2: "bvh2_persist", 3: "bvh4", 4: "bvh4_persist", 5: "bvh8", 6: "bvh8_persist"}
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("best", C.c_uint32), ("ms", C.c_float * 7), ("mismatches", C.c_uint32 * 7),
+                ("stack_need", C.c_uint32 * 3)]
+
+
+class RestirConfig(C.Structure):
+    _fields_ = [("candidates", C.c_uint32), ("temporal", C.c_uint32), ("spatial", C.c_uint32),
+                ("radius_px", C.c_float), ("m_cap", C.c_float)]
 
 POLICY_ALWAYS, POLICY_RAYHIT_BUDGET, POLICY_LEARNED = 0, 1, 2
 N_FEATURES = 24
@@ -132,6 +148,7 @@ VIEW_DTYPE = np.dtype([("camera_pos", "<f4", 3), ("viewport_u", "<f4", 3), ("vie
                        ("flags", "<u4")])
 VIEW_CLAMP = 1 << 0
 VIEW_RESTIR = 1 << 1
+VIEW_CENTER = 1 << 2
 
 
 def view_pinhole(position, look_at, up=(0.0, 1.0, 0.0), vfov=60.0, width=640, height=360, spp=1,
@@ -344,6 +361,21 @@ class Context:
     def set_stream(self, stream_handle: int):
         self._ck(self.lib.nomad_set_stream(self.h, _P(stream_handle) if stream_handle else None))
 
+    def autotune(self, rays, repeats=3, device=False) -> dict:
+        """Times every traversal variant on the sample rays (numpy records, or a device pointer
+        with device=True and rays=(ptr, n)), selects the fastest; returns the table."""
+        r = TuneResult()
+        if device:
+            ptr, n = rays
+            self._ck(self.lib.nomad_autotune(self.h, _P(ptr), n, repeats, TRACE_DEVICE_POINTERS, C.byref(r)))
+        else:
+            rr = np.ascontiguousarray(rays, RAY_DTYPE)
+            self._ck(self.lib.nomad_autotune(self.h, _ptr(rr), rr.shape[0], repeats, 0, C.byref(r)))
+        return {"best": KERNEL_NAMES.get(r.best, str(r.best)), "best_id": int(r.best),
+                "ms": {KERNEL_NAMES[k]: float(r.ms[k]) for k in range(1, 7)},
+                "mismatches": {KERNEL_NAMES[k]: int(r.mismatches[k]) for k in range(1, 7)},
+                "stack_need": list(r.stack_need)}
+
     def set_kernel(self, k: int):
         self._ck(self.lib.nomad_set_kernel(self.h, k))
 
@@ -490,6 +522,14 @@ class Context:
         b = np.ascontiguousarray(blob, np.float32)
         assert b.size == MLP_PARAMS
         self._ck(self.lib.nomad_mlp_set(self.h, _ptr(b)))
+
+    # ReSTIR DI
+    def set_restir(self, candidates=32, temporal=True, spatial=3, radius_px=30.0, m_cap=20.0):
+        cfg = RestirConfig(candidates, int(temporal), spatial, radius_px, m_cap)
+        self._ck(self.lib.nomad_set_restir(self.h, C.byref(cfg)))
+
+    def reset_restir(self):
+        self._ck(self.lib.nomad_reset_restir(self.h))
 
     def object_hits(self) -> np.ndarray:
         out = np.zeros(self.object_count, np.uint32)

@@ -119,3 +119,45 @@ def render(os_: "OracleScene", materials, views, pixels=None, obj_hits=False, th
                            _p(hits) if hits is not None else None, _p(stats), threads)
     assert rc == 0
     return out, hits, stats
+
+
+class RestirOracle:
+    """Chains oracle_render_restir over consecutive frames (keeps the previous frame's
+    reservoirs, surfaces and views)."""
+
+    def __init__(self, os_, materials, candidates=32, temporal=True, spatial=3, radius_px=30.0, m_cap=20.0):
+        lib = load()
+        if not hasattr(lib, "_restir_bound"):
+            lib.oracle_render_restir.argtypes = [_P, _P, C.c_uint32, _P, _P, _P, _P, _P, _P, C.c_uint32,
+                                                 C.c_uint32, _P, C.c_uint32, _P, _P, _P, _P, _P, C.c_int,
+                                                 _P, _P, _P, _P, C.c_uint32]
+            lib.oracle_render_restir.restype = C.c_int
+            lib._restir_bound = True
+        self.os_ = os_
+        self.mats = np.ascontiguousarray(materials, np.float32)
+        self.cfg_u = np.array([candidates, int(temporal), spatial], np.uint32)
+        self.cfg_f = np.array([radius_px, m_cap], np.float32)
+        self.prev = None
+
+    def render(self, views):
+        lib = load()
+        os_ = self.os_
+        views = np.ascontiguousarray(views).reshape(-1)
+        P = int((views["width"].astype(np.int64) * views["height"] * views["spp"]).sum())
+        npx = int((views["width"].astype(np.int64) * views["height"]).sum())
+        resv = np.zeros((P, 12), np.float32)
+        surf = np.zeros((P, 12), np.float32)
+        rgb = np.zeros((npx, 3), np.float32)
+        stats = np.zeros(4, np.uint64)
+        have = self.prev is not None and self.prev[2].shape == views.shape and all(
+            (self.prev[2][k] == views[k]).all() for k in ("width", "height", "spp"))
+        pr, ps, pv = self.prev if have else (resv, surf, views)
+        rc = lib.oracle_render_restir(_p(os_.bvh), _p(os_.tlas), os_.tlas.size // 8, _p(os_.prims),
+                                      _p(self.mats), _p(os_.prim_indices), _p(os_.active),
+                                      _p(os_.blas_root), _p(os_.prim_object), os_.object_count,
+                                      os_.prims.size // 28, _p(views), views.shape[0], _p(self.cfg_u),
+                                      _p(self.cfg_f), _p(pr), _p(ps), _p(np.ascontiguousarray(pv)),
+                                      int(have), _p(resv), _p(surf), _p(rgb), _p(stats), 0)
+        assert rc == 0
+        self.prev = (resv, surf, views.copy())
+        return rgb, stats

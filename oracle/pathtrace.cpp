@@ -384,13 +384,23 @@ bool occluded(const Ctx &c, const Ray &r) {
 }
 
 // One path; returns its radiance (unclamped) and counts closest hits per object.
+// Precomputed ReSTIR result of one path: the shadow ray and its unoccluded contribution.
+struct RestirOut {
+  bool valid = false;
+  V origin, dir, contrib;
+  float tmax = 0.0f;
+};
+const uint32_t VIEW_RESTIR = 2u;
+
 V path(const Ctx &c, const View &vw, uint32_t vi, uint32_t pixel, uint32_t sample, uint32_t *objHits,
-       uint64_t *stats) {
+       uint64_t *stats, const RestirOut *rs = nullptr) {
   uint32_t k0 = vw.seedLo, k1 = vw.seedHi + vw.frame;
   uint32_t px = pixel % vw.w, py = pixel / vw.w;
   U4 r0 = philox(U4{pixel, sample, 255u * 4u, vi}, k0, k1);
   float ux = ((float)px + 0.5f) / (float)vw.w, uy = ((float)py + 0.5f) / (float)vw.h;
-  float s = ux + (u01(r0.x) - 0.5f) / (float)vw.w, t = uy + (u01(r0.y) - 0.5f) / (float)vw.h;
+  bool center = (vw.flags & 4u) != 0;
+  float s = ux + (center ? 0.0f : (u01(r0.x) - 0.5f) / (float)vw.w);
+  float t = uy + (center ? 0.0f : (u01(r0.y) - 0.5f) / (float)vw.h);
   V d = v(vw.fp[0] + s * vw.vu[0] + t * vw.vv[0] - vw.cam[0], vw.fp[1] + s * vw.vu[1] + t * vw.vv[1] - vw.cam[1],
           vw.fp[2] + s * vw.vu[2] + t * vw.vv[2] - vw.cam[2]);
   V dir = nrmz(d);
@@ -423,7 +433,13 @@ V path(const Ctx &c, const View &vw, uint32_t vi, uint32_t pixel, uint32_t sampl
     Mat m = decode(c.mats, h.prim, lod);
     if (m.power * lum(m.emission) > 0.0f) rad = add(rad, scl(mul(thr, m.emission), m.power));
     V dc = scl(m.diffuse, m.opacity);
-    if (lum(dc) > 0.0f && !c.L.idx.empty() && c.L.total > 0.0f) {
+    bool restirHere = depth == 0 && (vw.flags & VIEW_RESTIR) != 0;
+    if (restirHere) {
+      if (rs && rs->valid) {
+        stats[2]++;
+        if (!occluded(c, mkray(rs->origin, rs->dir, rs->tmax))) rad = add(rad, rs->contrib);
+      }
+    } else if (lum(dc) > 0.0f && !c.L.idx.empty() && c.L.total > 0.0f) {
       uint32_t off = select_light(u01(b0.x), c.L);
       uint32_t lp = c.L.idx[off];
       V lpos, lnrm;
@@ -558,4 +574,314 @@ extern "C" void oracle_math(float u, float out[4]) {
   sincos_turns(u, out[0], out[1]);
   out[2] = log2_series(u > 0.0f ? u : 1.0f);
   out[3] = exp2_series(-u * 4.0f);
+}
+
+// ---------------------------------------------------------------------------------------------
+// ReSTIR DI (config mode), restated pass by pass in the CUDA core's order: initial RIS for all
+// paths, temporal reuse for all paths, spatial reuse for all paths, final sample + shadow ray,
+// then the rest of every path. Reservoirs and surfaces use the device layout
+// (12 floats each) so consecutive frames can be chained through the caller.
+namespace {
+
+struct ResvH {
+  float a[4], b[4], c[4];
+};
+struct SurfH {
+  float p[4], n[4], v[4];
+};
+inline int32_t fbi(float f) {
+  int32_t i;
+  std::memcpy(&i, &f, 4);
+  return i;
+}
+inline float ibf(int32_t i) {
+  float f;
+  std::memcpy(&f, &i, 4);
+  return f;
+}
+ResvH resv_empty() {
+  ResvH r{};
+  r.a[3] = ibf(-1);
+  return r;
+}
+
+float restir_target(const Ctx &c, const Mat &m, const SurfH &s, V lpos, V lnrm, int32_t lp, V &fa, V &wi,
+                    float &dist) {
+  fa = v(0, 0, 0);
+  if (lp < 0 || lp == fbi(s.n[3])) return 0.0f;
+  V p = v(s.p[0], s.p[1], s.p[2]), n = v(s.n[0], s.n[1], s.n[2]);
+  V toL = vsub(lpos, p);
+  float d2 = dt(toL, toL);
+  if (d2 <= RAY_EPS) return 0.0f;
+  dist = std::sqrt(d2);
+  wi = dvs(toL, dist);
+  float cosT = mx(dt(n, wi), 0.0f), cosL = mx(dt(lnrm, neg(wi)), 0.0f);
+  if (cosT <= 0.0f || cosL <= 0.0f) return 0.0f;
+  Mat lm = decode(c.mats, lp, 1.0f);
+  V lrad = scl(lm.emission, lm.power);
+  V f = scl(mul(bsdf(m, n, v(s.v[0], s.v[1], s.v[2]), wi), lrad), cosT);
+  float g = cosL / mx(d2, RAY_EPS);
+  fa = scl(f, g);
+  return mx(lum(fa), 0.0f);
+}
+
+bool restir_gate(const SurfH &s, const SurfH &q) {
+  if (q.v[3] <= 0.0f) return false;
+  float depth = s.p[3];
+  V dp = vsub(v(q.p[0], q.p[1], q.p[2]), v(s.p[0], s.p[1], s.p[2]));
+  float posTh = mx(0.01f * depth, 0.02f), depTh = mx(0.02f * depth, 0.05f);
+  if (!(std::sqrt(dt(dp, dp)) <= posTh)) return false;
+  if (!(std::fabs(q.p[3] - depth) <= depTh)) return false;
+  V qn = v(q.n[0], q.n[1], q.n[2]);
+  if (!(dt(qn, qn) > RAY_EPS)) return false;
+  return dt(nrmz(qn), nrmz(v(s.n[0], s.n[1], s.n[2]))) >= 0.9f;
+}
+
+void restir_merge(const Ctx &c, ResvH &out, const ResvH &src, const SurfH &s, const Mat &m, float capM, float u) {
+  int32_t lp = fbi(src.a[3]);
+  if (lp < 0 || !(src.c[2] > 0.0f) || !(src.c[1] > 0.0f) || !(src.c[3] > 0.0f)) return;
+  float Mp = mn(src.c[2], capM);
+  float Wp = src.c[1] / (src.c[2] * src.c[3]);
+  V fa, wi;
+  float dist;
+  float ph = restir_target(c, m, s, v(src.a[0], src.a[1], src.a[2]), v(src.b[0], src.b[1], src.b[2]), lp, fa, wi, dist);
+  float w = ph * Wp * Mp;
+  out.c[1] = out.c[1] + w;
+  out.c[2] = out.c[2] + Mp;
+  if (w > 0.0f && u * out.c[1] < w) {
+    std::memcpy(out.a, src.a, 16);
+    std::memcpy(out.b, src.b, 16);
+    out.c[3] = ph;
+  }
+}
+
+float view_lod(const View &vw) {
+  float dx[3] = {vw.vu[0] / (float)vw.w, vw.vu[1] / (float)vw.w, vw.vu[2] / (float)vw.w};
+  float dy[3] = {vw.vv[0] / (float)vw.h, vw.vv[1] / (float)vw.h, vw.vv[2] / (float)vw.h};
+  float cx = dx[1] * dy[2] - dx[2] * dy[1], cy = dx[2] * dy[0] - dx[0] * dy[2], cz = dx[0] * dy[1] - dx[1] * dy[0];
+  return 1.0f / (1.0f + std::sqrt(cx * cx + cy * cy + cz * cz));
+}
+
+}  // namespace
+
+extern "C" int oracle_render_restir(const float *bvh, const float *tlas, uint32_t tlas_count, const float *prims,
+                                    const float *materials, const int32_t *prim_indices, const uint8_t *active,
+                                    const int32_t *blas_root, const int32_t *prim_object, uint32_t object_count,
+                                    uint32_t prim_count, const void *views, uint32_t nviews, const uint32_t *cfg_u,
+                                    const float *cfg_f, const float *prev_resv, const float *prev_surf,
+                                    const void *prev_views, int have_prev, float *out_resv, float *out_surf,
+                                    float *out_rgb, uint64_t *stats, uint32_t threads) {
+  Ctx c{{bvh, tlas, tlas_count, prims, prim_indices, active, blas_root, prim_object}, materials, {}, object_count};
+  c.L = build_lights(prims, materials, active, blas_root, prim_object, prim_count);
+  const View *vs = static_cast<const View *>(views);
+  const View *pvs = static_cast<const View *>(prev_views);
+  const uint32_t C = cfg_u[0], temporal = cfg_u[1], spatialN = cfg_u[2];
+  const float radius = cfg_f[0], capM = cfg_f[1] * (float)C;
+  std::vector<uint64_t> poff(nviews + 1, 0), xoff(nviews + 1, 0);
+  for (uint32_t i = 0; i < nviews; ++i) {
+    poff[i + 1] = poff[i] + (uint64_t)vs[i].w * vs[i].h * vs[i].spp;
+    xoff[i + 1] = xoff[i] + (uint64_t)vs[i].w * vs[i].h;
+  }
+  const uint64_t P = poff[nviews];
+  auto view_of = [&](uint64_t pid) {
+    uint32_t i = 0;
+    while (i + 1 < nviews && poff[i + 1] <= pid) ++i;
+    return i;
+  };
+  if (threads == 0) threads = std::max(1u, std::thread::hardware_concurrency());
+  auto par = [&](auto fn) {
+    std::atomic<uint64_t> next{0};
+    std::vector<std::thread> pool;
+    for (uint32_t t = 0; t < threads; ++t)
+      pool.emplace_back([&, t]() {
+        for (;;) {
+          uint64_t b = next.fetch_add(64);
+          if (b >= P) break;
+          for (uint64_t q = b; q < std::min<uint64_t>(P, b + 64); ++q) fn(q, t);
+        }
+      });
+    for (auto &th : pool) th.join();
+  };
+  std::vector<ResvH> rInit(P), rTemp(P);
+  ResvH *rFin = reinterpret_cast<ResvH *>(out_resv);
+  SurfH *sCur = reinterpret_cast<SurfH *>(out_surf);
+  const ResvH *rPrev = reinterpret_cast<const ResvH *>(prev_resv);
+  const SurfH *sPrev = reinterpret_cast<const SurfH *>(prev_surf);
+  // initial
+  par([&](uint64_t pid, uint32_t) {
+    uint32_t vi = view_of(pid);
+    const View &vw = vs[vi];
+    ResvH r = resv_empty();
+    SurfH s{};
+    uint64_t local = pid - poff[vi];
+    uint32_t pixel = (uint32_t)(local / vw.spp), sample = (uint32_t)(local % vw.spp);
+    uint32_t k0 = vw.seedLo, k1 = vw.seedHi + vw.frame;
+    if ((vw.flags & VIEW_RESTIR) && !c.L.idx.empty() && c.L.total > 0.0f) {
+      uint32_t px = pixel % vw.w, py = pixel / vw.w;
+      U4 r0 = philox(U4{pixel, sample, 255u * 4u, vi}, k0, k1);
+      float ux = ((float)px + 0.5f) / (float)vw.w, uy = ((float)py + 0.5f) / (float)vw.h;
+      bool center = (vw.flags & 4u) != 0;
+      float ss = ux + (center ? 0.0f : (u01(r0.x) - 0.5f) / (float)vw.w);
+      float tt = uy + (center ? 0.0f : (u01(r0.y) - 0.5f) / (float)vw.h);
+      V d = nrmz(v(vw.fp[0] + ss * vw.vu[0] + tt * vw.vv[0] - vw.cam[0], vw.fp[1] + ss * vw.vu[1] + tt * vw.vv[1] - vw.cam[1],
+                  vw.fp[2] + ss * vw.vu[2] + tt * vw.vv[2] - vw.cam[2]));
+      V o = v(vw.cam[0], vw.cam[1], vw.cam[2]);
+      Hit h = closest(c, mkray(o, d, INFINITY));
+      if (h.prim >= 0) {
+        V p = v(o.x + h.t * d.x, o.y + h.t * d.y, o.z + h.t * d.z);
+        V n = geom_normal(prims, h.prim, p);
+        if (!(dt(n, d) < 0.0f)) n = neg(n);
+        Mat m = decode(materials, h.prim, view_lod(vw));
+        if (lum(scl(m.diffuse, m.opacity)) > 0.0f) {
+          V vd = nrmz(neg(d));
+          V dd = vsub(p, o);
+          s = SurfH{{p.x, p.y, p.z, std::sqrt(dt(dd, dd))}, {n.x, n.y, n.z, ibf(h.prim)}, {vd.x, vd.y, vd.z, 1.0f}};
+          for (uint32_t k = 0; k < C; ++k) {
+            U4 u = philox(U4{pixel, sample, 0x10000u + k, vi}, k0, k1);
+            uint32_t off = select_light(u01(u.x), c.L);
+            int32_t lp = (int32_t)c.L.idx[off];
+            V lpos{0, 0, 0}, lnrm{0, 0, 0};
+            float area = 0.0f, w = 0.0f, ph = 0.0f;
+            if (lp != h.prim && light_point(prims, (uint32_t)lp, u01(u.y), u01(u.z), lpos, lnrm, area) && area > 0.0f) {
+              float prev = off > 0 ? c.L.cdf[off - 1] : 0.0f;
+              float wgt = c.L.cdf[off] - prev;
+              float lpdf = wgt > 0.0f ? wgt / c.L.total : 0.0f;
+              float q = lpdf * (1.0f / area);
+              V fa, wi;
+              float dist;
+              ph = restir_target(c, m, s, lpos, lnrm, lp, fa, wi, dist);
+              w = q > 0.0f ? ph / q : 0.0f;
+            }
+            r.c[2] = r.c[2] + 1.0f;
+            r.c[1] = r.c[1] + w;
+            if (w > 0.0f && u01(u.w) * r.c[1] < w) {
+              r.a[0] = lpos.x; r.a[1] = lpos.y; r.a[2] = lpos.z; r.a[3] = ibf(lp);
+              r.b[0] = lnrm.x; r.b[1] = lnrm.y; r.b[2] = lnrm.z; r.b[3] = 0.0f;
+              r.c[3] = ph;
+            }
+          }
+        }
+      }
+    }
+    rInit[pid] = r;
+    sCur[pid] = s;
+  });
+  // temporal
+  par([&](uint64_t pid, uint32_t) {
+    ResvH out = rInit[pid];
+    const SurfH &s = sCur[pid];
+    if (have_prev && temporal && s.v[3] > 0.0f) {
+      uint32_t vi = view_of(pid);
+      const View &vw = vs[vi], &pv = pvs[vi];
+      V cam = v(pv.cam[0], pv.cam[1], pv.cam[2]), U = v(pv.vu[0], pv.vu[1], pv.vu[2]);
+      V Vv = v(pv.vv[0], pv.vv[1], pv.vv[2]), fp = v(pv.fp[0], pv.fp[1], pv.fp[2]);
+      V pn = crs(U, Vv);
+      V dd = vsub(v(s.p[0], s.p[1], s.p[2]), cam);
+      float den = dt(dd, pn), num = dt(vsub(fp, cam), pn);
+      if (den != 0.0f) {
+        float lam = num / den;
+        if (lam > 0.0f) {
+          V q = add(cam, scl(dd, lam));
+          V rel = vsub(q, fp);
+          float u = dt(rel, U) / dt(U, U), w = dt(rel, Vv) / dt(Vv, Vv);
+          if (u >= 0.0f && u < 1.0f && w >= 0.0f && w < 1.0f) {
+            uint32_t px = std::min((uint32_t)(u * (float)pv.w), pv.w - 1), py = std::min((uint32_t)(w * (float)pv.h), pv.h - 1);
+            uint64_t local = pid - poff[vi];
+            uint32_t pixel = (uint32_t)(local / vw.spp), sample = (uint32_t)(local % vw.spp);
+            uint64_t ppid = poff[vi] + ((uint64_t)py * pv.w + px) * pv.spp + sample;
+            if (restir_gate(s, sPrev[ppid])) {
+              Mat m = decode(materials, fbi(s.n[3]), view_lod(vw));
+              U4 rr = philox(U4{pixel, sample, 0x20000u, vi}, vw.seedLo, vw.seedHi + vw.frame);
+              restir_merge(c, out, rPrev[ppid], s, m, capM, u01(rr.x));
+            }
+          }
+        }
+      }
+    }
+    rTemp[pid] = out;
+  });
+  // spatial
+  par([&](uint64_t pid, uint32_t) {
+    ResvH out = rTemp[pid];
+    const SurfH &s = sCur[pid];
+    if (s.v[3] > 0.0f && spatialN > 0) {
+      uint32_t vi = view_of(pid);
+      const View &vw = vs[vi];
+      uint64_t local = pid - poff[vi];
+      uint32_t pixel = (uint32_t)(local / vw.spp), sample = (uint32_t)(local % vw.spp);
+      int px = (int)(pixel % vw.w), py = (int)(pixel / vw.w);
+      Mat m = decode(materials, fbi(s.n[3]), view_lod(vw));
+      for (uint32_t k = 0; k < spatialN; ++k) {
+        U4 rr = philox(U4{pixel, sample, 0x30000u + k, vi}, vw.seedLo, vw.seedHi + vw.frame);
+        float rad = radius * std::sqrt(u01(rr.x));
+        float sn, cs;
+        sincos_turns(u01(rr.y), sn, cs);
+        int nx = px + (int)std::floor(rad * cs + 0.5f), ny = py + (int)std::floor(rad * sn + 0.5f);
+        if ((nx == px && ny == py) || nx < 0 || ny < 0 || nx >= (int)vw.w || ny >= (int)vw.h) continue;
+        uint64_t npid = poff[vi] + ((uint64_t)ny * vw.w + nx) * vw.spp + sample;
+        if (!restir_gate(s, sCur[npid])) continue;
+        restir_merge(c, out, rTemp[npid], s, m, capM, u01(rr.z));
+      }
+    }
+    rFin[pid] = out;
+  });
+  // final sample + the rest of each path
+  std::vector<V> pathRad(P);
+  std::vector<std::vector<uint64_t>> st(threads, std::vector<uint64_t>(4, 0));
+  par([&](uint64_t pid, uint32_t tid) {
+    uint32_t vi = view_of(pid);
+    const View &vw = vs[vi];
+    RestirOut ro;
+    const ResvH &r = rFin[pid];
+    const SurfH &s = sCur[pid];
+    int32_t lp = fbi(r.a[3]);
+    if (s.v[3] > 0.0f && lp >= 0 && r.c[2] > 0.0f && r.c[1] > 0.0f && r.c[3] > 0.0f) {
+      Mat m = decode(materials, fbi(s.n[3]), view_lod(vw));
+      V fa, wi;
+      float dist = 0.0f;
+      float ph = restir_target(c, m, s, v(r.a[0], r.a[1], r.a[2]), v(r.b[0], r.b[1], r.b[2]), lp, fa, wi, dist);
+      if (ph > 0.0f) {
+        float W = r.c[1] / (r.c[2] * r.c[3]);
+        ro.valid = true;
+        ro.contrib = scl(fa, W);
+        ro.tmax = dist - RAY_EPS;
+        if (ro.tmax < RAY_EPS) ro.tmax = RAY_EPS;
+        ro.origin = add(v(s.p[0], s.p[1], s.p[2]), scl(v(s.n[0], s.n[1], s.n[2]), 5.0f * RAY_EPS));
+        ro.dir = wi;
+      }
+    }
+    uint64_t local = pid - poff[vi];
+    pathRad[pid] = path(c, vw, vi, (uint32_t)(local / vw.spp), (uint32_t)(local % vw.spp), nullptr, st[tid].data(), &ro);
+  });
+  for (uint32_t vi = 0; vi < nviews; ++vi) {
+    const View &vw = vs[vi];
+    bool cl = (vw.flags & VIEW_CLAMP) != 0;
+    for (uint64_t px = 0; px < (uint64_t)vw.w * vw.h; ++px) {
+      float ax = 0.0f, ay = 0.0f, az = 0.0f;
+      for (uint32_t sIdx = 0; sIdx < vw.spp; ++sIdx) {
+        V r = pathRad[poff[vi] + px * vw.spp + sIdx];
+        if (cl) r = v(c01(r.x), c01(r.y), c01(r.z));
+        ax = ax + r.x;
+        ay = ay + r.y;
+        az = az + r.z;
+      }
+      float ns = (float)vw.spp;
+      ax = ax / ns;
+      ay = ay / ns;
+      az = az / ns;
+      if (cl) {
+        ax = c01(ax);
+        ay = c01(ay);
+        az = c01(az);
+      }
+      float *o = out_rgb + 3 * (xoff[vi] + px);
+      o[0] = ax;
+      o[1] = ay;
+      o[2] = az;
+    }
+  }
+  if (stats)
+    for (auto &x : st)
+      for (int k = 0; k < 4; ++k) stats[k] += x[k];
+  return 0;
 }

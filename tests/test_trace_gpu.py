@@ -34,7 +34,7 @@ def ctx(nb):
     c.close()
 
 
-@pytest.mark.parametrize("kernel", [1, 2])
+@pytest.mark.parametrize("kernel", [1, 2, 3, 4, 5, 6])
 @pytest.mark.parametrize("which", ["ico", "city"])
 def test_closest_parity(nb, orc, ctx, ico_scene, small_city, which, kernel):
     scene, sb = ico_scene if which == "ico" else small_city
@@ -53,10 +53,12 @@ def test_closest_parity(nb, orc, ctx, ico_scene, small_city, which, kernel):
     ctx.set_kernel(1)
 
 
+@pytest.mark.parametrize("kernel", [1, 3, 5])
 @pytest.mark.parametrize("which", ["ico", "city"])
-def test_any_parity(orc, ctx, ico_scene, small_city, which):
+def test_any_parity(orc, ctx, ico_scene, small_city, which, kernel):
     scene, sb = ico_scene if which == "ico" else small_city
     ctx.upload(sb)
+    ctx.set_kernel(kernel)
     rays = _rays(sb, 50)
     # finite tmax: half of each ray's closest distance, so some rays become unoccluded
     ref = orc.OracleScene(sb)
@@ -68,6 +70,7 @@ def test_any_parity(orc, ctx, ico_scene, small_city, which):
         got = ctx.trace_any(rs)
         want = ref.any(rs)
         assert np.array_equal(got, want), f"{(got != want).sum()} any-hit mismatches"
+    ctx.set_kernel(1)
 
 
 def test_work_counters(orc, ctx, small_city):
@@ -93,9 +96,11 @@ def test_object_hit_counters(orc, ctx, small_city):
     assert ctx.object_hits().sum() == 0
 
 
-def test_residency_toggles(orc, ctx, small_city):
+@pytest.mark.parametrize("kernel", [1, 4, 5])
+def test_residency_toggles(orc, ctx, small_city, kernel):
     scene, sb = small_city
     ctx.upload(sb)
+    ctx.set_kernel(kernel)
     rays = _rays(sb, 80)
     rng = np.random.default_rng(9)
     off_objs = np.nonzero(rng.random(sb.object_count) < 0.3)[0]
@@ -123,6 +128,18 @@ def test_residency_toggles(orc, ctx, small_city):
         ctx.set_object_active(o, True)
     ctx.flush()
     _assert_hits_equal(ctx.trace_closest(rays), orc.OracleScene(sb).closest(rays))
+    ctx.set_kernel(1)
+
+
+def test_autotune(nb, orc, ctx, small_city):
+    scene, sb = small_city
+    ctx.upload(sb)
+    rays = _rays(sb, 110)
+    res = ctx.autotune(rays, repeats=2)
+    assert all(v == 0 for v in res["mismatches"].values()), res
+    assert res["ms"][res["best"]] > 0
+    _assert_hits_equal(ctx.trace_closest(rays), orc.OracleScene(sb).closest(rays))
+    ctx.set_kernel(1)
 
 
 def test_device_pointer_path(nb, orc, ctx, small_city):
