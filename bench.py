@@ -195,17 +195,26 @@ def multiview_leg(nb, ctx, frames=3):
     px = int((views["width"].astype(np.int64) * views["height"]).sum())
     paths = int((views["width"].astype(np.int64) * views["height"] * views["spp"]).sum())
     out = torch.empty(px * 3, dtype=torch.float32, device="cuda")
-    ctx.render_dev(views, out.data_ptr())
-    ctx.sync()
-    ctx.reset_render_stats()
-    t0 = time.perf_counter()
-    for f in range(frames):
-        views["frame"] = f
-        ctx.render_dev(views, out.data_ptr())
-    ctx.sync()
-    dt = (time.perf_counter() - t0) / frames
-    st = ctx.render_stats() / frames
+    timings = {}
+    for mode in ("direct", "graph"):
+        graph = mode == "graph"
+        ctx.render_dev(views, out.data_ptr(), graph=graph)  # warm-up (captures the graph)
+        ctx.sync()
+        g0 = ctx.frame_graph_stats()
+        ctx.reset_render_stats()
+        t0 = time.perf_counter()
+        for f in range(frames):
+            views["frame"] = f
+            ctx.render_dev(views, out.data_ptr(), graph=graph)
+        ctx.sync()
+        timings[mode] = (time.perf_counter() - t0) / frames
+        st = ctx.render_stats() / frames
+        g1 = ctx.frame_graph_stats()
+    dt = timings["graph"]
     return {"views": int(views.shape[0]), "pixels": px, "paths": paths, "ms_per_frame": dt * 1e3,
+            "ms_per_frame_direct_launches": timings["direct"] * 1e3,
+            "graph_replays_timed": g1["launches"] - g0["launches"],
+            "graph_captures_timed": g1["captures"] - g0["captures"],
             "mpaths_per_s": paths / dt / 1e6, "mrays_per_s_incl_shadow": (st[0] + st[2]) / dt / 1e6}
 
 
@@ -376,13 +385,22 @@ def main():
     bytes_b = alg_bytes(d_b, n_b)
     del d_w
 
-    # Autotune the traversal variant on a sample of this frame's rays (1M primary + 1M bounce).
+    # Autotune the traversal configuration on a sample of this frame's rays (1M primary + 1M
+    # bounce): width x short stack x regroup threshold x staged top levels x block, each checked
+    # bit for bit against the binary kernel.
     tune = None
     if args.kernel == 0:
         sample = torch.cat([d_prim[:1_000_000], d_b[:1_000_000]]).contiguous()
         torch.cuda.synchronize()
-        tune = ctx.autotune((sample.data_ptr(), sample.shape[0]), repeats=3, device=True)
+        sweep = ctx.autotune_sweep((sample.data_ptr(), sample.shape[0]), repeats=2, device=True)
         del sample
+        rows = sorted((e for e in sweep["entries"] if e[2] >= 0), key=lambda e: e[2])
+        tune = {"best": sweep["best_name"], "best_cfg": sweep["best"], "configs": len(sweep["entries"]),
+                "mismatching_configs": sum(1 for e in sweep["entries"] if e[3]),
+                "sample_rays": 2_000_000,
+                "fastest_ms": [[e[0], round(e[2], 4)] for e in rows[:10]],
+                "local_stack_ms": {e[0]: round(e[2], 4) for e in sweep["entries"] if e[1]["short_stack"] == 0},
+                "slowest_ms": [[e[0], round(e[2], 4)] for e in rows[-3:]]}
         log(f"autotune: {tune}")
 
     def step():

@@ -141,6 +141,45 @@ nomad_status nomad_autotune(nomad_ctx *ctx, const nomad_ray *rays, uint64_t n, u
 /* Chooses the traversal variant used by the trace calls (NOMAD_KERNEL_*). */
 nomad_status nomad_set_kernel(nomad_ctx *ctx, uint32_t kernel);
 
+/* Full traversal configuration (no counterpart in the reference, which has one kernel). The
+ * NOMAD_KERNEL_* variants are the configurations with short_stack = 0. With short_stack > 0 the
+ * kernel runs persistent warps that
+ *   - keep the top `short_stack` entries of each ray's traversal stack in shared memory and
+ *     spill older entries to local memory (exact for any depth the scene needs);
+ *   - refill idle lanes with new rays from a per-warp pool whenever fewer than `regroup` of the
+ *     warp's 32 lanes are still traversing (1: only when the whole warp is idle; 32: as soon as
+ *     one lane is idle);
+ *   - copy the first `staged_nodes` nodes of the layout (the TLAS top levels, numbered
+ *     breadth-first) into shared memory with one bulk asynchronous copy per block and read
+ *     them from there.
+ * Every configuration returns the same hits bit for bit. */
+typedef struct nomad_traversal {
+  uint32_t width;         /* 2 (pair nodes), 4 or 8                                            */
+  uint32_t persistent;    /* 0: one ray per thread; 1: persistent warps                        */
+  uint32_t short_stack;   /* 0, or 8 / 16 / 32 shared-memory entries per ray (persistent only) */
+  uint32_t regroup;       /* 1..32, refill threshold in busy lanes (short_stack > 0)           */
+  uint32_t staged_nodes;  /* top-level nodes staged in shared memory (short_stack > 0)         */
+  uint32_t block;         /* threads per block: 0 (default 128), 64, 128, 256                  */
+} nomad_traversal;
+nomad_status nomad_set_traversal(nomad_ctx *ctx, const nomad_traversal *cfg);
+nomad_status nomad_get_traversal(nomad_ctx *ctx, nomad_traversal *cfg);
+/* Nodes of the TLAS prefix of each layout (widths 2, 4, 8): the most that staging can use. */
+nomad_status nomad_tlas_nodes(nomad_ctx *ctx, uint32_t out[3]);
+
+/* One autotuner measurement. */
+typedef struct nomad_tune_entry {
+  nomad_traversal cfg;
+  float ms;               /* best of `repeats` timings; negative when not run                  */
+  uint32_t mismatches;    /* sample rays whose hit differs from the binary per-thread kernel's */
+} nomad_tune_entry;
+/* Sweeps width {2,4,8} x short stack {0 (local), 8, 16, 32} x regroup threshold {1, 16, 24, 32}
+ * x staged top levels {0, up to 32 KB} x block {128, 256} on n sample rays, checks every
+ * configuration against the binary kernel bit for bit, and selects the fastest one that agrees.
+ * Fills up to `capacity` entries; *count receives the number of configurations measured. */
+nomad_status nomad_autotune_sweep(nomad_ctx *ctx, const nomad_ray *rays, uint64_t n, uint32_t repeats,
+                                  uint32_t flags, nomad_tune_entry *entries, uint32_t capacity,
+                                  uint32_t *count, nomad_traversal *best);
+
 /* Work counters of a near-first binary traversal over the SceneBVH arrays, per ray:
  * out[4*i+0] nodes whose box was tested (TLAS + BLAS), [1] primitive tests, [2] instance
  * records read, [3] 1 when the ray hit. Defines the algorithmic bytes per ray:
@@ -191,9 +230,18 @@ nomad_status nomad_view_pinhole(const float position[3], const float look_at[3],
 /* Renders every view in one batched wavefront launch sequence (paths of all views share the
  * ray queues). radiance_out receives RGB floats per pixel, views concatenated
  * (sum of width*height*3 floats); host memory unless NOMAD_TRACE_DEVICE_POINTERS. With
- * NOMAD_TRACE_COUNT_HITS the per-object counters also count the closest hits of every bounce. */
+ * NOMAD_TRACE_COUNT_HITS the per-object counters also count the closest hits of every bounce.
+ * The frame's launches (raygen, per bounce closest hit, ReSTIR, shading, shadow any-hit,
+ * resolve, average) are captured once per frame shape as a CUDA graph and replayed: a shape is
+ * the view count, sizes and depths, the output buffer, the traversal configuration, the
+ * scene's device arrays and the ReSTIR state. Cameras, seeds and frame numbers are read from
+ * the device view table, so they change freely between replays. NOMAD_RENDER_DIRECT launches
+ * the same sequence without a graph. */
+enum { NOMAD_RENDER_DIRECT = 1u << 2 };
 nomad_status nomad_render_frame(nomad_ctx *ctx, const nomad_view *views, uint32_t nviews,
                                 float *radiance_out, uint32_t flags);
+/* out[0] frame graphs captured, [1] graph launches, [2] graphs cached now (at most 8). */
+nomad_status nomad_frame_graph_stats(nomad_ctx *ctx, uint64_t out[3]);
 
 /* ReSTIR DI at the first bounce of views flagged NOMAD_VIEW_RESTIR (replaces the reference's
  * inline reservoir block, PathTracing.h:1363-1742, by separate passes over FP32 reservoirs kept
@@ -248,8 +296,11 @@ typedef struct nomad_residency_params {
  * policy, selects the resident set greedily by score under budget_bytes (visible objects first
  * up to the visibility reserve, ties to the lower object index), and patches the TLAS so
  * non-resident objects are skipped (blas_root_index = -1). The light CDF follows the resident
- * set. *toggled receives the number of objects whose residency changed. Object geometry bytes =
- * 32 per BLAS node + 196 per primitive (packed primitive, material and index). */
+ * set. *toggled receives the number of objects whose residency changed; the call then waits for
+ * the step. With toggled = NULL the step is queued on the context's stream without any host
+ * synchronisation (the host-side residency state is refreshed when a residency call next reads
+ * it). Object geometry bytes = 32 per BLAS node + 196 per primitive (packed primitive, material
+ * and index). */
 nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residency_params *params,
                                   const nomad_view *camera, uint32_t *toggled);
 /* Per-object geometry bytes (object_count uint64). */

@@ -596,9 +596,25 @@ extern "C" nomad_status nomad_view_pinhole(const float pos[3], const float look[
 }
 
 namespace {
-struct RestirArgs;
-nomad_status restir_pass(nomad_ctx *ctx, uint32_t nviews, const nomad_view *views, unsigned long long P,
-                         const Lights &L, Counters *C);
+// ReSTIR state of one frame, fixed on the host before its kernels are launched or captured.
+struct RestirPlan {
+  bool on = false;
+  int cur = 0;           // reservoir / surface buffers written this frame
+  int temporal = 0;      // 1 when the previous frame's reservoirs are reused
+  nomad_restir_config cfg{};
+};
+nomad_status restir_prepare(nomad_ctx *ctx, uint32_t nviews, const nomad_view *views, unsigned long long P,
+                            RestirPlan &plan);
+nomad_status restir_launch(nomad_ctx *ctx, uint32_t nviews, unsigned long long P, const Lights &L, Counters *C,
+                           const RestirPlan &plan);
+void restir_commit(nomad_ctx *ctx, uint32_t nviews, const nomad_view *views);
+
+template <typename T>
+void key_put(std::vector<unsigned char> &k, const T &v) {
+  unsigned char b[sizeof(T)];
+  std::memcpy(b, (const void *)&v, sizeof(T));
+  k.insert(k.end(), b, b + sizeof(T));
+}
 }  // namespace
 
 extern "C" nomad_status nomad_render_frame(nomad_ctx *ctx, const nomad_view *views, uint32_t nviews,
@@ -671,37 +687,14 @@ extern "C" nomad_status nomad_render_frame(nomad_ctx *ctx, const nomad_view *vie
 
   const ViewDev *V = F.views.as<const ViewDev>();
   Counters *C = F.counters.as<Counters>();
-  int gridPT = ctx->smCount * 8;
-  k_raygen<<<gridPT, kPtBlock, 0, s>>>(V, nviews, P, F.qRays[0].as<float4>(), F.qIds[0].as<uint32_t>(),
-                                      F.thr.as<float4>(), F.rad.as<float4>(), C);
-  NOMAD_CUDA(ctx, cudaGetLastError());
   Lights L{F.lightIdx.as<const uint32_t>(), F.lightCdf.as<const float>(), F.lightMeta.as<const LightMeta>()};
   uint32_t *objHits = (flags & NOMAD_TRACE_COUNT_HITS) ? ctx->objHits.as<uint32_t>() : nullptr;
   bool anyRestir = false;
   for (uint32_t i = 0; i < nviews; ++i) anyRestir |= (views[i].flags & NOMAD_VIEW_RESTIR) != 0;
-  int cur = 0;
-  for (uint32_t depth = 0; depth < maxDepth; ++depth) {
-    k_bounce_reset<<<1, 1, 0, s>>>(C, cur);
-    st = nomad_trace_variant(ctx, ctx->kernel, false, F.qRays[cur].as<const float4>(), P, &C->qlen[cur], &C->cursor[0],
-                             F.hits.as<int32_t>(), nullptr, nullptr, s);
+  RestirPlan plan;
+  if (anyRestir) {
+    st = restir_prepare(ctx, nviews, views, P, plan);
     if (st != NOMAD_OK) return st;
-    if (depth == 0 && anyRestir) {
-      st = restir_pass(ctx, nviews, views, P, L, C);
-      if (st != NOMAD_OK) return st;
-    }
-    k_shade<<<gridPT, kPtBlock, 0, s>>>(depth, V, nviews, F.qRays[cur].as<const float4>(), F.qIds[cur].as<const uint32_t>(),
-                                       F.hits.as<const int32_t>(), F.qRays[cur ^ 1].as<float4>(),
-                                       F.qIds[cur ^ 1].as<uint32_t>(), F.sRays.as<float4>(), F.sIds.as<uint32_t>(),
-                                       F.sContrib.as<float4>(), F.thr.as<float4>(), F.rad.as<float4>(),
-                                       ctx->prims.as<const float4>(), ctx->materials.as<const float4>(), L, C, cur,
-                                       objHits, anyRestir ? 1 : 0);
-    st = nomad_trace_variant(ctx, ctx->kernel, true, F.sRays.as<const float4>(), P, &C->qlen[2], &C->cursor[1],
-                             nullptr, F.sOcc.as<uint8_t>(), nullptr, s);
-    if (st != NOMAD_OK) return st;
-    k_resolve<<<gridPT, kPtBlock, 0, s>>>(F.sIds.as<const uint32_t>(), F.sContrib.as<const float4>(),
-                                         F.sOcc.as<const uint8_t>(), F.rad.as<float4>(), C);
-    NOMAD_CUDA(ctx, cudaGetLastError());
-    cur ^= 1;
   }
   float *dOut = out;
   bool hostOut = !(flags & NOMAD_TRACE_DEVICE_POINTERS);
@@ -709,12 +702,122 @@ extern "C" nomad_status nomad_render_frame(nomad_ctx *ctx, const nomad_view *vie
     NOMAD_CUDA(ctx, ctx->stageAux.reserve(pixels * 12));
     dOut = ctx->stageAux.as<float>();
   }
-  k_finalize<<<gridPT, kPtBlock, 0, s>>>(V, nviews, pixels, F.rad.as<const float4>(), dOut);
-  NOMAD_CUDA(ctx, cudaGetLastError());
+
+  // The frame's device work: raygen, then per bounce closest hit, (ReSTIR at the first bounce),
+  // shading, shadow any-hit and resolve, then the per-pixel average. Queue lengths stay on the
+  // device, so the sequence needs no host synchronisation and can be captured as a graph.
+  auto body = [&]() -> nomad_status {
+    const int gridPT = ctx->smCount * 8;
+    k_raygen<<<gridPT, kPtBlock, 0, s>>>(V, nviews, P, F.qRays[0].as<float4>(), F.qIds[0].as<uint32_t>(),
+                                        F.thr.as<float4>(), F.rad.as<float4>(), C);
+    NOMAD_CUDA(ctx, cudaGetLastError());
+    int cur = 0;
+    for (uint32_t depth = 0; depth < maxDepth; ++depth) {
+      k_bounce_reset<<<1, 1, 0, s>>>(C, cur);
+      nomad_status rs = nomad_trace_variant(ctx, ctx->trav, false, F.qRays[cur].as<const float4>(), P, &C->qlen[cur],
+                                            &C->cursor[0], F.hits.as<int32_t>(), nullptr, nullptr, s);
+      if (rs != NOMAD_OK) return rs;
+      if (depth == 0 && plan.on) {
+        rs = restir_launch(ctx, nviews, P, L, C, plan);
+        if (rs != NOMAD_OK) return rs;
+      }
+      k_shade<<<gridPT, kPtBlock, 0, s>>>(depth, V, nviews, F.qRays[cur].as<const float4>(),
+                                         F.qIds[cur].as<const uint32_t>(), F.hits.as<const int32_t>(),
+                                         F.qRays[cur ^ 1].as<float4>(), F.qIds[cur ^ 1].as<uint32_t>(),
+                                         F.sRays.as<float4>(), F.sIds.as<uint32_t>(), F.sContrib.as<float4>(),
+                                         F.thr.as<float4>(), F.rad.as<float4>(), ctx->prims.as<const float4>(),
+                                         ctx->materials.as<const float4>(), L, C, cur, objHits, plan.on ? 1 : 0);
+      rs = nomad_trace_variant(ctx, ctx->trav, true, F.sRays.as<const float4>(), P, &C->qlen[2], &C->cursor[1],
+                               nullptr, F.sOcc.as<uint8_t>(), nullptr, s);
+      if (rs != NOMAD_OK) return rs;
+      k_resolve<<<gridPT, kPtBlock, 0, s>>>(F.sIds.as<const uint32_t>(), F.sContrib.as<const float4>(),
+                                           F.sOcc.as<const uint8_t>(), F.rad.as<float4>(), C);
+      NOMAD_CUDA(ctx, cudaGetLastError());
+      cur ^= 1;
+    }
+    k_finalize<<<gridPT, kPtBlock, 0, s>>>(V, nviews, pixels, F.rad.as<const float4>(), dOut);
+    NOMAD_CUDA(ctx, cudaGetLastError());
+    return NOMAD_OK;
+  };
+
+  if (flags & NOMAD_RENDER_DIRECT) {
+    st = body();
+    if (st != NOMAD_OK) return st;
+  } else {
+    // Everything the captured launches bake in: sizes, buffer addresses, kernel parameters.
+    std::vector<unsigned char> key;
+    key_put(key, nviews);
+    key_put(key, P);
+    key_put(key, pixels);
+    key_put(key, maxDepth);
+    key_put(key, objHits);
+    key_put(key, dOut);
+    key_put(key, ctx->trav);
+    key_put(key, ctx->scene);
+    for (const WideScene &w : ctx->ws) {
+      key_put(key, w.wn);
+      key_put(key, w.root);
+    }
+    key_put(key, ctx->smCount);
+    key_put(key, ctx->prims.p);
+    key_put(key, ctx->materials.p);
+    for (const DeviceBuf *b : {&F.thr, &F.rad, &F.qRays[0], &F.qRays[1], &F.qIds[0], &F.qIds[1], &F.hits, &F.sRays,
+                               &F.sIds, &F.sContrib, &F.sOcc, &F.counters, &F.views, &F.lightIdx, &F.lightCdf,
+                               &F.lightMeta, &F.rInit, &F.rTemp, &F.resv[0], &F.resv[1], &F.surf[0], &F.surf[1],
+                               &F.prevViews})
+      key_put(key, b->p);
+    key_put(key, plan.on);
+    key_put(key, plan.cur);
+    key_put(key, plan.temporal);
+    key_put(key, plan.cfg);
+    FrameState::Graph *g = nullptr;
+    for (FrameState::Graph &c : F.graphs)
+      if (c.key == key) g = &c;
+    if (!g) {
+      constexpr size_t kMaxGraphs = 8;
+      if (F.graphs.size() >= kMaxGraphs) {
+        auto old = std::min_element(F.graphs.begin(), F.graphs.end(),
+                                    [](const FrameState::Graph &a, const FrameState::Graph &b) { return a.lastUse < b.lastUse; });
+        if (old->exec) cudaGraphExecDestroy(old->exec);
+        if (old->graph) cudaGraphDestroy(old->graph);
+        F.graphs.erase(old);
+      }
+      FrameState::Graph ng;
+      ng.key = std::move(key);
+      NOMAD_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      nomad_status cst = body();
+      cudaError_t ce = cudaStreamEndCapture(s, &ng.graph);
+      if (cst != NOMAD_OK) {
+        if (ng.graph) cudaGraphDestroy(ng.graph);
+        return cst;
+      }
+      if (ce != cudaSuccess) return nomad_cuda_fail(ctx, ce, "frame capture");
+      ce = cudaGraphInstantiate(&ng.exec, ng.graph, 0);
+      if (ce != cudaSuccess) {
+        cudaGraphDestroy(ng.graph);
+        return nomad_cuda_fail(ctx, ce, "frame graph instantiate");
+      }
+      ++F.graphCaptures;
+      F.graphs.push_back(std::move(ng));
+      g = &F.graphs.back();
+    }
+    g->lastUse = ++F.graphTick;
+    NOMAD_CUDA(ctx, cudaGraphLaunch(g->exec, s));
+    ++F.graphLaunches;
+  }
+  if (plan.on) restir_commit(ctx, nviews, views);
   if (hostOut) {
     NOMAD_CUDA(ctx, cudaMemcpyAsync(out, dOut, pixels * 12, cudaMemcpyDeviceToHost, s));
     NOMAD_CUDA(ctx, cudaStreamSynchronize(s));
   }
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_frame_graph_stats(nomad_ctx *ctx, uint64_t out[3]) {
+  if (!ctx || !out) return NOMAD_ERR_INVALID_ARGUMENT;
+  out[0] = ctx->frame.graphCaptures;
+  out[1] = ctx->frame.graphLaunches;
+  out[2] = ctx->frame.graphs.size();
   return NOMAD_OK;
 }
 
@@ -1011,10 +1114,9 @@ __global__ void __launch_bounds__(kPtBlock) k_restir_shade(
   }
 }
 
-nomad_status restir_pass(nomad_ctx *ctx, uint32_t nviews, const nomad_view *views, unsigned long long P,
-                         const Lights &L, Counters *C) {
+nomad_status restir_prepare(nomad_ctx *ctx, uint32_t nviews, const nomad_view *views, unsigned long long P,
+                            RestirPlan &plan) {
   FrameState &F = ctx->frame;
-  cudaStream_t s = ctx->stream;
   if (F.restirPaths < P) {
     NOMAD_CUDA(ctx, F.rInit.reserve(P * sizeof(Resv)));
     NOMAD_CUDA(ctx, F.rTemp.reserve(P * sizeof(Resv)));
@@ -1031,11 +1133,22 @@ nomad_status restir_pass(nomad_ctx *ctx, uint32_t nviews, const nomad_view *view
     const nomad_view &a = views[i], &b = F.prevHostViews[i];
     compatible = a.width == b.width && a.height == b.height && a.spp == b.spp;
   }
-  const nomad_restir_config &cf = F.restir;
+  plan.on = true;
+  plan.cur = F.restirCur;
+  plan.cfg = F.restir;
+  plan.temporal = (compatible && F.restir.temporal) ? 1 : 0;
+  return NOMAD_OK;
+}
+
+nomad_status restir_launch(nomad_ctx *ctx, uint32_t nviews, unsigned long long P, const Lights &L, Counters *C,
+                           const RestirPlan &plan) {
+  FrameState &F = ctx->frame;
+  cudaStream_t s = ctx->stream;
+  const nomad_restir_config &cf = plan.cfg;
   RestirDev cfg{cf.candidates, cf.temporal, cf.spatial, cf.radius_px, cf.m_cap};
   const ViewDev *V = F.views.as<const ViewDev>();
-  int cur = F.restirCur;
-  int grid = ctx->smCount * 8;
+  const int cur = plan.cur;
+  const int grid = ctx->smCount * 8;
   Surf *sCur = F.surf[cur].as<Surf>();
   k_restir_initial<<<grid, kPtBlock, 0, s>>>(V, nviews, P, cfg, F.qRays[0].as<const float4>(), F.hits.as<const int32_t>(),
                                             ctx->prims.as<const float4>(), ctx->materials.as<const float4>(), L,
@@ -1043,17 +1156,21 @@ nomad_status restir_pass(nomad_ctx *ctx, uint32_t nviews, const nomad_view *view
   k_restir_temporal<<<grid, kPtBlock, 0, s>>>(V, F.prevViews.as<const ViewDev>(), nviews, P, cfg,
                                              ctx->materials.as<const float4>(), F.rInit.as<const Resv>(), sCur,
                                              F.resv[cur ^ 1].as<const Resv>(), F.surf[cur ^ 1].as<const Surf>(),
-                                             F.rTemp.as<Resv>(), (compatible && cf.temporal) ? 1 : 0);
+                                             F.rTemp.as<Resv>(), plan.temporal);
   k_restir_spatial<<<grid, kPtBlock, 0, s>>>(V, nviews, P, cfg, ctx->materials.as<const float4>(),
                                             F.rTemp.as<const Resv>(), sCur, F.resv[cur].as<Resv>());
   k_restir_shade<<<grid, kPtBlock, 0, s>>>(V, nviews, P, ctx->materials.as<const float4>(), F.resv[cur].as<const Resv>(),
                                           sCur, F.sRays.as<float4>(), F.sIds.as<uint32_t>(), F.sContrib.as<float4>(), C);
   NOMAD_CUDA(ctx, cudaGetLastError());
   NOMAD_CUDA(ctx, cudaMemcpyAsync(F.prevViews.p, F.views.p, nviews * sizeof(ViewDev), cudaMemcpyDeviceToDevice, s));
+  return NOMAD_OK;
+}
+
+void restir_commit(nomad_ctx *ctx, uint32_t nviews, const nomad_view *views) {
+  FrameState &F = ctx->frame;
   F.prevHostViews.assign(views, views + nviews);
   F.restirCur ^= 1;
   F.restirValid = true;
-  return NOMAD_OK;
 }
 
 }  // namespace

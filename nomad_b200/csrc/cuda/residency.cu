@@ -448,7 +448,26 @@ extern "C" nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residen
   nomad_status st = nomad_lights_update(ctx);
   if (st != NOMAD_OK) return st;
   ++R.frame;
-  // wide layouts follow the device flags (their root refs are fixed below with the host mirror)
+  ctx->frame.restirValid = false;
+  if (!toggled && ctx->layout.tlasPairCount > 0) {
+    // Asynchronous step: the wide layouts follow the device flags on the stream, the host mirror
+    // is refreshed from a pinned copy when a host call needs it. (Without a TLAS the root ref
+    // itself changes and is set on the host: the synchronous path below.)
+    if (ctx->resPinnedBytes < N) {
+      if (ctx->resPinned) cudaFreeHost(ctx->resPinned);
+      ctx->resPinned = nullptr;
+      ctx->resPinnedBytes = 0;
+      NOMAD_CUDA(ctx, cudaMallocHost(&ctx->resPinned, N));
+      ctx->resPinnedBytes = N;
+    }
+    if (!ctx->resEvent) NOMAD_CUDA(ctx, cudaEventCreateWithFlags(&ctx->resEvent, cudaEventDisableTiming));
+    st = nomad_patch_wide(ctx);
+    if (st != NOMAD_OK) return st;
+    NOMAD_CUDA(ctx, cudaMemcpyAsync(ctx->resPinned, R.objRes.p, N, cudaMemcpyDeviceToHost, s));
+    NOMAD_CUDA(ctx, cudaEventRecord(ctx->resEvent, s));
+    ctx->resHostStale = true;
+    return NOMAD_OK;
+  }
   // host mirror of the object residency
   uint32_t misc[3];
   NOMAD_CUDA(ctx, cudaMemcpyAsync(misc, R.misc.p, 12, cudaMemcpyDeviceToHost, s));
@@ -462,8 +481,19 @@ extern "C" nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residen
     ctx->instances[o].blas_root_index = ctx->objResident[o] ? ctx->layout.objRootNode[o] : -1;
   st = nomad_patch_wide(ctx);
   if (st != NOMAD_OK) return st;
-  ctx->frame.restirValid = false;
+  ctx->resHostStale = false;
   if (toggled) *toggled = misc[0];
+  return NOMAD_OK;
+}
+
+nomad_status nomad_residency_sync_host(nomad_ctx *ctx) {
+  if (!ctx->resHostStale) return NOMAD_OK;
+  NOMAD_CUDA(ctx, cudaEventSynchronize(ctx->resEvent));
+  ctx->resHostStale = false;
+  const uint32_t N = ctx->objectCount;
+  std::memcpy(ctx->objResident.data(), ctx->resPinned, N);
+  for (uint32_t o = 0; o < N; ++o)
+    ctx->instances[o].blas_root_index = ctx->objResident[o] ? ctx->layout.objRootNode[o] : -1;
   return NOMAD_OK;
 }
 
@@ -490,6 +520,8 @@ extern "C" nomad_status nomad_residency_last(nomad_ctx *ctx, float *features, fl
 extern "C" nomad_status nomad_residency_flags(nomad_ctx *ctx, uint8_t *out) {
   if (!ctx || !out) return NOMAD_ERR_INVALID_ARGUMENT;
   if (!ctx->sceneReady) return nomad_fail(ctx, NOMAD_ERR_NOT_READY, "no scene uploaded");
+  nomad_status st = nomad_residency_sync_host(ctx);
+  if (st != NOMAD_OK) return st;
   std::memcpy(out, ctx->objResident.data(), ctx->objectCount);
   return NOMAD_OK;
 }

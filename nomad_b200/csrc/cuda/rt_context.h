@@ -58,6 +58,26 @@ struct FrameState {
   bool restirValid = false;
   nomad_restir_config restir{32, 1, 3, 30.0f, 20.0f};
   std::vector<nomad_view> prevHostViews;
+  // Captured frames: one CUDA graph per frame shape (sizes, buffers, traversal configuration,
+  // scene parameters); the view table is read from device memory, so cameras, seeds and frame
+  // numbers change without a new capture.
+  struct Graph {
+    std::vector<unsigned char> key;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t lastUse = 0;
+  };
+  std::vector<Graph> graphs;
+  uint64_t graphTick = 0;
+  uint64_t graphCaptures = 0, graphLaunches = 0;
+  void clearGraphs() {
+    for (Graph &g : graphs) {
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+      if (g.graph) cudaGraphDestroy(g.graph);
+    }
+    graphs.clear();
+  }
+  ~FrameState() { clearGraphs(); }
 };
 
 struct nomad_ctx {
@@ -67,7 +87,7 @@ struct nomad_ctx {
   cudaStream_t ownStream = nullptr;
   cudaStream_t copyStreams[2] = {nullptr, nullptr};
   std::string err;
-  uint32_t kernel = NOMAD_KERNEL_BVH2;
+  nomad_traversal trav{2, 0, 0, 1, 0, 128};  // kernel configuration of the trace calls
   bool sceneReady = false;
   // scene sizes
   uint32_t primCount = 0, objectCount = 0;
@@ -112,7 +132,20 @@ struct nomad_ctx {
     std::vector<uint64_t> hostBytes;
   } res;
   void *mlp = nullptr;  // MlpState (mlp.cu)
+  // Host mirror of the device residency flags after a device step: copied asynchronously into
+  // pinned memory and applied to objResident / instances when a host call next needs them.
+  bool resHostStale = false;
+  uint8_t *resPinned = nullptr;
+  size_t resPinnedBytes = 0;
+  cudaEvent_t resEvent = nullptr;
+  ~nomad_ctx() {
+    if (resEvent) cudaEventDestroy(resEvent);
+    if (resPinned) cudaFreeHost(resPinned);
+  }
 };
+
+// Applies a pending device residency step to the host mirror (waits for its flag copy).
+nomad_status nomad_residency_sync_host(nomad_ctx *ctx);
 
 void nomad_mlp_free(void *p);
 nomad_status nomad_mlp_infer_device(nomad_ctx *ctx, const float *X, uint64_t n, float *y);
@@ -123,11 +156,21 @@ nomad_status nomad_residency_mirror(nomad_ctx *ctx);
 nomad_status nomad_lights_update(nomad_ctx *ctx);
 // Rewrites every object's instance slot in the wide layouts from the device residency flags.
 nomad_status nomad_patch_wide(nomad_ctx *ctx);
-// Launches a closest- or any-hit trace of n device rays with the context's chosen variant
+// Launches a closest- or any-hit trace of n device rays with traversal configuration `cfg`
 // (queue length read from the device when lenDev is set).
-nomad_status nomad_trace_variant(nomad_ctx *ctx, uint32_t kernel, bool any, const float4 *rays, uint64_t n,
+nomad_status nomad_trace_variant(nomad_ctx *ctx, const nomad_traversal &cfg, bool any, const float4 *rays, uint64_t n,
                                  const uint32_t *lenDev, unsigned long long *cursor, int32_t *hits5,
                                  uint8_t *occ, uint32_t *counts, cudaStream_t st);
+// The short-stack persistent kernels (trace_regroup.cu).
+nomad_status nomad_trace_regroup(nomad_ctx *ctx, const nomad_traversal &cfg, bool any, const float4 *rays, uint64_t n,
+                                 const uint32_t *lenDev, unsigned long long *cursor, int32_t *hits5, uint8_t *occ,
+                                 uint32_t *counts, cudaStream_t s);
+// Opts the short-stack kernels in to large dynamic shared memory (once per context creation).
+cudaError_t nomad_regroup_init();
+// NOMAD_KERNEL_* as a traversal configuration.
+nomad_traversal nomad_kernel_config(uint32_t kernel);
+// Whether `cfg` is valid and can run on the uploaded scene (stack depth, layout sizes).
+bool nomad_traversal_ok(const nomad_ctx *ctx, const nomad_traversal &cfg, std::string *why);
 
 inline nomad_status nomad_fail(nomad_ctx *c, nomad_status st, const std::string &msg) {
   if (c) c->err = msg;

@@ -163,6 +163,7 @@ extern "C" nomad_status nomad_create(const nomad_config *cfg, nomad_ctx **out) {
   if (cudaGetDeviceProperties(&prop, c->device) != cudaSuccess) return NOMAD_ERR_CUDA;
   if (prop.major < 10) return NOMAD_ERR_UNSUPPORTED;  // built for sm_100a only
   c->smCount = prop.multiProcessorCount;
+  if (nomad_regroup_init() != cudaSuccess) return NOMAD_ERR_CUDA;
   if (cudaStreamCreateWithFlags(&c->ownStream, cudaStreamNonBlocking) != cudaSuccess)
     return NOMAD_ERR_CUDA;
   c->stream = c->ownStream;
@@ -221,7 +222,13 @@ extern "C" nomad_status nomad_scene_upload(nomad_ctx *ctx, const float *bvh, uin
   if (!bvh || !tlas || !prims || !materials || !primIndices || !inst)
     return fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "null scene array");
   NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (ctx->resHostStale) {  // a pending flag copy must land before the pinned buffer is reused
+    NOMAD_CUDA(ctx, cudaEventSynchronize(ctx->resEvent));
+    ctx->resHostStale = false;
+  }
   ctx->sceneReady = false;
+  // Leaf refs are ~first record; the values just above INT32_MIN are kernel sentinels.
+  if (primCount > 0x7ffffff0u) return fail(ctx, NOMAD_ERR_LIMIT, "too many primitives");
   std::vector<nomad::ObjectRange> objs(objectCount);
   for (uint32_t o = 0; o < objectCount; ++o)
     objs[o] = {inst[o].blas_root_index, inst[o].primitive_base, inst[o].primitive_count};
@@ -308,12 +315,18 @@ extern "C" nomad_status nomad_scene_upload(nomad_ctx *ctx, const float *bvh, uin
   nomad_status rst = nomad_residency_init(ctx);
   if (rst != NOMAD_OK) return rst;
   ctx->sceneReady = true;
+  // A configuration chosen for another scene may need a deeper stack or more nodes than this one has.
+  if (!nomad_traversal_ok(ctx, ctx->trav, nullptr)) ctx->trav = nomad_kernel_config(NOMAD_KERNEL_BVH2);
   return NOMAD_OK;
 }
 
 extern "C" nomad_status nomad_residency_set_primitive_active(nomad_ctx *ctx, uint32_t prim,
                                                              int32_t active, int32_t *changed) {
   if (!ctx || !ctx->sceneReady) return NOMAD_ERR_NOT_READY;
+  {
+    nomad_status hs = nomad_residency_sync_host(ctx);
+    if (hs != NOMAD_OK) return hs;
+  }
   if (changed) *changed = 0;
   if (prim >= ctx->primCount) return fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "primitive out of range");
   uint8_t a = active ? 1 : 0;
@@ -339,6 +352,10 @@ extern "C" nomad_status nomad_residency_set_primitive_active(nomad_ctx *ctx, uin
 extern "C" nomad_status nomad_residency_set_object_active(nomad_ctx *ctx, uint32_t obj,
                                                           int32_t active, uint32_t *toggled) {
   if (!ctx || !ctx->sceneReady) return NOMAD_ERR_NOT_READY;
+  {
+    nomad_status hs = nomad_residency_sync_host(ctx);
+    if (hs != NOMAD_OK) return hs;
+  }
   if (toggled) *toggled = 0;
   if (obj >= ctx->objectCount) return fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "object out of range");
   const nomad_instance_record &r = ctx->instances[obj];
@@ -359,6 +376,10 @@ extern "C" nomad_status nomad_residency_set_object_active(nomad_ctx *ctx, uint32
 
 extern "C" nomad_status nomad_residency_flush(nomad_ctx *ctx) {
   if (!ctx || !ctx->sceneReady) return NOMAD_ERR_NOT_READY;
+  {
+    nomad_status hs = nomad_residency_sync_host(ctx);
+    if (hs != NOMAD_OK) return hs;
+  }
   std::vector<int64_t> offs;
   std::vector<int32_t> vals;
   const auto &L = ctx->layout;
@@ -412,6 +433,10 @@ extern "C" nomad_status nomad_residency_flush(nomad_ctx *ctx) {
 
 extern "C" nomad_status nomad_residency_get_instances(nomad_ctx *ctx, nomad_instance_record *out) {
   if (!ctx || !ctx->sceneReady) return NOMAD_ERR_NOT_READY;
+  {
+    nomad_status hs = nomad_residency_sync_host(ctx);
+    if (hs != NOMAD_OK) return hs;
+  }
   if (!out) return NOMAD_ERR_INVALID_ARGUMENT;
   for (uint32_t o = 0; o < ctx->objectCount; ++o) {
     out[o] = ctx->instances[o];
@@ -424,18 +449,6 @@ namespace {
 
 // Stack entries of each variant: pair nodes 64; 4-wide 64; 8-wide 96.
 constexpr int kStackW4 = 64, kStackW8 = 96;
-
-bool variant_ok(const nomad_ctx *ctx, uint32_t k) {
-  switch (k) {
-    case NOMAD_KERNEL_BVH2:
-    case NOMAD_KERNEL_BVH2_PERSIST: return ctx->stackNeed[0] <= (uint32_t)kStack;
-    case NOMAD_KERNEL_BVH4:
-    case NOMAD_KERNEL_BVH4_PERSIST: return ctx->wide[0].width == 4 && ctx->stackNeed[1] <= (uint32_t)kStackW4;
-    case NOMAD_KERNEL_BVH8:
-    case NOMAD_KERNEL_BVH8_PERSIST: return ctx->wide[1].width == 8 && ctx->stackNeed[2] <= (uint32_t)kStackW8;
-    default: return false;
-  }
-}
 
 template <int W, int STACK, bool ANY, bool PERSIST>
 nomad_status launch_one(nomad_ctx *ctx, const WideScene &WS, const float4 *rays, uint64_t n, const uint32_t *lenDev,
@@ -458,38 +471,43 @@ nomad_status launch_one(nomad_ctx *ctx, const WideScene &WS, const float4 *rays,
 }
 
 template <bool ANY>
-nomad_status dispatch(nomad_ctx *ctx, uint32_t k, const float4 *rays, uint64_t n, const uint32_t *lenDev,
+nomad_status dispatch(nomad_ctx *ctx, const nomad_traversal &c, const float4 *rays, uint64_t n, const uint32_t *lenDev,
                       unsigned long long *cursor, int32_t *hits5, uint8_t *occ, uint32_t *counts, cudaStream_t st) {
   const WideScene none{nullptr, kEmptyRef};
-  switch (k) {
-    case NOMAD_KERNEL_BVH2: return launch_one<2, kStack, ANY, false>(ctx, none, rays, n, lenDev, cursor, hits5, occ, counts, st);
-    case NOMAD_KERNEL_BVH2_PERSIST: return launch_one<2, kStack, ANY, true>(ctx, none, rays, n, lenDev, cursor, hits5, occ, counts, st);
-    case NOMAD_KERNEL_BVH4: return launch_one<4, kStackW4, ANY, false>(ctx, ctx->ws[0], rays, n, lenDev, cursor, hits5, occ, counts, st);
-    case NOMAD_KERNEL_BVH4_PERSIST: return launch_one<4, kStackW4, ANY, true>(ctx, ctx->ws[0], rays, n, lenDev, cursor, hits5, occ, counts, st);
-    case NOMAD_KERNEL_BVH8: return launch_one<8, kStackW8, ANY, false>(ctx, ctx->ws[1], rays, n, lenDev, cursor, hits5, occ, counts, st);
-    case NOMAD_KERNEL_BVH8_PERSIST: return launch_one<8, kStackW8, ANY, true>(ctx, ctx->ws[1], rays, n, lenDev, cursor, hits5, occ, counts, st);
+  const bool p = c.persistent != 0;
+  switch (c.width) {
+    case 2: return p ? launch_one<2, kStack, ANY, true>(ctx, none, rays, n, lenDev, cursor, hits5, occ, counts, st)
+                     : launch_one<2, kStack, ANY, false>(ctx, none, rays, n, lenDev, cursor, hits5, occ, counts, st);
+    case 4: return p ? launch_one<4, kStackW4, ANY, true>(ctx, ctx->ws[0], rays, n, lenDev, cursor, hits5, occ, counts, st)
+                     : launch_one<4, kStackW4, ANY, false>(ctx, ctx->ws[0], rays, n, lenDev, cursor, hits5, occ, counts, st);
+    case 8: return p ? launch_one<8, kStackW8, ANY, true>(ctx, ctx->ws[1], rays, n, lenDev, cursor, hits5, occ, counts, st)
+                     : launch_one<8, kStackW8, ANY, false>(ctx, ctx->ws[1], rays, n, lenDev, cursor, hits5, occ, counts, st);
     default: return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "unknown kernel variant");
   }
 }
 
 }  // namespace
 
-nomad_status nomad_trace_variant(nomad_ctx *ctx, uint32_t kernel, bool any, const float4 *rays, uint64_t n,
+nomad_status nomad_trace_variant(nomad_ctx *ctx, const nomad_traversal &cfg, bool any, const float4 *rays, uint64_t n,
                                  const uint32_t *lenDev, unsigned long long *cursor, int32_t *hits5,
                                  uint8_t *occ, uint32_t *counts, cudaStream_t st) {
   if (n == 0) return NOMAD_OK;
-  if (!variant_ok(ctx, kernel)) return nomad_fail(ctx, NOMAD_ERR_UNSUPPORTED, "kernel variant not available for this scene");
-  return any ? dispatch<true>(ctx, kernel, rays, n, lenDev, cursor, hits5, occ, counts, st)
-             : dispatch<false>(ctx, kernel, rays, n, lenDev, cursor, hits5, occ, counts, st);
+  std::string why;
+  if (!nomad_traversal_ok(ctx, cfg, &why)) return nomad_fail(ctx, NOMAD_ERR_UNSUPPORTED, why);
+  if (cfg.short_stack)
+    return nomad_trace_regroup(ctx, cfg, any, rays, n, lenDev, cursor, hits5, occ, counts, st);
+  return any ? dispatch<true>(ctx, cfg, rays, n, lenDev, cursor, hits5, occ, counts, st)
+             : dispatch<false>(ctx, cfg, rays, n, lenDev, cursor, hits5, occ, counts, st);
 }
 
 extern "C" nomad_status nomad_set_kernel(nomad_ctx *ctx, uint32_t kernel) {
   if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
   if (kernel == NOMAD_KERNEL_AUTO) kernel = NOMAD_KERNEL_BVH2;
   if (kernel >= NOMAD_KERNEL_COUNT) return fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "unknown kernel");
-  if (ctx->sceneReady && !variant_ok(ctx, kernel))
+  const nomad_traversal c = nomad_kernel_config(kernel);
+  if (ctx->sceneReady && !nomad_traversal_ok(ctx, c, nullptr))
     return fail(ctx, NOMAD_ERR_UNSUPPORTED, "kernel variant needs a deeper stack than it has for this scene");
-  ctx->kernel = kernel;
+  ctx->trav = c;
   return NOMAD_OK;
 }
 
@@ -512,9 +530,9 @@ nomad_status launch(nomad_ctx *ctx, Op op, const float4 *rays, uint64_t n, void 
     return NOMAD_OK;
   }
   if (op == Op::Any)
-    return nomad_trace_variant(ctx, ctx->kernel, true, rays, n, nullptr, cursor, nullptr, static_cast<uint8_t *>(out),
+    return nomad_trace_variant(ctx, ctx->trav, true, rays, n, nullptr, cursor, nullptr, static_cast<uint8_t *>(out),
                                nullptr, st);
-  return nomad_trace_variant(ctx, ctx->kernel, false, rays, n, nullptr, cursor, static_cast<int32_t *>(out), nullptr,
+  return nomad_trace_variant(ctx, ctx->trav, false, rays, n, nullptr, cursor, static_cast<int32_t *>(out), nullptr,
                              counts, st);
 }
 
@@ -718,10 +736,10 @@ nomad_status nomad_patch_wide(nomad_ctx *ctx) {
                                                           ctx->wideRef[w].as<const int32_t>(),
                                                           ctx->res.objRes.as<const uint8_t>(), n);
     NOMAD_CUDA(ctx, cudaGetLastError());
-    for (uint32_t o = 0; o < n; ++o)
-      if (WL.objSlot[o] == -1) ctx->ws[w].root = ctx->objResident[o] ? WL.objBlasRef[o] : kEmptyRef;
+    if (ctx->layout.tlasPairCount == 0)  // the single object is the root: its ref lives on the host
+      for (uint32_t o = 0; o < n; ++o)
+        if (WL.objSlot[o] == -1) ctx->ws[w].root = ctx->objResident[o] ? WL.objBlasRef[o] : kEmptyRef;
   }
-  NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return NOMAD_OK;
 }
 
@@ -752,12 +770,13 @@ extern "C" nomad_status nomad_autotune(nomad_ctx *ctx, const nomad_ray *rays, ui
   unsigned long long *cursor = static_cast<unsigned long long *>(ctx->cursor.p);
   for (uint32_t k = NOMAD_KERNEL_BVH2; k < NOMAD_KERNEL_COUNT; ++k) {
     out->ms[k] = -1.0f;
-    if (!variant_ok(ctx, k)) continue;
+    const nomad_traversal cfg = nomad_kernel_config(k);
+    if (!nomad_traversal_ok(ctx, cfg, nullptr)) continue;
     DeviceBuf &dst = (k == NOMAD_KERNEL_BVH2) ? ref : cur;
     float t = 1e30f;
     for (uint32_t rep = 0; rep < std::max(1u, repeats) + 1; ++rep) {
       NOMAD_CUDA(ctx, cudaEventRecord(e0, s));
-      nomad_status st = nomad_trace_variant(ctx, k, false, d, n, nullptr, cursor, dst.as<int32_t>(), nullptr, nullptr, s);
+      nomad_status st = nomad_trace_variant(ctx, cfg, false, d, n, nullptr, cursor, dst.as<int32_t>(), nullptr, nullptr, s);
       if (st != NOMAD_OK) return st;
       NOMAD_CUDA(ctx, cudaEventRecord(e1, s));
       NOMAD_CUDA(ctx, cudaEventSynchronize(e1));
@@ -783,7 +802,7 @@ extern "C" nomad_status nomad_autotune(nomad_ctx *ctx, const nomad_ray *rays, ui
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  ctx->kernel = best;
+  ctx->trav = nomad_kernel_config(best);
   out->best = best;
   return NOMAD_OK;
 }

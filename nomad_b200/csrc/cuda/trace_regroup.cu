@@ -1,0 +1,610 @@
+// Persistent-warp traversal with lane refill, a shared-memory short stack and staged top levels.
+//
+// Same contract as the kernels in rt_core.cu (box test, primitive tests, tie rule, pruning
+// margin of rt_device.cuh; the wide walk of rt_wide.cuh), so every configuration returns the
+// same hits bit for bit. What changes is how the work maps onto a warp:
+//   * Lane refill ("regrouping"). A warp keeps one ray per lane. After every traversal step it
+//     counts its busy lanes with a ballot; when fewer than `regroup` remain, the idle lanes take
+//     new rays from a per-warp pool of consecutive ray indices, refilled 64 at a time from the
+//     global cursor with one atomic. A warp therefore never idles behind its longest ray.
+//   * Short stack. The top SHORT entries of each ray's stack live in shared memory (one column
+//     per thread: conflict-free), older entries spill to a local-memory array sized for the
+//     deepest walk the scene can need, so no entry is ever lost.
+//   * Staged top levels. Nodes [0, staged) of the layout (the TLAS part, numbered breadth-first
+//     from the root by the layout builders) are copied into shared memory at block start by
+//     bulk asynchronous copies (cp.async.bulk, completion on an mbarrier; no multicast) and read
+//     from there. The wait is bounded: on expiry the block records the wait bit in the status
+//     word, waits once more (bounded) for its copy, and exits; other blocks take its rays.
+// Each iteration of the warp loop does one node step and, if the lane then stands on a leaf, the
+// leaf's primitive tests ("if-if" structure), so lanes at a leaf test their primitives together.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "rt_context.h"
+
+using namespace nomad_dev;
+
+namespace {
+
+constexpr int32_t kIdle = INT32_MIN + 1;      // lane holds no ray
+constexpr int32_t kFinished = INT32_MIN + 2;  // lane's ray is done, result not yet written
+constexpr uint32_t kChunk = 64;               // rays a warp takes from the global cursor at once
+constexpr uint32_t kStatusWaitExpired = 1u << 1;
+constexpr long long kWaitPolls = 1ll << 22;   // mbarrier try_wait polls before giving up
+constexpr uint32_t kStageHeader = 128;        // mbarrier, padded so the nodes start 128-B aligned
+constexpr int kStackW2 = 64, kStackW4 = 64, kStackW8 = 96;
+constexpr size_t kMaxDynSmem = 200 * 1024;   // opted in for every kernel at context creation
+
+template <int W> struct Lay;
+template <> struct Lay<2> { static constexpr int F4 = 4; using Entry = int32_t; static constexpr int STACK = kStackW2; };
+template <> struct Lay<4> { static constexpr int F4 = 8; using Entry = int2; static constexpr int STACK = kStackW4; };
+template <> struct Lay<8> { static constexpr int F4 = 16; using Entry = int2; static constexpr int STACK = kStackW8; };
+
+struct RgArgs {
+  const float4 *nodes;  // pair nodes (W = 2) or wide nodes
+  int32_t root;
+  uint32_t staged;      // nodes [0, staged) are read from shared memory
+  uint32_t regroup;     // refill idle lanes when fewer than this many are busy
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+  for (long long i = 0; i < kWaitPolls; ++i)
+    if (mbar_try(bar, parity)) return true;
+  return false;
+}
+
+// Copies `bytes` (a multiple of 16) from global `src` (16-byte aligned) into shared memory after
+// the barrier word. Returns false in every thread when the copy did not complete in time.
+__device__ bool stage_nodes(unsigned char *smem, const float4 *src, uint32_t bytes, uint32_t *status) {
+  const uint32_t bar = smem_u32(smem);
+  const uint32_t dst = bar + kStageHeader;
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+    const char *g = reinterpret_cast<const char *>(src);
+    for (uint32_t off = 0; off < bytes; off += 16384u) {
+      const uint32_t sz = min(16384u, bytes - off);
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst + off),
+          "l"(g + off), "r"(sz), "r"(bar)
+          : "memory");
+    }
+  }
+  bool ok = mbar_wait_bounded(bar, 0);
+  if (__syncthreads_and(ok ? 1 : 0)) return true;
+  if (threadIdx.x == 0) atomicOr(status, kStatusWaitExpired);
+  mbar_wait_bounded(bar, 0);  // let the copy land before the block's shared memory is released
+  return false;
+}
+
+// Traversal stack: the newest SHORT entries in this thread's shared-memory column, older ones in
+// local memory. sp counts all entries, lo those spilled (indices [0, lo) are in `spill`).
+template <int W, int SHORT>
+struct ShortStack {
+  using Entry = typename Lay<W>::Entry;
+  static constexpr int STACK = Lay<W>::STACK;
+  Entry *col;      // &ring[0][threadIdx.x]
+  uint32_t pitch;  // blockDim.x
+  int sp = 0, lo = 0;
+  Entry spill[STACK];
+
+  __device__ __forceinline__ Entry &slot(int i) { return col[(uint32_t)(i & (SHORT - 1)) * pitch]; }
+  __device__ __forceinline__ void push(Entry e, uint32_t *status) {
+    if (sp >= STACK) {
+      atomicOr(status, kStatusStackOverflow);
+      return;
+    }
+    if (sp - lo == SHORT) {
+      spill[lo] = slot(lo);
+      ++lo;
+    }
+    slot(sp) = e;
+    ++sp;
+  }
+  __device__ __forceinline__ Entry pop() {  // requires sp > 0
+    --sp;
+    if (sp >= lo) return slot(sp);
+    lo = sp;
+    return spill[sp];
+  }
+};
+
+template <int F4>
+__device__ __forceinline__ float4 node_f4(const float4 *__restrict__ g, const float4 *s, int32_t ref, uint32_t staged,
+                                          int k) {
+  if ((uint32_t)ref < staged) return s[(size_t)ref * F4 + k];
+  return __ldg(g + (size_t)ref * F4 + k);
+}
+
+template <int W, int SHORT, bool ANY>
+__global__ void __launch_bounds__(256) k_trace_rg(DevScene S, RgArgs A, const float4 *__restrict__ rays, uint64_t n,
+                                                  const uint32_t *__restrict__ lenDev,
+                                                  unsigned long long *__restrict__ cursor, int32_t *__restrict__ hits5,
+                                                  uint8_t *__restrict__ occ, uint32_t *__restrict__ counts) {
+  constexpr int F4 = Lay<W>::F4;
+  using Entry = typename Lay<W>::Entry;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const float4 *snodes = reinterpret_cast<const float4 *>(smem + kStageHeader);
+  const uint32_t staged = A.staged;
+  if (staged) {
+    if (!stage_nodes(smem, A.nodes, staged * (uint32_t)F4 * 16u, S.status)) return;
+  }
+  Entry *ring = reinterpret_cast<Entry *>(smem + kStageHeader + (size_t)staged * F4 * 16) + threadIdx.x;
+  ShortStack<W, SHORT> st;
+  st.col = ring;
+  st.pitch = blockDim.x;
+
+  const uint64_t N = lenDev ? (uint64_t)*lenDev : n;
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned lt = (1u << lane) - 1u;
+  const uint32_t thr = A.regroup < 1 ? 1u : (A.regroup > 32 ? 32u : A.regroup);
+  uint64_t pn = 0, pe = 0;  // this warp's pool of ray indices [pn, pe)
+  bool exhausted = false;
+
+  uint64_t idx = 0;
+  RayP r{};
+  float tmax = 0.0f;
+  HitRec h{};
+  int32_t ref = kIdle;
+
+  for (;;) {
+    // ---- refill (warp-uniform decision) ----
+    const unsigned busy = __ballot_sync(0xffffffffu, ref != kIdle);
+    if ((uint32_t)__popc(busy) < thr) {
+      const unsigned idle = ~busy;
+      const uint32_t nidle = (uint32_t)__popc(idle);
+      const uint64_t avail = pe - pn;
+      uint64_t nb = 0, ne = 0;
+      if (avail < nidle && !exhausted) {
+        unsigned long long b = 0;
+        if (lane == 0) b = atomicAdd(cursor, (unsigned long long)kChunk);
+        b = __shfl_sync(0xffffffffu, b, 0);
+        if (b >= N) {
+          exhausted = true;
+        } else {
+          nb = b;
+          ne = (b + kChunk < N) ? b + kChunk : N;
+        }
+      }
+      if (ref == kIdle) {
+        const uint64_t rank = (uint64_t)__popc(idle & lt);
+        uint64_t i = ~0ull;
+        if (rank < avail)
+          i = pn + rank;
+        else if (rank - avail < ne - nb)
+          i = nb + (rank - avail);
+        if (i != ~0ull) {
+          idx = i;
+          const float4 ra = __ldg(rays + 2 * i), rb = __ldg(rays + 2 * i + 1);
+          r = prep_ray(ra, rb);
+          tmax = rb.w;
+          h.t = tmax;
+          h.u = h.v = 0.0f;
+          h.prim = INT32_MIN;
+          h.inst = -1;
+          st.sp = st.lo = 0;
+          float tn0;
+          const bool in = tmax > kRayEps && A.root != kEmptyRef &&
+                          slab(r, S.rmin[0], S.rmin[1], S.rmin[2], S.rmax[0], S.rmax[1], S.rmax[2],
+                               ANY ? tmax : tmax * kPruneScale, tn0);
+          ref = in ? A.root : kFinished;
+        }
+      }
+      if (nidle <= avail) {
+        pn += nidle;
+      } else {
+        pn = nb + ((nidle - avail < ne - nb) ? nidle - avail : ne - nb);
+        pe = ne;
+      }
+      if (__ballot_sync(0xffffffffu, ref != kIdle) == 0) break;  // no rays left anywhere
+    }
+
+    // ---- one traversal step ----
+    if (ref != kIdle && ref != kFinished) {
+      if (ref >= 0) {
+        if constexpr (W == 2) {
+          const float4 a = node_f4<F4>(A.nodes, snodes, ref, staged, 0);
+          const float4 b = node_f4<F4>(A.nodes, snodes, ref, staged, 1);
+          const float4 c = node_f4<F4>(A.nodes, snodes, ref, staged, 2);
+          const float4 d = node_f4<F4>(A.nodes, snodes, ref, staged, 3);
+          const int32_t lref = __float_as_int(a.w), rref = __float_as_int(b.w);
+          const float bound = ANY ? tmax : h.t * kPruneScale;
+          float tl, tr;
+          const bool hl = slab(r, a.x, a.y, a.z, b.x, b.y, b.z, bound, tl) && lref != kEmptyRef;
+          const bool hr = slab(r, c.x, c.y, c.z, d.x, d.y, d.z, bound, tr) && rref != kEmptyRef;
+          if (hl && hr) {
+            const bool lf = !(tr < tl);
+            st.push(lf ? rref : lref, S.status);
+            ref = lf ? lref : rref;
+          } else if (hl) {
+            ref = lref;
+          } else if (hr) {
+            ref = rref;
+          } else if (st.sp > 0) {
+            ref = st.pop();
+          } else {
+            ref = kFinished;
+          }
+        } else {
+          const float bound = ANY ? tmax : h.t * kPruneScale;
+          float t[W];
+          int32_t cc[W];
+#pragma unroll
+          for (int q = 0; q < W / 4; ++q) {
+            const float4 mnx = node_f4<F4>(A.nodes, snodes, ref, staged, 0 * (W / 4) + q);
+            const float4 mny = node_f4<F4>(A.nodes, snodes, ref, staged, 1 * (W / 4) + q);
+            const float4 mnz = node_f4<F4>(A.nodes, snodes, ref, staged, 2 * (W / 4) + q);
+            const float4 mxx = node_f4<F4>(A.nodes, snodes, ref, staged, 3 * (W / 4) + q);
+            const float4 mxy = node_f4<F4>(A.nodes, snodes, ref, staged, 4 * (W / 4) + q);
+            const float4 mxz = node_f4<F4>(A.nodes, snodes, ref, staged, 5 * (W / 4) + q);
+            const float4 rf = node_f4<F4>(A.nodes, snodes, ref, staged, 6 * (W / 4) + q);
+            const float ax[4] = {mnx.x, mnx.y, mnx.z, mnx.w}, ay[4] = {mny.x, mny.y, mny.z, mny.w};
+            const float az[4] = {mnz.x, mnz.y, mnz.z, mnz.w}, bx[4] = {mxx.x, mxx.y, mxx.z, mxx.w};
+            const float by[4] = {mxy.x, mxy.y, mxy.z, mxy.w}, bz[4] = {mxz.x, mxz.y, mxz.z, mxz.w};
+            const int32_t rr[4] = {__float_as_int(rf.x), __float_as_int(rf.y), __float_as_int(rf.z),
+                                   __float_as_int(rf.w)};
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              float tk;
+              const bool hk = rr[k] != kEmptyRef && slab(r, ax[k], ay[k], az[k], bx[k], by[k], bz[k], bound, tk);
+              t[q * 4 + k] = hk ? tk : INFINITY;
+              cc[q * 4 + k] = hk ? rr[k] : kEmptyRef;
+            }
+          }
+          sort_children<W>(t, cc);
+          if (cc[0] != kEmptyRef) {
+#pragma unroll
+            for (int k = W - 1; k >= 1; --k) {
+              if (cc[k] != kEmptyRef) st.push(make_int2(cc[k], __float_as_int(t[k])), S.status);
+            }
+            ref = cc[0];
+          } else {
+            ref = kFinished;
+            while (st.sp > 0) {
+              const Entry e = st.pop();
+              if (!ANY && __int_as_float(e.y) > h.t * kPruneScale) continue;
+              ref = e.x;
+              break;
+            }
+          }
+        }
+      }
+      if (ref < 0 && ref != kFinished) {
+        // Leaf: records ~ref up to the one flagged kLastInLeaf.
+        int64_t k = ~ref;
+        bool hitAny = false;
+        for (;;) {
+          const float4 *q = S.tri + 3 * k;
+          const float4 Av = __ldg(q), Bv = __ldg(q + 1), Cv = __ldg(q + 2);
+          const int32_t pid = __float_as_int(Av.w);
+          const int32_t meta = __float_as_int(Cv.w);
+          if (pid >= 0 && test_prim(S, r, Av, Bv, Cv, pid, meta & 0xff, h) && ANY) {
+            hitAny = true;
+            break;
+          }
+          if (meta & kLastInLeaf) break;
+          ++k;
+        }
+        ref = kFinished;
+        if (!hitAny) {
+          while (st.sp > 0) {
+            const Entry e = st.pop();
+            if constexpr (W == 2) {
+              ref = e;
+            } else {
+              if (!ANY && __int_as_float(e.y) > h.t * kPruneScale) continue;
+              ref = e.x;
+            }
+            break;
+          }
+        }
+      }
+    }
+
+    // ---- results of the rays that finished in this iteration (converged) ----
+    const bool fin = ref == kFinished;
+    if (__any_sync(0xffffffffu, fin)) {
+      int32_t key = -1;
+      if (fin) {
+        const bool hit = h.prim != INT32_MIN;
+        if (ANY) {
+          occ[idx] = hit ? 1 : 0;
+        } else {
+          int32_t *o = hits5 + 5 * idx;
+          o[0] = hit ? h.inst : -1;
+          o[1] = hit ? h.prim : -1;
+          o[2] = __float_as_int(hit ? h.t : INFINITY);
+          o[3] = __float_as_int(h.u);
+          o[4] = __float_as_int(h.v);
+          if (hit) key = h.inst;
+        }
+      }
+      if (!ANY && counts) {
+        const unsigned peers = __match_any_sync(0xffffffffu, key);
+        if (key >= 0 && (int)lane == __ffs(peers) - 1) atomicAdd(counts + key, (uint32_t)__popc(peers));
+      }
+      if (fin) ref = kIdle;
+    }
+  }
+}
+
+// Number of hit records (5 words each) that differ between two buffers, accumulated in *bad.
+__global__ void k_count_mismatch(const int32_t *__restrict__ a, const int32_t *__restrict__ b, uint64_t n,
+                                 unsigned long long *__restrict__ bad) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  bool diff = false;
+  if (i < n)
+    for (int k = 0; k < 5; ++k) diff = diff || a[5 * i + k] != b[5 * i + k];
+  const unsigned m = __ballot_sync(0xffffffffu, diff);
+  if ((threadIdx.x & 31) == 0 && m) atomicAdd(bad, (unsigned long long)__popc(m));
+}
+
+template <int W, int SHORT, bool ANY>
+nomad_status launch_rg(nomad_ctx *ctx, const nomad_traversal &cfg, const RgArgs &A, const float4 *rays, uint64_t n,
+                       const uint32_t *lenDev, unsigned long long *cursor, int32_t *hits5, uint8_t *occ,
+                       uint32_t *counts, cudaStream_t s) {
+  using Entry = typename Lay<W>::Entry;
+  auto kern = k_trace_rg<W, SHORT, ANY>;
+  const uint32_t block = cfg.block ? cfg.block : 128u;
+  const size_t smem = kStageHeader + (size_t)A.staged * Lay<W>::F4 * 16 + (size_t)SHORT * block * sizeof(Entry);
+  if (smem > kMaxDynSmem) return nomad_fail(ctx, NOMAD_ERR_UNSUPPORTED, "staged nodes and short stack exceed shared memory");
+  int perSm = 0;
+  NOMAD_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kern, (int)block, smem));
+  if (perSm < 1) return nomad_fail(ctx, NOMAD_ERR_UNSUPPORTED, "traversal configuration does not fit on an SM");
+  uint64_t blocks = (uint64_t)ctx->smCount * (uint64_t)perSm;
+  blocks = std::max<uint64_t>(1, std::min(blocks, (n + block - 1) / block));
+  NOMAD_CUDA(ctx, cudaMemsetAsync(cursor, 0, 8, s));
+  kern<<<(unsigned)blocks, block, smem, s>>>(ctx->scene, A, rays, n, lenDev, cursor, hits5, occ, counts);
+  NOMAD_CUDA(ctx, cudaGetLastError());
+  return NOMAD_OK;
+}
+
+template <int W, bool ANY>
+nomad_status launch_w(nomad_ctx *ctx, const nomad_traversal &cfg, const RgArgs &A, const float4 *rays, uint64_t n,
+                      const uint32_t *lenDev, unsigned long long *cursor, int32_t *hits5, uint8_t *occ,
+                      uint32_t *counts, cudaStream_t s) {
+  switch (cfg.short_stack) {
+    case 8: return launch_rg<W, 8, ANY>(ctx, cfg, A, rays, n, lenDev, cursor, hits5, occ, counts, s);
+    case 16: return launch_rg<W, 16, ANY>(ctx, cfg, A, rays, n, lenDev, cursor, hits5, occ, counts, s);
+    case 32: return launch_rg<W, 32, ANY>(ctx, cfg, A, rays, n, lenDev, cursor, hits5, occ, counts, s);
+    default: return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "short stack must be 8, 16 or 32");
+  }
+}
+
+uint32_t layout_nodes(const nomad_ctx *ctx, uint32_t width) {
+  if (width == 2) return static_cast<uint32_t>(ctx->layout.pnodes.size() / 16);
+  const nomad::WideLayout &WL = ctx->wide[width == 4 ? 0 : 1];
+  return WL.floatsPerNode ? static_cast<uint32_t>(WL.nodes.size() / WL.floatsPerNode) : 0;
+}
+
+uint32_t tlas_prefix(const nomad_ctx *ctx, uint32_t width) {
+  if (width == 2) return ctx->layout.tlasPairCount;
+  return ctx->wide[width == 4 ? 0 : 1].tlasNodes;
+}
+
+}  // namespace
+
+// Raises the dynamic shared-memory limit of every short-stack kernel once, outside any stream
+// capture (the frame graphs launch them while capturing).
+template <int W, int SHORT>
+cudaError_t opt_in_w() {
+  cudaError_t e = cudaFuncSetAttribute(k_trace_rg<W, SHORT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kMaxDynSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_trace_rg<W, SHORT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxDynSmem);
+  return e;
+}
+
+cudaError_t nomad_regroup_init() {
+  cudaError_t e = cudaSuccess;
+  for (cudaError_t r : {opt_in_w<2, 8>(), opt_in_w<2, 16>(), opt_in_w<2, 32>(), opt_in_w<4, 8>(), opt_in_w<4, 16>(),
+                        opt_in_w<4, 32>(), opt_in_w<8, 8>(), opt_in_w<8, 16>(), opt_in_w<8, 32>()})
+    if (r != cudaSuccess) e = r;
+  return e;
+}
+
+nomad_traversal nomad_kernel_config(uint32_t kernel) {
+  nomad_traversal c{2, 0, 0, 1, 0, 128};
+  switch (kernel) {
+    case NOMAD_KERNEL_BVH2_PERSIST: c.persistent = 1; break;
+    case NOMAD_KERNEL_BVH4: c.width = 4; break;
+    case NOMAD_KERNEL_BVH4_PERSIST: c.width = 4; c.persistent = 1; break;
+    case NOMAD_KERNEL_BVH8: c.width = 8; break;
+    case NOMAD_KERNEL_BVH8_PERSIST: c.width = 8; c.persistent = 1; break;
+    default: break;
+  }
+  return c;
+}
+
+bool nomad_traversal_ok(const nomad_ctx *ctx, const nomad_traversal &c, std::string *why) {
+  auto no = [&](const char *m) {
+    if (why) *why = m;
+    return false;
+  };
+  if (c.width != 2 && c.width != 4 && c.width != 8) return no("width must be 2, 4 or 8");
+  if (c.block != 0 && c.block != 64 && c.block != 128 && c.block != 256) return no("block must be 64, 128 or 256");
+  if (c.short_stack != 0) {
+    if (c.short_stack != 8 && c.short_stack != 16 && c.short_stack != 32) return no("short stack must be 8, 16 or 32");
+    if (!c.persistent) return no("a short stack needs persistent warps");
+    if (c.regroup < 1 || c.regroup > 32) return no("regroup threshold must be 1..32");
+  } else if (c.staged_nodes != 0) {
+    return no("staged nodes need the short-stack kernel");
+  }
+  if (!ctx->sceneReady) return true;
+  const uint32_t wi = c.width == 2 ? 0 : (c.width == 4 ? 1 : 2);
+  const uint32_t cap = c.width == 8 ? (uint32_t)kStackW8 : (uint32_t)kStackW2;
+  if (c.width != 2 && ctx->wide[wi - 1].width != c.width) return no("wide layout missing");
+  if (ctx->stackNeed[wi] > cap) return no("traversal needs a deeper stack than the kernel has for this scene");
+  if (c.staged_nodes > layout_nodes(ctx, c.width)) return no("more staged nodes than the layout has");
+  const size_t nodeBytes = c.width == 2 ? 64 : (c.width == 4 ? 128 : 256);
+  const size_t ring = (size_t)c.short_stack * (c.block ? c.block : 128) * (c.width == 2 ? 4 : 8);
+  if (kStageHeader + c.staged_nodes * nodeBytes + ring > kMaxDynSmem)
+    return no("staged nodes and short stack exceed shared memory");
+  return true;
+}
+
+nomad_status nomad_trace_regroup(nomad_ctx *ctx, const nomad_traversal &cfg, bool any, const float4 *rays, uint64_t n,
+                                 const uint32_t *lenDev, unsigned long long *cursor, int32_t *hits5, uint8_t *occ,
+                                 uint32_t *counts, cudaStream_t s) {
+  RgArgs A;
+  A.regroup = cfg.regroup;
+  A.staged = cfg.staged_nodes;
+  if (cfg.width == 2) {
+    A.nodes = ctx->scene.pn;
+    A.root = ctx->scene.rootRef;
+  } else {
+    const WideScene &ws = ctx->ws[cfg.width == 4 ? 0 : 1];
+    A.nodes = ws.wn;
+    A.root = ws.root;
+  }
+  if (A.staged && (reinterpret_cast<uintptr_t>(A.nodes) & 15u))
+    return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "node array not 16-byte aligned for staging");
+  switch (cfg.width) {
+    case 2: return any ? launch_w<2, true>(ctx, cfg, A, rays, n, lenDev, cursor, hits5, occ, counts, s)
+                       : launch_w<2, false>(ctx, cfg, A, rays, n, lenDev, cursor, hits5, occ, counts, s);
+    case 4: return any ? launch_w<4, true>(ctx, cfg, A, rays, n, lenDev, cursor, hits5, occ, counts, s)
+                       : launch_w<4, false>(ctx, cfg, A, rays, n, lenDev, cursor, hits5, occ, counts, s);
+    case 8: return any ? launch_w<8, true>(ctx, cfg, A, rays, n, lenDev, cursor, hits5, occ, counts, s)
+                       : launch_w<8, false>(ctx, cfg, A, rays, n, lenDev, cursor, hits5, occ, counts, s);
+    default: return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "width must be 2, 4 or 8");
+  }
+}
+
+extern "C" nomad_status nomad_set_traversal(nomad_ctx *ctx, const nomad_traversal *cfg) {
+  if (!ctx || !cfg) return NOMAD_ERR_INVALID_ARGUMENT;
+  std::string why;
+  if (!nomad_traversal_ok(ctx, *cfg, &why)) return nomad_fail(ctx, NOMAD_ERR_UNSUPPORTED, why);
+  ctx->trav = *cfg;
+  if (!ctx->trav.block) ctx->trav.block = 128;
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_get_traversal(nomad_ctx *ctx, nomad_traversal *cfg) {
+  if (!ctx || !cfg) return NOMAD_ERR_INVALID_ARGUMENT;
+  *cfg = ctx->trav;
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_tlas_nodes(nomad_ctx *ctx, uint32_t out[3]) {
+  if (!ctx || !out) return NOMAD_ERR_INVALID_ARGUMENT;
+  if (!ctx->sceneReady) return nomad_fail(ctx, NOMAD_ERR_NOT_READY, "no scene uploaded");
+  out[0] = tlas_prefix(ctx, 2);
+  out[1] = tlas_prefix(ctx, 4);
+  out[2] = tlas_prefix(ctx, 8);
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_autotune_sweep(nomad_ctx *ctx, const nomad_ray *rays, uint64_t n, uint32_t repeats,
+                                             uint32_t flags, nomad_tune_entry *entries, uint32_t capacity,
+                                             uint32_t *count, nomad_traversal *best) {
+  if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
+  if (!ctx->sceneReady) return nomad_fail(ctx, NOMAD_ERR_NOT_READY, "no scene uploaded");
+  if (!rays || n == 0) return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "no sample rays");
+  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  const float4 *d = reinterpret_cast<const float4 *>(rays);
+  if (!(flags & NOMAD_TRACE_DEVICE_POINTERS)) {
+    NOMAD_CUDA(ctx, ctx->stageIn.reserve(n * sizeof(nomad_ray)));
+    NOMAD_CUDA(ctx, cudaMemcpyAsync(ctx->stageIn.p, rays, n * sizeof(nomad_ray), cudaMemcpyHostToDevice, s));
+    d = ctx->stageIn.as<const float4>();
+  }
+  // The grid: the six local-stack kernels, then every short-stack combination.
+  std::vector<nomad_traversal> grid;
+  for (uint32_t k = NOMAD_KERNEL_BVH2; k < NOMAD_KERNEL_COUNT; ++k) grid.push_back(nomad_kernel_config(k));
+  for (uint32_t w : {2u, 4u, 8u}) {
+    const uint32_t nodeBytes = w == 2 ? 64u : (w == 4 ? 128u : 256u);
+    std::vector<uint32_t> stages{0u};
+    const uint32_t stage = std::min(tlas_prefix(ctx, w), (32u * 1024u) / nodeBytes);
+    if (stage) stages.push_back(stage);
+    for (uint32_t sh : {8u, 16u, 32u})
+      for (uint32_t rg : {1u, 16u, 24u, 32u})
+        for (uint32_t sn : stages)
+          for (uint32_t bl : {128u, 256u}) grid.push_back(nomad_traversal{w, 1, sh, rg, sn, bl});
+  }
+  DeviceBuf ref, cur, bad;
+  NOMAD_CUDA(ctx, ref.reserve(n * 20));
+  NOMAD_CUDA(ctx, cur.reserve(n * 20));
+  NOMAD_CUDA(ctx, bad.reserve(8));
+  cudaEvent_t e0, e1;
+  NOMAD_CUDA(ctx, cudaEventCreate(&e0));
+  NOMAD_CUDA(ctx, cudaEventCreate(&e1));
+  unsigned long long *cursor = static_cast<unsigned long long *>(ctx->cursor.p);
+  float bestMs = 1e30f;
+  nomad_traversal bestCfg = grid[0];
+  uint32_t measured = 0;
+  nomad_status rc = NOMAD_OK;
+  for (size_t g = 0; g < grid.size() && rc == NOMAD_OK; ++g) {
+    const nomad_traversal &c = grid[g];
+    nomad_tune_entry e;
+    e.cfg = c;
+    e.ms = -1.0f;
+    e.mismatches = 0;
+    if (nomad_traversal_ok(ctx, c, nullptr)) {
+      int32_t *dst = g == 0 ? ref.as<int32_t>() : cur.as<int32_t>();
+      float t = 1e30f;
+      for (uint32_t rep = 0; rep < std::max(1u, repeats) + 1 && rc == NOMAD_OK; ++rep) {
+        if (cudaEventRecord(e0, s) != cudaSuccess) rc = nomad_fail(ctx, NOMAD_ERR_CUDA, "event record");
+        if (rc == NOMAD_OK) rc = nomad_trace_variant(ctx, c, false, d, n, nullptr, cursor, dst, nullptr, nullptr, s);
+        if (rc == NOMAD_OK && (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess))
+          rc = nomad_fail(ctx, NOMAD_ERR_CUDA, "event timing");
+        float ms = 0.0f;
+        if (rc == NOMAD_OK && cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+          rc = nomad_fail(ctx, NOMAD_ERR_CUDA, "event timing");
+        if (rep > 0) t = std::min(t, ms);  // the first launch is a warm-up
+      }
+      if (rc != NOMAD_OK) break;
+      e.ms = t;
+      if (g > 0) {
+        unsigned long long nbad = 0;
+        if (cudaMemsetAsync(bad.p, 0, 8, s) != cudaSuccess) rc = nomad_fail(ctx, NOMAD_ERR_CUDA, "memset");
+        if (rc == NOMAD_OK) {
+          k_count_mismatch<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(ref.as<const int32_t>(), cur.as<const int32_t>(), n,
+                                                                       bad.as<unsigned long long>());
+          if (cudaGetLastError() != cudaSuccess ||
+              cudaMemcpyAsync(&nbad, bad.p, 8, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+              cudaStreamSynchronize(s) != cudaSuccess)
+            rc = nomad_fail(ctx, NOMAD_ERR_CUDA, "mismatch count");
+        }
+        e.mismatches = static_cast<uint32_t>(std::min<unsigned long long>(nbad, 0xffffffffull));
+      }
+      if (e.mismatches == 0 && t < bestMs) {  // a configuration that disagrees is never chosen
+        bestMs = t;
+        bestCfg = c;
+      }
+    }
+    if (entries && measured < capacity) entries[measured] = e;
+    ++measured;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != NOMAD_OK) return rc;
+  ctx->trav = bestCfg;
+  if (count) *count = measured;
+  if (best) *best = bestCfg;
+  return NOMAD_OK;
+}

@@ -122,11 +122,28 @@ bool build_traversal_layout(const float *bvh, uint32_t bvhCount, const float *tl
     }
   }
 
-  // Pair-node numbering: TLAS internal nodes first, then BLAS internal nodes.
+  // Pair-node numbering: TLAS internal nodes first, in breadth-first order from the root so the
+  // top levels form a prefix that a kernel can stage in shared memory, then BLAS internal nodes.
   std::vector<int32_t> tPair(tlasCount, -1), bPair(bvhCount, -1);
   uint32_t np = 0;
-  for (uint32_t i = 0; i < tlasCount; ++i)
-    if (tn(i).a() >= 0) tPair[i] = static_cast<int32_t>(np++);
+  if (tn(0).a() >= 0) {
+    std::vector<uint32_t> queue{0};
+    std::vector<uint8_t> seen(tlasCount, 0);
+    seen[0] = 1;
+    for (size_t q = 0; q < queue.size(); ++q) {
+      uint32_t i = queue[q];
+      tPair[i] = static_cast<int32_t>(np++);
+      N2 n = tn(i);
+      for (int32_t c : {n.a(), n.b()}) {
+        if (seen[c]) {
+          err = "TLAS node " + std::to_string(c) + " referenced twice";
+          return false;
+        }
+        seen[c] = 1;
+        if (tn(c).a() >= 0) queue.push_back(static_cast<uint32_t>(c));
+      }
+    }
+  }
   out.tlasPairCount = np;
   for (uint32_t i = 0; i < bvhCount; ++i)
     if (bn(i).b() <= 0) bPair[i] = static_cast<int32_t>(np++);
@@ -168,7 +185,7 @@ bool build_traversal_layout(const float *bvh, uint32_t bvhCount, const float *tl
   };
   for (uint32_t i = 0; i < tlasCount; ++i) {
     N2 n = tn(i);
-    if (n.a() < 0) continue;
+    if (n.a() < 0 || tPair[i] < 0) continue;  // leaf, or not reachable from the root
     uint32_t pr = static_cast<uint32_t>(tPair[i]);
     put_child(pr, 0, tn(n.a()), tlasChildRef(n.a(), 2ll * pr + 0));
     put_child(pr, 1, tn(n.b()), tlasChildRef(n.b(), 2ll * pr + 1));

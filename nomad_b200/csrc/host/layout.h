@@ -55,6 +55,7 @@ struct WideLayout {
   std::vector<int32_t> objBlasRef;   // wide ref of each object's BLAS root
   std::vector<int64_t> objSlot;      // node * W + k of each instance link, -1 root, -2 none
   uint32_t maxDepth = 0;             // wide nodes on the longest path (+1 for the leaf)
+  uint32_t tlasNodes = 0;            // nodes [0, tlasNodes) are the TLAS part, breadth-first
 };
 
 void build_wide_layout(const TraversalLayout &L, int width, const std::vector<uint8_t> &resident, WideLayout &W);

@@ -108,6 +108,52 @@ uint32_t wide_depth(const WideLayout &W, int32_t ref) {
   return d + 1;
 }
 
+// Renumbers the nodes so the TLAS part (nodes reachable from the root without crossing an
+// instance link) comes first in breadth-first order, followed by the BLAS nodes in build order.
+// The top levels then form a prefix [0, tlasNodes) that a kernel can stage in shared memory.
+void reorder_tlas_first(WideLayout &W) {
+  const size_t fpn = W.floatsPerNode, nn = W.nodes.size() / fpn;
+  if (W.rootRef < 0 || nn == 0) return;
+  std::vector<uint8_t> isLink(nn * W.width, 0);
+  for (int64_t s : W.objSlot)
+    if (s >= 0) isLink[s] = 1;
+  std::vector<int32_t> perm(nn, -1), order;
+  order.reserve(nn);
+  order.push_back(W.rootRef);
+  perm[W.rootRef] = 0;
+  for (size_t q = 0; q < order.size(); ++q) {
+    const float *n = W.nodes.data() + (size_t)order[q] * fpn;
+    for (uint32_t i = 0; i < W.width; ++i) {
+      int32_t c = float_bits_as_int(n[6 * W.width + i]);
+      if (c < 0 || isLink[(size_t)order[q] * W.width + i] || perm[c] >= 0) continue;
+      perm[c] = static_cast<int32_t>(order.size());
+      order.push_back(c);
+    }
+  }
+  W.tlasNodes = static_cast<uint32_t>(order.size());
+  for (size_t i = 0; i < nn; ++i)
+    if (perm[i] < 0) {
+      perm[i] = static_cast<int32_t>(order.size());
+      order.push_back(static_cast<int32_t>(i));
+    }
+  std::vector<float> nodes(W.nodes.size());
+  for (size_t k = 0; k < nn; ++k) {
+    const float *src = W.nodes.data() + (size_t)order[k] * fpn;
+    float *dst = nodes.data() + k * fpn;
+    std::copy(src, src + fpn, dst);
+    for (uint32_t i = 0; i < W.width; ++i) {
+      int32_t c = float_bits_as_int(dst[6 * W.width + i]);
+      if (c >= 0) dst[6 * W.width + i] = int_bits_as_float(perm[c]);
+    }
+  }
+  W.nodes.swap(nodes);
+  W.rootRef = perm[W.rootRef];
+  for (int32_t &r : W.objBlasRef)
+    if (r >= 0) r = perm[r];
+  for (int64_t &s : W.objSlot)
+    if (s >= 0) s = (int64_t)perm[s / W.width] * W.width + s % W.width;
+}
+
 }  // namespace
 
 void build_wide_layout(const TraversalLayout &L, int width, const std::vector<uint8_t> &resident, WideLayout &W) {
@@ -135,6 +181,7 @@ void build_wide_layout(const TraversalLayout &L, int width, const std::vector<ui
         W.rootRef = resident[o] ? W.objBlasRef[o] : kEmptyRef;
       }
   }
+  reorder_tlas_first(W);
   // depth with every instance linked (bounds the stack for any residency state)
   uint32_t d = 0;
   if (L.tlasPairCount > 0) {

@@ -96,6 +96,7 @@ SIGNATURES = {
     "nomad_view_pinhole": (C.c_int32, [_P, _P, _P, C.c_float, C.c_uint32, C.c_uint32, _P]),
     "nomad_render_frame": (C.c_int32, [_P, _P, C.c_uint32, _P, C.c_uint32]),
     "nomad_render_stats": (C.c_int32, [_P, _P]),
+    "nomad_frame_graph_stats": (C.c_int32, [_P, _P]),
     "nomad_reset_render_stats": (C.c_int32, [_P]),
     "nomad_residency_step": (C.c_int32, [_P, _P, _P, C.POINTER(C.c_uint32)]),
     "nomad_object_bytes": (C.c_int32, [_P, _P]),
@@ -110,6 +111,11 @@ SIGNATURES = {
     "nomad_set_restir": (C.c_int32, [_P, _P]),
     "nomad_reset_restir": (C.c_int32, [_P]),
     "nomad_autotune": (C.c_int32, [_P, _P, C.c_uint64, C.c_uint32, C.c_uint32, _P]),
+    "nomad_set_traversal": (C.c_int32, [_P, _P]),
+    "nomad_get_traversal": (C.c_int32, [_P, _P]),
+    "nomad_tlas_nodes": (C.c_int32, [_P, _P]),
+    "nomad_autotune_sweep": (C.c_int32, [_P, _P, C.c_uint64, C.c_uint32, C.c_uint32, _P, C.c_uint32,
+                                         C.POINTER(C.c_uint32), _P]),
 }
 
 KERNEL_BVH4, KERNEL_BVH4_PERSIST, KERNEL_BVH8, KERNEL_BVH8_PERSIST, KERNEL_COUNT = 3, 4, 5, 6, 7
@@ -119,6 +125,25 @@ KERNEL_NAMES = {1: "bvh2", 2: "bvh2_persist", 3: "bvh4", 4: "bvh4_persist", 5: "
 class TuneResult(C.Structure):
     _fields_ = [("best", C.c_uint32), ("ms", C.c_float * 7), ("mismatches", C.c_uint32 * 7),
                 ("stack_need", C.c_uint32 * 3)]
+
+
+class Traversal(C.Structure):
+    """nomad_traversal: width, persistent, short_stack, regroup, staged_nodes, block."""
+    _fields_ = [("width", C.c_uint32), ("persistent", C.c_uint32), ("short_stack", C.c_uint32),
+                ("regroup", C.c_uint32), ("staged_nodes", C.c_uint32), ("block", C.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {f: int(getattr(self, f)) for f, _ in self._fields_}
+
+    def name(self) -> str:
+        if not self.short_stack:
+            return f"bvh{self.width}" + ("_persist" if self.persistent else "")
+        return (f"bvh{self.width}_ss{self.short_stack}_rg{self.regroup}"
+                + (f"_st{self.staged_nodes}" if self.staged_nodes else "") + f"_b{self.block}")
+
+
+class TuneEntry(C.Structure):
+    _fields_ = [("cfg", Traversal), ("ms", C.c_float), ("mismatches", C.c_uint32)]
 
 
 class RestirConfig(C.Structure):
@@ -149,6 +174,7 @@ VIEW_DTYPE = np.dtype([("camera_pos", "<f4", 3), ("viewport_u", "<f4", 3), ("vie
 VIEW_CLAMP = 1 << 0
 VIEW_RESTIR = 1 << 1
 VIEW_CENTER = 1 << 2
+RENDER_DIRECT = 1 << 2  # render flag: launch the frame without the cached CUDA graph
 
 
 def view_pinhole(position, look_at, up=(0.0, 1.0, 0.0), vfov=60.0, width=640, height=360, spp=1,
@@ -379,6 +405,40 @@ class Context:
     def set_kernel(self, k: int):
         self._ck(self.lib.nomad_set_kernel(self.h, k))
 
+    def set_traversal(self, width=2, persistent=1, short_stack=0, regroup=1, staged_nodes=0, block=128):
+        t = Traversal(width, persistent, short_stack, regroup, staged_nodes, block)
+        self._ck(self.lib.nomad_set_traversal(self.h, C.byref(t)))
+
+    def traversal(self) -> dict:
+        t = Traversal()
+        self._ck(self.lib.nomad_get_traversal(self.h, C.byref(t)))
+        return t.as_dict()
+
+    def tlas_nodes(self) -> list:
+        out = (C.c_uint32 * 3)()
+        self._ck(self.lib.nomad_tlas_nodes(self.h, out))
+        return list(out)
+
+    def autotune_sweep(self, rays, repeats=2, device=False) -> dict:
+        """Sweeps width x short stack x regroup threshold x staged top levels x block on the sample
+        rays, checks each configuration bit for bit against the binary kernel and selects the
+        fastest; returns {"best": cfg dict, "best_name", "entries": [(name, cfg, ms, mismatches)]}."""
+        cap = 512
+        entries = (TuneEntry * cap)()
+        count = C.c_uint32(0)
+        best = Traversal()
+        if device:
+            ptr, n = rays
+            self._ck(self.lib.nomad_autotune_sweep(self.h, _P(ptr), n, repeats, TRACE_DEVICE_POINTERS, entries, cap,
+                                                   C.byref(count), C.byref(best)))
+        else:
+            rr = np.ascontiguousarray(rays, RAY_DTYPE)
+            self._ck(self.lib.nomad_autotune_sweep(self.h, _ptr(rr), rr.shape[0], repeats, 0, entries, cap,
+                                                   C.byref(count), C.byref(best)))
+        rows = [(e.cfg.name(), e.cfg.as_dict(), float(e.ms), int(e.mismatches))
+                for e in entries[: min(count.value, cap)]]
+        return {"best": best.as_dict(), "best_name": best.name(), "entries": rows}
+
     def sync(self):
         self._ck(self.lib.nomad_sync(self.h))
 
@@ -441,14 +501,14 @@ class Context:
                                            TRACE_DEVICE_POINTERS))
 
     # path tracing
-    def render(self, views: np.ndarray, count_hits: bool = False) -> list:
-        """Renders the views in one batched frame; returns one (height, width, 3) float32 image
-        per view."""
+    def render(self, views: np.ndarray, count_hits: bool = False, graph: bool = True) -> list:
+        """Renders the views in one batched frame (replayed from a captured CUDA graph unless
+        graph=False); returns one (height, width, 3) float32 image per view."""
         views = np.ascontiguousarray(views, VIEW_DTYPE).reshape(-1)
         total = int((views["width"].astype(np.int64) * views["height"]).sum())
         out = np.empty(total * 3, np.float32)
-        self._ck(self.lib.nomad_render_frame(self.h, _ptr(views), views.shape[0], _ptr(out),
-                                             TRACE_COUNT_HITS if count_hits else 0))
+        flags = (TRACE_COUNT_HITS if count_hits else 0) | (0 if graph else RENDER_DIRECT)
+        self._ck(self.lib.nomad_render_frame(self.h, _ptr(views), views.shape[0], _ptr(out), flags))
         imgs, off = [], 0
         for v in views:
             n = int(v["width"]) * int(v["height"])
@@ -456,12 +516,18 @@ class Context:
             off += n
         return imgs
 
-    def render_dev(self, views: np.ndarray, out_ptr: int, count_hits: bool = False):
+    def render_dev(self, views: np.ndarray, out_ptr: int, count_hits: bool = False, graph: bool = True):
         views = np.ascontiguousarray(views, VIEW_DTYPE).reshape(-1)
         self._keep_views = views
         self._ck(self.lib.nomad_render_frame(self.h, _ptr(views), views.shape[0], _P(out_ptr),
                                              TRACE_DEVICE_POINTERS |
-                                             (TRACE_COUNT_HITS if count_hits else 0)))
+                                             (TRACE_COUNT_HITS if count_hits else 0) |
+                                             (0 if graph else RENDER_DIRECT)))
+
+    def frame_graph_stats(self) -> dict:
+        out = np.zeros(3, np.uint64)
+        self._ck(self.lib.nomad_frame_graph_stats(self.h, _ptr(out)))
+        return {"captures": int(out[0]), "launches": int(out[1]), "cached": int(out[2])}
 
     def render_stats(self) -> np.ndarray:
         out = np.zeros(4, np.uint64)
@@ -472,8 +538,14 @@ class Context:
         self._ck(self.lib.nomad_reset_render_stats(self.h))
 
     # residency policies
-    def residency_step(self, params: "ResidencyParams", camera_view: np.ndarray) -> int:
+    def residency_step(self, params: "ResidencyParams", camera_view: np.ndarray, toggles: bool = True):
+        """One device residency step. With toggles=True waits for and returns the number of
+        objects whose residency flipped; with toggles=False the step stays asynchronous on the
+        context's stream (returns None)."""
         v = np.ascontiguousarray(camera_view, VIEW_DTYPE).reshape(-1)[:1]
+        if not toggles:
+            self._ck(self.lib.nomad_residency_step(self.h, C.byref(params), _ptr(v), None))
+            return None
         t = C.c_uint32()
         self._ck(self.lib.nomad_residency_step(self.h, C.byref(params), _ptr(v), C.byref(t)))
         return t.value

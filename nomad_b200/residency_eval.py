@@ -138,7 +138,7 @@ class Workload:
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             ctx.render_dev(v, d_img.data_ptr(), count_hits=True)
-            ctx.residency_step(prm, v)
+            ctx.residency_step(prm, v, toggles=False)
             ctx.sync()
             dt = time.perf_counter() - t0
             num = torch.mean((d_img - d_ref) ** 2).item()

@@ -86,3 +86,36 @@ def test_render_city_1080p_sample(nb, orc, ctx):
     want, _, _ = orc.render(orc.OracleScene(sb), sb.materials, v, pixels=pix)
     _compare(img[pix.astype(np.int64)], want)
     assert np.isfinite(img).all()
+
+
+def test_frame_graph_replay(nb, orc, ctx, small_city):
+    """A frame replayed from the captured CUDA graph equals the directly launched frame and the
+    oracle; changing cameras and frame numbers reuses the graph, changing the traversal
+    configuration captures a new one."""
+    scene, sb = small_city
+    ctx.upload(sb)
+
+    def views(f):
+        return np.concatenate([
+            nb.view_pinhole((0 + f, 60, -180), (0, 0, 0), width=64, height=36, spp=3, max_depth=2, seed=5, frame=f),
+            nb.view_pinhole((100, 30 + f, 40), (0, 10, 0), width=24, height=20, spp=1, max_depth=3, seed=6, frame=f)])
+
+    s0 = ctx.frame_graph_stats()
+    for f in range(3):
+        v = views(f)
+        g = np.concatenate([i.reshape(-1, 3) for i in ctx.render(v)])
+        d = np.concatenate([i.reshape(-1, 3) for i in ctx.render(v, graph=False)])
+        assert np.array_equal(g.view(np.int32), d.view(np.int32)), f
+        if f == 0:
+            want, _, _ = orc.render(orc.OracleScene(sb), sb.materials, v)
+            _compare(g, want)
+    s1 = ctx.frame_graph_stats()
+    assert s1["captures"] - s0["captures"] == 1 and s1["launches"] - s0["launches"] == 3, (s0, s1)
+    ctx.set_traversal(width=4, persistent=1, short_stack=16, regroup=24, staged_nodes=0, block=128)
+    v = views(5)
+    g = np.concatenate([i.reshape(-1, 3) for i in ctx.render(v)])
+    d = np.concatenate([i.reshape(-1, 3) for i in ctx.render(v, graph=False)])
+    assert np.array_equal(g.view(np.int32), d.view(np.int32))
+    assert ctx.frame_graph_stats()["captures"] - s1["captures"] == 1
+    ctx.set_kernel(1)
+    assert ctx.status() == 0

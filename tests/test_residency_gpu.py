@@ -70,8 +70,9 @@ def _residency_frame(nb, ctx, view):
     return ctx.object_hits().astype(np.int64)
 
 
+@pytest.mark.parametrize("sync_toggles", [True, False])
 @pytest.mark.parametrize("policy", [0, 1, 2])
-def test_residency_step_against_oracle(nb, orc, ctx, small_city, policy):
+def test_residency_step_against_oracle(nb, orc, ctx, small_city, policy, sync_toggles):
     from oracle import residency as ores
 
     scene, sb = small_city
@@ -87,7 +88,7 @@ def test_residency_step_against_oracle(nb, orc, ctx, small_city, policy):
     for frame, pos in enumerate([(0, 60, -180), (20, 50, -150), (40, 45, -120)]):
         view = nb.view_pinhole(pos, (0, 0, 0), width=96, height=54, spp=2, max_depth=2, seed=frame)
         hits = _residency_frame(nb, ctx, view)
-        toggles = ctx.residency_step(prm, view)
+        toggles = ctx.residency_step(prm, view, toggles=sync_toggles)
         feats, keys = ctx.residency_last()
         score = (score.astype(np.float32) * np.float32(0.85) + hits.astype(np.float32)).astype(np.float32)
         visible = feats[:, 2] > 0.5
@@ -102,7 +103,7 @@ def test_residency_step_against_oracle(nb, orc, ctx, small_city, policy):
                                    always=(policy == nb.POLICY_ALWAYS))
         got = ctx.residency_flags()
         assert np.array_equal(got, want), (frame, np.nonzero(got != want)[0][:10])
-        assert toggles == want_t
+        assert toggles == (want_t if sync_toggles else None)
         flags = got
         if policy != nb.POLICY_ALWAYS:
             assert int(nbytes[flags.astype(bool)].sum()) <= budget + int(np.sort(nbytes)[-2:].sum())

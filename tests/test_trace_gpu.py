@@ -177,3 +177,86 @@ def test_full_city_sample(nb, orc, ctx):
     b = nb.bounce_rays(rays[idx], hits[idx], sb.prims, seed=6)
     _assert_hits_equal(ctx.trace_closest(b), ref.closest(b))
     assert ctx.status() == 0
+
+
+# Short-stack persistent kernels: lane refill threshold, shared-memory short stack with local
+# spill, staged top levels. Every configuration must return the oracle's hits bit for bit.
+_RG_CONFIGS = [
+    dict(width=2, short_stack=8, regroup=1, staged=False, block=128),
+    dict(width=2, short_stack=16, regroup=32, staged=True, block=256),
+    dict(width=4, short_stack=8, regroup=16, staged=True, block=128),
+    dict(width=4, short_stack=32, regroup=24, staged=False, block=256),
+    dict(width=8, short_stack=8, regroup=32, staged=True, block=256),
+    dict(width=8, short_stack=16, regroup=1, staged=False, block=64),
+]
+
+
+def _set_rg(ctx, c):
+    tl = ctx.tlas_nodes()[{2: 0, 4: 1, 8: 2}[c["width"]]]
+    cap = (32 * 1024) // {2: 64, 4: 128, 8: 256}[c["width"]]
+    ctx.set_traversal(width=c["width"], persistent=1, short_stack=c["short_stack"], regroup=c["regroup"],
+                      staged_nodes=min(tl, cap) if c["staged"] else 0, block=c["block"])
+
+
+@pytest.mark.parametrize("cfg", _RG_CONFIGS, ids=lambda c: "w{width}_ss{short_stack}_rg{regroup}_st{staged:d}_b{block}".format(**c))
+@pytest.mark.parametrize("which", ["ico", "city"])
+def test_regroup_parity(nb, orc, ctx, ico_scene, small_city, which, cfg):
+    scene, sb = ico_scene if which == "ico" else small_city
+    ctx.upload(sb)
+    _set_rg(ctx, cfg)
+    cam = nb.icosphere_camera(160, 90) if which == "ico" else nb.Camera((0, 60, -180), (0, 0, 0), width=160, height=90)
+    prim = cam.primary_rays(2, seed=13)
+    rays = np.concatenate([prim, _rays(sb, 140)])
+    ref = orc.OracleScene(sb)
+    want = ref.closest(rays)
+    ctx.reset_object_hits()
+    got = ctx.trace_closest(rays, count_hits=True)
+    _assert_hits_equal(got, want)
+    counts = np.bincount(want["inst"][want["prim"] >= 0], minlength=sb.object_count).astype(np.uint32)
+    assert np.array_equal(ctx.object_hits(), counts)
+    bounce = nb.bounce_rays(prim, want[: prim.shape[0]], sb.prims, seed=14)
+    _assert_hits_equal(ctx.trace_closest(bounce), ref.closest(bounce))
+    short = rays.copy()
+    hit = want["prim"] >= 0
+    short["tmax"][hit] = want["t"][hit] * np.float32(0.5)
+    for rs in (rays, short):
+        assert np.array_equal(ctx.trace_any(rs), ref.any(rs))
+    assert ctx.status() == 0
+    ctx.set_kernel(1)
+
+
+def test_regroup_residency(nb, orc, ctx, small_city):
+    scene, sb = small_city
+    ctx.upload(sb)
+    _set_rg(ctx, dict(width=4, short_stack=16, regroup=24, staged=True, block=128))
+    rays = _rays(sb, 150)
+    rng = np.random.default_rng(19)
+    off_objs = np.nonzero(rng.random(sb.object_count) < 0.4)[0]
+    for o in off_objs:
+        ctx.set_object_active(int(o), False)
+    ctx.flush()
+    root = sb.instances["blas_root_index"].copy()
+    root[off_objs] = -1
+    ref = orc.OracleScene(sb, blas_root=root)
+    _assert_hits_equal(ctx.trace_closest(rays), ref.closest(rays))
+    assert np.array_equal(ctx.trace_any(rays), ref.any(rays))
+    for o in off_objs:
+        ctx.set_object_active(int(o), True)
+    ctx.flush()
+    _assert_hits_equal(ctx.trace_closest(rays), orc.OracleScene(sb).closest(rays))
+    ctx.set_kernel(1)
+
+
+def test_autotune_sweep(nb, orc, ctx, small_city):
+    scene, sb = small_city
+    ctx.upload(sb)
+    rays = _rays(sb, 160)
+    res = ctx.autotune_sweep(rays, repeats=1)
+    names = [e[0] for e in res["entries"]]
+    assert len(names) > 100 and len(set(names)) == len(names)
+    assert all(e[3] == 0 for e in res["entries"] if e[2] >= 0), [e for e in res["entries"] if e[3]]
+    assert {e[1]["width"] for e in res["entries"]} == {2, 4, 8}
+    assert {e[1]["short_stack"] for e in res["entries"]} == {0, 8, 16, 32}
+    assert ctx.traversal() == res["best"]
+    _assert_hits_equal(ctx.trace_closest(rays), orc.OracleScene(sb).closest(rays))
+    ctx.set_kernel(1)
