@@ -142,24 +142,27 @@ nomad_status nomad_autotune(nomad_ctx *ctx, const nomad_ray *rays, uint64_t n, u
 nomad_status nomad_set_kernel(nomad_ctx *ctx, uint32_t kernel);
 
 /* Full traversal configuration (no counterpart in the reference, which has one kernel). The
- * NOMAD_KERNEL_* variants are the configurations with short_stack = 0. With short_stack > 0 the
- * kernel runs persistent warps that
- *   - keep the top `short_stack` entries of each ray's traversal stack in shared memory and
- *     spill older entries to local memory (exact for any depth the scene needs);
+ * NOMAD_KERNEL_* variants are the configurations with persistent = 0 or 1. persistent = 2 selects
+ * the regrouping kernel, whose persistent warps
  *   - refill idle lanes with new rays from a per-warp pool whenever fewer than `regroup` of the
  *     warp's 32 lanes are still traversing (1: only when the whole warp is idle; 32: as soon as
  *     one lane is idle);
+ *   - keep each ray's stack in local memory (short_stack = 0) or its newest `short_stack`
+ *     entries in shared memory with older entries spilled to local memory (exact for any depth
+ *     the scene needs);
+ *   - with postpone_leaves = 1, park the first leaf a lane reaches and keep descending while
+ *     other lanes of the warp still look for one, then test the parked leaves together;
  *   - copy the first `staged_nodes` nodes of the layout (the TLAS top levels, numbered
- *     breadth-first) into shared memory with one bulk asynchronous copy per block and read
- *     them from there.
+ *     breadth-first) into shared memory with bulk asynchronous copies and read them from there.
  * Every configuration returns the same hits bit for bit. */
 typedef struct nomad_traversal {
-  uint32_t width;         /* 2 (pair nodes), 4 or 8                                            */
-  uint32_t persistent;    /* 0: one ray per thread; 1: persistent warps                        */
-  uint32_t short_stack;   /* 0, or 8 / 16 / 32 shared-memory entries per ray (persistent only) */
-  uint32_t regroup;       /* 1..32, refill threshold in busy lanes (short_stack > 0)           */
-  uint32_t staged_nodes;  /* top-level nodes staged in shared memory (short_stack > 0)         */
-  uint32_t block;         /* threads per block: 0 (default 128), 64, 128, 256                  */
+  uint32_t width;           /* 2 (pair nodes), 4 or 8                                          */
+  uint32_t persistent;      /* 0: one ray per thread; 1: persistent warps; 2: regrouping warps */
+  uint32_t short_stack;     /* persistent = 2: 0 (local memory), 8, 16 or 32                   */
+  uint32_t regroup;         /* persistent = 2: refill threshold in busy lanes, 1..32           */
+  uint32_t staged_nodes;    /* persistent = 2: top-level nodes staged in shared memory         */
+  uint32_t block;           /* threads per block: 0 (default 128), 64, 128, 256                */
+  uint32_t postpone_leaves; /* persistent = 2: 1 = park the first leaf and keep descending     */
 } nomad_traversal;
 nomad_status nomad_set_traversal(nomad_ctx *ctx, const nomad_traversal *cfg);
 nomad_status nomad_get_traversal(nomad_ctx *ctx, nomad_traversal *cfg);
@@ -172,8 +175,9 @@ typedef struct nomad_tune_entry {
   float ms;               /* best of `repeats` timings; negative when not run                  */
   uint32_t mismatches;    /* sample rays whose hit differs from the binary per-thread kernel's */
 } nomad_tune_entry;
-/* Sweeps width {2,4,8} x short stack {0 (local), 8, 16, 32} x regroup threshold {1, 16, 24, 32}
- * x staged top levels {0, up to 32 KB} x block {128, 256} on n sample rays, checks every
+/* Sweeps the six NOMAD_KERNEL_* variants and, for the regrouping kernel, width {2,4,8} x short
+ * stack {0 (local), 8, 16, 32} x regroup threshold {1, 16, 24, 32} x postponed leaves {0, 1} x
+ * staged top levels {0, up to 8 KB} x block {128, 256} on n sample rays, checks every
  * configuration against the binary kernel bit for bit, and selects the fastest one that agrees.
  * Fills up to `capacity` entries; *count receives the number of configurations measured. */
 nomad_status nomad_autotune_sweep(nomad_ctx *ctx, const nomad_ray *rays, uint64_t n, uint32_t repeats,

@@ -97,7 +97,75 @@ __device__ __forceinline__ unsigned long long sort_key(float s, uint32_t idx) {
   return ((unsigned long long)(~b) << 32) | idx;     // descending score, then ascending index
 }
 
-// Single block: sort, select under the budget, apply toggles and patch the TLAS refs.
+// Block-wide exclusive scan of one u32 per thread (1024 threads); returns this thread's prefix
+// and writes the total to *total (shared).
+__device__ __forceinline__ uint32_t block_exscan(uint32_t v, uint32_t *warpSums, uint32_t *total) {
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+    if ((int)lane >= d) x += y;
+  }
+  if (lane == 31) warpSums[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = warpSums[lane];
+    uint32_t z = w;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, z, d);
+      if ((int)lane >= d) z += y;
+    }
+    warpSums[lane] = z - w;  // exclusive prefix of the warp totals
+    if (lane == 31) *total = z;
+  }
+  __syncthreads();
+  const uint32_t r = warpSums[warp] + x - v;
+  __syncthreads();
+  return r;
+}
+
+// Greedy fill in sorted order by one warp: candidates (cand[k] = 1) are taken while they fit in
+// the budget, skipping those that do not (the sequential rule), 32 positions at a time. Each round
+// first drops lanes that cannot fit on their own, then accepts the longest run of candidates whose
+// running byte total fits; the first candidate past that run is skipped.
+__device__ void warp_greedy(uint32_t n, const unsigned long long *__restrict__ sk,
+                            const unsigned long long *__restrict__ bytes, unsigned long long budget, bool unlimited,
+                            uint8_t *cand, uint8_t *dsel, unsigned long long *used) {
+  const unsigned lane = threadIdx.x & 31u;
+  unsigned long long u = *used;
+  for (uint32_t base = 0; base < n; base += 32) {
+    const uint32_t k = base + lane;
+    bool c = k < n && cand[k];
+    const unsigned long long b = c ? bytes[(uint32_t)(sk[k] & 0xffffffffu)] : 0ull;
+    for (;;) {
+      const unsigned long long rem = unlimited ? ~0ull : (u > budget ? 0ull : budget - u);
+      if (c && b > rem) c = false;
+      if (__ballot_sync(0xffffffffu, c) == 0) break;
+      unsigned long long p = c ? b : 0ull;  // inclusive prefix of candidate bytes
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, p, d);
+        if ((int)lane >= d) p += y;
+      }
+      const unsigned fail = __ballot_sync(0xffffffffu, c && p > rem);
+      const int f = fail ? __ffs(fail) - 1 : 32;
+      const bool take = c && (int)lane < f;
+      if (take) dsel[k] = 1;
+      // bytes taken this round: the prefix just before the first failing lane (or the total)
+      const unsigned long long pf = __shfl_sync(0xffffffffu, p, f < 32 ? f : 31);
+      const unsigned long long bf = __shfl_sync(0xffffffffu, b, f < 32 ? f : 31);
+      u += f < 32 ? pf - bf : pf;
+      c = c && (int)lane > f;
+    }
+  }
+  if (lane == 0) *used = u;
+}
+
+// Single block of 1024 threads: sort by score, select under the budget (min_active, visibility
+// reserve, fill), apply toggles in index order and patch the TLAS refs. Every pass but the two
+// budget walks is data-parallel; the budget walks run on one warp, 32 objects at a time.
 __global__ void __launch_bounds__(1024) k_select(uint32_t n, uint32_t npow2, uint32_t policy,
                                                  const float *__restrict__ keys, const uint8_t *__restrict__ visible,
                                                  const unsigned long long *__restrict__ bytes,
@@ -107,8 +175,14 @@ __global__ void __launch_bounds__(1024) k_select(uint32_t n, uint32_t npow2, uin
                                                  const int32_t *__restrict__ blasRef, int32_t *__restrict__ pnodeWords,
                                                  uint32_t *__restrict__ misc) {
   extern __shared__ unsigned long long sk[];
+  uint8_t *dsel = reinterpret_cast<uint8_t *>(sk + npow2);  // selected, by sorted position
+  uint8_t *cand = dsel + npow2;                             // candidates of the current walk
+  __shared__ uint32_t warpSums[32];
+  __shared__ uint32_t total;
+  __shared__ unsigned long long used;
   for (uint32_t i = threadIdx.x; i < npow2; i += blockDim.x)
     sk[i] = i < n ? sort_key(policy == NOMAD_POLICY_ALWAYS ? 1.0f : keys[i], i) : ~0ull;
+  if (threadIdx.x == 0) used = 0;
   __syncthreads();
   for (uint32_t k = 2; k <= npow2; k <<= 1) {
     for (uint32_t j = k >> 1; j > 0; j >>= 1) {
@@ -126,54 +200,61 @@ __global__ void __launch_bounds__(1024) k_select(uint32_t n, uint32_t npow2, uin
       __syncthreads();
     }
   }
+  const bool unlimited = budget == 0 || policy == NOMAD_POLICY_ALWAYS;
+  // min_active: the best-scored objects stay whatever the budget
+  for (uint32_t k = threadIdx.x; k < npow2; k += blockDim.x) {
+    const bool m = k < n && k < minActive;
+    dsel[k] = m ? 1 : 0;
+    if (m) atomicAdd(&used, bytes[(uint32_t)(sk[k] & 0xffffffffu)]);
+  }
+  __syncthreads();
+  // visibility reserve: the first `reserve` visible objects in score order (a contiguous segment
+  // of sorted positions per thread, so the scan keeps the sorted order)
+  const uint32_t per = (npow2 + blockDim.x - 1) / blockDim.x;
+  const uint32_t k0 = threadIdx.x * per;
+  uint32_t nv = 0;
+  for (uint32_t k = k0; k < k0 + per && k < n; ++k) nv += visible[(uint32_t)(sk[k] & 0xffffffffu)] ? 1u : 0u;
+  uint32_t before = block_exscan(nv, warpSums, &total);
+  for (uint32_t k = k0; k < k0 + per && k < npow2; ++k) {
+    bool c = false;
+    if (k < n && visible[(uint32_t)(sk[k] & 0xffffffffu)]) {
+      c = before < reserve && !dsel[k];
+      ++before;
+    }
+    cand[k] = c ? 1 : 0;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) warp_greedy(n, sk, bytes, budget, unlimited, cand, dsel, &used);
+  __syncthreads();
+  // fill in score order
+  for (uint32_t k = threadIdx.x; k < npow2; k += blockDim.x) cand[k] = (k < n && !dsel[k]) ? 1 : 0;
+  __syncthreads();
+  if (threadIdx.x < 32) warp_greedy(n, sk, bytes, budget, unlimited, cand, dsel, &used);
+  __syncthreads();
+  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) desired[(uint32_t)(sk[k] & 0xffffffffu)] = dsel[k];
+  __syncthreads();
+  // toggles in index order, the first max_toggles of them when bounded
+  uint32_t nd = 0;
+  for (uint32_t o = k0; o < k0 + per && o < n; ++o) nd += desired[o] != res[o] ? 1u : 0u;
+  uint32_t rank = block_exscan(nd, warpSums, &total);
+  for (uint32_t o = k0; o < k0 + per && o < n; ++o) {
+    const uint8_t want = desired[o];
+    if (want == res[o]) continue;
+    const bool apply = maxToggles == 0 || rank < maxToggles;
+    ++rank;
+    if (!apply) continue;
+    res[o] = want;
+    const long long s = slot[o];
+    const int32_t ref = want ? blasRef[o] : kEmptyRef;
+    if (s >= 0) {
+      pnodeWords[(s / 2) * 16 + ((s & 1) ? 7 : 3)] = ref;
+    } else if (s == -1) {
+      misc[1] = 1;
+      misc[2] = want;
+    }
+  }
   if (threadIdx.x == 0) {
-    for (uint32_t i = 0; i < n; ++i) desired[i] = 0;
-    unsigned long long used = 0;
-    bool unlimited = budget == 0 || policy == NOMAD_POLICY_ALWAYS;
-    // min_active: the best-scored objects stay whatever the budget
-    for (uint32_t k = 0; k < n && k < minActive; ++k) {
-      uint32_t o = (uint32_t)(sk[k] & 0xffffffffu);
-      desired[o] = 1;
-      used += bytes[o];
-    }
-    // visibility reserve
-    uint32_t promoted = 0;
-    for (uint32_t k = 0; k < n && promoted < reserve; ++k) {
-      uint32_t o = (uint32_t)(sk[k] & 0xffffffffu);
-      if (!visible[o]) continue;
-      ++promoted;
-      if (desired[o]) continue;
-      if (unlimited || used + bytes[o] <= budget) {
-        desired[o] = 1;
-        used += bytes[o];
-      }
-    }
-    // fill in score order
-    for (uint32_t k = 0; k < n; ++k) {
-      uint32_t o = (uint32_t)(sk[k] & 0xffffffffu);
-      if (desired[o]) continue;
-      if (unlimited || used + bytes[o] <= budget) {
-        desired[o] = 1;
-        used += bytes[o];
-      }
-    }
-    // toggles in index order, bounded by the toggle budget
-    uint32_t toggles = 0;
-    for (uint32_t o = 0; o < n; ++o) {
-      if (desired[o] == res[o]) continue;
-      if (maxToggles && toggles >= maxToggles) break;
-      res[o] = desired[o];
-      ++toggles;
-      long long s = slot[o];
-      int32_t ref = desired[o] ? blasRef[o] : kEmptyRef;
-      if (s >= 0) {
-        pnodeWords[(s / 2) * 16 + ((s & 1) ? 7 : 3)] = ref;
-      } else if (s == -1) {
-        misc[1] = 1;
-        misc[2] = desired[o];
-      }
-    }
-    misc[0] = toggles;
+    misc[0] = maxToggles == 0 ? total : min(total, maxToggles);
     misc[4] = misc[3];
     misc[3] = 0;
   }
@@ -433,7 +514,7 @@ extern "C" nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residen
   }
   uint32_t npow2 = 1;
   while (npow2 < N) npow2 <<= 1;
-  size_t smem = (size_t)npow2 * 8;
+  size_t smem = (size_t)npow2 * 10;  // sort keys, selected and candidate flags
   NOMAD_CUDA(ctx, cudaFuncSetAttribute(k_select, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   float motion = std::min(std::max(prm->camera_motion, 0.0f), 1.0f);
   uint32_t reserve = (uint32_t)std::min<double>(N, std::ceil(N * (prm->reserve_base + prm->reserve_motion * motion)));

@@ -494,7 +494,7 @@ nomad_status nomad_trace_variant(nomad_ctx *ctx, const nomad_traversal &cfg, boo
   if (n == 0) return NOMAD_OK;
   std::string why;
   if (!nomad_traversal_ok(ctx, cfg, &why)) return nomad_fail(ctx, NOMAD_ERR_UNSUPPORTED, why);
-  if (cfg.short_stack)
+  if (cfg.persistent == 2)
     return nomad_trace_regroup(ctx, cfg, any, rays, n, lenDev, cursor, hits5, occ, counts, st);
   return any ? dispatch<true>(ctx, cfg, rays, n, lenDev, cursor, hits5, occ, counts, st)
              : dispatch<false>(ctx, cfg, rays, n, lenDev, cursor, hits5, occ, counts, st);

@@ -1,4 +1,5 @@
-// Persistent-warp traversal with lane refill, a shared-memory short stack and staged top levels.
+// Regrouping traversal: persistent warps with lane refill, postponed leaves, a shared-memory short
+// stack and staged top levels.
 //
 // Same contract as the kernels in rt_core.cu (box test, primitive tests, tie rule, pruning
 // margin of rt_device.cuh; the wide walk of rt_wide.cuh), so every configuration returns the
@@ -15,8 +16,7 @@
 //     bulk asynchronous copies (cp.async.bulk, completion on an mbarrier; no multicast) and read
 //     from there. The wait is bounded: on expiry the block records the wait bit in the status
 //     word, waits once more (bounded) for its copy, and exits; other blocks take its rays.
-// Each iteration of the warp loop does one node step and, if the lane then stands on a leaf, the
-// leaf's primitive tests ("if-if" structure), so lanes at a leaf test their primitives together.
+//   * Postponed leaves (optional): see k_trace_rg.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -102,10 +102,11 @@ __device__ bool stage_nodes(unsigned char *smem, const float4 *src, uint32_t byt
   return false;
 }
 
-// Traversal stack: the newest SHORT entries in this thread's shared-memory column, older ones in
-// local memory. sp counts all entries, lo those spilled (indices [0, lo) are in `spill`).
+// Traversal stack. SHORT > 0: the newest SHORT entries in this thread's shared-memory column,
+// older ones in local memory (sp counts all entries, lo those spilled: indices [0, lo) are in
+// `spill`). SHORT == 0: every entry in local memory.
 template <int W, int SHORT>
-struct ShortStack {
+struct TravStack {
   using Entry = typename Lay<W>::Entry;
   static constexpr int STACK = Lay<W>::STACK;
   Entry *col;      // &ring[0][threadIdx.x]
@@ -113,26 +114,39 @@ struct ShortStack {
   int sp = 0, lo = 0;
   Entry spill[STACK];
 
-  __device__ __forceinline__ Entry &slot(int i) { return col[(uint32_t)(i & (SHORT - 1)) * pitch]; }
+  __device__ __forceinline__ Entry &slot(int i) { return col[(uint32_t)(i & (SHORT > 0 ? SHORT - 1 : 0)) * pitch]; }
   __device__ __forceinline__ void push(Entry e, uint32_t *status) {
     if (sp >= STACK) {
       atomicOr(status, kStatusStackOverflow);
       return;
     }
-    if (sp - lo == SHORT) {
-      spill[lo] = slot(lo);
-      ++lo;
+    if constexpr (SHORT == 0) {
+      spill[sp++] = e;
+    } else {
+      if (sp - lo == SHORT) {
+        spill[lo] = slot(lo);
+        ++lo;
+      }
+      slot(sp) = e;
+      ++sp;
     }
-    slot(sp) = e;
-    ++sp;
   }
   __device__ __forceinline__ Entry pop() {  // requires sp > 0
     --sp;
-    if (sp >= lo) return slot(sp);
-    lo = sp;
-    return spill[sp];
+    if constexpr (SHORT == 0) {
+      return spill[sp];
+    } else {
+      if (sp >= lo) return slot(sp);
+      lo = sp;
+      return spill[sp];
+    }
   }
 };
+
+constexpr int32_t kNoLeaf = INT32_MIN + 3;  // no postponed leaf
+
+// A leaf ref is ~first record; the values INT32_MIN .. INT32_MIN + 3 are sentinels.
+__device__ __forceinline__ bool is_leaf(int32_t r) { return r < 0 && r > kNoLeaf; }
 
 template <int F4>
 __device__ __forceinline__ float4 node_f4(const float4 *__restrict__ g, const float4 *s, int32_t ref, uint32_t staged,
@@ -141,7 +155,101 @@ __device__ __forceinline__ float4 node_f4(const float4 *__restrict__ g, const fl
   return __ldg(g + (size_t)ref * F4 + k);
 }
 
+// Next entry to visit from the stack, dropping wide entries whose box now starts beyond the best
+// hit; kFinished when the stack is empty.
 template <int W, int SHORT, bool ANY>
+__device__ __forceinline__ int32_t pop_next(TravStack<W, SHORT> &st, float bestT) {
+  while (st.sp > 0) {
+    const auto e = st.pop();
+    if constexpr (W == 2) {
+      return e;
+    } else {
+      if (!ANY && __int_as_float(e.y) > bestT * kPruneScale) continue;
+      return e.x;
+    }
+  }
+  return kFinished;
+}
+
+// One internal node: tests its children against the current bound, pushes all hit children but
+// the nearest and returns the nearest (or the next stack entry, or kFinished).
+template <int W, int SHORT, bool ANY>
+__device__ __forceinline__ int32_t node_step(const RayP &r, float tmax, float bestT, int32_t ref,
+                                             const float4 *__restrict__ nodes, const float4 *snodes, uint32_t staged,
+                                             TravStack<W, SHORT> &st, uint32_t *status) {
+  constexpr int F4 = Lay<W>::F4;
+  const float bound = ANY ? tmax : bestT * kPruneScale;
+  if constexpr (W == 2) {
+    const float4 a = node_f4<F4>(nodes, snodes, ref, staged, 0);
+    const float4 b = node_f4<F4>(nodes, snodes, ref, staged, 1);
+    const float4 c = node_f4<F4>(nodes, snodes, ref, staged, 2);
+    const float4 d = node_f4<F4>(nodes, snodes, ref, staged, 3);
+    const int32_t lref = __float_as_int(a.w), rref = __float_as_int(b.w);
+    float tl, tr;
+    const bool hl = slab(r, a.x, a.y, a.z, b.x, b.y, b.z, bound, tl) && lref != kEmptyRef;
+    const bool hr = slab(r, c.x, c.y, c.z, d.x, d.y, d.z, bound, tr) && rref != kEmptyRef;
+    if (hl && hr) {
+      const bool lf = !(tr < tl);
+      st.push(lf ? rref : lref, status);
+      return lf ? lref : rref;
+    }
+    if (hl) return lref;
+    if (hr) return rref;
+    return pop_next<W, SHORT, ANY>(st, bestT);
+  } else {
+    float t[W];
+    int32_t cc[W];
+#pragma unroll
+    for (int q = 0; q < W / 4; ++q) {
+      const float4 mnx = node_f4<F4>(nodes, snodes, ref, staged, 0 * (W / 4) + q);
+      const float4 mny = node_f4<F4>(nodes, snodes, ref, staged, 1 * (W / 4) + q);
+      const float4 mnz = node_f4<F4>(nodes, snodes, ref, staged, 2 * (W / 4) + q);
+      const float4 mxx = node_f4<F4>(nodes, snodes, ref, staged, 3 * (W / 4) + q);
+      const float4 mxy = node_f4<F4>(nodes, snodes, ref, staged, 4 * (W / 4) + q);
+      const float4 mxz = node_f4<F4>(nodes, snodes, ref, staged, 5 * (W / 4) + q);
+      const float4 rf = node_f4<F4>(nodes, snodes, ref, staged, 6 * (W / 4) + q);
+      const float ax[4] = {mnx.x, mnx.y, mnx.z, mnx.w}, ay[4] = {mny.x, mny.y, mny.z, mny.w};
+      const float az[4] = {mnz.x, mnz.y, mnz.z, mnz.w}, bx[4] = {mxx.x, mxx.y, mxx.z, mxx.w};
+      const float by[4] = {mxy.x, mxy.y, mxy.z, mxy.w}, bz[4] = {mxz.x, mxz.y, mxz.z, mxz.w};
+      const int32_t rr[4] = {__float_as_int(rf.x), __float_as_int(rf.y), __float_as_int(rf.z), __float_as_int(rf.w)};
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        float tk;
+        const bool hk = rr[k] != kEmptyRef && slab(r, ax[k], ay[k], az[k], bx[k], by[k], bz[k], bound, tk);
+        t[q * 4 + k] = hk ? tk : INFINITY;
+        cc[q * 4 + k] = hk ? rr[k] : kEmptyRef;
+      }
+    }
+    sort_children<W>(t, cc);
+    if (cc[0] == kEmptyRef) return pop_next<W, SHORT, ANY>(st, bestT);
+#pragma unroll
+    for (int k = W - 1; k >= 1; --k)
+      if (cc[k] != kEmptyRef) st.push(make_int2(cc[k], __float_as_int(t[k])), status);
+    return cc[0];
+  }
+}
+
+// Tests the records of one leaf; true when an any-hit query found an occluder.
+template <bool ANY>
+__device__ __forceinline__ bool leaf_step(const DevScene &S, const RayP &r, int32_t ref, HitRec &h) {
+  int64_t k = ~ref;
+  for (;;) {
+    const float4 *q = S.tri + 3 * k;
+    const float4 Av = __ldg(q), Bv = __ldg(q + 1), Cv = __ldg(q + 2);
+    const int32_t pid = __float_as_int(Av.w);
+    const int32_t meta = __float_as_int(Cv.w);
+    if (pid >= 0 && test_prim(S, r, Av, Bv, Cv, pid, meta & 0xff, h) && ANY) return true;
+    if (meta & kLastInLeaf) return false;
+    ++k;
+  }
+}
+
+// POST = false: every iteration of the warp loop does one node step and, when the lane then
+// stands on a leaf, that leaf ("if-if").
+// POST = true: postponed leaves ("while-while" with speculative descent, Aila & Laine, HPG 2009):
+// a lane that reaches its first leaf parks it and keeps descending while other lanes of the
+// warp are still looking for one; the warp then tests the parked leaves together.
+template <int W, int SHORT, bool ANY, bool POST>
 __global__ void __launch_bounds__(256) k_trace_rg(DevScene S, RgArgs A, const float4 *__restrict__ rays, uint64_t n,
                                                   const uint32_t *__restrict__ lenDev,
                                                   unsigned long long *__restrict__ cursor, int32_t *__restrict__ hits5,
@@ -154,9 +262,8 @@ __global__ void __launch_bounds__(256) k_trace_rg(DevScene S, RgArgs A, const fl
   if (staged) {
     if (!stage_nodes(smem, A.nodes, staged * (uint32_t)F4 * 16u, S.status)) return;
   }
-  Entry *ring = reinterpret_cast<Entry *>(smem + kStageHeader + (size_t)staged * F4 * 16) + threadIdx.x;
-  ShortStack<W, SHORT> st;
-  st.col = ring;
+  TravStack<W, SHORT> st;
+  st.col = reinterpret_cast<Entry *>(smem + kStageHeader + (size_t)staged * F4 * 16) + threadIdx.x;
   st.pitch = blockDim.x;
 
   const uint64_t N = lenDev ? (uint64_t)*lenDev : n;
@@ -224,103 +331,37 @@ __global__ void __launch_bounds__(256) k_trace_rg(DevScene S, RgArgs A, const fl
       if (__ballot_sync(0xffffffffu, ref != kIdle) == 0) break;  // no rays left anywhere
     }
 
-    // ---- one traversal step ----
+    // ---- traversal ----
     if (ref != kIdle && ref != kFinished) {
-      if (ref >= 0) {
-        if constexpr (W == 2) {
-          const float4 a = node_f4<F4>(A.nodes, snodes, ref, staged, 0);
-          const float4 b = node_f4<F4>(A.nodes, snodes, ref, staged, 1);
-          const float4 c = node_f4<F4>(A.nodes, snodes, ref, staged, 2);
-          const float4 d = node_f4<F4>(A.nodes, snodes, ref, staged, 3);
-          const int32_t lref = __float_as_int(a.w), rref = __float_as_int(b.w);
-          const float bound = ANY ? tmax : h.t * kPruneScale;
-          float tl, tr;
-          const bool hl = slab(r, a.x, a.y, a.z, b.x, b.y, b.z, bound, tl) && lref != kEmptyRef;
-          const bool hr = slab(r, c.x, c.y, c.z, d.x, d.y, d.z, bound, tr) && rref != kEmptyRef;
-          if (hl && hr) {
-            const bool lf = !(tr < tl);
-            st.push(lf ? rref : lref, S.status);
-            ref = lf ? lref : rref;
-          } else if (hl) {
-            ref = lref;
-          } else if (hr) {
-            ref = rref;
-          } else if (st.sp > 0) {
-            ref = st.pop();
-          } else {
-            ref = kFinished;
-          }
-        } else {
-          const float bound = ANY ? tmax : h.t * kPruneScale;
-          float t[W];
-          int32_t cc[W];
-#pragma unroll
-          for (int q = 0; q < W / 4; ++q) {
-            const float4 mnx = node_f4<F4>(A.nodes, snodes, ref, staged, 0 * (W / 4) + q);
-            const float4 mny = node_f4<F4>(A.nodes, snodes, ref, staged, 1 * (W / 4) + q);
-            const float4 mnz = node_f4<F4>(A.nodes, snodes, ref, staged, 2 * (W / 4) + q);
-            const float4 mxx = node_f4<F4>(A.nodes, snodes, ref, staged, 3 * (W / 4) + q);
-            const float4 mxy = node_f4<F4>(A.nodes, snodes, ref, staged, 4 * (W / 4) + q);
-            const float4 mxz = node_f4<F4>(A.nodes, snodes, ref, staged, 5 * (W / 4) + q);
-            const float4 rf = node_f4<F4>(A.nodes, snodes, ref, staged, 6 * (W / 4) + q);
-            const float ax[4] = {mnx.x, mnx.y, mnx.z, mnx.w}, ay[4] = {mny.x, mny.y, mny.z, mny.w};
-            const float az[4] = {mnz.x, mnz.y, mnz.z, mnz.w}, bx[4] = {mxx.x, mxx.y, mxx.z, mxx.w};
-            const float by[4] = {mxy.x, mxy.y, mxy.z, mxy.w}, bz[4] = {mxz.x, mxz.y, mxz.z, mxz.w};
-            const int32_t rr[4] = {__float_as_int(rf.x), __float_as_int(rf.y), __float_as_int(rf.z),
-                                   __float_as_int(rf.w)};
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-              float tk;
-              const bool hk = rr[k] != kEmptyRef && slab(r, ax[k], ay[k], az[k], bx[k], by[k], bz[k], bound, tk);
-              t[q * 4 + k] = hk ? tk : INFINITY;
-              cc[q * 4 + k] = hk ? rr[k] : kEmptyRef;
-            }
-          }
-          sort_children<W>(t, cc);
-          if (cc[0] != kEmptyRef) {
-#pragma unroll
-            for (int k = W - 1; k >= 1; --k) {
-              if (cc[k] != kEmptyRef) st.push(make_int2(cc[k], __float_as_int(t[k])), S.status);
-            }
-            ref = cc[0];
-          } else {
-            ref = kFinished;
-            while (st.sp > 0) {
-              const Entry e = st.pop();
-              if (!ANY && __int_as_float(e.y) > h.t * kPruneScale) continue;
-              ref = e.x;
-              break;
-            }
-          }
+      if constexpr (!POST) {
+        if (ref >= 0) ref = node_step<W, SHORT, ANY>(r, tmax, h.t, ref, A.nodes, snodes, staged, st, S.status);
+        if (is_leaf(ref)) {
+          const bool occl = leaf_step<ANY>(S, r, ref, h);
+          ref = (ANY && occl) ? kFinished : pop_next<W, SHORT, ANY>(st, h.t);
         }
-      }
-      if (ref < 0 && ref != kFinished) {
-        // Leaf: records ~ref up to the one flagged kLastInLeaf.
-        int64_t k = ~ref;
-        bool hitAny = false;
-        for (;;) {
-          const float4 *q = S.tri + 3 * k;
-          const float4 Av = __ldg(q), Bv = __ldg(q + 1), Cv = __ldg(q + 2);
-          const int32_t pid = __float_as_int(Av.w);
-          const int32_t meta = __float_as_int(Cv.w);
-          if (pid >= 0 && test_prim(S, r, Av, Bv, Cv, pid, meta & 0xff, h) && ANY) {
-            hitAny = true;
+      } else {
+        int32_t leaf = kNoLeaf;
+        if (is_leaf(ref)) {
+          leaf = ref;
+          ref = pop_next<W, SHORT, ANY>(st, h.t);
+        }
+        while (ref >= 0) {
+          ref = node_step<W, SHORT, ANY>(r, tmax, h.t, ref, A.nodes, snodes, staged, st, S.status);
+          if (is_leaf(ref) && leaf == kNoLeaf) {
+            leaf = ref;
+            ref = pop_next<W, SHORT, ANY>(st, h.t);
+          }
+          if (!__any_sync(__activemask(), leaf == kNoLeaf)) break;  // every lane here holds a leaf
+        }
+        while (leaf != kNoLeaf) {
+          if (leaf_step<ANY>(S, r, leaf, h) && ANY) {
+            ref = kFinished;
             break;
           }
-          if (meta & kLastInLeaf) break;
-          ++k;
-        }
-        ref = kFinished;
-        if (!hitAny) {
-          while (st.sp > 0) {
-            const Entry e = st.pop();
-            if constexpr (W == 2) {
-              ref = e;
-            } else {
-              if (!ANY && __int_as_float(e.y) > h.t * kPruneScale) continue;
-              ref = e.x;
-            }
-            break;
+          leaf = kNoLeaf;
+          if (is_leaf(ref)) {  // a second leaf was reached: test it too
+            leaf = ref;
+            ref = pop_next<W, SHORT, ANY>(st, h.t);
           }
         }
       }
@@ -364,12 +405,12 @@ __global__ void k_count_mismatch(const int32_t *__restrict__ a, const int32_t *_
   if ((threadIdx.x & 31) == 0 && m) atomicAdd(bad, (unsigned long long)__popc(m));
 }
 
-template <int W, int SHORT, bool ANY>
+template <int W, int SHORT, bool ANY, bool POST>
 nomad_status launch_rg(nomad_ctx *ctx, const nomad_traversal &cfg, const RgArgs &A, const float4 *rays, uint64_t n,
                        const uint32_t *lenDev, unsigned long long *cursor, int32_t *hits5, uint8_t *occ,
                        uint32_t *counts, cudaStream_t s) {
   using Entry = typename Lay<W>::Entry;
-  auto kern = k_trace_rg<W, SHORT, ANY>;
+  auto kern = k_trace_rg<W, SHORT, ANY, POST>;
   const uint32_t block = cfg.block ? cfg.block : 128u;
   const size_t smem = kStageHeader + (size_t)A.staged * Lay<W>::F4 * 16 + (size_t)SHORT * block * sizeof(Entry);
   if (smem > kMaxDynSmem) return nomad_fail(ctx, NOMAD_ERR_UNSUPPORTED, "staged nodes and short stack exceed shared memory");
@@ -384,16 +425,25 @@ nomad_status launch_rg(nomad_ctx *ctx, const nomad_traversal &cfg, const RgArgs 
   return NOMAD_OK;
 }
 
+template <int W, bool ANY, bool POST>
+nomad_status launch_s(nomad_ctx *ctx, const nomad_traversal &cfg, const RgArgs &A, const float4 *rays, uint64_t n,
+                      const uint32_t *lenDev, unsigned long long *cursor, int32_t *hits5, uint8_t *occ,
+                      uint32_t *counts, cudaStream_t s) {
+  switch (cfg.short_stack) {
+    case 0: return launch_rg<W, 0, ANY, POST>(ctx, cfg, A, rays, n, lenDev, cursor, hits5, occ, counts, s);
+    case 8: return launch_rg<W, 8, ANY, POST>(ctx, cfg, A, rays, n, lenDev, cursor, hits5, occ, counts, s);
+    case 16: return launch_rg<W, 16, ANY, POST>(ctx, cfg, A, rays, n, lenDev, cursor, hits5, occ, counts, s);
+    case 32: return launch_rg<W, 32, ANY, POST>(ctx, cfg, A, rays, n, lenDev, cursor, hits5, occ, counts, s);
+    default: return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "short stack must be 0, 8, 16 or 32");
+  }
+}
+
 template <int W, bool ANY>
 nomad_status launch_w(nomad_ctx *ctx, const nomad_traversal &cfg, const RgArgs &A, const float4 *rays, uint64_t n,
                       const uint32_t *lenDev, unsigned long long *cursor, int32_t *hits5, uint8_t *occ,
                       uint32_t *counts, cudaStream_t s) {
-  switch (cfg.short_stack) {
-    case 8: return launch_rg<W, 8, ANY>(ctx, cfg, A, rays, n, lenDev, cursor, hits5, occ, counts, s);
-    case 16: return launch_rg<W, 16, ANY>(ctx, cfg, A, rays, n, lenDev, cursor, hits5, occ, counts, s);
-    case 32: return launch_rg<W, 32, ANY>(ctx, cfg, A, rays, n, lenDev, cursor, hits5, occ, counts, s);
-    default: return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "short stack must be 8, 16 or 32");
-  }
+  return cfg.postpone_leaves ? launch_s<W, ANY, true>(ctx, cfg, A, rays, n, lenDev, cursor, hits5, occ, counts, s)
+                             : launch_s<W, ANY, false>(ctx, cfg, A, rays, n, lenDev, cursor, hits5, occ, counts, s);
 }
 
 uint32_t layout_nodes(const nomad_ctx *ctx, uint32_t width) {
@@ -407,29 +457,39 @@ uint32_t tlas_prefix(const nomad_ctx *ctx, uint32_t width) {
   return ctx->wide[width == 4 ? 0 : 1].tlasNodes;
 }
 
-}  // namespace
-
-// Raises the dynamic shared-memory limit of every short-stack kernel once, outside any stream
+// Raises the dynamic shared-memory limit of every regroup kernel once, outside any stream
 // capture (the frame graphs launch them while capturing).
-template <int W, int SHORT>
-cudaError_t opt_in_w() {
-  cudaError_t e = cudaFuncSetAttribute(k_trace_rg<W, SHORT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+template <int W, int SHORT, bool POST>
+cudaError_t opt_in_one() {
+  cudaError_t e = cudaFuncSetAttribute(k_trace_rg<W, SHORT, false, POST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)kMaxDynSmem);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_trace_rg<W, SHORT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxDynSmem);
+    e = cudaFuncSetAttribute(k_trace_rg<W, SHORT, true, POST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kMaxDynSmem);
   return e;
 }
 
+template <int W, bool POST>
+cudaError_t opt_in_w() {
+  cudaError_t e = cudaSuccess;
+  for (cudaError_t r : {opt_in_one<W, 0, POST>(), opt_in_one<W, 8, POST>(), opt_in_one<W, 16, POST>(),
+                        opt_in_one<W, 32, POST>()})
+    if (r != cudaSuccess) e = r;
+  return e;
+}
+
+}  // namespace
+
 cudaError_t nomad_regroup_init() {
   cudaError_t e = cudaSuccess;
-  for (cudaError_t r : {opt_in_w<2, 8>(), opt_in_w<2, 16>(), opt_in_w<2, 32>(), opt_in_w<4, 8>(), opt_in_w<4, 16>(),
-                        opt_in_w<4, 32>(), opt_in_w<8, 8>(), opt_in_w<8, 16>(), opt_in_w<8, 32>()})
+  for (cudaError_t r : {opt_in_w<2, false>(), opt_in_w<2, true>(), opt_in_w<4, false>(), opt_in_w<4, true>(),
+                        opt_in_w<8, false>(), opt_in_w<8, true>()})
     if (r != cudaSuccess) e = r;
   return e;
 }
 
 nomad_traversal nomad_kernel_config(uint32_t kernel) {
-  nomad_traversal c{2, 0, 0, 1, 0, 128};
+  nomad_traversal c{2, 0, 0, 1, 0, 128, 0};
   switch (kernel) {
     case NOMAD_KERNEL_BVH2_PERSIST: c.persistent = 1; break;
     case NOMAD_KERNEL_BVH4: c.width = 4; break;
@@ -448,12 +508,14 @@ bool nomad_traversal_ok(const nomad_ctx *ctx, const nomad_traversal &c, std::str
   };
   if (c.width != 2 && c.width != 4 && c.width != 8) return no("width must be 2, 4 or 8");
   if (c.block != 0 && c.block != 64 && c.block != 128 && c.block != 256) return no("block must be 64, 128 or 256");
-  if (c.short_stack != 0) {
-    if (c.short_stack != 8 && c.short_stack != 16 && c.short_stack != 32) return no("short stack must be 8, 16 or 32");
-    if (!c.persistent) return no("a short stack needs persistent warps");
+  if (c.persistent > 2) return no("persistent must be 0, 1 or 2");
+  if (c.persistent == 2) {
+    if (c.short_stack != 0 && c.short_stack != 8 && c.short_stack != 16 && c.short_stack != 32)
+      return no("short stack must be 0, 8, 16 or 32");
     if (c.regroup < 1 || c.regroup > 32) return no("regroup threshold must be 1..32");
-  } else if (c.staged_nodes != 0) {
-    return no("staged nodes need the short-stack kernel");
+    if (c.postpone_leaves > 1) return no("postpone_leaves must be 0 or 1");
+  } else if (c.short_stack != 0 || c.staged_nodes != 0 || c.postpone_leaves != 0) {
+    return no("short stack, staging and postponed leaves need the regrouping kernel (persistent = 2)");
   }
   if (!ctx->sceneReady) return true;
   const uint32_t wi = c.width == 2 ? 0 : (c.width == 4 ? 1 : 2);
@@ -539,12 +601,13 @@ extern "C" nomad_status nomad_autotune_sweep(nomad_ctx *ctx, const nomad_ray *ra
   for (uint32_t w : {2u, 4u, 8u}) {
     const uint32_t nodeBytes = w == 2 ? 64u : (w == 4 ? 128u : 256u);
     std::vector<uint32_t> stages{0u};
-    const uint32_t stage = std::min(tlas_prefix(ctx, w), (32u * 1024u) / nodeBytes);
+    const uint32_t stage = std::min(tlas_prefix(ctx, w), (8u * 1024u) / nodeBytes);
     if (stage) stages.push_back(stage);
-    for (uint32_t sh : {8u, 16u, 32u})
+    for (uint32_t sh : {0u, 8u, 16u, 32u})
       for (uint32_t rg : {1u, 16u, 24u, 32u})
-        for (uint32_t sn : stages)
-          for (uint32_t bl : {128u, 256u}) grid.push_back(nomad_traversal{w, 1, sh, rg, sn, bl});
+        for (uint32_t po : {0u, 1u})
+          for (uint32_t sn : stages)
+            for (uint32_t bl : {128u, 256u}) grid.push_back(nomad_traversal{w, 2, sh, rg, sn, bl, po});
   }
   DeviceBuf ref, cur, bad;
   NOMAD_CUDA(ctx, ref.reserve(n * 20));

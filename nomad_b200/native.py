@@ -128,17 +128,19 @@ class TuneResult(C.Structure):
 
 
 class Traversal(C.Structure):
-    """nomad_traversal: width, persistent, short_stack, regroup, staged_nodes, block."""
+    """nomad_traversal: width, persistent (0, 1, 2 = regrouping), short_stack, regroup,
+    staged_nodes, block, postpone_leaves."""
     _fields_ = [("width", C.c_uint32), ("persistent", C.c_uint32), ("short_stack", C.c_uint32),
-                ("regroup", C.c_uint32), ("staged_nodes", C.c_uint32), ("block", C.c_uint32)]
+                ("regroup", C.c_uint32), ("staged_nodes", C.c_uint32), ("block", C.c_uint32),
+                ("postpone_leaves", C.c_uint32)]
 
     def as_dict(self) -> dict:
         return {f: int(getattr(self, f)) for f, _ in self._fields_}
 
     def name(self) -> str:
-        if not self.short_stack:
+        if self.persistent < 2:
             return f"bvh{self.width}" + ("_persist" if self.persistent else "")
-        return (f"bvh{self.width}_ss{self.short_stack}_rg{self.regroup}"
+        return (f"bvh{self.width}_rg{self.regroup}_ss{self.short_stack}" + ("_post" if self.postpone_leaves else "")
                 + (f"_st{self.staged_nodes}" if self.staged_nodes else "") + f"_b{self.block}")
 
 
@@ -405,8 +407,9 @@ class Context:
     def set_kernel(self, k: int):
         self._ck(self.lib.nomad_set_kernel(self.h, k))
 
-    def set_traversal(self, width=2, persistent=1, short_stack=0, regroup=1, staged_nodes=0, block=128):
-        t = Traversal(width, persistent, short_stack, regroup, staged_nodes, block)
+    def set_traversal(self, width=2, persistent=2, short_stack=0, regroup=1, staged_nodes=0, block=128,
+                      postpone_leaves=0):
+        t = Traversal(width, persistent, short_stack, regroup, staged_nodes, block, postpone_leaves)
         self._ck(self.lib.nomad_set_traversal(self.h, C.byref(t)))
 
     def traversal(self) -> dict:
@@ -423,7 +426,7 @@ class Context:
         """Sweeps width x short stack x regroup threshold x staged top levels x block on the sample
         rays, checks each configuration bit for bit against the binary kernel and selects the
         fastest; returns {"best": cfg dict, "best_name", "entries": [(name, cfg, ms, mismatches)]}."""
-        cap = 512
+        cap = 1024
         entries = (TuneEntry * cap)()
         count = C.c_uint32(0)
         best = Traversal()

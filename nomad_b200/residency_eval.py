@@ -75,6 +75,19 @@ class Workload:
         self.budget_fraction = budget_fraction
         self.setup_s = time.perf_counter() - t0
 
+    def tune(self, ctx, judge=None):
+        """Autotunes the traversal on the primary rays of a path's first view; the judge context
+        gets the same configuration. Returns the configuration's name."""
+        from .rays import Camera
+
+        pos, look = camera_path(1, 2, *self.extent)[0]
+        cam = Camera(tuple(float(x) for x in pos), tuple(float(x) for x in look), width=self.width,
+                     height=self.height)
+        res = ctx.autotune_sweep(cam.primary_rays(self.spp, seed=3), repeats=2)
+        if judge is not None:
+            judge.set_traversal(**res["best"])
+        return res["best_name"]
+
     def context(self, device=0):
         c = nat.Context(device)
         c.upload(self.sb)
@@ -161,6 +174,8 @@ def run(paths=200, frames_per_path=8, steps=1500, frames=300, log=print):
     log(f"residency workload: {w.sb.prim_count} prims, {w.sb.object_count} objects, set-up {w.setup_s:.1f}s")
     ctx = w.context()
     judge = w.context()
+    traversal = w.tune(ctx, judge)
+    log(f"traversal: {traversal}")
     t1 = time.perf_counter()
     x, t = w.record(ctx, paths=paths, frames_per_path=frames_per_path)
     t2 = time.perf_counter()
@@ -171,6 +186,7 @@ def run(paths=200, frames_per_path=8, steps=1500, frames=300, log=print):
     out = {"workload": f"city {w.sb.object_count} objects / {w.sb.prim_count} prims, {frames}-frame path, "
                        f"{w.width}x{w.height} x {w.spp} spp, {w.depth} bounces, budget "
                        f"{int(100 * w.budget_fraction)}% of geometry bytes",
+           "traversal": traversal,
            "train": {"samples": int(x.shape[0]), "steps": steps, "loss_first": float(loss[:10].mean()),
                      "loss_last": float(loss[-50:].mean()), "record_s": t2 - t1, "train_s": t3 - t2}}
     for name, pol in (("always_resident", nat.POLICY_ALWAYS), ("ray_hit_budget", nat.POLICY_RAYHIT_BUDGET),

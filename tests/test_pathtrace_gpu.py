@@ -111,7 +111,8 @@ def test_frame_graph_replay(nb, orc, ctx, small_city):
             _compare(g, want)
     s1 = ctx.frame_graph_stats()
     assert s1["captures"] - s0["captures"] == 1 and s1["launches"] - s0["launches"] == 3, (s0, s1)
-    ctx.set_traversal(width=4, persistent=1, short_stack=16, regroup=24, staged_nodes=0, block=128)
+    ctx.set_traversal(width=4, persistent=2, short_stack=16, regroup=24, staged_nodes=0, block=128,
+                      postpone_leaves=1)
     v = views(5)
     g = np.concatenate([i.reshape(-1, 3) for i in ctx.render(v)])
     d = np.concatenate([i.reshape(-1, 3) for i in ctx.render(v, graph=False)])

@@ -182,23 +182,26 @@ def test_full_city_sample(nb, orc, ctx):
 # Short-stack persistent kernels: lane refill threshold, shared-memory short stack with local
 # spill, staged top levels. Every configuration must return the oracle's hits bit for bit.
 _RG_CONFIGS = [
-    dict(width=2, short_stack=8, regroup=1, staged=False, block=128),
-    dict(width=2, short_stack=16, regroup=32, staged=True, block=256),
-    dict(width=4, short_stack=8, regroup=16, staged=True, block=128),
-    dict(width=4, short_stack=32, regroup=24, staged=False, block=256),
-    dict(width=8, short_stack=8, regroup=32, staged=True, block=256),
-    dict(width=8, short_stack=16, regroup=1, staged=False, block=64),
+    dict(width=2, short_stack=8, regroup=1, staged=False, block=128, post=0),
+    dict(width=2, short_stack=0, regroup=24, staged=True, block=256, post=1),
+    dict(width=2, short_stack=16, regroup=32, staged=True, block=256, post=0),
+    dict(width=4, short_stack=8, regroup=16, staged=True, block=128, post=1),
+    dict(width=4, short_stack=32, regroup=24, staged=False, block=256, post=0),
+    dict(width=4, short_stack=0, regroup=32, staged=False, block=128, post=1),
+    dict(width=8, short_stack=8, regroup=32, staged=True, block=256, post=0),
+    dict(width=8, short_stack=16, regroup=1, staged=False, block=64, post=1),
 ]
 
 
 def _set_rg(ctx, c):
     tl = ctx.tlas_nodes()[{2: 0, 4: 1, 8: 2}[c["width"]]]
     cap = (32 * 1024) // {2: 64, 4: 128, 8: 256}[c["width"]]
-    ctx.set_traversal(width=c["width"], persistent=1, short_stack=c["short_stack"], regroup=c["regroup"],
-                      staged_nodes=min(tl, cap) if c["staged"] else 0, block=c["block"])
+    ctx.set_traversal(width=c["width"], persistent=2, short_stack=c["short_stack"], regroup=c["regroup"],
+                      staged_nodes=min(tl, cap) if c["staged"] else 0, block=c["block"],
+                      postpone_leaves=c["post"])
 
 
-@pytest.mark.parametrize("cfg", _RG_CONFIGS, ids=lambda c: "w{width}_ss{short_stack}_rg{regroup}_st{staged:d}_b{block}".format(**c))
+@pytest.mark.parametrize("cfg", _RG_CONFIGS, ids=lambda c: "w{width}_ss{short_stack}_rg{regroup}_st{staged:d}_b{block}_p{post}".format(**c))
 @pytest.mark.parametrize("which", ["ico", "city"])
 def test_regroup_parity(nb, orc, ctx, ico_scene, small_city, which, cfg):
     scene, sb = ico_scene if which == "ico" else small_city
@@ -228,7 +231,7 @@ def test_regroup_parity(nb, orc, ctx, ico_scene, small_city, which, cfg):
 def test_regroup_residency(nb, orc, ctx, small_city):
     scene, sb = small_city
     ctx.upload(sb)
-    _set_rg(ctx, dict(width=4, short_stack=16, regroup=24, staged=True, block=128))
+    _set_rg(ctx, dict(width=4, short_stack=16, regroup=24, staged=True, block=128, post=1))
     rays = _rays(sb, 150)
     rng = np.random.default_rng(19)
     off_objs = np.nonzero(rng.random(sb.object_count) < 0.4)[0]
@@ -253,7 +256,7 @@ def test_autotune_sweep(nb, orc, ctx, small_city):
     rays = _rays(sb, 160)
     res = ctx.autotune_sweep(rays, repeats=1)
     names = [e[0] for e in res["entries"]]
-    assert len(names) > 100 and len(set(names)) == len(names)
+    assert len(names) > 300 and len(set(names)) == len(names)
     assert all(e[3] == 0 for e in res["entries"] if e[2] >= 0), [e for e in res["entries"] if e[3]]
     assert {e[1]["width"] for e in res["entries"]} == {2, 4, 8}
     assert {e[1]["short_stack"] for e in res["entries"]} == {0, 8, 16, 32}
