@@ -399,7 +399,7 @@ def main():
                 "mismatching_configs": sum(1 for e in sweep["entries"] if e[3]),
                 "sample_rays": 2_000_000,
                 "fastest_ms": [[e[0], round(e[2], 4)] for e in rows[:10]],
-                "local_stack_ms": {e[0]: round(e[2], 4) for e in sweep["entries"] if e[1]["short_stack"] == 0},
+                "legacy_ms": {e[0]: round(e[2], 4) for e in sweep["entries"] if e[1]["persistent"] < 2},
                 "slowest_ms": [[e[0], round(e[2], 4)] for e in rows[-3:]]}
         log(f"autotune: {tune}")
 

@@ -163,6 +163,8 @@ typedef struct nomad_traversal {
   uint32_t staged_nodes;    /* persistent = 2: top-level nodes staged in shared memory         */
   uint32_t block;           /* threads per block: 0 (default 128), 64, 128, 256                */
   uint32_t postpone_leaves; /* persistent = 2: 1 = park the first leaf and keep descending     */
+  uint32_t min_blocks;      /* persistent = 0 or 1: resident blocks per SM the compiler must   */
+                            /* fit (0 = no bound; 10, 12 or 16 cap registers for occupancy)    */
 } nomad_traversal;
 nomad_status nomad_set_traversal(nomad_ctx *ctx, const nomad_traversal *cfg);
 nomad_status nomad_get_traversal(nomad_ctx *ctx, nomad_traversal *cfg);
@@ -175,7 +177,8 @@ typedef struct nomad_tune_entry {
   float ms;               /* best of `repeats` timings; negative when not run                  */
   uint32_t mismatches;    /* sample rays whose hit differs from the binary per-thread kernel's */
 } nomad_tune_entry;
-/* Sweeps the six NOMAD_KERNEL_* variants and, for the regrouping kernel, width {2,4,8} x short
+/* Sweeps the six NOMAD_KERNEL_* variants, each also with min_blocks 10, 12 and 16, and, for the
+ * regrouping kernel, width {2,4,8} x short
  * stack {0 (local), 8, 16, 32} x regroup threshold {1, 16, 24, 32} x postponed leaves {0, 1} x
  * staged top levels {0, up to 8 KB} x block {128, 256} on n sample rays, checks every
  * configuration against the binary kernel bit for bit, and selects the fastest one that agrees.

@@ -1,5 +1,7 @@
 // Learned residency scorer: MLP 24 -> 128 -> 128 -> 1 (ReLU), BF16 weights and activations,
-// FP32 accumulation on the tensor cores (mma.sync m16n8k16), trained on the device with AdamW.
+// FP32 accumulation on the tensor cores, trained on the device with AdamW. Inference (every
+// residency step) runs on tcgen05 with tensor-memory accumulators; training uses mma.sync
+// m16n8k16 kernels.
 //
 // The GEMMs are tiny (2,048 objects x 128 x 128 per frame), so the kernels are built for
 // latency: the forward pass is one fused kernel (both hidden layers and the output dot product
@@ -185,6 +187,191 @@ __global__ void __launch_bounds__(128) k_mlp_forward(const float *__restrict__ X
     uint64_t ra = row0 + wr + g, rb = ra + 8;
     if (ra < n) y[ra] = sa + sB3[0];
     if (rb < n) y[rb] = sb + sB3[0];
+  }
+}
+
+// ---- inference on the 5th-generation tensor cores (tcgen05) ---------------------------------
+// One CTA of 128 threads scores 128 rows. Both layers run as tcgen05.mma (kind::f16, BF16 inputs,
+// FP32 accumulators in tensor memory, M = 128, N = 128, K = 16 per instruction) issued by one
+// thread, with the operands in shared memory in the canonical K-major layout without swizzle:
+// 8 x 8 core matrices of 128 contiguous bytes, row groups 128 B apart (stride byte offset) and
+// 8-element K chunks (rows / 8) * 128 B apart (leading byte offset). Each thread then owns one
+// accumulator row (its tensor-memory lane) for the bias / ReLU epilogue and the final dot product.
+constexpr int kTcRows = 128;
+constexpr uint32_t kTcCols = 256;                   // tensor-memory columns: D1 [0,128), D2 [128,256)
+constexpr uint32_t kTcX = 0;                        // X tile, 128 x 32 bf16
+constexpr uint32_t kTcW1 = kTcX + 128 * kInPad * 2; // W1, 128 x 32
+constexpr uint32_t kTcH1 = kTcW1 + 128 * kInPad * 2;
+constexpr uint32_t kTcW2 = kTcH1 + 128 * kHid * 2;
+constexpr uint32_t kTcF = kTcW2 + 128 * kHid * 2;   // fp32: b1, b2, w3, b3, mean, istd
+constexpr uint32_t kTcBar = kTcF + 4 * (3 * kHid + 1 + 2 * kIn + 7);
+constexpr size_t kTcSmem = kTcBar + 16;
+constexpr uint32_t kStatusWaitExpired = 1u << 1;
+constexpr long long kTcWaitPolls = 1ll << 22;
+
+// Byte offset of element (r, k) of a 128-row K-major operand in the canonical layout.
+__device__ __forceinline__ uint32_t canon_off(int r, int k) {
+  return (uint32_t)((((k >> 3) * 16 + (r >> 3)) << 7) + ((r & 7) << 4) + ((k & 7) << 1));
+}
+
+// Shared-memory matrix descriptor: start, leading byte offset (next K chunk: 16 row groups of
+// 128 B), stride byte offset (next row group: 128 B), descriptor version 1, no swizzle.
+__device__ __forceinline__ uint64_t canon_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3fffu) | ((uint64_t)(2048u >> 4) << 16) | ((uint64_t)(128u >> 4) << 32) |
+         (1ull << 46);
+}
+
+// kind::f16 instruction descriptor: FP32 accumulator, BF16 A and B, both K-major, N = 128, M = 128.
+constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ void tc_mma(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(dtmem),
+      "l"(adesc), "l"(bdesc), "r"(kTcIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity) {
+  for (long long i = 0; i < kTcWaitPolls; ++i) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+// 32 consecutive accumulator columns of this thread's lane.
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+__global__ void __launch_bounds__(128) k_mlp_forward_tc(const float *__restrict__ X, uint64_t n,
+                                                        const float *__restrict__ P,
+                                                        const __nv_bfloat16 *__restrict__ W1b,
+                                                        const __nv_bfloat16 *__restrict__ W2b, float *__restrict__ y,
+                                                        uint32_t *__restrict__ status) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+  float *sB1 = reinterpret_cast<float *>(smem + kTcF);
+  float *sB2 = sB1 + kHid;
+  float *sW3 = sB2 + kHid;
+  float *sB3 = sW3 + kHid;
+  float *sMean = sB3 + 1;
+  float *sIstd = sMean + kIn;
+  const uint32_t bar = sbase + kTcBar;
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(smem + kTcBar + 8);
+  const int tid = threadIdx.x, warp = tid >> 5;
+
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sbase + kTcBar + 8),
+                 "r"(kTcCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  // operands: weights (bf16, already rounded) and the standardised X tile
+  for (int i = tid; i < kHid * kInPad; i += 128)
+    *reinterpret_cast<__nv_bfloat16 *>(smem + kTcW1 + canon_off(i / kInPad, i % kInPad)) = W1b[i];
+  for (int i = tid; i < kHid * kHid; i += 128)
+    *reinterpret_cast<__nv_bfloat16 *>(smem + kTcW2 + canon_off(i / kHid, i % kHid)) = W2b[i];
+  for (int i = tid; i < kHid; i += 128) {
+    sB1[i] = P[oB1 + i];
+    sB2[i] = P[oB2 + i];
+    sW3[i] = P[oW3 + i];
+  }
+  if (tid == 0) sB3[0] = P[oB3];
+  if (tid < kIn) {
+    sMean[tid] = P[oMean + tid];
+    sIstd[tid] = P[oIstd + tid];
+  }
+  __syncthreads();
+  const uint64_t row0 = (uint64_t)blockIdx.x * kTcRows;
+  for (int i = tid; i < kTcRows * kInPad; i += 128) {
+    const int r = i / kInPad, f = i % kInPad;
+    float v = 0.0f;
+    if (f < kIn && row0 + r < n) v = (X[(row0 + r) * kIn + f] - sMean[f]) * sIstd[f];
+    *reinterpret_cast<__nv_bfloat16 *>(smem + kTcX + canon_off(r, f)) = __float2bfloat16_rn(v);
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tslot;
+  const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+
+  // layer 1: D1 = X . W1^T, K = 32 in two steps
+  if (tid == 0) {
+#pragma unroll
+    for (int s = 0; s < kInPad / 16; ++s)
+      tc_mma(tmem, canon_desc(sbase + kTcX + s * 2 * 2048), canon_desc(sbase + kTcW1 + s * 2 * 2048), s > 0);
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+  }
+  bool ok = tc_wait(bar, 0);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  // epilogue 1: bias, ReLU, BF16 into the layer-2 operand (row = this thread's lane)
+  const int r = tid;
+#pragma unroll
+  for (int c0 = 0; c0 < kHid; c0 += 32) {
+    float v[32];
+    tc_ld32(lane_base + c0, v);
+#pragma unroll
+    for (int j = 0; j < 32; j += 2) {
+      const float a = fmaxf(v[j] + sB1[c0 + j], 0.0f), b = fmaxf(v[j + 1] + sB1[c0 + j + 1], 0.0f);
+      *reinterpret_cast<uint32_t *>(smem + kTcH1 + canon_off(r, c0 + j)) = pack_bf16(a, b);
+    }
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  // layer 2: D2 = H1 . W2^T, K = 128 in eight steps
+  if (tid == 0) {
+#pragma unroll
+    for (int s = 0; s < kHid / 16; ++s)
+      tc_mma(tmem + 128, canon_desc(sbase + kTcH1 + s * 2 * 2048), canon_desc(sbase + kTcW2 + s * 2 * 2048), s > 0);
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+  }
+  ok = tc_wait(bar, 1) && ok;
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  // epilogue 2: ReLU(D2 + b2) . w3 + b3 for this thread's row
+  float acc = 0.0f;
+#pragma unroll
+  for (int c0 = 0; c0 < kHid; c0 += 32) {
+    float v[32];
+    tc_ld32(lane_base + 128 + c0, v);
+#pragma unroll
+    for (int j = 0; j < 32; ++j) acc += fmaxf(v[j] + sB2[c0 + j], 0.0f) * sW3[c0 + j];
+  }
+  if (row0 + r < n) y[row0 + r] = ok ? acc + sB3[0] : 0.0f;
+  if (!ok && tid == 0) atomicOr(status, kStatusWaitExpired);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcCols) : "memory");
   }
 }
 
@@ -382,6 +569,7 @@ nomad_status ensure(nomad_ctx *ctx, MlpState &S) {
   static bool attr = false;
   if (!attr) {
     NOMAD_CUDA(ctx, cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwdSmem));
+    NOMAD_CUDA(ctx, cudaFuncSetAttribute(k_mlp_forward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
     attr = true;
   }
   return NOMAD_OK;
@@ -395,10 +583,9 @@ nomad_status nomad_mlp_infer_device(nomad_ctx *ctx, const float *X, uint64_t n, 
   MlpState &S = mlp(ctx);
   if (!S.ready) return nomad_fail(ctx, NOMAD_ERR_NOT_READY, "MLP not initialised or trained");
   if (n == 0) return NOMAD_OK;
-  unsigned blocks = (unsigned)((n + kFwdRows - 1) / kFwdRows);
-  k_mlp_forward<<<blocks, 128, kFwdSmem, ctx->stream>>>(X, n, S.P.as<const float>(), S.W1b.as<const __nv_bfloat16>(),
-                                                        S.W2b.as<const __nv_bfloat16>(), y, nullptr, nullptr,
-                                                        nullptr, nullptr);
+  const unsigned blocks = (unsigned)((n + kTcRows - 1) / kTcRows);
+  k_mlp_forward_tc<<<blocks, 128, kTcSmem, ctx->stream>>>(X, n, S.P.as<const float>(), S.W1b.as<const __nv_bfloat16>(),
+                                                          S.W2b.as<const __nv_bfloat16>(), y, ctx->status.as<uint32_t>());
   NOMAD_CUDA(ctx, cudaGetLastError());
   return NOMAD_OK;
 }

@@ -87,7 +87,7 @@ struct nomad_ctx {
   cudaStream_t ownStream = nullptr;
   cudaStream_t copyStreams[2] = {nullptr, nullptr};
   std::string err;
-  nomad_traversal trav{2, 0, 0, 1, 0, 128, 0};  // kernel configuration of the trace calls
+  nomad_traversal trav{2, 0, 0, 1, 0, 128, 0, 0};  // kernel configuration of the trace calls
   bool sceneReady = false;
   // scene sizes
   uint32_t primCount = 0, objectCount = 0;

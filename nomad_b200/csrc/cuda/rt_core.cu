@@ -72,8 +72,8 @@ __device__ __forceinline__ void trace_ray(const DevScene &S, const WideScene &WS
   }
 }
 
-template <int W, int STACK, bool ANY, bool PERSIST>
-__global__ void __launch_bounds__(kBlock) k_trace(DevScene S, WideScene WS, const float4 *__restrict__ rays,
+template <int W, int STACK, bool ANY, bool PERSIST, int MINB>
+__global__ void __launch_bounds__(kBlock, MINB) k_trace(DevScene S, WideScene WS, const float4 *__restrict__ rays,
                                                   uint64_t n, const uint32_t *__restrict__ lenDev,
                                                   unsigned long long *__restrict__ cursor,
                                                   int32_t *__restrict__ hits5, uint8_t *__restrict__ occ,
@@ -450,10 +450,10 @@ namespace {
 // Stack entries of each variant: pair nodes 64; 4-wide 64; 8-wide 96.
 constexpr int kStackW4 = 64, kStackW8 = 96;
 
-template <int W, int STACK, bool ANY, bool PERSIST>
+template <int W, int STACK, bool ANY, bool PERSIST, int MINB>
 nomad_status launch_one(nomad_ctx *ctx, const WideScene &WS, const float4 *rays, uint64_t n, const uint32_t *lenDev,
                         unsigned long long *cursor, int32_t *hits5, uint8_t *occ, uint32_t *counts, cudaStream_t st) {
-  auto kern = k_trace<W, STACK, ANY, PERSIST>;
+  auto kern = k_trace<W, STACK, ANY, PERSIST, MINB>;
   uint64_t blocks;
   if (PERSIST) {
     int perSm = 0;
@@ -470,18 +470,32 @@ nomad_status launch_one(nomad_ctx *ctx, const WideScene &WS, const float4 *rays,
   return NOMAD_OK;
 }
 
+template <int W, int STACK, bool ANY, bool PERSIST>
+nomad_status launch_minb(nomad_ctx *ctx, uint32_t minBlocks, const WideScene &WS, const float4 *rays, uint64_t n,
+                         const uint32_t *lenDev, unsigned long long *cursor, int32_t *hits5, uint8_t *occ,
+                         uint32_t *counts, cudaStream_t st) {
+  switch (minBlocks) {
+    case 0: return launch_one<W, STACK, ANY, PERSIST, 1>(ctx, WS, rays, n, lenDev, cursor, hits5, occ, counts, st);
+    case 10: return launch_one<W, STACK, ANY, PERSIST, 10>(ctx, WS, rays, n, lenDev, cursor, hits5, occ, counts, st);
+    case 12: return launch_one<W, STACK, ANY, PERSIST, 12>(ctx, WS, rays, n, lenDev, cursor, hits5, occ, counts, st);
+    case 16: return launch_one<W, STACK, ANY, PERSIST, 16>(ctx, WS, rays, n, lenDev, cursor, hits5, occ, counts, st);
+    default: return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "min_blocks must be 0, 10, 12 or 16");
+  }
+}
+
 template <bool ANY>
 nomad_status dispatch(nomad_ctx *ctx, const nomad_traversal &c, const float4 *rays, uint64_t n, const uint32_t *lenDev,
                       unsigned long long *cursor, int32_t *hits5, uint8_t *occ, uint32_t *counts, cudaStream_t st) {
   const WideScene none{nullptr, kEmptyRef};
   const bool p = c.persistent != 0;
+  const uint32_t mb = c.min_blocks;
   switch (c.width) {
-    case 2: return p ? launch_one<2, kStack, ANY, true>(ctx, none, rays, n, lenDev, cursor, hits5, occ, counts, st)
-                     : launch_one<2, kStack, ANY, false>(ctx, none, rays, n, lenDev, cursor, hits5, occ, counts, st);
-    case 4: return p ? launch_one<4, kStackW4, ANY, true>(ctx, ctx->ws[0], rays, n, lenDev, cursor, hits5, occ, counts, st)
-                     : launch_one<4, kStackW4, ANY, false>(ctx, ctx->ws[0], rays, n, lenDev, cursor, hits5, occ, counts, st);
-    case 8: return p ? launch_one<8, kStackW8, ANY, true>(ctx, ctx->ws[1], rays, n, lenDev, cursor, hits5, occ, counts, st)
-                     : launch_one<8, kStackW8, ANY, false>(ctx, ctx->ws[1], rays, n, lenDev, cursor, hits5, occ, counts, st);
+    case 2: return p ? launch_minb<2, kStack, ANY, true>(ctx, mb, none, rays, n, lenDev, cursor, hits5, occ, counts, st)
+                     : launch_minb<2, kStack, ANY, false>(ctx, mb, none, rays, n, lenDev, cursor, hits5, occ, counts, st);
+    case 4: return p ? launch_minb<4, kStackW4, ANY, true>(ctx, mb, ctx->ws[0], rays, n, lenDev, cursor, hits5, occ, counts, st)
+                     : launch_minb<4, kStackW4, ANY, false>(ctx, mb, ctx->ws[0], rays, n, lenDev, cursor, hits5, occ, counts, st);
+    case 8: return p ? launch_minb<8, kStackW8, ANY, true>(ctx, mb, ctx->ws[1], rays, n, lenDev, cursor, hits5, occ, counts, st)
+                     : launch_minb<8, kStackW8, ANY, false>(ctx, mb, ctx->ws[1], rays, n, lenDev, cursor, hits5, occ, counts, st);
     default: return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "unknown kernel variant");
   }
 }

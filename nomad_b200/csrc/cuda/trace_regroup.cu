@@ -489,7 +489,7 @@ cudaError_t nomad_regroup_init() {
 }
 
 nomad_traversal nomad_kernel_config(uint32_t kernel) {
-  nomad_traversal c{2, 0, 0, 1, 0, 128, 0};
+  nomad_traversal c{2, 0, 0, 1, 0, 128, 0, 0};
   switch (kernel) {
     case NOMAD_KERNEL_BVH2_PERSIST: c.persistent = 1; break;
     case NOMAD_KERNEL_BVH4: c.width = 4; break;
@@ -514,8 +514,12 @@ bool nomad_traversal_ok(const nomad_ctx *ctx, const nomad_traversal &c, std::str
       return no("short stack must be 0, 8, 16 or 32");
     if (c.regroup < 1 || c.regroup > 32) return no("regroup threshold must be 1..32");
     if (c.postpone_leaves > 1) return no("postpone_leaves must be 0 or 1");
-  } else if (c.short_stack != 0 || c.staged_nodes != 0 || c.postpone_leaves != 0) {
-    return no("short stack, staging and postponed leaves need the regrouping kernel (persistent = 2)");
+    if (c.min_blocks != 0) return no("min_blocks applies to persistent = 0 or 1");
+  } else {
+    if (c.short_stack != 0 || c.staged_nodes != 0 || c.postpone_leaves != 0)
+      return no("short stack, staging and postponed leaves need the regrouping kernel (persistent = 2)");
+    if (c.min_blocks != 0 && c.min_blocks != 10 && c.min_blocks != 12 && c.min_blocks != 16)
+      return no("min_blocks must be 0, 10, 12 or 16");
   }
   if (!ctx->sceneReady) return true;
   const uint32_t wi = c.width == 2 ? 0 : (c.width == 4 ? 1 : 2);
@@ -598,6 +602,12 @@ extern "C" nomad_status nomad_autotune_sweep(nomad_ctx *ctx, const nomad_ray *ra
   // The grid: the six local-stack kernels, then every short-stack combination.
   std::vector<nomad_traversal> grid;
   for (uint32_t k = NOMAD_KERNEL_BVH2; k < NOMAD_KERNEL_COUNT; ++k) grid.push_back(nomad_kernel_config(k));
+  for (uint32_t k = NOMAD_KERNEL_BVH2; k < NOMAD_KERNEL_COUNT; ++k)
+    for (uint32_t mb : {10u, 12u, 16u}) {
+      nomad_traversal c = nomad_kernel_config(k);
+      c.min_blocks = mb;
+      grid.push_back(c);
+    }
   for (uint32_t w : {2u, 4u, 8u}) {
     const uint32_t nodeBytes = w == 2 ? 64u : (w == 4 ? 128u : 256u);
     std::vector<uint32_t> stages{0u};
@@ -607,7 +617,7 @@ extern "C" nomad_status nomad_autotune_sweep(nomad_ctx *ctx, const nomad_ray *ra
       for (uint32_t rg : {1u, 16u, 24u, 32u})
         for (uint32_t po : {0u, 1u})
           for (uint32_t sn : stages)
-            for (uint32_t bl : {128u, 256u}) grid.push_back(nomad_traversal{w, 2, sh, rg, sn, bl, po});
+            for (uint32_t bl : {128u, 256u}) grid.push_back(nomad_traversal{w, 2, sh, rg, sn, bl, po, 0});
   }
   DeviceBuf ref, cur, bad;
   NOMAD_CUDA(ctx, ref.reserve(n * 20));

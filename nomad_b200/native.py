@@ -132,14 +132,15 @@ class Traversal(C.Structure):
     staged_nodes, block, postpone_leaves."""
     _fields_ = [("width", C.c_uint32), ("persistent", C.c_uint32), ("short_stack", C.c_uint32),
                 ("regroup", C.c_uint32), ("staged_nodes", C.c_uint32), ("block", C.c_uint32),
-                ("postpone_leaves", C.c_uint32)]
+                ("postpone_leaves", C.c_uint32), ("min_blocks", C.c_uint32)]
 
     def as_dict(self) -> dict:
         return {f: int(getattr(self, f)) for f, _ in self._fields_}
 
     def name(self) -> str:
         if self.persistent < 2:
-            return f"bvh{self.width}" + ("_persist" if self.persistent else "")
+            return (f"bvh{self.width}" + ("_persist" if self.persistent else "")
+                    + (f"_mb{self.min_blocks}" if self.min_blocks else ""))
         return (f"bvh{self.width}_rg{self.regroup}_ss{self.short_stack}" + ("_post" if self.postpone_leaves else "")
                 + (f"_st{self.staged_nodes}" if self.staged_nodes else "") + f"_b{self.block}")
 
@@ -408,8 +409,8 @@ class Context:
         self._ck(self.lib.nomad_set_kernel(self.h, k))
 
     def set_traversal(self, width=2, persistent=2, short_stack=0, regroup=1, staged_nodes=0, block=128,
-                      postpone_leaves=0):
-        t = Traversal(width, persistent, short_stack, regroup, staged_nodes, block, postpone_leaves)
+                      postpone_leaves=0, min_blocks=0):
+        t = Traversal(width, persistent, short_stack, regroup, staged_nodes, block, postpone_leaves, min_blocks)
         self._ck(self.lib.nomad_set_traversal(self.h, C.byref(t)))
 
     def traversal(self) -> dict:

@@ -37,6 +37,8 @@ def test_mlp_forward_matches_restatement(nb, ctx, small_city):
     want = ores.mlp_forward(ctx.mlp_get(), x)
     err = np.abs(got - want) / (1.0 + np.abs(want))
     assert err.max() < 1e-3, err.max()
+    # tensor-memory waits of the tcgen05 inference kernel all completed
+    assert ctx.status() == 0
 
 
 def test_mlp_training(nb, ctx, small_city):
