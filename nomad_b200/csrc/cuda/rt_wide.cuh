@@ -115,20 +115,8 @@ __device__ __forceinline__ void traverse_wide(const DevScene &S, const WideScene
         continue;
       }
     } else if (ref != kEmptyRef) {
-      int64_t k = ~ref;
-      for (;;) {
-        const float4 *q = S.tri + 3 * k;
-        float4 A = ldg4(q), B = ldg4(q + 1), C = ldg4(q + 2);
-        int32_t pid = __float_as_int(A.w);
-        int32_t meta = __float_as_int(C.w);
-        if (pid >= 0 && test_prim(S, r, A, B, C, pid, meta & 0xff, h) && ANY) {
-          done = true;
-          break;
-        }
-        if (meta & kLastInLeaf) break;
-        ++k;
-      }
-      if (done) break;
+      Work w{0, 0, 0};
+      if (leaf_walk<ANY, false>(S, r, ~(int64_t)ref, h, w)) break;
     }
     // pop, dropping entries that now start beyond the best hit
     ref = kEmptyRef;

@@ -232,16 +232,8 @@ __device__ __forceinline__ int32_t node_step(const RayP &r, float tmax, float be
 // Tests the records of one leaf; true when an any-hit query found an occluder.
 template <bool ANY>
 __device__ __forceinline__ bool leaf_step(const DevScene &S, const RayP &r, int32_t ref, HitRec &h) {
-  int64_t k = ~ref;
-  for (;;) {
-    const float4 *q = S.tri + 3 * k;
-    const float4 Av = __ldg(q), Bv = __ldg(q + 1), Cv = __ldg(q + 2);
-    const int32_t pid = __float_as_int(Av.w);
-    const int32_t meta = __float_as_int(Cv.w);
-    if (pid >= 0 && test_prim(S, r, Av, Bv, Cv, pid, meta & 0xff, h) && ANY) return true;
-    if (meta & kLastInLeaf) return false;
-    ++k;
-  }
+  Work w{0, 0, 0};
+  return leaf_walk<ANY, false>(S, r, ~(int64_t)ref, h, w);
 }
 
 // POST = false: every iteration of the warp loop does one node step and, when the lane then
