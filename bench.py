@@ -114,6 +114,26 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+TRAFFIC_PROFILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles",
+                               "launches_bench_city1080_bvh4_persist.md")
+
+
+def measured_traffic():
+    """Per-launch DRAM bytes (read + write) of the primary and bounce launches, as measured by ncu
+    on this workload and recorded in the profile summary; None when the summary is absent."""
+    try:
+        vals = {}
+        with open(TRAFFIC_PROFILE) as f:
+            for line in f:
+                for key in ("primary", "bounce"):
+                    tag = f"traffic_{key}_bytes:"
+                    if line.strip().startswith(tag):
+                        vals[key] = int(line.strip()[len(tag):].strip().strip("`"))
+        return vals if len(vals) == 2 else None
+    except OSError:
+        return None
+
+
 def build_workload(nb, spp=SPP):
     scene = nb.synth_city(seed=SEED)
     sb = nb.SceneBVH(scene)
@@ -511,8 +531,13 @@ def main():
 
     peak, peak_kind = measured_peaks()
     achieved = (bytes_prim + bytes_b) / ((t_prim + t_b) / 1e3) / 1e9
+    traffic = measured_traffic()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": None,
+                "frac": achieved / peak,
+                # DRAM bytes of the step's two launches (primary + bounce), the launches `achieved`
+                # covers; from the ncu capture summarised in profiles/
+                "traffic": (traffic["primary"] + traffic["bounce"]) if traffic else None,
+                "traffic_per_launch": traffic,
                 "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": {"primary": bytes_prim, "bounce": bytes_b},
                 "kernel_ms": {"primary": t_prim, "bounce": t_b}}

@@ -59,19 +59,6 @@ __device__ __forceinline__ RayP prep_ray(float4 a, float4 b) {
   return r;
 }
 
-// Three-input minimum / maximum (one instruction on sm_100). Inputs here are never NaN: the fast
-// slab path below only runs when no direction component is below kRayEps, so 1/d is finite.
-__device__ __forceinline__ float max3f(float a, float b, float c) {
-  float d;
-  asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
-  return d;
-}
-__device__ __forceinline__ float min3f(float a, float b, float c) {
-  float d;
-  asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
-  return d;
-}
-
 // intersectAABB over [kRayEps, bound]; returns the entry distance in tnear.
 __device__ __forceinline__ bool slab(const RayP &r, float mnx, float mny, float mnz, float mxx,
                                      float mxy, float mxz, float bound, float &tnear) {
@@ -80,8 +67,8 @@ __device__ __forceinline__ bool slab(const RayP &r, float mnx, float mny, float 
     float t0 = (mnx - r.ox) * r.ix, t1 = (mxx - r.ox) * r.ix;
     float u0 = (mny - r.oy) * r.iy, u1 = (mxy - r.oy) * r.iy;
     float w0 = (mnz - r.oz) * r.iz, w1 = (mxz - r.oz) * r.iz;
-    tn = max3f(fminf(t0, t1), fminf(u0, u1), fmaxf(fminf(w0, w1), tn));
-    tf = min3f(fmaxf(t0, t1), fmaxf(u0, u1), fminf(fmaxf(w0, w1), tf));
+    tn = fmaxf(fmaxf(fminf(t0, t1), fminf(u0, u1)), fmaxf(fminf(w0, w1), tn));
+    tf = fminf(fminf(fmaxf(t0, t1), fmaxf(u0, u1)), fminf(fmaxf(w0, w1), tf));
   } else {
     bool ok = true;
     if (r.par & 1) {
@@ -198,30 +185,19 @@ struct Work {
   uint32_t nodes, tests, insts;
 };
 
-// Tests the records of one leaf, from `k` to the one flagged kLastInLeaf. The next record's
-// loads are issued before the current record is tested (only when the current one is not the
-// last, so they stay inside the leaf). Returns true when an any-hit query found an occluder.
+// Tests the records of one leaf, from `k` to the one flagged kLastInLeaf. Returns true when an
+// any-hit query found an occluder.
 template <bool ANY, bool WORK>
 __device__ __forceinline__ bool leaf_walk(const DevScene &S, const RayP &r, int64_t k, HitRec &h, Work &w) {
-  const float4 *q = S.tri + 3 * k;
-  float4 A = ldg4(q), B = ldg4(q + 1), C = ldg4(q + 2);
   for (;;) {
-    const int32_t meta = __float_as_int(C.w);
-    const bool last = (meta & kLastInLeaf) != 0;
-    float4 An = A, Bn = B, Cn = C;
-    if (!last) {
-      q += 3;
-      An = ldg4(q);
-      Bn = ldg4(q + 1);
-      Cn = ldg4(q + 2);
-    }
+    const float4 *q = S.tri + 3 * k;
+    const float4 A = ldg4(q), B = ldg4(q + 1), C = ldg4(q + 2);
     const int32_t pid = __float_as_int(A.w);
+    const int32_t meta = __float_as_int(C.w);
     if (WORK) w.tests += 1;
     if (pid >= 0 && test_prim(S, r, A, B, C, pid, meta & 0xff, h) && ANY) return true;
-    if (last) return false;
-    A = An;
-    B = Bn;
-    C = Cn;
+    if (meta & kLastInLeaf) return false;
+    ++k;
   }
 }
 
