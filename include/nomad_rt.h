@@ -154,10 +154,14 @@ nomad_status nomad_set_kernel(nomad_ctx *ctx, uint32_t kernel);
  *     other lanes of the warp still look for one, then test the parked leaves together;
  *   - copy the first `staged_nodes` nodes of the layout (the TLAS top levels, numbered
  *     breadth-first) into shared memory with bulk asynchronous copies and read them from there.
+ * persistent = 3 selects the hybrid packet kernel: a warp whose 32 rays share an origin and lie in
+ * a narrow cone (primary rays) walks the tree as one packet, visiting a node when any lane's ray
+ * hits it, with broadcast node and triangle loads; other warps walk per ray.
  * Every configuration returns the same hits bit for bit. */
 typedef struct nomad_traversal {
   uint32_t width;           /* 2 (pair nodes), 4 or 8                                          */
-  uint32_t persistent;      /* 0: one ray per thread; 1: persistent warps; 2: regrouping warps */
+  uint32_t persistent;      /* 0: one ray per thread; 1: persistent warps; 2: regrouping warps; */
+                            /* 3: hybrid packets (coherent warps walk as one packet)          */
   uint32_t short_stack;     /* persistent = 2: 0 (local memory), 8, 16 or 32                   */
   uint32_t regroup;         /* persistent = 2: refill threshold in busy lanes, 1..32           */
   uint32_t staged_nodes;    /* persistent = 2: top-level nodes staged in shared memory         */
@@ -177,8 +181,8 @@ typedef struct nomad_tune_entry {
   float ms;               /* best of `repeats` timings; negative when not run                  */
   uint32_t mismatches;    /* sample rays whose hit differs from the binary per-thread kernel's */
 } nomad_tune_entry;
-/* Sweeps the six NOMAD_KERNEL_* variants, each also with min_blocks 10, 12 and 16, and, for the
- * regrouping kernel, width {2,4,8} x short
+/* Sweeps the six NOMAD_KERNEL_* variants, each also with min_blocks 10, 12 and 16, the hybrid
+ * packet kernel at widths 2, 4, 8, and, for the regrouping kernel, width {2,4,8} x short
  * stack {0 (local), 8, 16, 32} x regroup threshold {1, 16, 24, 32} x postponed leaves {0, 1} x
  * staged top levels {0, up to 8 KB} x block {128, 256} on n sample rays, checks every
  * configuration against the binary kernel bit for bit, and selects the fastest one that agrees.

@@ -167,6 +167,10 @@ nomad_status nomad_trace_regroup(nomad_ctx *ctx, const nomad_traversal &cfg, boo
                                  uint32_t *counts, cudaStream_t s);
 // Opts the short-stack kernels in to large dynamic shared memory (once per context creation).
 cudaError_t nomad_regroup_init();
+// The hybrid packet kernels (trace_packet.cu).
+nomad_status nomad_trace_packet(nomad_ctx *ctx, const nomad_traversal &cfg, bool any, const float4 *rays, uint64_t n,
+                                const uint32_t *lenDev, unsigned long long *cursor, int32_t *hits5, uint8_t *occ,
+                                uint32_t *counts, cudaStream_t s);
 // NOMAD_KERNEL_* as a traversal configuration.
 nomad_traversal nomad_kernel_config(uint32_t kernel);
 // Whether `cfg` is valid and can run on the uploaded scene (stack depth, layout sizes).

@@ -510,6 +510,8 @@ nomad_status nomad_trace_variant(nomad_ctx *ctx, const nomad_traversal &cfg, boo
   if (!nomad_traversal_ok(ctx, cfg, &why)) return nomad_fail(ctx, NOMAD_ERR_UNSUPPORTED, why);
   if (cfg.persistent == 2)
     return nomad_trace_regroup(ctx, cfg, any, rays, n, lenDev, cursor, hits5, occ, counts, st);
+  if (cfg.persistent == 3)
+    return nomad_trace_packet(ctx, cfg, any, rays, n, lenDev, cursor, hits5, occ, counts, st);
   return any ? dispatch<true>(ctx, cfg, rays, n, lenDev, cursor, hits5, occ, counts, st)
              : dispatch<false>(ctx, cfg, rays, n, lenDev, cursor, hits5, occ, counts, st);
 }
@@ -552,38 +554,67 @@ nomad_status launch(nomad_ctx *ctx, Op op, const float4 *rays, uint64_t n, void 
 
 // Host-pointer path: rays are copied in and results out in chunks, alternating two streams
 // so one chunk's copies overlap another chunk's traversal.
+// Host buffers: the batch is split into chunks; uploads run back to back on one copy stream,
+// each chunk's kernel on the context stream once its upload landed, and each chunk's download on
+// a second copy stream once its kernel finished, so both copy directions and the traversal
+// overlap.
 nomad_status trace_host(nomad_ctx *ctx, Op op, const nomad_ray *rays, uint64_t n, void *out,
                         size_t outStride, bool countHits) {
   NOMAD_CUDA(ctx, ctx->stageIn.reserve(n * sizeof(nomad_ray)));
   NOMAD_CUDA(ctx, ctx->stageOut.reserve(n * outStride));
-  const uint64_t chunk = std::max<uint64_t>(1 << 20, (n + 7) / 8);
+  const uint64_t chunk = std::max<uint64_t>(1 << 19, (n + 15) / 16);
+  cudaStream_t sIn = ctx->copyStreams[0], sOut = ctx->copyStreams[1], sK = ctx->stream;
+  std::vector<cudaEvent_t> evs;
+  auto event = [&](cudaEvent_t *e) -> cudaError_t {
+    cudaError_t r = cudaEventCreateWithFlags(e, cudaEventDisableTiming);
+    if (r == cudaSuccess) evs.push_back(*e);
+    return r;
+  };
+  auto cleanup = [&]() {
+    for (cudaEvent_t e : evs) cudaEventDestroy(e);
+  };
+  nomad_status st = NOMAD_OK;
   cudaEvent_t start;
-  NOMAD_CUDA(ctx, cudaEventCreateWithFlags(&start, cudaEventDisableTiming));
-  NOMAD_CUDA(ctx, cudaEventRecord(start, ctx->stream));
-  std::vector<cudaEvent_t> done;
-  int k = 0;
-  for (uint64_t off = 0; off < n; off += chunk, ++k) {
-    uint64_t m = std::min(chunk, n - off);
-    cudaStream_t s = ctx->copyStreams[k & 1];
-    cudaStreamWaitEvent(s, start, 0);
+  if (event(&start) != cudaSuccess || cudaEventRecord(start, sK) != cudaSuccess ||
+      cudaStreamWaitEvent(sIn, start, 0) != cudaSuccess)
+    st = fail(ctx, NOMAD_ERR_CUDA, "stream setup");
+  // Uploads and kernels first, downloads second: a copy to or from pageable host memory returns
+  // only once it is done, so issuing a download before the next upload would serialise them.
+  std::vector<cudaEvent_t> traced;
+  for (uint64_t off = 0; off < n && st == NOMAD_OK; off += chunk) {
+    const uint64_t m = std::min(chunk, n - off);
     char *din = static_cast<char *>(ctx->stageIn.p) + off * sizeof(nomad_ray);
     char *dout = static_cast<char *>(ctx->stageOut.p) + off * outStride;
-    NOMAD_CUDA(ctx, cudaMemcpyAsync(din, rays + off, m * sizeof(nomad_ray), cudaMemcpyHostToDevice, s));
-    nomad_status st = launch(ctx, op, reinterpret_cast<const float4 *>(din), m, dout, countHits, s, 1 + (k & 1));
-    if (st != NOMAD_OK) return st;
-    NOMAD_CUDA(ctx, cudaMemcpyAsync(static_cast<char *>(out) + off * outStride, dout, m * outStride,
-                                    cudaMemcpyDeviceToHost, s));
-    cudaEvent_t ev;
-    NOMAD_CUDA(ctx, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-    NOMAD_CUDA(ctx, cudaEventRecord(ev, s));
-    done.push_back(ev);
+    cudaEvent_t up, done;
+    if (event(&up) != cudaSuccess || event(&done) != cudaSuccess ||
+        cudaMemcpyAsync(din, rays + off, m * sizeof(nomad_ray), cudaMemcpyHostToDevice, sIn) != cudaSuccess ||
+        cudaEventRecord(up, sIn) != cudaSuccess || cudaStreamWaitEvent(sK, up, 0) != cudaSuccess) {
+      st = fail(ctx, NOMAD_ERR_CUDA, "chunk upload");
+      break;
+    }
+    st = launch(ctx, op, reinterpret_cast<const float4 *>(din), m, dout, countHits, sK, 0);
+    if (st != NOMAD_OK) break;
+    if (cudaEventRecord(done, sK) != cudaSuccess) {
+      st = fail(ctx, NOMAD_ERR_CUDA, "chunk event");
+      break;
+    }
+    traced.push_back(done);
   }
-  for (auto ev : done) {
-    cudaStreamWaitEvent(ctx->stream, ev, 0);
-    cudaEventDestroy(ev);
+  for (size_t k = 0; k < traced.size() && st == NOMAD_OK; ++k) {
+    const uint64_t off = k * chunk, m = std::min(chunk, n - off);
+    if (cudaStreamWaitEvent(sOut, traced[k], 0) != cudaSuccess ||
+        cudaMemcpyAsync(static_cast<char *>(out) + off * outStride,
+                        static_cast<char *>(ctx->stageOut.p) + off * outStride, m * outStride,
+                        cudaMemcpyDeviceToHost, sOut) != cudaSuccess)
+      st = fail(ctx, NOMAD_ERR_CUDA, "chunk download");
   }
-  cudaEventDestroy(start);
-  NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  // wait for every stream the batch touched, also after an error, before buffers are reused
+  cudaError_t e1 = cudaStreamSynchronize(sIn), e2 = cudaStreamSynchronize(sK), e3 = cudaStreamSynchronize(sOut);
+  cleanup();
+  if (st != NOMAD_OK) return st;
+  if (e1 != cudaSuccess) return nomad_cuda_fail(ctx, e1, "upload stream");
+  if (e2 != cudaSuccess) return nomad_cuda_fail(ctx, e2, "trace stream");
+  if (e3 != cudaSuccess) return nomad_cuda_fail(ctx, e3, "download stream");
   return NOMAD_OK;
 }
 

@@ -30,7 +30,10 @@ __device__ __forceinline__ void cswap(float &ta, int32_t &ra, float &tb, int32_t
 
 template <int W>
 __device__ __forceinline__ void sort_children(float (&t)[W], int32_t (&c)[W]) {
-  if (W == 4) {
+  static_assert(W == 2 || W == 4 || W == 8, "sorting networks exist for 2, 4 and 8 children");
+  if constexpr (W == 2) {
+    cswap(t[0], c[0], t[1], c[1]);
+  } else if constexpr (W == 4) {
     cswap(t[0], c[0], t[1], c[1]);
     cswap(t[2], c[2], t[3], c[3]);
     cswap(t[0], c[0], t[2], c[2]);

@@ -500,8 +500,11 @@ bool nomad_traversal_ok(const nomad_ctx *ctx, const nomad_traversal &c, std::str
   };
   if (c.width != 2 && c.width != 4 && c.width != 8) return no("width must be 2, 4 or 8");
   if (c.block != 0 && c.block != 64 && c.block != 128 && c.block != 256) return no("block must be 64, 128 or 256");
-  if (c.persistent > 2) return no("persistent must be 0, 1 or 2");
-  if (c.persistent == 2) {
+  if (c.persistent > 3) return no("persistent must be 0, 1, 2 or 3");
+  if (c.persistent == 3) {
+    if (c.short_stack != 0 || c.staged_nodes != 0 || c.postpone_leaves != 0 || c.min_blocks != 0)
+      return no("the packet kernel takes only width and block");
+  } else if (c.persistent == 2) {
     if (c.short_stack != 0 && c.short_stack != 8 && c.short_stack != 16 && c.short_stack != 32)
       return no("short stack must be 0, 8, 16 or 32");
     if (c.regroup < 1 || c.regroup > 32) return no("regroup threshold must be 1..32");
@@ -518,6 +521,7 @@ bool nomad_traversal_ok(const nomad_ctx *ctx, const nomad_traversal &c, std::str
   const uint32_t cap = c.width == 8 ? (uint32_t)kStackW8 : (uint32_t)kStackW2;
   if (c.width != 2 && ctx->wide[wi - 1].width != c.width) return no("wide layout missing");
   if (ctx->stackNeed[wi] > cap) return no("traversal needs a deeper stack than the kernel has for this scene");
+  if (c.persistent == 3 && ctx->stackNeed[wi] > 128u) return no("packet walk needs a deeper warp stack");
   if (c.staged_nodes > layout_nodes(ctx, c.width)) return no("more staged nodes than the layout has");
   const size_t nodeBytes = c.width == 2 ? 64 : (c.width == 4 ? 128 : 256);
   const size_t ring = (size_t)c.short_stack * (c.block ? c.block : 128) * (c.width == 2 ? 4 : 8);
@@ -594,6 +598,7 @@ extern "C" nomad_status nomad_autotune_sweep(nomad_ctx *ctx, const nomad_ray *ra
   // The grid: the six local-stack kernels, then every short-stack combination.
   std::vector<nomad_traversal> grid;
   for (uint32_t k = NOMAD_KERNEL_BVH2; k < NOMAD_KERNEL_COUNT; ++k) grid.push_back(nomad_kernel_config(k));
+  for (uint32_t w : {2u, 4u, 8u}) grid.push_back(nomad_traversal{w, 3, 0, 1, 0, 128, 0, 0});
   for (uint32_t k = NOMAD_KERNEL_BVH2; k < NOMAD_KERNEL_COUNT; ++k)
     for (uint32_t mb : {10u, 12u, 16u}) {
       nomad_traversal c = nomad_kernel_config(k);

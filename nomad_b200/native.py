@@ -138,6 +138,8 @@ class Traversal(C.Structure):
         return {f: int(getattr(self, f)) for f, _ in self._fields_}
 
     def name(self) -> str:
+        if self.persistent == 3:
+            return f"bvh{self.width}_packet"
         if self.persistent < 2:
             return (f"bvh{self.width}" + ("_persist" if self.persistent else "")
                     + (f"_mb{self.min_blocks}" if self.min_blocks else ""))

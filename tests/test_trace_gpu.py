@@ -257,9 +257,57 @@ def test_autotune_sweep(nb, orc, ctx, small_city):
     res = ctx.autotune_sweep(rays, repeats=1)
     names = [e[0] for e in res["entries"]]
     assert len(names) > 300 and len(set(names)) == len(names)
+    assert {"bvh2_packet", "bvh4_packet", "bvh8_packet"} <= set(names)
     assert all(e[3] == 0 for e in res["entries"] if e[2] >= 0), [e for e in res["entries"] if e[3]]
     assert {e[1]["width"] for e in res["entries"]} == {2, 4, 8}
     assert {e[1]["short_stack"] for e in res["entries"]} == {0, 8, 16, 32}
     assert ctx.traversal() == res["best"]
     _assert_hits_equal(ctx.trace_closest(rays), orc.OracleScene(sb).closest(rays))
+    ctx.set_kernel(1)
+
+
+@pytest.mark.parametrize("width", [2, 4, 8])
+@pytest.mark.parametrize("which", ["ico", "city"])
+def test_packet_parity(nb, orc, ctx, ico_scene, small_city, which, width):
+    """Hybrid packet kernel: coherent warps (primary rays) walk as packets, the rest per ray."""
+    scene, sb = ico_scene if which == "ico" else small_city
+    ctx.upload(sb)
+    ctx.set_traversal(width=width, persistent=3)
+    cam = nb.icosphere_camera(160, 90) if which == "ico" else nb.Camera((0, 60, -180), (0, 0, 0), width=160, height=90)
+    prim = cam.primary_rays(4, seed=23)
+    rays = np.concatenate([prim, _rays(sb, 170)])
+    ref = orc.OracleScene(sb)
+    want = ref.closest(rays)
+    ctx.reset_object_hits()
+    _assert_hits_equal(ctx.trace_closest(rays, count_hits=True), want)
+    counts = np.bincount(want["inst"][want["prim"] >= 0], minlength=sb.object_count).astype(np.uint32)
+    assert np.array_equal(ctx.object_hits(), counts)
+    short = rays.copy()
+    hit = want["prim"] >= 0
+    short["tmax"][hit] = want["t"][hit] * np.float32(0.5)
+    for rs in (rays, short):
+        assert np.array_equal(ctx.trace_any(rs), ref.any(rs))
+    assert ctx.status() == 0
+    ctx.set_kernel(1)
+
+
+def test_full_city_variants(nb, orc, ctx):
+    """The 2.5M-triangle city: a contiguous block of 1080p primary rays (coherent warps, so the
+    packet walks run) and their bounces through every kernel family against the oracle."""
+    scene = nb.synth_city(seed=2)
+    sb = nb.SceneBVH(scene)
+    ctx.upload(sb)
+    rays = nb.city_camera(1920, 1080).primary_rays(1, seed=5)[700_000:760_000]
+    ref = orc.OracleScene(sb)
+    want = ref.closest(rays)
+    b = nb.bounce_rays(rays, want, sb.prims, seed=8)
+    want_b = ref.closest(b)
+    configs = [dict(width=w, persistent=3) for w in (2, 4, 8)]
+    configs += [dict(width=w, persistent=2, short_stack=s, regroup=24, postpone_leaves=1) for w, s in ((2, 8), (4, 0), (8, 16))]
+    configs += [dict(width=w, persistent=1, min_blocks=10) for w in (2, 4, 8)]
+    for c in configs:
+        ctx.set_traversal(**c)
+        _assert_hits_equal(ctx.trace_closest(rays), want)
+        _assert_hits_equal(ctx.trace_closest(b), want_b)
+        assert ctx.status() == 0, c
     ctx.set_kernel(1)
