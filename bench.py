@@ -323,6 +323,30 @@ def run_profile_case(args):
     ctx.close()
 
 
+def run_profile_frame(args):
+    """Renders the city frame of the path-tracing leg twice (the second from the captured graph)
+    with the chosen traversal variant (--kernel, default bvh4_persist)."""
+    import torch
+
+    import nomad_b200 as nb
+
+    scene = nb.synth_city(seed=SEED)
+    sb = nb.SceneBVH(scene)
+    ctx = nb.Context(0)
+    ctx.upload(sb)
+    ctx.set_kernel(args.kernel or 4)
+    v = nb.view_pinhole((0.0, 220.0, -620.0), (0.0, 0.0, 60.0), width=WIDTH, height=HEIGHT, spp=SPP,
+                        max_depth=3, seed=SEED)
+    out = torch.empty(WIDTH * HEIGHT * 3, dtype=torch.float32, device="cuda")
+    for f in range(2):
+        v["frame"] = f
+        ctx.render_dev(v, out.data_ptr())
+    ctx.sync()
+    assert ctx.status() == 0
+    print(json.dumps({"profile_frame": "city 1920x1080 x 4 spp, 3 bounces", "stats": ctx.render_stats().tolist()}))
+    ctx.close()
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -381,12 +405,16 @@ def main():
     ap.add_argument("--profile-case", action="store_true",
                     help="small case for ncu captures: the city, 960x540 primary rays and their bounces in "
                          "one batch, one warm-up and two timed launches of the chosen kernel (--kernel)")
+    ap.add_argument("--profile-frame", action="store_true",
+                    help="path-traced city frame (1920x1080 x 4 spp, 3 bounces) rendered twice, for launch lists")
     args = ap.parse_args()
     CONFIG["spp"] = args.spp
     if args.impl == "reference":
         return run_reference(args)
     if args.profile_case:
         return run_profile_case(args)
+    if args.profile_frame:
+        return run_profile_frame(args)
 
     import torch
     import torch.distributed as dist
