@@ -115,7 +115,7 @@ class ClockSampler:
 
 
 TRAFFIC_PROFILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles",
-                               "launches_bench_city1080_bvh4_persist.md")
+                               "launches_bench_city1080_bvh4_persist_mb10.md")
 
 
 def measured_traffic():
@@ -306,7 +306,7 @@ def run_profile_case(args):
     prim = cam.primary_rays(1, seed=5)
     ph = ctx.trace_closest(prim)
     rays = np.concatenate([prim, nb.bounce_rays(prim, ph, sb.prims, seed=6)])
-    ctx.set_kernel(args.kernel or 4)
+    select_kernel(ctx, args.kernel or 4, args.min_blocks)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
@@ -323,6 +323,18 @@ def run_profile_case(args):
     ctx.close()
 
 
+def select_kernel(ctx, kernel, min_blocks=0):
+    """Fixes the traversal to a NOMAD_KERNEL_* variant, optionally with a min_blocks bound."""
+    import nomad_b200 as nb
+
+    ctx.set_kernel(kernel)
+    if min_blocks:
+        t = ctx.traversal()
+        t["min_blocks"] = min_blocks
+        ctx.set_traversal(**t)
+    return nb.KERNEL_NAMES.get(kernel, str(kernel)) + (f"_mb{min_blocks}" if min_blocks else "")
+
+
 def run_profile_frame(args):
     """Renders the city frame of the path-tracing leg twice (the second from the captured graph)
     with the chosen traversal variant (--kernel, default bvh4_persist)."""
@@ -334,7 +346,7 @@ def run_profile_frame(args):
     sb = nb.SceneBVH(scene)
     ctx = nb.Context(0)
     ctx.upload(sb)
-    ctx.set_kernel(args.kernel or 4)
+    select_kernel(ctx, args.kernel or 4, args.min_blocks)
     v = nb.view_pinhole((0.0, 220.0, -620.0), (0.0, 0.0, 60.0), width=WIDTH, height=HEIGHT, spp=SPP,
                         max_depth=3, seed=SEED)
     out = torch.empty(WIDTH * HEIGHT * 3, dtype=torch.float32, device="cuda")
@@ -397,6 +409,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="nomad", choices=["nomad", "reference"])
     ap.add_argument("--kernel", type=int, default=0)
+    ap.add_argument("--min-blocks", type=int, default=0,
+                    help="with --kernel: resident blocks per SM the kernel is compiled for (0, 10, 12, 16)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the path-tracing, multi-view, ReSTIR and residency legs")
@@ -434,7 +448,7 @@ def main():
     ctx = nb.Context(local)
     ctx.upload(sb)
     if args.kernel:
-        ctx.set_kernel(args.kernel)
+        select_kernel(ctx, args.kernel, args.min_blocks)
     # A dedicated stream: the kernels and the timing events must share it (the legacy default
     # stream has handle 0, which the C ABI reads as "the context's own stream").
     stream = torch.cuda.Stream()
@@ -605,7 +619,8 @@ def main():
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clk.summary(t_begin, t_end),
-            "kernel_variant": tune["best"] if tune else nb.KERNEL_NAMES.get(args.kernel),
+            "kernel_variant": tune["best"] if tune else nb.KERNEL_NAMES.get(args.kernel, str(args.kernel)) + (
+                f"_mb{args.min_blocks}" if args.min_blocks else ""),
             "autotune": tune,
         }
         line.update(extras)
