@@ -17,6 +17,7 @@
 #include <random>
 #include <vector>
 
+#include "residency_features.cuh"
 #include "rt_context.h"
 
 namespace {
@@ -200,12 +201,13 @@ __global__ void __launch_bounds__(128) k_mlp_forward(const float *__restrict__ X
 constexpr int kTcRows = 128;
 constexpr uint32_t kTcCols = 256;                   // tensor-memory columns: D1 [0,128), D2 [128,256)
 constexpr uint32_t kTcX = 0;                        // X tile, 128 x 32 bf16
-constexpr uint32_t kTcW1 = kTcX + 128 * kInPad * 2; // W1, 128 x 32
-constexpr uint32_t kTcH1 = kTcW1 + 128 * kInPad * 2;
-constexpr uint32_t kTcW2 = kTcH1 + 128 * kHid * 2;
-constexpr uint32_t kTcF = kTcW2 + 128 * kHid * 2;   // fp32: b1, b2, w3, b3, mean, istd
-constexpr uint32_t kTcBar = kTcF + 4 * (3 * kHid + 1 + 2 * kIn + 7);
-constexpr size_t kTcSmem = kTcBar + 16;
+constexpr uint32_t kTcW1 = kTcX + 128 * kInPad * 2; // W1, 128 x 32, then W2 right after it:
+constexpr uint32_t kTcW2 = kTcW1 + 128 * kInPad * 2; // both arrive pre-packed in one bulk copy
+constexpr uint32_t kTcWBytes = 128 * kInPad * 2 + 128 * kHid * 2;  // 40 KB
+constexpr uint32_t kTcH1 = kTcW2 + 128 * kHid * 2;
+constexpr uint32_t kTcF = kTcH1 + 128 * kHid * 2;   // fp32: b1, b2, w3, b3, mean, istd
+constexpr uint32_t kTcBar = kTcF + 4 * (3 * kHid + 1 + 2 * kIn + 7);  // copy barrier, MMA barrier, TMEM slot
+constexpr size_t kTcSmem = kTcBar + 24;
 constexpr uint32_t kStatusWaitExpired = 1u << 1;
 constexpr long long kTcWaitPolls = 1ll << 22;
 
@@ -263,11 +265,15 @@ __device__ __forceinline__ void tc_ld32(uint32_t taddr, float (&v)[32]) {
   for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
 }
 
+// Wc holds W1 and W2 (bf16) already in the canonical shared-memory layout (k_refresh_bf16 packs
+// them whenever the weights change), so one bulk asynchronous copy stages both.
+// FEAT: the rows are the residency step's objects; each thread computes its object's features
+// (nomad_res::object_features, the same code as the feature kernel) instead of reading X.
+template <bool FEAT>
 __global__ void __launch_bounds__(128) k_mlp_forward_tc(const float *__restrict__ X, uint64_t n,
                                                         const float *__restrict__ P,
-                                                        const __nv_bfloat16 *__restrict__ W1b,
-                                                        const __nv_bfloat16 *__restrict__ W2b, float *__restrict__ y,
-                                                        uint32_t *__restrict__ status) {
+                                                        const unsigned char *__restrict__ Wc, float *__restrict__ y,
+                                                        uint32_t *__restrict__ status, nomad_res::FeatArgs fa) {
   extern __shared__ __align__(16) unsigned char smem[];
   const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
   float *sB1 = reinterpret_cast<float *>(smem + kTcF);
@@ -276,25 +282,33 @@ __global__ void __launch_bounds__(128) k_mlp_forward_tc(const float *__restrict_
   float *sB3 = sW3 + kHid;
   float *sMean = sB3 + 1;
   float *sIstd = sMean + kIn;
-  const uint32_t bar = sbase + kTcBar;
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(smem + kTcBar + 8);
+  const uint32_t barCopy = sbase + kTcBar, bar = sbase + kTcBar + 8;
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(smem + kTcBar + 16);
   const int tid = threadIdx.x, warp = tid >> 5;
 
   if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(barCopy) : "memory");
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    // weights: one bulk copy (no multicast) of the pre-packed W1 | W2 block
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(barCopy), "r"(kTcWBytes) : "memory");
+    for (uint32_t off = 0; off < kTcWBytes; off += 16384u) {
+      const uint32_t sz = min(16384u, kTcWBytes - off);
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+              sbase + kTcW1 + off),
+          "l"(Wc + off), "r"(sz), "r"(barCopy)
+          : "memory");
+    }
   }
   if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sbase + kTcBar + 8),
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sbase + kTcBar + 16),
                  "r"(kTcCols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  // operands: weights (bf16, already rounded) and the standardised X tile
-  for (int i = tid; i < kHid * kInPad; i += 128)
-    *reinterpret_cast<__nv_bfloat16 *>(smem + kTcW1 + canon_off(i / kInPad, i % kInPad)) = W1b[i];
-  for (int i = tid; i < kHid * kHid; i += 128)
-    *reinterpret_cast<__nv_bfloat16 *>(smem + kTcW2 + canon_off(i / kHid, i % kHid)) = W2b[i];
+  // the standardised X tile and the fp32 vectors while the weights are in flight
   for (int i = tid; i < kHid; i += 128) {
     sB1[i] = P[oB1 + i];
     sB2[i] = P[oB2 + i];
@@ -307,11 +321,22 @@ __global__ void __launch_bounds__(128) k_mlp_forward_tc(const float *__restrict_
   }
   __syncthreads();
   const uint64_t row0 = (uint64_t)blockIdx.x * kTcRows;
-  for (int i = tid; i < kTcRows * kInPad; i += 128) {
-    const int r = i / kInPad, f = i % kInPad;
-    float v = 0.0f;
-    if (f < kIn && row0 + r < n) v = (X[(row0 + r) * kIn + f] - sMean[f]) * sIstd[f];
-    *reinterpret_cast<__nv_bfloat16 *>(smem + kTcX + canon_off(r, f)) = __float2bfloat16_rn(v);
+  if constexpr (FEAT) {
+    float f[NOMAD_FEATURES];
+    const bool live = row0 + tid < n;
+    if (live) nomad_res::object_features(fa, (uint32_t)(row0 + tid), f);
+#pragma unroll
+    for (int k = 0; k < kInPad; ++k) {
+      const float v = (live && k < kIn) ? (f[k < kIn ? k : 0] - sMean[k < kIn ? k : 0]) * sIstd[k < kIn ? k : 0] : 0.0f;
+      *reinterpret_cast<__nv_bfloat16 *>(smem + kTcX + canon_off(tid, k)) = __float2bfloat16_rn(v);
+    }
+  } else {
+    for (int i = tid; i < kTcRows * kInPad; i += 128) {
+      const int r = i / kInPad, f = i % kInPad;
+      float v = 0.0f;
+      if (f < kIn && row0 + r < n) v = (X[(row0 + r) * kIn + f] - sMean[f]) * sIstd[f];
+      *reinterpret_cast<__nv_bfloat16 *>(smem + kTcX + canon_off(r, f)) = __float2bfloat16_rn(v);
+    }
   }
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -319,6 +344,7 @@ __global__ void __launch_bounds__(128) k_mlp_forward_tc(const float *__restrict_
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tslot;
   const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+  bool ok = tc_wait(barCopy, 0);  // weights landed
 
   // layer 1: D1 = X . W1^T, K = 32 in two steps
   if (tid == 0) {
@@ -328,7 +354,7 @@ __global__ void __launch_bounds__(128) k_mlp_forward_tc(const float *__restrict_
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
                  : "memory");
   }
-  bool ok = tc_wait(bar, 0);
+  ok = tc_wait(bar, 0) && ok;
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   // epilogue 1: bias, ReLU, BF16 into the layer-2 operand (row = this thread's lane)
   const int r = tid;
@@ -515,12 +541,21 @@ __global__ void k_adamw(float *__restrict__ P, const float *__restrict__ G, floa
   }
 }
 
-// bf16 copies of W1 and W2 (W1's padded input columns stay zero).
+// bf16 copies of W1 and W2 (W1's padded input columns stay zero), row-major for the training
+// kernels and packed in the canonical layout of the tcgen05 inference kernel (W1 then W2).
 __global__ void k_refresh_bf16(const float *__restrict__ P, __nv_bfloat16 *__restrict__ W1b,
-                               __nv_bfloat16 *__restrict__ W2b) {
+                               __nv_bfloat16 *__restrict__ W2b, unsigned char *__restrict__ Wc) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < kHid * kInPad) W1b[i] = __float2bfloat16_rn((i % kInPad) < kIn ? P[oW1 + i] : 0.0f);
-  if (i < kHid * kHid) W2b[i] = __float2bfloat16_rn(P[oW2 + i]);
+  if (i < kHid * kInPad) {
+    const __nv_bfloat16 w = __float2bfloat16_rn((i % kInPad) < kIn ? P[oW1 + i] : 0.0f);
+    W1b[i] = w;
+    *reinterpret_cast<__nv_bfloat16 *>(Wc + canon_off(i / kInPad, i % kInPad)) = w;
+  }
+  if (i < kHid * kHid) {
+    const __nv_bfloat16 w = __float2bfloat16_rn(P[oW2 + i]);
+    W2b[i] = w;
+    *reinterpret_cast<__nv_bfloat16 *>(Wc + (kTcW2 - kTcW1) + canon_off(i / kHid, i % kHid)) = w;
+  }
 }
 
 // Gathers a mini-batch of raw features and targets.
@@ -537,7 +572,7 @@ __global__ void k_gather(const float *__restrict__ X, const float *__restrict__ 
 
 struct MlpState {
   bool ready = false;
-  DeviceBuf P, W1b, W2b, M, V, G;
+  DeviceBuf P, W1b, W2b, Wc, M, V, G;
   DeviceBuf X, T, idx, xb, tb, y, z1, h1, z2, xbf, dy, se, dz2b, dz2f, dh1, dz1b, dz1f, part;
   uint64_t trainCap = 0;
   int batchCap = 0;
@@ -554,7 +589,7 @@ MlpState &mlp(nomad_ctx *ctx) {
 nomad_status refresh(nomad_ctx *ctx, MlpState &S) {
   int n = kHid * kHid;
   k_refresh_bf16<<<(n + 255) / 256, 256, 0, ctx->stream>>>(S.P.as<const float>(), S.W1b.as<__nv_bfloat16>(),
-                                                            S.W2b.as<__nv_bfloat16>());
+                                                            S.W2b.as<__nv_bfloat16>(), S.Wc.as<unsigned char>());
   NOMAD_CUDA(ctx, cudaGetLastError());
   return NOMAD_OK;
 }
@@ -563,13 +598,17 @@ nomad_status ensure(nomad_ctx *ctx, MlpState &S) {
   NOMAD_CUDA(ctx, S.P.reserve(kParams * 4));
   NOMAD_CUDA(ctx, S.W1b.reserve(kHid * kInPad * 2));
   NOMAD_CUDA(ctx, S.W2b.reserve(kHid * kHid * 2));
+  NOMAD_CUDA(ctx, S.Wc.reserve(kTcWBytes));
   NOMAD_CUDA(ctx, S.M.reserve(kParams * 4));
   NOMAD_CUDA(ctx, S.V.reserve(kParams * 4));
   NOMAD_CUDA(ctx, S.G.reserve(kParams * 4));
   static bool attr = false;
   if (!attr) {
     NOMAD_CUDA(ctx, cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwdSmem));
-    NOMAD_CUDA(ctx, cudaFuncSetAttribute(k_mlp_forward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+    NOMAD_CUDA(ctx, cudaFuncSetAttribute(k_mlp_forward_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kTcSmem));
+    NOMAD_CUDA(ctx, cudaFuncSetAttribute(k_mlp_forward_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kTcSmem));
     attr = true;
   }
   return NOMAD_OK;
@@ -584,8 +623,21 @@ nomad_status nomad_mlp_infer_device(nomad_ctx *ctx, const float *X, uint64_t n, 
   if (!S.ready) return nomad_fail(ctx, NOMAD_ERR_NOT_READY, "MLP not initialised or trained");
   if (n == 0) return NOMAD_OK;
   const unsigned blocks = (unsigned)((n + kTcRows - 1) / kTcRows);
-  k_mlp_forward_tc<<<blocks, 128, kTcSmem, ctx->stream>>>(X, n, S.P.as<const float>(), S.W1b.as<const __nv_bfloat16>(),
-                                                          S.W2b.as<const __nv_bfloat16>(), y, ctx->status.as<uint32_t>());
+  k_mlp_forward_tc<false><<<blocks, 128, kTcSmem, ctx->stream>>>(X, n, S.P.as<const float>(),
+                                                                 S.Wc.as<const unsigned char>(), y,
+                                                                 ctx->status.as<uint32_t>(), nomad_res::FeatArgs{});
+  NOMAD_CUDA(ctx, cudaGetLastError());
+  return NOMAD_OK;
+}
+
+nomad_status nomad_mlp_score_objects(nomad_ctx *ctx, const nomad_res::FeatArgs *fa, float *keys) {
+  MlpState &S = mlp(ctx);
+  if (!S.ready) return nomad_fail(ctx, NOMAD_ERR_NOT_READY, "MLP not initialised or trained");
+  if (fa->n == 0) return NOMAD_OK;
+  const unsigned blocks = (fa->n + kTcRows - 1) / kTcRows;
+  k_mlp_forward_tc<true><<<blocks, 128, kTcSmem, ctx->stream>>>(nullptr, fa->n, S.P.as<const float>(),
+                                                                S.Wc.as<const unsigned char>(), keys,
+                                                                ctx->status.as<uint32_t>(), *fa);
   NOMAD_CUDA(ctx, cudaGetLastError());
   return NOMAD_OK;
 }

@@ -21,73 +21,23 @@
 #include <cstring>
 #include <vector>
 
+#include "residency_features.cuh"
 #include "rt_context.h"
 
 using namespace nomad_dev;
 
 namespace {
 
-constexpr int kHist = 8;
+using nomad_res::CamDev;
+using nomad_res::FeatArgs;
+using nomad_res::kHist;
 constexpr uint32_t kMaxSelectObjects = 16384;
 
-struct CamDev {
-  float pos[3], fwd[3], right[3], up[3];
-  float halfW, halfH, speed;
-};
-
-// misc words: [0] toggles, [1] root toggled flag, [2] root resident, [3] total hits this frame,
-// [4] total hits previous frame
-__global__ void k_features(uint32_t n, CamDev cam, const float4 *__restrict__ bounds,
-                           const unsigned long long *__restrict__ bytes, const uint32_t *__restrict__ tris,
-                           const float *__restrict__ emit, const uint8_t *__restrict__ res,
-                           uint32_t *__restrict__ hits, uint32_t *__restrict__ hist, float *__restrict__ score,
-                           uint32_t *__restrict__ lastHit, float *__restrict__ prevDist,
-                           uint8_t *__restrict__ visible, float *__restrict__ feat, float *__restrict__ keys,
-                           uint32_t *__restrict__ misc, uint32_t frame, float decay, float memPressure) {
-  uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
-  if (o >= n) return;
-  uint32_t h = hits[o];
-  hits[o] = 0;
-  if (h) atomicAdd(&misc[3], h);
-  hist[o * kHist + frame % kHist] = h;
-  float s = score[o] * decay + (float)h;
-  score[o] = s;
-  if (h) lastHit[o] = frame;
-  float4 b = bounds[o];
-  float dx = b.x - cam.pos[0], dy = b.y - cam.pos[1], dz = b.z - cam.pos[2];
-  float dist = sqrtf(dx * dx + dy * dy + dz * dz);
-  float z = dx * cam.fwd[0] + dy * cam.fwd[1] + dz * cam.fwd[2];
-  float x = dx * cam.right[0] + dy * cam.right[1] + dz * cam.right[2];
-  float y = dx * cam.up[0] + dy * cam.up[1] + dz * cam.up[2];
-  float r = b.w;
-  bool vis = z > -r && fabsf(x) - cam.halfW * z <= r * sqrtf(1.0f + cam.halfW * cam.halfW) &&
-             fabsf(y) - cam.halfH * z <= r * sqrtf(1.0f + cam.halfH * cam.halfH);
-  visible[o] = vis ? 1 : 0;
-  float* f = feat + (size_t)o * NOMAD_FEATURES;
-  float zc = fmaxf(z, 1e-3f);
-  f[0] = log1pf(dist);
-  f[1] = fminf(r / (fmaxf(dist, 1e-3f) * cam.halfH), 4.0f);
-  f[2] = vis ? 1.0f : 0.0f;
-  for (int k = 0; k < kHist; ++k) f[3 + k] = log1pf((float)hist[o * kHist + (frame + kHist - k) % kHist]);
-  f[11] = log1pf(s);
-  f[12] = log1pf((float)tris[o]);
-  f[13] = log1pf((float)bytes[o] / 1024.0f);
-  f[14] = log1pf(emit[o]);
-  f[15] = cam.speed;
-  f[16] = dist > 0.0f ? z / dist : 1.0f;
-  f[17] = log1pf(r);
-  f[18] = res[o] ? 1.0f : 0.0f;
-  f[19] = log1pf((float)min(frame - lastHit[o], 255u));
-  f[20] = (float)h / fmaxf(1.0f, (float)misc[4]);
-  f[21] = prevDist[o] > 0.0f ? prevDist[o] - dist : 0.0f;
-  f[22] = fminf(fabsf(x) / (zc * cam.halfW), 4.0f);
-  f[23] = fminf(fabsf(y) / (zc * cam.halfH), 4.0f);
-  prevDist[o] = dist;
-  // ray-hit-budget key (RendererResidency.cpp:2833-2840)
-  float key = s;
-  if (!vis) key = (h == 0) ? 0.0f : key * (0.5f + (0.2f - 0.5f) * memPressure);
-  else if (key <= 0.0f) key = 1.0f;
-  keys[o] = key;
+__global__ void k_features(FeatArgs A, float *__restrict__ keys) {
+  const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= A.n) return;
+  float f[NOMAD_FEATURES];
+  keys[o] = nomad_res::object_features(A, o, f);
 }
 
 __device__ __forceinline__ unsigned long long sort_key(float s, uint32_t idx) {
@@ -126,21 +76,55 @@ __device__ __forceinline__ uint32_t block_exscan(uint32_t v, uint32_t *warpSums,
   return r;
 }
 
-// Greedy fill in sorted order by one warp: candidates (cand[k] = 1) are taken while they fit in
-// the budget, skipping those that do not (the sequential rule), 32 positions at a time. Each round
-// first drops lanes that cannot fit on their own, then accepts the longest run of candidates whose
-// running byte total fits; the first candidate past that run is skipped.
-__device__ void warp_greedy(uint32_t n, const unsigned long long *__restrict__ sk,
-                            const unsigned long long *__restrict__ bytes, unsigned long long budget, bool unlimited,
-                            uint8_t *cand, uint8_t *dsel, unsigned long long *used) {
+// Block-wide exclusive scan of one u64 per thread (1024 threads); writes the total to *total.
+__device__ __forceinline__ unsigned long long block_exscan64(unsigned long long v, unsigned long long *warpSums,
+                                                             unsigned long long *total) {
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  unsigned long long x = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const unsigned long long y = __shfl_up_sync(0xffffffffu, x, d);
+    if ((int)lane >= d) x += y;
+  }
+  if (lane == 31) warpSums[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    const unsigned long long w = warpSums[lane];
+    unsigned long long z = w;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const unsigned long long y = __shfl_up_sync(0xffffffffu, z, d);
+      if ((int)lane >= d) z += y;
+    }
+    warpSums[lane] = z - w;
+    if (lane == 31) *total = z;
+  }
+  __syncthreads();
+  const unsigned long long r = warpSums[warp] + x - v;
+  __syncthreads();
+  return r;
+}
+
+// After the sort each key holds (object bytes / 4) in its high word and the object in its low
+// word. Object bytes are 32 per node + 196 per primitive, so always a multiple of 4, and
+// "used + b <= budget" holds exactly when "used/4 + b/4 <= budget/4" (rounded down).
+__device__ __forceinline__ uint32_t key_obj(unsigned long long k) { return (uint32_t)(k & 0xffffffffu); }
+__device__ __forceinline__ unsigned long long key_b4(unsigned long long k) { return k >> 32; }
+
+// Greedy fill in sorted order from position `from` by one warp: candidates are taken while they
+// fit, skipping those that do not (the sequential rule), 32 positions at a time. Each round
+// first drops lanes that cannot fit on their own, then accepts the longest run of candidates
+// whose running total fits; the first candidate past that run is skipped.
+__device__ void warp_greedy(uint32_t from, uint32_t n, const unsigned long long *sk, unsigned long long budget4,
+                            bool unlimited, const uint8_t *cand, uint8_t *dsel, unsigned long long *used4) {
   const unsigned lane = threadIdx.x & 31u;
-  unsigned long long u = *used;
-  for (uint32_t base = 0; base < n; base += 32) {
+  unsigned long long u = *used4;
+  for (uint32_t base = from; base < n; base += 32) {
     const uint32_t k = base + lane;
     bool c = k < n && cand[k];
-    const unsigned long long b = c ? bytes[(uint32_t)(sk[k] & 0xffffffffu)] : 0ull;
+    const unsigned long long b = c ? key_b4(sk[k]) : 0ull;
     for (;;) {
-      const unsigned long long rem = unlimited ? ~0ull : (u > budget ? 0ull : budget - u);
+      const unsigned long long rem = unlimited ? ~0ull : (u > budget4 ? 0ull : budget4 - u);
       if (c && b > rem) c = false;
       if (__ballot_sync(0xffffffffu, c) == 0) break;
       unsigned long long p = c ? b : 0ull;  // inclusive prefix of candidate bytes
@@ -151,126 +135,74 @@ __device__ void warp_greedy(uint32_t n, const unsigned long long *__restrict__ s
       }
       const unsigned fail = __ballot_sync(0xffffffffu, c && p > rem);
       const int f = fail ? __ffs(fail) - 1 : 32;
-      const bool take = c && (int)lane < f;
-      if (take) dsel[k] = 1;
-      // bytes taken this round: the prefix just before the first failing lane (or the total)
+      if (c && (int)lane < f) dsel[k] = 1;
       const unsigned long long pf = __shfl_sync(0xffffffffu, p, f < 32 ? f : 31);
       const unsigned long long bf = __shfl_sync(0xffffffffu, b, f < 32 ? f : 31);
       u += f < 32 ? pf - bf : pf;
       c = c && (int)lane > f;
     }
   }
-  if (lane == 0) *used = u;
+  if (lane == 0) *used4 = u;
 }
 
-// Single block of 1024 threads: sort by score, select under the budget (min_active, visibility
-// reserve, fill), apply toggles in index order and patch the TLAS refs. Every pass but the two
-// budget walks is data-parallel; the budget walks run on one warp, 32 objects at a time.
-__global__ void __launch_bounds__(1024) k_select(uint32_t n, uint32_t npow2, uint32_t policy,
-                                                 const float *__restrict__ keys, const uint8_t *__restrict__ visible,
-                                                 const unsigned long long *__restrict__ bytes,
-                                                 unsigned long long budget, uint32_t reserve, uint32_t minActive,
-                                                 uint32_t maxToggles, uint8_t *__restrict__ desired,
-                                                 uint8_t *__restrict__ res, const long long *__restrict__ slot,
-                                                 const int32_t *__restrict__ blasRef, int32_t *__restrict__ pnodeWords,
-                                                 uint32_t *__restrict__ misc) {
-  extern __shared__ unsigned long long sk[];
-  uint8_t *dsel = reinterpret_cast<uint8_t *>(sk + npow2);  // selected, by sorted position
-  uint8_t *cand = dsel + npow2;                             // candidates of the current walk
-  __shared__ uint32_t warpSums[32];
-  __shared__ uint32_t total;
-  __shared__ unsigned long long used;
-  for (uint32_t i = threadIdx.x; i < npow2; i += blockDim.x)
-    sk[i] = i < n ? sort_key(policy == NOMAD_POLICY_ALWAYS ? 1.0f : keys[i], i) : ~0ull;
-  if (threadIdx.x == 0) used = 0;
-  __syncthreads();
-  for (uint32_t k = 2; k <= npow2; k <<= 1) {
-    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-      for (uint32_t i = threadIdx.x; i < npow2; i += blockDim.x) {
-        uint32_t l = i ^ j;
-        if (l > i) {
-          unsigned long long a = sk[i], b = sk[l];
-          bool up = (i & k) == 0;
-          if ((a > b) == up) {
-            sk[i] = b;
-            sk[l] = a;
-          }
-        }
-      }
-      __syncthreads();
-    }
-  }
-  const bool unlimited = budget == 0 || policy == NOMAD_POLICY_ALWAYS;
-  // min_active: the best-scored objects stay whatever the budget
-  for (uint32_t k = threadIdx.x; k < npow2; k += blockDim.x) {
-    const bool m = k < n && k < minActive;
-    dsel[k] = m ? 1 : 0;
-    if (m) atomicAdd(&used, bytes[(uint32_t)(sk[k] & 0xffffffffu)]);
-  }
-  __syncthreads();
-  // visibility reserve: the first `reserve` visible objects in score order (a contiguous segment
-  // of sorted positions per thread, so the scan keeps the sorted order)
+struct SelectShared {
+  unsigned long long warpSums64[32];
+  unsigned long long total64;
+  unsigned long long used4;
+  unsigned long long add4;
+  uint32_t warpSums[32];
+  uint32_t total;
+  uint32_t first;
+};
+
+// One budget walk over the candidates (cand[k] = 1) in sorted order, with the whole block: a
+// block scan of candidate bytes finds the first candidate that no longer fits; every candidate
+// before it is taken at once, that one is skipped, and one warp finishes the walk after it
+// (where the remaining budget is below that candidate's size, so most objects drop at once).
+__device__ void budget_walk(uint32_t n, uint32_t npow2, const unsigned long long *sk, unsigned long long budget4,
+                            bool unlimited, const uint8_t *cand, uint8_t *dsel, SelectShared &sh) {
   const uint32_t per = (npow2 + blockDim.x - 1) / blockDim.x;
-  const uint32_t k0 = threadIdx.x * per;
-  uint32_t nv = 0;
-  for (uint32_t k = k0; k < k0 + per && k < n; ++k) nv += visible[(uint32_t)(sk[k] & 0xffffffffu)] ? 1u : 0u;
-  uint32_t before = block_exscan(nv, warpSums, &total);
-  for (uint32_t k = k0; k < k0 + per && k < npow2; ++k) {
-    bool c = false;
-    if (k < n && visible[(uint32_t)(sk[k] & 0xffffffffu)]) {
-      c = before < reserve && !dsel[k];
-      ++before;
-    }
-    cand[k] = c ? 1 : 0;
-  }
-  __syncthreads();
-  if (threadIdx.x < 32) warp_greedy(n, sk, bytes, budget, unlimited, cand, dsel, &used);
-  __syncthreads();
-  // fill in score order
-  for (uint32_t k = threadIdx.x; k < npow2; k += blockDim.x) cand[k] = (k < n && !dsel[k]) ? 1 : 0;
-  __syncthreads();
-  if (threadIdx.x < 32) warp_greedy(n, sk, bytes, budget, unlimited, cand, dsel, &used);
-  __syncthreads();
-  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) desired[(uint32_t)(sk[k] & 0xffffffffu)] = dsel[k];
-  __syncthreads();
-  // toggles in index order, the first max_toggles of them when bounded
-  uint32_t nd = 0;
-  for (uint32_t o = k0; o < k0 + per && o < n; ++o) nd += desired[o] != res[o] ? 1u : 0u;
-  uint32_t rank = block_exscan(nd, warpSums, &total);
-  for (uint32_t o = k0; o < k0 + per && o < n; ++o) {
-    const uint8_t want = desired[o];
-    if (want == res[o]) continue;
-    const bool apply = maxToggles == 0 || rank < maxToggles;
-    ++rank;
-    if (!apply) continue;
-    res[o] = want;
-    const long long s = slot[o];
-    const int32_t ref = want ? blasRef[o] : kEmptyRef;
-    if (s >= 0) {
-      pnodeWords[(s / 2) * 16 + ((s & 1) ? 7 : 3)] = ref;
-    } else if (s == -1) {
-      misc[1] = 1;
-      misc[2] = want;
+  const uint32_t k0 = threadIdx.x * per, k1 = min(k0 + per, n);
+  unsigned long long seg = 0;
+  for (uint32_t k = k0; k < k1; ++k)
+    if (cand[k]) seg += key_b4(sk[k]);
+  if (threadIdx.x == 0) sh.first = npow2;
+  const unsigned long long excl = block_exscan64(seg, sh.warpSums64, &sh.total64);  // syncs inside
+  const unsigned long long u0 = sh.used4;
+  const unsigned long long rem = unlimited ? ~0ull : (u0 > budget4 ? 0ull : budget4 - u0);
+  unsigned long long run = excl;
+  for (uint32_t k = k0; k < k1; ++k) {
+    if (!cand[k]) continue;
+    run += key_b4(sk[k]);
+    if (run > rem) {
+      atomicMin(&sh.first, k);
+      break;
     }
   }
-  if (threadIdx.x == 0) {
-    misc[0] = maxToggles == 0 ? total : min(total, maxToggles);
-    misc[4] = misc[3];
-    misc[3] = 0;
-  }
+  __syncthreads();
+  const uint32_t R = sh.first;
+  unsigned long long before = excl;  // candidate bytes before R inside this segment
+  for (uint32_t k = k0; k < k1 && k < R; ++k)
+    if (cand[k]) {
+      dsel[k] = 1;
+      before += key_b4(sk[k]);
+    }
+  if (R < npow2 && k0 <= R && R < k0 + per) sh.add4 = before;  // the segment holding R
+  if (R >= npow2 && threadIdx.x == 0) sh.add4 = sh.total64;
+  __syncthreads();
+  if (threadIdx.x == 0) sh.used4 = u0 + sh.add4;
+  __syncthreads();
+  if (R + 1 < n && threadIdx.x < 32) warp_greedy(R + 1, n, sk, budget4, unlimited, cand, dsel, &sh.used4);
+  __syncthreads();
 }
 
 // Light CDF over the emissive primitives whose primitive is active and whose object is
 // resident, summed sequentially in primitive order (one thread; the flags are gathered by the
-// block first). Also writes the per-primitive light pdf used by ReSTIR.
-__global__ void __launch_bounds__(1024) k_lights_rebuild(const uint4 *__restrict__ em, uint32_t ne,
-                                                         const uint8_t *__restrict__ primAct,
-                                                         const uint8_t *__restrict__ objRes,
-                                                         uint32_t *__restrict__ idx, float *__restrict__ cdf,
-                                                         float *__restrict__ pdf, LightMeta *__restrict__ meta) {
-  __shared__ uint8_t on[4096];
-  __shared__ float total_s;
-  __shared__ uint32_t count_s;
+// block first). Also writes the per-primitive light pdf used by ReSTIR. Called by one block.
+__device__ void lights_rebuild(const uint4 *__restrict__ em, uint32_t ne, const uint8_t *__restrict__ primAct,
+                               const uint8_t *objRes, uint32_t *__restrict__ idx, float *__restrict__ cdf,
+                               float *__restrict__ pdf, LightMeta *__restrict__ meta, uint8_t *on, float &total_s,
+                               uint32_t &count_s) {
   if (threadIdx.x == 0) {
     total_s = 0.0f;
     count_s = 0;
@@ -312,6 +244,150 @@ __global__ void __launch_bounds__(1024) k_lights_rebuild(const uint4 *__restrict
       if (w > 0.0f && total > 0.0f) pdf[idx[k]] = w / total;
     }
   }
+}
+
+__global__ void __launch_bounds__(1024) k_lights_rebuild(const uint4 *__restrict__ em, uint32_t ne,
+                                                         const uint8_t *__restrict__ primAct,
+                                                         const uint8_t *__restrict__ objRes,
+                                                         uint32_t *__restrict__ idx, float *__restrict__ cdf,
+                                                         float *__restrict__ pdf, LightMeta *__restrict__ meta) {
+  __shared__ uint8_t on[4096];
+  __shared__ float total_s;
+  __shared__ uint32_t count_s;
+  lights_rebuild(em, ne, primAct, objRes, idx, cdf, pdf, meta, on, total_s, count_s);
+}
+
+// Wide-layout instance slots that one step rewrites (4- and 8-wide).
+struct WidePatch {
+  int32_t *arena;
+  size_t base[2];
+  uint32_t fpn[2], width[2];
+  const long long *slot[2];
+  const int32_t *ref[2];
+};
+
+struct LightArgs {
+  const uint4 *em;
+  uint32_t ne;
+  const uint8_t *primAct;
+  uint32_t *idx;
+  float *cdf, *pdf;
+  LightMeta *meta;
+};
+
+// Single block of 1024 threads, the whole residency decision of one step: sort by score, select
+// under the budget (min_active, visibility reserve, fill), apply toggles in index order, patch the
+// instance links of the pair and wide layouts, and rebuild the light CDF over the new resident set.
+__global__ void __launch_bounds__(1024) k_select(uint32_t n, uint32_t npow2, uint32_t policy,
+                                                 const float *__restrict__ keys, const uint8_t *__restrict__ visible,
+                                                 const unsigned long long *__restrict__ bytes,
+                                                 unsigned long long budget, uint32_t reserve, uint32_t minActive,
+                                                 uint32_t maxToggles, uint8_t *__restrict__ desired,
+                                                 uint8_t *__restrict__ res, const long long *__restrict__ slot,
+                                                 const int32_t *__restrict__ blasRef, int32_t *__restrict__ pnodeWords,
+                                                 uint32_t *__restrict__ misc, WidePatch wp, LightArgs la) {
+  extern __shared__ unsigned long long sk[];
+  uint8_t *dsel = reinterpret_cast<uint8_t *>(sk + npow2);  // selected, by sorted position
+  uint8_t *cand = dsel + npow2;                             // candidates of the current walk
+  __shared__ SelectShared sh;
+  __shared__ uint8_t on[4096];
+  __shared__ float ltotal;
+  __shared__ uint32_t lcount;
+  for (uint32_t i = threadIdx.x; i < npow2; i += blockDim.x)
+    sk[i] = i < n ? sort_key(policy == NOMAD_POLICY_ALWAYS ? 1.0f : keys[i], i) : ~0ull;
+  if (threadIdx.x == 0) {
+    sh.used4 = 0;
+    misc[1] = 0;
+  }
+  __syncthreads();
+  for (uint32_t k = 2; k <= npow2; k <<= 1) {
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      for (uint32_t i = threadIdx.x; i < npow2; i += blockDim.x) {
+        uint32_t l = i ^ j;
+        if (l > i) {
+          unsigned long long a = sk[i], b = sk[l];
+          bool up = (i & k) == 0;
+          if ((a > b) == up) {
+            sk[i] = b;
+            sk[l] = a;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  // sorted keys -> (bytes / 4, object)
+  for (uint32_t k = threadIdx.x; k < npow2; k += blockDim.x) {
+    const uint32_t o = (uint32_t)(sk[k] & 0xffffffffu);
+    sk[k] = k < n ? ((unsigned long long)(bytes[o] >> 2) << 32) | o : 0ull;
+  }
+  __syncthreads();
+  const bool unlimited = budget == 0 || policy == NOMAD_POLICY_ALWAYS;
+  const unsigned long long budget4 = budget >> 2;
+  // min_active: the best-scored objects stay whatever the budget
+  for (uint32_t k = threadIdx.x; k < npow2; k += blockDim.x) {
+    const bool m = k < n && k < minActive;
+    dsel[k] = m ? 1 : 0;
+    if (m) atomicAdd(&sh.used4, key_b4(sk[k]));
+  }
+  __syncthreads();
+  // visibility reserve: the first `reserve` visible objects in score order (a contiguous segment
+  // of sorted positions per thread, so the scan keeps the sorted order)
+  const uint32_t per = (npow2 + blockDim.x - 1) / blockDim.x;
+  const uint32_t k0 = threadIdx.x * per;
+  uint32_t nv = 0;
+  for (uint32_t k = k0; k < k0 + per && k < n; ++k) nv += visible[key_obj(sk[k])] ? 1u : 0u;
+  uint32_t before = block_exscan(nv, sh.warpSums, &sh.total);
+  for (uint32_t k = k0; k < k0 + per && k < npow2; ++k) {
+    bool c = false;
+    if (k < n && visible[key_obj(sk[k])]) {
+      c = before < reserve && !dsel[k];
+      ++before;
+    }
+    cand[k] = c ? 1 : 0;
+  }
+  __syncthreads();
+  budget_walk(n, npow2, sk, budget4, unlimited, cand, dsel, sh);
+  // fill in score order
+  for (uint32_t k = threadIdx.x; k < npow2; k += blockDim.x) cand[k] = (k < n && !dsel[k]) ? 1 : 0;
+  __syncthreads();
+  budget_walk(n, npow2, sk, budget4, unlimited, cand, dsel, sh);
+  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) desired[key_obj(sk[k])] = dsel[k];
+  __syncthreads();
+  // toggles in index order, the first max_toggles of them when bounded
+  uint32_t nd = 0;
+  for (uint32_t o = k0; o < k0 + per && o < n; ++o) nd += desired[o] != res[o] ? 1u : 0u;
+  uint32_t rank = block_exscan(nd, sh.warpSums, &sh.total);
+  for (uint32_t o = k0; o < k0 + per && o < n; ++o) {
+    const uint8_t want = desired[o];
+    if (want == res[o]) continue;
+    const bool apply = maxToggles == 0 || rank < maxToggles;
+    ++rank;
+    if (!apply) continue;
+    res[o] = want;
+    const long long s = slot[o];
+    const int32_t ref = want ? blasRef[o] : kEmptyRef;
+    if (s >= 0) {
+      pnodeWords[(s / 2) * 16 + ((s & 1) ? 7 : 3)] = ref;
+    } else if (s == -1) {
+      misc[1] = 1;
+      misc[2] = want;
+    }
+    for (int w = 0; w < 2; ++w) {
+      if (!wp.width[w]) continue;
+      const long long ws = wp.slot[w][o];
+      if (ws < 0) continue;
+      wp.arena[wp.base[w] + (size_t)(ws / wp.width[w]) * wp.fpn[w] + 6 * wp.width[w] + (size_t)(ws % wp.width[w])] =
+          want ? wp.ref[w][o] : kEmptyRef;
+    }
+  }
+  if (threadIdx.x == 0) {
+    misc[0] = maxToggles == 0 ? sh.total : min(sh.total, maxToggles);
+    misc[4] = misc[3];
+    misc[3] = 0;
+  }
+  __syncthreads();  // res[] complete for the light rebuild
+  lights_rebuild(la.em, la.ne, la.primAct, res, la.idx, la.cdf, la.pdf, la.meta, on, ltotal, lcount);
 }
 
 float luminance_host(const float *c) { return c[0] * 0.2126f + c[1] * 0.7152f + c[2] * 0.0722f; }
@@ -366,6 +442,9 @@ nomad_status nomad_residency_init(nomad_ctx *ctx) {
   for (uint32_t o = 0; o < N; ++o) {
     const nomad_instance_record &r = ctx->instances[o];
     R.hostBytes[o] = 32ull * nodes[o] + 196ull * r.primitive_count;
+    // the selection kernel packs bytes / 4 into 32 bits
+    if (R.hostBytes[o] >= (1ull << 34))
+      return nomad_fail(ctx, NOMAD_ERR_LIMIT, "an object holds 16 GB or more of geometry");
     tris[o] = r.primitive_count;
     float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
     for (uint32_t p = r.primitive_base; p < r.primitive_base + r.primitive_count; ++p) {
@@ -500,38 +579,51 @@ extern "C" nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residen
   }
   for (int k = 0; k < 3; ++k) R.prevCam[k] = cam.pos[k];
   R.havePrevCam = true;
-  k_features<<<(N + 127) / 128, 128, 0, s>>>(N, cam, R.bounds.as<const float4>(), R.bytes.as<const unsigned long long>(),
-                                             R.tris.as<const uint32_t>(), R.emit.as<const float>(),
-                                             R.objRes.as<const uint8_t>(), ctx->objHits.as<uint32_t>(),
-                                             R.hist.as<uint32_t>(), R.score.as<float>(), R.lastHit.as<uint32_t>(),
-                                             R.prevDist.as<float>(), R.visible.as<uint8_t>(), R.features.as<float>(),
-                                             R.keys.as<float>(), R.misc.as<uint32_t>(), R.frame, prm->hit_decay,
-                                             prm->memory_pressure);
-  NOMAD_CUDA(ctx, cudaGetLastError());
+  FeatArgs fa{N, cam, R.bounds.as<const float4>(), R.bytes.as<const unsigned long long>(), R.tris.as<const uint32_t>(),
+              R.emit.as<const float>(), R.objRes.as<const uint8_t>(), ctx->objHits.as<uint32_t>(), R.hist.as<uint32_t>(),
+              R.score.as<float>(), R.lastHit.as<uint32_t>(), R.prevDist.as<float>(), R.visible.as<uint8_t>(),
+              R.features.as<float>(), R.misc.as<uint32_t>(), R.frame, prm->hit_decay, prm->memory_pressure};
   if (prm->policy == NOMAD_POLICY_LEARNED) {
-    nomad_status st = nomad_mlp_infer_device(ctx, R.features.as<const float>(), N, R.keys.as<float>());
+    // features and scores in one kernel (the scorer's CTAs compute their rows' features)
+    nomad_status st = nomad_mlp_score_objects(ctx, &fa, R.keys.as<float>());
     if (st != NOMAD_OK) return st;
+  } else {
+    k_features<<<(N + 127) / 128, 128, 0, s>>>(fa, R.keys.as<float>());
+    NOMAD_CUDA(ctx, cudaGetLastError());
   }
   uint32_t npow2 = 1;
   while (npow2 < N) npow2 <<= 1;
   size_t smem = (size_t)npow2 * 10;  // sort keys, selected and candidate flags
-  NOMAD_CUDA(ctx, cudaFuncSetAttribute(k_select, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (smem > 48 * 1024)
+    NOMAD_CUDA(ctx, cudaFuncSetAttribute(k_select, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   float motion = std::min(std::max(prm->camera_motion, 0.0f), 1.0f);
   uint32_t reserve = (uint32_t)std::min<double>(N, std::ceil(N * (prm->reserve_base + prm->reserve_motion * motion)));
-  NOMAD_CUDA(ctx, cudaMemsetAsync(R.misc.p, 0, 8, s));  // toggles, root flag
+  WidePatch wp{};
+  wp.arena = static_cast<int32_t *>(ctx->arena.p);
+  for (int w = 0; w < 2; ++w) {
+    const nomad::WideLayout &WL = ctx->wide[w];
+    wp.width[w] = WL.width;
+    wp.fpn[w] = WL.floatsPerNode;
+    wp.base[w] = ctx->wideWordBase[w];
+    wp.slot[w] = ctx->wideSlot[w].as<const long long>();
+    wp.ref[w] = ctx->wideRef[w].as<const int32_t>();
+  }
+  FrameState &F = ctx->frame;
+  LightArgs la{R.emissive.as<const uint4>(), R.emissiveCount, R.primAct.as<const uint8_t>(), F.lightIdx.as<uint32_t>(),
+               F.lightCdf.as<float>(), F.lightPdf.as<float>(), F.lightMeta.as<LightMeta>()};
+  // one kernel: selection, toggles, pair and wide layout patches, light CDF
   k_select<<<1, 1024, smem, s>>>(N, npow2, prm->policy, R.keys.as<const float>(), R.visible.as<const uint8_t>(),
                                  R.bytes.as<const unsigned long long>(), prm->budget_bytes, reserve, prm->min_active,
                                  prm->max_toggles, R.desired.as<uint8_t>(), R.objRes.as<uint8_t>(),
                                  R.objSlot.as<const long long>(), R.objBlasRef.as<const int32_t>(),
-                                 static_cast<int32_t *>(ctx->arena.p), R.misc.as<uint32_t>());
+                                 static_cast<int32_t *>(ctx->arena.p), R.misc.as<uint32_t>(), wp, la);
   NOMAD_CUDA(ctx, cudaGetLastError());
-  ctx->frame.lightsDirty = true;
-  nomad_status st = nomad_lights_update(ctx);
-  if (st != NOMAD_OK) return st;
+  F.lightsDirty = false;
+  nomad_status st = NOMAD_OK;
   ++R.frame;
   ctx->frame.restirValid = false;
   if (!toggled && ctx->layout.tlasPairCount > 0) {
-    // Asynchronous step: the wide layouts follow the device flags on the stream, the host mirror
+    // Asynchronous step: the selection kernel patched every layout on the stream; the host mirror
     // is refreshed from a pinned copy when a host call needs it. (Without a TLAS the root ref
     // itself changes and is set on the host: the synchronous path below.)
     if (ctx->resPinnedBytes < N) {
@@ -542,8 +634,6 @@ extern "C" nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residen
       ctx->resPinnedBytes = N;
     }
     if (!ctx->resEvent) NOMAD_CUDA(ctx, cudaEventCreateWithFlags(&ctx->resEvent, cudaEventDisableTiming));
-    st = nomad_patch_wide(ctx);
-    if (st != NOMAD_OK) return st;
     NOMAD_CUDA(ctx, cudaMemcpyAsync(ctx->resPinned, R.objRes.p, N, cudaMemcpyDeviceToHost, s));
     NOMAD_CUDA(ctx, cudaEventRecord(ctx->resEvent, s));
     ctx->resHostStale = true;

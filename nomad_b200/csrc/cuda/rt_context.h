@@ -149,6 +149,12 @@ nomad_status nomad_residency_sync_host(nomad_ctx *ctx);
 
 void nomad_mlp_free(void *p);
 nomad_status nomad_mlp_infer_device(nomad_ctx *ctx, const float *X, uint64_t n, float *y);
+namespace nomad_res {
+struct FeatArgs;
+}
+// Learned policy: per-object features (as the feature kernel computes them) and MLP scores in one
+// launch; keys[o] receives the score.
+nomad_status nomad_mlp_score_objects(nomad_ctx *ctx, const nomad_res::FeatArgs *fa, float *keys);
 // Residency device state: created at upload, mirrored after host-side flushes.
 nomad_status nomad_residency_init(nomad_ctx *ctx);
 nomad_status nomad_residency_mirror(nomad_ctx *ctx);

@@ -122,3 +122,38 @@ def test_residency_step_against_oracle(nb, orc, ctx, small_city, policy, sync_to
     img = ctx.render(v)[0].reshape(-1, 3)
     want_img, _, _ = orc.render(ref, sb.materials, v)
     assert (img == want_img).all(1).mean() > 0.99
+
+
+@pytest.mark.parametrize("policy", [1, 2])
+def test_residency_step_many_objects(nb, orc, ctx, policy):
+    """2,048 objects (the learned-residency object count): the selection kernel's block-parallel
+    budget walks span several sorted positions per thread; flags must equal the restatement."""
+    from oracle import residency as ores
+
+    scene = nb.synth_city(seed=31, grid=64, grid_z=32, size_m=2000.0, target_tris=150_000, median_tris=60,
+                          max_tris=2_000, emissive_quads=16)
+    sb = nb.SceneBVH(scene)
+    assert sb.object_count >= 2048
+    ctx.upload(sb)
+    if policy == nb.POLICY_LEARNED:
+        ctx.mlp_init(3)
+    nbytes = ctx.object_bytes()
+    for frac in (0.4, 0.1):
+        budget = int(frac * nbytes.sum())
+        prm = nb.ResidencyParams.make(policy, budget_bytes=budget, camera_motion=0.7, memory_pressure=0.5,
+                                      min_active=5)
+        flags = ctx.residency_flags()
+        for frame, pos in enumerate([(0, 80, -900), (100, 60, -700)]):
+            view = nb.view_pinhole(pos, (0, 0, 0), width=96, height=54, spp=2, max_depth=2, seed=frame)
+            ctx.reset_object_hits()
+            ctx.render(view, count_hits=True)
+            toggles = ctx.residency_step(prm, view)
+            feats, keys = ctx.residency_last()
+            visible = feats[:, 2] > 0.5
+            reserve = ores.reserve_count(sb.object_count, 0.02, 0.06, 0.7)
+            want, want_t = ores.select(keys, visible, nbytes, budget, reserve, 5, flags)
+            got = ctx.residency_flags()
+            assert np.array_equal(got, want), (frac, frame, np.nonzero(got != want)[0][:10])
+            assert toggles == want_t
+            flags = got
+    assert ctx.status() == 0
