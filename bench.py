@@ -359,6 +359,31 @@ def run_profile_frame(args):
     ctx.close()
 
 
+def run_profile_restir(args):
+    """The ReSTIR leg's timing frame: city with 4,096 emissive triangles, 1920x1080 x 1 spp,
+    direct lighting by ReSTIR (32 candidates, temporal + 3 spatial), three frames."""
+    import torch
+
+    import nomad_b200 as nb
+
+    scene = nb.synth_city(seed=SEED, emissive_tris=4096, emissive_sigma=1.5)
+    sb = nb.SceneBVH(scene)
+    ctx = nb.Context(0)
+    ctx.upload(sb)
+    select_kernel(ctx, args.kernel or 4, args.min_blocks)
+    ctx.set_restir(candidates=32, temporal=True, spatial=3, radius_px=30.0, m_cap=20.0)
+    v = nb.view_pinhole((0.0, 220.0, -620.0), (0.0, 0.0, 60.0), width=WIDTH, height=HEIGHT, spp=1, max_depth=1,
+                        seed=SEED, flags=nb.VIEW_RESTIR)
+    out = torch.empty(WIDTH * HEIGHT * 3, dtype=torch.float32, device="cuda")
+    for f in range(3):
+        v["frame"] = f + 1
+        ctx.render_dev(v, out.data_ptr())
+    ctx.sync()
+    assert ctx.status() == 0
+    print(json.dumps({"profile_restir": "city + 4,096 emissive tris, 1920x1080 x 1 spp", "frames": 3}))
+    ctx.close()
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -421,6 +446,8 @@ def main():
                          "one batch, one warm-up and two timed launches of the chosen kernel (--kernel)")
     ap.add_argument("--profile-frame", action="store_true",
                     help="path-traced city frame (1920x1080 x 4 spp, 3 bounces) rendered twice, for launch lists")
+    ap.add_argument("--profile-restir", action="store_true",
+                    help="ReSTIR city (4,096 emissive triangles), 1920x1080 x 1 spp, three frames, for launch lists")
     args = ap.parse_args()
     CONFIG["spp"] = args.spp
     if args.impl == "reference":
@@ -429,6 +456,8 @@ def main():
         return run_profile_case(args)
     if args.profile_frame:
         return run_profile_frame(args)
+    if args.profile_restir:
+        return run_profile_restir(args)
 
     import torch
     import torch.distributed as dist

@@ -12,4 +12,4 @@ from .native import (  # noqa: F401
     KERNEL_AUTO, KERNEL_BVH2, KERNEL_BVH2_PERSIST, KERNEL_BVH4, KERNEL_BVH4_PERSIST, KERNEL_BVH8,
     KERNEL_BVH8_PERSIST, KERNEL_NAMES, TRACE_COUNT_HITS, TRACE_DEVICE_POINTERS,
 )
-from .rays import Camera, bounce_rays, city_camera, icosphere_camera  # noqa: F401
+from .rays import Camera, bounce_rays, city_camera, icosphere_camera, shadow_rays  # noqa: F401

@@ -96,6 +96,46 @@ def bounce_rays(rays: np.ndarray, hits: np.ndarray, prims: np.ndarray, seed: int
     return out
 
 
+def shadow_rays(rays: np.ndarray, hits: np.ndarray, prims: np.ndarray, materials: np.ndarray,
+                seed: int = 1) -> np.ndarray:
+    """One shadow ray per hit ray (misses dropped), as the path tracer's next-event estimation
+    casts them: from the hit point offset 5e-4 along the normal toward a uniformly drawn point on
+    a uniformly drawn emissive primitive, tmax = distance - 1e-4 (any-hit queries)."""
+    g = prims.reshape(-1, 28)
+    m = materials.reshape(-1, 20)
+    lum = m[:, 8] * 0.2126 + m[:, 9] * 0.7152 + m[:, 10] * 0.0722
+    emissive = np.nonzero(m[:, 11] * lum > 0)[0]
+    keep = hits["prim"] >= 0
+    r, h = rays[keep], hits[keep]
+    o = np.stack([r["ox"], r["oy"], r["oz"]], 1)
+    d = np.stack([r["dx"], r["dy"], r["dz"]], 1)
+    p = (o + h["t"][:, None] * d).astype(np.float32)
+    n = _norm(hit_normals(prims, h))
+    flip = (n * d).sum(1) > 0
+    n[flip] = -n[flip]
+    rng = np.random.default_rng(seed)
+    e = emissive[rng.integers(0, emissive.shape[0], p.shape[0])]
+    u1 = rng.random(p.shape[0], dtype=np.float32)
+    u2 = rng.random(p.shape[0], dtype=np.float32)
+    a, b, c = g[e, 0:3], g[e, 4:7], g[e, 8:11]
+    tri = g[e, 3] == 1
+    su = np.sqrt(u1)[:, None]
+    q_tri = a * (1 - su) + b * (su * (1 - u2[:, None])) + c * (su * u2[:, None])
+    q_rect = a + (2 * u1[:, None] - 1) * b + (2 * u2[:, None] - 1) * c
+    q = np.where(tri[:, None], q_tri, q_rect).astype(np.float32)
+    org = (p + np.float32(5e-4) * n).astype(np.float32)
+    to = q - org
+    dist = np.linalg.norm(to, axis=1)
+    ok = dist > 2e-4
+    out = np.empty(int(ok.sum()), RAY_DTYPE)
+    dd = (to[ok] / dist[ok, None]).astype(np.float32)
+    out["ox"], out["oy"], out["oz"] = org[ok, 0], org[ok, 1], org[ok, 2]
+    out["tmin"] = RAY_EPS
+    out["dx"], out["dy"], out["dz"] = dd[:, 0], dd[:, 1], dd[:, 2]
+    out["tmax"] = (dist[ok] - np.float32(1e-4)).astype(np.float32)
+    return out
+
+
 def icosphere_camera(width=640, height=360) -> Camera:
     """Camera outside the 100 m cube of the icosphere scene, looking at its centre."""
     return Camera((0.0, 40.0, 170.0), (0.0, 0.0, 0.0), vfov=60.0, width=width, height=height)

@@ -302,6 +302,9 @@ def test_full_city_variants(nb, orc, ctx):
     want = ref.closest(rays)
     b = nb.bounce_rays(rays, want, sb.prims, seed=8)
     want_b = ref.closest(b)
+    sh = nb.shadow_rays(rays, want, sb.prims, sb.materials, seed=9)
+    want_s = ref.any(sh)
+    assert 0.05 < want_s.mean() < 0.999
     configs = [dict(width=w, persistent=3) for w in (2, 4, 8)]
     configs += [dict(width=w, persistent=2, short_stack=s, regroup=24, postpone_leaves=1) for w, s in ((2, 8), (4, 0), (8, 16))]
     configs += [dict(width=w, persistent=1, min_blocks=10) for w in (2, 4, 8)]
@@ -309,5 +312,6 @@ def test_full_city_variants(nb, orc, ctx):
         ctx.set_traversal(**c)
         _assert_hits_equal(ctx.trace_closest(rays), want)
         _assert_hits_equal(ctx.trace_closest(b), want_b)
+        assert np.array_equal(ctx.trace_any(sh), want_s), c
         assert ctx.status() == 0, c
     ctx.set_kernel(1)
