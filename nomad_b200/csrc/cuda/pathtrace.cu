@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <cstring>
 
+#include "pt_lights.cuh"
 #include "pt_math.cuh"
 #include "rt_context.h"
 
@@ -49,6 +50,7 @@ struct Lights {
   const uint32_t *idx;
   const float *cdf;
   const LightMeta *meta;
+  const float4 *rec;  // per CDF slot, 5 float4 (pt_lights.cuh)
 };
 
 __device__ __forceinline__ const ViewDev &find_view(const ViewDev *views, uint32_t nviews,
@@ -79,8 +81,6 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t *len, bool want) {
   base = __shfl_sync(act, base, leader);
   return base + __popc(m & ((1u << lane) - 1u));
 }
-
-__device__ __forceinline__ V3 ld3(const float4 &f) { return v3(f.x, f.y, f.z); }
 
 __global__ void __launch_bounds__(kPtBlock) k_raygen(const ViewDev *__restrict__ views, uint32_t nviews,
                                                       unsigned long long P, float4 *__restrict__ rays,
@@ -283,44 +283,11 @@ __device__ __forceinline__ V3 scatter(V3 inDir, V3 normal, bool frontFace, const
 // sampleLightPoint (PathTracing.h:582-643).
 __device__ __forceinline__ bool sample_light(const float4 *__restrict__ prims, uint32_t lp, float u1, float u2,
                                              V3 &pos, V3 &nrm, float &area) {
-  const float4 *g = prims + 7ll * lp;
-  float4 p0 = __ldg(g), p1 = __ldg(g + 1), p2 = __ldg(g + 2);
-  int type = (int)p0.w;
-  if (type == 0) {
-    float radius = p1.x;
-    if (radius <= 0.0f) return false;
-    float z = 2.0f * u1 - 1.0f;
-    float s, c;
-    sincos_turns(u2, s, c);
-    float r = sqrtf(fmax_ref(0.0f, 1.0f - z * z));
-    V3 dir = v3(r * c, r * s, z);
-    pos = ld3(p0) + dir * radius;
-    nrm = dir;
-    area = 4.0f * kPi * radius * radius;
-    return area > 0.0f;
-  } else if (type == 1) {
-    float su1 = sqrtf(u1);
-    float b0 = 1.0f - su1, b1 = su1 * (1.0f - u2), b2 = su1 * u2;
-    V3 v0 = ld3(p0), v1 = ld3(p1), v2 = ld3(p2);
-    pos = v0 * b0 + v1 * b1 + v2 * b2;
-    V3 n = cross(v1 - v0, v2 - v0);
-    float ln = length(n);
-    if (ln <= 0.0f) return false;
-    nrm = n / ln;
-    area = 0.5f * ln;
-    return area > 0.0f;
-  } else if (type == 2) {
-    float su = u1 * 2.0f - 1.0f, sv = u2 * 2.0f - 1.0f;
-    V3 c = ld3(p0), e1 = ld3(p1), e2 = ld3(p2);
-    pos = c + e1 * su + e2 * sv;
-    V3 n = cross(e1, e2);
-    float ln = length(n);
-    if (ln <= 0.0f) return false;
-    nrm = n / ln;
-    area = 4.0f * ln;
-    return area > 0.0f;
-  }
-  return false;
+  const LightShape s = light_shape(prims, lp);
+  if (!s.valid) return false;
+  pos = light_point(s, u1, u2, nrm);
+  area = s.area;
+  return true;
 }
 
 // selectLightOffset (PathTracing.h:219-235).
@@ -335,7 +302,7 @@ __device__ __forceinline__ uint32_t select_light(float xi, const Lights &L, uint
   return lo < count - 1 ? lo : count - 1;
 }
 
-__global__ void __launch_bounds__(kPtBlock) k_shade(
+__global__ void __launch_bounds__(kPtBlock, 3) k_shade(
     uint32_t depth, const ViewDev *__restrict__ views, uint32_t nviews, const float4 *__restrict__ qRays,
     const uint32_t *__restrict__ qIds, const int32_t *__restrict__ hits, float4 *__restrict__ nRays,
     uint32_t *__restrict__ nIds, float4 *__restrict__ sRays, uint32_t *__restrict__ sIds,
@@ -687,7 +654,8 @@ extern "C" nomad_status nomad_render_frame(nomad_ctx *ctx, const nomad_view *vie
 
   const ViewDev *V = F.views.as<const ViewDev>();
   Counters *C = F.counters.as<Counters>();
-  Lights L{F.lightIdx.as<const uint32_t>(), F.lightCdf.as<const float>(), F.lightMeta.as<const LightMeta>()};
+  Lights L{F.lightIdx.as<const uint32_t>(), F.lightCdf.as<const float>(), F.lightMeta.as<const LightMeta>(),
+           F.lightRec.as<const float4>()};
   uint32_t *objHits = (flags & NOMAD_TRACE_COUNT_HITS) ? ctx->objHits.as<uint32_t>() : nullptr;
   bool anyRestir = false;
   for (uint32_t i = 0; i < nviews; ++i) anyRestir |= (views[i].flags & NOMAD_VIEW_RESTIR) != 0;
@@ -907,6 +875,24 @@ __device__ __forceinline__ float restir_target(const float4 *__restrict__ mats, 
   return fmax_ref(luminance(fa), 0.0f);
 }
 
+// restir_target with the light's emitted radiance given (from its light record).
+__device__ __forceinline__ float restir_target_rad(const Material &m, const Surf &s, V3 lpos, V3 lnrm, int32_t lp,
+                                                   V3 lrad) {
+  if (lp < 0 || lp == __float_as_int(s.n.w)) return 0.0f;
+  V3 p = ld3(s.p), n = ld3(s.n);
+  V3 toL = lpos - p;
+  float dist2 = dot(toL, toL);
+  if (dist2 <= kRayEps) return 0.0f;
+  float dist = sqrtf(dist2);
+  V3 wi = toL / dist;
+  float cosT = fmax_ref(dot(n, wi), 0.0f), cosL = fmax_ref(dot(lnrm, -wi), 0.0f);
+  if (cosT <= 0.0f || cosL <= 0.0f) return 0.0f;
+  V3 f = eval_bsdf(m, n, ld3(s.v), wi) * lrad * cosT;
+  float g = cosL / fmax_ref(dist2, kRayEps);
+  V3 fa = f * g;
+  return fmax_ref(luminance(fa), 0.0f);
+}
+
 __device__ __forceinline__ bool restir_gate(const Surf &s, const Surf &q) {
   if (q.v.w <= 0.0f) return false;
   float depth = s.p.w;
@@ -940,7 +926,7 @@ __device__ __forceinline__ void restir_merge(Resv &out, const Resv &src, const S
   }
 }
 
-__global__ void __launch_bounds__(kPtBlock) k_restir_initial(
+__global__ void __launch_bounds__(kPtBlock, 3) k_restir_initial(
     const ViewDev *__restrict__ views, uint32_t nviews, unsigned long long P, RestirDev cfg,
     const float4 *__restrict__ rays, const int32_t *__restrict__ hits, const float4 *__restrict__ prims,
     const float4 *__restrict__ mats, Lights L, Resv *__restrict__ rOut, Surf *__restrict__ sOut) {
@@ -971,17 +957,17 @@ __global__ void __launch_bounds__(kPtBlock) k_restir_initial(
         for (uint32_t c = 0; c < cfg.candidates; ++c) {
           U4 u = philox(U4{pixel, sample, 0x10000u + c, v.index}, v.k0, v.k1);
           uint32_t off = select_light(u01(u.x), L, lightCount, lightTotal);
-          int32_t lp = (int32_t)__ldg(L.idx + off);
+          // the light's sample-independent values come from its per-frame record
+          const float4 *rec = L.rec + 5ull * off;
+          const float4 r3 = __ldg(rec + 3), r4 = __ldg(rec + 4);
+          int32_t lp = __float_as_int(r3.w);
           V3 lpos, lnrm;
-          float area = 0.0f, w = 0.0f, ph = 0.0f;
-          if (lp != prim && sample_light(prims, (uint32_t)lp, u01(u.y), u01(u.z), lpos, lnrm, area) && area > 0.0f) {
-            float prev = off > 0 ? __ldg(L.cdf + off - 1) : 0.0f;
-            float wgt = __ldg(L.cdf + off) - prev;
-            float lpdf = wgt > 0.0f ? wgt / lightTotal : 0.0f;
-            float q = lpdf * (1.0f / area);
-            V3 fa, wi;
-            float dist;
-            ph = restir_target(mats, m, s, lpos, lnrm, lp, fa, wi, dist);
+          float w = 0.0f, ph = 0.0f;
+          if (lp != prim && r4.w > 0.0f) {
+            const LightShape sh = record_shape(rec);
+            lpos = light_point(sh, u01(u.y), u01(u.z), lnrm);
+            const float q = __ldg(rec + 2).w;
+            ph = restir_target_rad(m, s, lpos, lnrm, lp, ld3(r4));
             w = q > 0.0f ? ph / q : 0.0f;
           }
           r.c.z = r.c.z + 1.0f;
@@ -1041,7 +1027,7 @@ __global__ void __launch_bounds__(kPtBlock) k_restir_temporal(
   }
 }
 
-__global__ void __launch_bounds__(kPtBlock) k_restir_spatial(
+__global__ void __launch_bounds__(kPtBlock, 3) k_restir_spatial(
     const ViewDev *__restrict__ views, uint32_t nviews, unsigned long long P, RestirDev cfg,
     const float4 *__restrict__ mats, const Resv *__restrict__ rIn, const Surf *__restrict__ sCur,
     Resv *__restrict__ rOut) {

@@ -21,6 +21,7 @@
 #include <cstring>
 #include <vector>
 
+#include "pt_lights.cuh"
 #include "residency_features.cuh"
 #include "rt_context.h"
 
@@ -202,7 +203,8 @@ __device__ void budget_walk(uint32_t n, uint32_t npow2, const unsigned long long
 __device__ void lights_rebuild(const uint4 *__restrict__ em, uint32_t ne, const uint8_t *__restrict__ primAct,
                                const uint8_t *objRes, uint32_t *__restrict__ idx, float *__restrict__ cdf,
                                float *__restrict__ pdf, LightMeta *__restrict__ meta, uint8_t *on, float &total_s,
-                               uint32_t &count_s) {
+                               uint32_t &count_s, const float4 *__restrict__ prims, const float4 *__restrict__ mats,
+                               float4 *__restrict__ rec) {
   if (threadIdx.x == 0) {
     total_s = 0.0f;
     count_s = 0;
@@ -244,17 +246,27 @@ __device__ void lights_rebuild(const uint4 *__restrict__ em, uint32_t ne, const 
       if (w > 0.0f && total > 0.0f) pdf[idx[k]] = w / total;
     }
   }
+  __syncthreads();
+  // light records of the new CDF (the weight of slot k is cdf[k] - cdf[k-1], as samplers read it)
+  const uint32_t c = count_s;
+  const float total = total_s;
+  for (uint32_t k = threadIdx.x; k < c; k += blockDim.x) {
+    const float prev = k > 0 ? cdf[k - 1] : 0.0f;
+    nomad_pt::light_record(prims, mats, idx[k], cdf[k] - prev, total, rec + 5ull * k);
+  }
 }
 
 __global__ void __launch_bounds__(1024) k_lights_rebuild(const uint4 *__restrict__ em, uint32_t ne,
                                                          const uint8_t *__restrict__ primAct,
                                                          const uint8_t *__restrict__ objRes,
                                                          uint32_t *__restrict__ idx, float *__restrict__ cdf,
-                                                         float *__restrict__ pdf, LightMeta *__restrict__ meta) {
+                                                         float *__restrict__ pdf, LightMeta *__restrict__ meta,
+                                                         const float4 *__restrict__ prims,
+                                                         const float4 *__restrict__ mats, float4 *__restrict__ rec) {
   __shared__ uint8_t on[4096];
   __shared__ float total_s;
   __shared__ uint32_t count_s;
-  lights_rebuild(em, ne, primAct, objRes, idx, cdf, pdf, meta, on, total_s, count_s);
+  lights_rebuild(em, ne, primAct, objRes, idx, cdf, pdf, meta, on, total_s, count_s, prims, mats, rec);
 }
 
 // Wide-layout instance slots that one step rewrites (4- and 8-wide).
@@ -273,6 +285,8 @@ struct LightArgs {
   uint32_t *idx;
   float *cdf, *pdf;
   LightMeta *meta;
+  const float4 *prims, *mats;
+  float4 *rec;
 };
 
 // Single block of 1024 threads, the whole residency decision of one step: sort by score, select
@@ -387,7 +401,8 @@ __global__ void __launch_bounds__(1024) k_select(uint32_t n, uint32_t npow2, uin
     misc[3] = 0;
   }
   __syncthreads();  // res[] complete for the light rebuild
-  lights_rebuild(la.em, la.ne, la.primAct, res, la.idx, la.cdf, la.pdf, la.meta, on, ltotal, lcount);
+  lights_rebuild(la.em, la.ne, la.primAct, res, la.idx, la.cdf, la.pdf, la.meta, on, ltotal, lcount, la.prims, la.mats,
+                 la.rec);
 }
 
 float luminance_host(const float *c) { return c[0] * 0.2126f + c[1] * 0.7152f + c[2] * 0.0722f; }
@@ -504,6 +519,7 @@ nomad_status nomad_residency_init(nomad_ctx *ctx) {
   NOMAD_CUDA(ctx, cudaMemcpy(R.emit.p, emit.data(), (size_t)N * 4, cudaMemcpyHostToDevice));
   FrameState &F = ctx->frame;
   NOMAD_CUDA(ctx, F.lightIdx.reserve(std::max<size_t>(1, em.size()) * 4));
+  NOMAD_CUDA(ctx, F.lightRec.reserve(std::max<size_t>(1, em.size()) * 80));
   NOMAD_CUDA(ctx, F.lightCdf.reserve(std::max<size_t>(1, em.size()) * 4));
   NOMAD_CUDA(ctx, F.lightPdf.reserve((size_t)P * 4));
   NOMAD_CUDA(ctx, F.lightMeta.reserve(sizeof(LightMeta)));
@@ -534,7 +550,8 @@ nomad_status nomad_lights_update(nomad_ctx *ctx) {
   k_lights_rebuild<<<1, 1024, 0, ctx->stream>>>(R.emissive.as<const uint4>(), R.emissiveCount,
                                                 R.primAct.as<const uint8_t>(), R.objRes.as<const uint8_t>(),
                                                 F.lightIdx.as<uint32_t>(), F.lightCdf.as<float>(), F.lightPdf.as<float>(),
-                                                F.lightMeta.as<LightMeta>());
+                                                F.lightMeta.as<LightMeta>(), ctx->prims.as<const float4>(),
+                                                ctx->materials.as<const float4>(), F.lightRec.as<float4>());
   NOMAD_CUDA(ctx, cudaGetLastError());
   F.lightsDirty = false;
   return NOMAD_OK;
@@ -610,7 +627,8 @@ extern "C" nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residen
   }
   FrameState &F = ctx->frame;
   LightArgs la{R.emissive.as<const uint4>(), R.emissiveCount, R.primAct.as<const uint8_t>(), F.lightIdx.as<uint32_t>(),
-               F.lightCdf.as<float>(), F.lightPdf.as<float>(), F.lightMeta.as<LightMeta>()};
+               F.lightCdf.as<float>(), F.lightPdf.as<float>(), F.lightMeta.as<LightMeta>(),
+               ctx->prims.as<const float4>(), ctx->materials.as<const float4>(), F.lightRec.as<float4>()};
   // one kernel: selection, toggles, pair and wide layout patches, light CDF
   k_select<<<1, 1024, smem, s>>>(N, npow2, prm->policy, R.keys.as<const float>(), R.visible.as<const uint8_t>(),
                                  R.bytes.as<const unsigned long long>(), prm->budget_bytes, reserve, prm->min_active,

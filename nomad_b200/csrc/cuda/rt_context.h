@@ -49,6 +49,7 @@ struct FrameState {
   DeviceBuf counters;                 // queue lengths, cursors, statistics
   DeviceBuf views;                    // view table
   DeviceBuf lightIdx, lightCdf, lightPdf, lightMeta;
+  DeviceBuf lightRec;                 // per CDF slot, 5 float4 (pt_lights.cuh)
   bool lightsDirty = true;
   // ReSTIR DI: per-path reservoirs (initial, temporal, final of this and the previous frame),
   // surface records (this and the previous frame) and the previous frame's view table
