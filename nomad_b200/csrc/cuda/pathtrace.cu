@@ -31,6 +31,11 @@ using namespace nomad_pt;
 namespace {
 
 constexpr int kPtBlock = 256;
+// Resident blocks per SM the ReSTIR candidate and spatial kernels are compiled for (a register
+// cap: measured faster than the uncapped build; the shading kernel is faster uncapped).
+#ifndef NOMAD_PT_MINB
+#define NOMAD_PT_MINB 3
+#endif
 constexpr float kPi = 3.14159265358979323846f;
 
 struct ViewDev {
@@ -302,7 +307,19 @@ __device__ __forceinline__ uint32_t select_light(float xi, const Lights &L, uint
   return lo < count - 1 ? lo : count - 1;
 }
 
-__global__ void __launch_bounds__(kPtBlock, 3) k_shade(
+// The same search over a CDF copy (shared memory): the same predicate, so the same slot.
+__device__ __forceinline__ uint32_t select_light_cdf(float xi, const float *cdf, uint32_t count, float total) {
+  float target = xi * total;
+  uint32_t lo = 0, hi = count;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) / 2;
+    if (cdf[mid] < target) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo < count - 1 ? lo : count - 1;
+}
+
+__global__ void __launch_bounds__(kPtBlock) k_shade(
     uint32_t depth, const ViewDev *__restrict__ views, uint32_t nviews, const float4 *__restrict__ qRays,
     const uint32_t *__restrict__ qIds, const int32_t *__restrict__ hits, float4 *__restrict__ nRays,
     uint32_t *__restrict__ nIds, float4 *__restrict__ sRays, uint32_t *__restrict__ sIds,
@@ -727,6 +744,7 @@ extern "C" nomad_status nomad_render_frame(nomad_ctx *ctx, const nomad_view *vie
       key_put(key, w.root);
     }
     key_put(key, ctx->smCount);
+    key_put(key, ctx->res.emissiveCount);
     key_put(key, ctx->prims.p);
     key_put(key, ctx->materials.p);
     for (const DeviceBuf *b : {&F.thr, &F.rad, &F.qRays[0], &F.qRays[1], &F.qIds[0], &F.qIds[1], &F.hits, &F.sRays,
@@ -926,12 +944,19 @@ __device__ __forceinline__ void restir_merge(Resv &out, const Resv &src, const S
   }
 }
 
-__global__ void __launch_bounds__(kPtBlock, 3) k_restir_initial(
+// The light CDF is staged in shared memory when it fits the block's allocation (cdfCap entries):
+// every candidate binary-searches it, 32 per path.
+__global__ void __launch_bounds__(kPtBlock, NOMAD_PT_MINB) k_restir_initial(
     const ViewDev *__restrict__ views, uint32_t nviews, unsigned long long P, RestirDev cfg,
     const float4 *__restrict__ rays, const int32_t *__restrict__ hits, const float4 *__restrict__ prims,
-    const float4 *__restrict__ mats, Lights L, Resv *__restrict__ rOut, Surf *__restrict__ sOut) {
+    const float4 *__restrict__ mats, Lights L, Resv *__restrict__ rOut, Surf *__restrict__ sOut, uint32_t cdfCap) {
+  extern __shared__ float sCdf[];
   const uint32_t lightCount = L.meta->count;
   const float lightTotal = L.meta->total;
+  const bool staged = lightCount <= cdfCap;
+  if (staged)
+    for (uint32_t i = threadIdx.x; i < lightCount; i += blockDim.x) sCdf[i] = L.cdf[i];
+  __syncthreads();
   for (unsigned long long pid = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; pid < P;
        pid += (unsigned long long)gridDim.x * blockDim.x) {
     const ViewDev &v = find_view(views, nviews, pid);
@@ -956,7 +981,8 @@ __global__ void __launch_bounds__(kPtBlock, 3) k_restir_initial(
         uint32_t pixel = (uint32_t)(local / v.spp), sample = (uint32_t)(local % v.spp);
         for (uint32_t c = 0; c < cfg.candidates; ++c) {
           U4 u = philox(U4{pixel, sample, 0x10000u + c, v.index}, v.k0, v.k1);
-          uint32_t off = select_light(u01(u.x), L, lightCount, lightTotal);
+          uint32_t off = staged ? select_light_cdf(u01(u.x), sCdf, lightCount, lightTotal)
+                                : select_light(u01(u.x), L, lightCount, lightTotal);
           // the light's sample-independent values come from its per-frame record
           const float4 *rec = L.rec + 5ull * off;
           const float4 r3 = __ldg(rec + 3), r4 = __ldg(rec + 4);
@@ -1027,7 +1053,7 @@ __global__ void __launch_bounds__(kPtBlock) k_restir_temporal(
   }
 }
 
-__global__ void __launch_bounds__(kPtBlock, 3) k_restir_spatial(
+__global__ void __launch_bounds__(kPtBlock, NOMAD_PT_MINB) k_restir_spatial(
     const ViewDev *__restrict__ views, uint32_t nviews, unsigned long long P, RestirDev cfg,
     const float4 *__restrict__ mats, const Resv *__restrict__ rIn, const Surf *__restrict__ sCur,
     Resv *__restrict__ rOut) {
@@ -1136,9 +1162,10 @@ nomad_status restir_launch(nomad_ctx *ctx, uint32_t nviews, unsigned long long P
   const int cur = plan.cur;
   const int grid = ctx->smCount * 8;
   Surf *sCur = F.surf[cur].as<Surf>();
-  k_restir_initial<<<grid, kPtBlock, 0, s>>>(V, nviews, P, cfg, F.qRays[0].as<const float4>(), F.hits.as<const int32_t>(),
-                                            ctx->prims.as<const float4>(), ctx->materials.as<const float4>(), L,
-                                            F.rInit.as<Resv>(), sCur);
+  const uint32_t cdfCap = std::min<uint32_t>(ctx->res.emissiveCount, 8192u);
+  k_restir_initial<<<grid, kPtBlock, cdfCap * sizeof(float), s>>>(
+      V, nviews, P, cfg, F.qRays[0].as<const float4>(), F.hits.as<const int32_t>(), ctx->prims.as<const float4>(),
+      ctx->materials.as<const float4>(), L, F.rInit.as<Resv>(), sCur, cdfCap);
   k_restir_temporal<<<grid, kPtBlock, 0, s>>>(V, F.prevViews.as<const ViewDev>(), nviews, P, cfg,
                                              ctx->materials.as<const float4>(), F.rInit.as<const Resv>(), sCur,
                                              F.resv[cur ^ 1].as<const Resv>(), F.surf[cur ^ 1].as<const Surf>(),
