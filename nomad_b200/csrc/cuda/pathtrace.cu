@@ -286,15 +286,6 @@ __device__ __forceinline__ V3 scatter(V3 inDir, V3 normal, bool frontFace, const
 }
 
 // sampleLightPoint (PathTracing.h:582-643).
-__device__ __forceinline__ bool sample_light(const float4 *__restrict__ prims, uint32_t lp, float u1, float u2,
-                                             V3 &pos, V3 &nrm, float &area) {
-  const LightShape s = light_shape(prims, lp);
-  if (!s.valid) return false;
-  pos = light_point(s, u1, u2, nrm);
-  area = s.area;
-  return true;
-}
-
 // selectLightOffset (PathTracing.h:219-235).
 __device__ __forceinline__ uint32_t select_light(float xi, const Lights &L, uint32_t count, float total) {
   float target = xi * total;
@@ -380,11 +371,14 @@ __global__ void __launch_bounds__(kPtBlock) k_shade(
         bool restirHere = restirDepth0 && depth == 0 && (v.flags & NOMAD_VIEW_RESTIR);
         if (!restirHere && luminance(dc) > 0.0f && lightCount > 0 && lightTotal > 0.0f) {
           uint32_t off = select_light(u01(b0.x), L, lightCount, lightTotal);
-          uint32_t lp = __ldg(L.idx + off);
+          // the light's sample-independent values come from its per-frame record
+          const float4 *rec = L.rec + 5ull * off;
+          const float4 r4 = __ldg(rec + 4);
+          uint32_t lp = (uint32_t)__float_as_int(__ldg(rec + 3).w);
           if ((int32_t)lp != prim) {
             V3 lpos, lnrm;
-            float area = 0.0f;
-            if (sample_light(prims, lp, u01(b0.y), u01(b0.z), lpos, lnrm, area) && area > 0.0f) {
+            if (r4.w > 0.0f) {
+              lpos = light_point(record_shape(rec), u01(b0.y), u01(b0.z), lnrm);
               V3 toL = lpos - p;
               float dist2 = dot(toL, toL);
               if (dist2 > kRayEps) {
@@ -393,17 +387,13 @@ __global__ void __launch_bounds__(kPtBlock) k_shade(
                 float cosT = fmax_ref(dot(nrm, wi), 0.0f);
                 float cosL = fmax_ref(dot(lnrm, -wi), 0.0f);
                 if (cosT > 0.0f && cosL > 0.0f) {
-                  float cur_ = __ldg(L.cdf + off);
-                  float prev = off > 0 ? __ldg(L.cdf + off - 1) : 0.0f;
-                  float wgt = cur_ - prev;
-                  float lpdf = (lightTotal > 0.0f && wgt > 0.0f) ? wgt / lightTotal : 0.0f;
+                  float lpdf = __ldg(rec).w;  // weight / total (lightTotal > 0 here)
                   if (lpdf > 0.0f) {
-                    float pdfArea = 1.0f / area;
+                    float pdfArea = __ldg(rec + 1).w;  // 1 / area
                     float pdfSolid = pdfArea * dist2 / cosL;
                     float totalPdf = lpdf * pdfSolid;
                     if (totalPdf > 0.0f) {
-                      Material lm = decode_material(mats, (int32_t)lp, 1.0f);
-                      V3 lrad = lm.emission * lm.power;
+                      V3 lrad = ld3(r4);
                       V3 view = normalize(-d);
                       V3 bsdf = eval_bsdf(m, nrm, view, wi);
                       V3 c = tp * bsdf * lrad * (cosT / totalPdf);

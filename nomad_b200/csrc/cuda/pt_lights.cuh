@@ -74,35 +74,38 @@ __device__ __forceinline__ V3 light_point(const LightShape &s, float u1, float u
   return s.a + s.b * su + s.c * sv;
 }
 
-// Per-frame light record of CDF slot k (5 float4): shape, normal and prim, the constant part of
-// the ReSTIR candidate pdf, emitted radiance.
-//   [0] a.xyz, type      [1] b.xyz, area      [2] c.xyz, q = (cdf weight / total) * (1 / area)
-//   [3] nrm.xyz, prim    [4] emission * power, valid (1 or 0)
+// Per-frame light record of CDF slot k (5 float4): shape, normal and prim, the light-selection
+// pdf and 1/area (as the samplers compute them), the ReSTIR candidate pdf constant, radiance.
+//   [0] a.xyz, lpdf = weight / total      [1] b.xyz, 1 / area
+//   [2] c.xyz, q = lpdf * (1 / area)      [3] nrm.xyz, prim
+//   [4] emission * power, type + 1 when the sampler accepts the primitive, else 0
 __device__ __forceinline__ void light_record(const float4 *__restrict__ prims, const float4 *__restrict__ mats,
                                              uint32_t lp, float wgt, float total, float4 *__restrict__ rec) {
   const LightShape s = light_shape(prims, lp);
   const float lpdf = wgt > 0.0f ? wgt / total : 0.0f;
-  const float q = s.valid ? lpdf * (1.0f / s.area) : 0.0f;
+  const float inv = s.valid ? 1.0f / s.area : 0.0f;
+  const float q = lpdf * inv;
   const float4 m2 = __ldg(mats + 5ll * lp + 2);
   const V3 emission = vmax0(ld3(m2));
   const float power = fmax_ref(m2.w, 0.0f);
   const V3 lrad = emission * power;
-  rec[0] = make_float4(s.a.x, s.a.y, s.a.z, __int_as_float(s.type));
-  rec[1] = make_float4(s.b.x, s.b.y, s.b.z, s.area);
+  rec[0] = make_float4(s.a.x, s.a.y, s.a.z, lpdf);
+  rec[1] = make_float4(s.b.x, s.b.y, s.b.z, inv);
   rec[2] = make_float4(s.c.x, s.c.y, s.c.z, q);
   rec[3] = make_float4(s.nrm.x, s.nrm.y, s.nrm.z, __int_as_float((int32_t)lp));
-  rec[4] = make_float4(lrad.x, lrad.y, lrad.z, s.valid ? 1.0f : 0.0f);
+  rec[4] = make_float4(lrad.x, lrad.y, lrad.z, s.valid ? (float)(s.type + 1) : 0.0f);
 }
 
+// Shape of a record whose [4].w is positive (the sampler accepts it); area is not restored.
 __device__ __forceinline__ LightShape record_shape(const float4 *__restrict__ rec) {
-  const float4 r0 = __ldg(rec), r1 = __ldg(rec + 1), r2 = __ldg(rec + 2), r3 = __ldg(rec + 3);
+  const float4 r0 = __ldg(rec), r1 = __ldg(rec + 1), r2 = __ldg(rec + 2), r3 = __ldg(rec + 3), r4 = __ldg(rec + 4);
   LightShape s;
-  s.type = __float_as_int(r0.w);
+  s.type = (int)r4.w - 1;
   s.a = ld3(r0);
   s.b = ld3(r1);
   s.c = ld3(r2);
   s.nrm = ld3(r3);
-  s.area = r1.w;
+  s.area = 0.0f;
   s.valid = true;
   return s;
 }
