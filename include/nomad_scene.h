@@ -105,6 +105,13 @@ typedef struct nomad_scenebvh nomad_scenebvh;
  * threads, like Scene::buildBVH). threads = 0 uses all hardware threads. */
 nomad_status nomad_scenebvh_build(const nomad_scene_desc *desc, uint32_t threads,
                                   nomad_scenebvh **out);
+/* The same arrays, bit for bit, with the per-object BLAS builds on CUDA device `device`: every
+ * node of a tree level (of all objects) is built by one thread block, from the primitive bounds
+ * reduction and the 12-bin SAH to the stable sort of the node's primitive range; the TLAS and the
+ * packing run on the host as in nomad_scenebvh_build. No counterpart in the reference, which
+ * builds BLASes on host threads (Scene::buildBVH). */
+nomad_status nomad_scenebvh_build_gpu(const nomad_scene_desc *desc, int32_t device,
+                                      nomad_scenebvh **out);
 nomad_status nomad_scenebvh_view_get(const nomad_scenebvh *h, nomad_scenebvh_view *out);
 void nomad_scenebvh_free(nomad_scenebvh *h);
 

@@ -26,6 +26,7 @@
 #include <thread>
 #include <vector>
 
+#include "scenebvh_internal.h"
 #include "vec3.h"
 
 namespace nomad {
@@ -146,12 +147,6 @@ float surface_area(V3 mn, V3 mx) {
   V3 d = mx - mn;
   return 2.0f * (d.x * d.y + d.y * d.z + d.z * d.x);
 }
-
-struct BNode {
-  V3 mn, mx;
-  int32_t leftFirst;
-  int32_t count;  // > 0 leaf prim count; <= 0 -(right child)
-};
 
 struct SahResult {
   int axis = -1;
@@ -361,14 +356,7 @@ struct TlasBuilder {
 
 }  // namespace
 
-struct SceneBVHData {
-  std::vector<float> bvh, tlas, prims, materials, objBounds;
-  std::vector<int32_t> primIndices;
-  std::vector<nomad_instance_record> instances;
-  uint32_t primCount = 0, objectCount = 0, maxDepth = 0;
-};
-
-static void pack_prims(const nomad_scene_desc &d, SceneBVHData &out) {
+void pack_prims(const nomad_scene_desc &d, SceneBVHData &out) {
   // createTransformsBuffer (SceneBVH.cpp:165-209) after the per-primitive frame set-up
   // done by Scene::addObjectInternal (Scene.cpp:137-146).
   size_t n = d.prim_count;
@@ -424,7 +412,7 @@ static void pack_prims(const nomad_scene_desc &d, SceneBVHData &out) {
   }
 }
 
-static nomad_status validate(const nomad_scene_desc *d) {
+nomad_status scenebvh_validate(const nomad_scene_desc *d) {
   if (!d || d->prim_count == 0 || d->object_count == 0) return NOMAD_ERR_INVALID_ARGUMENT;
   if (!d->prim_type || !d->prim_geom || !d->prim_material || !d->object_first ||
       !d->object_prims)
@@ -448,7 +436,7 @@ static nomad_status validate(const nomad_scene_desc *d) {
 }
 
 static nomad_status build_impl(const nomad_scene_desc *d, uint32_t threads, SceneBVHData &out) {
-  nomad_status st = validate(d);
+  nomad_status st = scenebvh_validate(d);
   if (st != NOMAD_OK) return st;
   const size_t n = d->prim_count;
   const size_t nobj = d->object_count;
@@ -457,12 +445,7 @@ static nomad_status build_impl(const nomad_scene_desc *d, uint32_t threads, Scen
   std::vector<int64_t> indices(n);
   std::iota(indices.begin(), indices.end(), 0);
 
-  struct Result {
-    std::vector<BNode> nodes;
-    int root = -1;
-    uint32_t depth = 0;
-  };
-  std::vector<Result> results(nobj);
+  std::vector<BlasResult> results(nobj);
   std::atomic<size_t> next{0};
   auto worker = [&]() {
     for (;;) {
@@ -473,20 +456,6 @@ static nomad_status build_impl(const nomad_scene_desc *d, uint32_t threads, Scen
       b.nodes.reserve(d->object_prims[o] * 2);
       size_t first = d->object_first[o];
       results[o].root = b.build(first, first + d->object_prims[o]);
-      // depth of this BLAS (iterative, nodes only)
-      std::vector<std::pair<int, uint32_t>> st{{results[o].root, 1u}};
-      uint32_t depth = 0;
-      while (!st.empty()) {
-        auto [ni, dd] = st.back();
-        st.pop_back();
-        depth = std::max(depth, dd);
-        const BNode &nd = b.nodes[ni];
-        if (nd.count <= 0) {
-          st.push_back({nd.leftFirst, dd + 1});
-          st.push_back({-nd.count, dd + 1});
-        }
-      }
-      results[o].depth = depth;
       results[o].nodes = std::move(b.nodes);
     }
   };
@@ -500,6 +469,34 @@ static nomad_status build_impl(const nomad_scene_desc *d, uint32_t threads, Scen
     for (unsigned t = 0; t < nt; ++t) pool.emplace_back(worker);
     for (auto &t : pool) t.join();
   }
+  std::vector<int32_t> idx32(n);
+  for (size_t i = 0; i < n; ++i) idx32[i] = static_cast<int32_t>(indices[i]);
+  return scenebvh_finish(d, results, idx32, out);
+}
+
+// Everything after the per-object BLAS builds: BLAS depths, concatenation with rebased
+// children, the TLAS, and the packed arrays.
+nomad_status scenebvh_finish(const nomad_scene_desc *d, std::vector<BlasResult> &results,
+                             const std::vector<int32_t> &indices, SceneBVHData &out) {
+  const size_t n = d->prim_count;
+  const size_t nobj = d->object_count;
+  for (BlasResult &r : results) {
+    if (r.root < 0) continue;
+    // depth of this BLAS (iterative, nodes only)
+    std::vector<std::pair<int, uint32_t>> st{{r.root, 1u}};
+    uint32_t depth = 0;
+    while (!st.empty()) {
+      auto [ni, dd] = st.back();
+      st.pop_back();
+      depth = std::max(depth, dd);
+      const BNode &nd = r.nodes[ni];
+      if (nd.count <= 0) {
+        st.push_back({nd.leftFirst, dd + 1});
+        st.push_back({-nd.count, dd + 1});
+      }
+    }
+    r.depth = depth;
+  }
 
   // Concatenate with rebased children (SceneBVH.cpp:117-150).
   std::vector<BNode> all;
@@ -512,7 +509,7 @@ static nomad_status build_impl(const nomad_scene_desc *d, uint32_t threads, Scen
   std::vector<V3> objMin(nobj, V3(0.0f)), objMax(nobj, V3(0.0f));
   std::vector<int64_t> objIdx;
   for (size_t o = 0; o < nobj; ++o) {
-    const Result &r = results[o];
+    const BlasResult &r = results[o];
     if (r.root < 0) continue;
     int32_t base = static_cast<int32_t>(all.size());
     for (BNode nd : r.nodes) {
@@ -570,7 +567,7 @@ static nomad_status build_impl(const nomad_scene_desc *d, uint32_t threads, Scen
     p[4] = t.mx.x; p[5] = t.mx.y; p[6] = t.mx.z; p[7] = int_bits_as_float(t.right);
   }
   out.primIndices.resize(n);
-  for (size_t i = 0; i < n; ++i) out.primIndices[i] = static_cast<int32_t>(indices[i]);
+  for (size_t i = 0; i < n; ++i) out.primIndices[i] = indices[i];
   out.instances.resize(nobj);
   out.objBounds.resize(nobj * 6);
   for (size_t o = 0; o < nobj; ++o) {
@@ -589,10 +586,6 @@ static nomad_status build_impl(const nomad_scene_desc *d, uint32_t threads, Scen
 }
 
 }  // namespace nomad
-
-struct nomad_scenebvh {
-  nomad::SceneBVHData data;
-};
 
 extern "C" nomad_status nomad_scenebvh_build(const nomad_scene_desc *desc, uint32_t threads,
                                              nomad_scenebvh **out) {

@@ -64,6 +64,7 @@ _P = C.c_void_p
 SIGNATURES = {
     # nomad_scene.h
     "nomad_scenebvh_build": (C.c_int32, [C.POINTER(SceneDesc), C.c_uint32, C.POINTER(_P)]),
+    "nomad_scenebvh_build_gpu": (C.c_int32, [C.POINTER(SceneDesc), C.c_int32, C.POINTER(_P)]),
     "nomad_scenebvh_view_get": (C.c_int32, [_P, C.POINTER(SceneBVHView)]),
     "nomad_scenebvh_free": (None, [_P]),
     "nomad_synth_icospheres": (C.c_int32, [C.c_uint64, C.c_uint32, C.c_float, C.POINTER(_P)]),
@@ -296,11 +297,16 @@ def synth_city(seed: int, grid: int = 32, size_m: float = 1000.0, target_tris: i
 class SceneBVH:
     """SceneBVH arrays (reference GPU layouts) built from a HostScene, as numpy copies."""
 
-    def __init__(self, scene: HostScene, threads: int = 0):
+    def __init__(self, scene: HostScene, threads: int = 0, device: int | None = None):
+        """Builds on host threads, or with the per-object BLAS builds on CUDA device `device`
+        (the same arrays, bit for bit)."""
         lib = load()
         h = _P()
         d = scene.desc()
-        _check(lib.nomad_scenebvh_build(C.byref(d), threads, C.byref(h)))
+        if device is None:
+            _check(lib.nomad_scenebvh_build(C.byref(d), threads, C.byref(h)))
+        else:
+            _check(lib.nomad_scenebvh_build_gpu(C.byref(d), device, C.byref(h)))
         try:
             v = SceneBVHView()
             _check(lib.nomad_scenebvh_view_get(h, C.byref(v)))
