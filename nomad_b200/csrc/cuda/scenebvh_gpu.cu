@@ -496,7 +496,7 @@ extern "C" nomad_status nomad_scenebvh_build_gpu(const nomad_scene_desc *desc, i
       }
     }
     std::unique_ptr<nomad_scenebvh> h(new nomad_scenebvh());
-    st = nomad::scenebvh_finish(desc, results, idx, h->data);
+    st = nomad::scenebvh_finish(desc, results, idx, h->data, 0);
     if (st != NOMAD_OK) return st;
     *out = h.release();
     return NOMAD_OK;

@@ -356,15 +356,13 @@ struct TlasBuilder {
 
 }  // namespace
 
-void pack_prims(const nomad_scene_desc &d, SceneBVHData &out) {
-  // createTransformsBuffer (SceneBVH.cpp:165-209) after the per-primitive frame set-up
-  // done by Scene::addObjectInternal (Scene.cpp:137-146).
-  size_t n = d.prim_count;
-  out.prims.assign(n * 28, 0.0f);
-  out.materials.assign(n * 20, 0.0f);
-  for (size_t i = 0; i < n; ++i) {
+namespace {
+
+void pack_range(const nomad_scene_desc &d, SceneBVHData &out, size_t lo, size_t hi) {
+  for (size_t i = lo; i < hi; ++i) {
     const float *g = d.prim_geom + i * NOMAD_PRIM_GEOM_FLOATS;
     float *o = out.prims.data() + i * 28;
+    for (int k = 0; k < 28; ++k) o[k] = 0.0f;
     int type = d.prim_type[i];
     auto put = [&](int slot, V3 v, float w) {
       o[slot * 4 + 0] = v.x;
@@ -410,6 +408,35 @@ void pack_prims(const nomad_scene_desc &d, SceneBVHData &out) {
     om[18] = static_cast<float>(static_cast<int>(m[18]));
     om[19] = m[19];
   }
+}
+
+}  // namespace
+
+void pack_prims(const nomad_scene_desc &d, SceneBVHData &out, uint32_t threads) {
+  // createTransformsBuffer (SceneBVH.cpp:165-209) after the per-primitive frame set-up
+  // done by Scene::addObjectInternal (Scene.cpp:137-146). Every primitive is packed on its
+  // own, so the range is split over host threads.
+  const size_t n = d.prim_count;
+  out.prims.resize(n * 28);
+  out.materials.resize(n * 20);
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t chunk = 65536;
+  const size_t nt = std::min<size_t>(threads ? threads : hw, (n + chunk - 1) / chunk);
+  if (nt <= 1) {
+    pack_range(d, out, 0, n);
+    return;
+  }
+  std::atomic<size_t> next{0};
+  auto worker = [&]() {
+    for (;;) {
+      const size_t lo = next.fetch_add(chunk);
+      if (lo >= n) break;
+      pack_range(d, out, lo, std::min(n, lo + chunk));
+    }
+  };
+  std::vector<std::thread> pool;
+  for (size_t t = 0; t < nt; ++t) pool.emplace_back(worker);
+  for (auto &t : pool) t.join();
 }
 
 nomad_status scenebvh_validate(const nomad_scene_desc *d) {
@@ -471,13 +498,14 @@ static nomad_status build_impl(const nomad_scene_desc *d, uint32_t threads, Scen
   }
   std::vector<int32_t> idx32(n);
   for (size_t i = 0; i < n; ++i) idx32[i] = static_cast<int32_t>(indices[i]);
-  return scenebvh_finish(d, results, idx32, out);
+  return scenebvh_finish(d, results, idx32, out, threads);
 }
 
 // Everything after the per-object BLAS builds: BLAS depths, concatenation with rebased
 // children, the TLAS, and the packed arrays.
 nomad_status scenebvh_finish(const nomad_scene_desc *d, std::vector<BlasResult> &results,
-                             const std::vector<int32_t> &indices, SceneBVHData &out) {
+                             const std::vector<int32_t> &indices, SceneBVHData &out,
+                             uint32_t threads) {
   const size_t n = d->prim_count;
   const size_t nobj = d->object_count;
   for (BlasResult &r : results) {
@@ -581,7 +609,7 @@ nomad_status scenebvh_finish(const nomad_scene_desc *d, std::vector<BlasResult> 
     b[0] = objMin[o].x; b[1] = objMin[o].y; b[2] = objMin[o].z;
     b[3] = objMax[o].x; b[4] = objMax[o].y; b[5] = objMax[o].z;
   }
-  pack_prims(*d, out);
+  pack_prims(*d, out, threads);
   return NOMAD_OK;
 }
 
