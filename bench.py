@@ -19,6 +19,7 @@ import subprocess
 import sys
 import threading
 import time
+import types
 
 import numpy as np
 
@@ -283,6 +284,74 @@ def restir_leg(nb, ctx, frames=8):
                 "restir_ms_per_frame_1080p_1spp": ms}
     finally:
         c2.close()
+
+
+def compaction_leg(nb, sb, primary, steps=10):
+    """Residency compaction on the device (nomad_scenebvh_compact_gpu) of the 2.5M-triangle city
+    under a seeded 40 % object mask: ms per compaction (CUDA events, inputs larger than L2), the
+    bytes it must move, and closest-hit Mrays/s of the primary rays on the compacted scene next
+    to the same scene with the mask applied to the full arrays."""
+    import torch
+
+    rng = np.random.default_rng(SEED + 40)
+    objs = rng.random(sb.object_count) < 0.4
+    active = objs[sb.prim_object].astype(np.uint8)
+    stream = torch.cuda.Stream()
+    prev = torch.cuda.current_stream()
+    torch.cuda.set_stream(stream)  # compaction, traces and events all on one stream
+    comp = nb.native.Compactor(sb)
+    act_dev = torch.from_numpy(active).cuda()
+    for _ in range(3):
+        comp.run(act_dev)
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(steps):
+        comp.run(act_dev)
+    t1.record()
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1) / steps
+    c = comp.result()
+    n, nodes, p = sb.prim_count, sb.bvh_node_count, c["prim_count"]
+    # read: index + flag per primitive, node words, the active primitives' records; written: the
+    # compact primitive, material, index, remap and the global map, the kept nodes
+    moved = n * (4 + 1 + 4) + nodes * 32 + p * (112 + 80) * 2 + p * 8 + n * 4 + c["bvh_node_count"] * 32
+    cs = types.SimpleNamespace(
+        bvh_nodes=c["bvh_nodes"], bvh_node_count=c["bvh_node_count"], tlas_nodes=sb.tlas_nodes,
+        tlas_node_count=sb.tlas_node_count, prims=c["prims"], materials=c["materials"],
+        prim_indices=c["prim_indices"], prim_count=p, instances=c["instances"], object_count=sb.object_count)
+    rays = np.ascontiguousarray(primary)
+    d_rays = torch.from_numpy(rays.view(np.uint8)).cuda()
+    d_hits = torch.empty(rays.shape[0] * 20, dtype=torch.uint8, device="cuda")
+    rates = {}
+    for name in ("masked", "compacted"):
+        ctx = nb.Context()
+        try:
+            if name == "masked":
+                ctx.upload(sb)
+                for o in np.nonzero(~objs)[0]:
+                    ctx.set_object_active(int(o), False)
+                ctx.flush()
+            else:
+                ctx.upload(cs)
+            ctx.set_stream(stream.cuda_stream)
+            for _ in range(3):
+                ctx.trace_closest_dev(d_rays.data_ptr(), rays.shape[0], d_hits.data_ptr())
+            torch.cuda.synchronize()
+            t0.record()
+            for _ in range(steps):
+                ctx.trace_closest_dev(d_rays.data_ptr(), rays.shape[0], d_hits.data_ptr())
+            t1.record()
+            torch.cuda.synchronize()
+            rates[name] = rays.shape[0] * steps / (t0.elapsed_time(t1) / 1e3) / 1e6
+        finally:
+            ctx.close()
+    torch.cuda.set_stream(prev)
+    return {"ms": ms, "active_objects": int(objs.sum()), "objects": int(sb.object_count),
+            "resident_prims": p, "prims": int(n), "compact_nodes": c["bvh_node_count"], "nodes": int(nodes),
+            "algorithmic_bytes": int(moved), "achieved_gbs": moved / (ms / 1e3) / 1e9,
+            "geometry_bytes": {"full": int(n * 196 + nodes * 32), "compacted": int(p * 196 + c["bvh_node_count"] * 32)},
+            "closest_mrays_s": rates}
 
 
 def residency_leg():
@@ -623,7 +692,8 @@ def main():
         for name, fn in (("city_frame", lambda: frame_leg(nb, ctx, sb)),
                          ("multiview", lambda: multiview_leg(nb, ctx)),
                          ("restir", lambda: restir_leg(nb, ctx)),
-                         ("residency", lambda: residency_leg())):
+                         ("residency", lambda: residency_leg()),
+                         ("compaction", lambda: compaction_leg(nb, sb, primary))):
             try:
                 t0 = time.perf_counter()
                 extras[name] = fn()

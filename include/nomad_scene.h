@@ -18,8 +18,12 @@
  * Plus seeded synthetic scene generators (icosphere instances, a procedural city) that
  * stand in for the reference's XML/OBJ scenes.
  *
- * All functions are host-only, thread-safe on distinct handles, and return nomad_status
- * (0 = OK). No exceptions cross this ABI.
+ * Plus two device stages: the per-object BLAS builds on a CUDA device
+ * (nomad_scenebvh_build_gpu) and the compacted residency arrays built on the device
+ * (nomad_scenebvh_compact_gpu).
+ *
+ * All other functions are host-only. All are thread-safe on distinct handles and return
+ * nomad_status (0 = OK). No exceptions cross this ABI.
  */
 #ifndef NOMAD_SCENE_H
 #define NOMAD_SCENE_H
@@ -113,6 +117,54 @@ nomad_status nomad_scenebvh_build(const nomad_scene_desc *desc, uint32_t threads
 nomad_status nomad_scenebvh_build_gpu(const nomad_scene_desc *desc, int32_t device,
                                       nomad_scenebvh **out);
 nomad_status nomad_scenebvh_view_get(const nomad_scenebvh *h, nomad_scenebvh_view *out);
+
+/* ---- residency compaction on the device ---- */
+
+/* SceneBVH arrays in device memory, as nomad_scenebvh_view lays them out (every pointer a CUDA
+ * device pointer). instances are the full-scene records (every object with primitives has its
+ * BLAS root; primitive_base == primitive_index_base == the object's first primitive). */
+typedef struct nomad_scenebvh_device {
+  uint32_t prim_count;
+  uint32_t object_count;
+  uint32_t bvh_node_count;
+  uint32_t reserved;
+  const float *bvh_nodes;                 /* [bvh_node_count * 8]  */
+  const float *prims;                     /* [prim_count * 28]     */
+  const float *materials;                 /* [prim_count * 20]     */
+  const int32_t *prim_indices;            /* [prim_count]          */
+  const nomad_instance_record *instances; /* [object_count]        */
+} nomad_scenebvh_device;
+
+/* Device output arrays of a compaction, each sized for the full scene (the compact arrays are
+ * never longer). counts (device) receives [0] resident primitives, [1] compact BLAS nodes,
+ * [2] error bits (0 = OK; 1 index out of range, 2 tree deeper than 128, 4 arrays not laid out
+ * as SceneBVH builds them). */
+typedef struct nomad_compact_out {
+  float *bvh_nodes;                 /* [bvh_node_count * 8] compactBVHNodes             */
+  float *prims;                     /* [prim_count * 28]    compactPrimitiveData        */
+  float *materials;                 /* [prim_count * 20]    compactMaterialData         */
+  int32_t *prim_indices;            /* [prim_count]         compactPrimitiveIndices     */
+  uint32_t *remap;                  /* [prim_count]         remapUpload: compact->global */
+  int32_t *prim_to_resident;        /* [prim_count]         global->compact, -1 inactive */
+  nomad_instance_record *instances; /* [object_count]       compact instance records    */
+  uint32_t *counts;                 /* [3]                                              */
+} nomad_compact_out;
+
+/* Device scratch bytes nomad_scenebvh_compact_gpu needs for these sizes. */
+size_t nomad_compact_workspace_bytes(uint32_t prim_count, uint32_t bvh_node_count, uint32_t object_count);
+
+/* Builds the compacted resident arrays of the reference's compacted residency path
+ * (Renderer::rebuildResidentResources, Renderer/Renderer.cpp:5359-5560: active primitives in
+ * object and BLAS-leaf order, each object's cached BLAS pruned to its active leaves, one-child
+ * nodes collapsed, nodes in post-order with unchanged bounds) from the full arrays and a
+ * per-primitive active mask (prim_active[global primitive] != 0), on the device, queued on
+ * `stream` (a cudaStream_t; NULL = the legacy default stream) without host synchronisation.
+ * The TLAS is unchanged. Allocates nothing. Returns NOMAD_ERR_INVALID_ARGUMENT for missing
+ * pointers or a workspace smaller than nomad_compact_workspace_bytes; data errors are reported
+ * in counts[2]. */
+nomad_status nomad_scenebvh_compact_gpu(const nomad_scenebvh_device *in, const uint8_t *prim_active,
+                                        void *workspace, size_t workspace_bytes,
+                                        const nomad_compact_out *out, void *stream);
 void nomad_scenebvh_free(nomad_scenebvh *h);
 
 /* ---- seeded synthetic scenes (no reference counterpart: stand-ins for its XML scenes) ---- */

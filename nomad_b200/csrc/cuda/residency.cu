@@ -442,9 +442,15 @@ nomad_status nomad_residency_init(nomad_ctx *ctx) {
     for (uint32_t o = 0; o < N; ++o)
       if (L.objRootNode[o] >= 0) roots.push_back({L.objRootNode[o], o});
     std::sort(roots.begin(), roots.end());
+    // every object's nodes are one block: root first (pre-order) or root last (post-order)
     for (size_t i = 0; i < roots.size(); ++i) {
-      uint32_t end = i + 1 < roots.size() ? (uint32_t)roots[i + 1].first : R.bvhNodeCount;
-      nodes[roots[i].second] = end - (uint32_t)roots[i].first;
+      if (L.blasPostOrder) {
+        const uint32_t begin = i ? (uint32_t)roots[i - 1].first + 1 : 0u;
+        nodes[roots[i].second] = (uint32_t)roots[i].first + 1 - begin;
+      } else {
+        const uint32_t end = i + 1 < roots.size() ? (uint32_t)roots[i + 1].first : R.bvhNodeCount;
+        nodes[roots[i].second] = end - (uint32_t)roots[i].first;
+      }
     }
   }
   R.hostBytes.assign(N, 0);

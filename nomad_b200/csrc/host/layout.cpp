@@ -60,8 +60,12 @@ bool build_traversal_layout(const float *bvh, uint32_t bvhCount, const float *tl
     out.primPos[p] = static_cast<int32_t>(k);
   }
 
-  // BLAS nodes: validate children and find roots (nodes nobody references).
+  // BLAS nodes: validate children and find roots (nodes nobody references). SceneBVH emits
+  // children after their parent (pre-order); the compacted residency arrays emit them before
+  // (post-order, Renderer.cpp:5513-5556). Either order is accepted, the same for every node,
+  // which also rules out cycles.
   std::vector<uint8_t> isChild(bvhCount, 0);
+  int childrenAfter = -1;  // 1 pre-order, 0 post-order, -1 not known yet
   for (uint32_t i = 0; i < bvhCount; ++i) {
     N2 n = bn(i);
     if (n.b() > 0) {
@@ -72,8 +76,9 @@ bool build_traversal_layout(const float *bvh, uint32_t bvhCount, const float *tl
       }
     } else {
       int32_t l = n.a(), r = -n.b();
-      if (l <= (int32_t)i || r <= (int32_t)i || (uint32_t)l >= bvhCount || (uint32_t)r >= bvhCount) {
-        // SceneBVH emits children after their parent (pre-order), which also rules out cycles.
+      if (childrenAfter < 0) childrenAfter = l > (int32_t)i ? 1 : 0;
+      const bool ordered = childrenAfter ? (l > (int32_t)i && r > (int32_t)i) : (l >= 0 && r >= 0 && l < (int32_t)i && r < (int32_t)i);
+      if (!ordered || (uint32_t)l >= bvhCount || (uint32_t)r >= bvhCount) {
         err = "BLAS node " + std::to_string(i) + " has an out-of-order or out-of-range child";
         return false;
       }
@@ -84,6 +89,7 @@ bool build_traversal_layout(const float *bvh, uint32_t bvhCount, const float *tl
       isChild[l] = isChild[r] = 1;
     }
   }
+  out.blasPostOrder = childrenAfter == 0;
   std::vector<int32_t> roots;
   for (uint32_t i = 0; i < bvhCount; ++i)
     if (!isChild[i]) roots.push_back(static_cast<int32_t>(i));
@@ -111,7 +117,9 @@ bool build_traversal_layout(const float *bvh, uint32_t bvhCount, const float *tl
     N2 n = tn(i);
     if (n.a() < 0) {
       int32_t o = -(n.a() + 1);
-      if (o < 0 || (uint32_t)o >= objectCount || objects[o].count == 0) {
+      // an empty object may stay in the TLAS when it is not resident (compacted arrays keep the
+      // full scene's TLAS, Renderer.cpp:5756)
+      if (o < 0 || (uint32_t)o >= objectCount || (objects[o].count == 0 && objects[o].blasRoot >= 0)) {
         err = "TLAS leaf " + std::to_string(i) + " names a bad object";
         return false;
       }

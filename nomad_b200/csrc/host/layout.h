@@ -36,6 +36,7 @@ struct TraversalLayout {
   int32_t rootRef = kEmptyRef;
   uint32_t tlasPairCount = 0;  // pair nodes [0, tlasPairCount) belong to the TLAS
   uint32_t maxDepth = 0;       // longest root-to-leaf chain of pair nodes plus the leaf
+  bool blasPostOrder = false;  // BLAS children stored before their parent (compacted arrays)
   // Per object: BLAS ref used when resident, and where the TLAS stores it:
   // slot = pairIndex * 2 + side (side 0 left, 1 right); -1 when the object is the TLAS root.
   std::vector<int32_t> objBlasRef;

@@ -55,6 +55,20 @@ class SceneBVHView(C.Structure):
                 ("object_bounds", C.POINTER(C.c_float)), ("max_depth", C.c_uint32)]
 
 
+class ScenebvhDevice(C.Structure):
+    """nomad_scenebvh_device: SceneBVH arrays in device memory."""
+    _fields_ = [("prim_count", C.c_uint32), ("object_count", C.c_uint32), ("bvh_node_count", C.c_uint32),
+                ("reserved", C.c_uint32), ("bvh_nodes", C.c_void_p), ("prims", C.c_void_p),
+                ("materials", C.c_void_p), ("prim_indices", C.c_void_p), ("instances", C.c_void_p)]
+
+
+class CompactOut(C.Structure):
+    """nomad_compact_out: device output arrays of a residency compaction."""
+    _fields_ = [("bvh_nodes", C.c_void_p), ("prims", C.c_void_p), ("materials", C.c_void_p),
+                ("prim_indices", C.c_void_p), ("remap", C.c_void_p), ("prim_to_resident", C.c_void_p),
+                ("instances", C.c_void_p), ("counts", C.c_void_p)]
+
+
 class Config(C.Structure):
     _fields_ = [("device", C.c_int32), ("flags", C.c_uint32)]
 
@@ -66,6 +80,9 @@ SIGNATURES = {
     "nomad_scenebvh_build": (C.c_int32, [C.POINTER(SceneDesc), C.c_uint32, C.POINTER(_P)]),
     "nomad_scenebvh_build_gpu": (C.c_int32, [C.POINTER(SceneDesc), C.c_int32, C.POINTER(_P)]),
     "nomad_scenebvh_view_get": (C.c_int32, [_P, C.POINTER(SceneBVHView)]),
+    "nomad_compact_workspace_bytes": (C.c_size_t, [C.c_uint32, C.c_uint32, C.c_uint32]),
+    "nomad_scenebvh_compact_gpu": (C.c_int32, [C.POINTER(ScenebvhDevice), _P, _P, C.c_size_t,
+                                               C.POINTER(CompactOut), _P]),
     "nomad_scenebvh_free": (None, [_P]),
     "nomad_synth_icospheres": (C.c_int32, [C.c_uint64, C.c_uint32, C.c_float, C.POINTER(_P)]),
     "nomad_synth_city": (C.c_int32, [C.c_uint64, C.c_uint32, C.c_uint32, C.c_float, C.c_uint32, C.c_uint32,
@@ -344,6 +361,70 @@ class SceneBVH:
         bounds = np.append(roots[order], self.bvh_node_count)
         nodes[order] = np.diff(bounds)
         return 32 * nodes + 196 * self.instances["primitive_count"].astype(np.int64)
+
+
+class Compactor:
+    """Residency compaction on the device (nomad_scenebvh_compact_gpu) of one SceneBVH, uploaded
+    once; outputs stay in device memory (torch tensors) until result() copies them back."""
+
+    def __init__(self, sb: SceneBVH, device: str = "cuda:0"):
+        import torch
+        self._torch = torch
+        lib = load()
+
+        def up(a):
+            return torch.from_numpy(np.ascontiguousarray(a)).to(device)
+
+        n, nn, nobj = int(sb.prim_count), int(sb.bvh_node_count), int(sb.object_count)
+        self.sizes = (n, nn, nobj)
+        self.bvh, self.prims, self.mats = up(sb.bvh_nodes), up(sb.prims), up(sb.materials)
+        self.idx = up(sb.prim_indices)
+        self.inst = up(sb.instances.view(np.int32).reshape(-1))
+        self.inp = ScenebvhDevice(n, nobj, nn, 0, self.bvh.data_ptr(), self.prims.data_ptr(),
+                                  self.mats.data_ptr(), self.idx.data_ptr(), self.inst.data_ptr())
+        self.ws_bytes = int(lib.nomad_compact_workspace_bytes(n, nn, nobj))
+        self.ws = torch.empty(self.ws_bytes, dtype=torch.uint8, device=device)
+        f32, i32 = torch.float32, torch.int32
+        self.o_bvh = torch.empty(max(nn, 1) * 8, dtype=f32, device=device)
+        self.o_prims = torch.empty(n * 28, dtype=f32, device=device)
+        self.o_mats = torch.empty(n * 20, dtype=f32, device=device)
+        self.o_idx = torch.empty(n, dtype=i32, device=device)
+        self.o_remap = torch.empty(n, dtype=i32, device=device)
+        self.o_p2r = torch.empty(n, dtype=i32, device=device)
+        self.o_inst = torch.empty(nobj * 4, dtype=i32, device=device)
+        self.o_counts = torch.zeros(3, dtype=i32, device=device)
+        self.out = CompactOut(self.o_bvh.data_ptr(), self.o_prims.data_ptr(), self.o_mats.data_ptr(),
+                              self.o_idx.data_ptr(), self.o_remap.data_ptr(), self.o_p2r.data_ptr(),
+                              self.o_inst.data_ptr(), self.o_counts.data_ptr())
+
+    def run(self, active) -> None:
+        """Queues one compaction for the per-primitive mask `active` (a uint8 device tensor, or a
+        host array uploaded first) on torch's current stream."""
+        torch = self._torch
+        if not isinstance(active, torch.Tensor):
+            active = torch.from_numpy(np.ascontiguousarray(active, np.uint8)).to(self.bvh.device)
+        assert active.dtype == torch.uint8 and active.numel() == self.sizes[0]
+        self._active = active
+        stream = torch.cuda.current_stream(self.bvh.device).cuda_stream
+        _check(load().nomad_scenebvh_compact_gpu(C.byref(self.inp), active.data_ptr(), self.ws.data_ptr(),
+                                                 self.ws_bytes, C.byref(self.out), stream))
+
+    def result(self) -> dict:
+        """The last compaction's arrays, trimmed to their lengths, as numpy (synchronises)."""
+        counts = self.o_counts.cpu().numpy().astype(np.uint32)
+        if counts[2]:
+            raise NomadError(5, f"compaction error bits {int(counts[2])}")
+        p, nodes = int(counts[0]), int(counts[1])
+        return {
+            "prim_count": p, "bvh_node_count": nodes,
+            "bvh_nodes": self.o_bvh[: nodes * 8].cpu().numpy(),
+            "prims": self.o_prims[: p * 28].cpu().numpy(),
+            "materials": self.o_mats[: p * 20].cpu().numpy(),
+            "prim_indices": self.o_idx[:p].cpu().numpy(),
+            "remap": self.o_remap[:p].cpu().numpy().view(np.uint32),
+            "prim_to_resident": self.o_p2r.cpu().numpy(),
+            "instances": self.o_inst.cpu().numpy().view(INSTANCE_DTYPE),
+        }
 
 
 def _check(st: int, ctx=None):

@@ -161,3 +161,36 @@ class RestirOracle:
         assert rc == 0
         self.prev = (resv, surf, views.copy())
         return rgb, stats
+
+
+def compact(sb, active):
+    """Compacted resident arrays of the reference's compacted residency path (compact.cpp) for
+    the per-primitive mask `active`, trimmed to their lengths."""
+    lib = load()
+    if not hasattr(lib, "_compact_bound"):
+        lib.oracle_compact.argtypes = [_P, C.c_uint32, _P, _P, _P, C.c_uint32, _P, C.c_uint32, _P, _P, _P,
+                                       _P, _P, _P, _P, _P, _P]
+        lib.oracle_compact.restype = C.c_int
+        lib._compact_bound = True
+    n, nn, nobj = int(sb.prim_count), int(sb.bvh_nodes.size // 8), int(sb.object_count)
+    bvh = np.ascontiguousarray(sb.bvh_nodes, np.float32)
+    prims = np.ascontiguousarray(sb.prims, np.float32)
+    mats = np.ascontiguousarray(sb.materials, np.float32)
+    idx = np.ascontiguousarray(sb.prim_indices, np.int32)
+    inst = np.ascontiguousarray(sb.instances.view(np.int32).reshape(-1))
+    act = np.ascontiguousarray(active, np.uint8)
+    o_bvh = np.zeros(max(nn, 1) * 8, np.float32)
+    o_prims = np.zeros(n * 28, np.float32)
+    o_mats = np.zeros(n * 20, np.float32)
+    o_idx = np.zeros(n, np.int32)
+    o_remap = np.zeros(n, np.uint32)
+    o_p2r = np.zeros(n, np.int32)
+    o_inst = np.zeros(nobj * 4, np.int32)
+    counts = np.zeros(2, np.uint32)
+    assert lib.oracle_compact(_p(bvh), nn, _p(prims), _p(mats), _p(idx), n, _p(inst), nobj, _p(act),
+                              _p(o_bvh), _p(o_prims), _p(o_mats), _p(o_idx), _p(o_remap), _p(o_p2r),
+                              _p(o_inst), _p(counts)) == 0
+    p, nodes = int(counts[0]), int(counts[1])
+    return {"prim_count": p, "bvh_node_count": nodes, "bvh_nodes": o_bvh[: nodes * 8], "prims": o_prims[: p * 28],
+            "materials": o_mats[: p * 20], "prim_indices": o_idx[:p], "remap": o_remap[:p],
+            "prim_to_resident": o_p2r, "instances": o_inst.view(sb.instances.dtype)}
