@@ -322,6 +322,50 @@ nomad_status nomad_residency_last(nomad_ctx *ctx, float *features, float *scores
 /* Current residency of each object (object_count bytes, 1 = resident). */
 nomad_status nomad_residency_flags(nomad_ctx *ctx, uint8_t *out);
 
+/* ---- geometry paging (the Cold -> Streaming -> Resident lifecycle of per-object GPU
+ *      resources, Renderer.h:63-106, ensureResident Renderer.cpp:613-650, the per-frame onload
+ *      loop with kMaxColdObjectOnloadsPerFrame Renderer.cpp:5828-5905) -------------------------
+ * Once enabled, every object's BLAS nodes (of the one traversal layout named by `width`) and
+ * triangle records live in pinned host memory and are streamed on demand into a fixed device
+ * pool of pool_bytes: a Cold object that the residency state wants resident is copied by the
+ * copy engine (asynchronously, at most max_onloads_per_frame objects started per update),
+ * relocated on the device to its pool offsets, and published into the TLAS when its copy has
+ * completed (Streaming -> Resident); an object no longer wanted is unlinked at once and its
+ * pool space reused after the work queued before the unlink has finished. An onload that does
+ * not fit in the pool is denied (the reference's geometry hard cap). Until an object is
+ * Resident it is skipped by traversal even if its residency flag is set. The TLAS and the
+ * shading arrays (packed primitives, materials) stay resident. Traversal configurations of
+ * other widths, nomad_trace_work and the allocation-free call need the pair layout and are
+ * refused while paging a wide layout. Paging lasts until the next nomad_scene_upload; every
+ * trace, render and residency call must use the context's stream. */
+typedef struct nomad_paging_config {
+  uint64_t pool_bytes;            /* device bytes for BLAS nodes + triangle records           */
+  uint32_t max_onloads_per_frame; /* Cold objects started per update; 0 = 32 (the reference's) */
+  uint32_t width;                 /* paged node layout: 2 (pair), 4 or 8                      */
+} nomad_paging_config;
+
+enum { NOMAD_PAGE_COLD = 0, NOMAD_PAGE_STREAMING = 1, NOMAD_PAGE_RESIDENT = 2 };
+
+typedef struct nomad_paging_stats {
+  uint64_t pool_bytes;            /* node + record pool capacity                              */
+  uint64_t used_bytes;            /* pool bytes held by Streaming and Resident objects        */
+  uint64_t full_bytes;            /* bytes the whole scene's BLAS nodes + records take        */
+  uint64_t bytes_streamed;        /* host -> device bytes of all onloads                      */
+  uint32_t cold, streaming, resident;
+  uint32_t onloads, evictions, denied, deferred; /* totals since enable                       */
+} nomad_paging_stats;
+
+nomad_status nomad_paging_enable(nomad_ctx *ctx, const nomad_paging_config *cfg);
+/* Applies the current residency state (after nomad_residency_flush or nomad_residency_step):
+ * publishes completed onloads, unlinks unwanted objects, starts new onloads. Does not wait for
+ * copies; call once per frame. */
+nomad_status nomad_paging_update(nomad_ctx *ctx);
+/* Waits for the copies in flight and publishes them (does not start new onloads). */
+nomad_status nomad_paging_wait(nomad_ctx *ctx);
+nomad_status nomad_paging_stats_get(nomad_ctx *ctx, nomad_paging_stats *out);
+/* Per-object NOMAD_PAGE_* state (object_count bytes). */
+nomad_status nomad_paging_states(nomad_ctx *ctx, uint8_t *out);
+
 /* ---- learned scorer: 24 -> 128 -> 128 -> 1 MLP, ReLU, BF16 weights, FP32 accumulation on the
  *      tensor cores, trained on device (no reference counterpart for the kernels; the reference
  *      trains a tiny FP32 MLP offline in PyTorch, Benchmarks/train_unified_neural_mlp.py) ---- */

@@ -625,7 +625,8 @@ extern "C" nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residen
   wp.arena = static_cast<int32_t *>(ctx->arena.p);
   for (int w = 0; w < 2; ++w) {
     const nomad::WideLayout &WL = ctx->wide[w];
-    wp.width[w] = WL.width;
+    // while paging, only the paged layout is on the device
+    wp.width[w] = (ctx->pagedWidth && ctx->pagedWidth != WL.width) ? 0u : WL.width;
     wp.fpn[w] = WL.floatsPerNode;
     wp.base[w] = ctx->wideWordBase[w];
     wp.slot[w] = ctx->wideSlot[w].as<const long long>();

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../../include/nomad_rt.h"
@@ -30,6 +31,10 @@ struct DeviceBuf {
     return e;
   }
   template <typename T> T *as() const { return static_cast<T *>(p); }
+  void swap(DeviceBuf &o) {
+    std::swap(p, o.p);
+    std::swap(bytes, o.bytes);
+  }
 };
 
 // Light tables on the device: rebuilt by one kernel whenever residency changes.
@@ -133,6 +138,9 @@ struct nomad_ctx {
     std::vector<uint64_t> hostBytes;
   } res;
   void *mlp = nullptr;  // MlpState (mlp.cu)
+  // Geometry paging (paging.cu): the paged node layout's width (0 = off) and its state.
+  uint32_t pagedWidth = 0;
+  void *paging = nullptr;
   // Host mirror of the device residency flags after a device step: copied asynchronously into
   // pinned memory and applied to objResident / instances when a host call next needs them.
   bool resHostStale = false;
@@ -149,6 +157,14 @@ struct nomad_ctx {
 nomad_status nomad_residency_sync_host(nomad_ctx *ctx);
 
 void nomad_mlp_free(void *p);
+void nomad_paging_free(nomad_ctx *ctx);
+// Paging: the arena word of the triangle record at leaf position `pos` (-1 when its object is
+// Cold), after updating the cold copy's activity word to `word`.
+int64_t nomad_paging_record_word(nomad_ctx *ctx, uint32_t pos, int32_t word);
+// Paging: the ref an object's TLAS link takes when it is resident (kEmptyRef until published).
+int32_t nomad_paging_ref(const nomad_ctx *ctx, uint32_t obj);
+// Paging: makes the context's stream wait for the copies queued so far.
+nomad_status nomad_paging_order(nomad_ctx *ctx);
 nomad_status nomad_mlp_infer_device(nomad_ctx *ctx, const float *X, uint64_t n, float *y);
 namespace nomad_res {
 struct FeatArgs;

@@ -184,6 +184,7 @@ extern "C" nomad_status nomad_destroy(nomad_ctx *ctx) {
     if (s) cudaStreamDestroy(s);
   if (ctx->ownStream) cudaStreamDestroy(ctx->ownStream);
   if (ctx->mlp) nomad_mlp_free(ctx->mlp);
+  nomad_paging_free(ctx);
   delete ctx;
   return NOMAD_OK;
 }
@@ -227,6 +228,10 @@ extern "C" nomad_status nomad_scene_upload(nomad_ctx *ctx, const float *bvh, uin
     ctx->resHostStale = false;
   }
   ctx->sceneReady = false;
+  if (ctx->paging) {  // a new scene ends paging: the arena is rebuilt whole below
+    nomad_paging_free(ctx);
+    ctx->frame.clearGraphs();
+  }
   // Leaf refs are ~first record; the values just above INT32_MIN are kernel sentinels.
   if (primCount > 0x7ffffff0u) return fail(ctx, NOMAD_ERR_LIMIT, "too many primitives");
   std::vector<nomad::ObjectRange> objs(objectCount);
@@ -383,20 +388,32 @@ extern "C" nomad_status nomad_residency_flush(nomad_ctx *ctx) {
   std::vector<int64_t> offs;
   std::vector<int32_t> vals;
   const auto &L = ctx->layout;
+  if (ctx->paging) {  // patches below must land after the copies that may hold these records
+    nomad_status ps = nomad_paging_order(ctx);
+    if (ps != NOMAD_OK) return ps;
+  }
   for (uint32_t p : ctx->dirtyPrims) {
     ctx->primDirtyFlag[p] = 0;
     int64_t pos = L.primPos[p];
-    offs.push_back((int64_t)ctx->pnodeWords + pos * 12 + 3);
-    vals.push_back(ctx->primActive[p] ? (int32_t)p : ~(int32_t)p);
+    const int32_t word = ctx->primActive[p] ? (int32_t)p : ~(int32_t)p;
+    if (ctx->paging) {
+      const int64_t w = nomad_paging_record_word(ctx, (uint32_t)pos, word);
+      if (w < 0) continue;  // a Cold object: its host copy holds the new word
+      offs.push_back(w);
+    } else {
+      offs.push_back((int64_t)ctx->pnodeWords + pos * 12 + 3);
+    }
+    vals.push_back(word);
   }
   for (uint32_t o : ctx->dirtyObjs) {
     ctx->objDirtyFlag[o] = 0;
     bool res = ctx->objActiveCount[o] > 0 && ctx->instances[o].primitive_count > 0;
     ctx->objResident[o] = res ? 1 : 0;
-    int32_t ref = res ? L.objBlasRef[o] : nomad::kEmptyRef;
+    int32_t ref = res ? (ctx->paging ? nomad_paging_ref(ctx, o) : L.objBlasRef[o]) : nomad::kEmptyRef;
     // Instance record as the reference fills it (Renderer.cpp:5344-5357).
     ctx->instances[o].blas_root_index = res ? L.objRootNode[o] : -1;
-    int64_t slot = L.objSlot[o];
+    // pair-layout links exist unless a wide layout is paged
+    int64_t slot = (ctx->pagedWidth == 0 || ctx->pagedWidth == 2) ? L.objSlot[o] : -2;
     if (slot == -1) {
       ctx->scene.rootRef = ref;
     } else if (slot >= 0) {
@@ -651,6 +668,8 @@ extern "C" nomad_status nomad_trace_any(nomad_ctx *ctx, const nomad_ray *rays, u
 
 extern "C" nomad_status nomad_trace_work(nomad_ctx *ctx, const nomad_ray *rays, uint64_t n,
                                          uint32_t *out, uint32_t flags) {
+  if (ctx && ctx->pagedWidth > 2)
+    return fail(ctx, NOMAD_ERR_UNSUPPORTED, "the counting walk needs the pair layout, which is not on the device while a wide layout is paged");
   return trace_entry(ctx, Op::Work, rays, n, out, 16, flags);
 }
 
@@ -733,6 +752,8 @@ extern "C" nomad_status nomad_trace_closest_noalloc(nomad_ctx *ctx, const nomad_
                                                     uint32_t *d_object_hits) {
   if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
   if (!ctx->sceneReady) return fail(ctx, NOMAD_ERR_NOT_READY, "no scene uploaded");
+  if (ctx->pagedWidth > 2)
+    return fail(ctx, NOMAD_ERR_UNSUPPORTED, "the allocation-free walk needs the pair layout, which is not on the device while a wide layout is paged");
   if (ctx->objectCount > kNoAllocMaxObjects)
     return fail(ctx, NOMAD_ERR_LIMIT,
                 "nomad_trace_closest_noalloc supports at most " +
@@ -776,6 +797,7 @@ nomad_status nomad_patch_wide(nomad_ctx *ctx) {
   for (int w = 0; w < 2; ++w) {
     const nomad::WideLayout &WL = ctx->wide[w];
     if (!WL.width) continue;
+    if (ctx->pagedWidth && ctx->pagedWidth != WL.width) continue;  // not on the device while paging
     k_patch_wide<<<(n + 255) / 256, 256, 0, ctx->stream>>>(static_cast<int32_t *>(ctx->arena.p), ctx->wideWordBase[w],
                                                           WL.floatsPerNode, WL.width, ctx->wideSlot[w].as<const long long>(),
                                                           ctx->wideRef[w].as<const int32_t>(),

@@ -517,6 +517,9 @@ bool nomad_traversal_ok(const nomad_ctx *ctx, const nomad_traversal &c, std::str
       return no("min_blocks must be 0, 10, 12 or 16");
   }
   if (!ctx->sceneReady) return true;
+  if (ctx->pagedWidth && c.width != ctx->pagedWidth) return no("only the paged layout's width is on the device");
+  if (ctx->pagedWidth && c.staged_nodes > tlas_prefix(ctx, c.width))
+    return no("while paging, staged nodes must lie in the TLAS part");
   const uint32_t wi = c.width == 2 ? 0 : (c.width == 4 ? 1 : 2);
   const uint32_t cap = c.width == 8 ? (uint32_t)kStackW8 : (uint32_t)kStackW2;
   if (c.width != 2 && ctx->wide[wi - 1].width != c.width) return no("wide layout missing");

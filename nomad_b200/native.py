@@ -69,6 +69,20 @@ class CompactOut(C.Structure):
                 ("instances", C.c_void_p), ("counts", C.c_void_p)]
 
 
+class PagingConfig(C.Structure):
+    _fields_ = [("pool_bytes", C.c_uint64), ("max_onloads_per_frame", C.c_uint32), ("width", C.c_uint32)]
+
+
+class PagingStats(C.Structure):
+    _fields_ = [("pool_bytes", C.c_uint64), ("used_bytes", C.c_uint64), ("full_bytes", C.c_uint64),
+                ("bytes_streamed", C.c_uint64), ("cold", C.c_uint32), ("streaming", C.c_uint32),
+                ("resident", C.c_uint32), ("onloads", C.c_uint32), ("evictions", C.c_uint32),
+                ("denied", C.c_uint32), ("deferred", C.c_uint32)]
+
+
+PAGE_COLD, PAGE_STREAMING, PAGE_RESIDENT = 0, 1, 2
+
+
 class Config(C.Structure):
     _fields_ = [("device", C.c_int32), ("flags", C.c_uint32)]
 
@@ -111,6 +125,11 @@ SIGNATURES = {
     "nomad_read_object_hits": (C.c_int32, [_P, _P]),
     "nomad_reset_object_hits": (C.c_int32, [_P]),
     "nomad_trace_closest_noalloc": (C.c_int32, [_P, _P, C.c_uint64, _P, _P]),
+    "nomad_paging_enable": (C.c_int32, [_P, C.POINTER(PagingConfig)]),
+    "nomad_paging_update": (C.c_int32, [_P]),
+    "nomad_paging_wait": (C.c_int32, [_P]),
+    "nomad_paging_stats_get": (C.c_int32, [_P, C.POINTER(PagingStats)]),
+    "nomad_paging_states": (C.c_int32, [_P, _P]),
     "nomad_view_pinhole": (C.c_int32, [_P, _P, _P, C.c_float, C.c_uint32, C.c_uint32, _P]),
     "nomad_render_frame": (C.c_int32, [_P, _P, C.c_uint32, _P, C.c_uint32]),
     "nomad_render_stats": (C.c_int32, [_P, _P]),
@@ -699,6 +718,27 @@ class Context:
     def object_hits(self) -> np.ndarray:
         out = np.zeros(self.object_count, np.uint32)
         self._ck(self.lib.nomad_read_object_hits(self.h, _ptr(out)))
+        return out
+
+    # geometry paging
+    def paging_enable(self, pool_bytes: int, width: int = 4, max_onloads: int = 0):
+        cfg = PagingConfig(int(pool_bytes), int(max_onloads), int(width))
+        self._ck(self.lib.nomad_paging_enable(self.h, C.byref(cfg)))
+
+    def paging_update(self):
+        self._ck(self.lib.nomad_paging_update(self.h))
+
+    def paging_wait(self):
+        self._ck(self.lib.nomad_paging_wait(self.h))
+
+    def paging_stats(self) -> dict:
+        st = PagingStats()
+        self._ck(self.lib.nomad_paging_stats_get(self.h, C.byref(st)))
+        return {f: int(getattr(st, f)) for f, _ in PagingStats._fields_}
+
+    def paging_states(self) -> np.ndarray:
+        out = np.zeros(self.object_count, np.uint8)
+        self._ck(self.lib.nomad_paging_states(self.h, _ptr(out)))
         return out
 
     def reset_object_hits(self):
