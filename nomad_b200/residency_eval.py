@@ -5,7 +5,8 @@ Workload (the learned-residency configuration): a city of 2,048 objects (~6M tri
 frame renders the view with the current resident set (per-object hit counting on), then runs
 one residency step. The image judge is the same frame rendered with every object resident
 (a second context, same Philox streams), compared in HDR:
-rel-MSE = mean((I - I_AR)^2) / mean(I_AR^2).
+rel-MSE = mean((I - I_AR)^2) / mean(I_AR^2), averaged over the frames whose reference is not
+black.
 
 The learned scorer is trained on the device on hit counts recorded along seeded training camera
 paths rendered with every object resident: features of frame f, target log1p(hits of frame
@@ -157,7 +158,8 @@ class Workload:
             num = torch.mean((d_img - d_ref) ** 2).item()
             den = torch.mean(d_ref ** 2).item()
             if f >= warm:
-                mse.append(num / max(den, 1e-12))
+                if den > 0:  # a black reference frame (camera inside geometry) has no relative error
+                    mse.append(num / den)
                 ms.append(dt * 1e3)
                 flags = ctx.residency_flags().astype(bool)
                 resident_bytes.append(int(nbytes[flags].sum()))
@@ -165,6 +167,71 @@ class Workload:
                 "ms_per_frame_p50": float(np.median(ms)),
                 "resident_fraction": float(np.mean(resident_bytes) / nbytes.sum()),
                 "frames": len(mse)}
+
+
+    def evaluate_paged(self, ctx, judge, policy, path_seed=1, frames=None, warm=5, pool_slack=1.25):
+        """The same run with geometry paging: a third context whose BLAS nodes (of the tuned
+        traversal width) and triangle records live in a device pool of pool_slack x the budget's
+        share of the paged bytes, streamed in by nomad_paging_update after every residency step
+        (at most 32 onloads per frame). ms/frame includes the update; rel-MSE includes the frames
+        where wanted objects are still streaming."""
+        import torch
+
+        frames = frames or self.frames
+        views = self.views(path_seed, frames)
+        trav = ctx.traversal()
+        probe = self.context()
+        probe.set_traversal(**trav)
+        probe.paging_enable(1 << 50, width=trav["width"])
+        full = probe.paging_stats()["full_bytes"]
+        probe.close()
+        pc = self.context()
+        try:
+            pc.set_traversal(**trav)
+            pc.mlp_set(ctx.mlp_get())
+            pool = int(min(full, full * self.budget_fraction * pool_slack))
+            pc.paging_enable(pool, width=trav["width"])
+            nbytes = pc.object_bytes()
+            budget = int(self.budget_fraction * nbytes.sum())
+            prm = nat.ResidencyParams.make(policy, budget_bytes=budget, camera_motion=0.3, min_active=0)
+            pc.reset_object_hits()
+            npix = self.width * self.height
+            d_img = torch.empty(npix * 3, dtype=torch.float32, device="cuda")
+            d_ref = torch.empty(npix * 3, dtype=torch.float32, device="cuda")
+            mse, ms, streamed, onl = [], [], [], []
+            prev = pc.paging_stats()
+            for f, v in enumerate(views):
+                judge.render_dev(v, d_ref.data_ptr())
+                judge.sync()
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                pc.render_dev(v, d_img.data_ptr(), count_hits=True)
+                pc.residency_step(prm, v, toggles=False)
+                pc.paging_update()
+                pc.sync()
+                dt = time.perf_counter() - t0
+                num = torch.mean((d_img - d_ref) ** 2).item()
+                den = torch.mean(d_ref ** 2).item()
+                st = pc.paging_stats()
+                if f >= warm:
+                    mse.append(num / den if den > 0 else None)
+                    ms.append(dt * 1e3)
+                    streamed.append(st["bytes_streamed"] - prev["bytes_streamed"])
+                    onl.append(st["onloads"] - prev["onloads"])
+                prev = st
+            st = pc.paging_stats()
+            late = [m for m in mse[max(0, 40 - warm):] if m is not None]
+            mse = [m for m in mse if m is not None]
+            return {"rel_mse": float(np.mean(mse)), "rel_mse_from_frame_40": float(np.mean(late)) if late else None,
+                    "ms_per_frame": float(np.mean(ms)),
+                    "ms_per_frame_p50": float(np.median(ms)), "frames": len(mse),
+                    "pool_bytes": st["pool_bytes"], "full_paged_bytes": st["full_bytes"],
+                    "mean_streamed_bytes_per_frame": float(np.mean(streamed)),
+                    "mean_onloads_per_frame": float(np.mean(onl)), "max_onloads_per_frame": int(np.max(onl)),
+                    "denied": st["denied"], "deferred": st["deferred"], "evictions": st["evictions"],
+                    "resident_objects_end": st["resident"]}
+        finally:
+            pc.close()
 
 
 def run(paths=200, frames_per_path=8, steps=1500, frames=300, log=print):
@@ -192,6 +259,12 @@ def run(paths=200, frames_per_path=8, steps=1500, frames=300, log=print):
     for name, pol in (("always_resident", nat.POLICY_ALWAYS), ("ray_hit_budget", nat.POLICY_RAYHIT_BUDGET),
                       ("learned", nat.POLICY_LEARNED)):
         out[name] = w.evaluate(ctx, judge, pol, frames=frames)
+        log(f"{name}: {out[name]}")
+    for name, pol in (("ray_hit_budget_paged", nat.POLICY_RAYHIT_BUDGET), ("learned_paged", nat.POLICY_LEARNED)):
+        try:
+            out[name] = w.evaluate_paged(ctx, judge, pol, frames=frames)
+        except nat.NomadError as exc:  # a traversal width the paging cannot hold
+            out[name] = {"error": str(exc)}
         log(f"{name}: {out[name]}")
     rh, le = out["ray_hit_budget"]["rel_mse"], out["learned"]["rel_mse"]
     out["learned_vs_rayhit_rel_mse_ratio"] = le / rh if rh > 0 else None
