@@ -102,7 +102,7 @@ struct ObjPage {
 
 struct Retire {
   Span node, rec;
-  cudaEvent_t after = nullptr;  // compute-stream event behind the unlink
+  cudaEvent_t after = nullptr;  // compute-stream event behind the unlink (shared by one update's evictions)
   cudaEvent_t copy = nullptr;   // the object's copy event when it was still streaming (not owned)
   uint32_t obj = 0;
 };
@@ -124,6 +124,7 @@ struct Paging {
   std::vector<int32_t> ref;     // host copy of the published ref table
   RangeAlloc nodeAlloc, recAlloc;
   std::vector<Retire> retiring;
+  std::vector<cudaEvent_t> eventPool;  // unlink events not in use
   std::vector<uint32_t> recObject;  // leaf position -> object
   cudaStream_t copy = nullptr;
   cudaEvent_t lastCopy = nullptr;   // behind the latest copy queued
@@ -141,8 +142,10 @@ struct Paging {
   ~Paging() {
     for (auto &o : obj)
       if (o.copied) cudaEventDestroy(o.copied);
+    std::vector<cudaEvent_t> evs = eventPool;
     for (auto &r : retiring)
-      if (r.after) cudaEventDestroy(r.after);
+      if (r.after && std::find(evs.begin(), evs.end(), r.after) == evs.end()) evs.push_back(r.after);
+    for (cudaEvent_t e : evs) cudaEventDestroy(e);
     if (lastCopy) cudaEventDestroy(lastCopy);
     if (itemsFree) cudaEventDestroy(itemsFree);
     if (copy) cudaStreamDestroy(copy);
@@ -463,18 +466,25 @@ void collect_ready(Paging *pg, std::vector<PubItem> &items, bool all) {
 
 void refresh_retired(Paging *pg) {
   size_t k = 0;
+  std::vector<cudaEvent_t> done, busy;
   for (size_t i = 0; i < pg->retiring.size(); ++i) {
     Retire &r = pg->retiring[i];
-    const bool done = cudaEventQuery(r.after) == cudaSuccess && (!r.copy || cudaEventQuery(r.copy) == cudaSuccess);
-    if (done) {
+    const bool ready = cudaEventQuery(r.after) == cudaSuccess && (!r.copy || cudaEventQuery(r.copy) == cudaSuccess);
+    if (ready) {
       pg->nodeAlloc.release(r.node.off, r.node.len);
       pg->recAlloc.release(r.rec.off, r.rec.len);
-      cudaEventDestroy(r.after);
+      done.push_back(r.after);
     } else {
+      busy.push_back(r.after);
       pg->retiring[k++] = r;
     }
   }
   pg->retiring.resize(k);
+  // an unlink event returns to the pool once no pending retire shares it
+  std::sort(done.begin(), done.end());
+  done.erase(std::unique(done.begin(), done.end()), done.end());
+  for (cudaEvent_t e : done)
+    if (std::find(busy.begin(), busy.end(), e) == busy.end()) pg->eventPool.push_back(e);
 }
 
 }  // namespace
@@ -507,10 +517,19 @@ extern "C" nomad_status nomad_paging_update(nomad_ctx *ctx) {
   collect_ready(pg, items, false);
   nomad_status st = publish(ctx, pg, items);
   if (st != NOMAD_OK) return st;
-  for (Retire &r : retire) {
-    NOMAD_CUDA(ctx, cudaEventCreateWithFlags(&r.after, cudaEventDisableTiming));
-    NOMAD_CUDA(ctx, cudaEventRecord(r.after, ctx->stream));
-    pg->retiring.push_back(r);
+  if (!retire.empty()) {
+    cudaEvent_t ev;
+    if (!pg->eventPool.empty()) {
+      ev = pg->eventPool.back();
+      pg->eventPool.pop_back();
+    } else {
+      NOMAD_CUDA(ctx, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    }
+    NOMAD_CUDA(ctx, cudaEventRecord(ev, ctx->stream));
+    for (Retire &r : retire) {
+      r.after = ev;
+      pg->retiring.push_back(r);
+    }
   }
   // onloads, in object order, at most maxOnloads
   uint32_t started = 0;

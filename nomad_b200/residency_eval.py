@@ -6,7 +6,8 @@ frame renders the view with the current resident set (per-object hit counting on
 one residency step. The image judge is the same frame rendered with every object resident
 (a second context, same Philox streams), compared in HDR:
 rel-MSE = mean((I - I_AR)^2) / mean(I_AR^2), averaged over the frames whose reference is not
-black.
+black (also reported: its median, and the energy-weighted sum(num) / sum(den) over the path, which
+near-black reference frames cannot dominate).
 
 The learned scorer is trained on the device on hit counts recorded along seeded training camera
 paths rendered with every object resident: features of frame f, target log1p(hits of frame
@@ -129,14 +130,14 @@ class Workload:
         return ctx.mlp_train(x, t, steps=steps, batch=batch, lr=lr, weight_decay=1e-4, seed=seed)
 
     # ---- evaluation ------------------------------------------------------------------------
-    def evaluate(self, ctx, judge, policy, path_seed=1, frames=None, warm=5):
+    def evaluate(self, ctx, judge, policy, path_seed=1, frames=None, warm=5, budget_fraction=None):
         """Runs the camera path with one policy; returns per-frame rel-MSE and timings."""
         import torch
 
         frames = frames or self.frames
         views = self.views(path_seed, frames)
         nbytes = ctx.object_bytes()
-        budget = int(self.budget_fraction * nbytes.sum())
+        budget = int((budget_fraction or self.budget_fraction) * nbytes.sum())
         prm = nat.ResidencyParams.make(policy, budget_bytes=budget if policy != nat.POLICY_ALWAYS else 0,
                                        camera_motion=0.3, min_active=0)
         # start from everything resident, as the reference's AlwaysResident warm-up does
@@ -146,6 +147,7 @@ class Workload:
         d_img = torch.empty(npix * 3, dtype=torch.float32, device="cuda")
         d_ref = torch.empty(npix * 3, dtype=torch.float32, device="cuda")
         mse, ms, resident_bytes = [], [], []
+        sum_num = sum_den = 0.0
         for f, v in enumerate(views):
             judge.render_dev(v, d_ref.data_ptr())
             judge.sync()
@@ -160,10 +162,14 @@ class Workload:
             if f >= warm:
                 if den > 0:  # a black reference frame (camera inside geometry) has no relative error
                     mse.append(num / den)
+                sum_num += num
+                sum_den += den
                 ms.append(dt * 1e3)
                 flags = ctx.residency_flags().astype(bool)
                 resident_bytes.append(int(nbytes[flags].sum()))
-        return {"rel_mse": float(np.mean(mse)), "ms_per_frame": float(np.mean(ms)),
+        return {"rel_mse": float(np.mean(mse)), "rel_mse_p50": float(np.median(mse)),
+                "rel_mse_energy": sum_num / sum_den if sum_den > 0 else None,
+                "ms_per_frame": float(np.mean(ms)),
                 "ms_per_frame_p50": float(np.median(ms)),
                 "resident_fraction": float(np.mean(resident_bytes) / nbytes.sum()),
                 "frames": len(mse)}
@@ -199,6 +205,7 @@ class Workload:
             d_img = torch.empty(npix * 3, dtype=torch.float32, device="cuda")
             d_ref = torch.empty(npix * 3, dtype=torch.float32, device="cuda")
             mse, ms, streamed, onl = [], [], [], []
+            sum_num = sum_den = 0.0
             prev = pc.paging_stats()
             for f, v in enumerate(views):
                 judge.render_dev(v, d_ref.data_ptr())
@@ -215,6 +222,8 @@ class Workload:
                 st = pc.paging_stats()
                 if f >= warm:
                     mse.append(num / den if den > 0 else None)
+                    sum_num += num
+                    sum_den += den
                     ms.append(dt * 1e3)
                     streamed.append(st["bytes_streamed"] - prev["bytes_streamed"])
                     onl.append(st["onloads"] - prev["onloads"])
@@ -222,7 +231,9 @@ class Workload:
             st = pc.paging_stats()
             late = [m for m in mse[max(0, 40 - warm):] if m is not None]
             mse = [m for m in mse if m is not None]
-            return {"rel_mse": float(np.mean(mse)), "rel_mse_from_frame_40": float(np.mean(late)) if late else None,
+            return {"rel_mse": float(np.mean(mse)), "rel_mse_p50": float(np.median(mse)),
+                    "rel_mse_energy": sum_num / sum_den if sum_den > 0 else None,
+                    "rel_mse_from_frame_40": float(np.mean(late)) if late else None,
                     "ms_per_frame": float(np.mean(ms)),
                     "ms_per_frame_p50": float(np.median(ms)), "frames": len(mse),
                     "pool_bytes": st["pool_bytes"], "full_paged_bytes": st["full_bytes"],
@@ -266,6 +277,18 @@ def run(paths=200, frames_per_path=8, steps=1500, frames=300, log=print):
         except nat.NomadError as exc:  # a traversal width the paging cannot hold
             out[name] = {"error": str(exc)}
         log(f"{name}: {out[name]}")
+    # The learned policy at smaller budgets: the smallest one whose rel-MSE is within 5 % of the
+    # ray-hit policy's at the full budget, and its ms/frame.
+    sweep = {}
+    for frac in (0.1, 0.15, 0.2, 0.25, 0.3):
+        sweep[f"{frac:.2f}"] = w.evaluate(ctx, judge, nat.POLICY_LEARNED, frames=frames, budget_fraction=frac)
+    out["learned_budget_sweep"] = sweep
+    target = 1.05 * out["ray_hit_budget"]["rel_mse"]
+    ok = [k for k, v in sorted(sweep.items()) if v["rel_mse"] <= target]
+    out["learned_matching_rayhit"] = ({"budget_fraction": float(ok[0]), **sweep[ok[0]],
+                                       "ray_hit_ms_per_frame": out["ray_hit_budget"]["ms_per_frame"]}
+                                      if ok else None)
+    log(f"learned budget sweep: { {k: (v['rel_mse'], v['ms_per_frame']) for k, v in sweep.items()} }")
     rh, le = out["ray_hit_budget"]["rel_mse"], out["learned"]["rel_mse"]
     out["learned_vs_rayhit_rel_mse_ratio"] = le / rh if rh > 0 else None
     out["total_s"] = time.perf_counter() - t0
