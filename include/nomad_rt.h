@@ -261,13 +261,23 @@ nomad_status nomad_frame_graph_stats(nomad_ctx *ctx, uint64_t out[3]);
  * `radius_px` from this frame's temporally resampled reservoirs, each reused reservoir's sample
  * count capped at m_cap * candidates, surface-similarity gates of the reference (position
  * max(1% depth, 0.02), depth max(2% depth, 0.05), normal dot >= 0.9), one visibility ray for the
- * final sample. Temporal reuse needs the same views (sizes, spp) as the previous frame. */
+ * final sample. Temporal reuse needs the same views (sizes, spp) as the previous frame.
+ *
+ * reference_mode = 1 runs the reference's own ReSTIR instead (PathTracing.h:308-480,
+ * :1363-1742): every candidate is traced for visibility before RIS and an occluded or
+ * rejected candidate is not counted; the candidate weight is target / solid-angle pdf; reuse
+ * reads only the previous frame: its reservoir at the reprojected pixel (temporal, with the
+ * reference's Jacobian clamped to 32) and at the 4 pixels +-1 around this one (spatial), each
+ * gated by the same surface tests, re-traced for visibility and combined with the reference's
+ * MIS weights, uncapped; the result is added without a further visibility ray. `spatial`,
+ * `radius_px` and `m_cap` are unused; candidates <= 64. */
 typedef struct nomad_restir_config {
-  uint32_t candidates;   /* 32                                                             */
-  uint32_t temporal;     /* 1 = reuse the previous frame                                   */
-  uint32_t spatial;      /* 3 neighbours                                                   */
-  float radius_px;       /* 30                                                             */
-  float m_cap;           /* 20                                                             */
+  uint32_t candidates;     /* 32                                                           */
+  uint32_t temporal;       /* 1 = reuse the previous frame                                 */
+  uint32_t spatial;        /* 3 neighbours                                                 */
+  float radius_px;         /* 30                                                           */
+  float m_cap;             /* 20                                                           */
+  uint32_t reference_mode; /* 0 = the configuration above, 1 = the reference's ReSTIR      */
 } nomad_restir_config;
 nomad_status nomad_set_restir(nomad_ctx *ctx, const nomad_restir_config *cfg);
 /* Forgets the previous frame's reservoirs (next frame starts without temporal reuse). */

@@ -165,17 +165,31 @@ __global__ void k_gather(const int32_t *__restrict__ primIdx, const uint32_t *__
   }
   const uint32_t mask = __ballot_sync(0xffffffffu, on);
   const uint32_t items = (uint32_t)__popc(mask) * 12u;  // 7 primitive + 5 material float4 each
-  for (uint32_t b = 0; b < items; b += 32u) {
-    const uint32_t q = b + (uint32_t)lane;
+  // All of a lane's loads are issued before its stores (up to 12 in flight per lane).
+  float4 buf[12];
+  float4 *dst[12];
+#pragma unroll
+  for (int i = 0; i < 12; ++i) {
+    const uint32_t q = (uint32_t)(i * 32 + lane);
     const bool valid = q < items;
     const uint32_t r = q / 12u, part = q - r * 12u;
     const int src = valid ? (int)__fns(mask, 0u, (int)r + 1) : 0;
     const int32_t gs = __shfl_sync(0xffffffffu, g, src);
     const uint32_t ks = __shfl_sync(0xffffffffu, k, src);
-    if (!valid) continue;
-    if (part < 7u) oPrims[(size_t)ks * 7 + part] = __ldg(&prims[(size_t)gs * 7 + part]);
-    else oMats[(size_t)ks * 5 + (part - 7u)] = __ldg(&mats[(size_t)gs * 5 + (part - 7u)]);
+    dst[i] = nullptr;
+    if (valid) {
+      if (part < 7u) {
+        buf[i] = __ldg(&prims[(size_t)gs * 7 + part]);
+        dst[i] = oPrims + (size_t)ks * 7 + part;
+      } else {
+        buf[i] = __ldg(&mats[(size_t)gs * 5 + (part - 7u)]);
+        dst[i] = oMats + (size_t)ks * 5 + (part - 7u);
+      }
+    }
   }
+#pragma unroll
+  for (int i = 0; i < 12; ++i)
+    if (dst[i]) *dst[i] = buf[i];
 }
 
 // First leaf position covered by the subtree of node u (walk left children to a leaf).

@@ -740,7 +740,8 @@ extern "C" nomad_status nomad_render_frame(nomad_ctx *ctx, const nomad_view *vie
     for (const DeviceBuf *b : {&F.thr, &F.rad, &F.qRays[0], &F.qRays[1], &F.qIds[0], &F.qIds[1], &F.hits, &F.sRays,
                                &F.sIds, &F.sContrib, &F.sOcc, &F.counters, &F.views, &F.lightIdx, &F.lightCdf,
                                &F.lightMeta, &F.rInit, &F.rTemp, &F.resv[0], &F.resv[1], &F.surf[0], &F.surf[1],
-                               &F.prevViews})
+                               &F.prevViews, &F.lightPdf, &F.refRays, &F.refIds, &F.refOcc, &F.refMask,
+                               &F.reuseMask, &F.refContrib})
       key_put(key, b->p);
     key_put(key, plan.on);
     key_put(key, plan.cur);
@@ -1116,6 +1117,424 @@ __global__ void __launch_bounds__(kPtBlock) k_restir_shade(
   }
 }
 
+// ---- reference mode: the reference's own ReSTIR (PathTracing.h:308-480, :1363-1742) ----------
+// Three passes around two visibility traces:
+//   cand  : the surface record and every candidate's geometry (sampleDirectLightCandidate up to
+//           its visibility test, :324-371); each surviving candidate queues its shadow ray;
+//   reuse : RIS over the candidates whose ray was unoccluded (target / solid-angle pdf, :1393-
+//           1398), then the reuse candidates of the previous frame (the reprojected pixel and
+//           the 4 pixels +-1, gated as at :1455-1473 and :1531-1550) rebuilt from the stored
+//           samples (buildRestirCandidateFromStored, :414-438), each queuing its shadow ray;
+//   final : spatial then temporal resampling with the reference's MIS weights and Jacobian
+//           (:1594-1706), the estimate weightSum / (M * selectedWeight) (:1708-1713), written to
+//           the path through the shadow queue as an entry whose ray has an empty interval (so
+//           it is added exactly where the configuration's estimate is).
+// Reservoirs keep the reference's data0..data2 (:1716-1727): a = (light position, bits(light
+// primitive)), b = (light normal, 1 / light area), c = (candidate pdf, weight sum, sample count,
+// selected weight); the id is kept as an integer and the area as the reciprocal it is read as.
+
+constexpr uint32_t kRefReuse = 5;  // 4 spatial neighbours (+x, -x, +y, -y) and the temporal sample
+
+struct RefCand {
+  V3 lpos, lnrm, wi, radG;  // radG = radiance * geometryFactor
+  float invArea, dist, pdf;
+  int32_t lp;
+};
+
+struct RefArgs {
+  const float *lightPdf;  // per primitive (lightPdfLookup)
+  uint32_t primCount;
+  uint32_t words;         // candidate mask words per path
+};
+
+// Candidate geometry before its visibility test; false when the reference rejects it.
+__device__ __forceinline__ bool ref_geometry(const Surf &s, const Material &m, V3 lpos, V3 lnrm, float invArea,
+                                             float lightPdf, V3 lrad, int32_t lp, RefCand &c) {
+  V3 p = ld3(s.p), n = ld3(s.n);
+  V3 toL = lpos - p;
+  float dist2 = dot(toL, toL);
+  if (dist2 <= kRayEps) return false;
+  float dist = sqrtf(dist2);
+  V3 wi = toL / dist;
+  float cosT = fmax_ref(dot(n, wi), 0.0f), cosL = fmax_ref(dot(lnrm, -wi), 0.0f);
+  if (cosT <= 0.0f || cosL <= 0.0f) return false;
+  if (lightPdf <= 0.0f) return false;
+  float pdfSolid = invArea * dist2 / cosL;
+  float pdf = lightPdf * pdfSolid;
+  if (pdf <= 0.0f) return false;
+  V3 rad = eval_bsdf(m, n, ld3(s.v), wi) * lrad * cosT;
+  float g = cosL / fmax_ref(dist2, kRayEps);
+  c.lpos = lpos;
+  c.lnrm = lnrm;
+  c.wi = wi;
+  c.radG = rad * g;
+  c.invArea = invArea;
+  c.dist = dist;
+  c.pdf = pdf;
+  c.lp = lp;
+  return true;
+}
+
+// New candidate c of a path (Philox stream 0x10000 + c, as in the configuration).
+__device__ __forceinline__ bool ref_new_candidate(const Surf &s, const Material &m, const Lights &L, uint32_t lightCount,
+                                                  float lightTotal, U4 u, RefCand &c) {
+  const uint32_t off = select_light(u01(u.x), L, lightCount, lightTotal);
+  const float4 *rec = L.rec + 5ull * off;
+  const float4 r3 = __ldg(rec + 3), r4 = __ldg(rec + 4);
+  const int32_t lp = __float_as_int(r3.w);
+  if (lp == __float_as_int(s.n.w) || !(r4.w > 0.0f)) return false;
+  V3 lnrm;
+  const V3 lpos = light_point(record_shape(rec), u01(u.y), u01(u.z), lnrm);
+  return ref_geometry(s, m, lpos, lnrm, __ldg(rec + 1).w, __ldg(rec).w, ld3(r4), lp, c);
+}
+
+// A candidate rebuilt from a stored reservoir sample.
+__device__ __forceinline__ bool ref_stored_candidate(const Surf &s, const Material &m, const float4 *__restrict__ mats,
+                                                     const RefArgs &ra, const Resv &src, RefCand &c) {
+  const int32_t lp = __float_as_int(src.a.w);
+  if (!(src.b.w > 0.0f) || lp == __float_as_int(s.n.w) || lp < 0 || (uint32_t)lp >= ra.primCount) return false;
+  const Material lm = decode_material(mats, lp, 1.0f);
+  return ref_geometry(s, m, ld3(src.a), ld3(src.b), src.b.w, ra.lightPdf[lp], lm.emission * lm.power, lp, c);
+}
+
+__device__ __forceinline__ bool ref_prev_valid(const Resv &q) {
+  return q.c.y > 0.0f && q.c.z > 0.0f && q.c.w > 0.0f;
+}
+
+// restirUpdateReservoir (:98-115); `contrib` follows the selected sample.
+__device__ __forceinline__ void ref_update(Resv &r, V3 &contrib, const RefCand &c, V3 cc, float w, float inc, float xi) {
+  if (w <= 0.0f || inc <= 0.0f) return;
+  r.c.y = r.c.y + w;
+  r.c.z = r.c.z + inc;
+  if (__float_as_int(r.a.w) < 0 || xi * r.c.y < w) {
+    r.a = make_float4(c.lpos.x, c.lpos.y, c.lpos.z, __int_as_float(c.lp));
+    r.b = make_float4(c.lnrm.x, c.lnrm.y, c.lnrm.z, c.invArea);
+    r.c.x = c.pdf;
+    r.c.w = w;
+    contrib = cc;
+  }
+}
+
+// The shadow ray of a candidate (isLightVisible, :511-521): origin offset 5e-4 along the normal.
+__device__ __forceinline__ void ref_ray(const Surf &s, const RefCand &c, float4 &A, float4 &B) {
+  V3 o = ld3(s.p) + ld3(s.n) * (5.0f * kRayEps);
+  float tmax = c.dist - kRayEps;
+  if (tmax < kRayEps) tmax = kRayEps;
+  A = make_float4(o.x, o.y, o.z, kRayEps);
+  B = make_float4(c.wi.x, c.wi.y, c.wi.z, tmax);
+}
+
+// The previous frame's path at the pixel this path's surface reprojects to, or -1.
+__device__ __forceinline__ long long ref_reproject(const ViewDev &v, const ViewDev &pv, const Surf &s, uint32_t sample) {
+  V3 cam = v3(pv.cam[0], pv.cam[1], pv.cam[2]), U = v3(pv.vu[0], pv.vu[1], pv.vu[2]);
+  V3 Vv = v3(pv.vv[0], pv.vv[1], pv.vv[2]), fp = v3(pv.fp[0], pv.fp[1], pv.fp[2]);
+  V3 pn = cross(U, Vv);
+  V3 dd = ld3(s.p) - cam;
+  float den = dot(dd, pn);
+  float num = dot(fp - cam, pn);
+  if (den == 0.0f) return -1;
+  float lam = num / den;
+  if (!(lam > 0.0f)) return -1;
+  V3 q = cam + dd * lam;
+  V3 rel = q - fp;
+  float u = dot(rel, U) / dot(U, U), w = dot(rel, Vv) / dot(Vv, Vv);
+  if (!(u >= 0.0f && u < 1.0f && w >= 0.0f && w < 1.0f)) return -1;
+  uint32_t px = min((uint32_t)(u * (float)pv.w), pv.w - 1), py = min((uint32_t)(w * (float)pv.h), pv.h - 1);
+  return (long long)(pv.pathOffset + ((unsigned long long)py * pv.w + px) * pv.spp + sample);
+}
+
+// The previous frame's path at neighbour k (0..3: +x, -x, +y, -y) of this path's pixel, or -1.
+__device__ __forceinline__ long long ref_neighbour(const ViewDev &v, const ViewDev &pv, uint32_t pixel, uint32_t sample,
+                                                   uint32_t k) {
+  const int dx[4] = {1, -1, 0, 0}, dy[4] = {0, 0, 1, -1};
+  int nx = (int)(pixel % v.w) + dx[k], ny = (int)(pixel / v.w) + dy[k];
+  if (nx < 0 || ny < 0 || nx >= (int)pv.w || ny >= (int)pv.h) return -1;
+  return (long long)(pv.pathOffset + ((unsigned long long)ny * pv.w + nx) * pv.spp + sample);
+}
+
+// Reuse candidate k of a path: the prior reservoir it comes from and the rebuilt candidate.
+__device__ __forceinline__ bool ref_reuse_candidate(uint32_t k, const ViewDev &v, const ViewDev &pv, const Surf &s,
+                                                    const Material &m, const float4 *__restrict__ mats,
+                                                    const RefArgs &ra, const Resv *__restrict__ rPrev,
+                                                    const Surf *__restrict__ sPrev, uint32_t pixel, uint32_t sample,
+                                                    Resv &q, long long &qid, bool &prevValid, RefCand &c) {
+  qid = k < 4 ? ref_neighbour(v, pv, pixel, sample, k) : ref_reproject(v, pv, s, sample);
+  prevValid = false;
+  if (qid < 0 || !restir_gate(s, sPrev[qid])) return false;
+  q = rPrev[qid];
+  if (!ref_prev_valid(q)) return false;
+  prevValid = true;
+  return ref_stored_candidate(s, m, mats, ra, q, c);
+}
+
+__global__ void __launch_bounds__(kPtBlock, NOMAD_PT_MINB) k_restir_ref_cand(
+    const ViewDev *__restrict__ views, uint32_t nviews, unsigned long long P, RestirDev cfg,
+    const float4 *__restrict__ rays, const int32_t *__restrict__ hits, const float4 *__restrict__ prims,
+    const float4 *__restrict__ mats, Lights L, Surf *__restrict__ sOut, uint32_t *__restrict__ mask, RefArgs ra,
+    float4 *__restrict__ qRays, uint32_t *__restrict__ qIds, Counters *cnt) {
+  const uint32_t lightCount = L.meta->count;
+  const float lightTotal = L.meta->total;
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  const unsigned long long iters = (P + stride - 1) / stride;
+  for (unsigned long long it = 0; it < iters; ++it) {
+    const unsigned long long pid = it * stride + (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    Surf s;
+    s.p = s.n = s.v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    Material m{};
+    uint32_t pixel = 0, sample = 0;
+    const ViewDev *vp = nullptr;
+    if (pid < P) {
+      const ViewDev &v = find_view(views, nviews, pid);
+      vp = &v;
+      const int32_t *h = hits + 5 * pid;
+      const int32_t prim = h[1];
+      if ((v.flags & NOMAD_VIEW_RESTIR) && prim >= 0 && lightCount > 0 && lightTotal > 0.0f) {
+        float t = __int_as_float(h[2]);
+        V3 o = ld3(rays[2 * pid]), d = ld3(rays[2 * pid + 1]);
+        V3 p = v3(o.x + t * d.x, o.y + t * d.y, o.z + t * d.z);
+        V3 n = hit_normal(prims, prim, p);
+        if (!(dot(n, d) < 0.0f)) n = -n;
+        m = decode_material(mats, prim, v.lod);
+        if (luminance(m.diffuse * m.opacity) > 0.0f) {
+          V3 vd = normalize(-d);
+          s.p = make_float4(p.x, p.y, p.z, length(p - o));
+          s.n = make_float4(n.x, n.y, n.z, __int_as_float(prim));
+          s.v = make_float4(vd.x, vd.y, vd.z, 1.0f);
+        }
+      }
+      unsigned long long local = pid - v.pathOffset;
+      pixel = (uint32_t)(local / v.spp);
+      sample = (uint32_t)(local % v.spp);
+      sOut[pid] = s;
+      for (uint32_t w = 0; w < ra.words; ++w) mask[pid * ra.words + w] = 0u;
+    }
+    for (uint32_t c = 0; c < cfg.candidates; ++c) {
+      RefCand cd;
+      bool want = false;
+      if (s.v.w > 0.0f) {
+        const U4 u = philox(U4{pixel, sample, 0x10000u + c, vp->index}, vp->k0, vp->k1);
+        want = ref_new_candidate(s, m, L, lightCount, lightTotal, u, cd);
+      }
+      const uint32_t slot = warp_append(&cnt->qlen[3], want);
+      if (want) {
+        float4 A, B;
+        ref_ray(s, cd, A, B);
+        qRays[2ull * slot] = A;
+        qRays[2ull * slot + 1] = B;
+        qIds[slot] = (uint32_t)(pid * cfg.candidates + c);
+      }
+    }
+  }
+}
+
+// Unoccluded entries of the visibility queue set their bit in the path's mask.
+__global__ void __launch_bounds__(kPtBlock) k_restir_ref_vis(const uint32_t *__restrict__ ids,
+                                                             const uint8_t *__restrict__ occ, uint32_t per,
+                                                             uint32_t words, uint32_t *__restrict__ mask,
+                                                             Counters *cnt) {
+  const uint32_t n = cnt->qlen[3];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (occ[i]) continue;
+    const uint32_t id = ids[i], pid = id / per, c = id - pid * per;
+    atomicOr(&mask[(unsigned long long)pid * words + c / 32], 1u << (c % 32));
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) cnt->stats[2] += n;
+}
+
+__global__ void k_restir_ref_reset(Counters *cnt) {
+  cnt->qlen[3] = 0;
+  cnt->cursor[1] = 0;
+}
+
+__global__ void __launch_bounds__(kPtBlock, NOMAD_PT_MINB) k_restir_ref_reuse(
+    const ViewDev *__restrict__ views, const ViewDev *__restrict__ prevViews, uint32_t nviews, unsigned long long P,
+    RestirDev cfg, const float4 *__restrict__ mats, Lights L, const Surf *__restrict__ sCur,
+    const uint32_t *__restrict__ candMask, RefArgs ra, const Resv *__restrict__ rPrev, const Surf *__restrict__ sPrev,
+    int usePrev, Resv *__restrict__ rMid, float4 *__restrict__ midContrib, uint32_t *__restrict__ reuseMask,
+    float4 *__restrict__ qRays, uint32_t *__restrict__ qIds, Counters *cnt) {
+  const uint32_t lightCount = L.meta->count;
+  const float lightTotal = L.meta->total;
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  const unsigned long long iters = (P + stride - 1) / stride;
+  for (unsigned long long it = 0; it < iters; ++it) {
+    const unsigned long long pid = it * stride + (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    Surf s;
+    s.v.w = 0.0f;
+    Material m{};
+    uint32_t pixel = 0, sample = 0;
+    const ViewDev *vp = nullptr;
+    if (pid < P) {
+      s = sCur[pid];
+      const ViewDev &v = find_view(views, nviews, pid);
+      vp = &v;
+      unsigned long long local = pid - v.pathOffset;
+      pixel = (uint32_t)(local / v.spp);
+      sample = (uint32_t)(local % v.spp);
+      Resv r = resv_empty();
+      V3 contrib = v3(0.0f, 0.0f, 0.0f);
+      if (s.v.w > 0.0f) {
+        m = decode_material(mats, __float_as_int(s.n.w), v.lod);
+        for (uint32_t c = 0; c < cfg.candidates; ++c) {
+          if (!((candMask[pid * ra.words + c / 32] >> (c % 32)) & 1u)) continue;
+          const U4 u = philox(U4{pixel, sample, 0x10000u + c, v.index}, v.k0, v.k1);
+          RefCand cd;
+          if (!ref_new_candidate(s, m, L, lightCount, lightTotal, u, cd)) continue;
+          const V3 cc = cd.radG / cd.pdf;
+          const float target = fmax_ref(luminance(cd.radG), 0.0f);
+          const float w = cd.pdf > 0.0f ? target / cd.pdf : 0.0f;
+          ref_update(r, contrib, cd, cc, w, 1.0f, u01(u.w));
+        }
+      }
+      rMid[pid] = r;
+      midContrib[pid] = make_float4(contrib.x, contrib.y, contrib.z, 0.0f);
+      reuseMask[pid] = 0u;
+    }
+    for (uint32_t k = 0; k < kRefReuse; ++k) {
+      RefCand cd;
+      bool want = false;
+      if (usePrev && s.v.w > 0.0f) {
+        Resv q;
+        long long qid;
+        bool pv;
+        want = ref_reuse_candidate(k, *vp, prevViews[vp->index], s, m, mats, ra, rPrev, sPrev, pixel, sample, q, qid,
+                                   pv, cd);
+      }
+      const uint32_t slot = warp_append(&cnt->qlen[3], want);
+      if (want) {
+        float4 A, B;
+        ref_ray(s, cd, A, B);
+        qRays[2ull * slot] = A;
+        qRays[2ull * slot + 1] = B;
+        qIds[slot] = (uint32_t)(pid * kRefReuse + k);
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kPtBlock, NOMAD_PT_MINB) k_restir_ref_final(
+    const ViewDev *__restrict__ views, const ViewDev *__restrict__ prevViews, uint32_t nviews, unsigned long long P,
+    const float4 *__restrict__ mats, const Surf *__restrict__ sCur, RefArgs ra, const Resv *__restrict__ rPrev,
+    const Surf *__restrict__ sPrev, int usePrev, const Resv *__restrict__ rMid, const float4 *__restrict__ midContrib,
+    const uint32_t *__restrict__ reuseMask, Resv *__restrict__ rOut, float4 *__restrict__ sRays,
+    uint32_t *__restrict__ sIds, float4 *__restrict__ sContrib, Counters *cnt) {
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  const unsigned long long iters = (P + stride - 1) / stride;
+  for (unsigned long long it = 0; it < iters; ++it) {
+    const unsigned long long pid = it * stride + (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    bool want = false;
+    float4 A = make_float4(0, 0, 0, 0), B = A, Cc = A;
+    if (pid < P) {
+      const Surf s = sCur[pid];
+      Resv r = rMid[pid];
+      if (s.v.w > 0.0f) {
+        const ViewDev &v = find_view(views, nviews, pid);
+        const unsigned long long local = pid - v.pathOffset;
+        const uint32_t pixel = (uint32_t)(local / v.spp), sample = (uint32_t)(local % v.spp);
+        const Material m = decode_material(mats, __float_as_int(s.n.w), v.lod);
+        const float4 mc = midContrib[pid];
+        V3 contrib = v3(mc.x, mc.y, mc.z);
+        const float currentM = r.c.z;
+        const uint32_t vis = reuseMask[pid];
+        if (usePrev) {
+          const ViewDev &pv = prevViews[v.index];
+          // temporal validity (the gate and a usable prior reservoir), needed by the spatial MIS
+          Resv tq;
+          long long tqid;
+          bool tPrevValid = false;
+          RefCand tc;
+          const bool tCand = ref_reuse_candidate(4, v, pv, s, m, mats, ra, rPrev, sPrev, pixel, sample, tq, tqid,
+                                                 tPrevValid, tc);
+          // spatial candidates that survived their visibility test (:1531-1591)
+          RefCand sc[4];
+          Resv sq[4];
+          bool sOk[4];
+          float totalSpatialM = 0.0f;
+          for (uint32_t k = 0; k < 4; ++k) {
+            long long qid;
+            bool pvv;
+            sOk[k] = ref_reuse_candidate(k, v, pv, s, m, mats, ra, rPrev, sPrev, pixel, sample, sq[k], qid, pvv,
+                                         sc[k]) &&
+                     ((vis >> k) & 1u);
+            if (sOk[k]) totalSpatialM = totalSpatialM + sq[k].c.z;
+          }
+          for (uint32_t k = 0; k < 4; ++k) {
+            if (!sOk[k]) continue;
+            const RefCand &c = sc[k];
+            const Resv &q = sq[k];
+            const V3 cc = c.radG / c.pdf;
+            const float target = fmax_ref(luminance(c.radG), 0.0f);
+            const float prevTarget = q.c.w * fmax_ref(q.c.x, kRayEps);
+            const float norm = q.c.z > 0.0f ? q.c.y / q.c.z : 0.0f;
+            float w = prevTarget > 0.0f ? norm * (target / prevTarget) : 0.0f;
+            const float sp = fmax_ref(c.pdf, 0.0f);
+            float den = sp * (currentM + totalSpatialM);
+            if (tPrevValid) den = den + tq.c.z * sp * 1.0f;
+            const float mis = den > 0.0f ? (q.c.z * sp) / den : 0.0f;
+            w = w * mis;
+            const U4 rr = philox(U4{pixel, sample, 0x31000u + k, v.index}, v.k0, v.k1);
+            ref_update(r, contrib, c, cc, w, q.c.z, u01(rr.x));
+          }
+          // temporal (:1633-1706)
+          if (tPrevValid && tCand && ((vis >> 4) & 1u)) {
+            const RefCand &c = tc;
+            const V3 cc = c.radG / c.pdf;
+            const float target = fmax_ref(luminance(c.radG), 0.0f);
+            const float prevTarget = tq.c.w * fmax_ref(c.pdf, kRayEps);
+            const float norm = tq.c.z > 0.0f ? tq.c.y / tq.c.z : 0.0f;
+            const Surf &ps = sPrev[tqid];
+            const V3 toCur = c.lpos - ld3(s.p), toPrev = c.lpos - ld3(ps.p);
+            const float curD2 = fmax_ref(dot(toCur, toCur), kRayEps), prevD2 = fmax_ref(dot(toPrev, toPrev), kRayEps);
+            const V3 wiCur = normalize(toCur), wiPrev = normalize(toPrev);
+            const float cosCur = fmax_ref(dot(normalize(ld3(s.n)), wiCur), 0.0f);
+            const float cosPrev = fmax_ref(dot(normalize(normalize(ld3(ps.n))), wiPrev), 0.0f);
+            float J = (prevD2 / curD2) * (cosCur / fmax_ref(cosPrev, kRayEps));
+            if (!isfinite(J) || J < 0.0f) J = 0.0f;
+            else J = fmin_ref(J, 32.0f);
+            float w = prevTarget > 0.0f ? norm * (target / prevTarget) * J : 0.0f;
+            const float tp = fmax_ref(c.pdf, 0.0f);
+            float den = tp * (currentM + totalSpatialM);
+            den = den + tq.c.z * tp * J;
+            const float mis = den > 0.0f ? (tq.c.z * tp * J) / den : 0.0f;
+            w = w * mis;
+            const U4 rr = philox(U4{pixel, sample, 0x21000u, v.index}, v.k0, v.k1);
+            ref_update(r, contrib, c, cc, w, tq.c.z, u01(rr.x));
+          }
+        }
+        if (__float_as_int(r.a.w) >= 0 && r.c.w > 0.0f && r.c.z > 0.0f) {
+          const float norm = r.c.y / (r.c.z * r.c.w);
+          const V3 add = contrib * norm;
+          // an entry whose ray interval is empty: never occluded, resolved with the shadow rays
+          A = make_float4(s.p.x, s.p.y, s.p.z, kRayEps);
+          B = make_float4(0.0f, 0.0f, 1.0f, kRayEps);
+          Cc = make_float4(add.x, add.y, add.z, 0.0f);
+          want = true;
+        }
+      }
+      rOut[pid] = r;
+    }
+    const uint32_t slot = warp_append(&cnt->qlen[2], want);
+    if (want) {
+      sRays[2 * slot] = A;
+      sRays[2 * slot + 1] = B;
+      sIds[slot] = (uint32_t)pid;
+      sContrib[slot] = Cc;
+    }
+  }
+}
+
+// Reuse visibility: bit k of the path's byte-sized mask word.
+__global__ void __launch_bounds__(kPtBlock) k_restir_ref_vis5(const uint32_t *__restrict__ ids,
+                                                              const uint8_t *__restrict__ occ,
+                                                              uint32_t *__restrict__ mask, Counters *cnt) {
+  const uint32_t n = cnt->qlen[3];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (occ[i]) continue;
+    const uint32_t id = ids[i], pid = id / kRefReuse, k = id - pid * kRefReuse;
+    atomicOr(&mask[pid], 1u << k);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) cnt->stats[2] += n;
+}
+
 nomad_status restir_prepare(nomad_ctx *ctx, uint32_t nviews, const nomad_view *views, unsigned long long P,
                             RestirPlan &plan) {
   FrameState &F = ctx->frame;
@@ -1128,6 +1547,22 @@ nomad_status restir_prepare(nomad_ctx *ctx, uint32_t nviews, const nomad_view *v
     }
     F.restirPaths = P;
     F.restirValid = false;
+  }
+  if (F.restir.reference_mode) {
+    const uint64_t per = std::max<uint64_t>(F.restir.candidates, kRefReuse);
+    if (P * per >= 0xffffffffull) return nomad_fail(ctx, NOMAD_ERR_LIMIT, "too many reference-mode ReSTIR candidates");
+    if (F.refRayCap < P * per) {
+      NOMAD_CUDA(ctx, F.refRays.reserve(P * per * 32));
+      NOMAD_CUDA(ctx, F.refIds.reserve(P * per * 4));
+      NOMAD_CUDA(ctx, F.refOcc.reserve(P * per));
+      F.refRayCap = P * per;
+    }
+    if (F.refPaths < P) {
+      NOMAD_CUDA(ctx, F.refMask.reserve(P * 8));
+      NOMAD_CUDA(ctx, F.reuseMask.reserve(P * 4));
+      NOMAD_CUDA(ctx, F.refContrib.reserve(P * 16));
+      F.refPaths = P;
+    }
   }
   NOMAD_CUDA(ctx, F.prevViews.reserve(nviews * sizeof(ViewDev)));
   bool compatible = F.restirValid && F.prevHostViews.size() == nviews;
@@ -1152,6 +1587,42 @@ nomad_status restir_launch(nomad_ctx *ctx, uint32_t nviews, unsigned long long P
   const int cur = plan.cur;
   const int grid = ctx->smCount * 8;
   Surf *sCur = F.surf[cur].as<Surf>();
+  if (cf.reference_mode) {
+    const RefArgs ra{F.lightPdf.as<const float>(), ctx->primCount, (cf.candidates + 31) / 32};
+    const ViewDev *PV = F.prevViews.as<const ViewDev>();
+    k_restir_ref_reset<<<1, 1, 0, s>>>(C);
+    k_restir_ref_cand<<<grid, kPtBlock, 0, s>>>(V, nviews, P, cfg, F.qRays[0].as<const float4>(),
+                                               F.hits.as<const int32_t>(), ctx->prims.as<const float4>(),
+                                               ctx->materials.as<const float4>(), L, sCur, F.refMask.as<uint32_t>(), ra,
+                                               F.refRays.as<float4>(), F.refIds.as<uint32_t>(), C);
+    NOMAD_CUDA(ctx, cudaGetLastError());
+    nomad_status ts = nomad_trace_variant(ctx, ctx->trav, true, F.refRays.as<const float4>(), P * cf.candidates,
+                                          &C->qlen[3], &C->cursor[1], nullptr, F.refOcc.as<uint8_t>(), nullptr, s);
+    if (ts != NOMAD_OK) return ts;
+    k_restir_ref_vis<<<grid, kPtBlock, 0, s>>>(F.refIds.as<const uint32_t>(), F.refOcc.as<const uint8_t>(),
+                                              cf.candidates, ra.words, F.refMask.as<uint32_t>(), C);
+    k_restir_ref_reset<<<1, 1, 0, s>>>(C);
+    k_restir_ref_reuse<<<grid, kPtBlock, 0, s>>>(V, PV, nviews, P, cfg, ctx->materials.as<const float4>(), L, sCur,
+                                                F.refMask.as<const uint32_t>(), ra, F.resv[cur ^ 1].as<const Resv>(),
+                                                F.surf[cur ^ 1].as<const Surf>(), plan.temporal, F.rInit.as<Resv>(),
+                                                F.refContrib.as<float4>(), F.reuseMask.as<uint32_t>(),
+                                                F.refRays.as<float4>(), F.refIds.as<uint32_t>(), C);
+    NOMAD_CUDA(ctx, cudaGetLastError());
+    ts = nomad_trace_variant(ctx, ctx->trav, true, F.refRays.as<const float4>(), P * kRefReuse, &C->qlen[3],
+                             &C->cursor[1], nullptr, F.refOcc.as<uint8_t>(), nullptr, s);
+    if (ts != NOMAD_OK) return ts;
+    k_restir_ref_vis5<<<grid, kPtBlock, 0, s>>>(F.refIds.as<const uint32_t>(), F.refOcc.as<const uint8_t>(),
+                                               F.reuseMask.as<uint32_t>(), C);
+    k_restir_ref_reset<<<1, 1, 0, s>>>(C);
+    k_restir_ref_final<<<grid, kPtBlock, 0, s>>>(V, PV, nviews, P, ctx->materials.as<const float4>(), sCur, ra,
+                                                F.resv[cur ^ 1].as<const Resv>(), F.surf[cur ^ 1].as<const Surf>(),
+                                                plan.temporal, F.rInit.as<const Resv>(), F.refContrib.as<const float4>(),
+                                                F.reuseMask.as<const uint32_t>(), F.resv[cur].as<Resv>(),
+                                                F.sRays.as<float4>(), F.sIds.as<uint32_t>(), F.sContrib.as<float4>(), C);
+    NOMAD_CUDA(ctx, cudaGetLastError());
+    NOMAD_CUDA(ctx, cudaMemcpyAsync(F.prevViews.p, F.views.p, nviews * sizeof(ViewDev), cudaMemcpyDeviceToDevice, s));
+    return NOMAD_OK;
+  }
   const uint32_t cdfCap = std::min<uint32_t>(ctx->res.emissiveCount, 8192u);
   k_restir_initial<<<grid, kPtBlock, cdfCap * sizeof(float), s>>>(
       V, nviews, P, cfg, F.qRays[0].as<const float4>(), F.hits.as<const int32_t>(), ctx->prims.as<const float4>(),
@@ -1181,7 +1652,7 @@ void restir_commit(nomad_ctx *ctx, uint32_t nviews, const nomad_view *views) {
 extern "C" nomad_status nomad_set_restir(nomad_ctx *ctx, const nomad_restir_config *cfg) {
   if (!ctx || !cfg) return NOMAD_ERR_INVALID_ARGUMENT;
   if (cfg->candidates == 0 || cfg->candidates > 1024 || cfg->spatial > 16 || !(cfg->radius_px >= 0.0f) ||
-      !(cfg->m_cap > 0.0f))
+      !(cfg->m_cap > 0.0f) || cfg->reference_mode > 1 || (cfg->reference_mode && cfg->candidates > 64))
     return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "ReSTIR config out of range");
   ctx->frame.restir = *cfg;
   ctx->frame.restirValid = false;

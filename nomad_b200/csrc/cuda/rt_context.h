@@ -62,7 +62,11 @@ struct FrameState {
   uint64_t restirPaths = 0;
   int restirCur = 0;
   bool restirValid = false;
-  nomad_restir_config restir{32, 1, 3, 30.0f, 20.0f};
+  nomad_restir_config restir{32, 1, 3, 30.0f, 20.0f, 0};
+  // reference-mode ReSTIR: candidate and reuse visibility queues, per-path visibility masks,
+  // the selected contribution after the candidates
+  DeviceBuf refRays, refIds, refOcc, refMask, reuseMask, refContrib;
+  uint64_t refRayCap = 0, refPaths = 0;
   std::vector<nomad_view> prevHostViews;
   // Captured frames: one CUDA graph per frame shape (sizes, buffers, traversal configuration,
   // scene parameters); the view table is read from device memory, so cameras, seeds and frame

@@ -190,7 +190,7 @@ class TuneEntry(C.Structure):
 
 class RestirConfig(C.Structure):
     _fields_ = [("candidates", C.c_uint32), ("temporal", C.c_uint32), ("spatial", C.c_uint32),
-                ("radius_px", C.c_float), ("m_cap", C.c_float)]
+                ("radius_px", C.c_float), ("m_cap", C.c_float), ("reference_mode", C.c_uint32)]
 
 POLICY_ALWAYS, POLICY_RAYHIT_BUDGET, POLICY_LEARNED = 0, 1, 2
 N_FEATURES = 24
@@ -708,8 +708,9 @@ class Context:
         self._ck(self.lib.nomad_mlp_set(self.h, _ptr(b)))
 
     # ReSTIR DI
-    def set_restir(self, candidates=32, temporal=True, spatial=3, radius_px=30.0, m_cap=20.0):
-        cfg = RestirConfig(candidates, int(temporal), spatial, radius_px, m_cap)
+    def set_restir(self, candidates=32, temporal=True, spatial=3, radius_px=30.0, m_cap=20.0,
+                   reference_mode=False):
+        cfg = RestirConfig(candidates, int(temporal), spatial, radius_px, m_cap, int(reference_mode))
         self._ck(self.lib.nomad_set_restir(self.h, C.byref(cfg)))
 
     def reset_restir(self):

@@ -125,7 +125,8 @@ class RestirOracle:
     """Chains oracle_render_restir over consecutive frames (keeps the previous frame's
     reservoirs, surfaces and views)."""
 
-    def __init__(self, os_, materials, candidates=32, temporal=True, spatial=3, radius_px=30.0, m_cap=20.0):
+    def __init__(self, os_, materials, candidates=32, temporal=True, spatial=3, radius_px=30.0, m_cap=20.0,
+                 reference_mode=False):
         lib = load()
         if not hasattr(lib, "_restir_bound"):
             lib.oracle_render_restir.argtypes = [_P, _P, C.c_uint32, _P, _P, _P, _P, _P, _P, C.c_uint32,
@@ -135,7 +136,7 @@ class RestirOracle:
             lib._restir_bound = True
         self.os_ = os_
         self.mats = np.ascontiguousarray(materials, np.float32)
-        self.cfg_u = np.array([candidates, int(temporal), spatial], np.uint32)
+        self.cfg_u = np.array([candidates, int(temporal), spatial, int(reference_mode)], np.uint32)
         self.cfg_f = np.array([radius_px, m_cap], np.float32)
         self.prev = None
 

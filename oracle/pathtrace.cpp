@@ -387,6 +387,7 @@ bool occluded(const Ctx &c, const Ray &r) {
 // Precomputed ReSTIR result of one path: the shadow ray and its unoccluded contribution.
 struct RestirOut {
   bool valid = false;
+  bool direct = false;  // reference mode: visibility already applied, added as is
   V origin, dir, contrib;
   float tmax = 0.0f;
 };
@@ -437,7 +438,7 @@ V path(const Ctx &c, const View &vw, uint32_t vi, uint32_t pixel, uint32_t sampl
     if (restirHere) {
       if (rs && rs->valid) {
         stats[2]++;
-        if (!occluded(c, mkray(rs->origin, rs->dir, rs->tmax))) rad = add(rad, rs->contrib);
+        if (rs->direct || !occluded(c, mkray(rs->origin, rs->dir, rs->tmax))) rad = add(rad, rs->contrib);
       }
     } else if (lum(dc) > 0.0f && !c.L.idx.empty() && c.L.total > 0.0f) {
       uint32_t off = select_light(u01(b0.x), c.L);
@@ -655,6 +656,58 @@ void restir_merge(const Ctx &c, ResvH &out, const ResvH &src, const SurfH &s, co
   }
 }
 
+// ---- reference mode (the reference's own ReSTIR, PathTracing.h:308-480, :1363-1742) ----
+// Reservoir layout: a = (light position, bits(light primitive)), b = (light normal, 1 / area),
+// c = (candidate pdf, weight sum, sample count, selected weight).
+struct RefC {
+  V lpos, lnrm, wi, radG;
+  float invArea, dist, pdf;
+  int32_t lp;
+};
+
+// Candidate geometry before the visibility test (sampleDirectLightCandidate :344-371,
+// buildRestirCandidateFromStored :414-438).
+bool ref_geometry(const SurfH &s, const Mat &m, V lpos, V lnrm, float invArea, float lightPdf, V lrad, int32_t lp,
+                  RefC &c) {
+  V p = v(s.p[0], s.p[1], s.p[2]), n = v(s.n[0], s.n[1], s.n[2]);
+  V toL = vsub(lpos, p);
+  float d2 = dt(toL, toL);
+  if (d2 <= RAY_EPS) return false;
+  float dist = std::sqrt(d2);
+  V wi = dvs(toL, dist);
+  float cosT = mx(dt(n, wi), 0.0f), cosL = mx(dt(lnrm, neg(wi)), 0.0f);
+  if (cosT <= 0.0f || cosL <= 0.0f) return false;
+  if (lightPdf <= 0.0f) return false;
+  float pdfSolid = invArea * d2 / cosL;
+  float pdf = lightPdf * pdfSolid;
+  if (pdf <= 0.0f) return false;
+  V rad = scl(mul(bsdf(m, n, v(s.v[0], s.v[1], s.v[2]), wi), lrad), cosT);
+  float g = cosL / mx(d2, RAY_EPS);
+  c = RefC{lpos, lnrm, wi, scl(rad, g), invArea, dist, pdf, lp};
+  return true;
+}
+
+// isLightVisible (:503-556) as the contract's any-hit: origin offset 5e-4 along the normal.
+bool ref_visible(const Ctx &cx, const SurfH &s, const RefC &c) {
+  float tmax = c.dist - RAY_EPS;
+  if (tmax < RAY_EPS) tmax = RAY_EPS;
+  V o = add(v(s.p[0], s.p[1], s.p[2]), scl(v(s.n[0], s.n[1], s.n[2]), 5.0f * RAY_EPS));
+  return !occluded(cx, mkray(o, c.wi, tmax));
+}
+
+void ref_update(ResvH &r, V &contrib, const RefC &c, V cc, float w, float inc, float xi) {
+  if (w <= 0.0f || inc <= 0.0f) return;
+  r.c[1] = r.c[1] + w;
+  r.c[2] = r.c[2] + inc;
+  if (fbi(r.a[3]) < 0 || xi * r.c[1] < w) {
+    r.a[0] = c.lpos.x; r.a[1] = c.lpos.y; r.a[2] = c.lpos.z; r.a[3] = ibf(c.lp);
+    r.b[0] = c.lnrm.x; r.b[1] = c.lnrm.y; r.b[2] = c.lnrm.z; r.b[3] = c.invArea;
+    r.c[0] = c.pdf;
+    r.c[3] = w;
+    contrib = cc;
+  }
+}
+
 float view_lod(const View &vw) {
   float dx[3] = {vw.vu[0] / (float)vw.w, vw.vu[1] / (float)vw.w, vw.vu[2] / (float)vw.w};
   float dy[3] = {vw.vv[0] / (float)vw.h, vw.vv[1] / (float)vw.h, vw.vv[2] / (float)vw.h};
@@ -707,8 +760,186 @@ extern "C" int oracle_render_restir(const float *bvh, const float *tlas, uint32_
   SurfH *sCur = reinterpret_cast<SurfH *>(out_surf);
   const ResvH *rPrev = reinterpret_cast<const ResvH *>(prev_resv);
   const SurfH *sPrev = reinterpret_cast<const SurfH *>(prev_surf);
+  const bool refMode = cfg_u[3] != 0;
+  std::vector<RestirOut> roAll;
+  std::vector<std::vector<uint64_t>> refStats(threads, std::vector<uint64_t>(4, 0));
+  if (refMode) {
+    // lightPdfLookup: the per-primitive light pdf of the current CDF
+    std::vector<float> lpdfOf(prim_count, 0.0f);
+    for (size_t k = 0; k < c.L.idx.size(); ++k) {
+      float w = c.L.cdf[k] - (k ? c.L.cdf[k - 1] : 0.0f);
+      if (w > 0.0f && c.L.total > 0.0f) lpdfOf[c.L.idx[k]] = w / c.L.total;
+    }
+    roAll.resize(P);
+    par([&](uint64_t pid, uint32_t tid) {
+      uint32_t vi = view_of(pid);
+      const View &vw = vs[vi];
+      ResvH r = resv_empty();
+      SurfH s{};
+      V contrib = v(0, 0, 0);
+      RestirOut ro;
+      uint64_t local = pid - poff[vi];
+      uint32_t pixel = (uint32_t)(local / vw.spp), sample = (uint32_t)(local % vw.spp);
+      uint32_t k0 = vw.seedLo, k1 = vw.seedHi + vw.frame;
+      int32_t hitPrim = -1;
+      if ((vw.flags & VIEW_RESTIR) && !c.L.idx.empty() && c.L.total > 0.0f) {
+        uint32_t px = pixel % vw.w, py = pixel / vw.w;
+        U4 r0 = philox(U4{pixel, sample, 255u * 4u, vi}, k0, k1);
+        float ux = ((float)px + 0.5f) / (float)vw.w, uy = ((float)py + 0.5f) / (float)vw.h;
+        bool center = (vw.flags & 4u) != 0;
+        float ss = ux + (center ? 0.0f : (u01(r0.x) - 0.5f) / (float)vw.w);
+        float tt = uy + (center ? 0.0f : (u01(r0.y) - 0.5f) / (float)vw.h);
+        V d = nrmz(v(vw.fp[0] + ss * vw.vu[0] + tt * vw.vv[0] - vw.cam[0], vw.fp[1] + ss * vw.vu[1] + tt * vw.vv[1] - vw.cam[1],
+                    vw.fp[2] + ss * vw.vu[2] + tt * vw.vv[2] - vw.cam[2]));
+        V o = v(vw.cam[0], vw.cam[1], vw.cam[2]);
+        Hit h = closest(c, mkray(o, d, INFINITY));
+        if (h.prim >= 0) {
+          V p = v(o.x + h.t * d.x, o.y + h.t * d.y, o.z + h.t * d.z);
+          V n = geom_normal(prims, h.prim, p);
+          if (!(dt(n, d) < 0.0f)) n = neg(n);
+          Mat m = decode(materials, h.prim, view_lod(vw));
+          if (lum(scl(m.diffuse, m.opacity)) > 0.0f) {
+            V vd = nrmz(neg(d));
+            V dd = vsub(p, o);
+            s = SurfH{{p.x, p.y, p.z, std::sqrt(dt(dd, dd))}, {n.x, n.y, n.z, ibf(h.prim)}, {vd.x, vd.y, vd.z, 1.0f}};
+            hitPrim = h.prim;
+          }
+        }
+      }
+      sCur[pid] = s;
+      if (s.v[3] > 0.0f) {
+        Mat m = decode(materials, hitPrim, view_lod(vw));
+        for (uint32_t k = 0; k < C; ++k) {
+          U4 u = philox(U4{pixel, sample, 0x10000u + k, vi}, k0, k1);
+          uint32_t off = select_light(u01(u.x), c.L);
+          int32_t lp = (int32_t)c.L.idx[off];
+          if (lp == hitPrim) continue;
+          V lpos, lnrm;
+          float area = 0.0f;
+          if (!light_point(prims, (uint32_t)lp, u01(u.y), u01(u.z), lpos, lnrm, area) || !(area > 0.0f)) continue;
+          float prev = off > 0 ? c.L.cdf[off - 1] : 0.0f;
+          float wgt = c.L.cdf[off] - prev;
+          float lightPdf = wgt > 0.0f ? wgt / c.L.total : 0.0f;
+          Mat lm = decode(materials, lp, 1.0f);
+          RefC cd;
+          if (!ref_geometry(s, m, lpos, lnrm, 1.0f / area, lightPdf, scl(lm.emission, lm.power), lp, cd)) continue;
+          refStats[tid][2]++;
+          if (!ref_visible(c, s, cd)) continue;
+          V cc = dvs(cd.radG, cd.pdf);
+          float target = mx(lum(cd.radG), 0.0f);
+          float w = cd.pdf > 0.0f ? target / cd.pdf : 0.0f;
+          ref_update(r, contrib, cd, cc, w, 1.0f, u01(u.w));
+        }
+        const float currentM = r.c[2];
+        if (have_prev && temporal) {
+          const View &pv = pvs[vi];
+          // reuse candidate k (0..3: the pixel +x, -x, +y, -y; 4: the reprojected pixel)
+          auto reuse = [&](uint32_t k, ResvH &q, int64_t &qid, bool &prevValid, RefC &cd) -> bool {
+            qid = -1;
+            prevValid = false;
+            if (k < 4) {
+              const int dx[4] = {1, -1, 0, 0}, dy[4] = {0, 0, 1, -1};
+              int nx = (int)(pixel % vw.w) + dx[k], ny = (int)(pixel / vw.w) + dy[k];
+              if (nx < 0 || ny < 0 || nx >= (int)pv.w || ny >= (int)pv.h) return false;
+              qid = (int64_t)(poff[vi] + ((uint64_t)ny * pv.w + nx) * pv.spp + sample);
+            } else {
+              V cam = v(pv.cam[0], pv.cam[1], pv.cam[2]), U = v(pv.vu[0], pv.vu[1], pv.vu[2]);
+              V Vv = v(pv.vv[0], pv.vv[1], pv.vv[2]), fp = v(pv.fp[0], pv.fp[1], pv.fp[2]);
+              V pn = crs(U, Vv);
+              V dd = vsub(v(s.p[0], s.p[1], s.p[2]), cam);
+              float den = dt(dd, pn), num = dt(vsub(fp, cam), pn);
+              if (den == 0.0f) return false;
+              float lam = num / den;
+              if (!(lam > 0.0f)) return false;
+              V qq = add(cam, scl(dd, lam));
+              V rel = vsub(qq, fp);
+              float uu = dt(rel, U) / dt(U, U), ww = dt(rel, Vv) / dt(Vv, Vv);
+              if (!(uu >= 0.0f && uu < 1.0f && ww >= 0.0f && ww < 1.0f)) return false;
+              uint32_t ppx = std::min((uint32_t)(uu * (float)pv.w), pv.w - 1);
+              uint32_t ppy = std::min((uint32_t)(ww * (float)pv.h), pv.h - 1);
+              qid = (int64_t)(poff[vi] + ((uint64_t)ppy * pv.w + ppx) * pv.spp + sample);
+            }
+            if (!restir_gate(s, sPrev[qid])) return false;
+            q = rPrev[qid];
+            if (!(q.c[1] > 0.0f && q.c[2] > 0.0f && q.c[3] > 0.0f)) return false;
+            prevValid = true;
+            int32_t lp = fbi(q.a[3]);
+            if (!(q.b[3] > 0.0f) || lp == hitPrim || lp < 0 || (uint32_t)lp >= prim_count) return false;
+            Mat lm = decode(materials, lp, 1.0f);
+            return ref_geometry(s, m, v(q.a[0], q.a[1], q.a[2]), v(q.b[0], q.b[1], q.b[2]), q.b[3], lpdfOf[lp],
+                                scl(lm.emission, lm.power), lp, cd);
+          };
+          RefC rc[5];
+          ResvH rq[5];
+          int64_t rid[5];
+          bool pvOk[5], cOk[5], visOk[5];
+          for (uint32_t k = 0; k < 5; ++k) {
+            cOk[k] = reuse(k, rq[k], rid[k], pvOk[k], rc[k]);
+            visOk[k] = false;
+            if (cOk[k]) {
+              refStats[tid][2]++;
+              visOk[k] = ref_visible(c, s, rc[k]);
+            }
+          }
+          float totalSpatialM = 0.0f;
+          for (uint32_t k = 0; k < 4; ++k)
+            if (cOk[k] && visOk[k]) totalSpatialM = totalSpatialM + rq[k].c[2];
+          for (uint32_t k = 0; k < 4; ++k) {
+            if (!(cOk[k] && visOk[k])) continue;
+            const RefC &cd = rc[k];
+            const ResvH &q = rq[k];
+            V cc = dvs(cd.radG, cd.pdf);
+            float target = mx(lum(cd.radG), 0.0f);
+            float prevTarget = q.c[3] * mx(q.c[0], RAY_EPS);
+            float norm = q.c[2] > 0.0f ? q.c[1] / q.c[2] : 0.0f;
+            float w = prevTarget > 0.0f ? norm * (target / prevTarget) : 0.0f;
+            float sp = mx(cd.pdf, 0.0f);
+            float den = sp * (currentM + totalSpatialM);
+            if (pvOk[4]) den = den + rq[4].c[2] * sp * 1.0f;
+            float mis = den > 0.0f ? (q.c[2] * sp) / den : 0.0f;
+            w = w * mis;
+            U4 rr = philox(U4{pixel, sample, 0x31000u + k, vi}, k0, k1);
+            ref_update(r, contrib, cd, cc, w, q.c[2], u01(rr.x));
+          }
+          if (pvOk[4] && cOk[4] && visOk[4]) {
+            const RefC &cd = rc[4];
+            const ResvH &q = rq[4];
+            const SurfH &ps = sPrev[rid[4]];
+            V cc = dvs(cd.radG, cd.pdf);
+            float target = mx(lum(cd.radG), 0.0f);
+            float prevTarget = q.c[3] * mx(cd.pdf, RAY_EPS);
+            float norm = q.c[2] > 0.0f ? q.c[1] / q.c[2] : 0.0f;
+            V toCur = vsub(cd.lpos, v(s.p[0], s.p[1], s.p[2])), toPrev = vsub(cd.lpos, v(ps.p[0], ps.p[1], ps.p[2]));
+            float curD2 = mx(dt(toCur, toCur), RAY_EPS), prevD2 = mx(dt(toPrev, toPrev), RAY_EPS);
+            V wiCur = nrmz(toCur), wiPrev = nrmz(toPrev);
+            float cosCur = mx(dt(nrmz(v(s.n[0], s.n[1], s.n[2])), wiCur), 0.0f);
+            float cosPrev = mx(dt(nrmz(nrmz(v(ps.n[0], ps.n[1], ps.n[2]))), wiPrev), 0.0f);
+            float J = (prevD2 / curD2) * (cosCur / mx(cosPrev, RAY_EPS));
+            if (!std::isfinite(J) || J < 0.0f) J = 0.0f;
+            else J = mn(J, 32.0f);
+            float w = prevTarget > 0.0f ? norm * (target / prevTarget) * J : 0.0f;
+            float tp = mx(cd.pdf, 0.0f);
+            float den = tp * (currentM + totalSpatialM);
+            den = den + q.c[2] * tp * J;
+            float mis = den > 0.0f ? (q.c[2] * tp * J) / den : 0.0f;
+            w = w * mis;
+            U4 rr = philox(U4{pixel, sample, 0x21000u, vi}, k0, k1);
+            ref_update(r, contrib, cd, cc, w, q.c[2], u01(rr.x));
+          }
+        }
+        if (fbi(r.a[3]) >= 0 && r.c[3] > 0.0f && r.c[2] > 0.0f) {
+          float norm = r.c[1] / (r.c[2] * r.c[3]);
+          ro.valid = true;
+          ro.direct = true;
+          ro.contrib = scl(contrib, norm);
+        }
+      }
+      rFin[pid] = r;
+      roAll[pid] = ro;
+    });
+  }
   // initial
-  par([&](uint64_t pid, uint32_t) {
+  if (!refMode) par([&](uint64_t pid, uint32_t) {
     uint32_t vi = view_of(pid);
     const View &vw = vs[vi];
     ResvH r = resv_empty();
@@ -767,7 +998,7 @@ extern "C" int oracle_render_restir(const float *bvh, const float *tlas, uint32_
     sCur[pid] = s;
   });
   // temporal
-  par([&](uint64_t pid, uint32_t) {
+  if (!refMode) par([&](uint64_t pid, uint32_t) {
     ResvH out = rInit[pid];
     const SurfH &s = sCur[pid];
     if (have_prev && temporal && s.v[3] > 0.0f) {
@@ -801,7 +1032,7 @@ extern "C" int oracle_render_restir(const float *bvh, const float *tlas, uint32_
     rTemp[pid] = out;
   });
   // spatial
-  par([&](uint64_t pid, uint32_t) {
+  if (!refMode) par([&](uint64_t pid, uint32_t) {
     ResvH out = rTemp[pid];
     const SurfH &s = sCur[pid];
     if (s.v[3] > 0.0f && spatialN > 0) {
@@ -835,7 +1066,9 @@ extern "C" int oracle_render_restir(const float *bvh, const float *tlas, uint32_
     const ResvH &r = rFin[pid];
     const SurfH &s = sCur[pid];
     int32_t lp = fbi(r.a[3]);
-    if (s.v[3] > 0.0f && lp >= 0 && r.c[2] > 0.0f && r.c[1] > 0.0f && r.c[3] > 0.0f) {
+    if (refMode) {
+      ro = roAll[pid];
+    } else if (s.v[3] > 0.0f && lp >= 0 && r.c[2] > 0.0f && r.c[1] > 0.0f && r.c[3] > 0.0f) {
       Mat m = decode(materials, fbi(s.n[3]), view_lod(vw));
       V fa, wi;
       float dist = 0.0f;
@@ -880,8 +1113,11 @@ extern "C" int oracle_render_restir(const float *bvh, const float *tlas, uint32_
       o[2] = az;
     }
   }
-  if (stats)
+  if (stats) {
     for (auto &x : st)
       for (int k = 0; k < 4; ++k) stats[k] += x[k];
+    for (auto &x : refStats)
+      for (int k = 0; k < 4; ++k) stats[k] += x[k];
+  }
   return 0;
 }

@@ -45,3 +45,19 @@ def test_oracle_render_converges(nb, orc, small_city):
         assert np.isfinite(rgb).all() and (rgb >= 0).all()
         means.append(rgb.mean(0))
     assert np.allclose(means[0], means[1], rtol=0.05), means
+
+
+def test_oracle_restir_reference_mode_reuses(nb, orc, small_city):
+    """The oracle's restatement of the reference's ReSTIR: finite, non-negative radiance, and on
+    the second frame the previous frame's reservoirs are reused (more visibility rays traced for
+    the same candidates)."""
+    _, sb = small_city
+    ref = orc.RestirOracle(orc.OracleScene(sb), sb.materials, candidates=8, temporal=True, reference_mode=True)
+    counts = []
+    for f, pos in enumerate([(0, 60, -120), (0.5, 60, -119.5)]):
+        v = nb.view_pinhole(pos, (0, 10, 0), width=24, height=16, spp=1, max_depth=1, seed=3, frame=f,
+                            flags=nb.VIEW_RESTIR | nb.VIEW_CENTER)
+        rgb, stats = ref.render(v)
+        assert np.isfinite(rgb).all() and (rgb >= 0).all()
+        counts.append(int(stats[2]))
+    assert counts[1] > counts[0]
