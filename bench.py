@@ -251,21 +251,25 @@ def restir_leg(nb, ctx, frames=8):
     scene = nb.synth_city(seed=SEED, emissive_tris=4096, emissive_sigma=1.5)
     sb2 = nb.SceneBVH(scene)
     c2 = nb.Context(0)
+    c3 = nb.Context(0)  # the reference's own ReSTIR, with its own reservoir history
     try:
         c2.upload(sb2)
         c2.set_restir(candidates=32, temporal=True, spatial=3, radius_px=30.0, m_cap=20.0)
+        c3.upload(sb2)
+        c3.set_restir(candidates=32, temporal=True, reference_mode=True)
         rng = np.random.default_rng(SEED + 3)
         ctrl = np.stack([rng.uniform(-150, 150, 5), rng.uniform(120, 220, 5), rng.uniform(-650, -500, 5)], 1)
         path = catmull_rom(ctrl, frames)
         W, H = 480, 270
-        errs = {"restir": [], "nee": []}
+        errs = {"restir": [], "nee": [], "restir_reference_mode": []}
         for f in range(frames):
             pos = tuple(float(x) for x in path[f])
             ref = c2.render(nb.view_pinhole(pos, (0.0, 0.0, 60.0), width=W, height=H, spp=1024, max_depth=1,
                                             seed=9000 + f, flags=nb.VIEW_CENTER))[0]
             den = float((ref.astype(np.float64) ** 2).mean())
-            for name, fl in (("restir", nb.VIEW_RESTIR), ("nee", 0)):
-                img = c2.render(nb.view_pinhole(pos, (0.0, 0.0, 60.0), width=W, height=H, spp=1, max_depth=1,
+            for name, cx, fl in (("restir", c2, nb.VIEW_RESTIR), ("nee", c2, 0),
+                                 ("restir_reference_mode", c3, nb.VIEW_RESTIR)):
+                img = cx.render(nb.view_pinhole(pos, (0.0, 0.0, 60.0), width=W, height=H, spp=1, max_depth=1,
                                                 seed=7, frame=f, flags=fl | nb.VIEW_CENTER))[0]
                 errs[name].append(float(((img.astype(np.float64) - ref) ** 2).mean() / den))
         out = torch.empty(WIDTH * HEIGHT * 3, dtype=torch.float32, device="cuda")
@@ -279,11 +283,21 @@ def restir_leg(nb, ctx, frames=8):
             c2.render_dev(v, out.data_ptr())
         c2.sync()
         ms = (time.perf_counter() - t0) / 4 * 1e3
+        c3.render_dev(v, out.data_ptr())
+        c3.sync()
+        t0 = time.perf_counter()
+        for f in range(4):
+            v["frame"] = f + 1
+            c3.render_dev(v, out.data_ptr())
+        c3.sync()
+        ms_ref = (time.perf_counter() - t0) / 4 * 1e3
         return {"config": "city + 4,096 emissive tris, 8-frame spline, 480x270 error / 1080p timing",
                 "rel_mse_per_frame": errs, "rel_mse_mean": {k: float(np.mean(v)) for k, v in errs.items()},
-                "restir_ms_per_frame_1080p_1spp": ms}
+                "restir_ms_per_frame_1080p_1spp": ms,
+                "restir_reference_mode_ms_per_frame_1080p_1spp": ms_ref}
     finally:
         c2.close()
+        c3.close()
 
 
 def compaction_leg(nb, sb, primary, steps=10):
