@@ -295,7 +295,8 @@ nomad_status nomad_reset_render_stats(nomad_ctx *ctx);
 enum {
   NOMAD_POLICY_ALWAYS = 0,        /* every object resident (the image judge)                  */
   NOMAD_POLICY_RAYHIT_BUDGET = 1, /* decayed per-object closest-hit score (the fallback)       */
-  NOMAD_POLICY_LEARNED = 2        /* BF16 MLP score over NOMAD_FEATURES per-object features    */
+  NOMAD_POLICY_LEARNED = 2,       /* BF16 MLP score over NOMAD_FEATURES per-object features    */
+  NOMAD_POLICY_RAYHIT_PRIM = 3    /* the reference's per-primitive ray-hit budget (see below)    */
 };
 #define NOMAD_FEATURES 24
 
@@ -308,7 +309,13 @@ typedef struct nomad_residency_params {
   float memory_pressure;    /* [0,1]: off-screen objects with hits keep lerp(0.5,0.2,p)      */
   float reserve_base;       /* visibility reserve = ceil(N * (base + motion * reserve_motion)) */
   float reserve_motion;
-  uint32_t min_active;      /* objects always kept (highest scores first)                     */
+  uint32_t min_active;      /* objects always kept (highest scores first); primitives for
+                               NOMAD_POLICY_RAYHIT_PRIM (rayHitMinActivePrimitives, 16)        */
+  /* NOMAD_POLICY_RAYHIT_PRIM only (rayHitTargetFraction 0.54, rayHitRebuildCooldownFrames 4,
+   * stateCooldownFrames 5; max_toggles is rayHitMaxTogglesPerFrame, 16, 0 = unlimited): */
+  float target_fraction;    /* primitives kept = ceil(N * clamp(f + 0.1 motion - 0.24 pressure, 0.34, 0.92)) */
+  uint32_t rebuild_cooldown;/* steps skipped after a step that changed residency              */
+  uint32_t state_cooldown;  /* steps a toggled primitive stays as it is                       */
 } nomad_residency_params;
 
 /* One residency step, all on the device: consumes the per-object closest-hit counts gathered
@@ -324,6 +331,23 @@ typedef struct nomad_residency_params {
  * and index). */
 nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residency_params *params,
                                   const nomad_view *camera, uint32_t *toggled);
+/* NOMAD_POLICY_RAYHIT_PRIM restates updateRayHitBudget per primitive, as the reference runs it
+ * (RendererResidency.cpp:2755-2964, with the per-frame cooldown decrement of :205-207): per-primitive
+ * closest hits (counted by nomad_render_frame with NOMAD_TRACE_COUNT_HITS once the policy has run
+ * a step) decay into a score (score * hit_decay + hits), off-screen primitives (bounding sphere
+ * outside the camera frustum) keep nothing without hits and lerp(0.5, 0.2, pressure) of their
+ * score with hits, visible ones at least 1; the top target by (score, lower index) are wanted,
+ * plus the best visible up to ceil(N * (0.02 + 0.06 motion)) and the min_active best; toggles
+ * go in primitive order, skip primitives in their cooldown and stop at
+ * max(1, round(max_toggles * (1 + 0.45 motion + 0.6 pressure))). It runs on the host over the
+ * device's counters and applies its toggles with nomad_residency_set_primitive_active and
+ * nomad_residency_flush (toggled != NULL is required). */
+/* Per-primitive closest hits counted since the last step (prim_count uint32), and the
+ * per-primitive policy's state after its last step: decayed scores (float), cooldowns (uint32),
+ * the frustum test of that step (uint8, isInView, Renderer.cpp:1765-1817), and every primitive's
+ * activity (uint8); any may be NULL. */
+nomad_status nomad_residency_prim_state(nomad_ctx *ctx, uint32_t *hits, float *scores, uint32_t *cooldowns,
+                                        uint8_t *visible, uint8_t *active);
 /* Per-object geometry bytes (object_count uint64). */
 nomad_status nomad_object_bytes(nomad_ctx *ctx, uint64_t *out);
 /* Features and policy scores of the last step: features[object_count * NOMAD_FEATURES],

@@ -316,7 +316,7 @@ __global__ void __launch_bounds__(kPtBlock) k_shade(
     uint32_t *__restrict__ nIds, float4 *__restrict__ sRays, uint32_t *__restrict__ sIds,
     float4 *__restrict__ sContrib, float4 *__restrict__ thr, float4 *__restrict__ rad,
     const float4 *__restrict__ prims, const float4 *__restrict__ mats, Lights L, Counters *cnt, int cur,
-    uint32_t *__restrict__ objHits, int restirDepth0) {
+    uint32_t *__restrict__ objHits, int restirDepth0, uint32_t *__restrict__ primHits) {
   const uint32_t n = cnt->qlen[cur];
   const uint32_t lightCount = L.meta->count;
   const float lightTotal = L.meta->total;
@@ -330,13 +330,14 @@ __global__ void __launch_bounds__(kPtBlock) k_shade(
     bool hit = false, wantShadow = false, wantNext = false;
     uint32_t pid = 0;
     float4 sA = make_float4(0, 0, 0, 0), sB = sA, sC = sA, nA = sA, nB = sA;
-    int32_t inst = -1;
+    int32_t inst = -1, hitPrim = -1;
     if (live) {
       pid = qIds[i];
       float4 ra = qRays[2 * i], rb = qRays[2 * i + 1];
       V3 o = ld3(ra), d = ld3(rb);
       const int32_t *h = hits + 5 * i;
       int32_t prim = h[1];
+      hitPrim = prim;
       float t = __int_as_float(h[2]);
       float4 T = thr[pid];
       V3 tp = ld3(T);
@@ -440,6 +441,10 @@ __global__ void __launch_bounds__(kPtBlock) k_shade(
       int key = hit ? inst : -1;
       unsigned peers = __match_any_sync(act, key);
       if (hit && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(objHits + inst, (uint32_t)__popc(peers));
+      if (primHits) {  // per-primitive closest hits (primitiveRayStats[2g], PathTracing.h:1216-1226)
+        unsigned pp = __match_any_sync(act, hit ? hitPrim : -1);
+        if (hit && (threadIdx.x & 31) == __ffs(pp) - 1) atomicAdd(primHits + hitPrim, (uint32_t)__popc(pp));
+      }
     }
     uint32_t ss = warp_append(shadowLen, wantShadow);
     if (wantShadow) {
@@ -664,6 +669,7 @@ extern "C" nomad_status nomad_render_frame(nomad_ctx *ctx, const nomad_view *vie
   Lights L{F.lightIdx.as<const uint32_t>(), F.lightCdf.as<const float>(), F.lightMeta.as<const LightMeta>(),
            F.lightRec.as<const float4>()};
   uint32_t *objHits = (flags & NOMAD_TRACE_COUNT_HITS) ? ctx->objHits.as<uint32_t>() : nullptr;
+  uint32_t *primHits = (objHits && ctx->res.primHitsOn) ? ctx->res.primHits.as<uint32_t>() : nullptr;
   bool anyRestir = false;
   for (uint32_t i = 0; i < nviews; ++i) anyRestir |= (views[i].flags & NOMAD_VIEW_RESTIR) != 0;
   RestirPlan plan;
@@ -701,7 +707,8 @@ extern "C" nomad_status nomad_render_frame(nomad_ctx *ctx, const nomad_view *vie
                                          F.qRays[cur ^ 1].as<float4>(), F.qIds[cur ^ 1].as<uint32_t>(),
                                          F.sRays.as<float4>(), F.sIds.as<uint32_t>(), F.sContrib.as<float4>(),
                                          F.thr.as<float4>(), F.rad.as<float4>(), ctx->prims.as<const float4>(),
-                                         ctx->materials.as<const float4>(), L, C, cur, objHits, plan.on ? 1 : 0);
+                                         ctx->materials.as<const float4>(), L, C, cur, objHits, plan.on ? 1 : 0,
+                                         primHits);
       rs = nomad_trace_variant(ctx, ctx->trav, true, F.sRays.as<const float4>(), P, &C->qlen[2], &C->cursor[1],
                                nullptr, F.sOcc.as<uint8_t>(), nullptr, s);
       if (rs != NOMAD_OK) return rs;
@@ -726,6 +733,7 @@ extern "C" nomad_status nomad_render_frame(nomad_ctx *ctx, const nomad_view *vie
     key_put(key, pixels);
     key_put(key, maxDepth);
     key_put(key, objHits);
+    key_put(key, primHits);
     key_put(key, dOut);
     key_put(key, ctx->trav);
     key_put(key, ctx->scene);

@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <vector>
 
 #include "pt_lights.cuh"
@@ -563,11 +564,254 @@ nomad_status nomad_lights_update(nomad_ctx *ctx) {
   return NOMAD_OK;
 }
 
+namespace {
+
+float clamp_unit(float v) { return std::min(std::max(v, 0.0f), 1.0f); }
+
+// Bounding sphere of every primitive (Renderer.cpp:3158-3173): spheres as they are; triangles
+// around the centroid, radius the farthest vertex; rectangles around the centre, radius |u| + |v|.
+void prim_spheres(const nomad_ctx *ctx, std::vector<float> &out) {
+  const uint32_t P = ctx->primCount;
+  out.assign((size_t)P * 4, 0.0f);
+  auto len = [](float x, float y, float z) { return std::sqrt(x * x + y * y + z * z); };
+  for (uint32_t i = 0; i < P; ++i) {
+    const float *g = ctx->hostPrims.data() + 28ull * i;
+    const int type = (int)g[3];
+    float *o = out.data() + 4ull * i;
+    if (type == 0) {
+      o[0] = g[0]; o[1] = g[1]; o[2] = g[2]; o[3] = g[4];
+    } else if (type == 1) {
+      const float cx = (g[0] + g[4] + g[8]) / 3.0f, cy = (g[1] + g[5] + g[9]) / 3.0f,
+                  cz = (g[2] + g[6] + g[10]) / 3.0f;
+      float r = len(g[0] - cx, g[1] - cy, g[2] - cz);
+      r = std::max(r, len(g[4] - cx, g[5] - cy, g[6] - cz));
+      r = std::max(r, len(g[8] - cx, g[9] - cy, g[10] - cz));
+      o[0] = cx; o[1] = cy; o[2] = cz; o[3] = r;
+    } else {
+      o[0] = g[0]; o[1] = g[1]; o[2] = g[2];
+      o[3] = len(g[4], g[5], g[6]) + len(g[8], g[9], g[10]);
+    }
+  }
+}
+
+// Camera of a view for the angular frustum test (Renderer::isInView, Renderer.cpp:1765-1817).
+struct AngleCam {
+  float pos[3], fwd[3], right[3], up[3];
+  float halfV, halfH;  // vertical and horizontal half field of view (radians)
+  bool fwdValid;
+};
+
+AngleCam angle_cam(const nomad_view &v) {
+  AngleCam c{};
+  float U[3], V[3], f[3];
+  for (int k = 0; k < 3; ++k) {
+    c.pos[k] = v.camera_pos[k];
+    U[k] = v.viewport_u[k];
+    V[k] = v.viewport_v[k];
+    f[k] = v.first_pixel[k] + 0.5f * U[k] + 0.5f * V[k] - c.pos[k];
+  }
+  const float fl = std::sqrt(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
+  for (int k = 0; k < 3; ++k) c.fwd[k] = f[k] / fl;
+  const float fl2 = c.fwd[0] * c.fwd[0] + c.fwd[1] * c.fwd[1] + c.fwd[2] * c.fwd[2];
+  c.fwdValid = fl2 >= 1e-6f;
+  // camera up: opposite of the viewport's v axis (rows run downwards)
+  float up[3] = {-V[0], -V[1], -V[2]};
+  float ul2 = up[0] * up[0] + up[1] * up[1] + up[2] * up[2];
+  if (ul2 < 1e-6f) {
+    up[0] = 0.0f; up[1] = 1.0f; up[2] = 0.0f;
+    ul2 = 1.0f;
+  }
+  const float ul = std::sqrt(ul2);
+  for (int k = 0; k < 3; ++k) up[k] /= ul;
+  float r[3] = {c.fwd[1] * up[2] - c.fwd[2] * up[1], c.fwd[2] * up[0] - c.fwd[0] * up[2],
+                c.fwd[0] * up[1] - c.fwd[1] * up[0]};
+  float rl2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+  if (rl2 < 1e-6f) {
+    r[0] = 1.0f; r[1] = 0.0f; r[2] = 0.0f;
+    rl2 = 1.0f;
+  }
+  const float rl = std::sqrt(rl2);
+  for (int k = 0; k < 3; ++k) c.right[k] = r[k] / rl;
+  float u2[3] = {c.right[1] * c.fwd[2] - c.right[2] * c.fwd[1], c.right[2] * c.fwd[0] - c.right[0] * c.fwd[2],
+                 c.right[0] * c.fwd[1] - c.right[1] * c.fwd[0]};
+  const float u2l = std::sqrt(u2[0] * u2[0] + u2[1] * u2[1] + u2[2] * u2[2]);
+  for (int k = 0; k < 3; ++k) c.up[k] = u2[k] / u2l;
+  // vertical half angle from the viewport height at unit distance; aspect from the pixel counts
+  const float vl = std::sqrt(V[0] * V[0] + V[1] * V[1] + V[2] * V[2]);
+  c.halfV = std::atan(0.5f * vl / fl);
+  if (c.halfV <= 0.0f) c.halfV = 1e-3f;
+  const float aspect = v.height > 0 ? (float)v.width / (float)v.height : 1.0f;
+  c.halfH = std::atan(std::tan(c.halfV) * aspect);
+  return c;
+}
+
+bool in_view(const AngleCam &c, const float *sph) {
+  const float tx = sph[0] - c.pos[0], ty = sph[1] - c.pos[1], tz = sph[2] - c.pos[2];
+  const float dist = std::sqrt(tx * tx + ty * ty + tz * tz);
+  if (dist < 1e-5f) return true;
+  if (!c.fwdValid) return true;
+  const float dx = tx / dist, dy = ty / dist, dz = tz / dist;
+  const float fd = dx * c.fwd[0] + dy * c.fwd[1] + dz * c.fwd[2];
+  if (fd <= 0.0f) return false;
+  const float ra = std::asin(std::min(sph[3] / dist, 1.0f));
+  const float h = std::atan2(std::fabs(dx * c.right[0] + dy * c.right[1] + dz * c.right[2]), fd);
+  const float vv = std::atan2(std::fabs(dx * c.up[0] + dy * c.up[1] + dz * c.up[2]), fd);
+  return h <= c.halfH + ra && vv <= c.halfV + ra;
+}
+
+float sanitize(float v) {
+  const float fmax = std::numeric_limits<float>::max();
+  if (std::isnan(v)) return -fmax;
+  if (v >= fmax) return fmax;
+  if (v <= -fmax) return -fmax;
+  return v;
+}
+
+// updateRayHitBudget per primitive (RendererResidency.cpp:2755-2964) with the cooldown decrement
+// of updateResidency (:205-207) and the counter pass of processRayHitCounters.
+nomad_status rayhit_prim_step(nomad_ctx *ctx, const nomad_residency_params *prm, const nomad_view &view,
+                              uint32_t *toggled) {
+  auto &R = ctx->res;
+  const uint32_t P = ctx->primCount;
+  if (!toggled) return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "the per-primitive policy runs synchronously");
+  nomad_status hs = nomad_residency_sync_host(ctx);
+  if (hs != NOMAD_OK) return hs;
+  if (!R.primHitsOn) {
+    NOMAD_CUDA(ctx, R.primHits.reserve((size_t)P * 4));
+    NOMAD_CUDA(ctx, cudaMemsetAsync(R.primHits.p, 0, (size_t)P * 4, ctx->stream));
+    R.primHitsHost.assign(P, 0);
+    R.primCooldown.assign(P, 0);
+    R.primScore.assign(P, 0.0f);
+    R.primVisible.assign(P, 0);
+    prim_spheres(ctx, R.primSphere);
+    R.primRebuild = 0;
+    R.primHitsOn = true;
+    ctx->frame.clearGraphs();  // the shading kernel now also counts per primitive
+  }
+  // counters -> decayed scores
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(R.primHitsHost.data(), R.primHits.p, (size_t)P * 4, cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+  NOMAD_CUDA(ctx, cudaMemsetAsync(R.primHits.p, 0, (size_t)P * 4, ctx->stream));
+  NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (uint32_t i = 0; i < P; ++i) R.primScore[i] = R.primScore[i] * prm->hit_decay + (float)R.primHitsHost[i];
+  for (uint32_t &c : R.primCooldown)
+    if (c > 0) --c;
+  *toggled = 0;
+  if (R.primRebuild > 0) {
+    --R.primRebuild;
+    return NOMAD_OK;
+  }
+  const float motion = clamp_unit(prm->camera_motion), pressure = clamp_unit(prm->memory_pressure);
+  const float frac = std::min(std::max(prm->target_fraction + 0.10f * motion - 0.24f * pressure, 0.34f), 0.92f);
+  const bool unlimited = prm->max_toggles == 0;
+  const size_t budget = std::max<size_t>(
+      1, (size_t)std::llround((double)std::max<uint32_t>(prm->max_toggles, 1) *
+                              (1.0 + 0.45 * (double)motion + 0.60 * (double)pressure)));
+  const AngleCam cam = angle_cam(view);
+  const float keep = 0.5f + (0.2f - 0.5f) * pressure;  // lerpFloat(0.5, 0.2, pressure)
+  std::vector<float> adj(P);
+  for (uint32_t i = 0; i < P; ++i) {
+    const bool vis = in_view(cam, R.primSphere.data() + 4ull * i);
+    R.primVisible[i] = vis ? 1 : 0;
+    float sc = R.primScore[i];
+    if (!vis) {
+      if (R.primHitsHost[i] == 0) sc = 0.0f;
+      else sc *= keep;
+    } else if (sc <= 0.0f) {
+      sc = 1.0f;
+    }
+    adj[i] = sanitize(sc);
+  }
+  const size_t minActive = std::min<size_t>(P, prm->min_active);
+  size_t target = (size_t)std::ceil((float)P * frac);
+  target = std::min<size_t>(std::max(target, minActive), P);
+  // every index in (score desc, index asc) order: the reference's partial_sort prefix, extended
+  // with the same order past it
+  std::vector<uint32_t> order(P);
+  for (uint32_t i = 0; i < P; ++i) order[i] = i;
+  std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+    if (adj[a] == adj[b]) return a < b;
+    return adj[a] > adj[b];
+  });
+  std::vector<uint8_t> desired(P, 0);
+  for (size_t k = 0; k < target; ++k) desired[order[k]] = 1;
+  const size_t reserve = std::min<size_t>(P, (size_t)std::ceil((float)P * (0.02f + 0.06f * motion)));
+  size_t promoted = 0;
+  for (uint32_t idx : order) {
+    if (promoted >= reserve) break;
+    if (!R.primVisible[idx]) continue;
+    desired[idx] = 1;
+    ++promoted;
+  }
+  for (size_t k = 0; k < minActive; ++k) desired[order[k]] = 1;
+  uint32_t toggles = 0;
+  for (uint32_t i = 0; i < P; ++i) {
+    const bool want = desired[i] != 0;
+    if (want == (ctx->primActive[i] != 0)) continue;
+    if (!unlimited) {
+      if (R.primCooldown[i] > 0) continue;
+      if (toggles >= budget) break;
+    }
+    int32_t changed = 0;
+    nomad_status st = nomad_residency_set_primitive_active(ctx, i, want ? 1 : 0, &changed);
+    if (st != NOMAD_OK) return st;
+    if (changed) {
+      R.primCooldown[i] = prm->state_cooldown;
+      ++toggles;
+    }
+  }
+  bool any = false;
+  for (uint32_t i = 0; i < P && !any; ++i) any = ctx->primActive[i] != 0;
+  if (!any && P > 0) {
+    int32_t changed = 0;
+    nomad_status st = nomad_residency_set_primitive_active(ctx, order[0], 1, &changed);
+    if (st != NOMAD_OK) return st;
+    if (changed) {
+      R.primCooldown[order[0]] = prm->state_cooldown;
+      ++toggles;
+    }
+  }
+  if (toggles) {
+    R.primRebuild = prm->rebuild_cooldown;
+    nomad_status st = nomad_residency_flush(ctx);
+    if (st != NOMAD_OK) return st;
+  }
+  *toggled = toggles;
+  return NOMAD_OK;
+}
+
+}  // namespace
+
+extern "C" nomad_status nomad_residency_prim_state(nomad_ctx *ctx, uint32_t *hits, float *scores, uint32_t *cooldowns,
+                                                   uint8_t *visible, uint8_t *active) {
+  if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
+  auto &R = ctx->res;
+  if (!R.primHitsOn) return nomad_fail(ctx, NOMAD_ERR_NOT_READY, "the per-primitive policy has not run");
+  const size_t P = ctx->primCount;
+  if (hits) {
+    NOMAD_CUDA(ctx, cudaMemcpyAsync(hits, R.primHits.p, P * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  if (scores) std::memcpy(scores, R.primScore.data(), P * 4);
+  if (cooldowns) std::memcpy(cooldowns, R.primCooldown.data(), P * 4);
+  if (visible) std::memcpy(visible, R.primVisible.data(), P);
+  if (active) {
+    nomad_status hs = nomad_residency_sync_host(ctx);
+    if (hs != NOMAD_OK) return hs;
+    std::memcpy(active, ctx->primActive.data(), P);
+  }
+  return NOMAD_OK;
+}
+
 extern "C" nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residency_params *prm,
                                              const nomad_view *camera, uint32_t *toggled) {
   if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
   if (!ctx->sceneReady || !ctx->res.ready) return nomad_fail(ctx, NOMAD_ERR_NOT_READY, "no scene uploaded");
   if (!prm || !camera) return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "null parameters or camera");
+  if (prm->policy == NOMAD_POLICY_RAYHIT_PRIM) {
+    NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+    return rayhit_prim_step(ctx, prm, *camera, toggled);
+  }
   if (prm->policy > NOMAD_POLICY_LEARNED) return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "unknown policy");
   const uint32_t N = ctx->objectCount;
   if (N > kMaxSelectObjects)

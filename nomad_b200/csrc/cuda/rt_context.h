@@ -140,6 +140,15 @@ struct nomad_ctx {
     float prevCam[3] = {0, 0, 0};
     bool havePrevCam = false;
     std::vector<uint64_t> hostBytes;
+    // per-primitive ray-hit policy (NOMAD_POLICY_RAYHIT_PRIM): device hit counters (counted by the
+    // path tracer once enabled) and the host-side state of the reference's policy
+    bool primHitsOn = false;
+    DeviceBuf primHits;
+    std::vector<uint32_t> primHitsHost, primCooldown;
+    std::vector<float> primScore;
+    std::vector<float> primSphere;  // centre xyz, radius per primitive
+    std::vector<uint8_t> primVisible;
+    uint32_t primRebuild = 0;
   } res;
   void *mlp = nullptr;  // MlpState (mlp.cu)
   // Geometry paging (paging.cu): the paged node layout's width (0 = off) and its state.

@@ -139,6 +139,7 @@ SIGNATURES = {
     "nomad_object_bytes": (C.c_int32, [_P, _P]),
     "nomad_residency_last": (C.c_int32, [_P, _P, _P]),
     "nomad_residency_flags": (C.c_int32, [_P, _P]),
+    "nomad_residency_prim_state": (C.c_int32, [_P, _P, _P, _P, _P, _P]),
     "nomad_mlp_init": (C.c_int32, [_P, C.c_uint64]),
     "nomad_mlp_train": (C.c_int32, [_P, _P, _P, C.c_uint64, C.c_uint32, C.c_uint32, C.c_float,
                                     C.c_float, C.c_uint64, _P]),
@@ -192,7 +193,7 @@ class RestirConfig(C.Structure):
     _fields_ = [("candidates", C.c_uint32), ("temporal", C.c_uint32), ("spatial", C.c_uint32),
                 ("radius_px", C.c_float), ("m_cap", C.c_float), ("reference_mode", C.c_uint32)]
 
-POLICY_ALWAYS, POLICY_RAYHIT_BUDGET, POLICY_LEARNED = 0, 1, 2
+POLICY_ALWAYS, POLICY_RAYHIT_BUDGET, POLICY_LEARNED, POLICY_RAYHIT_PRIM = 0, 1, 2, 3
 N_FEATURES = 24
 MLP_PARAMS = 128 * 32 + 128 + 128 * 128 + 128 + 128 + 1 + 2 * N_FEATURES
 
@@ -201,13 +202,16 @@ class ResidencyParams(C.Structure):
     _fields_ = [("policy", C.c_uint32), ("max_toggles", C.c_uint32), ("budget_bytes", C.c_uint64),
                 ("hit_decay", C.c_float), ("camera_motion", C.c_float),
                 ("memory_pressure", C.c_float), ("reserve_base", C.c_float),
-                ("reserve_motion", C.c_float), ("min_active", C.c_uint32)]
+                ("reserve_motion", C.c_float), ("min_active", C.c_uint32), ("target_fraction", C.c_float),
+                ("rebuild_cooldown", C.c_uint32), ("state_cooldown", C.c_uint32)]
 
     @staticmethod
     def make(policy, budget_bytes=0, max_toggles=0, hit_decay=0.85, camera_motion=0.0,
-             memory_pressure=0.0, reserve_base=0.02, reserve_motion=0.06, min_active=0):
+             memory_pressure=0.0, reserve_base=0.02, reserve_motion=0.06, min_active=0,
+             target_fraction=0.54, rebuild_cooldown=4, state_cooldown=5):
         return ResidencyParams(policy, max_toggles, budget_bytes, hit_decay, camera_motion,
-                               memory_pressure, reserve_base, reserve_motion, min_active)
+                               memory_pressure, reserve_base, reserve_motion, min_active, target_fraction,
+                               rebuild_cooldown, state_cooldown)
 
 VIEW_DTYPE = np.dtype([("camera_pos", "<f4", 3), ("viewport_u", "<f4", 3), ("viewport_v", "<f4", 3),
                        ("first_pixel", "<f4", 3), ("width", "<u4"), ("height", "<u4"), ("spp", "<u4"),
@@ -672,6 +676,17 @@ class Context:
         s = np.zeros(self.object_count, np.float32)
         self._ck(self.lib.nomad_residency_last(self.h, _ptr(f), _ptr(s)))
         return f, s
+
+    def residency_prim_state(self):
+        """(hits since the last step, decayed scores, cooldowns, frustum test of the last step,
+        activity) per primitive."""
+        h = np.zeros(self.prim_count, np.uint32)
+        sc = np.zeros(self.prim_count, np.float32)
+        cd = np.zeros(self.prim_count, np.uint32)
+        vis = np.zeros(self.prim_count, np.uint8)
+        act = np.zeros(self.prim_count, np.uint8)
+        self._ck(self.lib.nomad_residency_prim_state(self.h, _ptr(h), _ptr(sc), _ptr(cd), _ptr(vis), _ptr(act)))
+        return h, sc, cd, vis, act
 
     def residency_flags(self) -> np.ndarray:
         out = np.zeros(self.object_count, np.uint8)

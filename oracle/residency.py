@@ -101,3 +101,118 @@ def mlp_forward(blob, feats):
     h1 = _bf16(np.maximum(x @ w1.T + b1, 0.0).astype(np.float32)).astype(np.float64)
     h2 = np.maximum(h1 @ w2.T + b2, 0.0)
     return h2 @ w3 + b3
+
+
+class RayHitPrimOracle:
+    """updateRayHitBudget per primitive (RendererResidency.cpp:2755-2964) with the per-frame
+    cooldown decrement (:205-207) and the score pass of processRayHitCounters, restated in numpy
+    float32. The frustum test is checked separately (in_view_f64) and taken as given here."""
+
+    def __init__(self, prim_count, active=None):
+        self.n = prim_count
+        self.score = np.zeros(prim_count, np.float32)
+        self.cooldown = np.zeros(prim_count, np.uint32)
+        self.active = np.ones(prim_count, np.uint8) if active is None else active.astype(np.uint8).copy()
+        self.rebuild = 0
+
+    def step(self, hits, visible, decay=0.85, motion=0.0, pressure=0.0, target_fraction=0.54, max_toggles=16,
+             min_active=16, rebuild_cooldown=4, state_cooldown=5):
+        f32 = np.float32
+        n = self.n
+        self.score = (self.score * f32(decay) + hits.astype(f32)).astype(f32)
+        self.cooldown = np.where(self.cooldown > 0, self.cooldown - 1, 0).astype(np.uint32)
+        self.ran = self.rebuild == 0
+        if self.rebuild > 0:
+            self.rebuild -= 1
+            return 0
+        m = f32(min(max(motion, 0.0), 1.0))
+        p = f32(min(max(pressure, 0.0), 1.0))
+        frac = f32(min(max(f32(target_fraction) + f32(0.10) * m - f32(0.24) * p, f32(0.34)), f32(0.92)))
+        unlimited = max_toggles == 0
+        budget = max(1, int(np.floor(float(max(max_toggles, 1)) * (1.0 + 0.45 * float(m) + 0.60 * float(p)) + 0.5)))
+        keep = f32(0.5) + (f32(0.2) - f32(0.5)) * p
+        vis = visible.astype(bool)
+        adj = self.score.copy()
+        adj[~vis & (hits == 0)] = f32(0.0)
+        sel = ~vis & (hits != 0)
+        adj[sel] = (adj[sel] * keep).astype(f32)
+        adj[vis & (adj <= 0)] = f32(1.0)
+        big = np.finfo(np.float32).max
+        adj = np.where(np.isnan(adj), -big, np.clip(adj, -big, big)).astype(f32)
+        order = np.lexsort((np.arange(n), -adj.astype(np.float64)))
+        min_active_n = min(n, min_active)
+        target = int(np.ceil(f32(n) * frac))
+        target = min(max(target, min_active_n), n)
+        desired = np.zeros(n, bool)
+        desired[order[:target]] = True
+        reserve = min(n, int(np.ceil(f32(n) * (f32(0.02) + f32(0.06) * m))))
+        vis_order = order[vis[order]][:reserve]
+        desired[vis_order] = True
+        desired[order[:min_active_n]] = True
+        toggles = 0
+        for i in np.nonzero(desired != self.active.astype(bool))[0]:
+            if not unlimited:
+                if self.cooldown[i] > 0:
+                    continue
+                if toggles >= budget:
+                    break
+            self.active[i] = 1 if desired[i] else 0
+            self.cooldown[i] = state_cooldown
+            toggles += 1
+        if not self.active.any() and n > 0:
+            self.active[order[0]] = 1
+            self.cooldown[order[0]] = state_cooldown
+            toggles += 1
+        if toggles:
+            self.rebuild = rebuild_cooldown
+        return toggles
+
+
+def in_view_f64(spheres, view):
+    """Renderer::isInView (Renderer.cpp:1765-1817) in float64 with the view's camera; returns the
+    test and each sphere's margin (radians) from the decision boundary."""
+    v = np.asarray(view).reshape(-1)[0]
+    pos = v["camera_pos"].astype(np.float64)
+    U, V = v["viewport_u"].astype(np.float64), v["viewport_v"].astype(np.float64)
+    f = v["first_pixel"].astype(np.float64) + 0.5 * U + 0.5 * V - pos
+    fl = np.linalg.norm(f)
+    fwd = f / fl
+    up = -V / np.linalg.norm(V)
+    right = np.cross(fwd, up)
+    right /= np.linalg.norm(right)
+    up = np.cross(right, fwd)
+    up /= np.linalg.norm(up)
+    half_v = np.arctan(0.5 * np.linalg.norm(V) / fl)
+    half_h = np.arctan(np.tan(half_v) * float(v["width"]) / float(v["height"]))
+    c = spheres[:, :3].astype(np.float64) - pos
+    dist = np.linalg.norm(c, axis=1)
+    d = c / np.maximum(dist, 1e-30)[:, None]
+    fd = d @ fwd
+    ra = np.arcsin(np.minimum(spheres[:, 3] / np.maximum(dist, 1e-30), 1.0))
+    h = np.arctan2(np.abs(d @ right), fd)
+    vv = np.arctan2(np.abs(d @ up), fd)
+    margin = np.minimum(half_h + ra - h, half_v + ra - vv)
+    vis = (fd > 0) & (margin >= 0)
+    vis |= dist < 1e-5
+    margin = np.where(fd > 0, margin, np.abs(fd))
+    return vis, np.abs(margin)
+
+
+def prim_spheres(prims):
+    """Renderer.cpp:3158-3173: spheres as they are; triangles around the centroid, radius the
+    farthest vertex; rectangles around the centre, radius |u| + |v| (float64)."""
+    g = prims.reshape(-1, 28).astype(np.float64)
+    t = g[:, 3].astype(np.int32)
+    out = np.zeros((g.shape[0], 4))
+    v0, v1, v2 = g[:, 0:3], g[:, 4:7], g[:, 8:11]
+    c = (v0 + v1 + v2) / 3.0
+    r = np.maximum(np.maximum(np.linalg.norm(v0 - c, axis=1), np.linalg.norm(v1 - c, axis=1)),
+                   np.linalg.norm(v2 - c, axis=1))
+    tri = t == 1
+    out[tri, :3], out[tri, 3] = c[tri], r[tri]
+    sph = t == 0
+    out[sph, :3], out[sph, 3] = v0[sph], g[sph, 4]
+    rect = t == 2
+    out[rect, :3] = v0[rect]
+    out[rect, 3] = np.linalg.norm(v1[rect], axis=1) + np.linalg.norm(v2[rect], axis=1)
+    return out

@@ -157,3 +157,55 @@ def test_residency_step_many_objects(nb, orc, ctx, policy):
             assert toggles == want_t
             flags = got
     assert ctx.status() == 0
+
+
+@pytest.mark.parametrize("max_toggles", [16, 0])
+def test_rayhit_per_primitive_policy(nb, ctx, small_city, max_toggles):
+    """The reference's per-primitive ray-hit budget (NOMAD_POLICY_RAYHIT_PRIM) against the numpy
+    restatement frame by frame: decayed scores bit for bit, the same primitives toggled (budget,
+    cooldowns, rebuild cooldown), the frustum test equal to a float64 restatement except within
+    1e-4 rad of its boundary, and traversal after the toggles equal to the same activity set by hand."""
+    from oracle import residency as ores
+
+    _, sb = small_city
+    ctx.upload(sb)
+    prm = nb.ResidencyParams.make(nb.POLICY_RAYHIT_PRIM, max_toggles=max_toggles, camera_motion=0.3,
+                                  memory_pressure=0.2, min_active=16, target_fraction=0.54)
+    view0 = nb.view_pinhole((0, 60, -180), (0, 0, 0), width=96, height=54, spp=2, max_depth=2, seed=1)
+    ctx.residency_step(prm, view0)  # enables per-primitive counting (no hits yet)
+    _, sc0, cd0, _, act0 = ctx.residency_prim_state()
+    orc = ores.RayHitPrimOracle(sb.prim_count, act0)
+    orc.score, orc.cooldown = sc0.copy(), cd0.copy()
+    orc.rebuild = 0 if (act0 == 1).all() else 4
+    spheres = ores.prim_spheres(sb.prims)
+    for frame in range(8):
+        ang = 0.25 * frame
+        view = nb.view_pinhole((180 * np.sin(ang), 60, -180 * np.cos(ang)), (0, 0, 0), width=96, height=54,
+                               spp=2, max_depth=2, seed=frame + 2)
+        ctx.render(view, count_hits=True)
+        hits, _, _, _, _ = ctx.residency_prim_state()
+        assert hits.sum() > 0
+        toggled = ctx.residency_step(prm, view)
+        _, sc, cd, vis, act = ctx.residency_prim_state()
+        want_toggles = orc.step(hits, vis, decay=0.85, motion=0.3, pressure=0.2, target_fraction=0.54,
+                                max_toggles=max_toggles, min_active=16)
+        assert np.array_equal(sc.view(np.uint32), orc.score.view(np.uint32)), frame
+        assert toggled == want_toggles, (frame, toggled, want_toggles)
+        assert np.array_equal(act, orc.active), frame
+        assert np.array_equal(cd, orc.cooldown), frame
+        if orc.ran:
+            v64, margin = ores.in_view_f64(spheres, view)
+            assert ((vis.astype(bool) == v64) | (margin < 1e-4)).all(), frame
+    # traversal with the policy's activity equals the same activity set primitive by primitive
+    rays = raysets.aimed_rays(sb, 4000, 3)
+    got = ctx.trace_closest(rays)
+    c2 = nb.Context(0)
+    try:
+        c2.upload(sb)
+        for p in np.nonzero(act == 0)[0]:
+            c2.set_primitive_active(int(p), False)
+        c2.flush()
+        want = c2.trace_closest(rays)
+    finally:
+        c2.close()
+    assert np.array_equal(np.ascontiguousarray(got).view(np.int32), np.ascontiguousarray(want).view(np.int32))
