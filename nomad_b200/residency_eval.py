@@ -130,7 +130,7 @@ class Workload:
         return ctx.mlp_train(x, t, steps=steps, batch=batch, lr=lr, weight_decay=1e-4, seed=seed)
 
     # ---- evaluation ------------------------------------------------------------------------
-    def evaluate(self, ctx, judge, policy, path_seed=1, frames=None, warm=5, budget_fraction=None):
+    def evaluate(self, ctx, judge, policy, path_seed=1, frames=None, warm=5, budget_fraction=None, prm=None):
         """Runs the camera path with one policy; returns per-frame rel-MSE and timings."""
         import torch
 
@@ -138,8 +138,9 @@ class Workload:
         views = self.views(path_seed, frames)
         nbytes = ctx.object_bytes()
         budget = int((budget_fraction or self.budget_fraction) * nbytes.sum())
-        prm = nat.ResidencyParams.make(policy, budget_bytes=budget if policy != nat.POLICY_ALWAYS else 0,
-                                       camera_motion=0.3, min_active=0)
+        if prm is None:
+            prm = nat.ResidencyParams.make(policy, budget_bytes=budget if policy != nat.POLICY_ALWAYS else 0,
+                                           camera_motion=0.3, min_active=0)
         # start from everything resident, as the reference's AlwaysResident warm-up does
         ctx.residency_step(nat.ResidencyParams.make(nat.POLICY_ALWAYS), views[0])
         ctx.reset_object_hits()
@@ -154,7 +155,7 @@ class Workload:
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             ctx.render_dev(v, d_img.data_ptr(), count_hits=True)
-            ctx.residency_step(prm, v, toggles=False)
+            ctx.residency_step(prm, v, toggles=prm.policy == nat.POLICY_RAYHIT_PRIM)
             ctx.sync()
             dt = time.perf_counter() - t0
             num = torch.mean((d_img - d_ref) ** 2).item()
@@ -277,6 +278,17 @@ def run(paths=200, frames_per_path=8, steps=1500, frames=300, log=print):
         except nat.NomadError as exc:  # a traversal width the paging cannot hold
             out[name] = {"error": str(exc)}
         log(f"{name}: {out[name]}")
+    # The reference's own per-primitive ray-hit policy (host, per primitive, its defaults: 54 %
+    # of the primitives, 16 toggles a frame, cooldowns), on a fresh context and a shorter path.
+    pc = w.context()
+    try:
+        pc.set_traversal(**ctx.traversal())
+        out["ray_hit_per_primitive_reference"] = w.evaluate(
+            pc, judge, nat.POLICY_RAYHIT_PRIM, frames=min(frames, 100),
+            prm=nat.ResidencyParams.make(nat.POLICY_RAYHIT_PRIM, max_toggles=16, camera_motion=0.3, min_active=16))
+    finally:
+        pc.close()
+    log(f"ray_hit_per_primitive_reference: {out['ray_hit_per_primitive_reference']}")
     # The learned policy at smaller budgets: the smallest one whose rel-MSE is within 5 % of the
     # ray-hit policy's at the full budget, and its ms/frame.
     sweep = {}
