@@ -296,7 +296,8 @@ enum {
   NOMAD_POLICY_ALWAYS = 0,        /* every object resident (the image judge)                  */
   NOMAD_POLICY_RAYHIT_BUDGET = 1, /* decayed per-object closest-hit score (the fallback)       */
   NOMAD_POLICY_LEARNED = 2,       /* BF16 MLP score over NOMAD_FEATURES per-object features    */
-  NOMAD_POLICY_RAYHIT_PRIM = 3    /* the reference's per-primitive ray-hit budget (see below)    */
+  NOMAD_POLICY_RAYHIT_PRIM = 3,   /* the reference's per-primitive ray-hit budget (see below)    */
+  NOMAD_POLICY_DISTANCE_LOD = 4   /* the reference's DistanceLOD heuristic (see below)           */
 };
 #define NOMAD_FEATURES 24
 
@@ -316,6 +317,11 @@ typedef struct nomad_residency_params {
   float target_fraction;    /* primitives kept = ceil(N * clamp(f + 0.1 motion - 0.24 pressure, 0.34, 0.92)) */
   uint32_t rebuild_cooldown;/* steps skipped after a step that changed residency              */
   uint32_t state_cooldown;  /* steps a toggled primitive stays as it is                       */
+  /* NOMAD_POLICY_DISTANCE_LOD only (lodEnterDistance 225, lodExitDistance 275,
+   * lodEnterViewDegrees 5, lodExitViewDegrees 12; max_toggles is lodMaxTogglesPerFrame, 24;
+   * state_cooldown is the object cooldown): */
+  float lod_enter_distance, lod_exit_distance;
+  float lod_enter_view_degrees, lod_exit_view_degrees;
 } nomad_residency_params;
 
 /* One residency step, all on the device: consumes the per-object closest-hit counts gathered
@@ -342,6 +348,19 @@ nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residency_params *
  * max(1, round(max_toggles * (1 + 0.45 motion + 0.6 pressure))). It runs on the host over the
  * device's counters and applies its toggles with nomad_residency_set_primitive_active and
  * nomad_residency_flush (toggled != NULL is required). */
+/* NOMAD_POLICY_DISTANCE_LOD restates updateLODByDistance (RendererResidency.cpp:759-964): each
+ * object's bounding sphere (centre and half diagonal of its BLAS root box, Renderer.cpp:3272-3278)
+ * gives a distance (to the sphere, 0 inside, none behind the camera) and an angular frustum test
+ * with an entry and a wider exit margin; objects are visited nearest first and an inactive one is
+ * activated closer than lod_enter_distance inside the entry frustum, an active one kept up to
+ * lod_exit_distance inside the exit frustum, objects in their cooldown skipped, at most
+ * max(1, round(max_toggles * (1 + 0.4 motion + 0.6 pressure))) toggles. Host-side like the
+ * reference, applied with nomad_residency_set_object_active + nomad_residency_flush (toggled
+ * != NULL is required). */
+/* The DistanceLOD state after its last step, per object (any may be NULL): distance (float,
+ * FLT_MAX behind the camera), flags (uint8: 1 entry frustum, 2 exit frustum, 4 behind) and
+ * cooldowns (uint32). */
+nomad_status nomad_residency_object_state(nomad_ctx *ctx, float *distance, uint8_t *flags, uint32_t *cooldowns);
 /* Per-primitive closest hits counted since the last step (prim_count uint32), and the
  * per-primitive policy's state after its last step: decayed scores (float), cooldowns (uint32),
  * the frustum test of that step (uint8, isInView, Renderer.cpp:1765-1817), and every primitive's

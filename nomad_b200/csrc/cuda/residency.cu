@@ -780,7 +780,137 @@ nomad_status rayhit_prim_step(nomad_ctx *ctx, const nomad_residency_params *prm,
   return NOMAD_OK;
 }
 
+// Bounding sphere of object o from its BLAS root box (Renderer.cpp:3272-3278: centre of the box,
+// radius to its max corner); false for an object without primitives.
+bool object_sphere(const nomad_ctx *ctx, uint32_t o, float *sph) {
+  const nomad::TraversalLayout &L = ctx->layout;
+  const float *mn, *mx;
+  const int64_t slot = L.objSlot[o];
+  if (slot >= 0) {
+    const float *p = L.pnodes.data() + 16ull * (uint64_t)(slot / 2);
+    mn = (slot & 1) ? p + 8 : p;
+    mx = (slot & 1) ? p + 12 : p + 4;
+  } else if (slot == -1) {
+    mn = L.rootMin;
+    mx = L.rootMax;
+  } else {
+    return false;
+  }
+  float c[3];
+  for (int k = 0; k < 3; ++k) c[k] = (mn[k] + mx[k]) * 0.5f;
+  const float dx = mx[0] - c[0], dy = mx[1] - c[1], dz = mx[2] - c[2];
+  sph[0] = c[0];
+  sph[1] = c[1];
+  sph[2] = c[2];
+  sph[3] = std::sqrt(dx * dx + dy * dy + dz * dz);
+  return true;
+}
+
+// updateLODByDistance (RendererResidency.cpp:759-964) with the per-frame cooldown decrement of
+// updateResidency (:208-210) and setObjectActive's cooldown (:1025).
+nomad_status distance_lod_step(nomad_ctx *ctx, const nomad_residency_params *prm, const nomad_view &view,
+                               uint32_t *toggled) {
+  auto &R = ctx->res;
+  const uint32_t N = ctx->objectCount;
+  if (!toggled) return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "the DistanceLOD policy runs synchronously");
+  nomad_status hs = nomad_residency_sync_host(ctx);
+  if (hs != NOMAD_OK) return hs;
+  if (!R.lodOn) {
+    R.objCooldown.assign(N, 0);
+    R.lodDist.assign(N, 0.0f);
+    R.lodFlags.assign(N, 0);
+    R.lodOn = true;
+  }
+  for (uint32_t &c : R.objCooldown)
+    if (c > 0) --c;
+  const float motion = clamp_unit(prm->camera_motion), pressure = clamp_unit(prm->memory_pressure);
+  const size_t budget = std::max<size_t>(
+      1, (size_t)std::llround((double)std::max<uint32_t>(prm->max_toggles, 1) *
+                              (1.0 + 0.40 * (double)motion + 0.60 * (double)pressure)));
+  const AngleCam cam = angle_cam(view);
+  constexpr float kDegToRad = 0.0174532925199432957692f;
+  const float enterMargin = std::max(prm->lod_enter_view_degrees, 0.0f) * kDegToRad;
+  const float exitMargin = std::max(std::max(prm->lod_exit_view_degrees, 0.0f) * kDegToRad, enterMargin);
+  const float fmax = std::numeric_limits<float>::max();
+  std::vector<uint32_t> order(N);
+  for (uint32_t o = 0; o < N; ++o) {
+    order[o] = o;
+    float sph[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    object_sphere(ctx, o, sph);
+    const float tx = sph[0] - cam.pos[0], ty = sph[1] - cam.pos[1], tz = sph[2] - cam.pos[2];
+    const float dtc = std::sqrt(tx * tx + ty * ty + tz * tz);
+    const float dist = dtc - sph[3];
+    const float fd = cam.fwdValid ? tx * cam.fwd[0] + ty * cam.fwd[1] + tz * cam.fwd[2] : 0.0f;
+    const bool behind = cam.fwdValid && fd + sph[3] <= 0.0f;
+    R.lodDist[o] = behind ? fmax : std::max(dist, 0.0f);
+    bool enter = true, exit = true;
+    if (cam.fwdValid) {
+      if (dtc <= 1e-5f || behind) {
+        enter = exit = !behind;
+      } else {
+        const float depth = std::max(fd, 1e-5f);
+        const float horiz = tx * cam.right[0] + ty * cam.right[1] + tz * cam.right[2];
+        const float vert = tx * cam.up[0] + ty * cam.up[1] + tz * cam.up[2];
+        const float ha = std::atan2(std::fabs(horiz), depth), va = std::atan2(std::fabs(vert), depth);
+        const float ra = std::asin(std::min(sph[3] / dtc, 1.0f));
+        enter = ha <= cam.halfH + ra + enterMargin && va <= cam.halfV + ra + enterMargin;
+        exit = ha <= cam.halfH + ra + exitMargin && va <= cam.halfV + ra + exitMargin;
+      }
+    }
+    R.lodFlags[o] = (uint8_t)((enter ? 1 : 0) | (exit ? 2 : 0) | (behind ? 4 : 0));
+  }
+  // nearest first; equal distances by object index
+  std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+    if (R.lodDist[a] == R.lodDist[b]) return a < b;
+    return R.lodDist[a] < R.lodDist[b];
+  });
+  uint32_t toggles = 0;
+  for (uint32_t o : order) {
+    const nomad_instance_record &ir = ctx->instances[o];
+    const uint32_t count = ir.primitive_count, activeCount = ctx->objActiveCount[o];
+    const bool active = activeCount > 0;
+    const bool view_ok = active ? (R.lodFlags[o] & 2) != 0 : (R.lodFlags[o] & 1) != 0;
+    const bool behind = (R.lodFlags[o] & 4) != 0;
+    const float d = R.lodDist[o];
+    const bool want = view_ok && !behind && (active ? d <= prm->lod_exit_distance : d < prm->lod_enter_distance);
+    if (R.objCooldown[o] != 0 || want == active) continue;
+    const uint32_t needed = want ? count - activeCount : activeCount;
+    if (needed == 0) continue;
+    if ((size_t)toggles + 1 > budget) continue;
+    uint32_t n = 0;
+    nomad_status st = nomad_residency_set_object_active(ctx, o, want ? 1 : 0, &n);
+    if (st != NOMAD_OK) return st;
+    const bool fullyInactive = ctx->objActiveCount[o] == 0;
+    const bool nowActive = ctx->objActiveCount[o] > 0;
+    if (n > 0 || nowActive != active || fullyInactive) R.objCooldown[o] = prm->state_cooldown;
+    if (n > 0) ++toggles;
+  }
+  bool any = false;
+  for (uint32_t o = 0; o < N && !any; ++o) any = ctx->objActiveCount[o] > 0;
+  if (!any && ctx->primCount > 0) {
+    int32_t changed = 0;
+    nomad_status st = nomad_residency_set_primitive_active(ctx, 0, 1, &changed);
+    if (st != NOMAD_OK) return st;
+  }
+  nomad_status st = nomad_residency_flush(ctx);
+  if (st != NOMAD_OK) return st;
+  *toggled = toggles;
+  return NOMAD_OK;
+}
+
 }  // namespace
+
+extern "C" nomad_status nomad_residency_object_state(nomad_ctx *ctx, float *distance, uint8_t *flags,
+                                                     uint32_t *cooldowns) {
+  if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
+  auto &R = ctx->res;
+  if (!R.lodOn) return nomad_fail(ctx, NOMAD_ERR_NOT_READY, "the DistanceLOD policy has not run");
+  const size_t N = ctx->objectCount;
+  if (distance) std::memcpy(distance, R.lodDist.data(), N * 4);
+  if (flags) std::memcpy(flags, R.lodFlags.data(), N);
+  if (cooldowns) std::memcpy(cooldowns, R.objCooldown.data(), N * 4);
+  return NOMAD_OK;
+}
 
 extern "C" nomad_status nomad_residency_prim_state(nomad_ctx *ctx, uint32_t *hits, float *scores, uint32_t *cooldowns,
                                                    uint8_t *visible, uint8_t *active) {
@@ -811,6 +941,10 @@ extern "C" nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residen
   if (prm->policy == NOMAD_POLICY_RAYHIT_PRIM) {
     NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
     return rayhit_prim_step(ctx, prm, *camera, toggled);
+  }
+  if (prm->policy == NOMAD_POLICY_DISTANCE_LOD) {
+    NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+    return distance_lod_step(ctx, prm, *camera, toggled);
   }
   if (prm->policy > NOMAD_POLICY_LEARNED) return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "unknown policy");
   const uint32_t N = ctx->objectCount;

@@ -149,6 +149,11 @@ struct nomad_ctx {
     std::vector<float> primSphere;  // centre xyz, radius per primitive
     std::vector<uint8_t> primVisible;
     uint32_t primRebuild = 0;
+    // DistanceLOD policy (NOMAD_POLICY_DISTANCE_LOD): object cooldowns and the last step's tests
+    bool lodOn = false;
+    std::vector<uint32_t> objCooldown;
+    std::vector<float> lodDist;
+    std::vector<uint8_t> lodFlags;
   } res;
   void *mlp = nullptr;  // MlpState (mlp.cu)
   // Geometry paging (paging.cu): the paged node layout's width (0 = off) and its state.

@@ -140,6 +140,7 @@ SIGNATURES = {
     "nomad_residency_last": (C.c_int32, [_P, _P, _P]),
     "nomad_residency_flags": (C.c_int32, [_P, _P]),
     "nomad_residency_prim_state": (C.c_int32, [_P, _P, _P, _P, _P, _P]),
+    "nomad_residency_object_state": (C.c_int32, [_P, _P, _P, _P]),
     "nomad_mlp_init": (C.c_int32, [_P, C.c_uint64]),
     "nomad_mlp_train": (C.c_int32, [_P, _P, _P, C.c_uint64, C.c_uint32, C.c_uint32, C.c_float,
                                     C.c_float, C.c_uint64, _P]),
@@ -193,7 +194,7 @@ class RestirConfig(C.Structure):
     _fields_ = [("candidates", C.c_uint32), ("temporal", C.c_uint32), ("spatial", C.c_uint32),
                 ("radius_px", C.c_float), ("m_cap", C.c_float), ("reference_mode", C.c_uint32)]
 
-POLICY_ALWAYS, POLICY_RAYHIT_BUDGET, POLICY_LEARNED, POLICY_RAYHIT_PRIM = 0, 1, 2, 3
+POLICY_ALWAYS, POLICY_RAYHIT_BUDGET, POLICY_LEARNED, POLICY_RAYHIT_PRIM, POLICY_DISTANCE_LOD = 0, 1, 2, 3, 4
 N_FEATURES = 24
 MLP_PARAMS = 128 * 32 + 128 + 128 * 128 + 128 + 128 + 1 + 2 * N_FEATURES
 
@@ -203,15 +204,19 @@ class ResidencyParams(C.Structure):
                 ("hit_decay", C.c_float), ("camera_motion", C.c_float),
                 ("memory_pressure", C.c_float), ("reserve_base", C.c_float),
                 ("reserve_motion", C.c_float), ("min_active", C.c_uint32), ("target_fraction", C.c_float),
-                ("rebuild_cooldown", C.c_uint32), ("state_cooldown", C.c_uint32)]
+                ("rebuild_cooldown", C.c_uint32), ("state_cooldown", C.c_uint32),
+                ("lod_enter_distance", C.c_float), ("lod_exit_distance", C.c_float),
+                ("lod_enter_view_degrees", C.c_float), ("lod_exit_view_degrees", C.c_float)]
 
     @staticmethod
     def make(policy, budget_bytes=0, max_toggles=0, hit_decay=0.85, camera_motion=0.0,
              memory_pressure=0.0, reserve_base=0.02, reserve_motion=0.06, min_active=0,
-             target_fraction=0.54, rebuild_cooldown=4, state_cooldown=5):
+             target_fraction=0.54, rebuild_cooldown=4, state_cooldown=5, lod_enter_distance=225.0,
+             lod_exit_distance=275.0, lod_enter_view_degrees=5.0, lod_exit_view_degrees=12.0):
         return ResidencyParams(policy, max_toggles, budget_bytes, hit_decay, camera_motion,
                                memory_pressure, reserve_base, reserve_motion, min_active, target_fraction,
-                               rebuild_cooldown, state_cooldown)
+                               rebuild_cooldown, state_cooldown, lod_enter_distance, lod_exit_distance,
+                               lod_enter_view_degrees, lod_exit_view_degrees)
 
 VIEW_DTYPE = np.dtype([("camera_pos", "<f4", 3), ("viewport_u", "<f4", 3), ("viewport_v", "<f4", 3),
                        ("first_pixel", "<f4", 3), ("width", "<u4"), ("height", "<u4"), ("spp", "<u4"),
@@ -687,6 +692,15 @@ class Context:
         act = np.zeros(self.prim_count, np.uint8)
         self._ck(self.lib.nomad_residency_prim_state(self.h, _ptr(h), _ptr(sc), _ptr(cd), _ptr(vis), _ptr(act)))
         return h, sc, cd, vis, act
+
+    def residency_object_state(self):
+        """DistanceLOD state of the last step: (distance, flags 1 enter / 2 exit / 4 behind,
+        cooldowns) per object."""
+        d = np.zeros(self.object_count, np.float32)
+        f = np.zeros(self.object_count, np.uint8)
+        c = np.zeros(self.object_count, np.uint32)
+        self._ck(self.lib.nomad_residency_object_state(self.h, _ptr(d), _ptr(f), _ptr(c)))
+        return d, f, c
 
     def residency_flags(self) -> np.ndarray:
         out = np.zeros(self.object_count, np.uint8)

@@ -155,7 +155,7 @@ class Workload:
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             ctx.render_dev(v, d_img.data_ptr(), count_hits=True)
-            ctx.residency_step(prm, v, toggles=prm.policy == nat.POLICY_RAYHIT_PRIM)
+            ctx.residency_step(prm, v, toggles=prm.policy in (nat.POLICY_RAYHIT_PRIM, nat.POLICY_DISTANCE_LOD))
             ctx.sync()
             dt = time.perf_counter() - t0
             num = torch.mean((d_img - d_ref) ** 2).item()
@@ -289,6 +289,12 @@ def run(paths=200, frames_per_path=8, steps=1500, frames=300, log=print):
     finally:
         pc.close()
     log(f"ray_hit_per_primitive_reference: {out['ray_hit_per_primitive_reference']}")
+    # The reference's DistanceLOD heuristic with its defaults (225 / 275 m, 5 / 12 degrees, 24
+    # toggles a frame), host-side per object.
+    out["distance_lod_reference"] = w.evaluate(
+        ctx, judge, nat.POLICY_DISTANCE_LOD, frames=frames,
+        prm=nat.ResidencyParams.make(nat.POLICY_DISTANCE_LOD, max_toggles=24, camera_motion=0.3))
+    log(f"distance_lod_reference: {out['distance_lod_reference']}")
     # The learned policy at smaller budgets: the smallest one whose rel-MSE is within 5 % of the
     # ray-hit policy's at the full budget, and its ms/frame.
     sweep = {}

@@ -216,3 +216,98 @@ def prim_spheres(prims):
     out[rect, :3] = v0[rect]
     out[rect, 3] = np.linalg.norm(v1[rect], axis=1) + np.linalg.norm(v2[rect], axis=1)
     return out
+
+
+class DistanceLodOracle:
+    """updateLODByDistance (RendererResidency.cpp:759-964) restated over the per-object distance
+    and frustum flags of the step (checked separately by lod_tests_f64): nearest first (equal
+    distances by index), hysteresis between the entry and exit distances and frusta, object
+    cooldowns (:208-210, :1025), the toggle budget."""
+
+    def __init__(self, object_count, prim_counts):
+        self.n = object_count
+        self.count = prim_counts.astype(np.int64)
+        self.active_count = self.count.copy()
+        self.cooldown = np.zeros(object_count, np.uint32)
+
+    def step(self, dist, flags, motion=0.0, pressure=0.0, max_toggles=24, enter=225.0, exit_=275.0,
+             state_cooldown=5):
+        self.cooldown = np.where(self.cooldown > 0, self.cooldown - 1, 0).astype(np.uint32)
+        m, p = min(max(motion, 0.0), 1.0), min(max(pressure, 0.0), 1.0)
+        budget = max(1, int(np.floor(float(max(max_toggles, 1)) * (1.0 + 0.40 * np.float32(m) + 0.60 * np.float32(p))
+                                     + 0.5)))
+        order = np.lexsort((np.arange(self.n), dist.astype(np.float64)))
+        toggles = 0
+        for o in order:
+            active = self.active_count[o] > 0
+            view_ok = bool(flags[o] & 2) if active else bool(flags[o] & 1)
+            behind = bool(flags[o] & 4)
+            d = np.float32(dist[o])
+            want = view_ok and not behind and (d <= np.float32(exit_) if active else d < np.float32(enter))
+            if self.cooldown[o] != 0 or want == active:
+                continue
+            needed = self.count[o] - self.active_count[o] if want else self.active_count[o]
+            if needed == 0:
+                continue
+            if toggles + 1 > budget:
+                continue
+            self.active_count[o] = self.count[o] if want else 0
+            self.cooldown[o] = state_cooldown
+            toggles += 1
+        return toggles
+
+
+def lod_tests_f64(spheres, view, enter_deg=5.0, exit_deg=12.0):
+    """The per-object distance and entry/exit frustum tests of updateLODByDistance in float64;
+    returns (distance, enter, exit, behind, angular margin of the nearer frustum boundary)."""
+    v = np.asarray(view).reshape(-1)[0]
+    pos = v["camera_pos"].astype(np.float64)
+    U, V = v["viewport_u"].astype(np.float64), v["viewport_v"].astype(np.float64)
+    f = v["first_pixel"].astype(np.float64) + 0.5 * U + 0.5 * V - pos
+    fl = np.linalg.norm(f)
+    fwd = f / fl
+    up = -V / np.linalg.norm(V)
+    right = np.cross(fwd, up)
+    right /= np.linalg.norm(right)
+    up = np.cross(right, fwd)
+    up /= np.linalg.norm(up)
+    half_v = np.arctan(0.5 * np.linalg.norm(V) / fl)
+    half_h = np.arctan(np.tan(half_v) * float(v["width"]) / float(v["height"]))
+    em = np.radians(max(enter_deg, 0.0))
+    xm = max(np.radians(max(exit_deg, 0.0)), em)
+    t = spheres[:, :3] - pos
+    dtc = np.linalg.norm(t, axis=1)
+    r = spheres[:, 3]
+    fd = t @ fwd
+    behind = fd + r <= 0
+    dist = np.where(behind, np.finfo(np.float32).max, np.maximum(dtc - r, 0.0))
+    depth = np.maximum(fd, 1e-5)
+    ha = np.arctan2(np.abs(t @ right), depth)
+    va = np.arctan2(np.abs(t @ up), depth)
+    ra = np.arcsin(np.minimum(r / np.maximum(dtc, 1e-30), 1.0))
+    enter = (ha <= half_h + ra + em) & (va <= half_v + ra + em)
+    exit_ = (ha <= half_h + ra + xm) & (va <= half_v + ra + xm)
+    near = dtc <= 1e-5
+    enter = np.where(near | behind, ~behind, enter)
+    exit_ = np.where(near | behind, ~behind, exit_)
+    margin = np.minimum.reduce([np.abs(half_h + ra + em - ha), np.abs(half_v + ra + em - va),
+                                np.abs(half_h + ra + xm - ha), np.abs(half_v + ra + xm - va)])
+    margin = np.where(near | behind, np.inf, margin)
+    return dist, enter, exit_, behind, margin
+
+
+def object_spheres(sb):
+    """Each object's bounding sphere from its BLAS root box (Renderer.cpp:3272-3278), float32
+    arithmetic as the library does it."""
+    nodes = sb.bvh_nodes.reshape(-1, 8)
+    roots = sb.instances["blas_root_index"]
+    out = np.zeros((sb.object_count, 4), np.float32)
+    for o, r in enumerate(roots):
+        if r < 0:
+            continue
+        mn, mx = nodes[r, 0:3].astype(np.float32), nodes[r, 4:7].astype(np.float32)
+        c = ((mn + mx) * np.float32(0.5)).astype(np.float32)
+        d = (mx - c).astype(np.float32)
+        out[o, :3] = c
+        out[o, 3] = np.sqrt(np.float32(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]), dtype=np.float32)
+    return out

@@ -209,3 +209,49 @@ def test_rayhit_per_primitive_policy(nb, ctx, small_city, max_toggles):
     finally:
         c2.close()
     assert np.array_equal(np.ascontiguousarray(got).view(np.int32), np.ascontiguousarray(want).view(np.int32))
+
+
+def test_distance_lod_policy(nb, ctx, small_city):
+    """The reference's DistanceLOD heuristic (NOMAD_POLICY_DISTANCE_LOD) against the numpy
+    restatement over a camera fly-through: distances and frustum tests equal to a float64
+    restatement (up to float32 rounding and 1e-4 rad at the frustum boundary), the same objects
+    toggled (nearest first, hysteresis, cooldowns, toggle budget), traversal equal to the same
+    residency set by hand."""
+    from oracle import residency as ores
+
+    _, sb = small_city
+    ctx.upload(sb)
+    prm = nb.ResidencyParams.make(nb.POLICY_DISTANCE_LOD, max_toggles=6, camera_motion=0.2, memory_pressure=0.1,
+                                  lod_enter_distance=90.0, lod_exit_distance=120.0)
+    orc = ores.DistanceLodOracle(sb.object_count, sb.instances["primitive_count"])
+    spheres = ores.object_spheres(sb)
+    total = 0
+    for frame in range(10):
+        x = -120.0 + 24.0 * frame
+        view = nb.view_pinhole((x, 30, -60), (x + 10, 0, 60), width=96, height=54, spp=1, max_depth=1, seed=frame)
+        toggled = ctx.residency_step(prm, view)
+        dist, flags, cd = ctx.residency_object_state()
+        d64, en, ex, be, margin = ores.lod_tests_f64(spheres.astype(np.float64), view)
+        ok = np.abs(dist.astype(np.float64) - d64) <= 1e-3 * np.maximum(1.0, d64)
+        assert (ok | (dist == np.finfo(np.float32).max)).all(), frame
+        f64 = (en.astype(np.uint8) | (ex.astype(np.uint8) << 1) | (be.astype(np.uint8) << 2))
+        assert ((flags == f64) | (margin < 1e-4)).all(), frame
+        want = orc.step(dist, flags, motion=0.2, pressure=0.1, max_toggles=6, enter=90.0, exit_=120.0)
+        assert toggled == want, (frame, toggled, want)
+        assert np.array_equal(cd, orc.cooldown), frame
+        assert np.array_equal(ctx.residency_flags().astype(bool), orc.active_count > 0), frame
+        total += toggled
+    assert total > 0
+    rays = raysets.aimed_rays(sb, 4000, 5)
+    got = ctx.trace_closest(rays)
+    flags_obj = ctx.residency_flags()
+    c2 = nb.Context(0)
+    try:
+        c2.upload(sb)
+        for o in np.nonzero(flags_obj == 0)[0]:
+            c2.set_object_active(int(o), False)
+        c2.flush()
+        want_h = c2.trace_closest(rays)
+    finally:
+        c2.close()
+    assert np.array_equal(np.ascontiguousarray(got).view(np.int32), np.ascontiguousarray(want_h).view(np.int32))
