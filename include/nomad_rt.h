@@ -297,7 +297,8 @@ enum {
   NOMAD_POLICY_RAYHIT_BUDGET = 1, /* decayed per-object closest-hit score (the fallback)       */
   NOMAD_POLICY_LEARNED = 2,       /* BF16 MLP score over NOMAD_FEATURES per-object features    */
   NOMAD_POLICY_RAYHIT_PRIM = 3,   /* the reference's per-primitive ray-hit budget (see below)    */
-  NOMAD_POLICY_DISTANCE_LOD = 4   /* the reference's DistanceLOD heuristic (see below)           */
+  NOMAD_POLICY_DISTANCE_LOD = 4,  /* the reference's DistanceLOD heuristic (see below)           */
+  NOMAD_POLICY_SCREEN_SPACE = 5   /* the reference's ScreenSpaceFootprint heuristic (see below)  */
 };
 #define NOMAD_FEATURES 24
 
@@ -322,6 +323,10 @@ typedef struct nomad_residency_params {
    * state_cooldown is the object cooldown): */
   float lod_enter_distance, lod_exit_distance;
   float lod_enter_view_degrees, lod_exit_view_degrees;
+  /* NOMAD_POLICY_SCREEN_SPACE only (screenFootprintMinPixelCoverage 32; target_fraction is
+   * screenFootprintTargetFraction 0.68, min_active screenFootprintMinActivePrimitives 16,
+   * max_toggles screenFootprintMaxTogglesPerFrame 14, in primitives): */
+  float min_pixel_coverage;
 } nomad_residency_params;
 
 /* One residency step, all on the device: consumes the per-object closest-hit counts gathered
@@ -347,7 +352,9 @@ nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residency_params *
  * go in primitive order, skip primitives in their cooldown and stop at
  * max(1, round(max_toggles * (1 + 0.45 motion + 0.6 pressure))). It runs on the host over the
  * device's counters and applies its toggles with nomad_residency_set_primitive_active and
- * nomad_residency_flush (toggled != NULL is required). */
+ * nomad_residency_flush (toggled != NULL is required). For the host-side policies *toggled
+ * counts primitives (NOMAD_POLICY_RAYHIT_PRIM, NOMAD_POLICY_SCREEN_SPACE) or objects
+ * (NOMAD_POLICY_DISTANCE_LOD) toggled. */
 /* NOMAD_POLICY_DISTANCE_LOD restates updateLODByDistance (RendererResidency.cpp:759-964): each
  * object's bounding sphere (centre and half diagonal of its BLAS root box, Renderer.cpp:3272-3278)
  * gives a distance (to the sphere, 0 inside, none behind the camera) and an angular frustum test
@@ -357,6 +364,15 @@ nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residency_params *
  * max(1, round(max_toggles * (1 + 0.4 motion + 0.6 pressure))) toggles. Host-side like the
  * reference, applied with nomad_residency_set_object_active + nomad_residency_flush (toggled
  * != NULL is required). */
+/* NOMAD_POLICY_SCREEN_SPACE restates updateScreenSpaceFootprint (RendererResidency.cpp:4092-4396)
+ * with every object its own mesh group: each object's projected bounding-sphere area in pixels
+ * (0 outside the view, scaled by the cosine to the view axis, at most the screen), objects taken
+ * by coverage (ties to the lower index) until min_active primitives and
+ * clamp(target_fraction + 0.08 motion - 0.10 pressure, 0.5, 0.94) of the screen are covered,
+ * skipping objects under min_pixel_coverage once min_active is met; toggles in coverage order
+ * while fewer than max(1, round(max_toggles * (1 + 0.4 motion + 0.5 pressure))) primitives have
+ * been toggled, objects or primitives in their cooldown blocking. Host-side; the last step's
+ * coverage is returned by nomad_residency_object_state as `distance`. */
 /* The DistanceLOD state after its last step, per object (any may be NULL): distance (float,
  * FLT_MAX behind the camera), flags (uint8: 1 entry frustum, 2 exit frustum, 4 behind) and
  * cooldowns (uint32). */

@@ -415,6 +415,18 @@ nomad_status nomad_residency_init(nomad_ctx *ctx) {
   auto &R = ctx->res;
   const auto &L = ctx->layout;
   const uint32_t N = ctx->objectCount, P = ctx->primCount;
+  // a new scene starts the host-side policies afresh
+  R.primHitsOn = false;
+  R.primHitsHost.clear();
+  R.primCooldown.clear();
+  R.primScore.clear();
+  R.primSphere.clear();
+  R.primVisible.clear();
+  R.primRebuild = 0;
+  R.lodOn = false;
+  R.objCooldown.clear();
+  R.lodDist.clear();
+  R.lodFlags.clear();
   NOMAD_CUDA(ctx, R.objSlot.reserve((size_t)N * 8));
   NOMAD_CUDA(ctx, R.objBlasRef.reserve((size_t)N * 4));
   NOMAD_CUDA(ctx, R.objRes.reserve(N));
@@ -898,6 +910,151 @@ nomad_status distance_lod_step(nomad_ctx *ctx, const nomad_residency_params *prm
   return NOMAD_OK;
 }
 
+// updateScreenSpaceFootprint (RendererResidency.cpp:4092-4396), one mesh group per object.
+nomad_status screen_space_step(nomad_ctx *ctx, const nomad_residency_params *prm, const nomad_view &view,
+                               uint32_t *toggled) {
+  auto &R = ctx->res;
+  const uint32_t N = ctx->objectCount, P = ctx->primCount;
+  if (!toggled) return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "the ScreenSpace policy runs synchronously");
+  nomad_status hs = nomad_residency_sync_host(ctx);
+  if (hs != NOMAD_OK) return hs;
+  if (!R.lodOn) {
+    R.objCooldown.assign(N, 0);
+    R.lodDist.assign(N, 0.0f);
+    R.lodFlags.assign(N, 0);
+    R.lodOn = true;
+  }
+  if (R.primCooldown.size() != P) R.primCooldown.assign(P, 0);
+  for (uint32_t &c : R.objCooldown)
+    if (c > 0) --c;
+  for (uint32_t &c : R.primCooldown)
+    if (c > 0) --c;
+  const float motion = clamp_unit(prm->camera_motion), pressure = clamp_unit(prm->memory_pressure);
+  const float frac = std::min(std::max(prm->target_fraction + 0.08f * motion - 0.10f * pressure, 0.50f), 0.94f);
+  const size_t budget = std::max<size_t>(
+      1, (size_t)std::llround((double)std::max<uint32_t>(prm->max_toggles, 1) *
+                              (1.0 + 0.40 * (double)motion + 0.50 * (double)pressure)));
+  const float W = (float)view.width, H = (float)view.height;
+  float screenArea = W * H;
+  if (screenArea <= 0.0f) screenArea = 1.0f;
+  const AngleCam cam = angle_cam(view);
+  // objectCoverageForSphere (:4130-4182): the camera's own up, not re-orthogonalised
+  float tanHalf = std::tan(cam.halfV);
+  if (tanHalf <= 0.0f) tanHalf = 1e-3f;
+  float U[3], V[3], upRaw[3];
+  for (int k = 0; k < 3; ++k) {
+    U[k] = view.viewport_u[k];
+    V[k] = view.viewport_v[k];
+    upRaw[k] = -V[k];
+  }
+  const float ul = std::sqrt(upRaw[0] * upRaw[0] + upRaw[1] * upRaw[1] + upRaw[2] * upRaw[2]);
+  for (int k = 0; k < 3; ++k) upRaw[k] /= ul;
+  float right[3] = {cam.fwd[1] * upRaw[2] - cam.fwd[2] * upRaw[1], cam.fwd[2] * upRaw[0] - cam.fwd[0] * upRaw[2],
+                    cam.fwd[0] * upRaw[1] - cam.fwd[1] * upRaw[0]};
+  const float rl2 = right[0] * right[0] + right[1] * right[1] + right[2] * right[2];
+  if (rl2 < 1e-6f) {
+    right[0] = 1.0f; right[1] = 0.0f; right[2] = 0.0f;
+  } else {
+    const float rl = std::sqrt(rl2);
+    for (int k = 0; k < 3; ++k) right[k] /= rl;
+  }
+  const float aspect = H > 0.0f ? W / H : 1.0f;
+  const float hHalf = std::atan(tanHalf * aspect);
+  constexpr float kPi = 3.14159265358979323846f;
+  std::vector<float> cov(N, 0.0f);
+  std::vector<uint32_t> order(N);
+  for (uint32_t o = 0; o < N; ++o) {
+    order[o] = o;
+    float sph[4];
+    if (!object_sphere(ctx, o, sph)) continue;
+    if (!in_view(cam, sph)) continue;
+    const float tx = sph[0] - cam.pos[0], ty = sph[1] - cam.pos[1], tz = sph[2] - cam.pos[2];
+    const float depth = tx * cam.fwd[0] + ty * cam.fwd[1] + tz * cam.fwd[2];
+    if (depth <= 1e-3f) continue;
+    const float dist = std::sqrt(tx * tx + ty * ty + tz * tz);
+    const float cosAngle = depth / std::max(dist, 1e-3f);
+    const float horiz = tx * right[0] + ty * right[1] + tz * right[2];
+    if (std::atan2(std::fabs(horiz), depth) > hHalf + 0.1f) continue;
+    float rp = (sph[3] / depth) / tanHalf * (H * 0.5f);
+    rp = std::max(rp, 0.0f);
+    const float area = kPi * rp * rp;
+    cov[o] = std::min(area * std::max(cosAngle, 0.0f), screenArea);
+  }
+  for (uint32_t o = 0; o < N; ++o) R.lodDist[o] = cov[o];
+  std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+    const float ca = sanitize(cov[a]), cb = sanitize(cov[b]);
+    if (ca == cb) return a < b;
+    return ca > cb;
+  });
+  const size_t minActive = std::min<size_t>(P, prm->min_active);
+  const float target = screenArea * frac;
+  std::vector<uint8_t> desired(N, 0);
+  size_t enabled = 0;
+  float acc = 0.0f;
+  for (uint32_t g : order) {
+    const size_t count = ctx->instances[g].primitive_count;
+    if (count == 0) continue;
+    const float c = cov[g];
+    const bool minSat = enabled >= minActive, covSat = acc >= target;
+    if (minSat && covSat) break;
+    if (minSat && c < prm->min_pixel_coverage) continue;
+    if (minSat && c <= 0.0f) continue;
+    desired[g] = 1;
+    enabled += count;
+    acc += c;
+  }
+  for (uint32_t g : order) {
+    if (enabled >= minActive) break;
+    const size_t count = ctx->instances[g].primitive_count;
+    if (desired[g] || count == 0) continue;
+    desired[g] = 1;
+    enabled += count;
+    acc += cov[g];
+  }
+  size_t toggledPrims = 0;
+  for (uint32_t g : order) {
+    if (toggledPrims >= budget) break;
+    const bool want = desired[g] != 0, active = ctx->objActiveCount[g] > 0;
+    if (want == active) continue;
+    if (R.objCooldown[g] > 0) continue;
+    const nomad_instance_record &ir = ctx->instances[g];
+    bool blocked = false;
+    for (uint32_t p = ir.primitive_base; p < ir.primitive_base + ir.primitive_count && !blocked; ++p)
+      if ((ctx->primActive[p] != 0) != want && R.primCooldown[p] > 0) blocked = true;
+    if (blocked) continue;
+    for (uint32_t p = ir.primitive_base; p < ir.primitive_base + ir.primitive_count; ++p)
+      if ((ctx->primActive[p] != 0) != want) R.primCooldown[p] = prm->state_cooldown;
+    uint32_t n = 0;
+    nomad_status st = nomad_residency_set_object_active(ctx, g, want ? 1 : 0, &n);
+    if (st != NOMAD_OK) return st;
+    if (n > 0 || (ctx->objActiveCount[g] > 0) != active || ctx->objActiveCount[g] == 0)
+      R.objCooldown[g] = prm->state_cooldown;
+    if (n > 0) toggledPrims = std::min(toggledPrims + n, budget);
+  }
+  bool any = false;
+  for (uint32_t o = 0; o < N && !any; ++o) any = ctx->objActiveCount[o] > 0;
+  if (!any) {
+    size_t fallback = 0;
+    for (uint32_t g : order) {
+      const size_t count = ctx->instances[g].primitive_count;
+      if (count == 0) continue;
+      uint32_t n = 0;
+      nomad_status st = nomad_residency_set_object_active(ctx, g, 1, &n);
+      if (st != NOMAD_OK) return st;
+      if (n > 0) {
+        R.objCooldown[g] = prm->state_cooldown;
+        fallback += count;
+        any = true;
+      }
+      if (any && fallback >= minActive) break;
+    }
+  }
+  nomad_status st = nomad_residency_flush(ctx);
+  if (st != NOMAD_OK) return st;
+  *toggled = (uint32_t)toggledPrims;
+  return NOMAD_OK;
+}
+
 }  // namespace
 
 extern "C" nomad_status nomad_residency_object_state(nomad_ctx *ctx, float *distance, uint8_t *flags,
@@ -945,6 +1102,10 @@ extern "C" nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residen
   if (prm->policy == NOMAD_POLICY_DISTANCE_LOD) {
     NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
     return distance_lod_step(ctx, prm, *camera, toggled);
+  }
+  if (prm->policy == NOMAD_POLICY_SCREEN_SPACE) {
+    NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+    return screen_space_step(ctx, prm, *camera, toggled);
   }
   if (prm->policy > NOMAD_POLICY_LEARNED) return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "unknown policy");
   const uint32_t N = ctx->objectCount;

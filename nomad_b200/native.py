@@ -195,6 +195,7 @@ class RestirConfig(C.Structure):
                 ("radius_px", C.c_float), ("m_cap", C.c_float), ("reference_mode", C.c_uint32)]
 
 POLICY_ALWAYS, POLICY_RAYHIT_BUDGET, POLICY_LEARNED, POLICY_RAYHIT_PRIM, POLICY_DISTANCE_LOD = 0, 1, 2, 3, 4
+POLICY_SCREEN_SPACE = 5
 N_FEATURES = 24
 MLP_PARAMS = 128 * 32 + 128 + 128 * 128 + 128 + 128 + 1 + 2 * N_FEATURES
 
@@ -206,17 +207,19 @@ class ResidencyParams(C.Structure):
                 ("reserve_motion", C.c_float), ("min_active", C.c_uint32), ("target_fraction", C.c_float),
                 ("rebuild_cooldown", C.c_uint32), ("state_cooldown", C.c_uint32),
                 ("lod_enter_distance", C.c_float), ("lod_exit_distance", C.c_float),
-                ("lod_enter_view_degrees", C.c_float), ("lod_exit_view_degrees", C.c_float)]
+                ("lod_enter_view_degrees", C.c_float), ("lod_exit_view_degrees", C.c_float),
+                ("min_pixel_coverage", C.c_float)]
 
     @staticmethod
     def make(policy, budget_bytes=0, max_toggles=0, hit_decay=0.85, camera_motion=0.0,
              memory_pressure=0.0, reserve_base=0.02, reserve_motion=0.06, min_active=0,
              target_fraction=0.54, rebuild_cooldown=4, state_cooldown=5, lod_enter_distance=225.0,
-             lod_exit_distance=275.0, lod_enter_view_degrees=5.0, lod_exit_view_degrees=12.0):
+             lod_exit_distance=275.0, lod_enter_view_degrees=5.0, lod_exit_view_degrees=12.0,
+             min_pixel_coverage=32.0):
         return ResidencyParams(policy, max_toggles, budget_bytes, hit_decay, camera_motion,
                                memory_pressure, reserve_base, reserve_motion, min_active, target_fraction,
                                rebuild_cooldown, state_cooldown, lod_enter_distance, lod_exit_distance,
-                               lod_enter_view_degrees, lod_exit_view_degrees)
+                               lod_enter_view_degrees, lod_exit_view_degrees, min_pixel_coverage)
 
 VIEW_DTYPE = np.dtype([("camera_pos", "<f4", 3), ("viewport_u", "<f4", 3), ("viewport_v", "<f4", 3),
                        ("first_pixel", "<f4", 3), ("width", "<u4"), ("height", "<u4"), ("spp", "<u4"),

@@ -155,7 +155,8 @@ class Workload:
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             ctx.render_dev(v, d_img.data_ptr(), count_hits=True)
-            ctx.residency_step(prm, v, toggles=prm.policy in (nat.POLICY_RAYHIT_PRIM, nat.POLICY_DISTANCE_LOD))
+            ctx.residency_step(prm, v, toggles=prm.policy in (nat.POLICY_RAYHIT_PRIM, nat.POLICY_DISTANCE_LOD,
+                                                             nat.POLICY_SCREEN_SPACE))
             ctx.sync()
             dt = time.perf_counter() - t0
             num = torch.mean((d_img - d_ref) ** 2).item()
@@ -295,6 +296,13 @@ def run(paths=200, frames_per_path=8, steps=1500, frames=300, log=print):
         ctx, judge, nat.POLICY_DISTANCE_LOD, frames=frames,
         prm=nat.ResidencyParams.make(nat.POLICY_DISTANCE_LOD, max_toggles=24, camera_motion=0.3))
     log(f"distance_lod_reference: {out['distance_lod_reference']}")
+    # The reference's ScreenSpaceFootprint heuristic with its defaults (68 % of the screen, 32 px,
+    # 14 primitive toggles a frame), one mesh group per object.
+    out["screen_space_reference"] = w.evaluate(
+        ctx, judge, nat.POLICY_SCREEN_SPACE, frames=frames,
+        prm=nat.ResidencyParams.make(nat.POLICY_SCREEN_SPACE, max_toggles=14, camera_motion=0.3, min_active=16,
+                                     target_fraction=0.68, min_pixel_coverage=32.0))
+    log(f"screen_space_reference: {out['screen_space_reference']}")
     # The learned policy at smaller budgets: the smallest one whose rel-MSE is within 5 % of the
     # ray-hit policy's at the full budget, and its ms/frame.
     sweep = {}

@@ -311,3 +311,95 @@ def object_spheres(sb):
         out[o, :3] = c
         out[o, 3] = np.sqrt(np.float32(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]), dtype=np.float32)
     return out
+
+
+class ScreenSpaceOracle:
+    """updateScreenSpaceFootprint (RendererResidency.cpp:4092-4396) with one mesh group per object,
+    restated over the per-object coverage of the step (checked by coverage_f64): groups by
+    coverage until min_active primitives and the target share of the screen are covered, toggles
+    in coverage order under a primitive budget, object and primitive cooldowns (whole objects are
+    toggled here, so one cooldown per object carries both)."""
+
+    def __init__(self, prim_counts):
+        self.count = prim_counts.astype(np.int64)
+        self.n = self.count.size
+        self.active = self.count > 0
+        self.cooldown = np.zeros(self.n, np.uint32)
+
+    def step(self, cov, width, height, motion=0.0, pressure=0.0, target_fraction=0.68, min_pixel=32.0,
+             min_active=16, max_toggles=14, state_cooldown=5):
+        f32 = np.float32
+        self.cooldown = np.where(self.cooldown > 0, self.cooldown - 1, 0).astype(np.uint32)
+        m, p = f32(min(max(motion, 0.0), 1.0)), f32(min(max(pressure, 0.0), 1.0))
+        frac = f32(min(max(f32(target_fraction) + f32(0.08) * m - f32(0.10) * p, f32(0.50)), f32(0.94)))
+        budget = max(1, int(np.floor(float(max(max_toggles, 1)) * (1.0 + 0.40 * float(m) + 0.50 * float(p)) + 0.5)))
+        area = f32(width) * f32(height)
+        if area <= 0:
+            area = f32(1.0)
+        order = np.lexsort((np.arange(self.n), -cov.astype(np.float64)))
+        min_active_n = min(int(self.count.sum()), min_active)
+        target = f32(area * frac)
+        desired = np.zeros(self.n, bool)
+        enabled, acc = 0, f32(0.0)
+        for g in order:
+            c = self.count[g]
+            if c == 0:
+                continue
+            cv = f32(cov[g])
+            min_sat, cov_sat = enabled >= min_active_n, acc >= target
+            if min_sat and cov_sat:
+                break
+            if min_sat and cv < f32(min_pixel):
+                continue
+            if min_sat and cv <= 0:
+                continue
+            desired[g] = True
+            enabled += c
+            acc = f32(acc + cv)
+        for g in order:
+            if enabled >= min_active_n:
+                break
+            if desired[g] or self.count[g] == 0:
+                continue
+            desired[g] = True
+            enabled += self.count[g]
+            acc = f32(acc + f32(cov[g]))
+        toggled = 0
+        for g in order:
+            if toggled >= budget:
+                break
+            if desired[g] == self.active[g] or self.cooldown[g] > 0 or self.count[g] == 0:
+                continue
+            self.active[g] = desired[g]
+            self.cooldown[g] = state_cooldown
+            toggled = min(toggled + int(self.count[g]), budget)
+        return toggled
+
+
+def coverage_f64(spheres, view):
+    """objectCoverageForSphere (RendererResidency.cpp:4130-4182) in float64, with the margin of
+    each decision (frustum, depth, horizontal angle) for the comparison."""
+    vis, vmargin = in_view_f64(spheres.astype(np.float64), view)
+    v = np.asarray(view).reshape(-1)[0]
+    pos = v["camera_pos"].astype(np.float64)
+    U, V = v["viewport_u"].astype(np.float64), v["viewport_v"].astype(np.float64)
+    f = v["first_pixel"].astype(np.float64) + 0.5 * U + 0.5 * V - pos
+    fl = np.linalg.norm(f)
+    fwd = f / fl
+    up = -V / np.linalg.norm(V)
+    right = np.cross(fwd, up)
+    right /= np.linalg.norm(right)
+    tan_half = 0.5 * np.linalg.norm(V) / fl
+    W, H = float(v["width"]), float(v["height"])
+    h_half = np.arctan(tan_half * W / H)
+    t = spheres[:, :3].astype(np.float64) - pos
+    depth = t @ fwd
+    dist = np.linalg.norm(t, axis=1)
+    cos_a = depth / np.maximum(dist, 1e-3)
+    ha = np.arctan2(np.abs(t @ right), depth)
+    rp = np.maximum((spheres[:, 3] / depth) / tan_half * (H * 0.5), 0.0)
+    cov = np.minimum(np.pi * rp * rp * np.maximum(cos_a, 0.0), W * H)
+    ok = vis & (depth > 1e-3) & (ha <= h_half + 0.1)
+    cov = np.where(ok, cov, 0.0)
+    margin = np.minimum.reduce([vmargin, np.abs(depth - 1e-3), np.abs(h_half + 0.1 - ha)])
+    return cov, margin

@@ -255,3 +255,35 @@ def test_distance_lod_policy(nb, ctx, small_city):
     finally:
         c2.close()
     assert np.array_equal(np.ascontiguousarray(got).view(np.int32), np.ascontiguousarray(want_h).view(np.int32))
+
+
+def test_screen_space_policy(nb, ctx, small_city):
+    """The reference's ScreenSpaceFootprint heuristic (NOMAD_POLICY_SCREEN_SPACE) against the numpy
+    restatement over a camera orbit: coverage equal to a float64 restatement (relative 1e-3, or a
+    decision within 1e-4 of its boundary), the same objects toggled under the primitive budget and
+    cooldowns."""
+    from oracle import residency as ores
+
+    _, sb = small_city
+    ctx.upload(sb)
+    prm = nb.ResidencyParams.make(nb.POLICY_SCREEN_SPACE, max_toggles=3000, camera_motion=0.2, memory_pressure=0.1,
+                                  target_fraction=0.6, min_active=16, min_pixel_coverage=32.0)
+    orc = ores.ScreenSpaceOracle(sb.instances["primitive_count"])
+    spheres = ores.object_spheres(sb)
+    total = 0
+    for frame in range(10):
+        ang = 0.3 * frame
+        view = nb.view_pinhole((160 * np.sin(ang), 70, -160 * np.cos(ang)), (0, 0, 0), width=128, height=72, spp=1,
+                               max_depth=1, seed=frame)
+        toggled = ctx.residency_step(prm, view)
+        cov, _, cd = ctx.residency_object_state()
+        c64, margin = ores.coverage_f64(spheres, view)
+        ok = np.abs(cov.astype(np.float64) - c64) <= 1e-3 * np.maximum(1.0, c64)
+        assert (ok | (margin < 1e-4)).all(), frame
+        want = orc.step(cov, 128, 72, motion=0.2, pressure=0.1, target_fraction=0.6, min_pixel=32.0, min_active=16,
+                        max_toggles=3000)
+        assert toggled == want, (frame, toggled, want)
+        assert np.array_equal(ctx.residency_flags().astype(bool), orc.active), frame
+        assert np.array_equal(cd, orc.cooldown), frame
+        total += toggled
+    assert total > 0
