@@ -400,8 +400,9 @@ nomad_status nomad_residency_flags(nomad_ctx *ctx, uint8_t *out);
  * copy engine (asynchronously, at most max_onloads_per_frame objects started per update),
  * relocated on the device to its pool offsets, and published into the TLAS when its copy has
  * completed (Streaming -> Resident); an object no longer wanted is unlinked at once and its
- * pool space reused after the work queued before the unlink has finished. An onload that does
- * not fit in the pool is denied (the reference's geometry hard cap). Until an object is
+ * copy kept as a cache (Cached) until an onload needs the space, which is reused after the work
+ * queued before the unlink has finished. An onload that does not fit even after the cache is
+ * released is denied (the reference's geometry hard cap). Until an object is
  * Resident it is skipped by traversal even if its residency flag is set. The TLAS and the
  * shading arrays (packed primitives, materials) stay resident. Traversal configurations of
  * other widths, nomad_trace_work and the allocation-free call need the pair layout and are
@@ -413,7 +414,10 @@ typedef struct nomad_paging_config {
   uint32_t width;                 /* paged node layout: 2 (pair), 4 or 8                      */
 } nomad_paging_config;
 
-enum { NOMAD_PAGE_COLD = 0, NOMAD_PAGE_STREAMING = 1, NOMAD_PAGE_RESIDENT = 2 };
+/* CACHED: no longer wanted, unlinked, but its pool copy is kept until the space is needed (least
+ * recently unwanted first), so an object the residency state wants back is relinked without a
+ * copy and without counting against the onload cap. */
+enum { NOMAD_PAGE_COLD = 0, NOMAD_PAGE_STREAMING = 1, NOMAD_PAGE_RESIDENT = 2, NOMAD_PAGE_CACHED = 3 };
 
 typedef struct nomad_paging_stats {
   uint64_t pool_bytes;            /* node + record pool capacity                              */
@@ -422,6 +426,8 @@ typedef struct nomad_paging_stats {
   uint64_t bytes_streamed;        /* host -> device bytes of all onloads                      */
   uint32_t cold, streaming, resident;
   uint32_t onloads, evictions, denied, deferred; /* totals since enable                       */
+  uint32_t cached;                /* objects in NOMAD_PAGE_CACHED                              */
+  uint32_t relinks;               /* cached objects wanted again and relinked (total)          */
 } nomad_paging_stats;
 
 nomad_status nomad_paging_enable(nomad_ctx *ctx, const nomad_paging_config *cfg);

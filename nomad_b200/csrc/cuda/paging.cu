@@ -95,9 +95,11 @@ struct ObjPage {
   uint32_t firstRec = 0;             // leaf position of the object's first record
   int32_t rootRel = kEmptyRef;       // BLAS root ref relative to the object's blocks
   int64_t slotWord = -1;             // arena word of the object's TLAS link, -1 none
-  Span node, rec;                    // pool spans while Streaming or Resident
+  Span node, rec;                    // pool spans while Streaming, Resident or Cached
   uint8_t state = NOMAD_PAGE_COLD;
   cudaEvent_t copied = nullptr;      // copy + relocation done
+  int32_t poolRef = kEmptyRef;       // the relocated root ref of the pool copy
+  uint64_t unwantedAt = 0;           // update count when it became Cached (LRU order)
 };
 
 struct Retire {
@@ -136,6 +138,7 @@ struct Paging {
   DeviceBuf items;
   DeviceBuf slots;  // arena word of each object's TLAS link (int64, -1 none)
   nomad_paging_stats stats{};
+  uint64_t tick = 0;                // updates so far
   int32_t *refTable = nullptr;      // device ref table of the paged layout
   char *nodeBase = nullptr;         // arena: TLAS part then node pool
   float4 *recBase = nullptr;        // record pool
@@ -445,8 +448,9 @@ nomad_status publish(nomad_ctx *ctx, Paging *pg, const std::vector<PubItem> &ite
   return NOMAD_OK;
 }
 
-// Publishes every Streaming object whose copy has completed (or all of them, after a wait).
-void collect_ready(Paging *pg, std::vector<PubItem> &items, bool all) {
+// Publishes every Streaming object whose copy has completed (or all of them, after a wait); one
+// no longer wanted goes to the cache instead.
+void collect_ready(const nomad_ctx *ctx, Paging *pg, std::vector<PubItem> &items, bool all) {
   for (uint32_t o = 0; o < pg->obj.size(); ++o) {
     ObjPage &op = pg->obj[o];
     if (op.state != NOMAD_PAGE_STREAMING) continue;
@@ -456,11 +460,18 @@ void collect_ready(Paging *pg, std::vector<PubItem> &items, bool all) {
       ref = (int32_t)(pg->tlasNodes + op.node.off + (uint64_t)ref);
     else if (ref != kEmptyRef)
       ref = ~((~ref) + (int32_t)op.rec.off);
-    op.state = NOMAD_PAGE_RESIDENT;
-    pg->ref[o] = ref;
-    items.push_back(PubItem{o, ref});
+    op.poolRef = ref;
     --pg->stats.streaming;
-    ++pg->stats.resident;
+    if (ctx->objResident[o]) {
+      op.state = NOMAD_PAGE_RESIDENT;
+      pg->ref[o] = ref;
+      items.push_back(PubItem{o, ref});
+      ++pg->stats.resident;
+    } else {
+      op.state = NOMAD_PAGE_CACHED;
+      op.unwantedAt = pg->tick;
+      ++pg->stats.cached;
+    }
   }
 }
 
@@ -497,40 +508,58 @@ extern "C" nomad_status nomad_paging_update(nomad_ctx *ctx) {
   nomad_status hs = nomad_residency_sync_host(ctx);
   if (hs != NOMAD_OK) return hs;
   refresh_retired(pg);
+  ++pg->tick;
   std::vector<PubItem> items;
-  // Evictions first, so every object has at most one item (Streaming objects that are no longer
-  // wanted are retired, not published).
-  std::vector<Retire> retire;
+  // Unwanted Resident objects are unlinked into the cache; wanted Cached ones relinked. Every
+  // object gets at most one item per update.
   for (uint32_t o = 0; o < pg->obj.size(); ++o) {
     ObjPage &op = pg->obj[o];
-    if (ctx->objResident[o] || op.state == NOMAD_PAGE_COLD) continue;
-    if (op.state == NOMAD_PAGE_RESIDENT) --pg->stats.resident;
-    else --pg->stats.streaming;
-    ++pg->stats.cold;
-    ++pg->stats.evictions;
-    retire.push_back(Retire{op.node, op.rec, nullptr, op.state == NOMAD_PAGE_STREAMING ? op.copied : nullptr, o});
-    op.state = NOMAD_PAGE_COLD;
-    op.node = op.rec = Span{};
-    pg->ref[o] = kEmptyRef;
-    items.push_back(PubItem{o, kEmptyRef});
+    const bool want = ctx->objResident[o] != 0;
+    if (!want && op.state == NOMAD_PAGE_RESIDENT) {
+      op.state = NOMAD_PAGE_CACHED;
+      op.unwantedAt = pg->tick;
+      pg->ref[o] = kEmptyRef;
+      items.push_back(PubItem{o, kEmptyRef});
+      --pg->stats.resident;
+      ++pg->stats.cached;
+    } else if (want && op.state == NOMAD_PAGE_CACHED) {
+      op.state = NOMAD_PAGE_RESIDENT;
+      pg->ref[o] = op.poolRef;
+      items.push_back(PubItem{o, op.poolRef});
+      --pg->stats.cached;
+      ++pg->stats.resident;
+      ++pg->stats.relinks;
+    }
   }
-  collect_ready(pg, items, false);
+  collect_ready(ctx, pg, items, false);
   nomad_status st = publish(ctx, pg, items);
   if (st != NOMAD_OK) return st;
-  if (!retire.empty()) {
-    cudaEvent_t ev;
-    if (!pg->eventPool.empty()) {
-      ev = pg->eventPool.back();
-      pg->eventPool.pop_back();
-    } else {
-      NOMAD_CUDA(ctx, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  // Releases cached copies, least recently unwanted first, until `nodes` and `recs` more units
+  // are on their way back to the free lists (usable from a later update, once the work queued
+  // before their unlink is done).
+  uint64_t pendNodes = 0, pendRecs = 0;
+  std::vector<Retire> retire;
+  auto release_cache = [&](uint64_t nodes, uint64_t recs) {
+    while (pendNodes < nodes || pendRecs < recs) {
+      int64_t victim = -1;
+      for (uint32_t o = 0; o < pg->obj.size(); ++o)
+        if (pg->obj[o].state == NOMAD_PAGE_CACHED &&
+            (victim < 0 || pg->obj[o].unwantedAt < pg->obj[victim].unwantedAt))
+          victim = o;
+      if (victim < 0) return false;
+      ObjPage &vp = pg->obj[victim];
+      retire.push_back(Retire{vp.node, vp.rec, nullptr, nullptr, (uint32_t)victim});
+      pendNodes += vp.node.len;
+      pendRecs += vp.rec.len;
+      vp.state = NOMAD_PAGE_COLD;
+      vp.node = vp.rec = Span{};
+      vp.poolRef = kEmptyRef;
+      --pg->stats.cached;
+      ++pg->stats.cold;
+      ++pg->stats.evictions;
     }
-    NOMAD_CUDA(ctx, cudaEventRecord(ev, ctx->stream));
-    for (Retire &r : retire) {
-      r.after = ev;
-      pg->retiring.push_back(r);
-    }
-  }
+    return true;
+  };
   // onloads, in object order, at most maxOnloads
   uint32_t started = 0;
   for (uint32_t o = 0; o < pg->obj.size(); ++o) {
@@ -541,13 +570,15 @@ extern "C" nomad_status nomad_paging_update(nomad_ctx *ctx) {
       continue;
     }
     uint64_t noff = 0, roff = 0;
-    if (!pg->nodeAlloc.alloc(op.nNodes, noff)) {
-      ++pg->stats.denied;
-      continue;
-    }
-    if (!pg->recAlloc.alloc(op.nRecs, roff)) {
+    bool got = pg->nodeAlloc.alloc(op.nNodes, noff);
+    if (got && !pg->recAlloc.alloc(op.nRecs, roff)) {
       pg->nodeAlloc.release(noff, op.nNodes);
-      ++pg->stats.denied;
+      got = false;
+    }
+    if (!got) {
+      // make room from the cache for a later update; denied when the cache cannot
+      if (!release_cache(pendNodes + op.nNodes, pendRecs + op.nRecs)) ++pg->stats.denied;
+      else ++pg->stats.deferred;
       continue;
     }
     op.node = Span{noff, op.nNodes};
@@ -577,6 +608,20 @@ extern "C" nomad_status nomad_paging_update(nomad_ctx *ctx) {
     pg->stats.bytes_streamed += op.nNodes * pg->nodeBytes + op.nRecs * 48;
     ++started;
   }
+  if (!retire.empty()) {
+    cudaEvent_t ev;
+    if (!pg->eventPool.empty()) {
+      ev = pg->eventPool.back();
+      pg->eventPool.pop_back();
+    } else {
+      NOMAD_CUDA(ctx, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    }
+    NOMAD_CUDA(ctx, cudaEventRecord(ev, ctx->stream));
+    for (Retire &r : retire) {
+      r.after = ev;
+      pg->retiring.push_back(r);
+    }
+  }
   return NOMAD_OK;
 }
 
@@ -587,7 +632,7 @@ extern "C" nomad_status nomad_paging_wait(nomad_ctx *ctx) {
   NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
   NOMAD_CUDA(ctx, cudaStreamSynchronize(pg->copy));
   std::vector<PubItem> items;
-  collect_ready(pg, items, true);
+  collect_ready(ctx, pg, items, true);
   nomad_status st = publish(ctx, pg, items);
   if (st != NOMAD_OK) return st;
   NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));

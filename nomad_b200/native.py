@@ -77,10 +77,11 @@ class PagingStats(C.Structure):
     _fields_ = [("pool_bytes", C.c_uint64), ("used_bytes", C.c_uint64), ("full_bytes", C.c_uint64),
                 ("bytes_streamed", C.c_uint64), ("cold", C.c_uint32), ("streaming", C.c_uint32),
                 ("resident", C.c_uint32), ("onloads", C.c_uint32), ("evictions", C.c_uint32),
-                ("denied", C.c_uint32), ("deferred", C.c_uint32)]
+                ("denied", C.c_uint32), ("deferred", C.c_uint32), ("cached", C.c_uint32),
+                ("relinks", C.c_uint32)]
 
 
-PAGE_COLD, PAGE_STREAMING, PAGE_RESIDENT = 0, 1, 2
+PAGE_COLD, PAGE_STREAMING, PAGE_RESIDENT, PAGE_CACHED = 0, 1, 2, 3
 
 
 class Config(C.Structure):

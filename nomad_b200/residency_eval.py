@@ -242,7 +242,8 @@ class Workload:
                     "mean_streamed_bytes_per_frame": float(np.mean(streamed)),
                     "mean_onloads_per_frame": float(np.mean(onl)), "max_onloads_per_frame": int(np.max(onl)),
                     "denied": st["denied"], "deferred": st["deferred"], "evictions": st["evictions"],
-                    "resident_objects_end": st["resident"]}
+                    "relinks_from_cache": st["relinks"], "resident_objects_end": st["resident"],
+                    "cached_objects_end": st["cached"]}
         finally:
             pc.close()
 

@@ -143,36 +143,43 @@ def test_small_pool_denies_onloads(nb, small_city):
 
 
 def test_primitive_toggles_follow_pages(nb, small_city):
-    """Primitive activity set while an object is Resident or Cold reaches the device copy."""
+    """Primitive activity set while an object is Resident, Cached (unlinked, pool copy kept) or
+    Cold (never streamed in) reaches the copy that is traced once it is wanted again."""
     _, sb = small_city
     rays = _rays(sb, 17)
     rng = np.random.default_rng(1)
     off = rng.choice(sb.prim_count, size=sb.prim_count // 5, replace=False)
-    cold_obj = int(np.argmax(sb.instances["primitive_count"]))
+    by_size = np.argsort(-sb.instances["primitive_count"])
+    cold_obj, cache_obj = int(by_size[0]), int(by_size[1])
     ctx = _paged(nb, sb, 4, 1 << 40)
     try:
+        ctx.set_object_active(cold_obj, False)  # before any update: never streamed in
+        ctx.flush()
         for _ in range(10):
             ctx.paging_update()
             ctx.paging_wait()
-        # make one object Cold, then wanted again but not yet streamed in
-        ctx.set_object_active(cold_obj, False)
+        ctx.set_object_active(cache_obj, False)
         ctx.flush()
         for _ in range(3):
             ctx.paging_update()
             ctx.paging_wait()
-        assert ctx.paging_states()[cold_obj] == 0
-        ctx.set_object_active(cold_obj, True)
-        ctx.flush()
-        assert ctx.paging_states()[cold_obj] == 0
-        # primitive toggles now reach Resident objects' pool copies and the Cold object's host copy
-        assert (sb.prim_object[off] == cold_obj).any()
+        st = ctx.paging_states()
+        assert st[cold_obj] == nb.native.PAGE_COLD and st[cache_obj] == nb.native.PAGE_CACHED
+        assert (sb.prim_object[off] == cold_obj).any() and (sb.prim_object[off] == cache_obj).any()
         for p in off:
+            ctx.set_primitive_active(int(p), False)
+        ctx.flush()
+        ctx.set_object_active(cold_obj, True)
+        ctx.set_object_active(cache_obj, True)
+        # the object toggles re-activated their primitives: switch the chosen ones off again
+        for p in off[(sb.prim_object[off] == cold_obj) | (sb.prim_object[off] == cache_obj)]:
             ctx.set_primitive_active(int(p), False)
         ctx.flush()
         for _ in range(10):
             ctx.paging_update()
             ctx.paging_wait()
-        assert (ctx.paging_states()[sb.instances["primitive_count"] > 0] == 2).all()
+        assert (ctx.paging_states()[sb.instances["primitive_count"] > 0] == nb.native.PAGE_RESIDENT).all()
+        assert ctx.paging_stats()["relinks"] >= 1
         got = ctx.trace_closest(rays)
     finally:
         ctx.close()
