@@ -23,6 +23,7 @@
 // a violation sets a bit in counts[2] instead of faulting.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "../../../include/nomad_scene.h"
@@ -140,56 +141,37 @@ __global__ void k_prim_flags(const int32_t *__restrict__ primIdx, const uint8_t 
   a[j] = active[g] ? 1u : 0u;
 }
 
-// Active primitives to their compact slots: packed primitive (7 float4), material (5 float4),
-// remap (compact -> global), compact primitive index (its own slot), global -> compact map.
-// One warp moves 32 primitives; lanes stride over their float4s so stores stay contiguous.
+// Active primitives to their compact slots: remap (compact -> global), compact primitive index
+// (its own slot), global -> compact map.
 __global__ void k_gather(const int32_t *__restrict__ primIdx, const uint32_t *__restrict__ a,
-                         const uint32_t *__restrict__ cpos, uint32_t n, const float4 *__restrict__ prims,
-                         const float4 *__restrict__ mats, float4 *__restrict__ oPrims, float4 *__restrict__ oMats,
-                         uint32_t *__restrict__ oRemap, int32_t *__restrict__ oIdx, int32_t *__restrict__ oPrimToRes) {
-  const uint32_t j0 = (blockIdx.x * kT + (threadIdx.x & ~31u));
-  const int lane = threadIdx.x & 31;
-  const uint32_t j = j0 + lane;
-  int32_t g = -1;
-  uint32_t k = 0;
-  bool on = false;
-  if (j < n) {
-    g = primIdx[j];
-    on = a[j] != 0;  // only valid indices are flagged
-    k = cpos[j];
-    if (g >= 0 && (uint32_t)g < n) oPrimToRes[g] = on ? (int32_t)k : -1;
-    if (on) {
-      oRemap[k] = (uint32_t)g;
-      oIdx[k] = (int32_t)k;
-    }
+                         const uint32_t *__restrict__ cpos, uint32_t n, uint32_t *__restrict__ oRemap,
+                         int32_t *__restrict__ oIdx, int32_t *__restrict__ oPrimToRes) {
+  const uint32_t j = blockIdx.x * kT + threadIdx.x;
+  if (j >= n) return;
+  const int32_t g = primIdx[j];
+  const bool on = a[j] != 0;  // only valid indices are flagged
+  const uint32_t k = cpos[j];
+  if (g >= 0 && (uint32_t)g < n) oPrimToRes[g] = on ? (int32_t)k : -1;
+  if (on) {
+    oRemap[k] = (uint32_t)g;
+    oIdx[k] = (int32_t)k;
   }
-  const uint32_t mask = __ballot_sync(0xffffffffu, on);
-  const uint32_t items = (uint32_t)__popc(mask) * 12u;  // 7 primitive + 5 material float4 each
-  // All of a lane's loads are issued before its stores (up to 12 in flight per lane).
-  float4 buf[12];
-  float4 *dst[12];
-#pragma unroll
-  for (int i = 0; i < 12; ++i) {
-    const uint32_t q = (uint32_t)(i * 32 + lane);
-    const bool valid = q < items;
-    const uint32_t r = q / 12u, part = q - r * 12u;
-    const int src = valid ? (int)__fns(mask, 0u, (int)r + 1) : 0;
-    const int32_t gs = __shfl_sync(0xffffffffu, g, src);
-    const uint32_t ks = __shfl_sync(0xffffffffu, k, src);
-    dst[i] = nullptr;
-    if (valid) {
-      if (part < 7u) {
-        buf[i] = __ldg(&prims[(size_t)gs * 7 + part]);
-        dst[i] = oPrims + (size_t)ks * 7 + part;
-      } else {
-        buf[i] = __ldg(&mats[(size_t)gs * 5 + (part - 7u)]);
-        dst[i] = oMats + (size_t)ks * 5 + (part - 7u);
-      }
-    }
+}
+
+// The active primitives' packed primitive (7 float4) and material (5 float4), one float4 per
+// thread in compact order: reads follow the remap, writes are contiguous.
+__global__ void __launch_bounds__(kT) k_copy_prims(const uint32_t *__restrict__ remap, const uint32_t *__restrict__ count,
+                                                   const float4 *__restrict__ prims, const float4 *__restrict__ mats,
+                                                   float4 *__restrict__ oPrims, float4 *__restrict__ oMats) {
+  const unsigned long long items = (unsigned long long)(*count) * 12ull;
+  for (unsigned long long t = (unsigned long long)blockIdx.x * kT + threadIdx.x; t < items;
+       t += (unsigned long long)gridDim.x * kT) {
+    const unsigned long long k = t / 12ull;
+    const uint32_t part = (uint32_t)(t - k * 12ull);
+    const uint32_t g = __ldg(&remap[k]);
+    if (part < 7u) oPrims[k * 7 + part] = __ldg(&prims[(size_t)g * 7 + part]);
+    else oMats[k * 5 + (part - 7u)] = __ldg(&mats[(size_t)g * 5 + (part - 7u)]);
   }
-#pragma unroll
-  for (int i = 0; i < 12; ++i)
-    if (dst[i]) *dst[i] = buf[i];
 }
 
 // First leaf position covered by the subtree of node u (walk left children to a leaf).
@@ -430,10 +412,15 @@ extern "C" nomad_status nomad_scenebvh_compact_gpu(const nomad_scenebvh_device *
   if (N && cudaMemsetAsync(w.rootOf, 0xff, (size_t)N * 4, s) != cudaSuccess) return NOMAD_ERR_CUDA;
   k_prim_flags<<<gp, kT, 0, s>>>(in->prim_indices, prim_active, n, w.a, w.err);
   if (scan(w.a, n, w.sums, w.cpos, s) != cudaSuccess) return NOMAD_ERR_CUDA;
-  k_gather<<<gp, kT, 0, s>>>(in->prim_indices, w.a, w.cpos, n, reinterpret_cast<const float4 *>(in->prims),
-                             reinterpret_cast<const float4 *>(in->materials), reinterpret_cast<float4 *>(out->prims),
-                             reinterpret_cast<float4 *>(out->materials), out->remap, out->prim_indices,
-                             out->prim_to_resident);
+  k_gather<<<gp, kT, 0, s>>>(in->prim_indices, w.a, w.cpos, n, out->remap, out->prim_indices, out->prim_to_resident);
+  {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const unsigned gc = (unsigned)std::min<uint64_t>((uint64_t)sms * 16, ((uint64_t)n * 12 + kT - 1) / kT);
+    k_copy_prims<<<gc, kT, 0, s>>>(out->remap, w.cpos + n, reinterpret_cast<const float4 *>(in->prims),
+                                   reinterpret_cast<const float4 *>(in->materials),
+                                   reinterpret_cast<float4 *>(out->prims), reinterpret_cast<float4 *>(out->materials));
+  }
   if (N) {
     k_node_flags<<<gn, kT, 0, s>>>(bvh, N, w.cpos, n, w.nflag, w.e, w.err);
     k_node_roots<<<nobj, kT, 0, s>>>(bvh, N, in->instances, nobj, w.rootOf, w.objEnd, w.err);

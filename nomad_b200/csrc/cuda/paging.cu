@@ -109,6 +109,14 @@ struct Retire {
   uint32_t obj = 0;
 };
 
+// One onload of a batch: where the object's blocks are in the cold store and in the pools.
+struct StreamDesc {
+  uint64_t imgNode, nNodes, imgRec, nRecs;
+  int32_t nodeBase;  // absolute node index of the node span (TLAS part + pool offset)
+  int32_t recBase;   // record pool index of the record span
+  uint64_t dstNode;  // float4 offset of the node span in the arena
+};
+
 struct PubItem {
   uint32_t obj;
   int32_t ref;
@@ -122,6 +130,11 @@ struct Paging {
   uint64_t allNodes = 0, allRecs = 0;
   uint32_t maxOnloads = kDefaultOnloads;
   float *hostNodes = nullptr, *hostRecs = nullptr;  // pinned cold store
+  const float4 *devNodes = nullptr, *devRecs = nullptr;  // the same, as the device maps it
+  StreamDesc *pinnedDesc = nullptr;  // one update's onload batch
+  DeviceBuf descBuf;
+  cudaEvent_t descFree = nullptr;    // the previous batch's descriptors have been copied
+  bool descPending = false;
   std::vector<ObjPage> obj;
   std::vector<int32_t> ref;     // host copy of the published ref table
   RangeAlloc nodeAlloc, recAlloc;
@@ -155,6 +168,8 @@ struct Paging {
     if (hostNodes) cudaFreeHost(hostNodes);
     if (hostRecs) cudaFreeHost(hostRecs);
     if (pinnedItems) cudaFreeHost(pinnedItems);
+    if (pinnedDesc) cudaFreeHost(pinnedDesc);
+    if (descFree) cudaEventDestroy(descFree);
   }
 };
 
@@ -165,21 +180,36 @@ __device__ __forceinline__ uint32_t ref_word(uint32_t width, uint32_t k) {
   return width == 2 ? (k == 0 ? 3u : 7u) : 6u * width + k;
 }
 
-// Rebases the refs of `n` freshly copied nodes: internal refs by the node span's absolute base,
-// leaf refs (~record) by the record span's base; empty refs stay empty.
-__global__ void k_relocate(int32_t *__restrict__ nodes, uint64_t n, uint32_t fpn, uint32_t width,
-                           int32_t nodeBase, int32_t recBase) {
-  const uint32_t refs = width == 2 ? 2u : width;
-  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n * refs) return;
-  const uint64_t node = i / refs;
-  const uint32_t k = (uint32_t)(i - node * refs);
-  int32_t *w = nodes + node * fpn + ref_word(width, k);
-  const int32_t r = *w;
-  if (r >= 0)
-    *w = r + nodeBase;
-  else if (r != kEmptyRef)
-    *w = ~((~r) + recBase);
+// Streams a batch of onloads in one launch, one block per object: the object's nodes and records
+// are read from the pinned cold store (host memory the device maps) and written to their pool
+// spans, the node refs rebased on the way (internal refs by the node span's absolute base, leaf
+// refs ~record by the record span's base, empty refs unchanged).
+__global__ void __launch_bounds__(256) k_stream_in(const StreamDesc *__restrict__ desc, const float4 *hostNodes,
+                                                   const float4 *hostRecs, float4 *__restrict__ arena,
+                                                   float4 *__restrict__ recPool, uint32_t fpn, uint32_t width) {
+  const StreamDesc d = desc[blockIdx.x];
+  const uint32_t q = fpn / 4;  // float4 per node
+  const uint64_t nodeF4 = d.nNodes * q;
+  for (uint64_t i = threadIdx.x; i < nodeF4; i += blockDim.x) {
+    float4 v = hostNodes[d.imgNode * q + i];
+    const uint32_t w0 = (uint32_t)(i % q) * 4;  // first word of this float4 within its node
+    int32_t *w = reinterpret_cast<int32_t *>(&v);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const uint32_t word = w0 + (uint32_t)k;
+      const bool isRef = width == 2 ? (word == 3 || word == 7) : (word >= 6 * width && word < 7 * width);
+      if (!isRef) continue;
+      const int32_t r = w[k];
+      if (r >= 0)
+        w[k] = r + d.nodeBase;
+      else if (r != kEmptyRef)
+        w[k] = ~((~r) + d.recBase);
+    }
+    arena[d.dstNode + i] = v;
+  }
+  const uint64_t recF4 = d.nRecs * 3;
+  for (uint64_t i = threadIdx.x; i < recF4; i += blockDim.x)
+    recPool[(uint64_t)d.recBase * 3 + i] = hostRecs[d.imgRec * 3 + i];
 }
 
 // Publishes refs: the ref table entry always, the TLAS link as the object's residency flag says
@@ -322,8 +352,17 @@ extern "C" nomad_status nomad_paging_enable(nomad_ctx *ctx, const nomad_paging_c
     op.node.off = nlo;  // the object's first node, kept only until the image is filled below
   }
   // Cold store: node blocks with relative refs, record blocks verbatim.
-  NOMAD_CUDA(ctx, cudaHostAlloc(&pg->hostNodes, std::max<uint64_t>(pg->allNodes, 1) * fpn * 4, cudaHostAllocDefault));
-  NOMAD_CUDA(ctx, cudaHostAlloc(&pg->hostRecs, std::max<uint64_t>(pg->allRecs, 1) * 48, cudaHostAllocDefault));
+  NOMAD_CUDA(ctx, cudaHostAlloc(&pg->hostNodes, std::max<uint64_t>(pg->allNodes, 1) * fpn * 4, cudaHostAllocMapped));
+  NOMAD_CUDA(ctx, cudaHostAlloc(&pg->hostRecs, std::max<uint64_t>(pg->allRecs, 1) * 48, cudaHostAllocMapped));
+  {
+    void *dn = nullptr, *dr = nullptr;
+    NOMAD_CUDA(ctx, cudaHostGetDevicePointer(&dn, pg->hostNodes, 0));
+    NOMAD_CUDA(ctx, cudaHostGetDevicePointer(&dr, pg->hostRecs, 0));
+    pg->devNodes = static_cast<const float4 *>(dn);
+    pg->devRecs = static_cast<const float4 *>(dr);
+  }
+  NOMAD_CUDA(ctx, cudaHostAlloc(&pg->pinnedDesc, std::max<size_t>(nobj, 1) * sizeof(StreamDesc), cudaHostAllocDefault));
+  NOMAD_CUDA(ctx, pg->descBuf.reserve(std::max<size_t>(nobj, 1) * sizeof(StreamDesc)));
   for (uint32_t o = 0; o < nobj; ++o) {
     ObjPage &op = pg->obj[o];
     const uint64_t nlo = op.node.off;
@@ -383,6 +422,7 @@ extern "C" nomad_status nomad_paging_enable(nomad_ctx *ctx, const nomad_paging_c
   NOMAD_CUDA(ctx, cudaStreamCreateWithFlags(&pg->copy, cudaStreamNonBlocking));
   NOMAD_CUDA(ctx, cudaEventCreateWithFlags(&pg->lastCopy, cudaEventDisableTiming));
   NOMAD_CUDA(ctx, cudaEventCreateWithFlags(&pg->itemsFree, cudaEventDisableTiming));
+  NOMAD_CUDA(ctx, cudaEventCreateWithFlags(&pg->descFree, cudaEventDisableTiming));
   NOMAD_CUDA(ctx, cudaHostAlloc(&pg->pinnedItems, std::max<size_t>(nobj, 1) * sizeof(PubItem), cudaHostAllocDefault));
   pg->pinnedCap = std::max<size_t>(nobj, 1);
   NOMAD_CUDA(ctx, pg->items.reserve(pg->pinnedCap * sizeof(PubItem)));
@@ -560,8 +600,10 @@ extern "C" nomad_status nomad_paging_update(nomad_ctx *ctx) {
     }
     return true;
   };
-  // onloads, in object order, at most maxOnloads
+  // onloads, in object order, at most maxOnloads, streamed in by one launch on the copy stream
   uint32_t started = 0;
+  std::vector<StreamDesc> batch;
+  std::vector<uint32_t> batchObjs;
   for (uint32_t o = 0; o < pg->obj.size(); ++o) {
     ObjPage &op = pg->obj[o];
     if (!ctx->objResident[o] || op.state != NOMAD_PAGE_COLD || (op.nNodes == 0 && op.nRecs == 0)) continue;
@@ -584,29 +626,29 @@ extern "C" nomad_status nomad_paging_update(nomad_ctx *ctx) {
     op.node = Span{noff, op.nNodes};
     op.rec = Span{roff, op.nRecs};
     if (!op.copied) NOMAD_CUDA(ctx, cudaEventCreateWithFlags(&op.copied, cudaEventDisableTiming));
-    char *nodeDst = pg->nodeBase + (pg->tlasNodes + noff) * pg->nodeBytes;
-    if (op.nNodes)
-      NOMAD_CUDA(ctx, cudaMemcpyAsync(nodeDst, pg->hostNodes + op.imgNode * pg->fpn, op.nNodes * pg->nodeBytes,
-                                      cudaMemcpyHostToDevice, pg->copy));
-    if (op.nRecs)
-      NOMAD_CUDA(ctx, cudaMemcpyAsync(pg->recBase + roff * 3, pg->hostRecs + op.imgRec * 12, op.nRecs * 48,
-                                      cudaMemcpyHostToDevice, pg->copy));
-    if (op.nNodes) {
-      const uint32_t refs = pg->width == 2 ? 2u : pg->width;
-      const uint64_t threads = op.nNodes * refs;
-      k_relocate<<<(unsigned)((threads + 255) / 256), 256, 0, pg->copy>>>(
-          reinterpret_cast<int32_t *>(nodeDst), op.nNodes, pg->fpn, pg->width, (int32_t)(pg->tlasNodes + noff),
-          (int32_t)roff);
-      NOMAD_CUDA(ctx, cudaGetLastError());
-    }
-    NOMAD_CUDA(ctx, cudaEventRecord(op.copied, pg->copy));
-    pg->anyCopy = true;
+    batch.push_back(StreamDesc{op.imgNode, op.nNodes, op.imgRec, op.nRecs, (int32_t)(pg->tlasNodes + noff),
+                               (int32_t)roff, (pg->tlasNodes + noff) * (pg->fpn / 4)});
+    batchObjs.push_back(o);
     op.state = NOMAD_PAGE_STREAMING;
     --pg->stats.cold;
     ++pg->stats.streaming;
     ++pg->stats.onloads;
     pg->stats.bytes_streamed += op.nNodes * pg->nodeBytes + op.nRecs * 48;
     ++started;
+  }
+  if (!batch.empty()) {
+    if (pg->descPending) NOMAD_CUDA(ctx, cudaEventSynchronize(pg->descFree));
+    std::memcpy(pg->pinnedDesc, batch.data(), batch.size() * sizeof(StreamDesc));
+    NOMAD_CUDA(ctx, cudaMemcpyAsync(pg->descBuf.p, pg->pinnedDesc, batch.size() * sizeof(StreamDesc),
+                                    cudaMemcpyHostToDevice, pg->copy));
+    NOMAD_CUDA(ctx, cudaEventRecord(pg->descFree, pg->copy));
+    pg->descPending = true;
+    k_stream_in<<<(unsigned)batch.size(), 256, 0, pg->copy>>>(
+        pg->descBuf.as<const StreamDesc>(), pg->devNodes, pg->devRecs, reinterpret_cast<float4 *>(pg->nodeBase),
+        pg->recBase, pg->fpn, pg->width);
+    NOMAD_CUDA(ctx, cudaGetLastError());
+    for (uint32_t o : batchObjs) NOMAD_CUDA(ctx, cudaEventRecord(pg->obj[o].copied, pg->copy));
+    pg->anyCopy = true;
   }
   if (!retire.empty()) {
     cudaEvent_t ev;
