@@ -193,6 +193,91 @@ nomad_status nomad_synth_city(uint64_t seed, uint32_t grid, uint32_t grid_z, flo
 nomad_status nomad_scene_owned_desc(const nomad_scene_owned *s, nomad_scene_desc *out);
 void nomad_scene_owned_free(nomad_scene_owned *s);
 
+/* ---- scene ingest: the reference's XML scenes with OBJ/MTL meshes ---- */
+
+/* Scene-level settings of a <Scene> root (SceneLoader::LoadSceneFromXML,
+ * Scene/SceneLoader.cpp:369-687), with the defaults of Scene::clear (Scene/Scene.cpp:70-101)
+ * and ResidencyParameters (Scene/Scene.h). Only the residency parameters of the policies this
+ * library implements are carried. */
+typedef struct nomad_scene_settings {
+  float width, height;              /* screenSize; default 1280 x 720                       */
+  uint32_t max_ray_depth;           /* default 32                                           */
+  int32_t residency_strategy;       /* ResidencyStrategy numbering (Scene/Scene.h:15-26):
+                                       0 DistanceLOD (default), 1 EnergyImportance,
+                                       2 RayHitBudget, 3 ScreenSpaceFootprint, 4 Probabilistic,
+                                       5 AlwaysResident, 6 EnvironmentHit,
+                                       7 PredictiveEnvironment, 8 UnifiedScore, 9 UnifiedNeural */
+  int32_t start_compacted;          /* 0/1                                                  */
+  int32_t restir_enabled;           /* 0/1                                                  */
+  float environment_brightness;     /* default 1                                            */
+  uint32_t reserved;
+  double texture_cap_mb;            /* textureResidencyMemoryCapMB, default 2048            */
+  double geometry_cap_mb;           /* geometryResidencyMemoryCapMB, default 2048           */
+  double total_gpu_cap_mb;          /* totalGpuMemoryCapMB, default 4096                    */
+  uint64_t max_tile_work;           /* maxTileWork / maxTileWorkPerCommand (at least 1);
+                                       default 64 * 64 * 4                                  */
+  /* ResidencyParameters read by DistanceLOD, RayHitBudget and ScreenSpaceFootprint */
+  float lod_enter_distance, lod_exit_distance;          /* 225, 275                    */
+  float lod_enter_view_degrees, lod_exit_view_degrees;  /* 5, 12                       */
+  uint32_t state_cooldown_frames;                       /* residencyCooldown, 5        */
+  uint32_t ray_hit_cooldown_frames;                     /* rayHitCooldown, 4           */
+  uint64_t lod_max_toggles;                             /* lodToggleBudget, 24         */
+  float ray_hit_decay, ray_hit_target_fraction;         /* 0.85, 0.54                  */
+  uint64_t ray_hit_min_active, ray_hit_max_toggles;     /* 16, 16                      */
+  float screen_target_fraction;                         /* screenTargetFraction, 0.68  */
+  float screen_min_pixel_coverage;                      /* screenMinPixelCoverage, 32  */
+  uint64_t screen_min_active, screen_max_toggles;       /* 16, 14                      */
+  float ray_hit_target_memory_mb, screen_target_memory_mb, distance_target_memory_mb;
+  float target_memory_mb, target_resident_geometry_mb;  /* all 0 = not given           */
+  uint32_t reserved2;
+} nomad_scene_settings;
+
+/* <CameraPath><Keyframe …/> (CameraKeyframe, Scene/Scene.h:150-157). */
+typedef struct nomad_camera_keyframe {
+  uint32_t frame;
+  float position[3], look_at[3], up[3];
+  float aperture, focus_distance;
+} nomad_camera_keyframe;
+
+/* <ObserverCamera …/> (ObserverCamera, Scene/Scene.h:159-166). */
+typedef struct nomad_observer_camera {
+  float position[3], look_at[3], up[3];
+  float vertical_fov, aperture, focus_distance;
+} nomad_observer_camera;
+
+typedef struct nomad_loaded_scene nomad_loaded_scene;
+
+typedef struct nomad_loaded_scene_view {
+  nomad_scene_desc scene;             /* primitives in load order, objects as added          */
+  const int32_t *object_mesh_group;   /* [object_count] meshGroupId; -1 for <Sphere>/<Rectangle> */
+  nomad_scene_settings settings;
+  uint32_t keyframe_count;
+  int32_t has_observer;
+  const nomad_camera_keyframe *keyframes;
+  nomad_observer_camera observer;
+  const char *environment_texture;    /* resolved path, "" when none                         */
+  uint32_t mesh_files;                /* distinct OBJ files read                             */
+  uint32_t mesh_files_failed;         /* of which failed to parse (loaded as empty meshes)   */
+  const char *log;                    /* the loader's warnings, one per line                 */
+} nomad_loaded_scene_view;
+
+/* Loads a scene XML and the OBJ/MTL meshes it names into a scene description, like
+ * SceneLoader::LoadSceneFromXML (Scene/SceneLoader.cpp:344-858): <Sphere>, <Rectangle> (with
+ * Euler XYZ `rotation`), <Mesh> (OBJ world-space baked by position + scale/basis + rotation,
+ * material overrides and fallbacks, split into objects by clusterMaxTriangles /
+ * clusterMaxExtent), <CameraPath>, <ObserverCamera> and the root's settings. OBJ and MTL
+ * parsing follows the vendored tinyobjloader 2.0 (triangulation on: quads split on the shorter
+ * diagonal, larger polygons ear-clipped; its own decimal number parser). A mesh file that is
+ * missing or fails to parse contributes no triangles, as in the reference. Distinct OBJ files
+ * are parsed on `threads` host threads (0 = all hardware threads); the result does not depend
+ * on the thread count. Texture images are not decoded: every texture index is -1 (texture
+ * residency is not part of this library).
+ * Returns NOMAD_ERR_INVALID_ARGUMENT when the XML cannot be read or parsed or has no <Scene>
+ * root. */
+nomad_status nomad_scene_load_xml(const char *path, uint32_t threads, nomad_loaded_scene **out);
+nomad_status nomad_loaded_scene_view_get(const nomad_loaded_scene *s, nomad_loaded_scene_view *out);
+void nomad_loaded_scene_free(nomad_loaded_scene *s);
+
 #ifdef __cplusplus
 }
 #endif

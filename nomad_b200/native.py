@@ -46,6 +46,46 @@ class SceneDesc(C.Structure):
                 ("object_prims", C.POINTER(C.c_uint32))]
 
 
+class SceneSettings(C.Structure):
+    """nomad_scene_settings: a <Scene> root's settings (defaults of the reference's Scene)."""
+    _fields_ = [("width", C.c_float), ("height", C.c_float), ("max_ray_depth", C.c_uint32),
+                ("residency_strategy", C.c_int32), ("start_compacted", C.c_int32), ("restir_enabled", C.c_int32),
+                ("environment_brightness", C.c_float), ("reserved", C.c_uint32),
+                ("texture_cap_mb", C.c_double), ("geometry_cap_mb", C.c_double), ("total_gpu_cap_mb", C.c_double),
+                ("max_tile_work", C.c_uint64),
+                ("lod_enter_distance", C.c_float), ("lod_exit_distance", C.c_float),
+                ("lod_enter_view_degrees", C.c_float), ("lod_exit_view_degrees", C.c_float),
+                ("state_cooldown_frames", C.c_uint32), ("ray_hit_cooldown_frames", C.c_uint32),
+                ("lod_max_toggles", C.c_uint64), ("ray_hit_decay", C.c_float), ("ray_hit_target_fraction", C.c_float),
+                ("ray_hit_min_active", C.c_uint64), ("ray_hit_max_toggles", C.c_uint64),
+                ("screen_target_fraction", C.c_float), ("screen_min_pixel_coverage", C.c_float),
+                ("screen_min_active", C.c_uint64), ("screen_max_toggles", C.c_uint64),
+                ("ray_hit_target_memory_mb", C.c_float), ("screen_target_memory_mb", C.c_float),
+                ("distance_target_memory_mb", C.c_float), ("target_memory_mb", C.c_float),
+                ("target_resident_geometry_mb", C.c_float), ("reserved2", C.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("reserved")}
+
+
+class CameraKeyframe(C.Structure):
+    _fields_ = [("frame", C.c_uint32), ("position", C.c_float * 3), ("look_at", C.c_float * 3),
+                ("up", C.c_float * 3), ("aperture", C.c_float), ("focus_distance", C.c_float)]
+
+
+class ObserverCamera(C.Structure):
+    _fields_ = [("position", C.c_float * 3), ("look_at", C.c_float * 3), ("up", C.c_float * 3),
+                ("vertical_fov", C.c_float), ("aperture", C.c_float), ("focus_distance", C.c_float)]
+
+
+class LoadedSceneView(C.Structure):
+    _fields_ = [("scene", SceneDesc), ("object_mesh_group", C.POINTER(C.c_int32)), ("settings", SceneSettings),
+                ("keyframe_count", C.c_uint32), ("has_observer", C.c_int32),
+                ("keyframes", C.POINTER(CameraKeyframe)), ("observer", ObserverCamera),
+                ("environment_texture", C.c_char_p), ("mesh_files", C.c_uint32), ("mesh_files_failed", C.c_uint32),
+                ("log", C.c_char_p)]
+
+
 class SceneBVHView(C.Structure):
     _fields_ = [("prim_count", C.c_uint32), ("object_count", C.c_uint32),
                 ("bvh_node_count", C.c_uint32), ("tlas_node_count", C.c_uint32),
@@ -104,6 +144,9 @@ SIGNATURES = {
                                      C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.POINTER(_P)]),
     "nomad_scene_owned_desc": (C.c_int32, [_P, C.POINTER(SceneDesc)]),
     "nomad_scene_owned_free": (None, [_P]),
+    "nomad_scene_load_xml": (C.c_int32, [C.c_char_p, C.c_uint32, C.POINTER(_P)]),
+    "nomad_loaded_scene_view_get": (C.c_int32, [_P, C.c_void_p]),
+    "nomad_loaded_scene_free": (None, [_P]),
     # nomad_rt.h
     "nomad_create": (C.c_int32, [C.POINTER(Config), C.POINTER(_P)]),
     "nomad_destroy": (C.c_int32, [_P]),
@@ -324,6 +367,48 @@ class HostScene:
                       np.ctypeslib.as_array(d.object_prims, (m,)).copy())
         lib.nomad_scene_owned_free(h)
         return s
+
+
+class LoadedScene(HostScene):
+    """A scene read from the reference's XML format (nomad_scene_load_xml): the scene description
+    plus each object's mesh group, the root's settings, the camera path and the observer camera."""
+
+    def __init__(self, path: str, threads: int = 0):
+        lib = load()
+        h = _P()
+        _check(lib.nomad_scene_load_xml(os.fsencode(path), threads, C.byref(h)))
+        try:
+            v = LoadedSceneView()
+            _check(lib.nomad_loaded_scene_view_get(h, C.byref(v)))
+            d = v.scene
+            n, m = d.prim_count, d.object_count
+
+            def arr(ptr, count, dtype):
+                return np.ctypeslib.as_array(ptr, (count,)).copy() if count else np.zeros(0, dtype)
+
+            super().__init__(arr(d.prim_type, n, np.int32), arr(d.prim_geom, n * 15, np.float32),
+                             arr(d.prim_material, n * 20, np.float32), arr(d.object_first, m, np.uint32),
+                             arr(d.object_prims, m, np.uint32))
+            self.object_mesh_group = arr(v.object_mesh_group, m, np.int32)
+            self.settings = v.settings.as_dict()
+            self.keyframes = [
+                {"frame": k.frame, "position": tuple(k.position), "look_at": tuple(k.look_at), "up": tuple(k.up),
+                 "aperture": k.aperture, "focus_distance": k.focus_distance}
+                for k in (v.keyframes[i] for i in range(v.keyframe_count))]
+            o = v.observer
+            self.observer = ({"position": tuple(o.position), "look_at": tuple(o.look_at), "up": tuple(o.up),
+                              "vertical_fov": o.vertical_fov, "aperture": o.aperture,
+                              "focus_distance": o.focus_distance} if v.has_observer else None)
+            self.environment_texture = (v.environment_texture or b"").decode()
+            self.mesh_files, self.mesh_files_failed = v.mesh_files, v.mesh_files_failed
+            self.log = (v.log or b"").decode()
+        finally:
+            lib.nomad_loaded_scene_free(h)
+
+
+def load_scene_xml(path: str, threads: int = 0) -> LoadedScene:
+    """Reads a scene XML with its OBJ/MTL meshes (the reference's SceneLoader format)."""
+    return LoadedScene(path, threads)
 
 
 def synth_icospheres(seed: int, instances: int = 64, extent: float = 100.0) -> HostScene:
