@@ -3,12 +3,17 @@
 // residency update (updateResidency, RendererResidency.cpp:165-287) and the hit-counter readback
 // that feeds it (processRayHitCounters, Renderer.cpp:8004-8522).
 //
-// Per frame: move the camera along a seeded orbit, render the view (one batched call that
-// replays a captured CUDA graph after the first frame), read the radiance back to the host, then
-// run one device residency step under the chosen policy and byte budget. Prints one JSON line;
-// optionally writes the last frame as a PFM image (little-endian, bottom row first).
+// Per frame: move the camera along a seeded orbit (or along the scene file's camera path), render
+// the view (one batched call that replays a captured CUDA graph after the first frame), read the
+// radiance back to the host, then run one device residency step under the chosen policy and byte
+// budget. Prints one JSON line; optionally writes the last frame as a PFM image (little-endian,
+// bottom row first).
 //
-//   nomad_frame_loop [--scene city|icospheres] [--width W] [--height H] [--spp S] [--depth D]
+// --scene xml:FILE loads one of the reference's scene files (nomad_scene_load_xml); its
+// <CameraPath> keyframes, interpolated linearly by frame number, replace the orbit, and its
+// width, height and maxRayDepth apply unless given on the command line.
+//
+//   nomad_frame_loop [--scene city|icospheres|xml:FILE] [--width W] [--height H] [--spp S] [--depth D]
 //                    [--frames F] [--policy always|rayhit|learned] [--budget FRACTION]
 //                    [--mlp WEIGHTS] [--seed N] [--out FILE.pfm]
 //
@@ -30,6 +35,7 @@ struct Args {
   std::string scene = "city", policy = "always", out, mlp;
   uint32_t width = 640, height = 360, spp = 2, depth = 2, frames = 8, seed = 17;
   float budget = 0.4f;
+  bool widthSet = false, heightSet = false, depthSet = false;
 };
 
 bool parse(int argc, char **argv, Args &a) {
@@ -46,10 +52,10 @@ bool parse(int argc, char **argv, Args &a) {
     else if (k == "--policy") a.policy = next("--policy");
     else if (k == "--out") a.out = next("--out");
     else if (k == "--mlp") a.mlp = next("--mlp");
-    else if (k == "--width") a.width = (uint32_t)std::atoi(next("--width"));
-    else if (k == "--height") a.height = (uint32_t)std::atoi(next("--height"));
+    else if (k == "--width") a.width = (uint32_t)std::atoi(next("--width")), a.widthSet = true;
+    else if (k == "--height") a.height = (uint32_t)std::atoi(next("--height")), a.heightSet = true;
     else if (k == "--spp") a.spp = (uint32_t)std::atoi(next("--spp"));
-    else if (k == "--depth") a.depth = (uint32_t)std::atoi(next("--depth"));
+    else if (k == "--depth") a.depth = (uint32_t)std::atoi(next("--depth")), a.depthSet = true;
     else if (k == "--frames") a.frames = (uint32_t)std::atoi(next("--frames"));
     else if (k == "--seed") a.seed = (uint32_t)std::atoi(next("--seed"));
     else if (k == "--budget") a.budget = (float)std::atof(next("--budget"));
@@ -84,6 +90,20 @@ void orbit(const float bmin[3], const float bmax[3], uint32_t f, float pos[3], f
   look[2] = cz;
 }
 
+// Camera of frame f on a keyframed path: linear between the keyframes around f, clamped at the ends.
+void along_path(const nomad_camera_keyframe *k, uint32_t n, uint32_t f, float pos[3], float look[3], float up[3]) {
+  uint32_t i = 0;
+  while (i + 1 < n && k[i + 1].frame <= f) ++i;
+  const nomad_camera_keyframe &a = k[i], &b = k[i + 1 < n ? i + 1 : i];
+  float t = 0.0f;
+  if (b.frame > a.frame && f > a.frame) t = std::fmin(1.0f, (float)(f - a.frame) / (float)(b.frame - a.frame));
+  for (int c = 0; c < 3; ++c) {
+    pos[c] = a.position[c] + t * (b.position[c] - a.position[c]);
+    look[c] = a.look_at[c] + t * (b.look_at[c] - a.look_at[c]);
+    up[c] = a.up[c] + t * (b.up[c] - a.up[c]);
+  }
+}
+
 }  // namespace
 
 int main(int argc, char **argv) {
@@ -91,16 +111,32 @@ int main(int argc, char **argv) {
   if (!parse(argc, argv, a)) return 2;
   nomad_ctx *ctx = nullptr;
   nomad_scene_owned *scene = nullptr;
+  nomad_loaded_scene *loaded = nullptr;
+  nomad_loaded_scene_view lv;
+  std::memset(&lv, 0, sizeof(lv));
+  nomad_scene_desc desc;
   if (a.scene == "city") {
     CHECK(nomad_synth_city(a.seed, 32, 32, 1000.0f, 600000, 1000, 50000, 32, 0, 1.5f, &scene));
   } else if (a.scene == "icospheres") {
     CHECK(nomad_synth_icospheres(a.seed, 64, 100.0f, &scene));
+  } else if (a.scene.rfind("xml:", 0) == 0) {
+    CHECK(nomad_scene_load_xml(a.scene.c_str() + 4, 0, &loaded));
+    CHECK(nomad_loaded_scene_view_get(loaded, &lv));
+    if (lv.scene.prim_count == 0) {
+      std::fprintf(stderr, "%s holds no primitives\n", a.scene.c_str() + 4);
+      return 2;
+    }
+    if (!a.widthSet) a.width = (uint32_t)lv.settings.width;
+    if (!a.heightSet) a.height = (uint32_t)lv.settings.height;
+    if (!a.depthSet) a.depth = lv.settings.max_ray_depth;
   } else {
     std::fprintf(stderr, "unknown scene %s\n", a.scene.c_str());
     return 2;
   }
-  nomad_scene_desc desc;
-  CHECK(nomad_scene_owned_desc(scene, &desc));
+  if (loaded)
+    desc = lv.scene;
+  else
+    CHECK(nomad_scene_owned_desc(scene, &desc));
   nomad_scenebvh *bvh = nullptr;
   CHECK(nomad_scenebvh_build(&desc, 0, &bvh));
   nomad_scenebvh_view v;
@@ -157,11 +193,13 @@ int main(int argc, char **argv) {
   std::vector<float> radiance(pixels * 3);
   double render_ms = 0.0, step_ms = 0.0;
   nomad_view view;
-  const float up[3] = {0.0f, 1.0f, 0.0f};
   CHECK(nomad_reset_render_stats(ctx));
   for (uint32_t f = 0; f < a.frames; ++f) {
-    float pos[3], look[3];
-    orbit(bmin, bmax, f, pos, look);
+    float pos[3], look[3], up[3] = {0.0f, 1.0f, 0.0f};
+    if (loaded && lv.keyframe_count)
+      along_path(lv.keyframes, lv.keyframe_count, f, pos, look, up);
+    else
+      orbit(bmin, bmax, f, pos, look);
     CHECK(nomad_view_pinhole(pos, look, up, 60.0f, a.width, a.height, &view));
     view.spp = a.spp;
     view.max_depth = a.depth;
@@ -215,6 +253,7 @@ int main(int argc, char **argv) {
       view.first_pixel[2]);
   nomad_destroy(ctx);
   nomad_scenebvh_free(bvh);
-  nomad_scene_owned_free(scene);
+  if (scene) nomad_scene_owned_free(scene);
+  if (loaded) nomad_loaded_scene_free(loaded);
   return status == 0 ? 0 : 1;
 }

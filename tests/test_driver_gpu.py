@@ -61,3 +61,29 @@ def test_driver_budget_policy():
     assert r["status"] == 0
     assert 0.0 < r["resident_fraction"] <= 0.4 + 1e-9
     assert r["render_ms_per_frame"] > 0 and r["rays"] > 0
+
+
+def test_driver_renders_an_ingested_scene_like_the_binding(nb):
+    """--scene xml:FILE: the scene file's camera path and size drive the loop; the last frame equals
+    the binding's render of the same loaded scene and view."""
+    xml = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ingest", "edge.xml")
+    with tempfile.TemporaryDirectory() as d:
+        pfm = os.path.join(d, "last.pfm")
+        r = _run("--scene", "xml:" + xml, "--spp", "1", "--frames", "20", "--policy", "always", "--seed", "5",
+                 "--out", pfm)
+        img = _read_pfm(pfm)
+    s = nb.load_scene_xml(xml)
+    assert r["status"] == 0 and r["prims"] == s.prim_count and r["objects"] == s.object_count
+    assert (r["width"], r["height"], r["depth"]) == (640, 360, 6)
+    sb = nb.SceneBVH(s)
+    ctx = nb.Context(0)
+    try:
+        ctx.upload(sb)
+        v = nb.view_pinhole((0, 0, 10), (0, 0, 0), width=640, height=360)
+        for key in ("camera_pos", "viewport_u", "viewport_v", "first_pixel"):
+            v[key] = np.asarray(r["view"][key], np.float32)
+        v["spp"], v["max_depth"], v["seed_lo"], v["frame"] = 1, 6, 5, r["last_frame"]
+        want = ctx.render(v)[0]
+    finally:
+        ctx.close()
+    assert np.array_equal(img.view(np.int32), want.view(np.int32))
