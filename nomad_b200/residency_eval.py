@@ -280,29 +280,36 @@ def run(paths=200, frames_per_path=8, steps=1500, frames=300, log=print):
         except nat.NomadError as exc:  # a traversal width the paging cannot hold
             out[name] = {"error": str(exc)}
         log(f"{name}: {out[name]}")
+    # The reference's host-side heuristics switch objects and primitives through the residency
+    # interface, which a later device step does not undo: each runs on a fresh context with the
+    # tuned traversal, so no leg sees another's toggles.
+    def host_leg(policy, prm, n_frames):
+        pc = w.context()
+        try:
+            pc.set_traversal(**ctx.traversal())
+            return w.evaluate(pc, judge, policy, frames=n_frames, prm=prm)
+        finally:
+            pc.close()
+
     # The reference's own per-primitive ray-hit policy (host, per primitive, its defaults: 54 %
-    # of the primitives, 16 toggles a frame, cooldowns), on a fresh context and a shorter path.
-    pc = w.context()
-    try:
-        pc.set_traversal(**ctx.traversal())
-        out["ray_hit_per_primitive_reference"] = w.evaluate(
-            pc, judge, nat.POLICY_RAYHIT_PRIM, frames=min(frames, 100),
-            prm=nat.ResidencyParams.make(nat.POLICY_RAYHIT_PRIM, max_toggles=16, camera_motion=0.3, min_active=16))
-    finally:
-        pc.close()
+    # of the primitives, 16 toggles a frame, cooldowns), on a shorter path.
+    out["ray_hit_per_primitive_reference"] = host_leg(
+        nat.POLICY_RAYHIT_PRIM,
+        nat.ResidencyParams.make(nat.POLICY_RAYHIT_PRIM, max_toggles=16, camera_motion=0.3, min_active=16),
+        min(frames, 100))
     log(f"ray_hit_per_primitive_reference: {out['ray_hit_per_primitive_reference']}")
     # The reference's DistanceLOD heuristic with its defaults (225 / 275 m, 5 / 12 degrees, 24
     # toggles a frame), host-side per object.
-    out["distance_lod_reference"] = w.evaluate(
-        ctx, judge, nat.POLICY_DISTANCE_LOD, frames=frames,
-        prm=nat.ResidencyParams.make(nat.POLICY_DISTANCE_LOD, max_toggles=24, camera_motion=0.3))
+    out["distance_lod_reference"] = host_leg(
+        nat.POLICY_DISTANCE_LOD,
+        nat.ResidencyParams.make(nat.POLICY_DISTANCE_LOD, max_toggles=24, camera_motion=0.3), frames)
     log(f"distance_lod_reference: {out['distance_lod_reference']}")
     # The reference's ScreenSpaceFootprint heuristic with its defaults (68 % of the screen, 32 px,
     # 14 primitive toggles a frame), one mesh group per object.
-    out["screen_space_reference"] = w.evaluate(
-        ctx, judge, nat.POLICY_SCREEN_SPACE, frames=frames,
-        prm=nat.ResidencyParams.make(nat.POLICY_SCREEN_SPACE, max_toggles=14, camera_motion=0.3, min_active=16,
-                                     target_fraction=0.68, min_pixel_coverage=32.0))
+    out["screen_space_reference"] = host_leg(
+        nat.POLICY_SCREEN_SPACE,
+        nat.ResidencyParams.make(nat.POLICY_SCREEN_SPACE, max_toggles=14, camera_motion=0.3, min_active=16,
+                                 target_fraction=0.68, min_pixel_coverage=32.0), frames)
     log(f"screen_space_reference: {out['screen_space_reference']}")
     # The learned policy at smaller budgets: the smallest one whose rel-MSE is within 5 % of the
     # ray-hit policy's at the full budget, and its ms/frame.
