@@ -427,6 +427,71 @@ def run_profile_compaction(args):
     print(json.dumps({"profile_compaction": "city 2.48M triangles, 40 % of objects", "nodes": int(outs[0].size // 8)}))
 
 
+def write_obj_scene(scene, folder):
+    """Writes a HostScene's triangles as the reference's scene format: one OBJ file per object
+    (unshared vertices relative to the object's centre, 1-based faces, a material library with
+    a few materials), and a scene XML whose <Mesh> elements place each file at its centre.
+    Returns the XML path and the bytes written."""
+    geom = scene.prim_geom
+    tri = scene.prim_type == 1
+    lines_mtl = []
+    for k in range(4):
+        lines_mtl += [f"newmtl m{k}", f"Kd {0.2 + 0.2 * k:.2f} {0.5:.2f} {0.8 - 0.15 * k:.2f}",
+                      f"Ns {10 * (k + 1)}", ""]
+    total = 0
+    with open(os.path.join(folder, "mats.mtl"), "w") as f:
+        total += f.write("\n".join(lines_mtl))
+    xml = ['<Scene width="1920" height="1080" maxRayDepth="3" residencyStrategy="alwaysresident">',
+           '  <CameraPath><Keyframe frame="0" position="0,220,-620" lookAt="0,0,60"/></CameraPath>']
+    for o in range(scene.object_count):
+        a, n = int(scene.object_first[o]), int(scene.object_prims[o])
+        g = geom[a:a + n][tri[a:a + n]]
+        if g.shape[0] == 0:
+            continue
+        v = g[:, :9].reshape(-1, 3).astype(np.float64)
+        c = v.mean(0)
+        rel = v - c
+        body = ["mtllib mats.mtl", f"o part{o}", f"usemtl m{o % 4}"]
+        body += [f"v {x:.6f} {y:.6f} {z:.6f}" for x, y, z in rel]
+        body += [f"f {3 * i + 1} {3 * i + 2} {3 * i + 3}" for i in range(g.shape[0])]
+        with open(os.path.join(folder, f"obj{o}.obj"), "w") as f:
+            total += f.write("\n".join(body) + "\n")
+        xml.append(f'  <Mesh file="obj{o}.obj" position="{c[0]:.6f},{c[1]:.6f},{c[2]:.6f}" scale="1"/>')
+    xml.append("</Scene>")
+    path = os.path.join(folder, "scene.xml")
+    with open(path, "w") as f:
+        total += f.write("\n".join(xml) + "\n")
+    return path, total
+
+
+def ingest_leg(nb):
+    """Scene ingest (nomad_scene_load_xml): the bench city's generator at 0.6M triangles written
+    as the reference's XML scene format with one OBJ file per object, then read back on all host
+    threads and on one; load
+    time, triangles per second and OBJ text throughput. Parity with the reference's loader is
+    checked by the tests and the oracle's scene recipe, not here."""
+    import tempfile
+
+    scene = nb.synth_city(seed=SEED, target_tris=600_000)
+    with tempfile.TemporaryDirectory() as d:
+        t0 = time.perf_counter()
+        path, nbytes = write_obj_scene(scene, d)
+        write_s = time.perf_counter() - t0
+        out = {"workload": "city (1,024 objects, 0.6M triangles) as 1 XML + one OBJ per object "
+                           "(unshared vertices) + 1 MTL",
+               "bytes": nbytes, "write_s": write_s, "threads": len(os.sched_getaffinity(0))}
+        for name, threads in (("all_threads", 0), ("one_thread", 1)):
+            best = None
+            for _ in range(2 if threads == 0 else 1):
+                t0 = time.perf_counter()
+                s = nb.load_scene_xml(path, threads=threads)
+                dt = time.perf_counter() - t0
+                best = dt if best is None else min(best, dt)
+            out[name] = {"s": best, "mtris_per_s": s.prim_count / best / 1e6, "mb_per_s": nbytes / best / 1e6}
+        out["triangles"], out["objects"], out["obj_files"] = s.prim_count, s.object_count, s.mesh_files
+    return out
+
+
 def select_kernel(ctx, kernel, min_blocks=0):
     """Fixes the traversal to a NOMAD_KERNEL_* variant, optionally with a min_blocks bound."""
     import nomad_b200 as nb
@@ -732,7 +797,8 @@ def main():
                          ("multiview", lambda: multiview_leg(nb, ctx)),
                          ("restir", lambda: restir_leg(nb, ctx)),
                          ("residency", lambda: residency_leg()),
-                         ("compaction", lambda: compaction_leg(nb, sb, primary))):
+                         ("compaction", lambda: compaction_leg(nb, sb, primary)),
+                         ("ingest", lambda: ingest_leg(nb))):
             try:
                 t0 = time.perf_counter()
                 extras[name] = fn()

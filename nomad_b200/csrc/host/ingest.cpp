@@ -34,7 +34,9 @@
 #include <fstream>
 #include <iterator>
 #include <map>
+#include <limits>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <thread>
 #include <unordered_map>
@@ -400,17 +402,6 @@ struct nomad_loaded_scene {
   int32_t hasObserver = 0;
   std::string env, log;
   uint32_t meshFiles = 0, meshFailed = 0;
-
-  void add_object(size_t firstPrim, int grp) {
-    first.push_back(static_cast<uint32_t>(firstPrim));
-    count.push_back(static_cast<uint32_t>(type.size() - firstPrim));
-    group.push_back(grp);
-  }
-  void push(int32_t t, const float *g, const float *m) {
-    type.push_back(t);
-    geom.insert(geom.end(), g, g + 15);
-    mat.insert(mat.end(), m, m + 20);
-  }
 };
 
 namespace {
@@ -495,100 +486,30 @@ void load(const std::string &path, uint32_t threads, nomad_loaded_scene &S) {
     }
   }
 
+  // Every <Sphere>, <Rectangle> and <Mesh> owns a known range of primitives (a mesh's split into
+  // objects only permutes inside its range), so the output is sized first, the elements are baked
+  // and split on the worker threads into their own ranges, and the object lists are joined in
+  // element order: the same arrays for any thread count.
+  struct Part {
+    const XmlElem *e;
+    int kind;  // NOMAD_PRIM_SPHERE / NOMAD_PRIM_RECTANGLE, or -1 for a mesh
+    size_t mesh;
+    int group;
+    size_t base, count;
+    std::vector<std::pair<size_t, size_t>> objs;  // (first, count) relative to base
+  };
+  std::vector<Part> parts;
+  size_t total = 0;
   int nextGroup = 0;
-  const Mat fallback;
-  std::vector<Tri> tris;
-  std::vector<uint32_t> idx;
-  std::vector<std::pair<size_t, size_t>> parts;
   for (const XmlElem &e : root->children) {
-    if (e.name == "Sphere") {
-      float g[15] = {0};
-      put(g, vec3(e.attr("position")));
-      g[3] = f_attr(e, "radius", 1.0f);
-      const Mat m = parse_material(e);
-      const size_t f0 = S.type.size();
-      S.push(NOMAD_PRIM_SPHERE, g, m.v);
-      S.add_object(f0, -1);
-    } else if (e.name == "Rectangle") {
-      F3 c = vec3(e.attr("position")), u = vec3(e.attr("u")), v = vec3(e.attr("v"));
-      if (const char *r = e.attr("rotation")) {
-        const F3 rad = mul(vec3(r), kDegToRad);
-        u = rotate_xyz(u, rad);
-        v = rotate_xyz(v, rad);
-      }
-      float g[15] = {0};
-      put(g, c);
-      put(g + 3, u);
-      put(g + 6, v);
-      const Mat m = parse_material(e);
-      const size_t f0 = S.type.size();
-      S.push(NOMAD_PRIM_RECTANGLE, g, m.v);
-      S.add_object(f0, -1);
+    if (e.name == "Sphere" || e.name == "Rectangle") {
+      parts.push_back({&e, e.name == "Sphere" ? NOMAD_PRIM_SPHERE : NOMAD_PRIM_RECTANGLE, 0, -1, total, 1, {}});
+      total += 1;
     } else if (e.name == "Mesh") {
-      const Mesh &mesh = meshes[fileIndex.at(mesh_path(e))];
-      const F3 pos = vec3(e.attr("position"));
-      const float scale = f_attr(e, "scale", 1.0f);
-      F3 bx{scale, 0.0f, 0.0f}, by{0.0f, scale, 0.0f}, bz{0.0f, 0.0f, scale};
-      F3 rotDeg{0.0f, 0.0f, 0.0f};
-      if (const char *a = e.attr("rotation")) rotDeg = vec3(a);
-      if (const char *a = e.attr("basisX")) bx = vec3(a);
-      if (const char *a = e.attr("basisY")) by = vec3(a);
-      if (const char *a = e.attr("basisZ")) bz = vec3(a);
-      if (rotDeg.x != 0.0f || rotDeg.y != 0.0f || rotDeg.z != 0.0f) {
-        const F3 rad = mul(rotDeg, kDegToRad);
-        bx = rotate_xyz(bx, rad);
-        by = rotate_xyz(by, rad);
-        bz = rotate_xyz(bz, rad);
-      }
-      const Mat over = parse_material(e);
-      const bool explicitOver = has_override(e);
-      const uint64_t maxTris = u64_attr(e, "clusterMaxTriangles", 0);
-      const float maxExtent = f_attr(e, "clusterMaxExtent", 0.0f);
-      auto bake = [&](uint32_t vi) {
-        const float *p = &mesh.vertices[3 * static_cast<size_t>(vi)];
-        return add(add(add(pos, mul(bx, p[0])), mul(by, p[1])), mul(bz, p[2]));
-      };
-      const size_t nt = mesh.triMat.size();
-      tris.resize(nt);
-      for (size_t t = 0; t < nt; ++t) {
-        Tri &T = tris[t];
-        T.v0 = bake(mesh.tris[3 * t]);
-        T.v1 = bake(mesh.tris[3 * t + 1]);
-        T.v2 = bake(mesh.tris[3 * t + 2]);
-        std::memcpy(T.uv, &mesh.uvs[6 * t], sizeof(T.uv));
-        const Mat *chosen = &over;
-        bool usingOver = true;
-        const int mid = mesh.triMat[t];
-        if (mid >= 0 && static_cast<size_t>(mid) < mesh.materials.size()) {
-          chosen = &mesh.materials[mid];
-          usingOver = false;
-        }
-        const bool allowFallback = !(usingOver && explicitOver);
-        if (allowFallback && (mid < 0 || needs_fallback(*chosen))) chosen = &fallback;
-        T.mat = chosen;
-      }
-      const int grp = nextGroup++;
-      if (nt == 0) continue;
-      idx.resize(nt);
-      for (size_t t = 0; t < nt; ++t) idx[t] = static_cast<uint32_t>(t);
-      parts.clear();
-      if ((maxTris == 0 && maxExtent <= 0.0f) || nt <= 1)
-        parts.emplace_back(0, nt);
-      else
-        partition(tris, idx, 0, nt, maxTris, maxExtent, parts);
-      for (const auto &pr : parts) {
-        const size_t f0 = S.type.size();
-        for (size_t k = pr.first; k < pr.second; ++k) {
-          const Tri &T = tris[idx[k]];
-          float g[15];
-          put(g, T.v0);
-          put(g + 3, T.v1);
-          put(g + 6, T.v2);
-          std::memcpy(g + 9, T.uv, sizeof(T.uv));
-          S.push(NOMAD_PRIM_TRIANGLE, g, T.mat->v);
-        }
-        S.add_object(f0, grp);
-      }
+      const size_t m = fileIndex.at(mesh_path(e));
+      const size_t nt = meshes[m].triMat.size();
+      parts.push_back({&e, -1, m, nextGroup++, total, nt, {}});
+      total += nt;
     } else if (e.name == "CameraPath") {
       for (const XmlElem &k : e.children) {
         if (k.name != "Keyframe") continue;
@@ -613,6 +534,132 @@ void load(const std::string &path, uint32_t threads, nomad_loaded_scene &S) {
       S.hasObserver = 1;
     }
   }
+  S.type.resize(total);
+  S.geom.resize(total * 15);
+  S.mat.resize(total * 20);
+
+  const Mat fallback;
+  auto emit = [&](Part &P, std::vector<Tri> &tris, std::vector<uint32_t> &idx) {
+    const XmlElem &e = *P.e;
+    int32_t *type = S.type.data() + P.base;
+    float *geom = S.geom.data() + 15 * P.base;
+    float *mat = S.mat.data() + 20 * P.base;
+    if (P.kind == NOMAD_PRIM_SPHERE) {
+      std::memset(geom, 0, 15 * sizeof(float));
+      put(geom, vec3(e.attr("position")));
+      geom[3] = f_attr(e, "radius", 1.0f);
+      std::memcpy(mat, parse_material(e).v, 20 * sizeof(float));
+      type[0] = NOMAD_PRIM_SPHERE;
+      P.objs.emplace_back(0, 1);
+      return;
+    }
+    if (P.kind == NOMAD_PRIM_RECTANGLE) {
+      F3 c = vec3(e.attr("position")), u = vec3(e.attr("u")), v = vec3(e.attr("v"));
+      if (const char *r = e.attr("rotation")) {
+        const F3 rad = mul(vec3(r), kDegToRad);
+        u = rotate_xyz(u, rad);
+        v = rotate_xyz(v, rad);
+      }
+      std::memset(geom, 0, 15 * sizeof(float));
+      put(geom, c);
+      put(geom + 3, u);
+      put(geom + 6, v);
+      std::memcpy(mat, parse_material(e).v, 20 * sizeof(float));
+      type[0] = NOMAD_PRIM_RECTANGLE;
+      P.objs.emplace_back(0, 1);
+      return;
+    }
+    const Mesh &mesh = meshes[P.mesh];
+    const F3 pos = vec3(e.attr("position"));
+    const float scale = f_attr(e, "scale", 1.0f);
+    F3 bx{scale, 0.0f, 0.0f}, by{0.0f, scale, 0.0f}, bz{0.0f, 0.0f, scale};
+    F3 rotDeg{0.0f, 0.0f, 0.0f};
+    if (const char *a = e.attr("rotation")) rotDeg = vec3(a);
+    if (const char *a = e.attr("basisX")) bx = vec3(a);
+    if (const char *a = e.attr("basisY")) by = vec3(a);
+    if (const char *a = e.attr("basisZ")) bz = vec3(a);
+    if (rotDeg.x != 0.0f || rotDeg.y != 0.0f || rotDeg.z != 0.0f) {
+      const F3 rad = mul(rotDeg, kDegToRad);
+      bx = rotate_xyz(bx, rad);
+      by = rotate_xyz(by, rad);
+      bz = rotate_xyz(bz, rad);
+    }
+    const Mat over = parse_material(e);
+    const bool explicitOver = has_override(e);
+    const uint64_t maxTris = u64_attr(e, "clusterMaxTriangles", 0);
+    const float maxExtent = f_attr(e, "clusterMaxExtent", 0.0f);
+    auto bake = [&](uint32_t vi) {
+      const float *p = &mesh.vertices[3 * static_cast<size_t>(vi)];
+      return add(add(add(pos, mul(bx, p[0])), mul(by, p[1])), mul(bz, p[2]));
+    };
+    const size_t nt = P.count;
+    if (nt == 0) return;
+    tris.resize(nt);
+    for (size_t t = 0; t < nt; ++t) {
+      Tri &T = tris[t];
+      T.v0 = bake(mesh.tris[3 * t]);
+      T.v1 = bake(mesh.tris[3 * t + 1]);
+      T.v2 = bake(mesh.tris[3 * t + 2]);
+      std::memcpy(T.uv, &mesh.uvs[6 * t], sizeof(T.uv));
+      const Mat *chosen = &over;
+      bool usingOver = true;
+      const int mid = mesh.triMat[t];
+      if (mid >= 0 && static_cast<size_t>(mid) < mesh.materials.size()) {
+        chosen = &mesh.materials[mid];
+        usingOver = false;
+      }
+      const bool allowFallback = !(usingOver && explicitOver);
+      if (allowFallback && (mid < 0 || needs_fallback(*chosen))) chosen = &fallback;
+      T.mat = chosen;
+    }
+    idx.resize(nt);
+    for (size_t t = 0; t < nt; ++t) idx[t] = static_cast<uint32_t>(t);
+    if ((maxTris == 0 && maxExtent <= 0.0f) || nt <= 1)
+      P.objs.emplace_back(0, nt);
+    else
+      partition(tris, idx, 0, nt, maxTris, maxExtent, P.objs);
+    for (size_t k = 0; k < nt; ++k) {
+      const Tri &T = tris[idx[k]];
+      float *g = geom + 15 * k;
+      put(g, T.v0);
+      put(g + 3, T.v1);
+      put(g + 6, T.v2);
+      std::memcpy(g + 9, T.uv, sizeof(T.uv));
+      std::memcpy(mat + 20 * k, T.mat->v, 20 * sizeof(float));
+      type[k] = NOMAD_PRIM_TRIANGLE;
+    }
+    // partition() reports [begin, end) pairs; keep (first, count)
+    for (auto &o : P.objs) o.second -= o.first;
+  };
+  {
+    unsigned nt = threads ? threads : std::max(1u, std::thread::hardware_concurrency());
+    nt = static_cast<unsigned>(std::max<size_t>(1, std::min<size_t>(nt, parts.size())));
+    std::atomic<size_t> next{0};
+    std::exception_ptr failure;
+    std::mutex failureLock;
+    auto work = [&]() {
+      std::vector<Tri> tris;
+      std::vector<uint32_t> idx;
+      try {
+        for (size_t i; (i = next.fetch_add(1)) < parts.size();) emit(parts[i], tris, idx);
+      } catch (...) {
+        std::lock_guard<std::mutex> g(failureLock);
+        if (!failure) failure = std::current_exception();
+        next.store(parts.size());
+      }
+    };
+    std::vector<std::thread> pool;
+    for (unsigned t = 1; t < nt; ++t) pool.emplace_back(work);
+    work();
+    for (auto &t : pool) t.join();
+    if (failure) std::rethrow_exception(failure);
+  }
+  for (const Part &P : parts)
+    for (const auto &o : P.objs) {
+      S.first.push_back(static_cast<uint32_t>(P.base + o.first));
+      S.count.push_back(static_cast<uint32_t>(o.second));
+      S.group.push_back(P.group);
+    }
 }
 
 void default_observer(nomad_observer_camera &o) {
