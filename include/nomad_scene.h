@@ -275,6 +275,9 @@ typedef struct nomad_loaded_scene_view {
  * Returns NOMAD_ERR_INVALID_ARGUMENT when the XML cannot be read or parsed or has no <Scene>
  * root. */
 nomad_status nomad_scene_load_xml(const char *path, uint32_t threads, nomad_loaded_scene **out);
+/* Why the calling thread's last failed nomad_scene_load_xml failed ("" after a success); valid
+ * until the thread's next call. */
+const char *nomad_scene_last_error(void);
 nomad_status nomad_loaded_scene_view_get(const nomad_loaded_scene *s, nomad_loaded_scene_view *out);
 void nomad_loaded_scene_free(nomad_loaded_scene *s);
 

@@ -672,8 +672,18 @@ void default_observer(nomad_observer_camera &o) {
 
 }  // namespace
 
+namespace {
+thread_local std::string tLastError;
+}
+
+extern "C" const char *nomad_scene_last_error(void) { return tLastError.c_str(); }
+
 extern "C" nomad_status nomad_scene_load_xml(const char *path, uint32_t threads, nomad_loaded_scene **out) {
-  if (!path || !out) return NOMAD_ERR_INVALID_ARGUMENT;
+  tLastError.clear();
+  if (!path || !out) {
+    tLastError = "path and out must not be null";
+    return NOMAD_ERR_INVALID_ARGUMENT;
+  }
   *out = nullptr;
   try {
     std::unique_ptr<nomad_loaded_scene> s(new nomad_loaded_scene());
@@ -682,8 +692,10 @@ extern "C" nomad_status nomad_scene_load_xml(const char *path, uint32_t threads,
     *out = s.release();
     return NOMAD_OK;
   } catch (const std::bad_alloc &) {
+    tLastError = "out of host memory";
     return NOMAD_ERR_OUT_OF_MEMORY;
-  } catch (const std::exception &) {
+  } catch (const std::exception &e) {
+    tLastError = e.what();
     return NOMAD_ERR_INVALID_ARGUMENT;
   }
 }

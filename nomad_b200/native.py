@@ -147,6 +147,7 @@ SIGNATURES = {
     "nomad_scene_load_xml": (C.c_int32, [C.c_char_p, C.c_uint32, C.POINTER(_P)]),
     "nomad_loaded_scene_view_get": (C.c_int32, [_P, C.c_void_p]),
     "nomad_loaded_scene_free": (None, [_P]),
+    "nomad_scene_last_error": (C.c_char_p, []),
     # nomad_rt.h
     "nomad_create": (C.c_int32, [C.POINTER(Config), C.POINTER(_P)]),
     "nomad_destroy": (C.c_int32, [_P]),
@@ -376,7 +377,9 @@ class LoadedScene(HostScene):
     def __init__(self, path: str, threads: int = 0):
         lib = load()
         h = _P()
-        _check(lib.nomad_scene_load_xml(os.fsencode(path), threads, C.byref(h)))
+        st = lib.nomad_scene_load_xml(os.fsencode(path), threads, C.byref(h))
+        if st != NOMAD_OK:
+            raise NomadError(st, (lib.nomad_scene_last_error() or b"").decode())
         try:
             v = LoadedSceneView()
             _check(lib.nomad_loaded_scene_view_get(h, C.byref(v)))

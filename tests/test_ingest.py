@@ -84,8 +84,9 @@ def test_rejected_documents(nb):
     with open(os.path.join(GOLDEN, "rejected.json")) as f:
         rejected = json.load(f)
     assert sorted(rejected) == ["broken.xml", "noscene.xml"]
+    why = {"broken.xml": "mismatched end tag", "noscene.xml": "no <Scene> root", "does_not_exist.xml": "cannot read"}
     for name in rejected + ["does_not_exist.xml"]:
-        with pytest.raises(nb.NomadError):
+        with pytest.raises(nb.NomadError, match=why[name]):
             nb.load_scene_xml(os.path.join(GOLDEN, name))
 
 
