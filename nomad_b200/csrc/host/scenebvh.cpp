@@ -439,6 +439,31 @@ void pack_prims(const nomad_scene_desc &d, SceneBVHData &out, uint32_t threads) 
   for (auto &t : pool) t.join();
 }
 
+// Runs fn(lo, hi) over [0, n) in chunks on up to `threads` host threads (0 = all); each index is
+// visited by exactly one call, so work that writes only its own indices gives the same result
+// for any thread count.
+template <class F>
+static void parallel_chunks(size_t n, size_t chunk, uint32_t threads, F &&fn) {
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t nt = std::min<size_t>(threads ? threads : hw, (n + chunk - 1) / chunk);
+  if (nt <= 1) {
+    if (n) fn(size_t(0), n);
+    return;
+  }
+  std::atomic<size_t> next{0};
+  auto worker = [&]() {
+    for (;;) {
+      const size_t lo = next.fetch_add(chunk);
+      if (lo >= n) break;
+      fn(lo, std::min(n, lo + chunk));
+    }
+  };
+  std::vector<std::thread> pool;
+  for (size_t t = 1; t < nt; ++t) pool.emplace_back(worker);
+  worker();
+  for (auto &t : pool) t.join();
+}
+
 nomad_status scenebvh_validate(const nomad_scene_desc *d) {
   if (!d || d->prim_count == 0 || d->object_count == 0) return NOMAD_ERR_INVALID_ARGUMENT;
   if (!d->prim_type || !d->prim_geom || !d->prim_material || !d->object_first ||
@@ -451,15 +476,17 @@ nomad_status scenebvh_validate(const nomad_scene_desc *d) {
     expect += d->object_prims[o];
   }
   if (expect != d->prim_count) return NOMAD_ERR_SCENE_INVALID;
-  for (uint32_t i = 0; i < d->prim_count; ++i) {
-    int t = d->prim_type[i];
-    if (t != NOMAD_PRIM_SPHERE && t != NOMAD_PRIM_TRIANGLE && t != NOMAD_PRIM_RECTANGLE)
-      return NOMAD_ERR_SCENE_INVALID;
-    const float *g = d->prim_geom + (size_t)i * NOMAD_PRIM_GEOM_FLOATS;
-    for (int k = 0; k < 9; ++k)
-      if (!std::isfinite(g[k])) return NOMAD_ERR_SCENE_INVALID;
-  }
-  return NOMAD_OK;
+  std::atomic<bool> bad{false};
+  parallel_chunks(d->prim_count, 1 << 16, 0, [&](size_t lo, size_t hi) {
+    for (size_t i = lo; i < hi && !bad.load(std::memory_order_relaxed); ++i) {
+      int t = d->prim_type[i];
+      bool ok = t == NOMAD_PRIM_SPHERE || t == NOMAD_PRIM_TRIANGLE || t == NOMAD_PRIM_RECTANGLE;
+      const float *g = d->prim_geom + i * NOMAD_PRIM_GEOM_FLOATS;
+      for (int k = 0; k < 9 && ok; ++k) ok = std::isfinite(g[k]);
+      if (!ok) bad.store(true, std::memory_order_relaxed);
+    }
+  });
+  return bad.load() ? NOMAD_ERR_SCENE_INVALID : NOMAD_OK;
 }
 
 static nomad_status build_impl(const nomad_scene_desc *d, uint32_t threads, SceneBVHData &out) {
@@ -508,53 +535,69 @@ nomad_status scenebvh_finish(const nomad_scene_desc *d, std::vector<BlasResult> 
                              uint32_t threads) {
   const size_t n = d->prim_count;
   const size_t nobj = d->object_count;
-  for (BlasResult &r : results) {
-    if (r.root < 0) continue;
-    // depth of this BLAS (iterative, nodes only)
-    std::vector<std::pair<int, uint32_t>> st{{r.root, 1u}};
-    uint32_t depth = 0;
-    while (!st.empty()) {
-      auto [ni, dd] = st.back();
-      st.pop_back();
-      depth = std::max(depth, dd);
-      const BNode &nd = r.nodes[ni];
-      if (nd.count <= 0) {
-        st.push_back({nd.leftFirst, dd + 1});
-        st.push_back({-nd.count, dd + 1});
+  // depth of every BLAS (iterative, nodes only), one object per task
+  parallel_chunks(nobj, 16, threads, [&](size_t lo, size_t hi) {
+    std::vector<std::pair<int, uint32_t>> st;
+    for (size_t o = lo; o < hi; ++o) {
+      BlasResult &r = results[o];
+      if (r.root < 0) continue;
+      st.assign(1, {r.root, 1u});
+      uint32_t depth = 0;
+      while (!st.empty()) {
+        auto [ni, dd] = st.back();
+        st.pop_back();
+        depth = std::max(depth, dd);
+        const BNode &nd = r.nodes[ni];
+        if (nd.count <= 0) {
+          st.push_back({nd.leftFirst, dd + 1});
+          st.push_back({-nd.count, dd + 1});
+        }
       }
+      r.depth = depth;
     }
-    r.depth = depth;
-  }
+  });
 
-  // Concatenate with rebased children (SceneBVH.cpp:117-150).
-  std::vector<BNode> all;
+  // Concatenation with rebased children (SceneBVH.cpp:117-150): each object's nodes go to
+  // [base, base + size) of the packed array, base the node count of the objects before it.
+  std::vector<size_t> base(nobj, 0);
   size_t total = 0;
-  for (auto &r : results) total += r.nodes.size();
+  for (size_t o = 0; o < nobj; ++o) {
+    base[o] = total;
+    if (results[o].root >= 0) total += results[o].nodes.size();
+  }
   if (total > 0x7fffffffu) return NOMAD_ERR_LIMIT;
-  all.reserve(total);
   std::vector<int32_t> blasRoot(nobj, -1);
-  const float fmax = std::numeric_limits<float>::max();
   std::vector<V3> objMin(nobj, V3(0.0f)), objMax(nobj, V3(0.0f));
   std::vector<int64_t> objIdx;
   for (size_t o = 0; o < nobj; ++o) {
     const BlasResult &r = results[o];
     if (r.root < 0) continue;
-    int32_t base = static_cast<int32_t>(all.size());
-    for (BNode nd : r.nodes) {
-      if (nd.count < 0) {
-        int32_t l = nd.leftFirst + base;
-        int32_t rr = -nd.count + base;
-        nd.leftFirst = l;
-        nd.count = -rr;
-      }
-      all.push_back(nd);
-    }
-    blasRoot[o] = base + r.root;
+    blasRoot[o] = static_cast<int32_t>(base[o]) + r.root;
     objMin[o] = r.nodes[r.root].mn;
     objMax[o] = r.nodes[r.root].mx;
     objIdx.push_back(static_cast<int64_t>(o));
   }
-  (void)fmax;
+  out.bvh.resize(total * 8);
+  parallel_chunks(nobj, 4, threads, [&](size_t lo, size_t hi) {
+    for (size_t o = lo; o < hi; ++o) {
+      const BlasResult &r = results[o];
+      if (r.root < 0) continue;
+      const int32_t b = static_cast<int32_t>(base[o]);
+      float *p = out.bvh.data() + base[o] * 8;
+      for (const BNode &nd : r.nodes) {
+        int32_t lf = nd.leftFirst, cnt = nd.count;
+        if (cnt < 0) {
+          lf += b;
+          cnt = -(-cnt + b);
+        }
+        p[0] = nd.mn.x; p[1] = nd.mn.y; p[2] = nd.mn.z;
+        p[3] = int_bits_as_float(lf);
+        p[4] = nd.mx.x; p[5] = nd.mx.y; p[6] = nd.mx.z;
+        p[7] = int_bits_as_float(cnt);
+        p += 8;
+      }
+    }
+  });
 
   TlasBuilder tb{objMin, objMax, objIdx, {}};
   if (!objIdx.empty()) tb.build(0, objIdx.size());
@@ -579,14 +622,6 @@ nomad_status scenebvh_finish(const nomad_scene_desc *d, std::vector<BlasResult> 
   out.primCount = static_cast<uint32_t>(n);
   out.objectCount = static_cast<uint32_t>(nobj);
   out.maxDepth = maxDepth;
-  out.bvh.resize(all.size() * 8);
-  for (size_t i = 0; i < all.size(); ++i) {
-    float *p = out.bvh.data() + i * 8;
-    p[0] = all[i].mn.x; p[1] = all[i].mn.y; p[2] = all[i].mn.z;
-    p[3] = int_bits_as_float(all[i].leftFirst);
-    p[4] = all[i].mx.x; p[5] = all[i].mx.y; p[6] = all[i].mx.z;
-    p[7] = int_bits_as_float(all[i].count);
-  }
   out.tlas.resize(tb.nodes.size() * 8);
   for (size_t i = 0; i < tb.nodes.size(); ++i) {
     float *p = out.tlas.data() + i * 8;
@@ -594,8 +629,7 @@ nomad_status scenebvh_finish(const nomad_scene_desc *d, std::vector<BlasResult> 
     p[0] = t.mn.x; p[1] = t.mn.y; p[2] = t.mn.z; p[3] = int_bits_as_float(t.left);
     p[4] = t.mx.x; p[5] = t.mx.y; p[6] = t.mx.z; p[7] = int_bits_as_float(t.right);
   }
-  out.primIndices.resize(n);
-  for (size_t i = 0; i < n; ++i) out.primIndices[i] = indices[i];
+  out.primIndices.assign(indices.begin(), indices.begin() + static_cast<std::ptrdiff_t>(n));
   out.instances.resize(nobj);
   out.objBounds.resize(nobj * 6);
   for (size_t o = 0; o < nobj; ++o) {
