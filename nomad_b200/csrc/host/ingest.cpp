@@ -459,21 +459,31 @@ void load(const std::string &path, uint32_t threads, nomad_loaded_scene &S) {
     unsigned nt = threads ? threads : std::max(1u, std::thread::hardware_concurrency());
     nt = static_cast<unsigned>(std::min<size_t>(nt, files.size()));
     std::atomic<size_t> next{0};
+    std::exception_ptr failure;
+    std::mutex failureLock;
     auto work = [&]() {
-      for (size_t i; (i = next.fetch_add(1)) < files.size();) {
-        const fs::path p(files[i]);
-        std::string dir;
-        if (p.has_parent_path()) {
-          dir = p.parent_path().string();
-          if (!dir.empty() && dir.back() != fs::path::preferred_separator) dir.push_back(fs::path::preferred_separator);
+      try {
+        for (size_t i; (i = next.fetch_add(1)) < files.size();) {
+          const fs::path p(files[i]);
+          std::string dir;
+          if (p.has_parent_path()) {
+            dir = p.parent_path().string();
+            if (!dir.empty() && dir.back() != fs::path::preferred_separator)
+              dir.push_back(fs::path::preferred_separator);
+          }
+          load_obj(files[i], dir, meshes[i]);
         }
-        load_obj(files[i], dir, meshes[i]);
+      } catch (...) {  // handed to the calling thread, which turns it into a status
+        std::lock_guard<std::mutex> g(failureLock);
+        if (!failure) failure = std::current_exception();
+        next.store(files.size());
       }
     };
     std::vector<std::thread> pool;
     for (unsigned t = 1; t < nt; ++t) pool.emplace_back(work);
     work();
     for (auto &t : pool) t.join();
+    if (failure) std::rethrow_exception(failure);
   }
   S.meshFiles = static_cast<uint32_t>(files.size());
   for (size_t i = 0; i < files.size(); ++i) {

@@ -1,5 +1,5 @@
 // A small XML reader for scene files: elements, attributes, comments, processing instructions,
-// CDATA and DOCTYPE (the last three skipped). It accepts what the reference's vendored tinyxml2
+// CDATA and DOCTYPE (the last three skipped), elements nested at most 500 deep. It accepts what the reference's vendored tinyxml2
 // accepts for scene documents and reports mismatched or unclosed tags and malformed attributes.
 // Attribute values get tinyxml2's treatment: the five predefined entities and numeric character
 // references decoded (an unknown entity is kept as written), line endings normalised to "\n".
@@ -97,9 +97,13 @@ std::string decode(const char *s, size_t n) {
   return o;
 }
 
+// Deepest element nesting accepted (tinyxml2 rejects documents nested deeper than 500).
+constexpr int kMaxDepth = 500;
+
 struct Reader {
   const std::string &t;
   size_t p = 0;
+  int depth = 0;
   std::string &err;
   Reader(const std::string &text, std::string &e) : t(text), err(e) {}
 
@@ -127,6 +131,13 @@ struct Reader {
 
   // After '<' of a start tag.
   bool element(XmlElem &e) {
+    if (++depth > kMaxDepth) return fail("elements nested too deeply");
+    const bool ok = element_body(e);
+    --depth;
+    return ok;
+  }
+
+  bool element_body(XmlElem &e) {
     if (!name(e.name)) return fail("bad element name");
     for (;;) {
       skip_ws();

@@ -90,6 +90,17 @@ def test_rejected_documents(nb):
             nb.load_scene_xml(os.path.join(GOLDEN, name))
 
 
+def test_deep_nesting_is_rejected_not_crashed(nb, tmp_path):
+    """Nesting deeper than 500 elements is refused with a message (the reader is recursive)."""
+    deep = tmp_path / "deep.xml"
+    deep.write_text("<Scene>" + "<a>" * 20000 + "</a>" * 20000 + "</Scene>")
+    with pytest.raises(nb.NomadError, match="nested too deeply"):
+        nb.load_scene_xml(str(deep))
+    ok = tmp_path / "ok.xml"
+    ok.write_text("<Scene>" + "<a>" * 400 + "</a>" * 400 + '<Sphere position="0,0,0"/></Scene>')
+    assert nb.load_scene_xml(str(ok)).prim_count == 1
+
+
 def test_thread_count_does_not_change_the_result(nb):
     path = os.path.join(GOLDEN, "edge.xml")
     a, b = nb.load_scene_xml(path, threads=1), nb.load_scene_xml(path, threads=7)
