@@ -390,6 +390,13 @@ nomad_status nomad_object_bytes(nomad_ctx *ctx, uint64_t *out);
 nomad_status nomad_residency_last(nomad_ctx *ctx, float *features, float *scores);
 /* Current residency of each object (object_count bytes, 1 = resident). */
 nomad_status nomad_residency_flags(nomad_ctx *ctx, uint8_t *out);
+/* NOMAD_POLICY_LEARNED falls back to NOMAD_POLICY_RAYHIT_BUDGET (the same step with the same
+ * parameters) whenever the context holds no usable model: none initialised, set, trained or
+ * loaded yet, or the last nomad_mlp_set / nomad_mlp_load was rejected. The north star's fallback
+ * for a model that fails to load, in place of the reference's heuristic unified score
+ * (RendererUnifiedNeural.cpp:402-417). *out receives the number of steps that fell back since
+ * the scene was uploaded. */
+nomad_status nomad_residency_fallback_steps(nomad_ctx *ctx, uint64_t *out);
 
 /* ---- geometry paging (the Cold -> Streaming -> Resident lifecycle of per-object GPU
  *      resources, Renderer.h:63-106, ensureResident Renderer.cpp:613-650, the per-frame onload
@@ -458,7 +465,19 @@ nomad_status nomad_mlp_infer(nomad_ctx *ctx, const float *features, uint64_t n, 
 /* Model blob (NOMAD_MLP_PARAMS floats): W1[128][32] (inputs padded to 32), b1, W2[128][128],
  * b2, w3[128], b3, feature mean[24], feature inverse std[24]. Checkpoint and restore. */
 nomad_status nomad_mlp_get(nomad_ctx *ctx, float *out);
+/* A blob with a non-finite value is rejected (NOMAD_ERR_INVALID_ARGUMENT) and leaves the context
+ * without a usable model, so learned steps fall back to the ray-hit budget until a valid one is
+ * set. */
 nomad_status nomad_mlp_set(nomad_ctx *ctx, const float *in);
+/* The model as a versioned file (the checkpoint the reference keeps as a JSON model file,
+ * export_unified_neural_model.py): "NMLP", format version 1, NOMAD_MLP_PARAMS and NOMAD_FEATURES
+ * (uint32 little-endian each), the blob (float32 little-endian), then a 64-bit FNV-1a checksum
+ * of everything before it. nomad_mlp_load checks every field, the size, the checksum and that
+ * every value is finite; on any failure it returns NOMAD_ERR_INVALID_ARGUMENT with the reason
+ * in nomad_last_error and leaves the context without a usable model (learned steps then fall
+ * back to the ray-hit budget). */
+nomad_status nomad_mlp_save(nomad_ctx *ctx, const char *path);
+nomad_status nomad_mlp_load(nomad_ctx *ctx, const char *path);
 
 /* ---- allocation-free closest hit (no counterpart in the reference) ----------------------
  * For callers that cannot allocate GPU memory while tracing: a frame loop whose memory budget

@@ -12,7 +12,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
+#include <string>
 #include <numeric>
 #include <random>
 #include <vector>
@@ -676,10 +678,19 @@ extern "C" nomad_status nomad_mlp_get(nomad_ctx *ctx, float *out) {
   return NOMAD_OK;
 }
 
+bool nomad_mlp_ready(nomad_ctx *ctx) { return ctx->mlp && static_cast<MlpState *>(ctx->mlp)->ready; }
+
 extern "C" nomad_status nomad_mlp_set(nomad_ctx *ctx, const float *in) {
   if (!ctx || !in) return NOMAD_ERR_INVALID_ARGUMENT;
   NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
   MlpState &S = mlp(ctx);
+  for (int i = 0; i < kParams; ++i)
+    if (!std::isfinite(in[i])) {
+      S.ready = false;
+      return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT,
+                        "model parameter " + std::to_string(i) +
+                            " is not finite; learned steps fall back to the ray-hit budget");
+    }
   nomad_status st = ensure(ctx, S);
   if (st != NOMAD_OK) return st;
   NOMAD_CUDA(ctx, cudaMemcpy(S.P.p, in, kParams * 4, cudaMemcpyHostToDevice));
@@ -690,6 +701,95 @@ extern "C" nomad_status nomad_mlp_set(nomad_ctx *ctx, const float *in) {
   S.ready = true;
   NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return NOMAD_OK;
+}
+
+namespace {
+constexpr uint32_t kModelVersion = 1;
+constexpr size_t kModelHeader = 16;  // magic, version, parameter count, feature count
+
+uint64_t fnv1a(const unsigned char *p, size_t n) {
+  uint64_t h = 1469598103934665603ull;
+  for (size_t i = 0; i < n; ++i) {
+    h ^= p[i];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+void put_u32(unsigned char *p, uint32_t v) {
+  for (int k = 0; k < 4; ++k) p[k] = static_cast<unsigned char>(v >> (8 * k));
+}
+
+uint32_t get_u32(const unsigned char *p) {
+  return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
+}
+}  // namespace
+
+extern "C" nomad_status nomad_mlp_save(nomad_ctx *ctx, const char *path) {
+  if (!ctx || !path) return NOMAD_ERR_INVALID_ARGUMENT;
+  std::vector<float> p(kParams);
+  nomad_status st = nomad_mlp_get(ctx, p.data());
+  if (st != NOMAD_OK) return st;
+  std::vector<unsigned char> buf(kModelHeader + (size_t)kParams * 4 + 8);
+  std::memcpy(buf.data(), "NMLP", 4);
+  put_u32(buf.data() + 4, kModelVersion);
+  put_u32(buf.data() + 8, (uint32_t)kParams);
+  put_u32(buf.data() + 12, (uint32_t)kIn);
+  for (int i = 0; i < kParams; ++i) {
+    uint32_t bits;
+    std::memcpy(&bits, &p[i], 4);
+    put_u32(buf.data() + kModelHeader + 4 * (size_t)i, bits);
+  }
+  const size_t body = kModelHeader + (size_t)kParams * 4;
+  const uint64_t h = fnv1a(buf.data(), body);
+  put_u32(buf.data() + body, (uint32_t)h);
+  put_u32(buf.data() + body + 4, (uint32_t)(h >> 32));
+  FILE *f = std::fopen(path, "wb");
+  if (!f) return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, std::string("cannot write ") + path);
+  const bool ok = std::fwrite(buf.data(), 1, buf.size(), f) == buf.size();
+  const bool closed = std::fclose(f) == 0;
+  if (!ok || !closed) return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, std::string("cannot write ") + path);
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_mlp_load(nomad_ctx *ctx, const char *path) {
+  if (!ctx || !path) return NOMAD_ERR_INVALID_ARGUMENT;
+  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  MlpState &S = mlp(ctx);
+  auto reject = [&](const std::string &why) {
+    S.ready = false;
+    return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT,
+                      std::string("model file ") + path + ": " + why +
+                          "; learned steps fall back to the ray-hit budget");
+  };
+  const size_t body = kModelHeader + (size_t)kParams * 4;
+  std::vector<unsigned char> buf;
+  {
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return reject("cannot be opened");
+    unsigned char tmp[65536];
+    size_t got;
+    while ((got = std::fread(tmp, 1, sizeof(tmp), f)) > 0 && buf.size() <= body + 8)
+      buf.insert(buf.end(), tmp, tmp + got);
+    std::fclose(f);
+  }
+  if (buf.size() < kModelHeader || std::memcmp(buf.data(), "NMLP", 4) != 0) return reject("not a model file");
+  if (get_u32(buf.data() + 4) != kModelVersion)
+    return reject("format version " + std::to_string(get_u32(buf.data() + 4)) + ", expected " +
+                  std::to_string(kModelVersion));
+  if (get_u32(buf.data() + 8) != (uint32_t)kParams || get_u32(buf.data() + 12) != (uint32_t)kIn)
+    return reject("shape differs from this library's model");
+  if (buf.size() != body + 8) return reject("size " + std::to_string(buf.size()) + " bytes, expected " +
+                                            std::to_string(body + 8));
+  const uint64_t want = (uint64_t)get_u32(buf.data() + body) | ((uint64_t)get_u32(buf.data() + body + 4) << 32);
+  if (fnv1a(buf.data(), body) != want) return reject("checksum mismatch");
+  std::vector<float> p(kParams);
+  for (int i = 0; i < kParams; ++i) {
+    const uint32_t bits = get_u32(buf.data() + kModelHeader + 4 * (size_t)i);
+    std::memcpy(&p[i], &bits, 4);
+    if (!std::isfinite(p[i])) return reject("parameter " + std::to_string(i) + " is not finite");
+  }
+  return nomad_mlp_set(ctx, p.data());
 }
 
 extern "C" nomad_status nomad_mlp_infer(nomad_ctx *ctx, const float *features, uint64_t n, float *out,

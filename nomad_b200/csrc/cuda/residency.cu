@@ -424,6 +424,7 @@ nomad_status nomad_residency_init(nomad_ctx *ctx) {
   R.primVisible.clear();
   R.primRebuild = 0;
   R.lodOn = false;
+  R.fallbackSteps = 0;
   R.objCooldown.clear();
   R.lodDist.clear();
   R.lodFlags.clear();
@@ -1057,6 +1058,12 @@ nomad_status screen_space_step(nomad_ctx *ctx, const nomad_residency_params *prm
 
 }  // namespace
 
+extern "C" nomad_status nomad_residency_fallback_steps(nomad_ctx *ctx, uint64_t *out) {
+  if (!ctx || !out) return NOMAD_ERR_INVALID_ARGUMENT;
+  *out = ctx->res.fallbackSteps;
+  return NOMAD_OK;
+}
+
 extern "C" nomad_status nomad_residency_object_state(nomad_ctx *ctx, float *distance, uint8_t *flags,
                                                      uint32_t *cooldowns) {
   if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
@@ -1108,6 +1115,14 @@ extern "C" nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residen
     return screen_space_step(ctx, prm, *camera, toggled);
   }
   if (prm->policy > NOMAD_POLICY_LEARNED) return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "unknown policy");
+  // Without a usable model the learned policy runs the ray-hit budget step instead.
+  nomad_residency_params fallback;
+  if (prm->policy == NOMAD_POLICY_LEARNED && !nomad_mlp_ready(ctx)) {
+    fallback = *prm;
+    fallback.policy = NOMAD_POLICY_RAYHIT_BUDGET;
+    prm = &fallback;
+    ++ctx->res.fallbackSteps;
+  }
   const uint32_t N = ctx->objectCount;
   if (N > kMaxSelectObjects)
     return nomad_fail(ctx, NOMAD_ERR_LIMIT, "device residency selection supports at most 16384 objects");

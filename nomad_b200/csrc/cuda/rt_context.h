@@ -149,6 +149,8 @@ struct nomad_ctx {
     std::vector<float> primSphere;  // centre xyz, radius per primitive
     std::vector<uint8_t> primVisible;
     uint32_t primRebuild = 0;
+    // learned-policy steps that ran the ray-hit budget for want of a usable model
+    uint64_t fallbackSteps = 0;
     // DistanceLOD policy (NOMAD_POLICY_DISTANCE_LOD): object cooldowns and the last step's tests
     bool lodOn = false;
     std::vector<uint32_t> objCooldown;
@@ -190,6 +192,8 @@ struct FeatArgs;
 // Learned policy: per-object features (as the feature kernel computes them) and MLP scores in one
 // launch; keys[o] receives the score.
 nomad_status nomad_mlp_score_objects(nomad_ctx *ctx, const nomad_res::FeatArgs *fa, float *keys);
+// Whether the context holds a usable model (initialised, set, trained or loaded, not rejected).
+bool nomad_mlp_ready(nomad_ctx *ctx);
 // Residency device state: created at upload, mirrored after host-side flushes.
 nomad_status nomad_residency_init(nomad_ctx *ctx);
 nomad_status nomad_residency_mirror(nomad_ctx *ctx);

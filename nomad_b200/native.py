@@ -184,6 +184,7 @@ SIGNATURES = {
     "nomad_object_bytes": (C.c_int32, [_P, _P]),
     "nomad_residency_last": (C.c_int32, [_P, _P, _P]),
     "nomad_residency_flags": (C.c_int32, [_P, _P]),
+    "nomad_residency_fallback_steps": (C.c_int32, [_P, C.POINTER(C.c_uint64)]),
     "nomad_residency_prim_state": (C.c_int32, [_P, _P, _P, _P, _P, _P]),
     "nomad_residency_object_state": (C.c_int32, [_P, _P, _P, _P]),
     "nomad_mlp_init": (C.c_int32, [_P, C.c_uint64]),
@@ -192,6 +193,8 @@ SIGNATURES = {
     "nomad_mlp_infer": (C.c_int32, [_P, _P, C.c_uint64, _P, C.c_uint32]),
     "nomad_mlp_get": (C.c_int32, [_P, _P]),
     "nomad_mlp_set": (C.c_int32, [_P, _P]),
+    "nomad_mlp_save": (C.c_int32, [_P, C.c_char_p]),
+    "nomad_mlp_load": (C.c_int32, [_P, C.c_char_p]),
     "nomad_set_restir": (C.c_int32, [_P, _P]),
     "nomad_reset_restir": (C.c_int32, [_P]),
     "nomad_autotune": (C.c_int32, [_P, _P, C.c_uint64, C.c_uint32, C.c_uint32, _P]),
@@ -799,6 +802,12 @@ class Context:
         self._ck(self.lib.nomad_residency_flags(self.h, _ptr(out)))
         return out
 
+    def residency_fallback_steps(self) -> int:
+        """Learned-policy steps that ran the ray-hit budget for want of a usable model."""
+        out = C.c_uint64()
+        self._ck(self.lib.nomad_residency_fallback_steps(self.h, C.byref(out)))
+        return int(out.value)
+
     # learned scorer
     def mlp_init(self, seed: int = 0):
         self._ck(self.lib.nomad_mlp_init(self.h, seed))
@@ -827,6 +836,15 @@ class Context:
         b = np.ascontiguousarray(blob, np.float32)
         assert b.size == MLP_PARAMS
         self._ck(self.lib.nomad_mlp_set(self.h, _ptr(b)))
+
+    def mlp_save(self, path: str):
+        """Writes the model as a versioned, checksummed file."""
+        self._ck(self.lib.nomad_mlp_save(self.h, os.fsencode(path)))
+
+    def mlp_load(self, path: str):
+        """Reads a model file; a bad file raises and leaves the context without a usable model
+        (learned steps then run the ray-hit budget)."""
+        self._ck(self.lib.nomad_mlp_load(self.h, os.fsencode(path)))
 
     # ReSTIR DI
     def set_restir(self, candidates=32, temporal=True, spatial=3, radius_px=30.0, m_cap=20.0,
