@@ -17,8 +17,8 @@
 //                    [--frames F] [--policy always|rayhit|learned] [--budget FRACTION]
 //                    [--mlp WEIGHTS] [--seed N] [--out FILE.pfm]
 //
-// --mlp reads a parameter blob (NOMAD_MLP_PARAMS float32 values, as nomad_mlp_get writes it);
-// the learned policy needs one.
+// --mlp reads a model file (nomad_mlp_save) or a raw parameter blob (NOMAD_MLP_PARAMS float32
+// values, as nomad_mlp_get writes it); the learned policy needs one.
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -177,16 +177,28 @@ int main(int argc, char **argv) {
       std::fprintf(stderr, "the learned policy needs --mlp WEIGHTS\n");
       return 2;
     }
-    std::vector<float> blob(NOMAD_MLP_PARAMS);
+    char magic[4] = {0, 0, 0, 0};
     FILE *f = std::fopen(a.mlp.c_str(), "rb");
-    if (!f || std::fread(blob.data(), 4, blob.size(), f) != blob.size()) {
+    if (!f || std::fread(magic, 1, 4, f) != 4) {
       std::fprintf(stderr, "cannot read %s\n", a.mlp.c_str());
       if (f) std::fclose(f);
       return 2;
     }
-    std::fclose(f);
-    CHECK(nomad_mlp_init(ctx, 1));
-    CHECK(nomad_mlp_set(ctx, blob.data()));
+    if (std::memcmp(magic, "NMLP", 4) == 0) {  // a model file written by nomad_mlp_save
+      std::fclose(f);
+      CHECK(nomad_mlp_load(ctx, a.mlp.c_str()));
+    } else {  // a raw parameter blob
+      std::vector<float> blob(NOMAD_MLP_PARAMS);
+      std::rewind(f);
+      const bool ok = std::fread(blob.data(), 4, blob.size(), f) == blob.size();
+      std::fclose(f);
+      if (!ok) {
+        std::fprintf(stderr, "cannot read %s\n", a.mlp.c_str());
+        return 2;
+      }
+      CHECK(nomad_mlp_init(ctx, 1));
+      CHECK(nomad_mlp_set(ctx, blob.data()));
+    }
   }
 
   const size_t pixels = (size_t)a.width * a.height;

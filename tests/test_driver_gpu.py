@@ -87,3 +87,17 @@ def test_driver_renders_an_ingested_scene_like_the_binding(nb):
     finally:
         ctx.close()
     assert np.array_equal(img.view(np.int32), want.view(np.int32))
+
+
+def test_driver_learned_policy_from_a_model_file(nb, tmp_path):
+    """--mlp takes a model file written by nomad_mlp_save."""
+    ctx = nb.Context(0)
+    try:
+        ctx.mlp_init(7)
+        path = str(tmp_path / "scorer.nmlp")
+        ctx.mlp_save(path)
+    finally:
+        ctx.close()
+    r = _run("--scene", "city", "--width", "160", "--height", "90", "--spp", "1", "--depth", "2", "--frames", "4",
+             "--policy", "learned", "--budget", "0.4", "--mlp", path)
+    assert r["status"] == 0 and 0.0 < r["resident_fraction"] <= 0.4 + 1e-9
