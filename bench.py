@@ -553,6 +553,25 @@ def run_profile_restir(args):
     ctx.close()
 
 
+def ranks_max(x: float, world: int, device: str = "cuda") -> float:
+    """The maximum of x over the ranks of the process group (x itself with one rank). A timing
+    taken on every rank becomes the slowest rank's, as the whole job finishes with it."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world: int, units_per_rank: int, steps: int, seconds: float) -> float:
+    """Whole-job throughput in millions of units per second: every rank processes
+    units_per_rank per step (weak scaling), the job lasts `seconds` (the slowest rank's)."""
+    return world * units_per_rank * steps / seconds / 1e6
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -736,12 +755,9 @@ def main():
     total_ms = start.elapsed_time(end)
     t_prim = np.mean([e[0].elapsed_time(e[1]) for e in ev])
     t_b = np.mean([e[1].elapsed_time(e[2]) for e in ev])
-    if world > 1:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = ranks_max(total_ms, world)
     ms_step = total_ms / args.steps
-    value = world * rays_per_step * args.steps / (total_ms / 1e3) / 1e6
+    value = job_rate(world, rays_per_step, args.steps, total_ms / 1e3)
 
     # e2e through the C ABI with pinned host buffers (copies inside the timed region).
     h_rays = torch.from_numpy(np.concatenate([primary, bounce]).view(np.uint8)).pin_memory()
@@ -765,11 +781,8 @@ def main():
     for _ in range(e_steps):
         e2e_step()
     e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * rays_per_step * e_steps / e2e_s / 1e6
+    e2e_s = ranks_max(e2e_s, world)
+    e2e_value = job_rate(world, rays_per_step, e_steps, e2e_s)
     ok = np.array_equal(hits_np.view(np.int32).reshape(-1, 5)[:n_prim],
                         d_ph.cpu().numpy()) if True else True
 
