@@ -84,6 +84,13 @@ nomad_status nomad_sync(nomad_ctx *ctx);
 nomad_status nomad_set_stream(nomad_ctx *ctx, void *cuda_stream);
 /* Device status word: bit 0 stack overflow guard, bit 1 bounded wait expired. Cleared by reading. */
 nomad_status nomad_get_status(nomad_ctx *ctx, uint32_t *status_word);
+/* Self-test of the failure path of the bounded device waits (no counterpart in the reference):
+ * one block waits, with a short poll limit, on a shared-memory mbarrier with the helper the
+ * traversal's staged-node copy uses. With complete = 0 nothing completes the barrier, the polls
+ * run out and bit 1 of the status word is set; otherwise the barrier is completed first and the
+ * wait succeeds. The GPU is neither faulted nor held: the kernel returns, the context stays
+ * usable. Synchronous on the context's stream. */
+nomad_status nomad_selftest_bounded_wait(nomad_ctx *ctx, int32_t complete);
 
 /* ---- scene upload (replaces the GPU uploads of Renderer::rebuildResidentResources,
  *      Renderer.cpp:5983-6292, for the non-compacted resident set) ------------------------ */

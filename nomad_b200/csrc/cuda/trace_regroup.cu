@@ -67,10 +67,30 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
   return ok != 0;
 }
 
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
-  for (long long i = 0; i < kWaitPolls; ++i)
+__device__ __forceinline__ bool mbar_wait_polls(uint32_t bar, uint32_t parity, long long polls) {
+  for (long long i = 0; i < polls; ++i)
     if (mbar_try(bar, parity)) return true;
   return false;
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+  return mbar_wait_polls(bar, parity, kWaitPolls);
+}
+
+// Self-test of the bounded wait's failure path: one block waits on a shared-memory mbarrier that
+// is completed only when `complete` is set; when the polls run out the status bit is set, as in
+// stage_nodes, and the kernel returns. Nothing is copied, so nothing is left in flight.
+__global__ void k_wait_selftest(uint32_t *status, int complete, long long polls) {
+  __shared__ __align__(8) unsigned long long barrier;
+  const uint32_t bar = smem_u32(&barrier);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (complete && threadIdx.x == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+  const bool ok = mbar_wait_polls(bar, 0, polls);
+  if (!__syncthreads_and(ok ? 1 : 0) && threadIdx.x == 0) atomicOr(status, kStatusWaitExpired);
 }
 
 // Copies `bytes` (a multiple of 16) from global `src` (16-byte aligned) into shared memory after
@@ -558,6 +578,15 @@ nomad_status nomad_trace_regroup(nomad_ctx *ctx, const nomad_traversal &cfg, boo
                        : launch_w<8, false>(ctx, cfg, A, rays, n, lenDev, cursor, hits5, occ, counts, s);
     default: return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "width must be 2, 4 or 8");
   }
+}
+
+extern "C" nomad_status nomad_selftest_bounded_wait(nomad_ctx *ctx, int32_t complete) {
+  if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
+  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  k_wait_selftest<<<1, 32, 0, ctx->stream>>>(ctx->status.as<uint32_t>(), complete ? 1 : 0, 1ll << 12);
+  NOMAD_CUDA(ctx, cudaGetLastError());
+  NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return NOMAD_OK;
 }
 
 extern "C" nomad_status nomad_set_traversal(nomad_ctx *ctx, const nomad_traversal *cfg) {

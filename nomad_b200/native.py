@@ -185,6 +185,7 @@ SIGNATURES = {
     "nomad_residency_last": (C.c_int32, [_P, _P, _P]),
     "nomad_residency_flags": (C.c_int32, [_P, _P]),
     "nomad_residency_fallback_steps": (C.c_int32, [_P, C.POINTER(C.c_uint64)]),
+    "nomad_selftest_bounded_wait": (C.c_int32, [_P, C.c_int32]),
     "nomad_residency_prim_state": (C.c_int32, [_P, _P, _P, _P, _P, _P]),
     "nomad_residency_object_state": (C.c_int32, [_P, _P, _P, _P]),
     "nomad_mlp_init": (C.c_int32, [_P, C.c_uint64]),
@@ -801,6 +802,10 @@ class Context:
         out = np.zeros(self.object_count, np.uint8)
         self._ck(self.lib.nomad_residency_flags(self.h, _ptr(out)))
         return out
+
+    def selftest_bounded_wait(self, complete: bool):
+        """Runs the bounded-wait self-test; read the outcome with status()."""
+        self._ck(self.lib.nomad_selftest_bounded_wait(self.h, 1 if complete else 0))
 
     def residency_fallback_steps(self) -> int:
         """Learned-policy steps that ran the ray-hit budget for want of a usable model."""
