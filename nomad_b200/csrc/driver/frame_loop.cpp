@@ -10,7 +10,7 @@
 // bottom row first).
 //
 // --scene xml:FILE loads one of the reference's scene files (nomad_scene_load_xml); its
-// <CameraPath> keyframes, interpolated linearly by frame number, replace the orbit, and its
+// <CameraPath> keyframes, interpolated by frame number as the reference does, replace the orbit, and its
 // width, height and maxRayDepth apply unless given on the command line.
 //
 //   nomad_frame_loop [--scene city|icospheres|xml:FILE] [--width W] [--height H] [--spp S] [--depth D]
@@ -90,17 +90,30 @@ void orbit(const float bmin[3], const float bmax[3], uint32_t f, float pos[3], f
   look[2] = cz;
 }
 
-// Camera of frame f on a keyframed path: linear between the keyframes around f, clamped at the ends.
+// Camera of frame f on a keyframed path, as Renderer::updateCameraStates interpolates it
+// (Renderer.cpp:6826-6880): the first keyframe up to its frame, the last one from its frame on,
+// otherwise linear on the first segment with k0.frame <= f <= k1.frame.
 void along_path(const nomad_camera_keyframe *k, uint32_t n, uint32_t f, float pos[3], float look[3], float up[3]) {
-  uint32_t i = 0;
-  while (i + 1 < n && k[i + 1].frame <= f) ++i;
-  const nomad_camera_keyframe &a = k[i], &b = k[i + 1 < n ? i + 1 : i];
+  const nomad_camera_keyframe *a = &k[0], *b = &k[0];
   float t = 0.0f;
-  if (b.frame > a.frame && f > a.frame) t = std::fmin(1.0f, (float)(f - a.frame) / (float)(b.frame - a.frame));
+  if (f <= k[0].frame) {
+    a = b = &k[0];
+  } else if (f >= k[n - 1].frame) {
+    a = b = &k[n - 1];
+  } else {
+    for (uint32_t i = 0; i + 1 < n; ++i)
+      if (f >= k[i].frame && f <= k[i + 1].frame) {
+        a = &k[i];
+        b = &k[i + 1];
+        // two keyframes on one frame: the earlier one (the reference divides 0 by 0 there)
+        t = b->frame > a->frame ? (float)(f - a->frame) / (float)(b->frame - a->frame) : 0.0f;
+        break;
+      }
+  }
   for (int c = 0; c < 3; ++c) {
-    pos[c] = a.position[c] + t * (b.position[c] - a.position[c]);
-    look[c] = a.look_at[c] + t * (b.look_at[c] - a.look_at[c]);
-    up[c] = a.up[c] + t * (b.up[c] - a.up[c]);
+    pos[c] = a->position[c] + t * (b->position[c] - a->position[c]);
+    look[c] = a->look_at[c] + t * (b->look_at[c] - a->look_at[c]);
+    up[c] = a->up[c] + t * (b->up[c] - a->up[c]);
   }
 }
 
