@@ -646,7 +646,7 @@ nomad_status nomad_mlp_score_objects(nomad_ctx *ctx, const nomad_res::FeatArgs *
 
 extern "C" nomad_status nomad_mlp_init(nomad_ctx *ctx, uint64_t seed) {
   if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
-  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  NOMAD_DEVICE_SCOPE(ctx);
   MlpState &S = mlp(ctx);
   nomad_status st = ensure(ctx, S);
   if (st != NOMAD_OK) return st;
@@ -682,7 +682,7 @@ bool nomad_mlp_ready(nomad_ctx *ctx) { return ctx->mlp && static_cast<MlpState *
 
 extern "C" nomad_status nomad_mlp_set(nomad_ctx *ctx, const float *in) {
   if (!ctx || !in) return NOMAD_ERR_INVALID_ARGUMENT;
-  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  NOMAD_DEVICE_SCOPE(ctx);
   MlpState &S = mlp(ctx);
   for (int i = 0; i < kParams; ++i)
     if (!std::isfinite(in[i])) {
@@ -754,7 +754,7 @@ extern "C" nomad_status nomad_mlp_save(nomad_ctx *ctx, const char *path) {
 
 extern "C" nomad_status nomad_mlp_load(nomad_ctx *ctx, const char *path) {
   if (!ctx || !path) return NOMAD_ERR_INVALID_ARGUMENT;
-  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  NOMAD_DEVICE_SCOPE(ctx);
   MlpState &S = mlp(ctx);
   auto reject = [&](const std::string &why) {
     S.ready = false;
@@ -795,7 +795,7 @@ extern "C" nomad_status nomad_mlp_load(nomad_ctx *ctx, const char *path) {
 extern "C" nomad_status nomad_mlp_infer(nomad_ctx *ctx, const float *features, uint64_t n, float *out,
                                         uint32_t flags) {
   if (!ctx || (!features && n) || (!out && n)) return NOMAD_ERR_INVALID_ARGUMENT;
-  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  NOMAD_DEVICE_SCOPE(ctx);
   MlpState &S = mlp(ctx);
   if (flags & NOMAD_TRACE_DEVICE_POINTERS) return nomad_mlp_infer_device(ctx, features, n, out);
   NOMAD_CUDA(ctx, S.inX.reserve(std::max<uint64_t>(1, n) * kIn * 4));
@@ -814,7 +814,7 @@ extern "C" nomad_status nomad_mlp_train(nomad_ctx *ctx, const float *features, c
   if (!ctx || !features || !targets || n == 0 || batch == 0 || batch % 64 != 0 || batch > 65536)
     return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "training needs samples and a batch that is a multiple of 64");
   if (n > 0xffffffffull) return nomad_fail(ctx, NOMAD_ERR_LIMIT, "too many samples");
-  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  NOMAD_DEVICE_SCOPE(ctx);
   MlpState &S = mlp(ctx);
   if (!S.ready) {
     nomad_status st = nomad_mlp_init(ctx, seed);

@@ -270,7 +270,7 @@ extern "C" nomad_status nomad_paging_enable(nomad_ctx *ctx, const nomad_paging_c
   if (ctx->paging) return fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "paging is already enabled");
   if (cfg->width != 2 && cfg->width != 4 && cfg->width != 8)
     return fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "paged width must be 2, 4 or 8");
-  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  NOMAD_DEVICE_SCOPE(ctx);
   nomad_status hs = nomad_residency_sync_host(ctx);
   if (hs != NOMAD_OK) return hs;
   NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -544,7 +544,7 @@ extern "C" nomad_status nomad_paging_update(nomad_ctx *ctx) {
   if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
   Paging *pg = pg_of(ctx);
   if (!pg) return fail(ctx, NOMAD_ERR_NOT_READY, "paging is not enabled");
-  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  NOMAD_DEVICE_SCOPE(ctx);
   nomad_status hs = nomad_residency_sync_host(ctx);
   if (hs != NOMAD_OK) return hs;
   refresh_retired(pg);
@@ -671,7 +671,7 @@ extern "C" nomad_status nomad_paging_wait(nomad_ctx *ctx) {
   if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
   Paging *pg = pg_of(ctx);
   if (!pg) return fail(ctx, NOMAD_ERR_NOT_READY, "paging is not enabled");
-  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  NOMAD_DEVICE_SCOPE(ctx);
   NOMAD_CUDA(ctx, cudaStreamSynchronize(pg->copy));
   std::vector<PubItem> items;
   collect_ready(ctx, pg, items, true);

@@ -398,7 +398,11 @@ __global__ void __launch_bounds__(kPtBlock) k_shade(
                       V3 view = normalize(-d);
                       V3 bsdf = eval_bsdf(m, nrm, view, wi);
                       V3 c = tp * bsdf * lrad * (cosT / totalPdf);
-                      float tmax = dist - kRayEps;
+                      // The reference accepts the light as visible when its closest hit is the
+                      // light itself at t >= dist - 0.001 (PathTracing.h:1832-1834); a hit on the
+                      // light a float rounding short of dist must not occlude it, so the any-hit
+                      // window ends 1e-3 before the sampled point.
+                      float tmax = dist - kNeeShadowEps;
                       if (tmax < kRayEps) tmax = kRayEps;
                       V3 so = p + nrm * 0.0005f;
                       sA = make_float4(so.x, so.y, so.z, kRayEps);
@@ -601,7 +605,7 @@ extern "C" nomad_status nomad_render_frame(nomad_ctx *ctx, const nomad_view *vie
   if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
   if (!ctx->sceneReady) return nomad_fail(ctx, NOMAD_ERR_NOT_READY, "no scene uploaded");
   if (!views || nviews == 0 || !out) return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "no views or output");
-  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  NOMAD_DEVICE_SCOPE(ctx);
   std::vector<ViewDev> vd(nviews);
   unsigned long long P = 0, pixels = 0;
   uint32_t maxDepth = 0;

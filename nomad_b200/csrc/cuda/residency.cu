@@ -11,11 +11,9 @@
 //   * selection in score order with ties to the lower index (:2883-2896), a visibility reserve
 //     of ceil(N * (0.02 + 0.06 * motion)) visible objects (:2908-2923), min_active always kept
 //     (:2925-2926) and a per-step toggle budget applied in index order (:2930-2946).
-// Changes for the B200 build (documented in the design notes): the unit is the object (the
-// reference toggles primitives), the target is a geometry byte budget rather than a primitive
-// fraction (greedy in score order, skipping objects that do not fit), and the Beta-posterior
-// prior is not applied (it needs per-object leaf-test counts whose values depend on traversal
-// order).
+// Changes for the B200 build: the unit is the object (the reference toggles primitives), and the
+// target is a geometry byte budget rather than a primitive fraction (greedy in score order,
+// skipping objects that do not fit).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -1103,15 +1101,15 @@ extern "C" nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residen
   if (!ctx->sceneReady || !ctx->res.ready) return nomad_fail(ctx, NOMAD_ERR_NOT_READY, "no scene uploaded");
   if (!prm || !camera) return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "null parameters or camera");
   if (prm->policy == NOMAD_POLICY_RAYHIT_PRIM) {
-    NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+    NOMAD_DEVICE_SCOPE(ctx);
     return rayhit_prim_step(ctx, prm, *camera, toggled);
   }
   if (prm->policy == NOMAD_POLICY_DISTANCE_LOD) {
-    NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+    NOMAD_DEVICE_SCOPE(ctx);
     return distance_lod_step(ctx, prm, *camera, toggled);
   }
   if (prm->policy == NOMAD_POLICY_SCREEN_SPACE) {
-    NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+    NOMAD_DEVICE_SCOPE(ctx);
     return screen_space_step(ctx, prm, *camera, toggled);
   }
   if (prm->policy > NOMAD_POLICY_LEARNED) return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "unknown policy");
@@ -1126,7 +1124,7 @@ extern "C" nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residen
   const uint32_t N = ctx->objectCount;
   if (N > kMaxSelectObjects)
     return nomad_fail(ctx, NOMAD_ERR_LIMIT, "device residency selection supports at most 16384 objects");
-  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  NOMAD_DEVICE_SCOPE(ctx);
   auto &R = ctx->res;
   cudaStream_t s = ctx->stream;
   // camera frame from the view (populateViewportUniforms: first_pixel = pos - w - U/2 - V/2)

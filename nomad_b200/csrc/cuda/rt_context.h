@@ -9,6 +9,7 @@
 
 #include "../../../include/nomad_rt.h"
 #include "../host/layout.h"
+#include "device_scope.h"
 #include "rt_device.cuh"
 #include "rt_wide.cuh"
 
@@ -212,6 +213,9 @@ nomad_status nomad_trace_regroup(nomad_ctx *ctx, const nomad_traversal &cfg, boo
                                  uint32_t *counts, cudaStream_t s);
 // Opts the short-stack kernels in to large dynamic shared memory (once per context creation).
 cudaError_t nomad_regroup_init();
+// Looks up (again) the device address of the allocation-free entry point's static scratch array
+// on `device`, which must be current; called when a context is created on that device.
+cudaError_t nomad_noalloc_lookup(int device);
 // The hybrid packet kernels (trace_packet.cu).
 nomad_status nomad_trace_packet(nomad_ctx *ctx, const nomad_traversal &cfg, bool any, const float4 *rays, uint64_t n,
                                 const uint32_t *lenDev, unsigned long long *cursor, int32_t *hits5, uint8_t *occ,
@@ -235,4 +239,9 @@ inline nomad_status nomad_cuda_fail(nomad_ctx *c, cudaError_t e, const char *wha
     cudaError_t e_ = (call);                                          \
     if (e_ != cudaSuccess) return nomad_cuda_fail(ctx, e_, #call);    \
   } while (0)
+
+#define NOMAD_DEVICE_SCOPE(ctx)                                                  \
+  NomadDeviceScope nomad_device_scope_((ctx)->device);                           \
+  if (nomad_device_scope_.err != cudaSuccess)                                    \
+  return nomad_cuda_fail(ctx, nomad_device_scope_.err, "cudaSetDevice")
 

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -148,17 +149,20 @@ bool is_device_ptr(const void *p) {
 extern "C" nomad_status nomad_create(const nomad_config *cfg, nomad_ctx **out) {
   if (!out) return NOMAD_ERR_INVALID_ARGUMENT;
   *out = nullptr;
-  std::unique_ptr<nomad_ctx> c(new (std::nothrow) nomad_ctx());
-  if (!c) return NOMAD_ERR_OUT_OF_MEMORY;
-  c->device = cfg ? cfg->device : 0;
+  const int device = cfg ? cfg->device : 0;
   int count = 0;
   cudaError_t e = cudaGetDeviceCount(&count);
   if (e != cudaSuccess || count == 0) {
     cudaGetLastError();
     return NOMAD_ERR_CUDA;
   }
-  if (c->device < 0 || c->device >= count) return NOMAD_ERR_INVALID_ARGUMENT;
-  if (cudaSetDevice(c->device) != cudaSuccess) return NOMAD_ERR_CUDA;
+  if (device < 0 || device >= count) return NOMAD_ERR_INVALID_ARGUMENT;
+  NomadDeviceScope scope(device);  // outlives the context's buffers on every failure path
+  if (scope.err != cudaSuccess) return NOMAD_ERR_CUDA;
+  std::unique_ptr<nomad_ctx> c(new (std::nothrow) nomad_ctx());
+  if (!c) return NOMAD_ERR_OUT_OF_MEMORY;
+  c->device = device;
+  if (nomad_noalloc_lookup(device) != cudaSuccess) return NOMAD_ERR_CUDA;
   cudaDeviceProp prop;
   if (cudaGetDeviceProperties(&prop, c->device) != cudaSuccess) return NOMAD_ERR_CUDA;
   if (prop.major < 10) return NOMAD_ERR_UNSUPPORTED;  // built for sm_100a only
@@ -178,14 +182,16 @@ extern "C" nomad_status nomad_create(const nomad_config *cfg, nomad_ctx **out) {
 
 extern "C" nomad_status nomad_destroy(nomad_ctx *ctx) {
   if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
-  cudaSetDevice(ctx->device);
-  cudaStreamSynchronize(ctx->stream);
-  for (auto s : ctx->copyStreams)
-    if (s) cudaStreamDestroy(s);
-  if (ctx->ownStream) cudaStreamDestroy(ctx->ownStream);
-  if (ctx->mlp) nomad_mlp_free(ctx->mlp);
-  nomad_paging_free(ctx);
-  delete ctx;
+  {
+    NomadDeviceScope scope(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (auto s : ctx->copyStreams)
+      if (s) cudaStreamDestroy(s);
+    if (ctx->ownStream) cudaStreamDestroy(ctx->ownStream);
+    if (ctx->mlp) nomad_mlp_free(ctx->mlp);
+    nomad_paging_free(ctx);
+    delete ctx;  // frees the context's device buffers with its device current
+  }
   return NOMAD_OK;
 }
 
@@ -222,7 +228,7 @@ extern "C" nomad_status nomad_scene_upload(nomad_ctx *ctx, const float *bvh, uin
   if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
   if (!bvh || !tlas || !prims || !materials || !primIndices || !inst)
     return fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "null scene array");
-  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  NOMAD_DEVICE_SCOPE(ctx);
   if (ctx->resHostStale) {  // a pending flag copy must land before the pinned buffer is reused
     NOMAD_CUDA(ctx, cudaEventSynchronize(ctx->resEvent));
     ctx->resHostStale = false;
@@ -641,7 +647,7 @@ nomad_status trace_entry(nomad_ctx *ctx, Op op, const nomad_ray *rays, uint64_t 
   if (!ctx->sceneReady) return fail(ctx, NOMAD_ERR_NOT_READY, "no scene uploaded");
   if (n == 0) return NOMAD_OK;
   if (!rays || !out) return fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "null rays or output");
-  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  NOMAD_DEVICE_SCOPE(ctx);
   bool countHits = (flags & NOMAD_TRACE_COUNT_HITS) != 0 && op == Op::Closest;
   if (flags & NOMAD_TRACE_DEVICE_POINTERS) {
     if (reinterpret_cast<uintptr_t>(rays) % 16 != 0)
@@ -676,7 +682,7 @@ extern "C" nomad_status nomad_trace_work(nomad_ctx *ctx, const nomad_ray *rays, 
 extern "C" nomad_status nomad_read_object_hits(nomad_ctx *ctx, uint32_t *out) {
   if (!ctx || !ctx->sceneReady) return NOMAD_ERR_NOT_READY;
   if (!out) return NOMAD_ERR_INVALID_ARGUMENT;
-  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  NOMAD_DEVICE_SCOPE(ctx);
   NOMAD_CUDA(ctx, cudaMemcpyAsync(out, ctx->objHits.p, (size_t)ctx->objectCount * 4,
                                   cudaMemcpyDeviceToHost, ctx->stream));
   NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -685,7 +691,7 @@ extern "C" nomad_status nomad_read_object_hits(nomad_ctx *ctx, uint32_t *out) {
 
 extern "C" nomad_status nomad_reset_object_hits(nomad_ctx *ctx) {
   if (!ctx || !ctx->sceneReady) return NOMAD_ERR_NOT_READY;
-  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  NOMAD_DEVICE_SCOPE(ctx);
   NOMAD_CUDA(ctx, cudaMemsetAsync(ctx->objHits.p, 0, (size_t)ctx->objectCount * 4, ctx->stream));
   return NOMAD_OK;
 }
@@ -704,8 +710,10 @@ extern "C" nomad_status nomad_reset_object_hits(nomad_ctx *ctx) {
 //   * at most kNoAllocMaxObjects objects (64 KiB of accumulators + one 256-byte cursor line);
 //     larger scenes are rejected with NOMAD_ERR_LIMIT;
 //   * the array lives in every GPU that loads this library, until the process exits;
-//   * the first call on a device looks up the array's device address (cudaGetSymbolAddress,
-//     with that device current) and caches it; make that first call before any stream capture;
+//   * the array's device address is looked up (cudaGetSymbolAddress, with that device current)
+//     when a context is created on a device, and by the first call on a device that has none
+//     cached; make that first call before any stream capture. The lookup is repeated by every
+//     nomad_create, so contexts created after a cudaDeviceReset use the reloaded module's array;
 //   * every call shares the one array: calls on the same device that overlap on the GPU (two
 //     streams, or two contexts) race on it. Serialise them;
 //   * each call clears the cursor and the accumulators it uses before the launch.
@@ -717,7 +725,9 @@ constexpr int kNoAllocMaxDevices = 64;
 
 static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocCursorWords + kNoAllocMaxObjects];
 
-uint32_t *g_noalloc_addr[kNoAllocMaxDevices] = {};
+// Per device: the scratch array's device address (null until looked up). Atomic, so host threads
+// that make their first call at the same time may both look it up and store the same address.
+std::atomic<uint32_t *> g_noalloc_addr[kNoAllocMaxDevices] = {};
 
 __global__ void __launch_bounds__(kPersistBlock) k_closest_persist_noalloc(
     DevScene S, const float4 *__restrict__ rays, uint64_t n, nomad_hit *__restrict__ out,
@@ -747,6 +757,15 @@ __global__ void __launch_bounds__(kPersistBlock) k_closest_persist_noalloc(
 
 }  // namespace
 
+cudaError_t nomad_noalloc_lookup(int device) {
+  if (device < 0 || device >= kNoAllocMaxDevices) return cudaSuccess;  // the entry point refuses it
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return e;
+  g_noalloc_addr[device].store(static_cast<uint32_t *>(p), std::memory_order_release);
+  return cudaSuccess;
+}
+
 extern "C" nomad_status nomad_trace_closest_noalloc(nomad_ctx *ctx, const nomad_ray *d_rays,
                                                     uint64_t n, nomad_hit *d_hits,
                                                     uint32_t *d_object_hits) {
@@ -765,13 +784,11 @@ extern "C" nomad_status nomad_trace_closest_noalloc(nomad_ctx *ctx, const nomad_
     return fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "device rays must be 16-byte aligned");
   if (ctx->device < 0 || ctx->device >= kNoAllocMaxDevices)
     return fail(ctx, NOMAD_ERR_LIMIT, "device ordinal too large for the static scratch table");
-  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
-  uint32_t *scratch = g_noalloc_addr[ctx->device];
+  NOMAD_DEVICE_SCOPE(ctx);
+  uint32_t *scratch = g_noalloc_addr[ctx->device].load(std::memory_order_acquire);
   if (!scratch) {
-    void *p = nullptr;
-    NOMAD_CUDA(ctx, cudaGetSymbolAddress(&p, g_noalloc_scratch));
-    scratch = static_cast<uint32_t *>(p);
-    g_noalloc_addr[ctx->device] = scratch;
+    NOMAD_CUDA(ctx, nomad_noalloc_lookup(ctx->device));
+    scratch = g_noalloc_addr[ctx->device].load(std::memory_order_acquire);
   }
   size_t clearBytes = (kNoAllocCursorWords + (size_t)ctx->objectCount) * 4;
   NOMAD_CUDA(ctx, cudaMemsetAsync(scratch, 0, clearBytes, ctx->stream));
@@ -815,7 +832,7 @@ extern "C" nomad_status nomad_autotune(nomad_ctx *ctx, const nomad_ray *rays, ui
   if (!ctx || !out) return NOMAD_ERR_INVALID_ARGUMENT;
   if (!ctx->sceneReady) return fail(ctx, NOMAD_ERR_NOT_READY, "no scene uploaded");
   if (!rays || n == 0) return fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "no sample rays");
-  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  NOMAD_DEVICE_SCOPE(ctx);
   cudaStream_t s = ctx->stream;
   const float4 *d = reinterpret_cast<const float4 *>(rays);
   if (!(flags & NOMAD_TRACE_DEVICE_POINTERS)) {

@@ -24,6 +24,9 @@
 namespace nomad_dev {
 
 constexpr float kRayEps = 1e-4f;
+// One-sample NEE: a light counts as visible when the closest hit is the light itself no nearer
+// than dist - 0.001 (PathTracing.h:1832-1834), so the shadow ray's any-hit window ends there.
+constexpr float kNeeShadowEps = 0.001f;
 constexpr float kPruneScale = 1.0009765625f;  // 1 + 2^-10
 constexpr int32_t kEmptyRef = INT32_MIN;
 constexpr int32_t kLastInLeaf = 1 << 8;

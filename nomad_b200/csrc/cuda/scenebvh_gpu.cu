@@ -27,6 +27,7 @@
 
 #include "../../../include/nomad_scene.h"
 #include "../host/scenebvh_internal.h"
+#include "device_scope.h"
 
 namespace {
 
@@ -406,7 +407,8 @@ extern "C" nomad_status nomad_scenebvh_build_gpu(const nomad_scene_desc *desc, i
   *out = nullptr;
   nomad_status st = nomad::scenebvh_validate(desc);
   if (st != NOMAD_OK) return st;
-  if (cudaSetDevice(device) != cudaSuccess) {
+  NomadDeviceScope scope(device);  // outlives the device buffers below
+  if (scope.err != cudaSuccess) {
     cudaGetLastError();
     return NOMAD_ERR_CUDA;
   }

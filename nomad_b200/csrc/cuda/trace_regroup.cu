@@ -118,7 +118,12 @@ __device__ bool stage_nodes(unsigned char *smem, const float4 *src, uint32_t byt
   bool ok = mbar_wait_bounded(bar, 0);
   if (__syncthreads_and(ok ? 1 : 0)) return true;
   if (threadIdx.x == 0) atomicOr(status, kStatusWaitExpired);
-  mbar_wait_bounded(bar, 0);  // let the copy land before the block's shared memory is released
+  // Give the copy more time to land before the block's shared memory is released. This too is
+  // bounded, so it is a bound, not a guarantee: the copy is at most kMaxDynSmem bytes of this
+  // GPU's own memory, which the bulk-copy unit moves in microseconds, while the two waits
+  // together poll 9 * 2^22 times (each try_wait itself suspends for a while), far over a second.
+  // Returning with the copy still in flight would take a copy engine that has already stalled.
+  mbar_wait_polls(bar, 0, 8 * kWaitPolls);
   return false;
 }
 
@@ -582,7 +587,7 @@ nomad_status nomad_trace_regroup(nomad_ctx *ctx, const nomad_traversal &cfg, boo
 
 extern "C" nomad_status nomad_selftest_bounded_wait(nomad_ctx *ctx, int32_t complete) {
   if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
-  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  NOMAD_DEVICE_SCOPE(ctx);
   k_wait_selftest<<<1, 32, 0, ctx->stream>>>(ctx->status.as<uint32_t>(), complete ? 1 : 0, 1ll << 12);
   NOMAD_CUDA(ctx, cudaGetLastError());
   NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -619,7 +624,7 @@ extern "C" nomad_status nomad_autotune_sweep(nomad_ctx *ctx, const nomad_ray *ra
   if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
   if (!ctx->sceneReady) return nomad_fail(ctx, NOMAD_ERR_NOT_READY, "no scene uploaded");
   if (!rays || n == 0) return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "no sample rays");
-  NOMAD_CUDA(ctx, cudaSetDevice(ctx->device));
+  NOMAD_DEVICE_SCOPE(ctx);
   cudaStream_t s = ctx->stream;
   const float4 *d = reinterpret_cast<const float4 *>(rays);
   if (!(flags & NOMAD_TRACE_DEVICE_POINTERS)) {

@@ -121,9 +121,125 @@ def render(os_: "OracleScene", materials, views, pixels=None, obj_hits=False, th
     return out, hits, stats
 
 
+def render_tape(os_: "OracleScene", materials, views, tapes, pixels=None, threads=0):
+    """render() in tape mode: tapes[q] (float32, T per listed pixel) are the pixel's random numbers,
+    drawn in the reference's order (pathtrace.cpp, Draws). Returns rgb[n, 3]."""
+    lib = load()
+    if not hasattr(lib, "_render_tape_bound"):
+        lib.oracle_render_tape.argtypes = [_P, _P, C.c_uint32, _P, _P, _P, _P, _P, _P, C.c_uint32, C.c_uint32,
+                                           _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint32, _P, C.c_uint32]
+        lib.oracle_render_tape.restype = C.c_int
+        lib._render_tape_bound = True
+    views = np.ascontiguousarray(views).reshape(-1)
+    if pixels is None:
+        total = int((views["width"].astype(np.int64) * views["height"]).sum())
+        pixels = np.arange(total, dtype=np.uint64)
+    pixels = np.ascontiguousarray(pixels, np.uint64)
+    tapes = np.ascontiguousarray(tapes, np.float32)
+    assert tapes.shape[0] == pixels.size
+    out = np.zeros((pixels.size, 3), np.float32)
+    rc = lib.oracle_render_tape(_p(os_.bvh), _p(os_.tlas), os_.tlas.size // 8, _p(os_.prims),
+                                _p(np.ascontiguousarray(materials, np.float32)), _p(os_.prim_indices),
+                                _p(os_.active), _p(os_.blas_root), _p(os_.prim_object), os_.object_count,
+                                os_.prims.size // 28, _p(views), views.shape[0], _p(pixels), pixels.size, _p(out),
+                                threads, _p(tapes), tapes.shape[1])
+    assert rc == 0
+    return out
+
+
+RULE_VISIBILITY, RULE_REPROJECTION = 1, 2
+
+
+def set_reference_rules(rules: int, track: bool = False):
+    """Reference rules of the oracle's shading, for the pin against the reference's own code only
+    (pathtrace.cpp): RULE_VISIBILITY = the reference's closest-hit light test instead of the
+    contract's any-hit; RULE_REPROJECTION = temporal reprojection through the float matrix the pin
+    hands the reference. 0 = the contract (what the CUDA path does). With track, every light test
+    also evaluates the other visibility rule. Returns (tests, disagreements) since the last call."""
+    counts = np.zeros(2, np.uint64)
+    _bind("oracle_set_reference_rules", [C.c_int, C.c_int, _P])(int(rules), int(track), _p(counts))
+    return int(counts[0]), int(counts[1])
+
+
+def light_tables(os_: "OracleScene", materials):
+    """(indices, cdf, total, pdf per primitive) of the resident emissive primitives."""
+    lib = load()
+    if not hasattr(lib, "_lights_bound"):
+        lib.oracle_light_tables.argtypes = [_P, _P, _P, _P, _P, C.c_uint32, _P, _P, _P, _P]
+        lib.oracle_light_tables.restype = C.c_uint32
+        lib._lights_bound = True
+    n = os_.prims.size // 28
+    idx, cdf, pdf = np.zeros(n, np.uint32), np.zeros(n, np.float32), np.zeros(n, np.float32)
+    total = np.zeros(1, np.float32)
+    k = lib.oracle_light_tables(_p(os_.prims), _p(np.ascontiguousarray(materials, np.float32)), _p(os_.active),
+                                _p(os_.blas_root), _p(os_.prim_object), n, _p(idx), _p(cdf), _p(total), _p(pdf))
+    return idx[:k].copy(), cdf[:k].copy(), float(total[0]), pdf
+
+
+def _bind(name, argtypes):
+    lib = load()
+    fn = getattr(lib, name)
+    if not getattr(fn, "_bound", False):
+        fn.argtypes, fn.restype, fn._bound = argtypes, None, True
+    return fn
+
+
+def _c(a, dt, cols=None):
+    a = np.ascontiguousarray(a, dt)
+    return a if cols is None else a.reshape(-1, cols)
+
+
+def decode_material(mats, lod=1.0):
+    """decode() of each packed material: 17 floats (ref_decode_material's first 17)."""
+    mats = _c(mats, np.float32, 20)
+    out = np.zeros((mats.shape[0], 17), np.float32)
+    _bind("oracle_decode_material", [_P, C.c_uint32, C.c_float, _P])(_p(mats), mats.shape[0], lod, _p(out))
+    return out
+
+
+def bsdf(mats, nvl):
+    mats, nvl = _c(mats, np.float32, 20), _c(nvl, np.float32, 9)
+    out = np.zeros((nvl.shape[0], 3), np.float32)
+    _bind("oracle_bsdf", [_P, _P, C.c_uint32, _P])(_p(mats), _p(nvl), nvl.shape[0], _p(out))
+    return out
+
+
+def select_light(xi, cdf, total):
+    xi, cdf = _c(xi, np.float32), _c(cdf, np.float32)
+    off, pdf = np.zeros(xi.size, np.uint32), np.zeros(xi.size, np.float32)
+    _bind("oracle_select_light", [_P, C.c_uint32, _P, C.c_uint32, C.c_float, _P, _P])(
+        _p(xi), xi.size, _p(cdf), cdf.size, float(total), _p(off), _p(pdf))
+    return off, pdf
+
+
+def sample_light_point(prims, uv):
+    prims, uv = _c(prims, np.float32, 28), _c(uv, np.float32, 2)
+    out, ok = np.zeros((uv.shape[0], 7), np.float32), np.zeros(uv.shape[0], np.uint8)
+    _bind("oracle_light_point", [_P, _P, C.c_uint32, _P, _P])(_p(prims), _p(uv), uv.shape[0], _p(out), _p(ok))
+    return out, ok
+
+
+def scatter(dn, front, mats, tape4):
+    dn, mats, tape4 = _c(dn, np.float32, 6), _c(mats, np.float32, 20), _c(tape4, np.float32, 4)
+    n = dn.shape[0]
+    d, w, k = np.zeros((n, 3), np.float32), np.zeros((n, 3), np.float32), np.zeros(n, np.uint32)
+    _bind("oracle_scatter", [_P, _P, _P, _P, C.c_uint32, _P, _P, _P])(
+        _p(dn), _p(_c(front, np.uint8)), _p(mats), _p(tape4), n, _p(d), _p(w), _p(k))
+    return d, w, k
+
+
+def reservoir_chain(cand, xi):
+    chains, k = xi.shape
+    cand, xi = _c(cand, np.float32, 16), _c(xi, np.float32)
+    out = np.zeros((chains, 18), np.float32)
+    _bind("oracle_reservoir_chain", [_P, _P, C.c_uint32, C.c_uint32, _P])(_p(cand), _p(xi), chains, k, _p(out))
+    return out
+
+
 class RestirOracle:
     """Chains oracle_render_restir over consecutive frames (keeps the previous frame's
-    reservoirs, surfaces and views)."""
+    reservoirs, surfaces and views). With tapes (reference mode only), render(views, tapes)
+    draws each path's random numbers from tapes[path] in the reference's order."""
 
     def __init__(self, os_, materials, candidates=32, temporal=True, spatial=3, radius_px=30.0, m_cap=20.0,
                  reference_mode=False):
@@ -133,6 +249,8 @@ class RestirOracle:
                                                  C.c_uint32, _P, C.c_uint32, _P, _P, _P, _P, _P, C.c_int,
                                                  _P, _P, _P, _P, C.c_uint32]
             lib.oracle_render_restir.restype = C.c_int
+            lib.oracle_render_restir_tape.argtypes = lib.oracle_render_restir.argtypes + [_P, C.c_uint32]
+            lib.oracle_render_restir_tape.restype = C.c_int
             lib._restir_bound = True
         self.os_ = os_
         self.mats = np.ascontiguousarray(materials, np.float32)
@@ -140,7 +258,7 @@ class RestirOracle:
         self.cfg_f = np.array([radius_px, m_cap], np.float32)
         self.prev = None
 
-    def render(self, views):
+    def render(self, views, tapes=None):
         lib = load()
         os_ = self.os_
         views = np.ascontiguousarray(views).reshape(-1)
@@ -153,14 +271,19 @@ class RestirOracle:
         have = self.prev is not None and self.prev[2].shape == views.shape and all(
             (self.prev[2][k] == views[k]).all() for k in ("width", "height", "spp"))
         pr, ps, pv = self.prev if have else (resv, surf, views)
-        rc = lib.oracle_render_restir(_p(os_.bvh), _p(os_.tlas), os_.tlas.size // 8, _p(os_.prims),
-                                      _p(self.mats), _p(os_.prim_indices), _p(os_.active),
-                                      _p(os_.blas_root), _p(os_.prim_object), os_.object_count,
-                                      os_.prims.size // 28, _p(views), views.shape[0], _p(self.cfg_u),
-                                      _p(self.cfg_f), _p(pr), _p(ps), _p(np.ascontiguousarray(pv)),
-                                      int(have), _p(resv), _p(surf), _p(rgb), _p(stats), 0)
+        args = (_p(os_.bvh), _p(os_.tlas), os_.tlas.size // 8, _p(os_.prims), _p(self.mats), _p(os_.prim_indices),
+                _p(os_.active), _p(os_.blas_root), _p(os_.prim_object), os_.object_count, os_.prims.size // 28,
+                _p(views), views.shape[0], _p(self.cfg_u), _p(self.cfg_f), _p(pr), _p(ps),
+                _p(np.ascontiguousarray(pv)), int(have), _p(resv), _p(surf), _p(rgb), _p(stats), 0)
+        if tapes is None:
+            rc = lib.oracle_render_restir(*args)
+        else:
+            tapes = np.ascontiguousarray(tapes, np.float32)
+            assert tapes.shape[0] == P
+            rc = lib.oracle_render_restir_tape(*args, _p(tapes), tapes.shape[1])
         assert rc == 0
         self.prev = (resv, surf, views.copy())
+        self.last = (resv, surf)
         return rgb, stats
 
 

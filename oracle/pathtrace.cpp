@@ -16,7 +16,9 @@
 //   * sin/cos(2 pi u), log2, exp2 and x^5 are defined by fixed polynomials/products (below) so
 //     that host and device round identically;
 //   * traversal and shadow visibility follow the contract (contract_core.h): lowest-index tie
-//     rule, true any-hit shadow rays over (1e-4, dist - 1e-4);
+//     rule, true any-hit shadow rays over (1e-4, dist - 0.001) for one-sample NEE (the reference's
+//     acceptance window, PathTracing.h:1832-1834) and (1e-4, dist - 1e-4) for ReSTIR's
+//     isLightVisible (:549-552);
 //   * a path whose throughput becomes exactly zero stops (the reference keeps tracing it with no
 //     effect on radiance);
 //   * clamping to [0, 1] is optional (NOMAD_VIEW_CLAMP) so HDR radiance can be compared.
@@ -27,6 +29,7 @@
 #include <vector>
 
 #include "contract_core.h"
+#include "view_projection.h"
 
 using namespace oracle_core;
 
@@ -82,6 +85,28 @@ U4 philox(U4 c, uint32_t k0, uint32_t k1) {
   return c;
 }
 inline float u01(uint32_t x) { return (float)(x >> 8) * (1.0f / 16777216.0f); }
+
+// Where a path's random numbers come from. Philox mode (tape == nullptr; the CUDA kernels'
+// scheme): every draw has a fixed slot, a lane of a Philox block, and take() returns that slot's
+// value, so a draw that a branch skips leaves every other draw unchanged. Tape mode: take()
+// returns the caller's numbers in the order the draws are made and skip() drops one, which is the
+// reference's scheme (u = randomFloat(seed); seed = random(seed), Random.h:6-17), where a skipped
+// draw shifts the later ones. Every draw below is made at the point, and under the conditions,
+// where the reference makes it, so the same code runs on identical numbers as the reference's
+// shader code does when that code is handed the same tape (oracle/ref/ref_shade.cpp).
+struct Draws {
+  const float *tape = nullptr;
+  uint32_t pos = 0, len = 0;
+  float take(float slot) {
+    if (!tape) return slot;
+    const float u = pos < len ? tape[pos] : 0.5f;
+    ++pos;
+    return u;
+  }
+  void skip() {
+    if (tape) ++pos;
+  }
+};
 
 void sincos_turns(float u, float &s, float &c) {
   float t = u * 8.0f;
@@ -205,7 +230,8 @@ void onb(V n, V &t, V &b) {
   b = nrmz(crs(n, t));
 }
 
-V scatter(V inDir, V normal, bool front, const Mat &m, float xiLobe, float u1, float u2, float xiF, V &out) {
+V scatter(V inDir, V normal, bool front, const Mat &m, Draws &dr, float xiLobe, float u1, float u2, float xiF,
+          V &out) {
   float dw = mx(lum(m.diffuse) * m.opacity, 0.0f);
   float sw = mx(lum(m.specular) * m.opacity, 0.0f);
   float tw = mx(lum(m.transmission) * (1.0f - m.opacity), 0.0f);
@@ -215,8 +241,10 @@ V scatter(V inDir, V normal, bool front, const Mat &m, float xiLobe, float u1, f
     out = normal;
     return v(0, 0, 0);
   }
-  float xi = xiLobe * total;
+  float xi = dr.take(xiLobe) * total;
   if (xi < dw) {
+    u1 = dr.take(u1);
+    u2 = dr.take(u2);
     float r = std::sqrt(mx(0.0f, u1));
     float s, c;
     sincos_turns(u2, s, c);
@@ -234,6 +262,8 @@ V scatter(V inDir, V normal, bool front, const Mat &m, float xiLobe, float u1, f
       float sm = c01(1.0f - m.roughness);
       ex = mx(ex, mx(1.0f, sm * sm * 256.0f));
     }
+    u1 = dr.take(u1);
+    u2 = dr.take(u2);
     float ct = pow_pos(u1, 1.0f / (ex + 1.0f));
     float st = std::sqrt(mx(0.0f, 1.0f - ct * ct));
     float s, c;
@@ -251,6 +281,7 @@ V scatter(V inDir, V normal, bool front, const Mat &m, float xiLobe, float u1, f
   float r0 = (1.0f - ratio) / (1.0f + ratio);
   r0 = r0 * r0;
   float refl_ = r0 + (1.0f - r0) * p5(1.0f - cosT);
+  xiF = dr.take(xiF);
   if ((ratio * sinT > 1.0f) || (refl_ > xiF)) {
     out = refl(inDir, normal);
     return dvs(m.specular, prob);
@@ -270,12 +301,14 @@ V scatter(V inDir, V normal, bool front, const Mat &m, float xiLobe, float u1, f
   return dvs(m.transmission, prob);
 }
 
-bool light_point(const float *prims, uint32_t lp, float u1, float u2, V &pos, V &nrm, float &area) {
+bool light_point(const float *prims, uint32_t lp, Draws &dr, float u1, float u2, V &pos, V &nrm, float &area) {
   const float *g = prims + 28ll * lp;
   int type = (int)g[3];
   if (type == 0) {
     float radius = g[4];
     if (radius <= 0.0f) return false;
+    u1 = dr.take(u1);
+    u2 = dr.take(u2);
     float z = 2.0f * u1 - 1.0f;
     float s, c;
     sincos_turns(u2, s, c);
@@ -287,6 +320,8 @@ bool light_point(const float *prims, uint32_t lp, float u1, float u2, V &pos, V 
     return area > 0.0f;
   }
   if (type == 1) {
+    u1 = dr.take(u1);
+    u2 = dr.take(u2);
     float su1 = std::sqrt(u1);
     float b0 = 1.0f - su1, b1 = su1 * (1.0f - u2), b2 = su1 * u2;
     V v0 = v(g[0], g[1], g[2]), v1 = v(g[4], g[5], g[6]), v2 = v(g[8], g[9], g[10]);
@@ -299,6 +334,8 @@ bool light_point(const float *prims, uint32_t lp, float u1, float u2, V &pos, V 
     return area > 0.0f;
   }
   if (type == 2) {
+    u1 = dr.take(u1);
+    u2 = dr.take(u2);
     float su = u1 * 2.0f - 1.0f, sv = u2 * 2.0f - 1.0f;
     V c = v(g[0], g[1], g[2]), e1 = v(g[4], g[5], g[6]), e2 = v(g[8], g[9], g[10]);
     pos = add(add(c, scl(e1, su)), scl(e2, sv));
@@ -362,6 +399,23 @@ uint32_t select_light(float xi, const LightsH &L) {
   return lo < n - 1 ? lo : n - 1;
 }
 
+// lightPdfFromCdf (PathTracing.h:237-247): the chosen slot's share of the total weight.
+float light_pdf(const LightsH &L, uint32_t off) {
+  float prev = off > 0 ? L.cdf[off - 1] : 0.0f;
+  float w = L.cdf[off] - prev;
+  return (L.total > 0.0f && w > 0.0f) ? w / L.total : 0.0f;
+}
+
+// The per-primitive light pdf the reservoir reuse reads (lightPdfLookup, Renderer.cpp:5195-5208).
+std::vector<float> light_pdf_lookup(const LightsH &L, uint32_t prim_count) {
+  std::vector<float> out(prim_count, 0.0f);
+  for (size_t k = 0; k < L.idx.size(); ++k) {
+    float w = L.cdf[k] - (k ? L.cdf[k - 1] : 0.0f);
+    if (w > 0.0f && L.total > 0.0f) out[L.idx[k]] = w / L.total;
+  }
+  return out;
+}
+
 struct Ctx {
   Scene s;
   const float *mats;
@@ -377,6 +431,40 @@ Hit closest(const Ctx &c, const Ray &r) {
   if (h.prim < 0) h.t = INFINITY;
   return h;
 }
+// Reference rules for the shading pin (oracle_set_reference_rules; off by default, and off for
+// everything the CUDA path is checked against):
+//   kRuleVisibility: light visibility by the reference's own test, a closest hit over the whole
+//     ray, visible iff nothing is hit or the hit is the light primitive itself at t >= dist - eps
+//     (isLightVisible :549-552, NEE :1828-1834), instead of the contract's any-hit over
+//     (1e-4, dist - eps). They differ only when the light is numerically missed with something
+//     behind it, or an occluder lies within eps in front of the light; the counters record how
+//     many shadow decisions the two rules take differently.
+//   kRuleReprojection: ReSTIR reference mode finds the temporal source pixel through the float
+//     view-projection matrix the pin hands the reference, with the reference's arithmetic
+//     (view_projection.h), instead of the contract's ray-plane intersection with the previous
+//     view; the two round differently within a hair of a pixel boundary.
+constexpr int kRuleVisibility = 1, kRuleReprojection = 2;
+std::atomic<int> g_vis_rule{0}, g_vis_track{0};
+std::atomic<uint64_t> g_vis_tests{0}, g_vis_differ{0};
+
+bool occluded(const Ctx &c, const Ray &r);
+
+// Is the light primitive `lp`, sampled at distance dist, visible along r (r.tmax = dist - eps,
+// at least 1e-4)? Counts rule disagreements while tracking is on.
+bool light_visible(const Ctx &c, const Ray &r, int32_t lp, float dist, float eps) {
+  const bool contractVis = !occluded(c, r);
+  if (!(g_vis_rule.load(std::memory_order_relaxed) & kRuleVisibility) && !g_vis_track.load(std::memory_order_relaxed))
+    return contractVis;
+  Hit h{INFINITY, 0.0f, 0.0f, -1, -1};
+  Ray full = r;
+  full.tmax = INFINITY;
+  trace_near_first<false>(c.s, full, h, nullptr);
+  const bool refVis = h.prim < 0 || (h.prim == lp && h.t >= dist - eps);
+  g_vis_tests.fetch_add(1, std::memory_order_relaxed);
+  if (refVis != contractVis) g_vis_differ.fetch_add(1, std::memory_order_relaxed);
+  return (g_vis_rule.load(std::memory_order_relaxed) & kRuleVisibility) ? refVis : contractVis;
+}
+
 bool occluded(const Ctx &c, const Ray &r) {
   Hit h{r.tmax, 0.0f, 0.0f, -1, -1};
   trace_near_first<true>(c.s, r, h, nullptr);
@@ -390,18 +478,23 @@ struct RestirOut {
   bool direct = false;  // reference mode: visibility already applied, added as is
   V origin, dir, contrib;
   float tmax = 0.0f;
+  uint32_t tapePos = 0;  // tape mode: where the rest of the path continues drawing
 };
 const uint32_t VIEW_RESTIR = 2u;
 
+// Tape mode: the pixel's two jitter numbers are drawn first, as pathTraceKernel draws them
+// (PathTraceKernel.metal:91-94), whether or not the view jitters.
 V path(const Ctx &c, const View &vw, uint32_t vi, uint32_t pixel, uint32_t sample, uint32_t *objHits,
-       uint64_t *stats, const RestirOut *rs = nullptr) {
+       uint64_t *stats, const RestirOut *rs, Draws &dr) {
   uint32_t k0 = vw.seedLo, k1 = vw.seedHi + vw.frame;
   uint32_t px = pixel % vw.w, py = pixel / vw.w;
   U4 r0 = philox(U4{pixel, sample, 255u * 4u, vi}, k0, k1);
   float ux = ((float)px + 0.5f) / (float)vw.w, uy = ((float)py + 0.5f) / (float)vw.h;
   bool center = (vw.flags & 4u) != 0;
-  float s = ux + (center ? 0.0f : (u01(r0.x) - 0.5f) / (float)vw.w);
-  float t = uy + (center ? 0.0f : (u01(r0.y) - 0.5f) / (float)vw.h);
+  const float jx = dr.take(u01(r0.x)), jy = dr.take(u01(r0.y));
+  if (dr.tape && rs) dr.pos = rs->tapePos;  // the ReSTIR pass drew the pixel's numbers up to here
+  float s = ux + (center ? 0.0f : (jx - 0.5f) / (float)vw.w);
+  float t = uy + (center ? 0.0f : (jy - 0.5f) / (float)vw.h);
   V d = v(vw.fp[0] + s * vw.vu[0] + t * vw.vv[0] - vw.cam[0], vw.fp[1] + s * vw.vu[1] + t * vw.vv[1] - vw.cam[1],
           vw.fp[2] + s * vw.vu[2] + t * vw.vv[2] - vw.cam[2]);
   V dir = nrmz(d);
@@ -441,11 +534,12 @@ V path(const Ctx &c, const View &vw, uint32_t vi, uint32_t pixel, uint32_t sampl
         if (rs->direct || !occluded(c, mkray(rs->origin, rs->dir, rs->tmax))) rad = add(rad, rs->contrib);
       }
     } else if (lum(dc) > 0.0f && !c.L.idx.empty() && c.L.total > 0.0f) {
-      uint32_t off = select_light(u01(b0.x), c.L);
+      uint32_t off = select_light(dr.take(u01(b0.x)), c.L);
       uint32_t lp = c.L.idx[off];
       V lpos, lnrm;
       float area = 0.0f;
-      if ((int32_t)lp != h.prim && light_point(c.s.prims, lp, u01(b0.y), u01(b0.z), lpos, lnrm, area) && area > 0.0f) {
+      if ((int32_t)lp != h.prim && light_point(c.s.prims, lp, dr, u01(b0.y), u01(b0.z), lpos, lnrm, area) &&
+          area > 0.0f) {
         V toL = vsub(lpos, p);
         float d2 = dt(toL, toL);
         if (d2 > RAY_EPS) {
@@ -453,17 +547,17 @@ V path(const Ctx &c, const View &vw, uint32_t vi, uint32_t pixel, uint32_t sampl
           V wi = dvs(toL, dist);
           float cosT = mx(dt(n, wi), 0.0f), cosL = mx(dt(lnrm, neg(wi)), 0.0f);
           if (cosT > 0.0f && cosL > 0.0f) {
-            float prev = off > 0 ? c.L.cdf[off - 1] : 0.0f;
-            float w = c.L.cdf[off] - prev;
-            float lpdf = (c.L.total > 0.0f && w > 0.0f) ? w / c.L.total : 0.0f;
+            float lpdf = light_pdf(c.L, off);
             if (lpdf > 0.0f) {
               float totalPdf = lpdf * ((1.0f / area) * d2 / cosL);
               if (totalPdf > 0.0f) {
-                float tmax = dist - RAY_EPS;
+                // visible when the closest hit is the light itself at t >= dist - 0.001
+                // (PathTracing.h:1832-1834): the any-hit window ends there
+                float tmax = dist - 0.001f;
                 if (tmax < RAY_EPS) tmax = RAY_EPS;
                 stats[2]++;
                 Ray sr = mkray(add(p, scl(n, 0.0005f)), wi, tmax);
-                if (!occluded(c, sr)) {
+                if (light_visible(c, sr, (int32_t)lp, dist, 0.001f)) {
                   Mat lm = decode(c.mats, (int32_t)lp, 1.0f);
                   V lrad = scl(lm.emission, lm.power);
                   V b = bsdf(m, n, nrmz(neg(dir)), wi);
@@ -476,14 +570,15 @@ V path(const Ctx &c, const View &vw, uint32_t vi, uint32_t pixel, uint32_t sampl
       }
     }
     V nd;
-    V wgt = scatter(dir, n, front, m, u01(b0.w), u01(b1.x), u01(b1.y), u01(b1.w), nd);
+    V wgt = scatter(dir, n, front, m, dr, u01(b0.w), u01(b1.x), u01(b1.y), u01(b1.w), nd);
+    dr.skip();  // the reference advances its seed once more after scatter (PathTracing.h:1855)
     V bias = dt(nd, n) < 0.0f ? neg(n) : n;
     org = add(p, scl(bias, RAY_EPS));
     dir = nd;
     thr = mul(thr, wgt);
     if (depth >= 5) {
       float pm = mx(thr.x, mx(thr.y, thr.z));
-      if (u01(b1.z) >= pm) break;
+      if (dr.take(u01(b1.z)) >= pm) break;
       thr = dvs(thr, pm);
     }
     if (thr.x == 0.0f && thr.y == 0.0f && thr.z == 0.0f) break;
@@ -491,19 +586,12 @@ V path(const Ctx &c, const View &vw, uint32_t vi, uint32_t pixel, uint32_t sampl
   return rad;
 }
 
-}  // namespace
-
-extern "C" {
-
-// Renders the listed pixels (global pixel indices over the concatenated views) into out
-// (3 floats per listed pixel). views: nomad_view structs. obj_hits (object_count counters) and
-// stats (4 counters: rays, escapes, shadow rays, hits) may be null; they accumulate over the
-// listed pixels only.
-int oracle_render(const float *bvh, const float *tlas, uint32_t tlas_count, const float *prims,
-                  const float *materials, const int32_t *prim_indices, const uint8_t *active,
-                  const int32_t *blas_root, const int32_t *prim_object, uint32_t object_count,
-                  uint32_t prim_count, const void *views, uint32_t nviews, const uint64_t *pixels,
-                  uint64_t npix, float *out, uint32_t *obj_hits, uint64_t *stats, uint32_t threads) {
+int render_impl(const float *bvh, const float *tlas, uint32_t tlas_count, const float *prims,
+                const float *materials, const int32_t *prim_indices, const uint8_t *active,
+                const int32_t *blas_root, const int32_t *prim_object, uint32_t object_count,
+                uint32_t prim_count, const void *views, uint32_t nviews, const uint64_t *pixels,
+                uint64_t npix, float *out, uint32_t *obj_hits, uint64_t *stats, uint32_t threads,
+                const float *tapes, uint32_t tape_len) {
   if (!bvh || !tlas || !prims || !materials || !views || !out || !pixels) return 1;
   Ctx c{{bvh, tlas, tlas_count, prims, prim_indices, active, blas_root, prim_object}, materials, {}, object_count};
   c.L = build_lights(prims, materials, active, blas_root, prim_object, prim_count);
@@ -527,8 +615,10 @@ int oracle_render(const float *bvh, const float *tlas, uint32_t tlas_count, cons
         uint32_t pixel = (uint32_t)(g - voff[vi]);
         bool cl = (vw.flags & VIEW_CLAMP) != 0;
         float ax = 0.0f, ay = 0.0f, az = 0.0f;
+        Draws dr;  // tape mode: one tape per listed pixel, drawn on across its samples
+        if (tapes) dr = Draws{tapes + q * tape_len, 0, tape_len};
         for (uint32_t s = 0; s < vw.spp; ++s) {
-          V r = path(c, vw, vi, pixel, s, obj_hits ? hits[tid].data() : nullptr, st[tid].data());
+          V r = path(c, vw, vi, pixel, s, obj_hits ? hits[tid].data() : nullptr, st[tid].data(), nullptr, dr);
           if (cl) r = v(c01(r.x), c01(r.y), c01(r.z));
           ax = ax + r.x;
           ay = ay + r.y;
@@ -559,6 +649,38 @@ int oracle_render(const float *bvh, const float *tlas, uint32_t tlas_count, cons
     for (auto &s : st)
       for (int k = 0; k < 4; ++k) stats[k] += s[k];
   return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Renders the listed pixels (global pixel indices over the concatenated views) into out
+// (3 floats per listed pixel). views: nomad_view structs. obj_hits (object_count counters) and
+// stats (4 counters: rays, escapes, shadow rays, hits) may be null; they accumulate over the
+// listed pixels only.
+int oracle_render(const float *bvh, const float *tlas, uint32_t tlas_count, const float *prims,
+                  const float *materials, const int32_t *prim_indices, const uint8_t *active,
+                  const int32_t *blas_root, const int32_t *prim_object, uint32_t object_count,
+                  uint32_t prim_count, const void *views, uint32_t nviews, const uint64_t *pixels,
+                  uint64_t npix, float *out, uint32_t *obj_hits, uint64_t *stats, uint32_t threads) {
+  return render_impl(bvh, tlas, tlas_count, prims, materials, prim_indices, active, blas_root, prim_object,
+                     object_count, prim_count, views, nviews, pixels, npix, out, obj_hits, stats, threads,
+                     nullptr, 0);
+}
+
+// oracle_render in tape mode: `tapes` holds tape_len uniforms per listed pixel, drawn in the
+// reference's order (Draws), so the output can be compared with the reference's own
+// pathTraceKernel / rayColor run on the same numbers.
+int oracle_render_tape(const float *bvh, const float *tlas, uint32_t tlas_count, const float *prims,
+                       const float *materials, const int32_t *prim_indices, const uint8_t *active,
+                       const int32_t *blas_root, const int32_t *prim_object, uint32_t object_count,
+                       uint32_t prim_count, const void *views, uint32_t nviews, const uint64_t *pixels,
+                       uint64_t npix, float *out, uint32_t threads, const float *tapes, uint32_t tape_len) {
+  if (!tapes || tape_len == 0) return 1;
+  return render_impl(bvh, tlas, tlas_count, prims, materials, prim_indices, active, blas_root, prim_object,
+                     object_count, prim_count, views, nviews, pixels, npix, out, nullptr, nullptr, threads,
+                     tapes, tape_len);
 }
 
 }  // extern "C"
@@ -692,13 +814,15 @@ bool ref_visible(const Ctx &cx, const SurfH &s, const RefC &c) {
   float tmax = c.dist - RAY_EPS;
   if (tmax < RAY_EPS) tmax = RAY_EPS;
   V o = add(v(s.p[0], s.p[1], s.p[2]), scl(v(s.n[0], s.n[1], s.n[2]), 5.0f * RAY_EPS));
-  return !occluded(cx, mkray(o, c.wi, tmax));
+  return light_visible(cx, mkray(o, c.wi, tmax), c.lp, c.dist, RAY_EPS);
 }
 
-void ref_update(ResvH &r, V &contrib, const RefC &c, V cc, float w, float inc, float xi) {
+// restirUpdateReservoir (:97-115): the acceptance number is drawn only for a positive weight.
+void ref_update(ResvH &r, V &contrib, const RefC &c, V cc, float w, float inc, Draws &dr, float xiSlot) {
   if (w <= 0.0f || inc <= 0.0f) return;
   r.c[1] = r.c[1] + w;
   r.c[2] = r.c[2] + inc;
+  const float xi = dr.take(xiSlot);
   if (fbi(r.a[3]) < 0 || xi * r.c[1] < w) {
     r.a[0] = c.lpos.x; r.a[1] = c.lpos.y; r.a[2] = c.lpos.z; r.a[3] = ibf(c.lp);
     r.b[0] = c.lnrm.x; r.b[1] = c.lnrm.y; r.b[2] = c.lnrm.z; r.b[3] = c.invArea;
@@ -717,13 +841,15 @@ float view_lod(const View &vw) {
 
 }  // namespace
 
-extern "C" int oracle_render_restir(const float *bvh, const float *tlas, uint32_t tlas_count, const float *prims,
-                                    const float *materials, const int32_t *prim_indices, const uint8_t *active,
-                                    const int32_t *blas_root, const int32_t *prim_object, uint32_t object_count,
-                                    uint32_t prim_count, const void *views, uint32_t nviews, const uint32_t *cfg_u,
-                                    const float *cfg_f, const float *prev_resv, const float *prev_surf,
-                                    const void *prev_views, int have_prev, float *out_resv, float *out_surf,
-                                    float *out_rgb, uint64_t *stats, uint32_t threads) {
+namespace {
+
+int restir_impl(const float *bvh, const float *tlas, uint32_t tlas_count, const float *prims,
+                const float *materials, const int32_t *prim_indices, const uint8_t *active,
+                const int32_t *blas_root, const int32_t *prim_object, uint32_t object_count,
+                uint32_t prim_count, const void *views, uint32_t nviews, const uint32_t *cfg_u,
+                const float *cfg_f, const float *prev_resv, const float *prev_surf,
+                const void *prev_views, int have_prev, float *out_resv, float *out_surf,
+                float *out_rgb, uint64_t *stats, uint32_t threads, const float *tapes, uint32_t tape_len) {
   Ctx c{{bvh, tlas, tlas_count, prims, prim_indices, active, blas_root, prim_object}, materials, {}, object_count};
   c.L = build_lights(prims, materials, active, blas_root, prim_object, prim_count);
   const View *vs = static_cast<const View *>(views);
@@ -764,12 +890,7 @@ extern "C" int oracle_render_restir(const float *bvh, const float *tlas, uint32_
   std::vector<RestirOut> roAll;
   std::vector<std::vector<uint64_t>> refStats(threads, std::vector<uint64_t>(4, 0));
   if (refMode) {
-    // lightPdfLookup: the per-primitive light pdf of the current CDF
-    std::vector<float> lpdfOf(prim_count, 0.0f);
-    for (size_t k = 0; k < c.L.idx.size(); ++k) {
-      float w = c.L.cdf[k] - (k ? c.L.cdf[k - 1] : 0.0f);
-      if (w > 0.0f && c.L.total > 0.0f) lpdfOf[c.L.idx[k]] = w / c.L.total;
-    }
+    const std::vector<float> lpdfOf = light_pdf_lookup(c.L, prim_count);
     roAll.resize(P);
     par([&](uint64_t pid, uint32_t tid) {
       uint32_t vi = view_of(pid);
@@ -782,13 +903,16 @@ extern "C" int oracle_render_restir(const float *bvh, const float *tlas, uint32_
       uint32_t pixel = (uint32_t)(local / vw.spp), sample = (uint32_t)(local % vw.spp);
       uint32_t k0 = vw.seedLo, k1 = vw.seedHi + vw.frame;
       int32_t hitPrim = -1;
+      Draws dr;  // tape mode: one tape per path
+      if (tapes) dr = Draws{tapes + pid * tape_len, 0, tape_len};
+      U4 r0 = philox(U4{pixel, sample, 255u * 4u, vi}, k0, k1);
+      const float jx = dr.take(u01(r0.x)), jy = dr.take(u01(r0.y));
       if ((vw.flags & VIEW_RESTIR) && !c.L.idx.empty() && c.L.total > 0.0f) {
         uint32_t px = pixel % vw.w, py = pixel / vw.w;
-        U4 r0 = philox(U4{pixel, sample, 255u * 4u, vi}, k0, k1);
         float ux = ((float)px + 0.5f) / (float)vw.w, uy = ((float)py + 0.5f) / (float)vw.h;
         bool center = (vw.flags & 4u) != 0;
-        float ss = ux + (center ? 0.0f : (u01(r0.x) - 0.5f) / (float)vw.w);
-        float tt = uy + (center ? 0.0f : (u01(r0.y) - 0.5f) / (float)vw.h);
+        float ss = ux + (center ? 0.0f : (jx - 0.5f) / (float)vw.w);
+        float tt = uy + (center ? 0.0f : (jy - 0.5f) / (float)vw.h);
         V d = nrmz(v(vw.fp[0] + ss * vw.vu[0] + tt * vw.vv[0] - vw.cam[0], vw.fp[1] + ss * vw.vu[1] + tt * vw.vv[1] - vw.cam[1],
                     vw.fp[2] + ss * vw.vu[2] + tt * vw.vv[2] - vw.cam[2]));
         V o = v(vw.cam[0], vw.cam[1], vw.cam[2]);
@@ -811,15 +935,14 @@ extern "C" int oracle_render_restir(const float *bvh, const float *tlas, uint32_
         Mat m = decode(materials, hitPrim, view_lod(vw));
         for (uint32_t k = 0; k < C; ++k) {
           U4 u = philox(U4{pixel, sample, 0x10000u + k, vi}, k0, k1);
-          uint32_t off = select_light(u01(u.x), c.L);
+          uint32_t off = select_light(dr.take(u01(u.x)), c.L);
           int32_t lp = (int32_t)c.L.idx[off];
           if (lp == hitPrim) continue;
           V lpos, lnrm;
           float area = 0.0f;
-          if (!light_point(prims, (uint32_t)lp, u01(u.y), u01(u.z), lpos, lnrm, area) || !(area > 0.0f)) continue;
-          float prev = off > 0 ? c.L.cdf[off - 1] : 0.0f;
-          float wgt = c.L.cdf[off] - prev;
-          float lightPdf = wgt > 0.0f ? wgt / c.L.total : 0.0f;
+          if (!light_point(prims, (uint32_t)lp, dr, u01(u.y), u01(u.z), lpos, lnrm, area) || !(area > 0.0f))
+            continue;
+          float lightPdf = light_pdf(c.L, off);
           Mat lm = decode(materials, lp, 1.0f);
           RefC cd;
           if (!ref_geometry(s, m, lpos, lnrm, 1.0f / area, lightPdf, scl(lm.emission, lm.power), lp, cd)) continue;
@@ -828,7 +951,7 @@ extern "C" int oracle_render_restir(const float *bvh, const float *tlas, uint32_
           V cc = dvs(cd.radG, cd.pdf);
           float target = mx(lum(cd.radG), 0.0f);
           float w = cd.pdf > 0.0f ? target / cd.pdf : 0.0f;
-          ref_update(r, contrib, cd, cc, w, 1.0f, u01(u.w));
+          ref_update(r, contrib, cd, cc, w, 1.0f, dr, u01(u.w));
         }
         const float currentM = r.c[2];
         if (have_prev && temporal) {
@@ -842,6 +965,12 @@ extern "C" int oracle_render_restir(const float *bvh, const float *tlas, uint32_
               int nx = (int)(pixel % vw.w) + dx[k], ny = (int)(pixel / vw.w) + dy[k];
               if (nx < 0 || ny < 0 || nx >= (int)pv.w || ny >= (int)pv.h) return false;
               qid = (int64_t)(poff[vi] + ((uint64_t)ny * pv.w + nx) * pv.spp + sample);
+            } else if (g_vis_rule.load(std::memory_order_relaxed) & kRuleReprojection) {
+              float m[16];
+              oracle_vp::build(pv.cam, pv.vu, pv.vv, pv.fp, m);
+              uint32_t ppx = 0, ppy = 0;
+              if (!oracle_vp::reproject(m, s.p, pv.w, pv.h, ppx, ppy)) return false;
+              qid = (int64_t)(poff[vi] + ((uint64_t)ppy * pv.w + ppx) * pv.spp + sample);
             } else {
               V cam = v(pv.cam[0], pv.cam[1], pv.cam[2]), U = v(pv.vu[0], pv.vu[1], pv.vu[2]);
               V Vv = v(pv.vv[0], pv.vv[1], pv.vv[2]), fp = v(pv.fp[0], pv.fp[1], pv.fp[2]);
@@ -899,7 +1028,7 @@ extern "C" int oracle_render_restir(const float *bvh, const float *tlas, uint32_
             float mis = den > 0.0f ? (q.c[2] * sp) / den : 0.0f;
             w = w * mis;
             U4 rr = philox(U4{pixel, sample, 0x31000u + k, vi}, k0, k1);
-            ref_update(r, contrib, cd, cc, w, q.c[2], u01(rr.x));
+            ref_update(r, contrib, cd, cc, w, q.c[2], dr, u01(rr.x));
           }
           if (pvOk[4] && cOk[4] && visOk[4]) {
             const RefC &cd = rc[4];
@@ -924,7 +1053,7 @@ extern "C" int oracle_render_restir(const float *bvh, const float *tlas, uint32_
             float mis = den > 0.0f ? (q.c[2] * tp * J) / den : 0.0f;
             w = w * mis;
             U4 rr = philox(U4{pixel, sample, 0x21000u, vi}, k0, k1);
-            ref_update(r, contrib, cd, cc, w, q.c[2], u01(rr.x));
+            ref_update(r, contrib, cd, cc, w, q.c[2], dr, u01(rr.x));
           }
         }
         if (fbi(r.a[3]) >= 0 && r.c[3] > 0.0f && r.c[2] > 0.0f) {
@@ -934,6 +1063,7 @@ extern "C" int oracle_render_restir(const float *bvh, const float *tlas, uint32_
           ro.contrib = scl(contrib, norm);
         }
       }
+      ro.tapePos = dr.pos;
       rFin[pid] = r;
       roAll[pid] = ro;
     });
@@ -973,7 +1103,9 @@ extern "C" int oracle_render_restir(const float *bvh, const float *tlas, uint32_
             int32_t lp = (int32_t)c.L.idx[off];
             V lpos{0, 0, 0}, lnrm{0, 0, 0};
             float area = 0.0f, w = 0.0f, ph = 0.0f;
-            if (lp != h.prim && light_point(prims, (uint32_t)lp, u01(u.y), u01(u.z), lpos, lnrm, area) && area > 0.0f) {
+            Draws slots;
+            if (lp != h.prim && light_point(prims, (uint32_t)lp, slots, u01(u.y), u01(u.z), lpos, lnrm, area) &&
+                area > 0.0f) {
               float prev = off > 0 ? c.L.cdf[off - 1] : 0.0f;
               float wgt = c.L.cdf[off] - prev;
               float lpdf = wgt > 0.0f ? wgt / c.L.total : 0.0f;
@@ -1084,7 +1216,10 @@ extern "C" int oracle_render_restir(const float *bvh, const float *tlas, uint32_
       }
     }
     uint64_t local = pid - poff[vi];
-    pathRad[pid] = path(c, vw, vi, (uint32_t)(local / vw.spp), (uint32_t)(local % vw.spp), nullptr, st[tid].data(), &ro);
+    Draws dr;
+    if (tapes) dr = Draws{tapes + pid * tape_len, 0, tape_len};
+    pathRad[pid] = path(c, vw, vi, (uint32_t)(local / vw.spp), (uint32_t)(local % vw.spp), nullptr, st[tid].data(), &ro,
+                        dr);
   });
   for (uint32_t vi = 0; vi < nviews; ++vi) {
     const View &vw = vs[vi];
@@ -1120,4 +1255,151 @@ extern "C" int oracle_render_restir(const float *bvh, const float *tlas, uint32_
       for (int k = 0; k < 4; ++k) stats[k] += x[k];
   }
   return 0;
+}
+
+}  // namespace
+
+extern "C" int oracle_render_restir(const float *bvh, const float *tlas, uint32_t tlas_count, const float *prims,
+                                    const float *materials, const int32_t *prim_indices, const uint8_t *active,
+                                    const int32_t *blas_root, const int32_t *prim_object, uint32_t object_count,
+                                    uint32_t prim_count, const void *views, uint32_t nviews, const uint32_t *cfg_u,
+                                    const float *cfg_f, const float *prev_resv, const float *prev_surf,
+                                    const void *prev_views, int have_prev, float *out_resv, float *out_surf,
+                                    float *out_rgb, uint64_t *stats, uint32_t threads) {
+  return restir_impl(bvh, tlas, tlas_count, prims, materials, prim_indices, active, blas_root, prim_object,
+                     object_count, prim_count, views, nviews, cfg_u, cfg_f, prev_resv, prev_surf, prev_views,
+                     have_prev, out_resv, out_surf, out_rgb, stats, threads, nullptr, 0);
+}
+
+// oracle_render_restir in tape mode (reference mode only): `tapes` holds tape_len uniforms per
+// path, drawn in the reference's order, for comparison with the reference's own rayColor run on
+// the same numbers.
+extern "C" int oracle_render_restir_tape(const float *bvh, const float *tlas, uint32_t tlas_count,
+                                         const float *prims, const float *materials, const int32_t *prim_indices,
+                                         const uint8_t *active, const int32_t *blas_root,
+                                         const int32_t *prim_object, uint32_t object_count, uint32_t prim_count,
+                                         const void *views, uint32_t nviews, const uint32_t *cfg_u,
+                                         const float *cfg_f, const float *prev_resv, const float *prev_surf,
+                                         const void *prev_views, int have_prev, float *out_resv, float *out_surf,
+                                         float *out_rgb, uint64_t *stats, uint32_t threads, const float *tapes,
+                                         uint32_t tape_len) {
+  if (!tapes || tape_len == 0 || cfg_u[3] == 0) return 1;
+  return restir_impl(bvh, tlas, tlas_count, prims, materials, prim_indices, active, blas_root, prim_object,
+                     object_count, prim_count, views, nviews, cfg_u, cfg_f, prev_resv, prev_surf, prev_views,
+                     have_prev, out_resv, out_surf, out_rgb, stats, threads, tapes, tape_len);
+}
+
+// ---------------------------------------------------------------------------------------------
+// The functions above one at a time, for the pin against the reference's own functions
+// (oracle/ref/ref_shade.cpp exports the reference's counterparts with the same arguments).
+extern "C" {
+
+// Light tables of the scene (build_lights: indices, CDF, total) and the per-primitive pdf.
+// idx / cdf must hold prim_count entries; returns the light count.
+uint32_t oracle_light_tables(const float *prims, const float *materials, const uint8_t *active,
+                             const int32_t *blas_root, const int32_t *prim_object, uint32_t prim_count,
+                             uint32_t *idx, float *cdf, float *total, float *pdf_of_prim) {
+  LightsH L = build_lights(prims, materials, active, blas_root, prim_object, prim_count);
+  std::copy(L.idx.begin(), L.idx.end(), idx);
+  std::copy(L.cdf.begin(), L.cdf.end(), cdf);
+  *total = L.total;
+  std::vector<float> lk = light_pdf_lookup(L, prim_count);
+  std::copy(lk.begin(), lk.end(), pdf_of_prim);
+  return (uint32_t)L.idx.size();
+}
+
+// decode: per material 17 floats (decodeMaterial's numeric fields in ref_decode_material's order).
+void oracle_decode_material(const float *mats, uint32_t n, float lod, float *out) {
+  for (uint32_t i = 0; i < n; ++i) {
+    Mat m = decode(mats, (int32_t)i, lod);
+    const float vals[17] = {m.diffuse.x, m.diffuse.y, m.diffuse.z, m.opacity, m.specular.x, m.specular.y,
+                            m.specular.z, m.shininess, m.emission.x, m.emission.y, m.emission.z, m.power,
+                            m.transmission.x, m.transmission.y, m.transmission.z, m.ior, m.roughness};
+    std::memcpy(out + 17ull * i, vals, sizeof(vals));
+  }
+}
+
+void oracle_bsdf(const float *mats, const float *nvl, uint32_t n, float *out) {
+  for (uint32_t i = 0; i < n; ++i) {
+    Mat m = decode(mats, (int32_t)i, 1.0f);
+    const float *q = nvl + 9ull * i;
+    V f = bsdf(m, v(q[0], q[1], q[2]), v(q[3], q[4], q[5]), v(q[6], q[7], q[8]));
+    out[3 * i] = f.x, out[3 * i + 1] = f.y, out[3 * i + 2] = f.z;
+  }
+}
+
+void oracle_select_light(const float *xi, uint32_t n, const float *cdf, uint32_t count, float total, uint32_t *off,
+                         float *pdf) {
+  LightsH L;
+  L.idx.assign(count, 0);
+  L.cdf.assign(cdf, cdf + count);
+  L.total = total;
+  for (uint32_t i = 0; i < n; ++i) {
+    off[i] = select_light(xi[i], L);
+    pdf[i] = light_pdf(L, off[i]);
+  }
+}
+
+void oracle_light_point(const float *prims, const float *uv, uint32_t n, float *out, uint8_t *ok) {
+  for (uint32_t i = 0; i < n; ++i) {
+    Draws dr{uv + 2ull * i, 0, 2};
+    V p = v(0, 0, 0), nn = v(0, 0, 0);
+    float area = 0.0f;
+    ok[i] = light_point(prims, i, dr, 0.0f, 0.0f, p, nn, area) ? 1 : 0;
+    const float vals[7] = {p.x, p.y, p.z, nn.x, nn.y, nn.z, area};
+    std::memcpy(out + 7ull * i, vals, sizeof(vals));
+  }
+}
+
+void oracle_scatter(const float *dn, const uint8_t *front, const float *mats, const float *tape4, uint32_t n,
+                    float *out_dir, float *out_w, uint32_t *draws) {
+  for (uint32_t i = 0; i < n; ++i) {
+    Mat m = decode(mats, (int32_t)i, 1.0f);
+    Draws dr{tape4 + 4ull * i, 0, 4};
+    const float *q = dn + 6ull * i;
+    V d = v(0, 0, 0);
+    V w = scatter(v(q[0], q[1], q[2]), v(q[3], q[4], q[5]), front[i] != 0, m, dr, 0.0f, 0.0f, 0.0f, 0.0f, d);
+    out_dir[3 * i] = d.x, out_dir[3 * i + 1] = d.y, out_dir[3 * i + 2] = d.z;
+    out_w[3 * i] = w.x, out_w[3 * i + 1] = w.y, out_w[3 * i + 2] = w.z;
+    draws[i] = dr.pos;
+  }
+}
+
+// ref_update chains on ref_reservoir_chain's inputs; per chain 18 floats in its order, except
+// that slot 7 holds the stored 1 / area and slot 3 the light id.
+void oracle_reservoir_chain(const float *cand, const float *xi, uint32_t chains, uint32_t k, float *out) {
+  for (uint32_t c = 0; c < chains; ++c) {
+    ResvH r = resv_empty();
+    V contrib = v(0, 0, 0);
+    Draws dr{xi + (uint64_t)c * k, 0, k};
+    for (uint32_t j = 0; j < k; ++j) {
+      const float *q = cand + 16ull * ((uint64_t)c * k + j);
+      RefC cd{v(q[0], q[1], q[2]), v(q[4], q[5], q[6]), v(0, 0, 0), scl(v(q[9], q[10], q[11]), q[12]),
+              1.0f / q[7], 0.0f, q[8], (int32_t)q[3]};
+      V cc = dvs(cd.radG, cd.pdf);
+      float target = mx(lum(cd.radG), 0.0f);
+      float w = (cd.pdf > 0.0f ? target / cd.pdf : 0.0f) * q[13];
+      ref_update(r, contrib, cd, cc, w, q[14], dr, 0.0f);
+    }
+    const bool valid = fbi(r.a[3]) >= 0;
+    const float vals[18] = {r.a[0], r.a[1], r.a[2], valid ? (float)fbi(r.a[3]) : 0.0f, r.b[0], r.b[1], r.b[2],
+                            r.b[3], r.c[0], r.c[1], r.c[2], r.c[3], contrib.x, contrib.y, contrib.z,
+                            valid ? 1.0f : 0.0f, (float)dr.pos, 0.0f};
+    std::memcpy(out + 18ull * c, vals, sizeof(vals));
+  }
+}
+
+}  // extern "C"
+
+// Reference rules of the oracle's shading (bits kRuleVisibility, kRuleReprojection; 0 = the
+// contract, the default); track != 0 also evaluates the other visibility rule on every light test
+// and counts disagreements. Returns the counts since the last call (tests, decisions on which the
+// two visibility rules differ) and resets them.
+extern "C" void oracle_set_reference_rules(int rule, int track, uint64_t *counts) {
+  g_vis_rule.store(rule);
+  g_vis_track.store(track);
+  if (counts) {
+    counts[0] = g_vis_tests.exchange(0);
+    counts[1] = g_vis_differ.exchange(0);
+  }
 }

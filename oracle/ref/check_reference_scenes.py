@@ -1,5 +1,6 @@
 """ORACLE recipe — test infrastructure only. Loads every scene XML shipped with the reference
-(under /root/reference/Nomad Path Tracer, where the reference tree is present) with both the
+(under $NOMAD_REFERENCE/Nomad Path Tracer, default /root/reference, where the reference tree is
+present) with both the
 reference's own loader (oracle/_ref/libref_ingest.so, built by `make -C oracle ref`) and
 nomad_scene_load_xml, and compares the results array by array, bit for bit. Prints one line per
 scene with the primitive and object counts, the two load times and the verdict.
@@ -19,7 +20,7 @@ sys.path.insert(0, ROOT)
 import nomad_b200 as nb  # noqa: E402
 from oracle import reference_ingest as ri  # noqa: E402
 
-REF_SCENES = "/root/reference/Nomad Path Tracer"
+REF_SCENES = os.path.join(os.environ.get("NOMAD_REFERENCE", "/root/reference"), "Nomad Path Tracer")
 ARRAYS = ("prim_type", "prim_geom", "prim_material", "object_first", "object_prims", "object_mesh_group")
 
 

@@ -23,10 +23,17 @@ struct float2 {
   float &operator[](int i) { return (&x)[i]; }
   float operator[](int i) const { return (&x)[i]; }
 };
+struct float3;
+// Plain triple used for the read-only .xyz swizzle of a float3 (a member cannot have its own type).
+struct float3_view {
+  float x, y, z;
+  operator float3() const;
+};
 struct float3 {
   union {
     struct { float x, y, z; };
     float2 xy;
+    float3_view xyz;
   };
   float3() = default;
   explicit float3(float s) : x(s), y(s), z(s) {}
@@ -34,6 +41,7 @@ struct float3 {
   float &operator[](int i) { return (&x)[i]; }
   float operator[](int i) const { return (&x)[i]; }
 };
+inline float3_view::operator float3() const { return float3(x, y, z); }
 // Plain pair used for the read-only .zw swizzle (anonymous members may not have constructors).
 struct float2_view {
   float x, y;
@@ -88,6 +96,7 @@ inline float2 operator/(float2 a, float s) { return float2(a.x / s, a.y / s); }
 inline bool2 operator>=(float2 a, float2 b) { return bool2{a.x >= b.x, a.y >= b.y}; }
 inline bool2 operator<=(float2 a, float2 b) { return bool2{a.x <= b.x, a.y <= b.y}; }
 inline int2 operator+(int2 a, int2 b) { return int2(a.x + b.x, a.y + b.y); }
+inline uint2 operator+(uint2 a, uint2 b) { return uint2(a.x + b.x, a.y + b.y); }
 
 inline float3 operator+(float3 a, float3 b) { return float3(a.x + b.x, a.y + b.y, a.z + b.z); }
 inline float3 operator-(float3 a, float3 b) { return float3(a.x - b.x, a.y - b.y, a.z - b.z); }
@@ -189,6 +198,11 @@ template <typename T, access::Mode M = access::sample> struct texture2d {
   }
   float4 sample(sampler, float2) const { return float4(1.0f); }
   float4 sample(sampler, float2, level) const { return float4(1.0f); }
+};
+template <typename T, unsigned N> struct array {
+  T items[N];
+  const T &operator[](unsigned i) const { return items[i]; }
+  T &operator[](unsigned i) { return items[i]; }
 };
 typedef std::atomic<uint32_t> atomic_uint;
 const std::memory_order memory_order_relaxed = std::memory_order_relaxed;

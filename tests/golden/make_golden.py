@@ -10,6 +10,12 @@ For two seeded scenes it stores
   * the reference traversal's closest hits (firstHitTLAS, verbatim) on a seeded ray set;
   * the contract oracle's closest hits on the same rays.
 Rays are regenerated from their seeds by tests/raysets.py, so only hits are stored.
+
+shading_ref.npz (needs oracle/_ref/libref_shade.so, from PathTraceKernel.metal, PathTracing.h and
+Scatter.h): the reference's shading functions on the seeded cases of tests/shading_pin.py (digests
+of the bit-exact ones, the first 2,000 cases of the others), its path-traced frames and its
+ReSTIR reference-mode sequence (radiance, selected light and sample count per pixel, a digest of
+the surface records), all on the seeded random-number tapes.
 """
 import hashlib
 import json
@@ -24,7 +30,8 @@ sys.path.insert(0, ROOT)
 
 import nomad_b200 as nb  # noqa: E402
 from oracle import oracle as orc, reference as ref  # noqa: E402
-from tests import raysets  # noqa: E402
+from oracle import reference_shade as rshade  # noqa: E402
+from tests import raysets, shading_pin as sp  # noqa: E402
 
 SCENES = {
     "ico": lambda: nb.synth_icospheres(seed=11, instances=64, extent=100.0),
@@ -57,6 +64,15 @@ def main():
                             contract=h_con.view(np.int32), ray_sha=np.array(sha(rays)))
     with open(os.path.join(HERE, "scenebvh_sha256.json"), "w") as f:
         json.dump(manifest, f, indent=1, sort_keys=True)
+    d = sp.function_inputs()
+    full = sp.reference_function_outputs(rshade, d)
+    a = np.array(full["resv"], np.float32)  # slot 7 as 1 / area where valid (the oracle's form)
+    valid = a[:, 15] > 0
+    a[:, 7] = np.where(valid, np.float32(1) / np.where(valid, a[:, 7], np.float32(1)), np.float32(0))
+    full["resv"] = a
+    g = sp.golden_function_outputs(full)
+    g.update(sp.golden_frames(sp.reference_frames(nb, orc, rshade)))
+    np.savez_compressed(os.path.join(HERE, sp.GOLDEN_FILE), **g)
 
 
 if __name__ == "__main__":
