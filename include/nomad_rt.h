@@ -463,10 +463,19 @@ nomad_status nomad_paging_states(nomad_ctx *ctx, uint8_t *out);
 nomad_status nomad_mlp_init(nomad_ctx *ctx, uint64_t seed);
 /* Trains on n samples (features n*NOMAD_FEATURES, targets n, host arrays): standardises the
  * features, then `steps` AdamW steps of mean-squared error on mini-batches of `batch` samples
- * drawn with a seeded permutation. loss_out[steps] (may be NULL) receives each step's loss. */
+ * drawn with a seeded permutation (beta 0.9 / 0.999, eps 1e-8, decoupled weight decay on the
+ * weights, not the biases). Each call starts a fresh optimiser state (zero moments) from the
+ * current weights. loss_out[steps] (may be NULL) receives each step's loss. */
 nomad_status nomad_mlp_train(nomad_ctx *ctx, const float *features, const float *targets, uint64_t n,
                              uint32_t steps, uint32_t batch, float lr, float weight_decay, uint64_t seed,
                              float *loss_out);
+/* The mean-squared-error gradient of the current model over n samples taken in order (host
+ * arrays; n a multiple of 64, at most 65,536), with the model's stored feature statistics, by
+ * the same forward and backward kernels as one training step: grad[NOMAD_MLP_PARAMS] in the
+ * blob's layout (0 for W1's padded columns and the statistics), *loss (may be NULL) the mean
+ * squared error. For gradient checks of the training kernels. */
+nomad_status nomad_mlp_gradient(nomad_ctx *ctx, const float *features, const float *targets, uint64_t n,
+                                float *grad, float *loss);
 /* Inference on n samples (host arrays unless NOMAD_TRACE_DEVICE_POINTERS). */
 nomad_status nomad_mlp_infer(nomad_ctx *ctx, const float *features, uint64_t n, float *out, uint32_t flags);
 /* Model blob (NOMAD_MLP_PARAMS floats): W1[128][32] (inputs padded to 32), b1, W2[128][128],

@@ -808,6 +808,95 @@ extern "C" nomad_status nomad_mlp_infer(nomad_ctx *ctx, const float *features, u
   return NOMAD_OK;
 }
 
+namespace {
+
+nomad_status ensure_batch(nomad_ctx *ctx, MlpState &S, int B, int splits) {
+  if (S.batchCap < B) {
+    NOMAD_CUDA(ctx, S.idx.reserve((size_t)B * 4));
+    NOMAD_CUDA(ctx, S.xb.reserve((size_t)B * kIn * 4));
+    NOMAD_CUDA(ctx, S.tb.reserve((size_t)B * 4));
+    NOMAD_CUDA(ctx, S.y.reserve((size_t)B * 4));
+    NOMAD_CUDA(ctx, S.z1.reserve((size_t)B * kHid * 4));
+    NOMAD_CUDA(ctx, S.h1.reserve((size_t)B * kHid * 2));
+    NOMAD_CUDA(ctx, S.z2.reserve((size_t)B * kHid * 4));
+    NOMAD_CUDA(ctx, S.xbf.reserve((size_t)B * kInPad * 2));
+    NOMAD_CUDA(ctx, S.dy.reserve((size_t)B * 4));
+    NOMAD_CUDA(ctx, S.se.reserve((size_t)B * 4));
+    NOMAD_CUDA(ctx, S.dz2b.reserve((size_t)B * kHid * 2));
+    NOMAD_CUDA(ctx, S.dz2f.reserve((size_t)B * kHid * 4));
+    NOMAD_CUDA(ctx, S.dh1.reserve((size_t)B * kHid * 4));
+    NOMAD_CUDA(ctx, S.dz1b.reserve((size_t)B * kHid * 2));
+    NOMAD_CUDA(ctx, S.dz1f.reserve((size_t)B * kHid * 4));
+    S.batchCap = B;
+  }
+  NOMAD_CUDA(ctx, S.part.reserve((size_t)std::max(splits, 1) * kHid * kHid * 4));
+  return NOMAD_OK;
+}
+
+int batch_splits(int B) { return std::max(1, std::min(32, B / 256)); }
+
+// Forward and backward of the batch in S.xb / S.tb (B rows, B a multiple of 64): the gradient of
+// the mean squared error with respect to every trainable parameter into S.G (the blob's layout;
+// W1's padded input columns get 0), the per-row squared errors into S.se. Mixed precision as in
+// the forward pass: BF16 operands of every product (standardised inputs, weights, hidden
+// activations, the gradients that flow into a product), FP32 accumulation, FP32 biases and
+// output layer; split-K partial sums reduced in a fixed order.
+nomad_status batch_gradient(nomad_ctx *ctx, MlpState &S, int B) {
+  cudaStream_t s = ctx->stream;
+  const int splits = batch_splits(B);
+  float *Pm = S.P.as<float>(), *G = S.G.as<float>();
+  k_mlp_forward<<<B / kFwdRows, 128, kFwdSmem, s>>>(S.xb.as<const float>(), B, Pm, S.W1b.as<const __nv_bfloat16>(),
+                                                    S.W2b.as<const __nv_bfloat16>(), S.y.as<float>(), S.z1.as<float>(),
+                                                    S.h1.as<__nv_bfloat16>(), S.z2.as<float>(),
+                                                    S.xbf.as<__nv_bfloat16>());
+  k_mse_grad<<<(B + 255) / 256, 256, 0, s>>>(S.y.as<const float>(), S.tb.as<const float>(), B, S.dy.as<float>(),
+                                             S.se.as<float>());
+  k_dz2<<<(B * kHid + 255) / 256, 256, 0, s>>>(S.dy.as<const float>(), S.z2.as<const float>(), Pm, B,
+                                               S.dz2b.as<__nv_bfloat16>(), S.dz2f.as<float>());
+  // dw3[c] = sum_r relu(z2[r][c]) * dy[r]; db3 = sum_r dy[r]
+  {
+    // relu(z2) into dh1, which is free until dH1 below (z2 itself feeds dz2 above)
+    float *h2 = S.dh1.as<float>();
+    size_t cnt = (size_t)B * kHid;
+    k_dz1<<<(unsigned)((cnt + 255) / 256), 256, 0, s>>>(S.z2.as<const float>(), S.z2.as<const float>(), B,
+                                                       S.dz1b.as<__nv_bfloat16>(), h2);
+    k_colsum<<<1, kHid, 0, s>>>(h2, S.dy.as<const float>(), B, kHid, G + oW3);
+    k_colsum<<<1, 1, 0, s>>>(S.dy.as<const float>(), nullptr, B, 1, G + oB3);
+  }
+  k_colsum<<<1, kHid, 0, s>>>(S.dz2f.as<const float>(), nullptr, B, kHid, G + oB2);
+  // dW2[n][k] = sum_i dZ2[i][n] H1[i][k]: A = dZ2^T (stored [B][128]), B = H1 [B][128]
+  {
+    int kPer = ((B / splits) + 15) / 16 * 16;
+    int sp = (B + kPer - 1) / kPer;
+    dim3 grid(kHid / 64, kHid / 64, sp);
+    k_gemm_bf16<true, false><<<grid, 128, 0, s>>>(S.dz2b.as<const __nv_bfloat16>(), S.h1.as<const __nv_bfloat16>(),
+                                                  S.part.as<float>(), kHid, kHid, B, kHid, kHid, kPer);
+    k_reduce_splits<<<64, 256, 0, s>>>(S.part.as<const float>(), sp, (size_t)kHid * kHid, G + oW2);
+  }
+  // dH1[i][k] = sum_n dZ2[i][n] W2[n][k]: A = dZ2 [B][128], B = W2 [128(n)][128(k)] row-major = [K][N]
+  {
+    dim3 grid(kHid / 64, (B + 63) / 64, 1);
+    k_gemm_bf16<false, false><<<grid, 128, 0, s>>>(S.dz2b.as<const __nv_bfloat16>(), S.W2b.as<const __nv_bfloat16>(),
+                                                   S.dh1.as<float>(), B, kHid, kHid, kHid, kHid, kHid);
+  }
+  k_dz1<<<(B * kHid + 255) / 256, 256, 0, s>>>(S.dh1.as<const float>(), S.z1.as<const float>(), B,
+                                               S.dz1b.as<__nv_bfloat16>(), S.dz1f.as<float>());
+  k_colsum<<<1, kHid, 0, s>>>(S.dz1f.as<const float>(), nullptr, B, kHid, G + oB1);
+  // dW1[n][k] = sum_i dZ1[i][n] X[i][k]: A = dZ1^T, B = Xbf [B][32]
+  {
+    int kPer = ((B / splits) + 15) / 16 * 16;
+    int sp = (B + kPer - 1) / kPer;
+    dim3 grid(1, kHid / 64, sp);
+    k_gemm_bf16<true, false><<<grid, 128, 0, s>>>(S.dz1b.as<const __nv_bfloat16>(), S.xbf.as<const __nv_bfloat16>(),
+                                                  S.part.as<float>(), kHid, kInPad, B, kHid, kInPad, kPer);
+    k_reduce_splits<<<16, 256, 0, s>>>(S.part.as<const float>(), sp, (size_t)kHid * kInPad, G + oW1);
+  }
+  NOMAD_CUDA(ctx, cudaGetLastError());
+  return NOMAD_OK;
+}
+
+}  // namespace
+
 extern "C" nomad_status nomad_mlp_train(nomad_ctx *ctx, const float *features, const float *targets, uint64_t n,
                                         uint32_t steps, uint32_t batch, float lr, float wd, uint64_t seed,
                                         float *loss_out) {
@@ -837,6 +926,10 @@ extern "C" nomad_status nomad_mlp_train(nomad_ctx *ctx, const float *features, c
     stats[kIn + f] = (float)(1.0 / std::max(std::sqrt(var), 1e-6));
   }
   NOMAD_CUDA(ctx, cudaMemcpyAsync(S.P.as<float>() + oMean, stats, sizeof(stats), cudaMemcpyHostToDevice, s));
+  // Every call is a fresh AdamW run from the current weights: the moments start at zero, as the
+  // bias correction (from step 1) assumes.
+  NOMAD_CUDA(ctx, cudaMemsetAsync(S.M.p, 0, kParams * 4, s));
+  NOMAD_CUDA(ctx, cudaMemsetAsync(S.V.p, 0, kParams * 4, s));
   const int B = (int)batch;
   if (S.trainCap < n) {
     NOMAD_CUDA(ctx, S.X.reserve(n * kIn * 4));
@@ -845,26 +938,10 @@ extern "C" nomad_status nomad_mlp_train(nomad_ctx *ctx, const float *features, c
   }
   NOMAD_CUDA(ctx, cudaMemcpyAsync(S.X.p, features, n * kIn * 4, cudaMemcpyHostToDevice, s));
   NOMAD_CUDA(ctx, cudaMemcpyAsync(S.T.p, targets, n * 4, cudaMemcpyHostToDevice, s));
-  const int splits = std::max(1, std::min(32, B / 256));
-  if (S.batchCap < B) {
-    NOMAD_CUDA(ctx, S.idx.reserve((size_t)B * 4));
-    NOMAD_CUDA(ctx, S.xb.reserve((size_t)B * kIn * 4));
-    NOMAD_CUDA(ctx, S.tb.reserve((size_t)B * 4));
-    NOMAD_CUDA(ctx, S.y.reserve((size_t)B * 4));
-    NOMAD_CUDA(ctx, S.z1.reserve((size_t)B * kHid * 4));
-    NOMAD_CUDA(ctx, S.h1.reserve((size_t)B * kHid * 2));
-    NOMAD_CUDA(ctx, S.z2.reserve((size_t)B * kHid * 4));
-    NOMAD_CUDA(ctx, S.xbf.reserve((size_t)B * kInPad * 2));
-    NOMAD_CUDA(ctx, S.dy.reserve((size_t)B * 4));
-    NOMAD_CUDA(ctx, S.se.reserve((size_t)B * 4));
-    NOMAD_CUDA(ctx, S.dz2b.reserve((size_t)B * kHid * 2));
-    NOMAD_CUDA(ctx, S.dz2f.reserve((size_t)B * kHid * 4));
-    NOMAD_CUDA(ctx, S.dh1.reserve((size_t)B * kHid * 4));
-    NOMAD_CUDA(ctx, S.dz1b.reserve((size_t)B * kHid * 2));
-    NOMAD_CUDA(ctx, S.dz1f.reserve((size_t)B * kHid * 4));
-    S.batchCap = B;
+  {
+    nomad_status st = ensure_batch(ctx, S, B, batch_splits(B));
+    if (st != NOMAD_OK) return st;
   }
-  NOMAD_CUDA(ctx, S.part.reserve((size_t)std::max(splits, 1) * kHid * kHid * 4));
   std::mt19937_64 rng(seed ^ 0x5EEDull);
   std::vector<uint32_t> perm(n);
   std::iota(perm.begin(), perm.end(), 0u);
@@ -883,58 +960,12 @@ extern "C" nomad_status nomad_mlp_train(nomad_ctx *ctx, const float *features, c
     NOMAD_CUDA(ctx, cudaMemcpyAsync(S.idx.p, bidx.data(), (size_t)B * 4, cudaMemcpyHostToDevice, s));
     k_gather<<<(B * kIn + 255) / 256, 256, 0, s>>>(S.X.as<const float>(), S.T.as<const float>(),
                                                    S.idx.as<const uint32_t>(), B, S.xb.as<float>(), S.tb.as<float>());
-    k_mlp_forward<<<B / kFwdRows, 128, kFwdSmem, s>>>(S.xb.as<const float>(), B, Pm, S.W1b.as<const __nv_bfloat16>(),
-                                                      S.W2b.as<const __nv_bfloat16>(), S.y.as<float>(), S.z1.as<float>(),
-                                                      S.h1.as<__nv_bfloat16>(), S.z2.as<float>(),
-                                                      S.xbf.as<__nv_bfloat16>());
-    k_mse_grad<<<(B + 255) / 256, 256, 0, s>>>(S.y.as<const float>(), S.tb.as<const float>(), B, S.dy.as<float>(),
-                                               S.se.as<float>());
-    // H2 = relu(Z2) is needed for dw3: recompute on the fly in a column sum over z2 via a mask.
-    k_dz2<<<(B * kHid + 255) / 256, 256, 0, s>>>(S.dy.as<const float>(), S.z2.as<const float>(), Pm, B,
-                                                 S.dz2b.as<__nv_bfloat16>(), S.dz2f.as<float>());
-    // dw3[c] = sum_r relu(z2[r][c]) * dy[r]; db3 = sum_r dy[r]
-    {
-      // relu in place is not allowed (z2 feeds dz2 above, already consumed): use dh1 as scratch.
-      float *h2 = S.dh1.as<float>();
-      size_t cnt = (size_t)B * kHid;
-      // h2 = max(z2, 0)
-      k_dz1<<<(unsigned)((cnt + 255) / 256), 256, 0, s>>>(S.z2.as<const float>(), S.z2.as<const float>(), B,
-                                                         S.dz1b.as<__nv_bfloat16>(), h2);
-      k_colsum<<<1, kHid, 0, s>>>(h2, S.dy.as<const float>(), B, kHid, G + oW3);
-      k_colsum<<<1, 1, 0, s>>>(S.dy.as<const float>(), nullptr, B, 1, G + oB3);
-    }
-    k_colsum<<<1, kHid, 0, s>>>(S.dz2f.as<const float>(), nullptr, B, kHid, G + oB2);
-    // dW2[n][k] = sum_i dZ2[i][n] H1[i][k]: A = dZ2^T (stored [B][128]), B = H1 [B][128]
-    {
-      int kPer = ((B / splits) + 15) / 16 * 16;
-      int sp = (B + kPer - 1) / kPer;
-      dim3 grid(kHid / 64, kHid / 64, sp);
-      k_gemm_bf16<true, false><<<grid, 128, 0, s>>>(S.dz2b.as<const __nv_bfloat16>(), S.h1.as<const __nv_bfloat16>(),
-                                                    S.part.as<float>(), kHid, kHid, B, kHid, kHid, kPer);
-      k_reduce_splits<<<64, 256, 0, s>>>(S.part.as<const float>(), sp, (size_t)kHid * kHid, G + oW2);
-    }
-    // dH1[i][k] = sum_n dZ2[i][n] W2[n][k]: A = dZ2 [B][128], B = W2 [128(n)][128(k)] row-major = [K][N]
-    {
-      dim3 grid(kHid / 64, (B + 63) / 64, 1);
-      k_gemm_bf16<false, false><<<grid, 128, 0, s>>>(S.dz2b.as<const __nv_bfloat16>(), S.W2b.as<const __nv_bfloat16>(),
-                                                     S.dh1.as<float>(), B, kHid, kHid, kHid, kHid, kHid);
-    }
-    k_dz1<<<(B * kHid + 255) / 256, 256, 0, s>>>(S.dh1.as<const float>(), S.z1.as<const float>(), B,
-                                                 S.dz1b.as<__nv_bfloat16>(), S.dz1f.as<float>());
-    k_colsum<<<1, kHid, 0, s>>>(S.dz1f.as<const float>(), nullptr, B, kHid, G + oB1);
-    // dW1[n][k] = sum_i dZ1[i][n] X[i][k]: A = dZ1^T, B = Xbf [B][32]
-    {
-      int kPer = ((B / splits) + 15) / 16 * 16;
-      int sp = (B + kPer - 1) / kPer;
-      dim3 grid(1, kHid / 64, sp);
-      k_gemm_bf16<true, false><<<grid, 128, 0, s>>>(S.dz1b.as<const __nv_bfloat16>(), S.xbf.as<const __nv_bfloat16>(),
-                                                    S.part.as<float>(), kHid, kInPad, B, kHid, kInPad, kPer);
-      k_reduce_splits<<<16, 256, 0, s>>>(S.part.as<const float>(), sp, (size_t)kHid * kInPad, G + oW1);
-    }
+    nomad_status st = batch_gradient(ctx, S, B);
+    if (st != NOMAD_OK) return st;
     float bc1 = 1.0f - std::pow(b1, (float)(step + 1)), bc2 = 1.0f - std::pow(b2, (float)(step + 1));
     k_adamw<<<(oMean + 255) / 256, 256, 0, s>>>(Pm, G, S.M.as<float>(), S.V.as<float>(), oMean, lr, b1, b2, eps, wd,
                                                 bc1, bc2);
-    nomad_status st = refresh(ctx, S);
+    st = refresh(ctx, S);
     if (st != NOMAD_OK) return st;
     NOMAD_CUDA(ctx, cudaGetLastError());
     if (loss_out) {
@@ -946,5 +977,34 @@ extern "C" nomad_status nomad_mlp_train(nomad_ctx *ctx, const float *features, c
     }
   }
   NOMAD_CUDA(ctx, cudaStreamSynchronize(s));
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_mlp_gradient(nomad_ctx *ctx, const float *features, const float *targets, uint64_t n,
+                                           float *grad, float *loss) {
+  if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
+  if (!features || !targets || !grad || n == 0 || n % 64 != 0 || n > 65536)
+    return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "the gradient needs 64 to 65,536 samples, a multiple of 64");
+  NOMAD_DEVICE_SCOPE(ctx);
+  MlpState &S = mlp(ctx);
+  if (!S.ready) return nomad_fail(ctx, NOMAD_ERR_NOT_READY, "MLP not initialised or trained");
+  const int B = (int)n;
+  nomad_status st = ensure_batch(ctx, S, B, batch_splits(B));
+  if (st != NOMAD_OK) return st;
+  cudaStream_t s = ctx->stream;
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(S.xb.p, features, n * kIn * 4, cudaMemcpyHostToDevice, s));
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(S.tb.p, targets, n * 4, cudaMemcpyHostToDevice, s));
+  NOMAD_CUDA(ctx, cudaMemsetAsync(S.G.p, 0, kParams * 4, s));
+  st = batch_gradient(ctx, S, B);
+  if (st != NOMAD_OK) return st;
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(grad, S.G.p, kParams * 4, cudaMemcpyDeviceToHost, s));
+  std::vector<float> se(B);
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(se.data(), S.se.p, (size_t)B * 4, cudaMemcpyDeviceToHost, s));
+  NOMAD_CUDA(ctx, cudaStreamSynchronize(s));
+  if (loss) {
+    double acc = 0.0;
+    for (int i = 0; i < B; ++i) acc += se[i];
+    *loss = (float)(acc / B);
+  }
   return NOMAD_OK;
 }

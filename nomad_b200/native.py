@@ -189,6 +189,7 @@ SIGNATURES = {
     "nomad_residency_prim_state": (C.c_int32, [_P, _P, _P, _P, _P, _P]),
     "nomad_residency_object_state": (C.c_int32, [_P, _P, _P, _P]),
     "nomad_mlp_init": (C.c_int32, [_P, C.c_uint64]),
+    "nomad_mlp_gradient": (C.c_int32, [_P, _P, _P, C.c_uint64, _P, _P]),
     "nomad_mlp_train": (C.c_int32, [_P, _P, _P, C.c_uint64, C.c_uint32, C.c_uint32, C.c_float,
                                     C.c_float, C.c_uint64, _P]),
     "nomad_mlp_infer": (C.c_int32, [_P, _P, C.c_uint64, _P, C.c_uint32]),
@@ -825,6 +826,15 @@ class Context:
         self._ck(self.lib.nomad_mlp_train(self.h, _ptr(x), _ptr(t), t.shape[0], steps, batch, lr,
                                           weight_decay, seed, _ptr(loss)))
         return loss
+
+    def mlp_gradient(self, features, targets):
+        """(gradient blob, mean squared error) of the current model over the samples in order."""
+        x = np.ascontiguousarray(features, np.float32).reshape(-1, N_FEATURES)
+        t = np.ascontiguousarray(targets, np.float32).reshape(-1)
+        g = np.zeros(MLP_PARAMS, np.float32)
+        loss = np.zeros(1, np.float32)
+        self._ck(self.lib.nomad_mlp_gradient(self.h, _ptr(x), _ptr(t), t.shape[0], _ptr(g), _ptr(loss)))
+        return g, float(loss[0])
 
     def mlp_infer(self, features) -> np.ndarray:
         x = np.ascontiguousarray(features, np.float32)

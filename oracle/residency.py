@@ -103,6 +103,81 @@ def mlp_forward(blob, feats):
     return h2 @ w3 + b3
 
 
+def _blob_parts(blob):
+    nf = 24
+    o = {"w1": 0, "b1": 128 * 32}
+    o["w2"] = o["b1"] + 128
+    o["b2"] = o["w2"] + 128 * 128
+    o["w3"] = o["b2"] + 128
+    o["b3"] = o["w3"] + 128
+    o["mean"] = o["b3"] + 1
+    o["istd"] = o["mean"] + nf
+    return o
+
+
+def mlp_gradient(blob, feats, targets):
+    """Mean-squared-error gradient of the scorer over the samples, restated in float64 with the
+    device's BF16 roundings (nomad_mlp_gradient / one training step, mlp.cu): BF16 standardised
+    inputs, weights W1 and W2, hidden activations H1 and the gradients dZ2, dZ1 that enter a
+    product; FP32 biases and output layer. Returns (gradient blob, loss)."""
+    o = _blob_parts(blob)
+    nf = 24
+    B = feats.shape[0]
+    w1 = _bf16(blob[o["w1"]:o["b1"]].reshape(128, 32)[:, :nf]).astype(np.float64)
+    b1 = blob[o["b1"]:o["w2"]].astype(np.float64)
+    w2 = _bf16(blob[o["w2"]:o["b2"]].reshape(128, 128)).astype(np.float64)
+    b2 = blob[o["b2"]:o["w3"]].astype(np.float64)
+    w3 = blob[o["w3"]:o["b3"]].astype(np.float64)
+    b3 = float(blob[o["b3"]])
+    mean, istd = blob[o["mean"]:o["istd"]], blob[o["istd"]:o["istd"] + nf]
+    x = _bf16((feats.astype(np.float32) - mean) * istd).astype(np.float64)
+    z1 = x @ w1.T + b1
+    h1 = _bf16(np.maximum(z1, 0.0).astype(np.float32)).astype(np.float64)
+    z2 = h1 @ w2.T + b2
+    h2 = np.maximum(z2, 0.0)
+    y = h2 @ w3 + b3
+    d = y - targets.astype(np.float64)
+    dy = 2.0 * d / B
+    dz2 = np.where(z2 > 0, dy[:, None] * w3[None, :], 0.0)
+    dz2b = _bf16(dz2.astype(np.float32)).astype(np.float64)
+    dh1 = dz2b @ w2
+    dz1 = np.where(z1 > 0, dh1, 0.0)
+    dz1b = _bf16(dz1.astype(np.float32)).astype(np.float64)
+    g = np.zeros(blob.size, np.float64)
+    gw1 = np.zeros((128, 32))
+    gw1[:, :nf] = dz1b.T @ x
+    g[o["w1"]:o["b1"]] = gw1.reshape(-1)
+    g[o["b1"]:o["w2"]] = dz1.sum(0)
+    g[o["w2"]:o["b2"]] = (dz2b.T @ h1).reshape(-1)
+    g[o["b2"]:o["w3"]] = dz2.sum(0)
+    g[o["w3"]:o["b3"]] = (h2 * dy[:, None]).sum(0)
+    g[o["b3"]] = dy.sum()
+    return g, float((d * d).mean())
+
+
+def adamw_step(blob, grad, m, v, step, lr, wd, b1=0.9, b2=0.999, eps=1e-8):
+    """One AdamW step (k_adamw, mlp.cu) in float32 over the trainable part of the blob (everything
+    before the feature statistics): decoupled weight decay on W1, W2 and w3, not on the biases.
+    Returns (blob, m, v)."""
+    o = _blob_parts(blob)
+    f = np.float32
+    n = o["mean"]
+    p, g = blob[:n].astype(f).copy(), grad[:n].astype(f)
+    m, v = m[:n].astype(f), v[:n].astype(f)
+    mi = f(b1) * m + (f(1) - f(b1)) * g
+    vi = f(b2) * v + (f(1) - f(b2)) * g * g
+    bc1 = f(1) - np.power(f(b1), f(step))
+    bc2 = f(1) - np.power(f(b2), f(step))
+    mh, vh = mi / bc1, vi / bc2
+    i = np.arange(n)
+    weight = (i < o["b1"]) | ((i >= o["w2"]) & (i < o["b2"])) | ((i >= o["w3"]) & (i < o["b3"]))
+    p = np.where(weight, p - f(lr) * f(wd) * p, p)
+    p = p - f(lr) * mh / (np.sqrt(vh) + f(eps))
+    out = blob.astype(f).copy()
+    out[:n] = p
+    return out, mi, vi
+
+
 class RayHitPrimOracle:
     """updateRayHitBudget per primitive (RendererResidency.cpp:2755-2964) with the per-frame
     cooldown decrement (:205-207) and the score pass of processRayHitCounters, restated in numpy

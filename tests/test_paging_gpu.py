@@ -2,8 +2,9 @@
 streamed from pinned host memory into a device pool.
 
 Once every wanted object is Resident, traversal and rendering must equal the same scene uploaded
-whole with the same residency (bit for bit); objects that are wanted but not yet Resident are
-skipped; evicted pool space is reused; onloads are capped per update and denied past the pool.
+whole with the same residency (bit for bit), which in turn equals the oracle under that residency;
+objects that are wanted but not yet Resident are skipped; evicted pool space is reused; onloads
+are capped per update and denied past the pool.
 """
 import numpy as np
 import pytest
@@ -18,11 +19,17 @@ def _rays(sb, seed=5):
 
 
 def _masked(nb, sb, active_objs, rays, views=None, prim_off=()):
-    """Hits (and images) of the whole scene with only `active_objs` resident."""
+    """Hits (and images) of the whole scene with only `active_objs` resident, traced by the CUDA
+    path without paging and checked against the oracle under the same residency (instance
+    records with blasRoot = -1 for the evicted objects, activeMask 0 for the primitives off):
+    hits bit for bit, images within the path tracer's bar."""
+    from oracle import oracle as orc
+
+    active_objs = np.asarray(active_objs, bool)
     ctx = nb.Context()
     try:
         ctx.upload(sb)
-        for o in np.nonzero(~np.asarray(active_objs, bool))[0]:
+        for o in np.nonzero(~active_objs)[0]:
             ctx.set_object_active(int(o), False)
         for p in prim_off:
             ctx.set_primitive_active(int(p), False)
@@ -31,6 +38,19 @@ def _masked(nb, sb, active_objs, rays, views=None, prim_off=()):
         imgs = ctx.render(views) if views is not None else None
     finally:
         ctx.close()
+    active = np.ones(sb.prim_count, np.uint8)
+    active[np.asarray(prim_off, np.int64)] = 0
+    root = np.ascontiguousarray(sb.instances["blas_root_index"], np.int32).copy()
+    root[~active_objs] = -1
+    os_ = orc.OracleScene(sb, active=active, blas_root=root)
+    want = os_.closest(rays, orc.MODE_REFERENCE_ORDER)
+    assert np.array_equal(_bits(hits), _bits(want)), "CUDA path differs from the oracle under this residency"
+    if views is not None:
+        ref, _, _ = orc.render(os_, sb.materials, views)
+        got = np.concatenate([i.reshape(-1, 3) for i in imgs])
+        exact = (got == ref).all(1).mean()
+        err = (np.abs(got - ref).sum(1) / np.maximum(np.abs(ref).sum(1), 1e-6)).mean()
+        assert exact > 0.99 and err < 1e-4, (exact, err)
     return hits, imgs
 
 

@@ -287,3 +287,47 @@ def test_screen_space_policy(nb, ctx, small_city):
         assert np.array_equal(cd, orc.cooldown), frame
         total += toggled
     assert total > 0
+
+
+def test_mlp_gradient_and_adamw_match_restatement(nb, ctx, small_city):
+    """The training kernels against a float64 restatement with the device's BF16 roundings: the
+    gradient of every parameter group (W1, b1, W2, b2, w3, b3) from nomad_mlp_gradient, and the
+    parameters after one and after two AdamW steps of nomad_mlp_train on the whole batch."""
+    from oracle import residency as ores
+
+    ctx.upload(small_city[1])
+    B = 512
+    x = _features(B, 9)
+    t = np.log1p(np.abs(x[:, 0] * 2 + x[:, 5] - 0.5 * x[:, 11] ** 2)).astype(np.float32)
+    ctx.mlp_init(3)
+    ctx.mlp_train(x, t, steps=0, batch=B)  # stores the feature statistics only
+    blob0 = ctx.mlp_get()
+    g, loss = ctx.mlp_gradient(x, t)
+    r, rloss = ores.mlp_gradient(blob0, x, t)
+    assert abs(loss - rloss) <= 1e-4 * rloss
+    o = ores._blob_parts(blob0)
+    groups = [("w1", "b1"), ("b1", "w2"), ("w2", "b2"), ("b2", "w3"), ("w3", "b3")]
+    for a, b in groups + [("b3", None)]:
+        lo, hi = o[a], (o[b] if b else o[a] + 1)
+        ga, ra = g[lo:hi].astype(np.float64), r[lo:hi]
+        scale = np.abs(ra).max()
+        assert scale > 0 and np.abs(ga - ra).max() <= 2e-3 * scale, (a, np.abs(ga - ra).max(), scale)
+    assert (g[o["mean"]:] == 0).all() and (g[:o["b1"]].reshape(128, 32)[:, 24:] == 0).all()
+    # AdamW: one step, then two steps from the same start (each call starts fresh moments); the
+    # second step's gradient is restated at the device's parameters after the first
+    lr, wd = 2e-3, 1e-2
+    ctx.mlp_train(x, t, steps=1, batch=B, lr=lr, weight_decay=wd, seed=5)
+    blob1 = ctx.mlp_get()
+    z = np.zeros(blob0.size, np.float32)
+    want1, m1, v1 = ores.adamw_step(blob0, r, z, z, 1, lr, wd)
+    sig = np.abs(r[:o["mean"]]) > 1e-3 * np.abs(r[:o["mean"]]).max()  # sign(g) decides step 1
+    assert np.abs(blob1 - want1)[:o["mean"]][sig].max() <= 1e-6
+    assert np.array_equal(blob1[o["mean"]:], blob0[o["mean"]:])
+    ctx.mlp_set(blob0)
+    ctx.mlp_train(x, t, steps=2, batch=B, lr=lr, weight_decay=wd, seed=5)
+    blob2 = ctx.mlp_get()
+    r1, _ = ores.mlp_gradient(blob1, x, t)
+    want2, _, _ = ores.adamw_step(blob1, r1, m1, v1, 2, lr, wd)
+    big = np.abs(r1[:o["mean"]]) > 1e-2 * np.abs(r1[:o["mean"]]).max()
+    assert np.abs(blob2 - want2)[:o["mean"]][big].max() <= 1e-5
+    assert np.median(np.abs(blob2 - want2)[:o["mean"]]) <= 1e-6

@@ -4,8 +4,8 @@ It serves callers that cannot allocate GPU memory while tracing — a frame loop
 budget is fully committed to resident geometry, or one that cannot take the implicit device
 synchronisation of cudaMalloc/cudaFree mid-frame — by keeping its scratch in a static device
 array. Its results must equal the regular entry point's (nomad_trace_closest with per-object
-hit counting): hits bit for bit, counts exactly. Two calls in a row check that the shared
-scratch is cleared between calls. This file is collected last on purpose.
+hit counting) and the oracle's: hits bit for bit, counts exactly. Two calls in a row check that
+the shared scratch is cleared between calls. This file is collected last on purpose.
 """
 import ctypes
 
@@ -17,7 +17,7 @@ from tests import raysets
 pytestmark = pytest.mark.gpu
 
 
-def test_noalloc_matches_regular_entry_point(nb):
+def test_noalloc_matches_regular_entry_point(nb, orc):
     import torch
 
     scene = nb.synth_city(seed=5, grid=8, size_m=250.0, target_tris=120_000, median_tris=1000,
@@ -51,6 +51,13 @@ def test_noalloc_matches_regular_entry_point(nb):
             assert np.array_equal(d_counts.cpu().numpy().view(np.uint32), want_counts), \
                 f"call {call}: per-object hit counts differ"
             assert want_counts.sum() == (want["prim"] >= 0).sum()
+            # and both equal the oracle: its closest hits bit for bit, its per-object counts
+            ref = orc.OracleScene(sb).closest(rays, orc.MODE_REFERENCE_ORDER)
+            assert np.array_equal(got, np.ascontiguousarray(ref).view(np.int32).reshape(-1, 5)), \
+                f"call {call}: hits differ from the oracle"
+            ref_counts = np.bincount(ref["inst"][ref["prim"] >= 0], minlength=sb.object_count)
+            assert np.array_equal(d_counts.cpu().numpy().view(np.uint32), ref_counts.astype(np.uint32)), \
+                f"call {call}: per-object hit counts differ from the oracle's"
         assert ctx.status() == 0
     finally:
         ctx.close()
