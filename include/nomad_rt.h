@@ -305,7 +305,8 @@ enum {
   NOMAD_POLICY_LEARNED = 2,       /* BF16 MLP score over NOMAD_FEATURES per-object features    */
   NOMAD_POLICY_RAYHIT_PRIM = 3,   /* the reference's per-primitive ray-hit budget (see below)    */
   NOMAD_POLICY_DISTANCE_LOD = 4,  /* the reference's DistanceLOD heuristic (see below)           */
-  NOMAD_POLICY_SCREEN_SPACE = 5   /* the reference's ScreenSpaceFootprint heuristic (see below)  */
+  NOMAD_POLICY_SCREEN_SPACE = 5,  /* the reference's ScreenSpaceFootprint heuristic (see below)  */
+  NOMAD_POLICY_PROBABILISTIC = 6  /* the reference's Probabilistic heuristic (see below)         */
 };
 #define NOMAD_FEATURES 24
 
@@ -334,6 +335,35 @@ typedef struct nomad_residency_params {
    * screenFootprintTargetFraction 0.68, min_active screenFootprintMinActivePrimitives 16,
    * max_toggles screenFootprintMaxTogglesPerFrame 14, in primitives): */
   float min_pixel_coverage;
+  /* The per-object Beta hit-probability posterior that every device step updates
+   * (processRayHitCounters, Renderer.cpp:8004-8522): alpha, beta decay by probability_decay and
+   * gain the step's closest hits and misses (rays tested - hits); a step without tested rays cools
+   * the probability (optionally with a grace of probability_idle_frames steps at
+   * probability_idle_decay for visible or resident objects); the mass alpha + beta stays in
+   * [1e-3, probability_window] (0 = no upper clamp). "Rays tested" of an object: closest-hit ray
+   * segments [1e-4, t of the hit] that enter its TLAS leaf box (the reference counts leaf
+   * primitive tests, which depend on the traversal order), counted by render and trace calls with
+   * NOMAD_TRACE_COUNT_HITS once a step has asked for them (NOMAD_POLICY_PROBABILISTIC, or a
+   * ray-hit prior). Defaults: probabilityDecay 0.9, probabilityEvidenceWindow 64,
+   * probabilityIdleCooldownFrames 0, probabilityIdleDecay 0.9, probabilityThreshold 0.5. */
+  float probability_decay;
+  float probability_window;
+  uint32_t probability_idle_frames;
+  float probability_idle_decay;
+  float probability_threshold;
+  /* NOMAD_POLICY_RAYHIT_BUDGET: the reference's ray-hit prior (enableRayHitPrior,
+   * RendererResidency.cpp:2842-2861): every key times clamp(1 + (p - 0.5) * scale, 0.25, 1) with
+   * p the object's hit probability. The reference's default is rayHitPriorScale 0.5; 0 = off. */
+  float rayhit_prior_scale;
+  /* NOMAD_POLICY_PROBABILISTIC only (updateProbabilisticResidency, RendererResidency.cpp:3389-4090,
+   * one object at a time; target_fraction is probabilityTargetFraction 0.60, min_active
+   * probabilityMinActivePrimitives 16 and max_toggles probabilityMaxTogglesPerFrame 20, both in
+   * primitives; state_cooldown the object cooldown, stateCooldownFrames 5): */
+  float uncertainty_boost;           /* probabilityUncertaintyBoost 0.25                       */
+  float desired_hysteresis;          /* probabilityDesiredHysteresis 0.02                      */
+  float visible_floor;               /* probabilityVisibleFloor 0                              */
+  uint32_t recent_promotion_frames;  /* probabilityRecentPromotionFrames 4                     */
+  uint32_t demotion_dwell_frames;    /* probabilityVisibleDemotionDwellFrames 0                */
 } nomad_residency_params;
 
 /* One residency step, all on the device: consumes the per-object closest-hit counts gathered
@@ -349,6 +379,15 @@ typedef struct nomad_residency_params {
  * and index). */
 nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residency_params *params,
                                   const nomad_view *camera, uint32_t *toggled);
+/* The per-object hit-probability posterior after the last step (the reference's _objectHitAlpha,
+ * _objectHitBeta, _objectHitProbability, _objectHitVariance, _objectPosteriorMass,
+ * _objectExplorationScore, _objectIdleFrames, _objectHitLastFrame, _objectRaysTestedLastFrame):
+ * 9 words per object, 6 float32 then 3 uint32. */
+nomad_status nomad_residency_posterior(nomad_ctx *ctx, float *out);
+/* Switches the per-object "rays tested" counting of render and trace calls with
+ * NOMAD_TRACE_COUNT_HITS on or off (steps that need it switch it on themselves). tests (may be
+ * NULL) receives the counts gathered since the last step or read, which are then cleared. */
+nomad_status nomad_residency_count_tests(nomad_ctx *ctx, int32_t on, uint32_t *tests);
 /* NOMAD_POLICY_RAYHIT_PRIM restates updateRayHitBudget per primitive, as the reference runs it
  * (RendererResidency.cpp:2755-2964, with the per-frame cooldown decrement of :205-207): per-primitive
  * closest hits (counted by nomad_render_frame with NOMAD_TRACE_COUNT_HITS once the policy has run

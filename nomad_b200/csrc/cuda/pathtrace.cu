@@ -702,6 +702,11 @@ extern "C" nomad_status nomad_render_frame(nomad_ctx *ctx, const nomad_view *vie
       nomad_status rs = nomad_trace_variant(ctx, ctx->trav, false, F.qRays[cur].as<const float4>(), P, &C->qlen[cur],
                                             &C->cursor[0], F.hits.as<int32_t>(), nullptr, nullptr, s);
       if (rs != NOMAD_OK) return rs;
+      if (objHits && ctx->res.testsOn) {  // per-object "rays tested" for the hit posterior
+        rs = nomad_count_object_tests(ctx, F.qRays[cur].as<const float4>(), F.hits.as<const int32_t>(), P,
+                                      &C->qlen[cur]);
+        if (rs != NOMAD_OK) return rs;
+      }
       if (depth == 0 && plan.on) {
         rs = restir_launch(ctx, nviews, P, L, C, plan);
         if (rs != NOMAD_OK) return rs;
@@ -738,6 +743,9 @@ extern "C" nomad_status nomad_render_frame(nomad_ctx *ctx, const nomad_view *vie
     key_put(key, maxDepth);
     key_put(key, objHits);
     key_put(key, primHits);
+    key_put(key, ctx->res.testsOn);
+    key_put(key, ctx->res.tests.p);
+    key_put(key, ctx->res.tlas.p);
     key_put(key, dOut);
     key_put(key, ctx->trav);
     key_put(key, ctx->scene);

@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <numeric>
 #include <vector>
 
 #include "pt_lights.cuh"
@@ -38,6 +39,112 @@ __global__ void k_features(FeatArgs A, float *__restrict__ keys) {
   if (o >= A.n) return;
   float f[NOMAD_FEATURES];
   keys[o] = nomad_res::object_features(A, o, f);
+}
+
+// The per-object Beta hit-probability posterior of processRayHitCounters (Renderer.cpp:
+// 8420-8522, restated in the same float operation order), one thread per object, after the
+// feature pass of the same step (which stored the step's closest hits in the history and the
+// visibility flag). post holds kPostWords words per object: alpha, beta, probability (clamped),
+// variance, posterior mass, exploration score (f32), idle steps, hits, rays tested (u32).
+struct PostArgs {
+  uint32_t n, frame;
+  const uint32_t *hist;
+  uint32_t *tests;
+  const uint8_t *visible, *res;
+  float *post;
+  float decay, hitDecay, maxMass, idleDecay, threshold;
+  int clampMass;
+  uint32_t idleFrames;
+  float *keys;       // ray-hit keys to multiply by the prior weight, or null
+  float priorScale;
+};
+
+__device__ __forceinline__ float renormalize_posterior(float &alpha, float &beta, const PostArgs &A) {
+  constexpr float kMinMass = 1.0e-3f;
+  float sum = alpha + beta;
+  if (!(sum > 0.0f)) {
+    alpha = beta = kMinMass * 0.5f;
+    sum = kMinMass;
+  } else if (sum < kMinMass) {
+    const float scale = kMinMass / sum;
+    alpha *= scale;
+    beta *= scale;
+    sum = kMinMass;
+  }
+  if (A.clampMass && sum > A.maxMass) {
+    const float scale = A.maxMass / sum;
+    alpha *= scale;
+    beta *= scale;
+    sum = A.maxMass;
+  }
+  return sum;
+}
+
+__device__ __forceinline__ float clamp01(float v) { return v < 0.0f ? 0.0f : (1.0f < v ? 1.0f : v); }
+__device__ __forceinline__ float maxf_ref(float a, float b) { return a < b ? b : a; }  // std::max
+
+__global__ void k_posterior(PostArgs A) {
+  const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= A.n) return;
+  float *p = A.post + (size_t)o * kPostWords;
+  uint32_t *pu = reinterpret_cast<uint32_t *>(p);
+  const uint32_t h = A.hist[o * kHist + A.frame % kHist];
+  const uint32_t t = A.tests[o];
+  A.tests[o] = 0;
+  const float success = (float)h, rays = (float)t;
+  const bool visible = A.visible[o] != 0, active = A.res[o] != 0;
+  const float failure = maxf_ref(rays - success, 0.0f);
+  float alpha = p[0] * A.decay + success;
+  float beta = p[1] * A.decay + failure;
+  float sum = alpha + beta;
+  float prob = sum > 0.0f ? alpha / sum : 0.5f;
+  uint32_t idle = pu[6];
+  if (t == 0) {
+    const bool grace = A.idleFrames > 0 && (visible || active) && idle < A.idleFrames;
+    float cooling = A.decay;
+    bool apply = true;
+    if (grace) {
+      if (A.idleDecay >= 0.999f) apply = false;
+      else cooling = A.idleDecay;
+    }
+    if (apply) {
+      const float cp = clamp01(prob * cooling);
+      float cm = maxf_ref(sum, 1.0e-3f);
+      if (A.clampMass && cm > A.maxMass) cm = A.maxMass;
+      alpha = cp * cm;
+      beta = maxf_ref(cm - alpha, 0.0f);
+    }
+  }
+  sum = renormalize_posterior(alpha, beta, A);
+  prob = sum > 0.0f ? alpha / sum : 0.5f;
+  const float clamped = clamp01(prob);
+  float var = 0.0f;
+  if (sum > 1.0f) var = (alpha * beta) / ((sum * sum) * (sum + 1.0f));
+  float ex = p[5] * A.decay;
+  if (t > 0) {
+    idle = 0;
+    if (clamped < A.threshold) ex += rays;
+    else ex *= A.hitDecay;
+  } else {
+    if (idle < 0xffffffffu) ++idle;
+    ex *= A.hitDecay;
+    if (visible || active) ex = maxf_ref(ex, 1.0f);  // kIdleVisibleExploreSeed
+  }
+  p[0] = alpha;
+  p[1] = beta;
+  p[2] = clamped;
+  p[3] = maxf_ref(var, 0.0f);
+  p[4] = sum;
+  p[5] = ex;
+  pu[6] = idle;
+  pu[7] = h;
+  pu[8] = t;
+  // ray-hit prior (RendererResidency.cpp:2842-2861, rayHitPriorFavorHighProbability off)
+  if (A.keys && A.priorScale > 0.0f) {
+    float w = 1.0f + (clamped - 0.5f) * A.priorScale * 1.0f;
+    w = w < 0.25f ? 0.25f : (1.0f < w ? 1.0f : w);
+    A.keys[o] *= w;
+  }
 }
 
 __device__ __forceinline__ unsigned long long sort_key(float s, uint32_t idx) {
@@ -542,6 +649,27 @@ nomad_status nomad_residency_init(nomad_ctx *ctx) {
   NOMAD_CUDA(ctx, F.lightPdf.reserve((size_t)P * 4));
   NOMAD_CUDA(ctx, F.lightMeta.reserve(sizeof(LightMeta)));
   NOMAD_CUDA(ctx, cudaMemset(F.lightPdf.p, 0, (size_t)P * 4));
+  // hit-probability posterior: Beta(1, 1), probability 0.5, variance 1/12, mass 2
+  NOMAD_CUDA(ctx, R.tlas.reserve(std::max<size_t>(1, R.hostTlas.size()) * 4));
+  if (!R.hostTlas.empty())
+    NOMAD_CUDA(ctx, cudaMemcpy(R.tlas.p, R.hostTlas.data(), R.hostTlas.size() * 4, cudaMemcpyHostToDevice));
+  NOMAD_CUDA(ctx, R.tests.reserve((size_t)N * 4));
+  NOMAD_CUDA(ctx, cudaMemset(R.tests.p, 0, (size_t)N * 4));
+  NOMAD_CUDA(ctx, R.post.reserve((size_t)N * kPostWords * 4));
+  {
+    std::vector<float> post((size_t)N * kPostWords, 0.0f);
+    for (uint32_t o = 0; o < N; ++o) {
+      float *q = post.data() + (size_t)o * kPostWords;
+      q[0] = 1.0f;
+      q[1] = 1.0f;
+      q[2] = 0.5f;
+      q[3] = 1.0f / 12.0f;
+      q[4] = 2.0f;
+    }
+    NOMAD_CUDA(ctx, cudaMemcpy(R.post.p, post.data(), post.size() * 4, cudaMemcpyHostToDevice));
+  }
+  R.testsOn = false;
+  R.probOn = false;
   R.frame = 0;
   R.havePrevCam = false;
   R.ready = true;
@@ -1056,6 +1184,34 @@ nomad_status screen_space_step(nomad_ctx *ctx, const nomad_residency_params *prm
 
 }  // namespace
 
+extern "C" nomad_status nomad_residency_posterior(nomad_ctx *ctx, float *out) {
+  if (!ctx || !out) return NOMAD_ERR_INVALID_ARGUMENT;
+  if (!ctx->sceneReady || !ctx->res.ready) return nomad_fail(ctx, NOMAD_ERR_NOT_READY, "no scene uploaded");
+  NOMAD_DEVICE_SCOPE(ctx);
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(out, ctx->res.post.p, (size_t)ctx->objectCount * kPostWords * 4,
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+  NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_residency_count_tests(nomad_ctx *ctx, int32_t on, uint32_t *tests) {
+  if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
+  if (!ctx->sceneReady || !ctx->res.ready) return nomad_fail(ctx, NOMAD_ERR_NOT_READY, "no scene uploaded");
+  NOMAD_DEVICE_SCOPE(ctx);
+  auto &R = ctx->res;
+  if (tests) {
+    NOMAD_CUDA(ctx, cudaMemcpyAsync(tests, R.tests.p, (size_t)ctx->objectCount * 4, cudaMemcpyDeviceToHost,
+                                    ctx->stream));
+    NOMAD_CUDA(ctx, cudaMemsetAsync(R.tests.p, 0, (size_t)ctx->objectCount * 4, ctx->stream));
+    NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  if ((on != 0) != R.testsOn) {
+    R.testsOn = on != 0;
+    ctx->frame.clearGraphs();
+  }
+  return NOMAD_OK;
+}
+
 extern "C" nomad_status nomad_residency_fallback_steps(nomad_ctx *ctx, uint64_t *out) {
   if (!ctx || !out) return NOMAD_ERR_INVALID_ARGUMENT;
   *out = ctx->res.fallbackSteps;
@@ -1095,36 +1251,13 @@ extern "C" nomad_status nomad_residency_prim_state(nomad_ctx *ctx, uint32_t *hit
   return NOMAD_OK;
 }
 
-extern "C" nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residency_params *prm,
-                                             const nomad_view *camera, uint32_t *toggled) {
-  if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
-  if (!ctx->sceneReady || !ctx->res.ready) return nomad_fail(ctx, NOMAD_ERR_NOT_READY, "no scene uploaded");
-  if (!prm || !camera) return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "null parameters or camera");
-  if (prm->policy == NOMAD_POLICY_RAYHIT_PRIM) {
-    NOMAD_DEVICE_SCOPE(ctx);
-    return rayhit_prim_step(ctx, prm, *camera, toggled);
-  }
-  if (prm->policy == NOMAD_POLICY_DISTANCE_LOD) {
-    NOMAD_DEVICE_SCOPE(ctx);
-    return distance_lod_step(ctx, prm, *camera, toggled);
-  }
-  if (prm->policy == NOMAD_POLICY_SCREEN_SPACE) {
-    NOMAD_DEVICE_SCOPE(ctx);
-    return screen_space_step(ctx, prm, *camera, toggled);
-  }
-  if (prm->policy > NOMAD_POLICY_LEARNED) return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "unknown policy");
-  // Without a usable model the learned policy runs the ray-hit budget step instead.
-  nomad_residency_params fallback;
-  if (prm->policy == NOMAD_POLICY_LEARNED && !nomad_mlp_ready(ctx)) {
-    fallback = *prm;
-    fallback.policy = NOMAD_POLICY_RAYHIT_BUDGET;
-    prm = &fallback;
-    ++ctx->res.fallbackSteps;
-  }
+namespace {
+
+// The per-object pass of a residency step on the context's stream: camera frame, features and
+// keys (the learned scorer's or the ray-hit key), then the hit-probability posterior and the
+// ray-hit prior. Counting of rays tested starts with the first step that asks for it.
+nomad_status object_pass(nomad_ctx *ctx, const nomad_residency_params *prm, const nomad_view *camera) {
   const uint32_t N = ctx->objectCount;
-  if (N > kMaxSelectObjects)
-    return nomad_fail(ctx, NOMAD_ERR_LIMIT, "device residency selection supports at most 16384 objects");
-  NOMAD_DEVICE_SCOPE(ctx);
   auto &R = ctx->res;
   cudaStream_t s = ctx->stream;
   // camera frame from the view (populateViewportUniforms: first_pixel = pos - w - U/2 - V/2)
@@ -1165,6 +1298,411 @@ extern "C" nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residen
   } else {
     k_features<<<(N + 127) / 128, 128, 0, s>>>(fa, R.keys.as<float>());
     NOMAD_CUDA(ctx, cudaGetLastError());
+  }
+  // the hit-probability posterior, and the ray-hit prior on the keys
+  const float window = prm->probability_window;
+  PostArgs pa{N, R.frame, R.hist.as<const uint32_t>(), R.tests.as<uint32_t>(), R.visible.as<const uint8_t>(),
+              R.objRes.as<const uint8_t>(), R.post.as<float>(), prm->probability_decay, prm->hit_decay,
+              std::max(window, 1.0e-3f), (window > 0.0f && std::isfinite(window)) ? 1 : 0,
+              prm->probability_idle_decay, prm->probability_threshold, prm->probability_idle_frames,
+              prm->policy == NOMAD_POLICY_RAYHIT_BUDGET ? R.keys.as<float>() : nullptr, prm->rayhit_prior_scale};
+  k_posterior<<<(N + 127) / 128, 128, 0, s>>>(pa);
+  NOMAD_CUDA(ctx, cudaGetLastError());
+  return NOMAD_OK;
+}
+
+// updateProbabilisticResidency (RendererResidency.cpp:2966-4090), its object-level path
+// (:3389-4090), over the device posterior of the same step. One object at a time: every
+// primitive of an object toggles with it, so the primitive cooldowns the reference checks equal
+// the object's, and the primitive counts are the objects' (contribution = max(count, 1)).
+// Visibility is the device frustum test of the per-object pass; the reference's "became
+// visible" test compares isInView with the flag processRayHitCounters set from the same camera
+// earlier in the frame, so it never fires and is left out. setObjectActive's side effects on the
+// policy (desired state, promotion / demotion frame, pending flag, cooldown; :965-1031) are
+// applied where it toggles.
+nomad_status probabilistic_step(nomad_ctx *ctx, const nomad_residency_params *prm, const nomad_view &view,
+                                uint32_t *toggled) {
+  auto &R = ctx->res;
+  const uint32_t N = ctx->objectCount;
+  if (!toggled) return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "the Probabilistic policy runs synchronously");
+  if (N > kMaxSelectObjects)
+    return nomad_fail(ctx, NOMAD_ERR_LIMIT, "the residency policies support at most 16384 objects");
+  nomad_status hs = nomad_residency_sync_host(ctx);
+  if (hs != NOMAD_OK) return hs;
+  if (!R.testsOn) {
+    R.testsOn = true;
+    ctx->frame.clearGraphs();  // the frame now also counts rays tested per object
+  }
+  if (!R.probOn) {
+    R.probDesired.assign(N, 0);
+    R.probPending.assign(N, 0);
+    R.probPromoted.assign(N, 0);
+    R.probDemoted.assign(N, 0);
+    R.probDwell.assign(N, 0);
+    R.probEvidence.assign(N, 0.0f);
+    R.probOrder.resize(N);
+    std::iota(R.probOrder.begin(), R.probOrder.end(), 0u);
+    R.objCooldown.assign(N, 0);
+    R.probOn = true;
+  }
+  for (uint32_t &c : R.objCooldown)
+    if (c > 0) --c;
+  cudaStream_t s = ctx->stream;
+  nomad_status st = object_pass(ctx, prm, &view);
+  if (st != NOMAD_OK) return st;
+  const uint32_t frameNo = R.frame + 1;  // _renderedFrameCount: 0 means "never"
+  ++R.frame;
+  std::vector<float> post((size_t)N * kPostWords);
+  std::vector<uint8_t> vis(N);
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(post.data(), R.post.p, post.size() * 4, cudaMemcpyDeviceToHost, s));
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(vis.data(), R.visible.p, N, cudaMemcpyDeviceToHost, s));
+  NOMAD_CUDA(ctx, cudaStreamSynchronize(s));
+  auto P = [&](uint32_t o, int k) -> float & { return post[(size_t)o * kPostWords + k]; };
+  auto testsLast = [&](uint32_t o) {
+    uint32_t v;
+    std::memcpy(&v, &post[(size_t)o * kPostWords + 8], 4);
+    return v;
+  };
+  const size_t primCount = ctx->primCount;
+  auto primitives = [&](uint32_t o) { return (size_t)std::max<uint32_t>(ctx->instances[o].primitive_count, 1u); };
+  auto active = [&](uint32_t o) { return ctx->objActiveCount[o] > 0; };
+
+  const float motion = clamp_unit(prm->camera_motion), pressure = clamp_unit(prm->memory_pressure);
+  const float targetFraction =
+      std::min(std::max(prm->target_fraction + 0.08f * motion - 0.12f * pressure, 0.45f), 0.93f);
+  const size_t baseBudget = std::max<size_t>(prm->max_toggles, 1);
+  const size_t toggleBudget = std::max<size_t>(
+      1, (size_t)std::llround((double)baseBudget * (1.0 + 0.40 * (double)motion + 0.50 * (double)pressure)));
+  constexpr float kPosteriorFloor = 1.0e-3f, kMinimalEvidence = 1.0e-3f, kEvidenceDecay = 0.9f, kSeed = 1.0f;
+  const float window = prm->probability_window;
+  const bool finiteWindow = window > 0.0f && std::isfinite(window);
+  const float floorVisible = std::min(std::max(prm->visible_floor, 0.0f), 1.0f);
+  const float scoringWindow = finiteWindow ? std::max(window, kPosteriorFloor) : std::max(64.0f, kPosteriorFloor);
+  auto cl = [](float v) { return std::min(std::max(v, 0.0f), 1.0f); };
+  auto evidence = [&](float mass, bool visible) {
+    if (!(mass > 0.0f) || !std::isfinite(mass) || !visible) return 0.0f;
+    return finiteWindow ? cl(mass / scoringWindow) : cl(mass / (mass + scoringWindow));
+  };
+  auto saneP = [&](float p) { return std::isfinite(p) ? cl(p) : 0.5f; };
+  auto saneVar = [](float v) { return (!std::isfinite(v) || v < 0.0f) ? 0.0f : v; };
+  auto regressedE = [&](float p, float e) {
+    const float ce = cl(e);
+    return saneP(p) * ce + 0.5f * (1.0f - ce);
+  };
+  auto scoreE = [&](float p, float var, float e) {
+    return regressedE(p, e) + prm->uncertainty_boost * std::sqrt(std::max(saneVar(var), 0.0f));
+  };
+  auto score = [&](uint32_t o) { return scoreE(P(o, 2), P(o, 3), evidence(P(o, 4), vis[o] != 0)); };
+
+  std::vector<uint8_t> desired = R.probDesired;
+  auto &pending = R.probPending;
+  const float threshold = prm->probability_threshold;
+  const float hyst = std::min(std::max(prm->desired_hysteresis, 0.0f), 0.5f);
+  const float enterT = cl(threshold + hyst), exitT = cl(threshold - hyst);
+  const uint32_t dwellFrames = prm->demotion_dwell_frames;
+  size_t desiredCount = 0;
+  for (uint32_t i = 0; i < N; ++i) {
+    const float prob = P(i, 2), var = P(i, 3), mass = P(i, 4);
+    const bool visible = vis[i] != 0;
+    const float rawE = evidence(mass, visible);
+    const float buffered = std::max(cl(rawE), R.probEvidence[i] * kEvidenceDecay);
+    R.probEvidence[i] = buffered;
+    const float eff = regressedE(saneP(prob), buffered);
+    const float boosted = scoreE(prob, var, buffered);
+    const float enterScore = std::max(eff, boosted), exitScore = eff;
+    const bool prev = desired[i] != 0;
+    bool want = prev;
+    const bool cooldownExpired = R.objCooldown[i] == 0;
+    const bool lowEvidence = std::min(buffered, cl(rawE)) <= kMinimalEvidence;
+    float promotion = enterScore, demotion = exitScore, evaluation = lowEvidence ? eff : enterScore;
+    const bool dwellApplies = visible && dwellFrames > 0;
+    if (!dwellApplies || demotion > exitT) R.probDwell[i] = 0;
+    if (visible) {
+      demotion = std::max(demotion, floorVisible);
+      evaluation = std::max(evaluation, floorVisible);
+    }
+    if (promotion >= enterT) {
+      want = true;
+      R.probDwell[i] = 0;
+    } else if (demotion <= exitT) {
+      if (dwellApplies && prev) {
+        if (R.probDwell[i] < dwellFrames) ++R.probDwell[i];
+        want = R.probDwell[i] < dwellFrames;
+      } else {
+        want = false;
+        R.probDwell[i] = 0;
+      }
+    } else if (cooldownExpired && !prev) {
+      want = evaluation >= threshold;
+      if (want) R.probDwell[i] = 0;
+    }
+    if (want && !prev) R.probPromoted[i] = frameNo;
+    else if (!want && prev) R.probDemoted[i] = frameNo;
+    desired[i] = want ? 1 : 0;
+    if (!want) pending[i] = 0;
+    if (want && !pending[i]) desiredCount += primitives(i);
+  }
+  const size_t minActive = std::min<size_t>(prm->min_active, primCount);
+  auto &order = R.probOrder;
+  std::vector<float> keys(N);
+  for (uint32_t o = 0; o < N; ++o) keys[o] = sanitize(score(o));
+  std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+    if (keys[a] == keys[b]) return a < b;
+    return keys[a] > keys[b];
+  });
+  size_t target = (size_t)std::ceil((float)primCount * targetFraction);
+  target = std::max(target, minActive);
+  if (target == 0 && primCount > 0) target = 1;
+  target = std::min(target, primCount);
+  auto trim = [&]() {
+    if (target == 0 || desiredCount <= target) return;
+    for (size_t pos = order.size(); pos-- > 0;) {
+      if (desiredCount <= target) break;
+      const uint32_t idx = order[pos];
+      if (!desired[idx] || pending[idx]) continue;
+      const size_t c = primitives(idx);
+      desired[idx] = 0;
+      pending[idx] = 0;
+      R.probDemoted[idx] = frameNo;
+      desiredCount = desiredCount > c ? desiredCount - c : 0;
+    }
+  };
+  trim();
+  std::vector<uint32_t> visibleExplore, hiddenExplore;
+  for (uint32_t idx : order) {
+    if (active(idx) || desired[idx]) continue;
+    const float prob = P(idx, 2), mass = P(idx, 4);
+    const bool visible = vis[idx] != 0;
+    const float rawE = evidence(mass, visible);
+    const float buffered = R.probEvidence[idx];
+    const float eff = regressedE(prob, buffered);
+    const bool lowEvidence = std::min(buffered, cl(rawE)) <= kMinimalEvidence;
+    const float gated = (visible && lowEvidence) ? std::min(eff, threshold) : eff;
+    if (gated > threshold) continue;
+    const uint32_t rays = testsLast(idx);
+    float ex = P(idx, 5);
+    if (visible && (rays == 0 || lowEvidence)) ex = std::max(ex, kSeed);
+    if (visible && rays > 0 && !lowEvidence) ex = std::max(ex, kPosteriorFloor);
+    P(idx, 5) = ex;
+    if (ex <= 0.0f) continue;
+    (visible ? visibleExplore : hiddenExplore).push_back(idx);
+  }
+  auto exploreFirst = [&](uint32_t a, uint32_t b) {
+    const float ea = sanitize(P(a, 5)), eb = sanitize(P(b, 5));
+    if (ea == eb) {
+      const uint32_t ra = testsLast(a), rb = testsLast(b);
+      if (ra == rb) return a < b;
+      return ra > rb;
+    }
+    return ea > eb;
+  };
+  std::sort(visibleExplore.begin(), visibleExplore.end(), exploreFirst);
+  std::sort(hiddenExplore.begin(), hiddenExplore.end(), exploreFirst);
+  auto recent = [&](uint32_t idx) {
+    const uint32_t w = prm->recent_promotion_frames;
+    if (w == 0) return false;
+    const uint32_t last = std::max(R.probPromoted[idx], R.probDemoted[idx]);
+    if (last == 0) return false;
+    if (frameNo <= last) return true;
+    return frameNo - last < w;
+  };
+  auto markDesired = [&](uint32_t idx) {
+    desired[idx] = 1;
+    R.probPromoted[idx] = frameNo;
+    const size_t c = primitives(idx);
+    if (!pending[idx]) desiredCount += c;
+    if (vis[idx] && testsLast(idx) == 0 && P(idx, 5) < kSeed) P(idx, 5) = kSeed;
+    return c;
+  };
+  auto promote = [&](const std::vector<uint32_t> &cands, size_t &slots, bool allowSuppressed) {
+    if (slots == 0) return;
+    for (uint32_t idx : cands) {
+      if (slots == 0) break;
+      if (desired[idx]) continue;
+      if (!allowSuppressed && recent(idx)) continue;
+      const size_t c = markDesired(idx);
+      slots = slots <= c ? 0 : slots - c;
+    }
+  };
+  auto remainingOf = [&](const std::vector<uint32_t> &cands) {
+    size_t r = 0;
+    for (uint32_t idx : cands)
+      if (!desired[idx] && !pending[idx]) r += primitives(idx);
+    return r;
+  };
+  if (desiredCount < minActive) {
+    size_t slots = std::min(minActive - desiredCount, primCount > desiredCount ? primCount - desiredCount : 0);
+    promote(visibleExplore, slots, false);
+    promote(hiddenExplore, slots, false);
+    if (slots > 0) {
+      promote(visibleExplore, slots, true);
+      promote(hiddenExplore, slots, true);
+    }
+  }
+  if (desiredCount < minActive) {
+    for (int allow = 0; allow < 2 && desiredCount < minActive; ++allow)
+      for (uint32_t idx : order) {
+        if (desiredCount >= minActive) break;
+        if (desired[idx]) continue;
+        if (!allow && recent(idx)) continue;
+        markDesired(idx);
+      }
+  }
+  const size_t remaining = remainingOf(visibleExplore) + remainingOf(hiddenExplore);
+  if (remaining > 0 && desiredCount < primCount) {
+    size_t slots = std::min({std::max<size_t>(1, minActive / 2), remaining, primCount - desiredCount});
+    promote(visibleExplore, slots, false);
+    promote(hiddenExplore, slots, false);
+    if (slots > 0) {
+      promote(visibleExplore, slots, true);
+      promote(hiddenExplore, slots, true);
+    }
+  }
+  desiredCount = 0;
+  for (uint32_t idx = 0; idx < N; ++idx)
+    if (desired[idx] && !pending[idx]) desiredCount += primitives(idx);
+  trim();
+  uint32_t fallback = N;
+  if (!visibleExplore.empty()) fallback = visibleExplore.front();
+  else if (!hiddenExplore.empty()) fallback = hiddenExplore.front();
+  else if (!order.empty()) fallback = order.front();
+
+  // setObjectActive with its side effects on the policy state
+  auto setObject = [&](uint32_t o, bool want, uint32_t &n) -> nomad_status {
+    const bool prevState = active(o);
+    nomad_status r = nomad_residency_set_object_active(ctx, o, want ? 1 : 0, &n);
+    if (r != NOMAD_OK) return r;
+    const bool newState = active(o), fullyInactive = !newState;
+    R.probDesired[o] = newState ? 1 : 0;
+    if (newState) R.probPromoted[o] = frameNo;
+    else R.probDemoted[o] = frameNo;
+    if (!newState || n > 0) pending[o] = 0;
+    if (n > 0 || prevState != newState || fullyInactive) R.objCooldown[o] = prm->state_cooldown;
+    return NOMAD_OK;
+  };
+  std::vector<uint32_t> toggleOrder;
+  std::vector<uint8_t> added(N, 0), appliedDesired(N, 0);
+  auto append = [&](const std::vector<uint32_t> &cands) {
+    for (uint32_t idx : cands)
+      if (!added[idx]) {
+        toggleOrder.push_back(idx);
+        added[idx] = 1;
+      }
+  };
+  std::vector<uint32_t> byPriority, pendingList;
+  for (uint32_t idx : order)
+    if (desired[idx]) byPriority.push_back(idx);
+  for (uint32_t idx = 0; idx < N; ++idx)
+    if (pending[idx]) pendingList.push_back(idx);
+  append(pendingList);
+  append(byPriority);
+  append(visibleExplore);
+  append(hiddenExplore);
+  append(order);
+  size_t toggledPrims = 0;
+  const size_t maxToggles = toggleBudget;
+  for (uint32_t idx : toggleOrder) {
+    if (maxToggles == 0 || toggledPrims >= maxToggles) break;
+    const bool want = desired[idx] != 0, current = active(idx);
+    if (want == current) continue;
+    if (R.objCooldown[idx] > 0) {
+      if (want) pending[idx] = 1;
+      continue;
+    }
+    const uint32_t count = ctx->instances[idx].primitive_count, activeCount = ctx->objActiveCount[idx];
+    const size_t pendingToggles = want ? count - activeCount : activeCount;
+    if (pendingToggles == 0) continue;
+    const size_t remainingBudget = maxToggles > toggledPrims ? maxToggles - toggledPrims : 0;
+    if (pendingToggles > remainingBudget) {
+      if (want) pending[idx] = 1;
+      continue;
+    }
+    uint32_t n = 0;
+    st = setObject(idx, want, n);
+    if (st != NOMAD_OK) return st;
+    if (n > 0) {
+      toggledPrims += std::min<size_t>(n, remainingBudget);
+      if (want && !appliedDesired[idx]) {
+        appliedDesired[idx] = 1;
+        pending[idx] = 0;
+        R.probDesired[idx] = 1;
+      }
+      if (!want) {
+        P(idx, 5) = 0.0f;
+        pending[idx] = 0;
+        R.probDesired[idx] = 0;
+      }
+    }
+  }
+  bool anyActive = false;
+  for (uint32_t o = 0; o < N && !anyActive; ++o) anyActive = active(o);
+  if (!anyActive && N > 0) {
+    const uint32_t fb = fallback < N ? fallback : 0u;
+    const size_t remainingBudget = maxToggles > toggledPrims ? maxToggles - toggledPrims : 0;
+    if (remainingBudget > 0) {
+      uint32_t n = 0;
+      st = setObject(fb, true, n);
+      if (st != NOMAD_OK) return st;
+      toggledPrims += std::min<size_t>(n, remainingBudget);
+    }
+    R.probDesired[fb] = 1;
+    R.probPromoted[fb] = frameNo;
+  }
+  // the exploration scores the policy updated go back to the device posterior (one strided copy)
+  NOMAD_CUDA(ctx, cudaMemcpy2DAsync(R.post.as<float>() + 5, kPostWords * 4, post.data() + 5, kPostWords * 4, 4, N,
+                                    cudaMemcpyHostToDevice, s));
+  NOMAD_CUDA(ctx, cudaStreamSynchronize(s));
+  st = nomad_residency_flush(ctx);
+  if (st != NOMAD_OK) return st;
+  *toggled = (uint32_t)toggledPrims;
+  return NOMAD_OK;
+}
+
+}  // namespace
+
+extern "C" nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residency_params *prm,
+                                             const nomad_view *camera, uint32_t *toggled) {
+  if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
+  if (!ctx->sceneReady || !ctx->res.ready) return nomad_fail(ctx, NOMAD_ERR_NOT_READY, "no scene uploaded");
+  if (!prm || !camera) return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "null parameters or camera");
+  if (prm->policy == NOMAD_POLICY_RAYHIT_PRIM) {
+    NOMAD_DEVICE_SCOPE(ctx);
+    return rayhit_prim_step(ctx, prm, *camera, toggled);
+  }
+  if (prm->policy == NOMAD_POLICY_DISTANCE_LOD) {
+    NOMAD_DEVICE_SCOPE(ctx);
+    return distance_lod_step(ctx, prm, *camera, toggled);
+  }
+  if (prm->policy == NOMAD_POLICY_SCREEN_SPACE) {
+    NOMAD_DEVICE_SCOPE(ctx);
+    return screen_space_step(ctx, prm, *camera, toggled);
+  }
+  if (prm->policy == NOMAD_POLICY_PROBABILISTIC) {
+    NOMAD_DEVICE_SCOPE(ctx);
+    return probabilistic_step(ctx, prm, *camera, toggled);
+  }
+  if (prm->policy > NOMAD_POLICY_LEARNED) return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "unknown policy");
+  // Without a usable model the learned policy runs the ray-hit budget step instead.
+  nomad_residency_params fallback;
+  if (prm->policy == NOMAD_POLICY_LEARNED && !nomad_mlp_ready(ctx)) {
+    fallback = *prm;
+    fallback.policy = NOMAD_POLICY_RAYHIT_BUDGET;
+    prm = &fallback;
+    ++ctx->res.fallbackSteps;
+  }
+  const uint32_t N = ctx->objectCount;
+  if (N > kMaxSelectObjects)
+    return nomad_fail(ctx, NOMAD_ERR_LIMIT, "device residency selection supports at most 16384 objects");
+  NOMAD_DEVICE_SCOPE(ctx);
+  auto &R = ctx->res;
+  cudaStream_t s = ctx->stream;
+  if (!R.testsOn && prm->policy == NOMAD_POLICY_RAYHIT_BUDGET && prm->rayhit_prior_scale > 0.0f) {
+    R.testsOn = true;
+    ctx->frame.clearGraphs();  // the frame now also counts rays tested per object
+  }
+  {
+    nomad_status ps = object_pass(ctx, prm, camera);
+    if (ps != NOMAD_OK) return ps;
   }
   uint32_t npow2 = 1;
   while (npow2 < N) npow2 <<= 1;

@@ -152,6 +152,22 @@ struct nomad_ctx {
     uint32_t primRebuild = 0;
     // learned-policy steps that ran the ray-hit budget for want of a usable model
     uint64_t fallbackSteps = 0;
+    // Per-object Beta hit-probability posterior (processRayHitCounters, Renderer.cpp:8004-8522),
+    // fed by per-object closest hits and "rays tested": the closest-hit ray segments that enter
+    // the object's TLAS leaf box before their hit (counted on the device once testsOn is set).
+    // post: per object alpha, beta, probability, variance, mass, exploration (f32) then idle
+    // frames, hits and tests of the last step (u32), 9 words.
+    DeviceBuf tlas;        // SceneBVH TLAS nodes (2 float4 each), as uploaded
+    uint32_t tlasCount = 0;
+    std::vector<float> hostTlas;
+    DeviceBuf tests, post;
+    bool testsOn = false;
+    // Probabilistic policy (NOMAD_POLICY_PROBABILISTIC), host state of updateProbabilisticResidency
+    bool probOn = false;
+    std::vector<uint8_t> probDesired, probPending;
+    std::vector<uint32_t> probPromoted, probDemoted, probDwell;
+    std::vector<float> probEvidence;
+    std::vector<uint32_t> probOrder;
     // DistanceLOD policy (NOMAD_POLICY_DISTANCE_LOD): object cooldowns and the last step's tests
     bool lodOn = false;
     std::vector<uint32_t> objCooldown;
@@ -176,6 +192,11 @@ struct nomad_ctx {
 
 // Applies a pending device residency step to the host mirror (waits for its flag copy).
 nomad_status nomad_residency_sync_host(nomad_ctx *ctx);
+// Per-object "rays tested" of n closest-hit rays (2 float4 each) and their hits (5 words each;
+// the count from lenDev when set), added to ctx->res.tests on the context's stream.
+nomad_status nomad_count_object_tests(nomad_ctx *ctx, const float4 *rays, const int32_t *hits5, uint64_t n,
+                                      const uint32_t *lenDev);
+constexpr int kPostWords = 9;
 
 void nomad_mlp_free(void *p);
 void nomad_paging_free(nomad_ctx *ctx);

@@ -109,6 +109,48 @@ __global__ void __launch_bounds__(kBlock) k_work(DevScene S, const float4 *__res
   out[i] = make_uint4(w.nodes, w.tests, w.insts, h.prim >= 0 ? 1u : 0u);
 }
 
+// "Rays tested" per object: the resident objects whose TLAS leaf box (SceneBVH TLAS array:
+// leaf left = -(object + 1)) the ray segment [1e-4, t of its closest hit] enters, infinite for a
+// miss. A node's box contains its children's, and the slab test is monotone under containment,
+// so walking the TLAS and pruning failed boxes finds exactly the leaves whose own box passes:
+// the count does not depend on any traversal order. One thread per ray; a warp's lanes that
+// count the same object add once.
+constexpr int kTlasStack = 64;
+
+__global__ void __launch_bounds__(kBlock) k_object_tests(const float4 *__restrict__ tlas, const float4 *__restrict__ rays,
+                                                         const int32_t *__restrict__ hits5, uint64_t n,
+                                                         const uint32_t *__restrict__ lenDev,
+                                                         const uint8_t *__restrict__ resident,
+                                                         uint32_t *__restrict__ tests, uint32_t *__restrict__ status) {
+  const uint64_t N = lenDev ? (uint64_t)*lenDev : n;
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const float4 a = __ldg(rays + 2 * i), b = __ldg(rays + 2 * i + 1);
+  const RayP r = prep_ray(a, b);
+  const float bound = __int_as_float(hits5[5 * i + 2]);
+  int32_t stack[kTlasStack];
+  int sp = 0;
+  stack[sp++] = 0;
+  while (sp > 0) {
+    const int32_t node = stack[--sp];
+    const float4 lo = __ldg(tlas + 2 * node), hi = __ldg(tlas + 2 * node + 1);
+    float tn;
+    if (!slab(r, lo.x, lo.y, lo.z, hi.x, hi.y, hi.z, bound, tn)) continue;
+    const int32_t left = __float_as_int(lo.w), right = __float_as_int(hi.w);
+    if (left < 0) {
+      const int32_t obj = -(left + 1);
+      if (resident[obj]) atomicAdd(tests + obj, 1u);
+      continue;
+    }
+    if (sp + 2 > kTlasStack) {
+      atomicOr(status, kStatusStackOverflow);
+      continue;
+    }
+    stack[sp++] = right;
+    stack[sp++] = left;
+  }
+}
+
 // Instance slots of the wide layouts from the device residency flags.
 __global__ void k_patch_wide(int32_t *__restrict__ arena, size_t base, uint32_t fpn, uint32_t width,
                              const long long *__restrict__ slot, const int32_t *__restrict__ ref,
@@ -313,6 +355,8 @@ extern "C" nomad_status nomad_scene_upload(nomad_ctx *ctx, const float *bvh, uin
   for (uint32_t o = 0; o < objectCount; ++o) ctx->objActiveCount[o] = inst[o].primitive_count;
   ctx->instances.assign(inst, inst + objectCount);
   ctx->hostPrims.assign(prims, prims + (size_t)primCount * 28);
+  ctx->res.hostTlas.assign(tlas, tlas + (size_t)tlasCount * 8);
+  ctx->res.tlasCount = tlasCount;
   ctx->hostMaterials.assign(materials, materials + (size_t)primCount * 20);
   ctx->frame.lightsDirty = true;
   ctx->frame.restirValid = false;
@@ -571,8 +615,11 @@ nomad_status launch(nomad_ctx *ctx, Op op, const float4 *rays, uint64_t n, void 
   if (op == Op::Any)
     return nomad_trace_variant(ctx, ctx->trav, true, rays, n, nullptr, cursor, nullptr, static_cast<uint8_t *>(out),
                                nullptr, st);
-  return nomad_trace_variant(ctx, ctx->trav, false, rays, n, nullptr, cursor, static_cast<int32_t *>(out), nullptr,
-                             counts, st);
+  nomad_status rs = nomad_trace_variant(ctx, ctx->trav, false, rays, n, nullptr, cursor,
+                                        static_cast<int32_t *>(out), nullptr, counts, st);
+  if (rs != NOMAD_OK || !countHits) return rs;
+  // st is the context's stream on every caller's path
+  return nomad_count_object_tests(ctx, rays, static_cast<const int32_t *>(out), n, nullptr);
 }
 
 // Host-pointer path: rays are copied in and results out in chunks, alternating two streams
@@ -806,6 +853,18 @@ extern "C" nomad_status nomad_trace_closest_noalloc(nomad_ctx *ctx, const nomad_
   NOMAD_CUDA(ctx, cudaMemcpyAsync(d_object_hits, scratch + kNoAllocCursorWords,
                                   (size_t)ctx->objectCount * 4, cudaMemcpyDeviceToDevice,
                                   ctx->stream));
+  return NOMAD_OK;
+}
+
+nomad_status nomad_count_object_tests(nomad_ctx *ctx, const float4 *rays, const int32_t *hits5, uint64_t n,
+                                      const uint32_t *lenDev) {
+  auto &R = ctx->res;
+  if (!R.testsOn || n == 0 || R.tlasCount == 0) return NOMAD_OK;
+  const uint64_t blocks = (n + kBlock - 1) / kBlock;
+  k_object_tests<<<(unsigned)blocks, kBlock, 0, ctx->stream>>>(R.tlas.as<const float4>(), rays, hits5, n, lenDev,
+                                                               R.objRes.as<const uint8_t>(), R.tests.as<uint32_t>(),
+                                                               ctx->status.as<uint32_t>());
+  NOMAD_CUDA(ctx, cudaGetLastError());
   return NOMAD_OK;
 }
 

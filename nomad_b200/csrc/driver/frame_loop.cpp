@@ -185,6 +185,11 @@ int main(int argc, char **argv) {
   prm.memory_pressure = 0.0f;
   prm.reserve_base = 0.02f;
   prm.reserve_motion = 0.06f;
+  // hit-probability posterior with the reference's defaults (ResidencyParameters, Scene.h:90-100)
+  prm.probability_decay = 0.9f;
+  prm.probability_window = 64.0f;
+  prm.probability_idle_decay = 0.9f;
+  prm.probability_threshold = 0.5f;
   if (prm.policy == NOMAD_POLICY_LEARNED) {
     if (a.mlp.empty()) {
       std::fprintf(stderr, "the learned policy needs --mlp WEIGHTS\n");

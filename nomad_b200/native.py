@@ -190,6 +190,8 @@ SIGNATURES = {
     "nomad_residency_object_state": (C.c_int32, [_P, _P, _P, _P]),
     "nomad_mlp_init": (C.c_int32, [_P, C.c_uint64]),
     "nomad_mlp_gradient": (C.c_int32, [_P, _P, _P, C.c_uint64, _P, _P]),
+    "nomad_residency_posterior": (C.c_int32, [_P, _P]),
+    "nomad_residency_count_tests": (C.c_int32, [_P, C.c_int32, _P]),
     "nomad_mlp_train": (C.c_int32, [_P, _P, _P, C.c_uint64, C.c_uint32, C.c_uint32, C.c_float,
                                     C.c_float, C.c_uint64, _P]),
     "nomad_mlp_infer": (C.c_int32, [_P, _P, C.c_uint64, _P, C.c_uint32]),
@@ -246,6 +248,7 @@ class RestirConfig(C.Structure):
 
 POLICY_ALWAYS, POLICY_RAYHIT_BUDGET, POLICY_LEARNED, POLICY_RAYHIT_PRIM, POLICY_DISTANCE_LOD = 0, 1, 2, 3, 4
 POLICY_SCREEN_SPACE = 5
+POLICY_PROBABILISTIC = 6
 N_FEATURES = 24
 MLP_PARAMS = 128 * 32 + 128 + 128 * 128 + 128 + 128 + 1 + 2 * N_FEATURES
 
@@ -258,18 +261,34 @@ class ResidencyParams(C.Structure):
                 ("rebuild_cooldown", C.c_uint32), ("state_cooldown", C.c_uint32),
                 ("lod_enter_distance", C.c_float), ("lod_exit_distance", C.c_float),
                 ("lod_enter_view_degrees", C.c_float), ("lod_exit_view_degrees", C.c_float),
-                ("min_pixel_coverage", C.c_float)]
+                ("min_pixel_coverage", C.c_float),
+                ("probability_decay", C.c_float), ("probability_window", C.c_float),
+                ("probability_idle_frames", C.c_uint32), ("probability_idle_decay", C.c_float),
+                ("probability_threshold", C.c_float), ("rayhit_prior_scale", C.c_float),
+                ("uncertainty_boost", C.c_float), ("desired_hysteresis", C.c_float),
+                ("visible_floor", C.c_float), ("recent_promotion_frames", C.c_uint32),
+                ("demotion_dwell_frames", C.c_uint32)]
 
     @staticmethod
     def make(policy, budget_bytes=0, max_toggles=0, hit_decay=0.85, camera_motion=0.0,
              memory_pressure=0.0, reserve_base=0.02, reserve_motion=0.06, min_active=0,
              target_fraction=0.54, rebuild_cooldown=4, state_cooldown=5, lod_enter_distance=225.0,
              lod_exit_distance=275.0, lod_enter_view_degrees=5.0, lod_exit_view_degrees=12.0,
-             min_pixel_coverage=32.0):
+             min_pixel_coverage=32.0, probability_decay=0.9, probability_window=64.0,
+             probability_idle_frames=0, probability_idle_decay=0.9, probability_threshold=0.5,
+             rayhit_prior_scale=0.0, uncertainty_boost=0.25, desired_hysteresis=0.02, visible_floor=0.0,
+             recent_promotion_frames=4, demotion_dwell_frames=0):
         return ResidencyParams(policy, max_toggles, budget_bytes, hit_decay, camera_motion,
                                memory_pressure, reserve_base, reserve_motion, min_active, target_fraction,
                                rebuild_cooldown, state_cooldown, lod_enter_distance, lod_exit_distance,
-                               lod_enter_view_degrees, lod_exit_view_degrees, min_pixel_coverage)
+                               lod_enter_view_degrees, lod_exit_view_degrees, min_pixel_coverage,
+                               probability_decay, probability_window, probability_idle_frames,
+                               probability_idle_decay, probability_threshold, rayhit_prior_scale,
+                               uncertainty_boost, desired_hysteresis, visible_floor, recent_promotion_frames,
+                               demotion_dwell_frames)
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
 
 VIEW_DTYPE = np.dtype([("camera_pos", "<f4", 3), ("viewport_u", "<f4", 3), ("viewport_v", "<f4", 3),
                        ("first_pixel", "<f4", 3), ("width", "<u4"), ("height", "<u4"), ("spp", "<u4"),
@@ -798,6 +817,22 @@ class Context:
         c = np.zeros(self.object_count, np.uint32)
         self._ck(self.lib.nomad_residency_object_state(self.h, _ptr(d), _ptr(f), _ptr(c)))
         return d, f, c
+
+    def residency_posterior(self) -> dict:
+        """The per-object hit-probability posterior after the last step."""
+        out = np.zeros((self.object_count, 9), np.float32)
+        self._ck(self.lib.nomad_residency_posterior(self.h, _ptr(out)))
+        u = out.view(np.uint32)
+        return {"alpha": out[:, 0].copy(), "beta": out[:, 1].copy(), "probability": out[:, 2].copy(),
+                "variance": out[:, 3].copy(), "mass": out[:, 4].copy(), "exploration": out[:, 5].copy(),
+                "idle": u[:, 6].copy(), "hits": u[:, 7].copy(), "tests": u[:, 8].copy()}
+
+    def count_object_tests(self, on: bool = True, read: bool = False):
+        """Switches per-object rays-tested counting on or off; with read, returns and clears the
+        counts gathered since the last step or read."""
+        out = np.zeros(self.object_count, np.uint32) if read else None
+        self._ck(self.lib.nomad_residency_count_tests(self.h, 1 if on else 0, _ptr(out) if read else None))
+        return out
 
     def residency_flags(self) -> np.ndarray:
         out = np.zeros(self.object_count, np.uint8)

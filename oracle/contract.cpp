@@ -24,6 +24,9 @@
 // summed as (x + y) + z, normalize(v) = v / sqrt(dot(v, v)).
 #include "contract_core.h"
 
+#include <utility>
+#include <vector>
+
 using namespace oracle_core;
 
 extern "C" {
@@ -69,6 +72,32 @@ int oracle_trace_work(const float *bvh, const float *tlas, uint32_t tlas_count, 
   Job j{{bvh, tlas, tlas_count, prims, prim_indices, active, blas_root, prim_object},
         rays, n, 1, false, object_count, hits_out, nullptr, work_out};
   run(j, threads);
+  return 0;
+}
+
+// Per-object "rays tested": for every ray, every resident object (blas_root >= 0) whose TLAS
+// leaf box the segment [1e-4, t_hit[i]] enters (t_hit infinite for a miss), by a test of every
+// leaf box (no walk, so no pruning: the device walks the TLAS and relies on a node's box
+// containing its children's). counts: object_count words, added to.
+int oracle_object_tests(const float *tlas, uint32_t tlas_count, const int32_t *blas_root, uint32_t object_count,
+                        const float *rays, const float *t_hit, uint64_t n, uint32_t *counts) {
+  if (!tlas || !blas_root || !rays || !t_hit || !counts) return 1;
+  std::vector<std::pair<uint32_t, int32_t>> leaves;  // node, object
+  for (uint32_t k = 0; k < tlas_count; ++k) {
+    const int32_t l = fbits(tlas[8ull * k + 3]);
+    if (l < 0) {
+      const int32_t obj = -(l + 1);
+      if ((uint32_t)obj < object_count && blas_root[obj] >= 0) leaves.push_back({k, obj});
+    }
+  }
+  for (uint64_t i = 0; i < n; ++i) {
+    const float *q = rays + 8 * i;
+    Ray r{mk(q[0], q[1], q[2]), mk(q[4], q[5], q[6]), t_hit[i]};
+    for (const auto &lf : leaves) {
+      const float *nd = tlas + 8ull * lf.first;
+      if (aabb(r, nd, nd + 4, RAY_EPS, t_hit[i], nullptr)) counts[lf.second]++;
+    }
+  }
   return 0;
 }
 

@@ -478,3 +478,408 @@ def coverage_f64(spheres, view):
     cov = np.where(ok, cov, 0.0)
     margin = np.minimum.reduce([vmargin, np.abs(depth - 1e-3), np.abs(h_half + 0.1 - ha)])
     return cov, margin
+
+
+# ------------------------------------------------------------------------------------------------
+# Per-object hit-probability posterior and the Probabilistic policy
+
+def object_tests(os_, rays, t_hit):
+    """Per-object "rays tested" (oracle_object_tests, contract.cpp): the resident objects whose
+    TLAS leaf box each ray's segment [1e-4, t_hit] enters."""
+    import ctypes as C
+    from . import oracle as orc
+
+    lib = orc.load()
+    fn = lib.oracle_object_tests
+    fn.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]
+    fn.restype = C.c_int
+    rays = np.ascontiguousarray(rays)
+    t = np.ascontiguousarray(t_hit, np.float32)
+    out = np.zeros(os_.object_count, np.uint32)
+    assert fn(os_.tlas.ctypes.data, os_.tlas.size // 8, os_.blas_root.ctypes.data, os_.object_count,
+              rays.ctypes.data, t.ctypes.data, rays.shape[0], out.ctypes.data) == 0
+    return out
+
+
+class ObjectPosterior:
+    """processRayHitCounters' per-object Beta posterior (Renderer.cpp:8420-8522) in numpy float32,
+    in the device kernel's operation order (k_posterior, residency.cu): alpha, beta, clamped
+    probability, variance, mass, exploration score, idle steps."""
+
+    def __init__(self, n):
+        f = np.float32
+        self.alpha = np.ones(n, f)
+        self.beta = np.ones(n, f)
+        self.probability = np.full(n, 0.5, f)
+        self.variance = np.full(n, f(1.0) / f(12.0), f)
+        self.mass = np.full(n, 2.0, f)
+        self.exploration = np.zeros(n, f)
+        self.idle = np.zeros(n, np.uint32)
+
+    def step(self, hits, tests, visible, active, decay=0.9, hit_decay=0.85, window=64.0, idle_frames=0,
+             idle_decay=0.9, threshold=0.5):
+        f = np.float32
+        decay, hit_decay, idle_decay, threshold = f(decay), f(hit_decay), f(idle_decay), f(threshold)
+        clamp_mass = window > 0 and np.isfinite(window)
+        max_mass = max(f(window), f(1.0e-3))
+        visible, active = np.asarray(visible, bool), np.asarray(active, bool)
+        success, rays = hits.astype(f), tests.astype(f)
+        failure = np.maximum(rays - success, f(0))
+        alpha = self.alpha * decay + success
+        beta = self.beta * decay + failure
+        s = alpha + beta
+        with np.errstate(all="ignore"):
+            prob = np.where(s > 0, alpha / s, f(0.5)).astype(f)
+        idle = self.idle.copy()
+        cool = tests == 0
+        grace = (idle_frames > 0) & (visible | active) & (idle < idle_frames)
+        factor = np.full(alpha.shape, decay, f)
+        apply = cool.copy()
+        if idle_decay >= f(0.999):
+            apply &= ~grace
+        else:
+            factor = np.where(grace, idle_decay, factor).astype(f)
+        cp = np.clip(prob * factor, f(0), f(1))
+        cm = np.maximum(s, f(1.0e-3))
+        if clamp_mass:
+            cm = np.where(cm > max_mass, max_mass, cm).astype(f)
+        alpha = np.where(apply, cp * cm, alpha).astype(f)
+        beta = np.where(apply, np.maximum(cm - cp * cm, f(0)), beta).astype(f)
+        # renormalise the mass into [1e-3, window]
+        s = alpha + beta
+        zero = ~(s > 0)
+        small = (~zero) & (s < f(1.0e-3))
+        with np.errstate(all="ignore"):
+            scale = np.where(small, f(1.0e-3) / s, f(1)).astype(f)
+        alpha = np.where(small, alpha * scale, alpha).astype(f)
+        beta = np.where(small, beta * scale, beta).astype(f)
+        alpha = np.where(zero, f(1.0e-3) * f(0.5), alpha).astype(f)
+        beta = np.where(zero, f(1.0e-3) * f(0.5), beta).astype(f)
+        s = np.where(zero | small, f(1.0e-3), s).astype(f)
+        if clamp_mass:
+            big = s > max_mass
+            with np.errstate(all="ignore"):
+                scale = np.where(big, max_mass / s, f(1)).astype(f)
+            alpha = np.where(big, alpha * scale, alpha).astype(f)
+            beta = np.where(big, beta * scale, beta).astype(f)
+            s = np.where(big, max_mass, s).astype(f)
+        with np.errstate(all="ignore"):
+            prob = np.where(s > 0, alpha / s, f(0.5)).astype(f)
+            var = np.where(s > 1, (alpha * beta) / ((s * s) * (s + f(1))), f(0)).astype(f)
+        clamped = np.clip(prob, f(0), f(1))
+        ex = self.exploration * decay
+        tested = tests > 0
+        ex = np.where(tested, np.where(clamped < threshold, ex + rays, ex * hit_decay), ex * hit_decay).astype(f)
+        ex = np.where((~tested) & (visible | active), np.maximum(ex, f(1)), ex).astype(f)
+        idle = np.where(tested, 0, np.minimum(idle.astype(np.uint64) + 1, 0xFFFFFFFF)).astype(np.uint32)
+        self.alpha, self.beta, self.probability = alpha, beta, clamped
+        self.variance, self.mass, self.exploration, self.idle = np.maximum(var, f(0)), s, ex, idle
+
+
+def rayhit_prior(probability, scale):
+    """The reference's ray-hit prior weight clamp(1 + (p - 0.5) * scale, 0.25, 1)
+    (RendererResidency.cpp:2842-2861, favouring high probability off)."""
+    f = np.float32
+    w = f(1) + (probability.astype(f) - f(0.5)) * f(scale) * f(1)
+    return np.clip(w, f(0.25), f(1)).astype(f)
+
+
+class ProbabilisticOracle:
+    """updateProbabilisticResidency's object-level path (RendererResidency.cpp:3389-4090), one
+    object at a time (primitive counts are the objects'; their cooldowns are the object's), in
+    numpy float32, over the posterior of the same step (ObjectPosterior, whose exploration scores
+    it updates as the reference does). step() returns the object activity after the toggles."""
+
+    def __init__(self, prim_counts):
+        n = len(prim_counts)
+        self.counts = np.asarray(prim_counts, np.int64)
+        self.desired_state = np.zeros(n, np.uint8)
+        self.pending = np.zeros(n, np.uint8)
+        self.promoted = np.zeros(n, np.int64)
+        self.demoted = np.zeros(n, np.int64)
+        self.dwell = np.zeros(n, np.int64)
+        self.evidence = np.zeros(n, np.float32)
+        self.order = list(range(n))
+        self.cooldown = np.zeros(n, np.int64)
+
+    def decrement_cooldowns(self):
+        self.cooldown = np.maximum(self.cooldown - 1, 0)
+
+    def step(self, post, tests_last, visible, active, frame_no, target_fraction=0.60, min_active=16,
+             max_toggles=20, camera_motion=0.0, memory_pressure=0.0, window=64.0, threshold=0.5,
+             uncertainty_boost=0.25, desired_hysteresis=0.02, visible_floor=0.0, recent_promotion_frames=4,
+             demotion_dwell_frames=0, state_cooldown=5):
+        import math
+
+        f = np.float32
+        n = len(self.counts)
+        active = np.asarray(active, bool).copy()
+        vis = np.asarray(visible, bool)
+        prim_count = int(self.counts.sum())
+        contribution = np.maximum(self.counts, 1)
+
+        def cl(v):
+            return min(max(f(v), f(0)), f(1))
+
+        motion, pressure = cl(camera_motion), cl(memory_pressure)
+        tf = min(max(f(target_fraction) + f(0.08) * motion - f(0.12) * pressure, f(0.45)), f(0.93))
+        base = max(int(max_toggles), 1)
+        budget = max(1, int(math.floor(base * (1.0 + 0.40 * float(motion) + 0.50 * float(pressure)) + 0.5)))
+        finite = window > 0 and np.isfinite(window)
+        scoring = max(f(window), f(1e-3)) if finite else max(f(64.0), f(1e-3))
+        thr = f(threshold)
+
+        def evidence(mass, visible_):
+            if not (mass > 0) or not np.isfinite(mass) or not visible_:
+                return f(0)
+            return cl(mass / scoring) if finite else cl(mass / (mass + scoring))
+
+        def sane(p):
+            return cl(p) if np.isfinite(p) else f(0.5)
+
+        def regressed(p, e):
+            ce = cl(e)
+            return sane(p) * ce + f(0.5) * (f(1) - ce)
+
+        def score_e(p, var, e):
+            v = f(0) if (not np.isfinite(var) or var < 0) else f(var)
+            return regressed(p, e) + f(uncertainty_boost) * np.sqrt(max(v, f(0)))
+
+        P, V, M, X = post.probability, post.variance, post.mass, post.exploration
+        desired = self.desired_state.copy()
+        pending = self.pending
+        hyst = min(max(f(desired_hysteresis), f(0)), f(0.5))
+        enter_t, exit_t = cl(thr + hyst), cl(thr - hyst)
+        floor_v = cl(visible_floor)
+        desired_count = 0
+        for i in range(n):
+            raw = evidence(M[i], vis[i])
+            buffered = max(cl(raw), self.evidence[i] * f(0.9))
+            self.evidence[i] = buffered
+            eff = regressed(sane(P[i]), buffered)
+            boosted = score_e(P[i], V[i], buffered)
+            enter_s, exit_s = max(eff, boosted), eff
+            prev = bool(desired[i])
+            want = prev
+            low = min(buffered, cl(raw)) <= f(1e-3)
+            promotion, demotion, evaluation = enter_s, exit_s, (eff if low else enter_s)
+            dwell_applies = bool(vis[i]) and demotion_dwell_frames > 0
+            if not dwell_applies or demotion > exit_t:
+                self.dwell[i] = 0
+            if vis[i]:
+                demotion = max(demotion, floor_v)
+                evaluation = max(evaluation, floor_v)
+            if promotion >= enter_t:
+                want = True
+                self.dwell[i] = 0
+            elif demotion <= exit_t:
+                if dwell_applies and prev:
+                    if self.dwell[i] < demotion_dwell_frames:
+                        self.dwell[i] += 1
+                    want = self.dwell[i] < demotion_dwell_frames
+                else:
+                    want = False
+                    self.dwell[i] = 0
+            elif self.cooldown[i] == 0 and not prev:
+                want = evaluation >= thr
+                if want:
+                    self.dwell[i] = 0
+            if want and not prev:
+                self.promoted[i] = frame_no
+            elif not want and prev:
+                self.demoted[i] = frame_no
+            desired[i] = 1 if want else 0
+            if not want:
+                pending[i] = 0
+            if want and not pending[i]:
+                desired_count += int(contribution[i])
+        min_act = min(int(min_active), prim_count)
+        keys = [_sanitize(score_e(P[o], V[o], evidence(M[o], vis[o]))) for o in range(n)]
+        self.order.sort(key=lambda o: (-keys[o], o))
+        order = self.order
+        target = int(math.ceil(f(prim_count) * tf))
+        target = max(target, min_act)
+        if target == 0 and prim_count > 0:
+            target = 1
+        target = min(target, prim_count)
+
+        def trim():
+            nonlocal desired_count
+            if target == 0 or desired_count <= target:
+                return
+            for idx in reversed(order):
+                if desired_count <= target:
+                    break
+                if not desired[idx] or pending[idx]:
+                    continue
+                c = int(contribution[idx])
+                desired[idx] = 0
+                pending[idx] = 0
+                self.demoted[idx] = frame_no
+                desired_count = desired_count - c if desired_count > c else 0
+
+        trim()
+        vis_x, hid_x = [], []
+        for idx in order:
+            if active[idx] or desired[idx]:
+                continue
+            raw = evidence(M[idx], vis[idx])
+            buffered = self.evidence[idx]
+            eff = regressed(P[idx], buffered)
+            low = min(buffered, cl(raw)) <= f(1e-3)
+            gated = min(eff, thr) if (vis[idx] and low) else eff
+            if gated > thr:
+                continue
+            rays = int(tests_last[idx])
+            ex = f(X[idx])
+            if vis[idx] and (rays == 0 or low):
+                ex = max(ex, f(1))
+            if vis[idx] and rays > 0 and not low:
+                ex = max(ex, f(1e-3))
+            X[idx] = ex
+            if ex <= 0:
+                continue
+            (vis_x if vis[idx] else hid_x).append(idx)
+        vis_x.sort(key=lambda o: (-_sanitize(X[o]), -int(tests_last[o]), o))
+        hid_x.sort(key=lambda o: (-_sanitize(X[o]), -int(tests_last[o]), o))
+
+        def recent(idx):
+            w = recent_promotion_frames
+            if w == 0:
+                return False
+            last = max(self.promoted[idx], self.demoted[idx])
+            if last == 0:
+                return False
+            if frame_no <= last:
+                return True
+            return frame_no - last < w
+
+        def mark(idx):
+            nonlocal desired_count
+            desired[idx] = 1
+            self.promoted[idx] = frame_no
+            c = int(contribution[idx])
+            if not pending[idx]:
+                desired_count += c
+            if vis[idx] and int(tests_last[idx]) == 0 and X[idx] < f(1):
+                X[idx] = f(1)
+            return c
+
+        def promote(cands, slots, allow):
+            if slots == 0:
+                return 0
+            for idx in cands:
+                if slots == 0:
+                    break
+                if desired[idx]:
+                    continue
+                if not allow and recent(idx):
+                    continue
+                c = mark(idx)
+                slots = 0 if slots <= c else slots - c
+            return slots
+
+        def remaining_of(cands):
+            return sum(int(contribution[i]) for i in cands if not desired[i] and not pending[i])
+
+        if desired_count < min_act:
+            slots = min(min_act - desired_count, prim_count - desired_count if prim_count > desired_count else 0)
+            slots = promote(vis_x, slots, False)
+            slots = promote(hid_x, slots, False)
+            if slots > 0:
+                slots = promote(vis_x, slots, True)
+                slots = promote(hid_x, slots, True)
+        if desired_count < min_act:
+            for allow in (False, True):
+                if desired_count >= min_act:
+                    break
+                for idx in order:
+                    if desired_count >= min_act:
+                        break
+                    if desired[idx]:
+                        continue
+                    if not allow and recent(idx):
+                        continue
+                    mark(idx)
+        remaining = remaining_of(vis_x) + remaining_of(hid_x)
+        if remaining > 0 and desired_count < prim_count:
+            slots = min(max(1, min_act // 2), remaining, prim_count - desired_count)
+            slots = promote(vis_x, slots, False)
+            slots = promote(hid_x, slots, False)
+            if slots > 0:
+                slots = promote(vis_x, slots, True)
+                slots = promote(hid_x, slots, True)
+        desired_count = sum(int(contribution[i]) for i in range(n) if desired[i] and not pending[i])
+        trim()
+        fallback = vis_x[0] if vis_x else (hid_x[0] if hid_x else (order[0] if order else n))
+
+        def set_object(o, want):
+            prev_state = bool(active[o])
+            toggled = int(self.counts[o]) if (want != prev_state) else 0
+            active[o] = want and self.counts[o] > 0
+            new_state = bool(active[o])
+            self.desired_state[o] = 1 if new_state else 0
+            if new_state:
+                self.promoted[o] = frame_no
+            else:
+                self.demoted[o] = frame_no
+            if not new_state or toggled > 0:
+                pending[o] = 0
+            if toggled > 0 or prev_state != new_state or not new_state:
+                self.cooldown[o] = state_cooldown
+            return toggled
+
+        toggle_order, added = [], np.zeros(n, bool)
+        applied = np.zeros(n, bool)
+        for cands in ([i for i in range(n) if pending[i]], [i for i in order if desired[i]], vis_x, hid_x, order):
+            for idx in cands:
+                if not added[idx]:
+                    toggle_order.append(idx)
+                    added[idx] = True
+        toggled_prims = 0
+        for idx in toggle_order:
+            if budget == 0 or toggled_prims >= budget:
+                break
+            want, current = bool(desired[idx]), bool(active[idx])
+            if want == current:
+                continue
+            if self.cooldown[idx] > 0:
+                if want:
+                    pending[idx] = 1
+                continue
+            pend = int(self.counts[idx]) if want else int(self.counts[idx]) * int(current)
+            if pend == 0:
+                continue
+            rem = budget - toggled_prims if budget > toggled_prims else 0
+            if pend > rem:
+                if want:
+                    pending[idx] = 1
+                continue
+            t = set_object(idx, want)
+            if t > 0:
+                toggled_prims += min(t, rem)
+                if want and not applied[idx]:
+                    applied[idx] = True
+                    pending[idx] = 0
+                    self.desired_state[idx] = 1
+                if not want:
+                    X[idx] = f(0)
+                    pending[idx] = 0
+                    self.desired_state[idx] = 0
+        if not active.any() and n > 0:
+            fb = fallback if fallback < n else 0
+            rem = budget - toggled_prims if budget > toggled_prims else 0
+            if rem > 0:
+                t = set_object(fb, True)
+                toggled_prims += min(t, rem)
+            self.desired_state[fb] = 1
+            self.promoted[fb] = frame_no
+        return active, toggled_prims
+
+
+def _sanitize(v):
+    fmax = np.finfo(np.float32).max
+    v = np.float32(v)
+    if np.isnan(v):
+        return -fmax
+    return min(max(v, -fmax), fmax)
