@@ -306,7 +306,9 @@ enum {
   NOMAD_POLICY_RAYHIT_PRIM = 3,   /* the reference's per-primitive ray-hit budget (see below)    */
   NOMAD_POLICY_DISTANCE_LOD = 4,  /* the reference's DistanceLOD heuristic (see below)           */
   NOMAD_POLICY_SCREEN_SPACE = 5,  /* the reference's ScreenSpaceFootprint heuristic (see below)  */
-  NOMAD_POLICY_PROBABILISTIC = 6  /* the reference's Probabilistic heuristic (see below)         */
+  NOMAD_POLICY_PROBABILISTIC = 6, /* the reference's Probabilistic heuristic (see below)         */
+  NOMAD_POLICY_ENVIRONMENT_HIT = 7, /* the reference's EnvironmentHit heuristic (see below)      */
+  NOMAD_POLICY_PREDICTIVE = 8     /* the reference's PredictiveEnvironment heuristic (see below) */
 };
 #define NOMAD_FEATURES 24
 
@@ -364,6 +366,13 @@ typedef struct nomad_residency_params {
   float visible_floor;               /* probabilityVisibleFloor 0                              */
   uint32_t recent_promotion_frames;  /* probabilityRecentPromotionFrames 4                     */
   uint32_t demotion_dwell_frames;    /* probabilityVisibleDemotionDwellFrames 0                */
+  /* NOMAD_POLICY_ENVIRONMENT_HIT and NOMAD_POLICY_PREDICTIVE (updateEnvironmentHitResidency,
+   * RendererResidency.cpp:4759-5155; updatePredictiveResidency :4397-4757; target_fraction is
+   * environmentTargetActiveFraction 0.25, min_active environmentMinActivePrimitives 16 and
+   * max_toggles environmentMaxTogglesPerFrame 20, in primitives): */
+  float env_escape_threshold;        /* environmentEscapeThreshold 0.4                         */
+  float env_high_escape;             /* envHighEscapeThreshold 0.6 (EnvironmentHit only)       */
+  float env_low_escape;              /* envLowEscapeThreshold 0.3 (EnvironmentHit only)        */
 } nomad_residency_params;
 
 /* One residency step, all on the device: consumes the per-object closest-hit counts gathered

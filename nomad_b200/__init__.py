@@ -7,7 +7,8 @@ builds host-side ray batches; it has no CPU fallback.
 from .native import (  # noqa: F401
     VIEW_DTYPE, VIEW_CLAMP, VIEW_RESTIR, VIEW_CENTER, view_pinhole, ResidencyParams, N_FEATURES, MLP_PARAMS,
     POLICY_ALWAYS, POLICY_RAYHIT_BUDGET, POLICY_LEARNED, POLICY_RAYHIT_PRIM, POLICY_DISTANCE_LOD,
-    POLICY_SCREEN_SPACE, POLICY_PROBABILISTIC, RestirConfig,
+    POLICY_SCREEN_SPACE, POLICY_PROBABILISTIC, POLICY_ENVIRONMENT_HIT, POLICY_PREDICTIVE,
+    RestirConfig,
     Context, HostScene, LoadedScene, SceneBVH, NomadError, load, load_scene_xml, synth_city, synth_icospheres,
     RAY_DTYPE, HIT_DTYPE, INSTANCE_DTYPE, LIB_PATH, SIGNATURES,
     KERNEL_AUTO, KERNEL_BVH2, KERNEL_BVH2_PERSIST, KERNEL_BVH4, KERNEL_BVH4_PERSIST, KERNEL_BVH8,

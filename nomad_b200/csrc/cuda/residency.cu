@@ -670,6 +670,8 @@ nomad_status nomad_residency_init(nomad_ctx *ctx) {
   }
   R.testsOn = false;
   R.probOn = false;
+  R.probOrder.clear();
+  R.prevSegments = R.prevEscapes = 0;
   R.frame = 0;
   R.havePrevCam = false;
   R.ready = true;
@@ -1658,6 +1660,199 @@ nomad_status probabilistic_step(nomad_ctx *ctx, const nomad_residency_params *pr
   return NOMAD_OK;
 }
 
+// updateEnvironmentHitResidency (RendererResidency.cpp:4759-5155) and updatePredictiveResidency
+// (:4397-4757), over the device posterior of the same step. Both rank objects by a weighted
+// importance (EnvironmentHit: the hit probability, raised to an exploration prior for objects
+// without evidence; Predictive: that times the ray-hit score per primitive), want objects in that
+// order until the activation floor is reached and the mean escape probability of the wanted
+// primitives is at most the escape threshold, then toggle with a budget that grows with the
+// off-screen resident primitives and lets low-importance off-screen objects leave despite their
+// cooldown. EnvironmentHit also moves the activation floor with the last frame's fraction of ray
+// segments that escaped to the environment. Visibility is the device frustum test; no depth
+// weights are configured (environmentDepthWeights empty: weight 1). setObjectActive's cooldown
+// rule (:1025-1026) applies where an object toggles.
+nomad_status environment_step(nomad_ctx *ctx, const nomad_residency_params *prm, const nomad_view &view,
+                              uint32_t *toggled, bool predictive) {
+  auto &R = ctx->res;
+  const uint32_t N = ctx->objectCount;
+  if (!toggled) return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "the environment policies run synchronously");
+  if (N > kMaxSelectObjects)
+    return nomad_fail(ctx, NOMAD_ERR_LIMIT, "the residency policies support at most 16384 objects");
+  nomad_status hs = nomad_residency_sync_host(ctx);
+  if (hs != NOMAD_OK) return hs;
+  if (!R.testsOn) {
+    R.testsOn = true;
+    ctx->frame.clearGraphs();  // the frame now also counts rays tested per object
+  }
+  if (R.objCooldown.size() != N) R.objCooldown.assign(N, 0);
+  if (R.probOrder.size() != N) {
+    R.probOrder.resize(N);
+    std::iota(R.probOrder.begin(), R.probOrder.end(), 0u);
+  }
+  for (uint32_t &c : R.objCooldown)
+    if (c > 0) --c;
+  cudaStream_t s = ctx->stream;
+  nomad_status st = object_pass(ctx, prm, &view);
+  if (st != NOMAD_OK) return st;
+  ++R.frame;
+  std::vector<float> post((size_t)N * kPostWords), score(N);
+  std::vector<uint8_t> vis(N);
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(post.data(), R.post.p, post.size() * 4, cudaMemcpyDeviceToHost, s));
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(vis.data(), R.visible.p, N, cudaMemcpyDeviceToHost, s));
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(score.data(), R.score.p, (size_t)N * 4, cudaMemcpyDeviceToHost, s));
+  NOMAD_CUDA(ctx, cudaStreamSynchronize(s));
+  // the last frame's fraction of closest-hit segments that escaped (processRayHitCounters :8324-8328)
+  uint64_t stats[4];
+  st = nomad_render_stats(ctx, stats);
+  if (st != NOMAD_OK) return st;
+  if (stats[0] < R.prevSegments || stats[1] < R.prevEscapes) R.prevSegments = R.prevEscapes = 0;  // stats reset
+  const uint64_t segments = stats[0] - R.prevSegments, escapes = stats[1] - R.prevEscapes;
+  R.prevSegments = stats[0];
+  R.prevEscapes = stats[1];
+  const float globalEscape =
+      segments > 0 ? (float)(uint32_t)escapes / (float)std::max<uint32_t>((uint32_t)segments, 1u) : 0.0f;
+
+  auto Pf = [&](uint32_t o, int k) { return post[(size_t)o * kPostWords + k]; };
+  auto testsLast = [&](uint32_t o) {
+    uint32_t v;
+    std::memcpy(&v, &post[(size_t)o * kPostWords + 8], 4);
+    return v;
+  };
+  auto active = [&](uint32_t o) { return ctx->objActiveCount[o] > 0; };
+  const size_t primCount = ctx->primCount;
+  const float motion = clamp_unit(prm->camera_motion), pressure = clamp_unit(prm->memory_pressure);
+  const float escapeThreshold =
+      std::min(std::max(prm->env_escape_threshold + 0.03f * motion + 0.08f * pressure, 0.12f), 0.95f);
+  const float targetFraction = std::min(std::max(prm->target_fraction + 0.08f * motion - 0.10f * pressure, 0.12f),
+                                        predictive ? 0.92f : 0.94f);
+  const size_t baseBudget = std::max<size_t>(prm->max_toggles, 1);
+  const size_t toggleBudget = std::max<size_t>(
+      1, (size_t)std::llround((double)baseBudget * (1.0 + 0.40 * (double)motion + 0.70 * (double)pressure)));
+  constexpr float kPriorFloor = 1.0e-4f, kPriorScale = 0.5f, kVisibleBoost = 2.0f, kHiddenPenalty = 0.05f;
+  constexpr float kSeed = 1.0f;  // kIdleVisibleExploreSeed
+  std::vector<float> importance(N), weighted(N);
+  for (uint32_t o = 0; o < N; ++o) {
+    float prob = std::min(std::max(Pf(o, 2), 0.0f), 1.0f);
+    const bool hasEvidence = testsLast(o) > 0, current = active(o), visible = vis[o] != 0;
+    if (!hasEvidence && !current) {
+      const float ex = std::max(Pf(o, 5), 0.0f);
+      float prior = 1.0f - std::exp(-ex * kPriorScale);
+      if (visible) prior = std::max(prior, 1.0f - std::exp(-kSeed * kPriorScale));
+      prior = std::min(std::max(prior, kPriorFloor), 1.0f);
+      prob = std::max(prob, prior);
+    }
+    importance[o] = prob;
+    float sc = prob;
+    if (predictive) {
+      float hitScore = score[o];
+      const uint32_t count = ctx->instances[o].primitive_count;
+      if (count > 0) hitScore /= (float)count;
+      if (hitScore <= 0.0f && (current || visible)) hitScore = 1.0f;
+      sc = hitScore * prob;
+    }
+    const float depthWeight = 1.0f, visibilityWeight = visible ? kVisibleBoost : kHiddenPenalty;
+    const float w = sc * std::max(depthWeight, 0.0f) * std::max(visibilityWeight, 0.0f);
+    weighted[o] = std::isfinite(w) ? w : 0.0f;
+  }
+  auto &order = R.probOrder;
+  std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+    if (weighted[a] == weighted[b]) {
+      if (importance[a] == importance[b]) return a < b;
+      return importance[a] > importance[b];
+    }
+    return weighted[a] > weighted[b];
+  });
+  size_t minActive = std::min<size_t>(primCount, prm->min_active);
+  if (minActive == 0 && primCount > 0) minActive = 1;
+  size_t targetCount = 0;
+  if (targetFraction > 0.0f && primCount > 0)
+    targetCount = std::min((size_t)std::ceil(targetFraction * (float)primCount), primCount);
+  size_t floorCount = std::max(minActive, targetCount);
+  if (!predictive) {
+    const float high = std::min(std::max(prm->env_high_escape, 0.0f), 1.0f);
+    const float low = std::min(std::max(prm->env_low_escape, 0.0f), high);
+    if (globalEscape > high) floorCount = std::min(primCount, (size_t)((float)floorCount * 1.5f));
+    else if (globalEscape < low) floorCount = std::max(minActive, (size_t)((float)floorCount * 0.8f));
+  }
+  if (floorCount == 0 && primCount > 0) floorCount = 1;
+  std::vector<uint8_t> desired(N, 0);
+  size_t desiredCount = 0;
+  float weightedEscape = 0.0f;
+  auto averageEscape = [](size_t count, float w) { return count == 0 ? 1.0f : w / (float)count; };
+  for (uint32_t idx : order) {
+    const uint32_t count = ctx->instances[idx].primitive_count;
+    if (count == 0) continue;
+    if (!(desiredCount < floorCount) && !(averageEscape(desiredCount, weightedEscape) > escapeThreshold)) break;
+    desired[idx] = 1;
+    desiredCount += count;
+    weightedEscape += (1.0f - importance[idx]) * (float)count;
+  }
+  if (desiredCount == 0 && primCount > 0)
+    for (uint32_t idx : order) {
+      const uint32_t count = ctx->instances[idx].primitive_count;
+      if (count == 0) continue;
+      desired[idx] = 1;
+      desiredCount = count;
+      weightedEscape = (1.0f - importance[idx]) * (float)count;
+      break;
+    }
+  size_t offscreenActive = 0;
+  for (uint32_t o = 0; o < N; ++o)
+    if (active(o) && !vis[o]) offscreenActive += ctx->instances[o].primitive_count;
+  size_t maxBudget = toggleBudget;
+  if (offscreenActive > toggleBudget) maxBudget = std::max(toggleBudget, (offscreenActive + 1) / 2);
+  const size_t reserved = maxBudget == 0 ? 0 : std::max<size_t>(1, maxBudget / 4);
+  const size_t general = maxBudget > reserved ? maxBudget - reserved : 0;
+  const size_t total = maxBudget + reserved;
+  size_t toggledPrims = 0;
+  auto setObject = [&](uint32_t o, bool want, uint32_t &n) -> nomad_status {
+    const bool prevState = active(o);
+    nomad_status r = nomad_residency_set_object_active(ctx, o, want ? 1 : 0, &n);
+    if (r != NOMAD_OK) return r;
+    const bool newState = active(o);
+    if (n > 0 || prevState != newState || !newState) R.objCooldown[o] = prm->state_cooldown;
+    return NOMAD_OK;
+  };
+  for (uint32_t idx : order) {
+    const bool want = desired[idx] != 0, current = active(idx);
+    if (want == current) continue;
+    const bool visible = vis[idx] != 0;
+    const bool bypass = current && !want && !visible && importance[idx] < escapeThreshold;
+    if (!bypass && R.objCooldown[idx] > 0) continue;
+    const uint32_t count = ctx->instances[idx].primitive_count;
+    if (count == 0) continue;
+    const size_t pendingToggles = want ? count - ctx->objActiveCount[idx] : ctx->objActiveCount[idx];
+    if (pendingToggles == 0) continue;
+    if (toggledPrims >= (bypass ? total : general)) continue;
+    uint32_t n = 0;
+    st = setObject(idx, want, n);
+    if (st != NOMAD_OK) return st;
+    if (n > 0) toggledPrims = std::min(toggledPrims + n, total);
+  }
+  bool anyActive = false;
+  for (uint32_t o = 0; o < N && !anyActive; ++o) anyActive = ctx->instances[o].primitive_count > 0 && active(o);
+  if (!anyActive)
+    for (uint32_t idx : order) {
+      if (ctx->instances[idx].primitive_count == 0) continue;
+      uint32_t n = 0;
+      st = setObject(idx, true, n);
+      if (st != NOMAD_OK) return st;
+      if (n > 0) {
+        anyActive = true;
+        break;
+      }
+    }
+  if (!anyActive && ctx->primCount > 0) {
+    int32_t changed = 0;
+    st = nomad_residency_set_primitive_active(ctx, 0, 1, &changed);
+    if (st != NOMAD_OK) return st;
+  }
+  st = nomad_residency_flush(ctx);
+  if (st != NOMAD_OK) return st;
+  *toggled = (uint32_t)toggledPrims;
+  return NOMAD_OK;
+}
+
 }  // namespace
 
 extern "C" nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residency_params *prm,
@@ -1680,6 +1875,10 @@ extern "C" nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residen
   if (prm->policy == NOMAD_POLICY_PROBABILISTIC) {
     NOMAD_DEVICE_SCOPE(ctx);
     return probabilistic_step(ctx, prm, *camera, toggled);
+  }
+  if (prm->policy == NOMAD_POLICY_ENVIRONMENT_HIT || prm->policy == NOMAD_POLICY_PREDICTIVE) {
+    NOMAD_DEVICE_SCOPE(ctx);
+    return environment_step(ctx, prm, *camera, toggled, prm->policy == NOMAD_POLICY_PREDICTIVE);
   }
   if (prm->policy > NOMAD_POLICY_LEARNED) return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "unknown policy");
   // Without a usable model the learned policy runs the ray-hit budget step instead.

@@ -167,7 +167,9 @@ struct nomad_ctx {
     std::vector<uint8_t> probDesired, probPending;
     std::vector<uint32_t> probPromoted, probDemoted, probDwell;
     std::vector<float> probEvidence;
-    std::vector<uint32_t> probOrder;
+    std::vector<uint32_t> probOrder;  // also the order of the environment policies
+    // EnvironmentHit: render statistics at the previous step (segments, escapes)
+    uint64_t prevSegments = 0, prevEscapes = 0;
     // DistanceLOD policy (NOMAD_POLICY_DISTANCE_LOD): object cooldowns and the last step's tests
     bool lodOn = false;
     std::vector<uint32_t> objCooldown;

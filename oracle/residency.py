@@ -883,3 +883,142 @@ def _sanitize(v):
     if np.isnan(v):
         return -fmax
     return min(max(v, -fmax), fmax)
+
+
+def _libm_expf():
+    import ctypes
+
+    lm = ctypes.CDLL("libm.so.6")
+    lm.expf.restype, lm.expf.argtypes = ctypes.c_float, [ctypes.c_float]
+    return lambda x: np.float32(lm.expf(float(x)))
+
+
+class EnvironmentOracle:
+    """updateEnvironmentHitResidency (RendererResidency.cpp:4759-5155) and, with predictive=True,
+    updatePredictiveResidency (:4397-4757), one object at a time, in numpy float32 (exp by libm
+    expf, as the host build calls it), over the posterior of the same step."""
+
+    def __init__(self, prim_counts, predictive=False):
+        self.counts = np.asarray(prim_counts, np.int64)
+        self.predictive = predictive
+        self.cooldown = np.zeros(len(self.counts), np.int64)
+        self.expf = _libm_expf()
+
+    def decrement_cooldowns(self):
+        self.cooldown = np.maximum(self.cooldown - 1, 0)
+
+    def step(self, post, tests_last, score, visible, active, global_escape, target_fraction=0.25, min_active=16,
+             max_toggles=20, camera_motion=0.0, memory_pressure=0.0, escape_threshold=0.4, high_escape=0.6,
+             low_escape=0.3, state_cooldown=5):
+        import math
+
+        f = np.float32
+        n = len(self.counts)
+        active = np.asarray(active, bool).copy()
+        vis = np.asarray(visible, bool)
+        prim_count = int(self.counts.sum())
+
+        def cl(v, lo=0.0, hi=1.0):
+            return min(max(f(v), f(lo)), f(hi))
+
+        motion, pressure = cl(camera_motion), cl(memory_pressure)
+        thr = cl(f(escape_threshold) + f(0.03) * motion + f(0.08) * pressure, 0.12, 0.95)
+        tf = cl(f(target_fraction) + f(0.08) * motion - f(0.10) * pressure, 0.12, 0.92 if self.predictive else 0.94)
+        base = max(int(max_toggles), 1)
+        budget = max(1, int(math.floor(base * (1.0 + 0.40 * float(motion) + 0.70 * float(pressure)) + 0.5)))
+        importance = np.zeros(n, f)
+        weighted = np.zeros(n, f)
+        for o in range(n):
+            prob = cl(post.probability[o])
+            if not (int(tests_last[o]) > 0) and not active[o]:
+                ex = max(f(post.exploration[o]), f(0))
+                prior = f(1) - self.expf(-ex * f(0.5))
+                if vis[o]:
+                    prior = max(prior, f(1) - self.expf(-f(1) * f(0.5)))
+                prior = cl(prior, 1.0e-4, 1.0)
+                prob = max(prob, prior)
+            importance[o] = prob
+            sc = prob
+            if self.predictive:
+                hs = f(score[o])
+                if self.counts[o] > 0:
+                    hs = hs / f(self.counts[o])
+                if hs <= 0 and (active[o] or vis[o]):
+                    hs = f(1)
+                sc = hs * prob
+            w = sc * max(f(1), f(0)) * max(f(2) if vis[o] else f(0.05), f(0))
+            weighted[o] = w if np.isfinite(w) else f(0)
+        order = sorted(range(n), key=lambda o: (-weighted[o], -importance[o], o))
+        min_act = min(prim_count, int(min_active))
+        if min_act == 0 and prim_count > 0:
+            min_act = 1
+        target = 0
+        if tf > 0 and prim_count > 0:
+            target = min(int(math.ceil(tf * f(prim_count))), prim_count)
+        floor = max(min_act, target)
+        if not self.predictive:
+            high = cl(high_escape)
+            low = min(max(f(low_escape), f(0)), high)
+            if f(global_escape) > high:
+                floor = min(prim_count, int(f(floor) * f(1.5)))
+            elif f(global_escape) < low:
+                floor = max(min_act, int(f(floor) * f(0.8)))
+        if floor == 0 and prim_count > 0:
+            floor = 1
+        desired = np.zeros(n, bool)
+        count = 0
+        wesc = f(0)
+        for idx in order:
+            c = int(self.counts[idx])
+            if c == 0:
+                continue
+            avg = f(1) if count == 0 else wesc / f(count)
+            if not (count < floor) and not (avg > thr):
+                break
+            desired[idx] = True
+            count += c
+            wesc = wesc + (f(1) - importance[idx]) * f(c)
+        if count == 0 and prim_count > 0:
+            for idx in order:
+                if self.counts[idx] == 0:
+                    continue
+                desired[idx] = True
+                break
+        offscreen = int(sum(self.counts[o] for o in range(n) if active[o] and not vis[o]))
+        max_budget = budget
+        if offscreen > budget:
+            max_budget = max(budget, (offscreen + 1) // 2)
+        reserved = 0 if max_budget == 0 else max(1, max_budget // 4)
+        general = max_budget - reserved if max_budget > reserved else 0
+        total = max_budget + reserved
+        toggled = 0
+
+        def set_object(o, want):
+            prev_state = bool(active[o])
+            t = int(self.counts[o]) if want != prev_state else 0
+            active[o] = want and self.counts[o] > 0
+            if t > 0 or prev_state != bool(active[o]) or not active[o]:
+                self.cooldown[o] = state_cooldown
+            return t
+
+        for idx in order:
+            want, current = bool(desired[idx]), bool(active[idx])
+            if want == current:
+                continue
+            bypass = current and not want and not vis[idx] and importance[idx] < thr
+            if not bypass and self.cooldown[idx] > 0:
+                continue
+            if self.counts[idx] == 0:
+                continue
+            if toggled >= (total if bypass else general):
+                continue
+            t = set_object(idx, want)
+            if t > 0:
+                toggled = min(toggled + t, total)
+        if not any(active[o] and self.counts[o] > 0 for o in range(n)):
+            for idx in order:
+                if self.counts[idx] == 0:
+                    continue
+                if set_object(idx, True) > 0:
+                    break
+        return active, toggled

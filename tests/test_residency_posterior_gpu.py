@@ -140,3 +140,46 @@ def test_rayhit_budget_with_prior_matches_oracle(nb, orc, ctx, small_city):
         assert np.array_equal(got, want), frame
         flags = got
     assert (post.probability != 0.5).any() and ctx.status() == 0
+
+
+@pytest.mark.parametrize("predictive", [False, True])
+def test_environment_policies_match_oracle(nb, orc, ctx, small_city, predictive):
+    """updateEnvironmentHitResidency / updatePredictiveResidency over a moving camera against
+    their numpy restatement, fed the device's per-step hits, tests and escape statistics."""
+    from oracle import residency as ores
+
+    _, sb = small_city
+    ctx.upload(sb)
+    N = sb.object_count
+    counts = sb.instances["primitive_count"].astype(np.int64)
+    policy = nb.POLICY_PREDICTIVE if predictive else nb.POLICY_ENVIRONMENT_HIT
+    kw = dict(target_fraction=0.25, min_active=16, max_toggles=3000, camera_motion=0.3, state_cooldown=5)
+    prm = nb.ResidencyParams.make(policy, **kw)
+    post = ores.ObjectPosterior(N)
+    pol = ores.EnvironmentOracle(counts, predictive=predictive)
+    score = np.zeros(N, np.float32)
+    active = ctx.residency_flags().astype(bool)
+    ctx.reset_render_stats()
+    prev = np.zeros(4, np.uint64)
+    changed = 0
+    for frame in range(12):
+        view = _orbit(nb, frame)
+        ctx.render(view, count_hits=True)
+        stats = ctx.render_stats()
+        seg, esc = int(stats[0] - prev[0]), int(stats[1] - prev[1])
+        prev = stats.copy()
+        escape = np.float32(esc) / np.float32(max(seg, 1)) if seg > 0 else np.float32(0)
+        pol.decrement_cooldowns()
+        ctx.residency_step(prm, view, toggles=True)
+        dev = ctx.residency_posterior()
+        feats, _ = ctx.residency_last()
+        visible = feats[:, 2] > 0.5
+        post.step(dev["hits"], dev["tests"], visible, active)
+        assert np.array_equal(_bits(dev["probability"]), _bits(post.probability)), frame
+        score = (score * np.float32(0.85) + dev["hits"].astype(np.float32)).astype(np.float32)
+        want, _ = pol.step(post, dev["tests"], score, visible, active, escape, **kw)
+        got = ctx.residency_flags().astype(bool)
+        assert np.array_equal(got, want), (frame, np.nonzero(got != want)[0][:10])
+        changed += int((got != active).sum())
+        active = got
+    assert changed > 0 and ctx.status() == 0
