@@ -1039,6 +1039,60 @@ nomad_status distance_lod_step(nomad_ctx *ctx, const nomad_residency_params *prm
   return NOMAD_OK;
 }
 
+// objectCoverageForSphere (RendererResidency.cpp:4130-4182) of every object's bounding sphere:
+// the projected disc's pixel area times the cosine to the view axis, at most the screen, 0 outside
+// the angular frustum (isInView), behind the camera or well outside horizontally. inView receives
+// the frustum test of each sphere.
+void object_coverage(const nomad_ctx *ctx, const nomad_view &view, std::vector<float> &cov,
+                     std::vector<uint8_t> &inView) {
+  const uint32_t N = ctx->objectCount;
+  cov.assign(N, 0.0f);
+  inView.assign(N, 0);
+  const float W = (float)view.width, H = (float)view.height;
+  float screenArea = W * H;
+  if (screenArea <= 0.0f) screenArea = 1.0f;
+  const AngleCam cam = angle_cam(view);
+  // the camera's own up, not re-orthogonalised
+  float tanHalf = std::tan(cam.halfV);
+  if (tanHalf <= 0.0f) tanHalf = 1e-3f;
+  float V[3], upRaw[3];
+  for (int k = 0; k < 3; ++k) {
+    V[k] = view.viewport_v[k];
+    upRaw[k] = -V[k];
+  }
+  const float ul = std::sqrt(upRaw[0] * upRaw[0] + upRaw[1] * upRaw[1] + upRaw[2] * upRaw[2]);
+  for (int k = 0; k < 3; ++k) upRaw[k] /= ul;
+  float right[3] = {cam.fwd[1] * upRaw[2] - cam.fwd[2] * upRaw[1], cam.fwd[2] * upRaw[0] - cam.fwd[0] * upRaw[2],
+                    cam.fwd[0] * upRaw[1] - cam.fwd[1] * upRaw[0]};
+  const float rl2 = right[0] * right[0] + right[1] * right[1] + right[2] * right[2];
+  if (rl2 < 1e-6f) {
+    right[0] = 1.0f; right[1] = 0.0f; right[2] = 0.0f;
+  } else {
+    const float rl = std::sqrt(rl2);
+    for (int k = 0; k < 3; ++k) right[k] /= rl;
+  }
+  const float aspect = H > 0.0f ? W / H : 1.0f;
+  const float hHalf = std::atan(tanHalf * aspect);
+  constexpr float kPi = 3.14159265358979323846f;
+  for (uint32_t o = 0; o < N; ++o) {
+    float sph[4];
+    if (!object_sphere(ctx, o, sph)) continue;
+    if (!in_view(cam, sph)) continue;
+    inView[o] = 1;
+    const float tx = sph[0] - cam.pos[0], ty = sph[1] - cam.pos[1], tz = sph[2] - cam.pos[2];
+    const float depth = tx * cam.fwd[0] + ty * cam.fwd[1] + tz * cam.fwd[2];
+    if (depth <= 1e-3f) continue;
+    const float dist = std::sqrt(tx * tx + ty * ty + tz * tz);
+    const float cosAngle = depth / std::max(dist, 1e-3f);
+    const float horiz = tx * right[0] + ty * right[1] + tz * right[2];
+    if (std::atan2(std::fabs(horiz), depth) > hHalf + 0.1f) continue;
+    float rp = (sph[3] / depth) / tanHalf * (H * 0.5f);
+    rp = std::max(rp, 0.0f);
+    const float area = kPi * rp * rp;
+    cov[o] = std::min(area * std::max(cosAngle, 0.0f), screenArea);
+  }
+}
+
 // updateScreenSpaceFootprint (RendererResidency.cpp:4092-4396), one mesh group per object.
 nomad_status screen_space_step(nomad_ctx *ctx, const nomad_residency_params *prm, const nomad_view &view,
                                uint32_t *toggled) {
@@ -1066,49 +1120,11 @@ nomad_status screen_space_step(nomad_ctx *ctx, const nomad_residency_params *prm
   const float W = (float)view.width, H = (float)view.height;
   float screenArea = W * H;
   if (screenArea <= 0.0f) screenArea = 1.0f;
-  const AngleCam cam = angle_cam(view);
-  // objectCoverageForSphere (:4130-4182): the camera's own up, not re-orthogonalised
-  float tanHalf = std::tan(cam.halfV);
-  if (tanHalf <= 0.0f) tanHalf = 1e-3f;
-  float U[3], V[3], upRaw[3];
-  for (int k = 0; k < 3; ++k) {
-    U[k] = view.viewport_u[k];
-    V[k] = view.viewport_v[k];
-    upRaw[k] = -V[k];
-  }
-  const float ul = std::sqrt(upRaw[0] * upRaw[0] + upRaw[1] * upRaw[1] + upRaw[2] * upRaw[2]);
-  for (int k = 0; k < 3; ++k) upRaw[k] /= ul;
-  float right[3] = {cam.fwd[1] * upRaw[2] - cam.fwd[2] * upRaw[1], cam.fwd[2] * upRaw[0] - cam.fwd[0] * upRaw[2],
-                    cam.fwd[0] * upRaw[1] - cam.fwd[1] * upRaw[0]};
-  const float rl2 = right[0] * right[0] + right[1] * right[1] + right[2] * right[2];
-  if (rl2 < 1e-6f) {
-    right[0] = 1.0f; right[1] = 0.0f; right[2] = 0.0f;
-  } else {
-    const float rl = std::sqrt(rl2);
-    for (int k = 0; k < 3; ++k) right[k] /= rl;
-  }
-  const float aspect = H > 0.0f ? W / H : 1.0f;
-  const float hHalf = std::atan(tanHalf * aspect);
-  constexpr float kPi = 3.14159265358979323846f;
-  std::vector<float> cov(N, 0.0f);
+  std::vector<float> cov;
+  std::vector<uint8_t> inView;
+  object_coverage(ctx, view, cov, inView);
   std::vector<uint32_t> order(N);
-  for (uint32_t o = 0; o < N; ++o) {
-    order[o] = o;
-    float sph[4];
-    if (!object_sphere(ctx, o, sph)) continue;
-    if (!in_view(cam, sph)) continue;
-    const float tx = sph[0] - cam.pos[0], ty = sph[1] - cam.pos[1], tz = sph[2] - cam.pos[2];
-    const float depth = tx * cam.fwd[0] + ty * cam.fwd[1] + tz * cam.fwd[2];
-    if (depth <= 1e-3f) continue;
-    const float dist = std::sqrt(tx * tx + ty * ty + tz * tz);
-    const float cosAngle = depth / std::max(dist, 1e-3f);
-    const float horiz = tx * right[0] + ty * right[1] + tz * right[2];
-    if (std::atan2(std::fabs(horiz), depth) > hHalf + 0.1f) continue;
-    float rp = (sph[3] / depth) / tanHalf * (H * 0.5f);
-    rp = std::max(rp, 0.0f);
-    const float area = kPi * rp * rp;
-    cov[o] = std::min(area * std::max(cosAngle, 0.0f), screenArea);
-  }
+  for (uint32_t o = 0; o < N; ++o) order[o] = o;
   for (uint32_t o = 0; o < N; ++o) R.lodDist[o] = cov[o];
   std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
     const float ca = sanitize(cov[a]), cb = sanitize(cov[b]);
@@ -1305,8 +1321,8 @@ nomad_status object_pass(nomad_ctx *ctx, const nomad_residency_params *prm, cons
   const float window = prm->probability_window;
   PostArgs pa{N, R.frame, R.hist.as<const uint32_t>(), R.tests.as<uint32_t>(), R.visible.as<const uint8_t>(),
               R.objRes.as<const uint8_t>(), R.post.as<float>(), prm->probability_decay, prm->hit_decay,
-              std::max(window, 1.0e-3f), (window > 0.0f && std::isfinite(window)) ? 1 : 0,
-              prm->probability_idle_decay, prm->probability_threshold, prm->probability_idle_frames,
+              std::max(window, 1.0e-3f), prm->probability_idle_decay, prm->probability_threshold,
+              (window > 0.0f && std::isfinite(window)) ? 1 : 0, prm->probability_idle_frames,
               prm->policy == NOMAD_POLICY_RAYHIT_BUDGET ? R.keys.as<float>() : nullptr, prm->rayhit_prior_scale};
   k_posterior<<<(N + 127) / 128, 128, 0, s>>>(pa);
   NOMAD_CUDA(ctx, cudaGetLastError());
