@@ -308,7 +308,8 @@ enum {
   NOMAD_POLICY_SCREEN_SPACE = 5,  /* the reference's ScreenSpaceFootprint heuristic (see below)  */
   NOMAD_POLICY_PROBABILISTIC = 6, /* the reference's Probabilistic heuristic (see below)         */
   NOMAD_POLICY_ENVIRONMENT_HIT = 7, /* the reference's EnvironmentHit heuristic (see below)      */
-  NOMAD_POLICY_PREDICTIVE = 8     /* the reference's PredictiveEnvironment heuristic (see below) */
+  NOMAD_POLICY_PREDICTIVE = 8,    /* the reference's PredictiveEnvironment heuristic (see below) */
+  NOMAD_POLICY_ENERGY = 9         /* the reference's EnergyImportance heuristic (see below)      */
 };
 #define NOMAD_FEATURES 24
 
@@ -373,6 +374,14 @@ typedef struct nomad_residency_params {
   float env_escape_threshold;        /* environmentEscapeThreshold 0.4                         */
   float env_high_escape;             /* envHighEscapeThreshold 0.6 (EnvironmentHit only)       */
   float env_low_escape;              /* envLowEscapeThreshold 0.3 (EnvironmentHit only)        */
+  /* NOMAD_POLICY_ENERGY (updateEnergyImportance, RendererResidency.cpp:1344-1860, scenes without
+   * mesh groups; target_fraction is energyTargetFraction 0.88, min_active
+   * energyMinActivePrimitives 16, max_toggles energyMaxTogglesPerFrame 32, in primitives;
+   * state_cooldown both the object cooldown and the minimum duration between an object's
+   * residency changes, stateCooldownFrames 5): */
+  float energy_visibility_boost;     /* energyVisibilityBoost 1.75                             */
+  float energy_smoothing;            /* energyImportanceSmoothing 0.85                         */
+  uint32_t energy_use_average;       /* energyUseAverageImportance 1                           */
 } nomad_residency_params;
 
 /* One residency step, all on the device: consumes the per-object closest-hit counts gathered

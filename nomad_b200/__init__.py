@@ -7,7 +7,7 @@ builds host-side ray batches; it has no CPU fallback.
 from .native import (  # noqa: F401
     VIEW_DTYPE, VIEW_CLAMP, VIEW_RESTIR, VIEW_CENTER, view_pinhole, ResidencyParams, N_FEATURES, MLP_PARAMS,
     POLICY_ALWAYS, POLICY_RAYHIT_BUDGET, POLICY_LEARNED, POLICY_RAYHIT_PRIM, POLICY_DISTANCE_LOD,
-    POLICY_SCREEN_SPACE, POLICY_PROBABILISTIC, POLICY_ENVIRONMENT_HIT, POLICY_PREDICTIVE,
+    POLICY_SCREEN_SPACE, POLICY_PROBABILISTIC, POLICY_ENVIRONMENT_HIT, POLICY_PREDICTIVE, POLICY_ENERGY,
     RestirConfig,
     Context, HostScene, LoadedScene, SceneBVH, NomadError, load, load_scene_xml, synth_city, synth_icospheres,
     RAY_DTYPE, HIT_DTYPE, INSTANCE_DTYPE, LIB_PATH, SIGNATURES,

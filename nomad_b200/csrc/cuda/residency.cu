@@ -672,6 +672,10 @@ nomad_status nomad_residency_init(nomad_ctx *ctx) {
   R.probOn = false;
   R.probOrder.clear();
   R.prevSegments = R.prevEscapes = 0;
+  R.lastToggle.clear();
+  R.energyHist.clear();
+  R.energyTotal.clear();
+  R.energyEmit.clear();
   R.frame = 0;
   R.havePrevCam = false;
   R.ready = true;
@@ -1869,6 +1873,263 @@ nomad_status environment_step(nomad_ctx *ctx, const nomad_residency_params *prm,
   return NOMAD_OK;
 }
 
+// updateEnergyImportance (RendererResidency.cpp:1344-2239), its object path for scenes without
+// mesh groups (:1462-1860), over the device posterior and ray-hit score of the same step.
+// Per object: the summed primitive importance (area times emitted + diffuse + specular +
+// transmitted luminance, primitiveImportance Renderer.cpp:1482-1490), raised by the visibility
+// boost with the object's screen coverage, times a transport boost from its hit probability,
+// normalised ray-hit score, visibility and normalised emitted power, smoothed over steps and
+// divided by the primitive count; objects are wanted in that order until min_active primitives
+// and the target share of the importance are reached, and toggled in index order under a
+// primitive budget and two cooldowns (the per-step object cooldown and the minimum residency
+// duration since the last change, :1664-1678). No depth weights are configured (weight 1).
+nomad_status energy_step(nomad_ctx *ctx, const nomad_residency_params *prm, const nomad_view &view,
+                         uint32_t *toggled) {
+  auto &R = ctx->res;
+  const uint32_t N = ctx->objectCount;
+  if (!toggled) return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "the EnergyImportance policy runs synchronously");
+  if (N > kMaxSelectObjects)
+    return nomad_fail(ctx, NOMAD_ERR_LIMIT, "the residency policies support at most 16384 objects");
+  nomad_status hs = nomad_residency_sync_host(ctx);
+  if (hs != NOMAD_OK) return hs;
+  if (!R.testsOn) {
+    R.testsOn = true;
+    ctx->frame.clearGraphs();  // the frame now also counts rays tested per object
+  }
+  if (R.objCooldown.size() != N) R.objCooldown.assign(N, 0);
+  if (R.lodDist.size() != N) R.lodDist.assign(N, 0.0f);
+  if (R.lodFlags.size() != N) R.lodFlags.assign(N, 0);
+  if (R.lastToggle.size() != N) R.lastToggle.assign(N, 0);
+  bool resetHistory = false;
+  if (R.energyHist.size() != N) {
+    R.energyHist.assign(N, 0.0f);
+    resetHistory = true;
+  }
+  if (R.energyTotal.size() != N) {
+    // static per-object sums over the primitives (primitiveImportance and the emitted power times
+    // the area), in primitive order, and their total over the scene (_totalPrimitiveImportance)
+    R.energyTotal.assign(N, 0.0f);
+    R.energyEmit.assign(N, 0.0f);
+    std::vector<float> perPrim(ctx->primCount, 0.0f), perEmit(ctx->primCount, 0.0f);
+    const float *Pp = ctx->hostPrims.data(), *Mm = ctx->hostMaterials.data();
+    auto lum = [](const float *c) { return 0.2126f * c[0] + 0.7152f * c[1] + 0.0722f * c[2]; };
+    constexpr float kPi = 3.14159265358979323846f;
+    for (uint32_t p = 0; p < ctx->primCount; ++p) {
+      const float *g = Pp + 28ull * p, *m = Mm + 20ull * p;
+      const int type = (int)g[3];
+      float area;
+      if (type == 0) {
+        area = 4.0f * kPi * g[4] * g[4];
+      } else {
+        float ax, ay, az, bx, by, bz;
+        if (type == 1) {
+          ax = g[4] - g[0]; ay = g[5] - g[1]; az = g[6] - g[2];
+          bx = g[8] - g[0]; by = g[9] - g[1]; bz = g[10] - g[2];
+        } else {
+          ax = g[4]; ay = g[5]; az = g[6];
+          bx = g[8]; by = g[9]; bz = g[10];
+        }
+        const float cx = ay * bz - az * by, cy = az * bx - ax * bz, cz = ax * by - ay * bx;
+        const float len = std::sqrt(cx * cx + cy * cy + cz * cz);
+        area = type == 1 ? 0.5f * len : 4.0f * len;
+      }
+      const float emissive = m[11] * lum(m + 8);
+      perPrim[p] = std::max(area, 1e-4f) *
+                   (emissive + lum(m) * m[3] + lum(m + 4) * m[3] + (1.0f - m[3]) * lum(m + 12));
+      perEmit[p] = std::max(emissive * area, 0.0f);
+    }
+    for (uint32_t o = 0; o < N; ++o) {
+      const nomad_instance_record &ir = ctx->instances[o];
+      for (uint32_t p = ir.primitive_base; p < ir.primitive_base + ir.primitive_count; ++p) {
+        R.energyTotal[o] += std::max(perPrim[p], 0.0f);
+        R.energyEmit[o] += perEmit[p];
+      }
+    }
+    R.energyPrimTotal = 0.0f;
+    for (float v : perPrim) R.energyPrimTotal += std::max(v, 0.0f);
+  }
+  for (uint32_t &c : R.objCooldown)
+    if (c > 0) --c;
+  cudaStream_t s = ctx->stream;
+  nomad_status st = object_pass(ctx, prm, &view);
+  if (st != NOMAD_OK) return st;
+  const uint32_t frameNo = R.frame + 1;
+  ++R.frame;
+  std::vector<float> post((size_t)N * kPostWords), score(N);
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(post.data(), R.post.p, post.size() * 4, cudaMemcpyDeviceToHost, s));
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(score.data(), R.score.p, (size_t)N * 4, cudaMemcpyDeviceToHost, s));
+  NOMAD_CUDA(ctx, cudaStreamSynchronize(s));
+  std::vector<float> cov;
+  std::vector<uint8_t> inView;
+  object_coverage(ctx, view, cov, inView);
+  for (uint32_t o = 0; o < N; ++o) {
+    R.lodDist[o] = cov[o];
+    R.lodFlags[o] = inView[o];
+  }
+  auto active = [&](uint32_t o) { return ctx->objActiveCount[o] > 0; };
+  const size_t primCount = ctx->primCount;
+  const float motion = clamp_unit(prm->camera_motion), pressure = clamp_unit(prm->memory_pressure);
+  const float targetFraction = std::min(std::max(prm->target_fraction + 0.08f * motion - 0.12f * pressure, 0.65f), 0.97f);
+  const size_t budget = std::max<size_t>(
+      1, (size_t)std::llround((double)std::max<uint32_t>(prm->max_toggles, 1) *
+                              (1.0 + 0.55 * (double)motion + 0.35 * (double)pressure)));
+  float screenArea = (float)view.width * (float)view.height;
+  if (screenArea <= 0.0f) screenArea = 1.0f;
+  const float boost = std::max(prm->energy_visibility_boost, 1.0f);
+  const bool applyBoost = boost > 1.0001f;
+  float maxEmit = 0.0f, maxHit = 0.0f, boostedTotal = 0.0f;
+  std::vector<float> imp(N);
+  for (uint32_t o = 0; o < N; ++o) {
+    maxEmit = std::max(maxEmit, R.energyEmit[o]);
+    maxHit = std::max(maxHit, std::max(score[o], 0.0f));
+    if (applyBoost) {
+      const float frac = std::min(std::max(cov[o] / screenArea, 0.0f), 1.0f);
+      imp[o] = R.energyTotal[o] * (1.0f + (boost - 1.0f) * frac);
+      boostedTotal += std::max(imp[o], 0.0f);
+    } else {
+      imp[o] = R.energyTotal[o];
+    }
+  }
+  auto normByMax = [](float v, float m) { return !(m > 0.0f) ? 0.0f : std::min(std::max(v / m, 0.0f), 1.0f); };
+  for (uint32_t o = 0; o < N; ++o) {
+    const float hp = std::min(std::max(post[(size_t)o * kPostWords + 2], 0.0f), 1.0f);
+    const float rh = normByMax(std::max(score[o], 0.0f), maxHit);
+    const float en = normByMax(R.energyEmit[o], maxEmit);
+    const float depthWeight = 1.0f, visibleWeight = inView[o] ? 1.0f : 0.0f;
+    const float transport = 1.0f + 0.90f * hp + 0.55f * rh + 0.40f * depthWeight + 0.45f * visibleWeight + 0.90f * en;
+    imp[o] *= transport;
+  }
+  const float historyWeight = std::min(std::max(prm->energy_smoothing, 0.0f), 0.999f);
+  const float currentWeight = 1.0f - historyWeight;
+  std::vector<float> smoothed(N);
+  for (uint32_t o = 0; o < N; ++o) {
+    float v = imp[o];
+    if (historyWeight > 0.0f) {
+      const float prev = resetHistory ? imp[o] : R.energyHist[o];
+      v = prev * historyWeight + imp[o] * currentWeight;
+    }
+    R.energyHist[o] = v;
+    smoothed[o] = v;
+  }
+  if (applyBoost) {
+    boostedTotal = 0.0f;
+    for (float v : smoothed) boostedTotal += std::max(v, 0.0f);
+  }
+  const float targetBase = applyBoost ? boostedTotal : R.energyPrimTotal;
+  const bool average = prm->energy_use_average != 0;
+  std::vector<float> sel(N, 0.0f);
+  float totalSel = 0.0f;
+  for (uint32_t o = 0; o < N; ++o) {
+    const uint32_t count = ctx->instances[o].primitive_count;
+    float v = smoothed[o];
+    if (average) {
+      if (count == 0) continue;
+      v /= (float)count;
+    }
+    sel[o] = v;
+    totalSel += std::max(v, 0.0f);
+  }
+  std::vector<uint32_t> order(N);
+  std::iota(order.begin(), order.end(), 0u);
+  std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+    const float sa = sanitize(sel[a]), sb = sanitize(sel[b]);
+    if (sa == sb) return a < b;
+    return sa > sb;
+  });
+  const size_t minActive = std::min<size_t>(primCount, prm->min_active);
+  std::vector<uint8_t> desired(N, 0);
+  size_t enabled = 0;
+  if (R.energyPrimTotal <= 0.0f) {
+    for (uint32_t idx : order) {
+      const uint32_t count = ctx->instances[idx].primitive_count;
+      if (count == 0) continue;
+      desired[idx] = 1;
+      enabled += count;
+      if (enabled >= minActive) break;
+    }
+  } else {
+    float cumulative = 0.0f;
+    const float target = (totalSel > 0.0f ? totalSel : targetBase) * targetFraction;
+    for (uint32_t idx : order) {
+      const uint32_t count = ctx->instances[idx].primitive_count;
+      if (count == 0 && sel[idx] <= 0.0f) continue;
+      desired[idx] = 1;
+      enabled += count;
+      cumulative += std::max(sel[idx], 0.0f);
+      if (enabled >= minActive && cumulative >= target) break;
+    }
+  }
+  if (enabled < minActive)
+    for (uint32_t idx : order) {
+      if (desired[idx]) continue;
+      const uint32_t count = ctx->instances[idx].primitive_count;
+      if (count == 0) continue;
+      desired[idx] = 1;
+      enabled += count;
+      if (enabled >= minActive) break;
+    }
+  size_t toggledPrims = 0;
+  const uint32_t minDuration = prm->state_cooldown;
+  auto attempt = [&](uint32_t o, bool want, uint32_t &n) -> nomad_status {
+    n = 0;
+    if (want == active(o)) return NOMAD_OK;
+    if (R.objCooldown[o] > 0) return NOMAD_OK;
+    if (minDuration > 0 && R.lastToggle[o] != 0 && frameNo >= R.lastToggle[o] && frameNo - R.lastToggle[o] < minDuration)
+      return NOMAD_OK;
+    const uint32_t count = ctx->instances[o].primitive_count;
+    const size_t needed = want ? count - ctx->objActiveCount[o] : ctx->objActiveCount[o];
+    if (needed == 0) return NOMAD_OK;
+    if (toggledPrims >= budget) return NOMAD_OK;
+    const bool prevState = active(o);
+    nomad_status r = nomad_residency_set_object_active(ctx, o, want ? 1 : 0, &n);
+    if (r != NOMAD_OK) return r;
+    const bool newState = active(o);
+    if (prevState != newState) R.lastToggle[o] = frameNo;
+    if (n > 0 || prevState != newState || !newState) R.objCooldown[o] = prm->state_cooldown;
+    if (n > 0) toggledPrims = std::min(toggledPrims + n, budget);
+    return NOMAD_OK;
+  };
+  for (uint32_t o = 0; o < N; ++o) {
+    uint32_t n = 0;
+    st = attempt(o, desired[o] != 0, n);
+    if (st != NOMAD_OK) return st;
+  }
+  bool anyActive = false;
+  for (uint32_t o = 0; o < N && !anyActive; ++o) anyActive = ctx->instances[o].primitive_count > 0 && active(o);
+  if (!anyActive)
+    for (uint32_t idx : order) {
+      if (ctx->instances[idx].primitive_count == 0) continue;
+      uint32_t n = 0;
+      st = attempt(idx, true, n);
+      if (st != NOMAD_OK) return st;
+      if (n > 0) {
+        anyActive = true;
+        break;
+      }
+    }
+  if (!anyActive) {
+    uint32_t fb = N;
+    for (uint32_t idx : order)
+      if (ctx->instances[idx].primitive_count > 0) {
+        fb = idx;
+        break;
+      }
+    if (fb < N) {
+      uint32_t n = 0;
+      st = attempt(fb, true, n);
+      if (st != NOMAD_OK) return st;
+    } else if (ctx->primCount > 0) {
+      int32_t changed = 0;
+      st = nomad_residency_set_primitive_active(ctx, 0, 1, &changed);
+      if (st != NOMAD_OK) return st;
+    }
+  }
+  st = nomad_residency_flush(ctx);
+  if (st != NOMAD_OK) return st;
+  *toggled = (uint32_t)toggledPrims;
+  return NOMAD_OK;
+}
+
 }  // namespace
 
 extern "C" nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residency_params *prm,
@@ -1891,6 +2152,10 @@ extern "C" nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residen
   if (prm->policy == NOMAD_POLICY_PROBABILISTIC) {
     NOMAD_DEVICE_SCOPE(ctx);
     return probabilistic_step(ctx, prm, *camera, toggled);
+  }
+  if (prm->policy == NOMAD_POLICY_ENERGY) {
+    NOMAD_DEVICE_SCOPE(ctx);
+    return energy_step(ctx, prm, *camera, toggled);
   }
   if (prm->policy == NOMAD_POLICY_ENVIRONMENT_HIT || prm->policy == NOMAD_POLICY_PREDICTIVE) {
     NOMAD_DEVICE_SCOPE(ctx);

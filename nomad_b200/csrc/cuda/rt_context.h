@@ -170,6 +170,11 @@ struct nomad_ctx {
     std::vector<uint32_t> probOrder;  // also the order of the environment policies
     // EnvironmentHit: render statistics at the previous step (segments, escapes)
     uint64_t prevSegments = 0, prevEscapes = 0;
+    // EnergyImportance: last residency change per object (step number), smoothed importance,
+    // static per-object importance and emitted power, the scene's total primitive importance
+    std::vector<uint32_t> lastToggle;
+    std::vector<float> energyHist, energyTotal, energyEmit;
+    float energyPrimTotal = 0.0f;
     // DistanceLOD policy (NOMAD_POLICY_DISTANCE_LOD): object cooldowns and the last step's tests
     bool lodOn = false;
     std::vector<uint32_t> objCooldown;
