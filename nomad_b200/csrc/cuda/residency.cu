@@ -1900,6 +1900,7 @@ nomad_status energy_step(nomad_ctx *ctx, const nomad_residency_params *prm, cons
   if (R.lodDist.size() != N) R.lodDist.assign(N, 0.0f);
   if (R.lodFlags.size() != N) R.lodFlags.assign(N, 0);
   if (R.lastToggle.size() != N) R.lastToggle.assign(N, 0);
+  R.lodOn = true;  // nomad_residency_object_state reports this step's coverage and frustum flags
   bool resetHistory = false;
   if (R.energyHist.size() != N) {
     R.energyHist.assign(N, 0.0f);

@@ -1022,3 +1022,194 @@ class EnvironmentOracle:
                 if set_object(idx, True) > 0:
                     break
         return active, toggled
+
+
+def energy_static(sb):
+    """Per-object summed primitive importance (primitiveImportance, Renderer.cpp:1482-1490) and
+    emitted power times area, in primitive order, and the scene's total primitive importance,
+    float32 as the library sums them."""
+    f = np.float32
+    g = sb.prims.reshape(-1, 28).astype(f)
+    m = sb.materials.reshape(-1, 20).astype(f)
+    t = g[:, 3].astype(np.int32)
+
+    def lum(c):
+        return (f(0.2126) * c[:, 0] + f(0.7152) * c[:, 1]) + f(0.0722) * c[:, 2]
+
+    a = np.where((t == 1)[:, None], g[:, 4:7] - g[:, 0:3], g[:, 4:7]).astype(f)
+    b = np.where((t == 1)[:, None], g[:, 8:11] - g[:, 0:3], g[:, 8:11]).astype(f)
+    cx = a[:, 1] * b[:, 2] - a[:, 2] * b[:, 1]
+    cy = a[:, 2] * b[:, 0] - a[:, 0] * b[:, 2]
+    cz = a[:, 0] * b[:, 1] - a[:, 1] * b[:, 0]
+    ln = np.sqrt((cx * cx + cy * cy) + cz * cz)
+    area = np.where(t == 1, f(0.5) * ln, f(4.0) * ln).astype(f)
+    area = np.where(t == 0, f(4.0) * f(np.pi) * g[:, 4] * g[:, 4], area).astype(f)
+    emissive = m[:, 11] * lum(m[:, 8:11])
+    op = m[:, 3]
+    imp = (np.maximum(area, f(1e-4)) * (((emissive + lum(m[:, 0:3]) * op) + lum(m[:, 4:7]) * op) +
+                                        (f(1) - op) * lum(m[:, 12:15]))).astype(f)
+    emit = np.maximum(emissive * area, f(0)).astype(f)
+    n = sb.object_count
+    total, emit_o = np.zeros(n, f), np.zeros(n, f)
+    inst = sb.instances
+    for o in range(n):
+        b0, c = int(inst["primitive_base"][o]), int(inst["primitive_count"][o])
+        if c:
+            total[o] = np.cumsum(np.maximum(imp[b0:b0 + c], f(0)), dtype=f)[-1]
+            emit_o[o] = np.cumsum(emit[b0:b0 + c], dtype=f)[-1]
+    return total, emit_o, np.cumsum(np.maximum(imp, f(0)), dtype=f)[-1]
+
+
+class EnergyOracle:
+    """updateEnergyImportance's object path without mesh groups (RendererResidency.cpp:1462-1860)
+    in numpy float32, over the posterior, ray-hit score and screen coverage of the same step."""
+
+    def __init__(self, sb):
+        self.total, self.emit, self.prim_total = energy_static(sb)
+        self.counts = sb.instances["primitive_count"].astype(np.int64)
+        n = len(self.counts)
+        self.hist = None
+        self.cooldown = np.zeros(n, np.int64)
+        self.last_toggle = np.zeros(n, np.int64)
+
+    def decrement_cooldowns(self):
+        self.cooldown = np.maximum(self.cooldown - 1, 0)
+
+    def step(self, post, score, coverage, in_view, active, frame_no, width, height, target_fraction=0.88,
+             min_active=16, max_toggles=32, camera_motion=0.0, memory_pressure=0.0, boost=1.75, smoothing=0.85,
+             use_average=True, state_cooldown=5):
+        import math
+
+        f = np.float32
+        n = len(self.counts)
+        active = np.asarray(active, bool).copy()
+        inv = np.asarray(in_view, bool)
+        prim_count = int(self.counts.sum())
+
+        def cl(v, lo=0.0, hi=1.0):
+            return min(max(f(v), f(lo)), f(hi))
+
+        motion, pressure = cl(camera_motion), cl(memory_pressure)
+        tf = cl(f(target_fraction) + f(0.08) * motion - f(0.12) * pressure, 0.65, 0.97)
+        budget = max(1, int(math.floor(max(int(max_toggles), 1) * (1.0 + 0.55 * float(motion) +
+                                                                   0.35 * float(pressure)) + 0.5)))
+        screen = f(width) * f(height)
+        if screen <= 0:
+            screen = f(1)
+        bst = max(f(boost), f(1))
+        apply_boost = bst > f(1.0001)
+        max_emit = f(0)
+        max_hit = f(0)
+        imp = np.zeros(n, f)
+        for o in range(n):
+            max_emit = max(max_emit, self.emit[o])
+            max_hit = max(max_hit, max(f(score[o]), f(0)))
+            if apply_boost:
+                frac = cl(f(coverage[o]) / screen)
+                imp[o] = self.total[o] * (f(1) + (bst - f(1)) * frac)
+            else:
+                imp[o] = self.total[o]
+
+        def norm(v, m):
+            return f(0) if not (m > 0) else cl(f(v) / m)
+
+        for o in range(n):
+            hp = cl(post.probability[o])
+            rh = norm(max(f(score[o]), f(0)), max_hit)
+            en = norm(self.emit[o], max_emit)
+            vw = f(1) if inv[o] else f(0)
+            tr = ((((f(1) + f(0.90) * hp) + f(0.55) * rh) + f(0.40) * f(1)) + f(0.45) * vw) + f(0.90) * en
+            imp[o] = imp[o] * tr
+        hw = min(max(f(smoothing), f(0)), f(0.999))
+        cw = f(1) - hw
+        reset = self.hist is None
+        if reset:
+            self.hist = np.zeros(n, f)
+        smoothed = np.zeros(n, f)
+        for o in range(n):
+            v = imp[o]
+            if hw > 0:
+                prev = imp[o] if reset else self.hist[o]
+                v = prev * hw + imp[o] * cw
+            self.hist[o] = v
+            smoothed[o] = v
+        boosted_total = f(0)
+        if apply_boost:
+            for v in smoothed:
+                boosted_total = boosted_total + max(v, f(0))
+        base = boosted_total if apply_boost else self.prim_total
+        sel = np.zeros(n, f)
+        total_sel = f(0)
+        for o in range(n):
+            v = smoothed[o]
+            if use_average:
+                if self.counts[o] == 0:
+                    continue
+                v = v / f(self.counts[o])
+            sel[o] = v
+            total_sel = total_sel + max(v, f(0))
+        order = sorted(range(n), key=lambda o: (-_sanitize(sel[o]), o))
+        min_act = min(prim_count, int(min_active))
+        desired = np.zeros(n, bool)
+        enabled = 0
+        if self.prim_total <= 0:
+            for idx in order:
+                if self.counts[idx] == 0:
+                    continue
+                desired[idx] = True
+                enabled += int(self.counts[idx])
+                if enabled >= min_act:
+                    break
+        else:
+            cum = f(0)
+            target = (total_sel if total_sel > 0 else base) * tf
+            for idx in order:
+                c = int(self.counts[idx])
+                if c == 0 and sel[idx] <= 0:
+                    continue
+                desired[idx] = True
+                enabled += c
+                cum = cum + max(sel[idx], f(0))
+                if enabled >= min_act and cum >= target:
+                    break
+        if enabled < min_act:
+            for idx in order:
+                if desired[idx] or self.counts[idx] == 0:
+                    continue
+                desired[idx] = True
+                enabled += int(self.counts[idx])
+                if enabled >= min_act:
+                    break
+        toggled = 0
+
+        def attempt(o, want):
+            nonlocal toggled
+            if want == bool(active[o]):
+                return 0
+            if self.cooldown[o] > 0:
+                return 0
+            last = self.last_toggle[o]
+            if state_cooldown > 0 and last != 0 and frame_no >= last and frame_no - last < state_cooldown:
+                return 0
+            if self.counts[o] == 0:
+                return 0
+            if toggled >= budget:
+                return 0
+            prev = bool(active[o])
+            t = int(self.counts[o])
+            active[o] = want
+            if prev != bool(active[o]):
+                self.last_toggle[o] = frame_no
+            self.cooldown[o] = state_cooldown
+            toggled = min(toggled + t, budget)
+            return t
+
+        for o in range(n):
+            attempt(o, bool(desired[o]))
+        if not any(active[o] and self.counts[o] > 0 for o in range(n)):
+            for idx in order:
+                if self.counts[idx] == 0:
+                    continue
+                if attempt(idx, True) > 0:
+                    break
+        return active, toggled

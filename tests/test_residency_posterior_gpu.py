@@ -183,3 +183,39 @@ def test_environment_policies_match_oracle(nb, orc, ctx, small_city, predictive)
         changed += int((got != active).sum())
         active = got
     assert changed > 0 and ctx.status() == 0
+
+
+def test_energy_policy_matches_oracle(nb, orc, ctx, small_city):
+    """updateEnergyImportance over a moving camera against its numpy restatement, fed the device's
+    posterior and the step's screen coverage (checked against a float64 restatement)."""
+    from oracle import residency as ores
+
+    _, sb = small_city
+    ctx.upload(sb)
+    N = sb.object_count
+    kw = dict(target_fraction=0.7, min_active=16, max_toggles=6000, camera_motion=0.3, state_cooldown=3)
+    prm = nb.ResidencyParams.make(nb.POLICY_ENERGY, **kw)
+    post = ores.ObjectPosterior(N)
+    pol = ores.EnergyOracle(sb)
+    spheres = ores.object_spheres(sb)
+    score = np.zeros(N, np.float32)
+    active = ctx.residency_flags().astype(bool)
+    changed = 0
+    for frame in range(12):
+        view = _orbit(nb, frame)
+        ctx.render(view, count_hits=True)
+        pol.decrement_cooldowns()
+        ctx.residency_step(prm, view, toggles=True)
+        dev = ctx.residency_posterior()
+        feats, _ = ctx.residency_last()
+        post.step(dev["hits"], dev["tests"], feats[:, 2] > 0.5, active)
+        score = (score * np.float32(0.85) + dev["hits"].astype(np.float32)).astype(np.float32)
+        cov, in_view, _ = ctx.residency_object_state()
+        c64, margin = ores.coverage_f64(spheres, view)
+        assert ((np.abs(cov.astype(np.float64) - c64) <= 1e-3 * np.maximum(1.0, c64)) | (margin < 1e-4)).all(), frame
+        want, _ = pol.step(post, score, cov, in_view.astype(bool), active, frame + 1, 96, 54, **kw)
+        got = ctx.residency_flags().astype(bool)
+        assert np.array_equal(got, want), (frame, np.nonzero(got != want)[0][:10])
+        changed += int((got != active).sum())
+        active = got
+    assert changed > 0 and ctx.status() == 0
