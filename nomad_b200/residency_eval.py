@@ -5,14 +5,20 @@ Workload (the learned-residency configuration): a city of 2,048 objects (~6M tri
 frame renders the view with the current resident set (per-object hit counting on), then runs
 one residency step. The image judge is the same frame rendered with every object resident
 (a second context, same Philox streams), compared in HDR:
-rel-MSE = mean((I - I_AR)^2) / mean(I_AR^2), averaged over the frames whose reference is not
-black (also reported: its median, and the energy-weighted sum(num) / sum(den) over the path, which
-near-black reference frames cannot dominate).
+the headline error is the energy-weighted rel-MSE sum_f sum_px (I - I_AR)^2 / sum_f sum_px I_AR^2
+over the path, which near-black reference frames cannot dominate (also reported: the per-frame
+rel-MSE mean((I - I_AR)^2) / mean(I_AR^2), averaged over the frames whose reference is not black,
+and its median). ms/frame is device time: CUDA events recorded on the stream the context runs on,
+around the frame's render, residency step and (when paging) streaming update; each policy's path is
+run `repeats` times and reported as the mean with its spread (min, max of the per-run means).
 
 The learned scorer is trained on the device on hit counts recorded along seeded training camera
 paths rendered with every object resident: features of frame f, target log1p(hits of frame
 f+1). To cover what the policy sees once it evicts objects (no hits, decaying history), a copy
-of every sample has its hit-history features replaced by the evicted pattern.
+of every sample has its hit-history features replaced by the evicted pattern. The cost-aware
+scorer is the same network trained on hits per byte, log1p(hits(f+1) * mean_kib / kib): its
+key orders objects by image contribution per byte of geometry, the greedy rule for filling a
+byte budget, so at equal image impact it prefers cheap geometry.
 """
 from __future__ import annotations
 
@@ -23,6 +29,9 @@ import numpy as np
 from . import native as nat
 
 HIST_FEATURES = list(range(3, 12)) + [19, 20]
+# the reference's host-side heuristics, which toggle through the residency interface
+HOST_POLICIES = (nat.POLICY_RAYHIT_PRIM, nat.POLICY_DISTANCE_LOD, nat.POLICY_SCREEN_SPACE,
+                 nat.POLICY_PROBABILISTIC, nat.POLICY_ENVIRONMENT_HIT, nat.POLICY_PREDICTIVE, nat.POLICY_ENERGY)
 
 
 def catmull_rom(points: np.ndarray, n: int) -> np.ndarray:
@@ -61,6 +70,49 @@ def camera_path(seed: int, frames: int, extent_x: float, extent_z: float, contro
 def make_view(pos, look, width, height, spp, depth, seed, frame):
     return nat.view_pinhole(pos, look, width=width, height=height, spp=spp, max_depth=depth,
                             seed=seed, frame=frame)
+
+
+class FrameClock:
+    """Device time of a frame: the context runs on a stream of its own, and CUDA events recorded
+    on that stream bracket the frame's work (host-side policy steps included, since the end event
+    is recorded after they have queued their last copy)."""
+
+    def __init__(self, ctx):
+        import torch
+
+        self.ctx = ctx
+        self.stream = torch.cuda.Stream()
+        ctx.set_stream(self.stream.cuda_stream)
+        self.e0 = torch.cuda.Event(enable_timing=True)
+        self.e1 = torch.cuda.Event(enable_timing=True)
+
+    def start(self):
+        self.e0.record(self.stream)
+
+    def stop(self) -> float:
+        self.e1.record(self.stream)
+        self.e1.synchronize()
+        return self.e0.elapsed_time(self.e1)
+
+    def close(self):
+        self.ctx.set_stream(0)
+
+
+def spread(runs, key):
+    vals = [r[key] for r in runs]
+    return {"mean": float(np.mean(vals)), "min": float(np.min(vals)), "max": float(np.max(vals)), "runs": vals}
+
+
+def repeat(fn, repeats):
+    """Runs fn() `repeats` times; the first run's record with ms_per_frame replaced by its mean
+    and spread over the runs."""
+    runs = [fn() for _ in range(repeats)]
+    out = dict(runs[0])
+    out["ms_per_frame"] = spread(runs, "ms_per_frame")["mean"]
+    out["ms_per_frame_spread"] = spread(runs, "ms_per_frame")
+    out["rel_mse_energy_runs"] = [r["rel_mse_energy"] for r in runs]
+    out["repeats"] = repeats
+    return out
 
 
 class Workload:
@@ -125,6 +177,14 @@ class Workload:
         xe[:, 18] = 0.0
         return np.concatenate([x, xe]), np.concatenate([t, t])
 
+    @staticmethod
+    def cost_targets(x, t):
+        """Hits per byte: log1p(hits * mean_kib / kib), the object's KiB read back from its
+        geometry-size feature log1p(kib)."""
+        kib = np.expm1(x[:, 13].astype(np.float64))
+        kib = np.maximum(kib, 1e-3)
+        return np.log1p(np.expm1(t.astype(np.float64)) * kib.mean() / kib).astype(np.float32)
+
     def train(self, ctx, x, t, steps=1500, batch=4096, lr=2e-3, seed=5):
         ctx.mlp_init(seed)
         return ctx.mlp_train(x, t, steps=steps, batch=batch, lr=lr, weight_decay=1e-4, seed=seed)
@@ -141,34 +201,37 @@ class Workload:
         if prm is None:
             prm = nat.ResidencyParams.make(policy, budget_bytes=budget if policy != nat.POLICY_ALWAYS else 0,
                                            camera_motion=0.3, min_active=0)
-        # start from everything resident, as the reference's AlwaysResident warm-up does
-        ctx.residency_step(nat.ResidencyParams.make(nat.POLICY_ALWAYS), views[0])
-        ctx.reset_object_hits()
         npix = self.width * self.height
         d_img = torch.empty(npix * 3, dtype=torch.float32, device="cuda")
         d_ref = torch.empty(npix * 3, dtype=torch.float32, device="cuda")
         mse, ms, resident_bytes = [], [], []
         sum_num = sum_den = 0.0
-        for f, v in enumerate(views):
-            judge.render_dev(v, d_ref.data_ptr())
-            judge.sync()
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            ctx.render_dev(v, d_img.data_ptr(), count_hits=True)
-            ctx.residency_step(prm, v, toggles=prm.policy in (nat.POLICY_RAYHIT_PRIM, nat.POLICY_DISTANCE_LOD,
-                                                             nat.POLICY_SCREEN_SPACE))
-            ctx.sync()
-            dt = time.perf_counter() - t0
-            num = torch.mean((d_img - d_ref) ** 2).item()
-            den = torch.mean(d_ref ** 2).item()
-            if f >= warm:
-                if den > 0:  # a black reference frame (camera inside geometry) has no relative error
-                    mse.append(num / den)
-                sum_num += num
-                sum_den += den
-                ms.append(dt * 1e3)
-                flags = ctx.residency_flags().astype(bool)
-                resident_bytes.append(int(nbytes[flags].sum()))
+        # host-side policies step synchronously (the toggles come back to the host)
+        host_step = prm.policy in HOST_POLICIES
+        clock = FrameClock(ctx)
+        try:
+            # start from everything resident, as the reference's AlwaysResident warm-up does
+            ctx.residency_step(nat.ResidencyParams.make(nat.POLICY_ALWAYS), views[0])
+            ctx.reset_object_hits()
+            for f, v in enumerate(views):
+                judge.render_dev(v, d_ref.data_ptr())
+                judge.sync()
+                clock.start()
+                ctx.render_dev(v, d_img.data_ptr(), count_hits=True)
+                ctx.residency_step(prm, v, toggles=host_step)
+                dt = clock.stop()
+                num = torch.mean((d_img - d_ref) ** 2).item()
+                den = torch.mean(d_ref ** 2).item()
+                if f >= warm:
+                    if den > 0:  # a black reference frame (camera inside geometry) has no relative error
+                        mse.append(num / den)
+                    sum_num += num
+                    sum_den += den
+                    ms.append(dt)
+                    flags = ctx.residency_flags().astype(bool)
+                    resident_bytes.append(int(nbytes[flags].sum()))
+        finally:
+            clock.close()
         return {"rel_mse": float(np.mean(mse)), "rel_mse_p50": float(np.median(mse)),
                 "rel_mse_energy": sum_num / sum_den if sum_den > 0 else None,
                 "ms_per_frame": float(np.mean(ms)),
@@ -177,12 +240,14 @@ class Workload:
                 "frames": len(mse)}
 
 
-    def evaluate_paged(self, ctx, judge, policy, path_seed=1, frames=None, warm=5, pool_slack=1.25):
+    def evaluate_paged(self, ctx, judge, policy, path_seed=1, frames=None, warm=5, pool_slack=1.25,
+                       budget_fraction=None, mlp=None):
         """The same run with geometry paging: a third context whose BLAS nodes (of the tuned
         traversal width) and triangle records live in a device pool of pool_slack x the budget's
         share of the paged bytes, streamed in by nomad_paging_update after every residency step
         (at most 32 onloads per frame). ms/frame includes the update; rel-MSE includes the frames
-        where wanted objects are still streaming."""
+        where wanted objects are still streaming. The scorer is ctx's unless mlp (a weight blob)
+        is given."""
         import torch
 
         frames = frames or self.frames
@@ -196,29 +261,29 @@ class Workload:
         pc = self.context()
         try:
             pc.set_traversal(**trav)
-            pc.mlp_set(ctx.mlp_get())
-            pool = int(min(full, full * self.budget_fraction * pool_slack))
+            pc.mlp_set(ctx.mlp_get() if mlp is None else mlp)
+            frac = budget_fraction or self.budget_fraction
+            pool = int(min(full, full * frac * pool_slack))
             pc.paging_enable(pool, width=trav["width"])
             nbytes = pc.object_bytes()
-            budget = int(self.budget_fraction * nbytes.sum())
+            budget = int(frac * nbytes.sum())
             prm = nat.ResidencyParams.make(policy, budget_bytes=budget, camera_motion=0.3, min_active=0)
-            pc.reset_object_hits()
             npix = self.width * self.height
             d_img = torch.empty(npix * 3, dtype=torch.float32, device="cuda")
             d_ref = torch.empty(npix * 3, dtype=torch.float32, device="cuda")
             mse, ms, streamed, onl = [], [], [], []
             sum_num = sum_den = 0.0
+            clock = FrameClock(pc)  # paging work must run on the context's stream: this one
+            pc.reset_object_hits()
             prev = pc.paging_stats()
             for f, v in enumerate(views):
                 judge.render_dev(v, d_ref.data_ptr())
                 judge.sync()
-                torch.cuda.synchronize()
-                t0 = time.perf_counter()
+                clock.start()
                 pc.render_dev(v, d_img.data_ptr(), count_hits=True)
                 pc.residency_step(prm, v, toggles=False)
                 pc.paging_update()
-                pc.sync()
-                dt = time.perf_counter() - t0
+                dt = clock.stop()
                 num = torch.mean((d_img - d_ref) ** 2).item()
                 den = torch.mean(d_ref ** 2).item()
                 st = pc.paging_stats()
@@ -226,10 +291,11 @@ class Workload:
                     mse.append(num / den if den > 0 else None)
                     sum_num += num
                     sum_den += den
-                    ms.append(dt * 1e3)
+                    ms.append(dt)
                     streamed.append(st["bytes_streamed"] - prev["bytes_streamed"])
                     onl.append(st["onloads"] - prev["onloads"])
                 prev = st
+            clock.close()
             st = pc.paging_stats()
             late = [m for m in mse[max(0, 40 - warm):] if m is not None]
             mse = [m for m in mse if m is not None]
@@ -248,8 +314,9 @@ class Workload:
             pc.close()
 
 
-def run(paths=200, frames_per_path=8, steps=1500, frames=300, log=print):
-    """Full comparison; returns a dict for the bench line."""
+def run(paths=200, frames_per_path=8, steps=1500, frames=300, repeats=3, log=print):
+    """Full comparison; returns a dict for the bench line. The headline error is the
+    energy-weighted rel-MSE; ms/frame is device time, the mean of `repeats` runs with its spread."""
     t0 = time.perf_counter()
     w = Workload(frames=frames)
     log(f"residency workload: {w.sb.prim_count} prims, {w.sb.object_count} objects, set-up {w.setup_s:.1f}s")
@@ -260,29 +327,50 @@ def run(paths=200, frames_per_path=8, steps=1500, frames=300, log=print):
     t1 = time.perf_counter()
     x, t = w.record(ctx, paths=paths, frames_per_path=frames_per_path)
     t2 = time.perf_counter()
+    loss_c = w.train(ctx, x, w.cost_targets(x, t), steps=steps)
+    blob_cost = ctx.mlp_get()
     loss = w.train(ctx, x, t, steps=steps)
+    blob_hits = ctx.mlp_get()
     t3 = time.perf_counter()
-    log(f"recorded {x.shape[0]} samples in {t2 - t1:.1f}s, trained {steps} steps in {t3 - t2:.1f}s, "
-        f"loss {loss[:10].mean():.4f} -> {loss[-50:].mean():.4f}")
+    log(f"recorded {x.shape[0]} samples in {t2 - t1:.1f}s, trained 2 x {steps} steps in {t3 - t2:.1f}s, "
+        f"loss {loss[:10].mean():.4f} -> {loss[-50:].mean():.4f} (hits per byte: {loss_c[-50:].mean():.4f})")
     out = {"workload": f"city {w.sb.object_count} objects / {w.sb.prim_count} prims, {frames}-frame path, "
                        f"{w.width}x{w.height} x {w.spp} spp, {w.depth} bounces, budget "
                        f"{int(100 * w.budget_fraction)}% of geometry bytes",
+           "error_metric": "energy-weighted rel-MSE (rel_mse_energy)",
+           "timing": f"CUDA events on the context's stream around render + residency step (+ paging update); "
+                     f"mean of {repeats} runs of the path, spread = min/max of the run means",
            "traversal": traversal,
            "train": {"samples": int(x.shape[0]), "steps": steps, "loss_first": float(loss[:10].mean()),
-                     "loss_last": float(loss[-50:].mean()), "record_s": t2 - t1, "train_s": t3 - t2}}
+                     "loss_last": float(loss[-50:].mean()), "cost_loss_last": float(loss_c[-50:].mean()),
+                     "record_s": t2 - t1, "train_s": t3 - t2}}
+
+    def with_model(blob, fn):
+        ctx.mlp_set(blob)
+        try:
+            return fn()
+        finally:
+            ctx.mlp_set(blob_hits)
+
     for name, pol in (("always_resident", nat.POLICY_ALWAYS), ("ray_hit_budget", nat.POLICY_RAYHIT_BUDGET),
                       ("learned", nat.POLICY_LEARNED)):
-        out[name] = w.evaluate(ctx, judge, pol, frames=frames)
+        out[name] = repeat(lambda: w.evaluate(ctx, judge, pol, frames=frames), repeats)
         log(f"{name}: {out[name]}")
-    for name, pol in (("ray_hit_budget_paged", nat.POLICY_RAYHIT_BUDGET), ("learned_paged", nat.POLICY_LEARNED)):
+    out["learned_cost"] = with_model(blob_cost, lambda: repeat(
+        lambda: w.evaluate(ctx, judge, nat.POLICY_LEARNED, frames=frames), repeats))
+    log(f"learned_cost: {out['learned_cost']}")
+    for name, pol, blob in (("ray_hit_budget_paged", nat.POLICY_RAYHIT_BUDGET, None),
+                            ("learned_paged", nat.POLICY_LEARNED, blob_hits),
+                            ("learned_cost_paged", nat.POLICY_LEARNED, blob_cost)):
         try:
-            out[name] = w.evaluate_paged(ctx, judge, pol, frames=frames)
+            out[name] = repeat(lambda: w.evaluate_paged(ctx, judge, pol, frames=frames, mlp=blob), repeats)
         except nat.NomadError as exc:  # a traversal width the paging cannot hold
             out[name] = {"error": str(exc)}
         log(f"{name}: {out[name]}")
+
     # The reference's host-side heuristics switch objects and primitives through the residency
     # interface, which a later device step does not undo: each runs on a fresh context with the
-    # tuned traversal, so no leg sees another's toggles.
+    # tuned traversal, so no leg sees another's toggles. Each uses the reference's defaults.
     def host_leg(policy, prm, n_frames):
         pc = w.context()
         try:
@@ -291,40 +379,66 @@ def run(paths=200, frames_per_path=8, steps=1500, frames=300, log=print):
         finally:
             pc.close()
 
-    # The reference's own per-primitive ray-hit policy (host, per primitive, its defaults: 54 %
-    # of the primitives, 16 toggles a frame, cooldowns), on a shorter path.
-    out["ray_hit_per_primitive_reference"] = host_leg(
-        nat.POLICY_RAYHIT_PRIM,
-        nat.ResidencyParams.make(nat.POLICY_RAYHIT_PRIM, max_toggles=16, camera_motion=0.3, min_active=16),
-        min(frames, 100))
-    log(f"ray_hit_per_primitive_reference: {out['ray_hit_per_primitive_reference']}")
-    # The reference's DistanceLOD heuristic with its defaults (225 / 275 m, 5 / 12 degrees, 24
-    # toggles a frame), host-side per object.
-    out["distance_lod_reference"] = host_leg(
-        nat.POLICY_DISTANCE_LOD,
-        nat.ResidencyParams.make(nat.POLICY_DISTANCE_LOD, max_toggles=24, camera_motion=0.3), frames)
-    log(f"distance_lod_reference: {out['distance_lod_reference']}")
-    # The reference's ScreenSpaceFootprint heuristic with its defaults (68 % of the screen, 32 px,
-    # 14 primitive toggles a frame), one mesh group per object.
-    out["screen_space_reference"] = host_leg(
-        nat.POLICY_SCREEN_SPACE,
-        nat.ResidencyParams.make(nat.POLICY_SCREEN_SPACE, max_toggles=14, camera_motion=0.3, min_active=16,
-                                 target_fraction=0.68, min_pixel_coverage=32.0), frames)
-    log(f"screen_space_reference: {out['screen_space_reference']}")
-    # The learned policy at smaller budgets: the smallest one whose rel-MSE is within 5 % of the
-    # ray-hit policy's at the full budget, and its ms/frame.
-    sweep = {}
-    for frac in (0.1, 0.15, 0.2, 0.25, 0.3):
-        sweep[f"{frac:.2f}"] = w.evaluate(ctx, judge, nat.POLICY_LEARNED, frames=frames, budget_fraction=frac)
-    out["learned_budget_sweep"] = sweep
-    target = 1.05 * out["ray_hit_budget"]["rel_mse"]
-    ok = [k for k, v in sorted(sweep.items()) if v["rel_mse"] <= target]
-    out["learned_matching_rayhit"] = ({"budget_fraction": float(ok[0]), **sweep[ok[0]],
-                                       "ray_hit_ms_per_frame": out["ray_hit_budget"]["ms_per_frame"]}
-                                      if ok else None)
-    log(f"learned budget sweep: { {k: (v['rel_mse'], v['ms_per_frame']) for k, v in sweep.items()} }")
-    rh, le = out["ray_hit_budget"]["rel_mse"], out["learned"]["rel_mse"]
-    out["learned_vs_rayhit_rel_mse_ratio"] = le / rh if rh > 0 else None
+    P = nat.ResidencyParams.make
+    legs = (
+        # per-primitive ray-hit policy: 54 % of the primitives, 16 toggles a frame, cooldowns
+        ("ray_hit_per_primitive_reference", nat.POLICY_RAYHIT_PRIM,
+         dict(max_toggles=16, min_active=16), min(frames, 100)),
+        # DistanceLOD: 225 / 275 m, 5 / 12 degrees, 24 toggles a frame, per object
+        ("distance_lod_reference", nat.POLICY_DISTANCE_LOD, dict(max_toggles=24), frames),
+        # ScreenSpaceFootprint: 68 % of the screen, 32 px, 14 toggles, one mesh group per object
+        ("screen_space_reference", nat.POLICY_SCREEN_SPACE,
+         dict(max_toggles=14, min_active=16, target_fraction=0.68, min_pixel_coverage=32.0), frames),
+        # Probabilistic: 60 %, 16 minimum, 20 toggles a frame, over the hit posterior
+        ("probabilistic_reference", nat.POLICY_PROBABILISTIC,
+         dict(max_toggles=20, min_active=16, target_fraction=0.60), frames),
+        # EnvironmentHit and Predictive: 25 %, escape threshold 0.4, 20 toggles a frame
+        ("environment_hit_reference", nat.POLICY_ENVIRONMENT_HIT,
+         dict(max_toggles=20, min_active=16, target_fraction=0.25), frames),
+        ("predictive_reference", nat.POLICY_PREDICTIVE,
+         dict(max_toggles=20, min_active=16, target_fraction=0.25), frames),
+        # EnergyImportance: 88 %, 16 minimum, 32 toggles a frame
+        ("energy_importance_reference", nat.POLICY_ENERGY,
+         dict(max_toggles=32, min_active=16, target_fraction=0.88), frames),
+    )
+    for name, pol, kw, n_frames in legs:
+        try:
+            out[name] = host_leg(pol, P(pol, camera_motion=0.3, **kw), n_frames)
+        except nat.NomadError as exc:
+            out[name] = {"error": str(exc)}
+        log(f"{name}: {out[name]}")
+
+    # Smaller budgets for both scorers: the smallest whose energy-weighted rel-MSE is within 5 %
+    # of the ray-hit policy's at the full budget, then that budget paged (which bounds the
+    # device memory by it) against the ray-hit policy paged at the full budget.
+    target = 1.05 * out["ray_hit_budget"]["rel_mse_energy"]
+    for tag, blob in (("learned", blob_hits), ("learned_cost", blob_cost)):
+        sweep = {}
+        for frac in (0.1, 0.15, 0.2, 0.25, 0.3, 0.35):
+            sweep[f"{frac:.2f}"] = with_model(blob, lambda: w.evaluate(ctx, judge, nat.POLICY_LEARNED,
+                                                                      frames=frames, budget_fraction=frac))
+        out[f"{tag}_budget_sweep"] = sweep
+        log(f"{tag} budget sweep: { {k: (v['rel_mse_energy'], v['ms_per_frame']) for k, v in sweep.items()} }")
+        ok = [k for k, v in sorted(sweep.items()) if v["rel_mse_energy"] <= target]
+        if not ok:
+            out[f"{tag}_matching_rayhit"] = None
+            continue
+        frac = float(ok[0])
+        try:
+            paged = repeat(lambda: w.evaluate_paged(ctx, judge, nat.POLICY_LEARNED, frames=frames,
+                                                    budget_fraction=frac, mlp=blob), repeats)
+        except nat.NomadError as exc:
+            paged = {"error": str(exc)}
+        rh = out["ray_hit_budget_paged"]
+        out[f"{tag}_matching_rayhit"] = {
+            "budget_fraction": frac, "unpaged": sweep[ok[0]], "paged": paged,
+            "ray_hit_paged_ms_per_frame_spread": rh.get("ms_per_frame_spread"),
+            "faster_outside_spread": bool("ms_per_frame_spread" in paged and "ms_per_frame_spread" in rh and
+                                          paged["ms_per_frame_spread"]["max"] < rh["ms_per_frame_spread"]["min"])}
+        log(f"{tag} matching ray-hit at {frac}: {out[f'{tag}_matching_rayhit']}")
+    rh, le = out["ray_hit_budget"]["rel_mse_energy"], out["learned"]["rel_mse_energy"]
+    out["learned_vs_rayhit_energy_rel_mse_ratio"] = le / rh if rh else None
+    out["learned_cost_vs_rayhit_energy_rel_mse_ratio"] = out["learned_cost"]["rel_mse_energy"] / rh if rh else None
     out["total_s"] = time.perf_counter() - t0
     ctx.close()
     judge.close()
@@ -337,5 +451,6 @@ if __name__ == "__main__":
 
     args = dict(a.split("=") for a in sys.argv[1:])
     res = run(paths=int(args.get("paths", 200)), frames_per_path=int(args.get("fpp", 8)),
-              steps=int(args.get("steps", 1500)), frames=int(args.get("frames", 300)))
+              steps=int(args.get("steps", 1500)), frames=int(args.get("frames", 300)),
+              repeats=int(args.get("repeats", 3)))
     print(json.dumps(res))
