@@ -117,21 +117,25 @@ class ClockSampler:
 
 
 TRAFFIC_PROFILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles",
-                               "launches_bench_city1080_bvh4_persist_mb10.md")
+                               "k_trace_dram_profile_case_bvh4_persist_mb10.md")
 
 
-def measured_traffic():
-    """Per-launch DRAM bytes (read + write) of the primary and bounce launches, as measured by ncu
-    on this workload and recorded in the profile summary; None when the summary is absent."""
+def measured_traffic(rays):
+    """Per-launch DRAM bytes (read + write) of the primary and bounce launches: the DRAM bytes per
+    ray that one ncu capture of the two k_trace launches of `--profile-case` measured (recorded in
+    the profile summary), times this step's rays per launch (`rays`: {"primary": n, "bounce": n}).
+    None when the summary is absent."""
     try:
         vals = {}
         with open(TRAFFIC_PROFILE) as f:
             for line in f:
                 for key in ("primary", "bounce"):
-                    tag = f"traffic_{key}_bytes:"
+                    tag = f"traffic_{key}_bytes_per_ray:"
                     if line.strip().startswith(tag):
-                        vals[key] = int(line.strip()[len(tag):].strip().strip("`"))
-        return vals if len(vals) == 2 else None
+                        vals[key] = float(line.strip()[len(tag):].strip().strip("`"))
+        if len(vals) != 2:
+            return None
+        return {k: int(round(vals[k] * rays[k])) for k in vals}
     except OSError:
         return None
 
@@ -376,8 +380,12 @@ def residency_leg():
 
 
 def run_profile_case(args):
-    """960x540 primary rays of the city camera plus their diffuse bounces (834,959 rays), traced
-    three times as one batch with the chosen traversal variant; checks the hits agree."""
+    """The bench workload at a quarter of the pixels, for ncu captures: the city, 960x540 x 4
+    jittered primary rays (2,073,600, the bench's density of rays per pixel and seeds) and one
+    diffuse bounce per primary hit, all on the device. k_trace launches: one to make the
+    primary hits the bounces start from, then three iterations of (primary launch, bounce
+    launch) with the chosen variant; the hits must agree across iterations. Capturing
+    `-k regex:k_trace -s 3 -c 2` takes the second iteration's primary and bounce launches."""
     import torch
 
     import nomad_b200 as nb
@@ -386,24 +394,30 @@ def run_profile_case(args):
     sb = nb.SceneBVH(scene)
     ctx = nb.Context(0)
     ctx.upload(sb)
-    cam = nb.city_camera(960, 540)
-    prim = cam.primary_rays(1, seed=5)
-    ph = ctx.trace_closest(prim)
-    rays = np.concatenate([prim, nb.bounce_rays(prim, ph, sb.prims, seed=6)])
     select_kernel(ctx, args.kernel or 4, args.min_blocks)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
-    d = torch.from_numpy(rays.view(np.float32).reshape(-1, 8)).cuda()
-    h = torch.empty((rays.shape[0], 5), dtype=torch.int32, device="cuda")
+    cam = nb.city_camera(WIDTH // 2, HEIGHT // 2)
+    prim = cam.primary_rays(SPP, seed=SEED + 10)
+    d_p = torch.from_numpy(prim.view(np.float32).reshape(-1, 8)).cuda()
+    h_p = torch.empty((prim.shape[0], 5), dtype=torch.int32, device="cuda")
+    ctx.trace_closest_dev(d_p.data_ptr(), prim.shape[0], h_p.data_ptr())
+    torch.cuda.synchronize()
+    ph = h_p.cpu().numpy().view(nb.HIT_DTYPE).reshape(-1)
+    bounce = nb.bounce_rays(prim, ph, sb.prims, seed=SEED + 11)
+    d_b = torch.from_numpy(bounce.view(np.float32).reshape(-1, 8)).cuda()
+    h_b = torch.empty((bounce.shape[0], 5), dtype=torch.int32, device="cuda")
     outs = []
     for _ in range(3):
-        ctx.trace_closest_dev(d.data_ptr(), rays.shape[0], h.data_ptr())
+        ctx.trace_closest_dev(d_p.data_ptr(), prim.shape[0], h_p.data_ptr())
+        ctx.trace_closest_dev(d_b.data_ptr(), bounce.shape[0], h_b.data_ptr())
         torch.cuda.synchronize()
-        outs.append(h.cpu().numpy())
-    assert all(np.array_equal(o, outs[0]) for o in outs) and ctx.status() == 0
-    print(json.dumps({"profile_case": "city 960x540 primary + bounce", "rays": int(rays.shape[0]),
-                      "kernel": nb.KERNEL_NAMES.get(args.kernel or 4)}))
+        outs.append((h_p.cpu().numpy(), h_b.cpu().numpy()))
+    assert all(np.array_equal(o[0], outs[0][0]) and np.array_equal(o[1], outs[0][1]) for o in outs)
+    assert ctx.status() == 0
+    print(json.dumps({"profile_case": "city 960x540 x 4 spp primary, then bounce", "primary_rays": int(prim.shape[0]),
+                      "bounce_rays": int(bounce.shape[0]), "kernel": nb.KERNEL_NAMES.get(args.kernel or 4)}))
     ctx.close()
 
 
@@ -636,8 +650,8 @@ def main():
     ap.add_argument("--profile-compaction", action="store_true",
                     help="run only the device residency compaction of the city (for ncu)")
     ap.add_argument("--profile-case", action="store_true",
-                    help="small case for ncu captures: the city, 960x540 primary rays and their bounces in "
-                         "one batch, one warm-up and two timed launches of the chosen kernel (--kernel)")
+                    help="small case for ncu captures: the city, 960x540 x 4 spp primary rays and their "
+                         "bounces as separate launches, three iterations of the chosen kernel (--kernel)")
     ap.add_argument("--profile-frame", action="store_true",
                     help="path-traced city frame (1920x1080 x 4 spp, 3 bounces) rendered twice, for launch lists")
     ap.add_argument("--profile-restir", action="store_true",
@@ -792,11 +806,12 @@ def main():
 
     peak, peak_kind = measured_peaks()
     achieved = (bytes_prim + bytes_b) / ((t_prim + t_b) / 1e3) / 1e9
-    traffic = measured_traffic()
+    traffic = measured_traffic({"primary": n_prim, "bounce": n_b})
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak,
                 # DRAM bytes of the step's two launches (primary + bounce), the launches `achieved`
-                # covers; from the ncu capture summarised in profiles/
+                # covers: bytes per ray from a single-kernel ncu capture of the profile case
+                # (profiles/), scaled by this step's rays
                 "traffic": (traffic["primary"] + traffic["bounce"]) if traffic else None,
                 "traffic_per_launch": traffic,
                 "peak_source": peak_kind,

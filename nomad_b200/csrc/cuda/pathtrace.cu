@@ -150,11 +150,9 @@ __device__ __forceinline__ Material decode_material(const float4 *__restrict__ m
 }
 
 // Geometric normal at a hit, as firstHitBVH sets intersection.normal before the front-face flip
-// (triangle :779-806, rectangle :853-863, sphere :766).
-__device__ __forceinline__ V3 hit_normal(const float4 *__restrict__ prims, int32_t prim, V3 p) {
-  const float4 *g = prims + 7ll * prim;
-  float4 p0 = __ldg(g), p1 = __ldg(g + 1), p2 = __ldg(g + 2), p6 = __ldg(g + 6);
-  int type = (int)p0.w;
+// (triangle :779-806, rectangle :853-863, sphere :766). For triangles and rectangles it does not
+// depend on the hit point: surface_normal computes it from the primitive record alone.
+__device__ __forceinline__ V3 surface_normal(int type, float4 p0, float4 p1, float4 p2, float4 p6) {
   V3 sn = ld3(p6);
   if (type == 1) {
     V3 e1 = ld3(p1) - ld3(p0), e2 = ld3(p2) - ld3(p0);
@@ -167,14 +165,46 @@ __device__ __forceinline__ V3 hit_normal(const float4 *__restrict__ prims, int32
     else n = fb;
     if (!finite3(n) || dot(n, n) <= kRayEps) n = fb;
     return n;
-  } else if (type == 2) {
-    V3 fb = cross(ld3(p1), ld3(p2));
-    float fl = dot(fb, fb);
-    fb = (fl > kRayEps && finite3(fb)) ? normalize(fb) : v3(0.0f, 1.0f, 0.0f);
-    float sl = dot(sn, sn);
-    return (sl > kRayEps && finite3(sn)) ? normalize(sn) : fb;
   }
+  V3 fb = cross(ld3(p1), ld3(p2));
+  float fl = dot(fb, fb);
+  fb = (fl > kRayEps && finite3(fb)) ? normalize(fb) : v3(0.0f, 1.0f, 0.0f);
+  float sl = dot(sn, sn);
+  return (sl > kRayEps && finite3(sn)) ? normalize(sn) : fb;
+}
+
+__device__ __forceinline__ V3 hit_normal(const float4 *__restrict__ prims, int32_t prim, V3 p) {
+  const float4 *g = prims + 7ll * prim;
+  float4 p0 = __ldg(g);
+  int type = (int)p0.w;
+  if (type == 1 || type == 2) return surface_normal(type, p0, __ldg(g + 1), __ldg(g + 2), __ldg(g + 6));
   return normalize(p - ld3(p0));
+}
+
+// The compact shading record of a primitive: (normal, bits(material | type << 30)) for
+// triangles and rectangles, (center, bits(material)) for spheres (type 0), whose normal is
+// normalize(p - center) at the hit. 16 bytes gathered per hit instead of the 64 bytes of the
+// primitive record and the 80 of its material.
+constexpr uint32_t kShadeMatMask = 0x3fffffffu;
+
+__device__ __forceinline__ V3 record_normal(float4 rec, V3 p) {
+  return (__float_as_uint(rec.w) >> 30) == 0u ? normalize(p - ld3(rec)) : ld3(rec);
+}
+
+__global__ void k_shade_records(const float4 *__restrict__ prims, const uint32_t *__restrict__ matIdx, uint32_t n,
+                                float4 *__restrict__ out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 *g = prims + 7ll * i;
+  const float4 p0 = g[0];
+  const int type = (int)p0.w;
+  const uint32_t m = matIdx[i] & kShadeMatMask;
+  if (type == 1 || type == 2) {
+    const V3 nn = surface_normal(type, p0, g[1], g[2], g[6]);
+    out[i] = make_float4(nn.x, nn.y, nn.z, __uint_as_float(m | ((uint32_t)type << 30)));
+  } else {
+    out[i] = make_float4(p0.x, p0.y, p0.z, __uint_as_float(m));
+  }
 }
 
 // evaluateDirectLightingBsdf (PathTracing.h:249-293): Lambert + GGX D, Schlick-GGX G, Schlick F.
@@ -315,7 +345,7 @@ __global__ void __launch_bounds__(kPtBlock) k_shade(
     const uint32_t *__restrict__ qIds, const int32_t *__restrict__ hits, float4 *__restrict__ nRays,
     uint32_t *__restrict__ nIds, float4 *__restrict__ sRays, uint32_t *__restrict__ sIds,
     float4 *__restrict__ sContrib, float4 *__restrict__ thr, float4 *__restrict__ rad,
-    const float4 *__restrict__ prims, const float4 *__restrict__ mats, Lights L, Counters *cnt, int cur,
+    const float4 *__restrict__ shadeRec, const float4 *__restrict__ matTable, Lights L, Counters *cnt, int cur,
     uint32_t *__restrict__ objHits, int restirDepth0, uint32_t *__restrict__ primHits) {
   const uint32_t n = cnt->qlen[cur];
   const uint32_t lightCount = L.meta->count;
@@ -357,10 +387,11 @@ __global__ void __launch_bounds__(kPtBlock) k_shade(
         U4 b0 = philox(U4{pixel, sample, depth * 4u + 0u, v.index}, v.k0, v.k1);
         U4 b1 = philox(U4{pixel, sample, depth * 4u + 1u, v.index}, v.k0, v.k1);
         V3 p = v3(o.x + t * d.x, o.y + t * d.y, o.z + t * d.z);
-        V3 nrm = hit_normal(prims, prim, p);
+        const float4 rec = __ldg(shadeRec + prim);
+        V3 nrm = record_normal(rec, p);
         bool front = dot(nrm, d) < 0.0f;
         if (!front) nrm = -nrm;
-        Material m = decode_material(mats, prim, v.lod);
+        Material m = decode_material(matTable, (int32_t)(__float_as_uint(rec.w) & kShadeMatMask), v.lod);
         float4 R = rad[pid];
         if (m.power * luminance(m.emission) > 0.0f) {
           R.x = R.x + tp.x * m.emission.x * m.power;
@@ -532,10 +563,57 @@ __global__ void __launch_bounds__(kPtBlock) k_finalize(const ViewDev *__restrict
 
 }  // namespace
 
-namespace {
-
-
-}  // namespace
+// Builds the compact shading records at scene upload: the distinct 80-byte material records
+// (compared bit for bit) go to a table, each primitive's record holds its table index, and the
+// normal (or sphere center) is computed on the device by the same code the hit path used.
+nomad_status nomad_build_shade_records(nomad_ctx *ctx, const float *materials, uint32_t primCount) {
+  constexpr size_t kWords = 20;
+  std::vector<uint32_t> idx(primCount);
+  std::vector<float> table;
+  {
+    size_t cap = 1024;
+    while (cap < 2ull * primCount) cap <<= 1;
+    std::vector<int32_t> slots(cap, -1);
+    for (uint32_t i = 0; i < primCount; ++i) {
+      const float *m = materials + (size_t)i * kWords;
+      uint32_t w[kWords];
+      std::memcpy(w, m, sizeof(w));
+      uint64_t h = 1469598103934665603ull;
+      for (size_t k = 0; k < kWords; ++k) h = (h ^ w[k]) * 1099511628211ull;
+      size_t at = (size_t)(h ^ (h >> 29)) & (cap - 1);
+      while (true) {
+        const int32_t e = slots[at];
+        if (e < 0) {
+          slots[at] = (int32_t)(table.size() / kWords);
+          idx[i] = (uint32_t)slots[at];
+          table.insert(table.end(), m, m + kWords);
+          break;
+        }
+        if (std::memcmp(&table[(size_t)e * kWords], m, sizeof(w)) == 0) {
+          idx[i] = (uint32_t)e;
+          break;
+        }
+        at = (at + 1) & (cap - 1);
+      }
+    }
+  }
+  const uint32_t count = (uint32_t)(table.size() / kWords);
+  if (count > kShadeMatMask) return nomad_fail(ctx, NOMAD_ERR_LIMIT, "more than 2^30 distinct materials");
+  ctx->matCount = count;
+  NOMAD_CUDA(ctx, ctx->matTable.reserve(std::max<size_t>(table.size() * 4, 80)));
+  NOMAD_CUDA(ctx, ctx->shadeRec.reserve(std::max<size_t>((size_t)primCount * 16, 16)));
+  if (primCount == 0) return NOMAD_OK;
+  NOMAD_CUDA(ctx, cudaMemcpy(ctx->matTable.p, table.data(), table.size() * 4, cudaMemcpyHostToDevice));
+  DeviceBuf d;
+  NOMAD_CUDA(ctx, d.reserve((size_t)primCount * 4));
+  NOMAD_CUDA(ctx, cudaMemcpy(d.p, idx.data(), (size_t)primCount * 4, cudaMemcpyHostToDevice));
+  k_shade_records<<<(primCount + 255) / 256, 256, 0, ctx->stream>>>(ctx->prims.as<const float4>(),
+                                                                    d.as<const uint32_t>(), primCount,
+                                                                    ctx->shadeRec.as<float4>());
+  NOMAD_CUDA(ctx, cudaGetLastError());
+  NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return NOMAD_OK;
+}
 
 extern "C" nomad_status nomad_view_pinhole(const float pos[3], const float look[3], const float up[3],
                                            float vfov, uint32_t width, uint32_t height, nomad_view *out) {
@@ -715,8 +793,8 @@ extern "C" nomad_status nomad_render_frame(nomad_ctx *ctx, const nomad_view *vie
                                          F.qIds[cur].as<const uint32_t>(), F.hits.as<const int32_t>(),
                                          F.qRays[cur ^ 1].as<float4>(), F.qIds[cur ^ 1].as<uint32_t>(),
                                          F.sRays.as<float4>(), F.sIds.as<uint32_t>(), F.sContrib.as<float4>(),
-                                         F.thr.as<float4>(), F.rad.as<float4>(), ctx->prims.as<const float4>(),
-                                         ctx->materials.as<const float4>(), L, C, cur, objHits, plan.on ? 1 : 0,
+                                         F.thr.as<float4>(), F.rad.as<float4>(), ctx->shadeRec.as<const float4>(),
+                                         ctx->matTable.as<const float4>(), L, C, cur, objHits, plan.on ? 1 : 0,
                                          primHits);
       rs = nomad_trace_variant(ctx, ctx->trav, true, F.sRays.as<const float4>(), P, &C->qlen[2], &C->cursor[1],
                                nullptr, F.sOcc.as<uint8_t>(), nullptr, s);
@@ -757,6 +835,8 @@ extern "C" nomad_status nomad_render_frame(nomad_ctx *ctx, const nomad_view *vie
     key_put(key, ctx->res.emissiveCount);
     key_put(key, ctx->prims.p);
     key_put(key, ctx->materials.p);
+    key_put(key, ctx->shadeRec.p);
+    key_put(key, ctx->matTable.p);
     for (const DeviceBuf *b : {&F.thr, &F.rad, &F.qRays[0], &F.qRays[1], &F.qIds[0], &F.qIds[1], &F.hits, &F.sRays,
                                &F.sIds, &F.sContrib, &F.sOcc, &F.counters, &F.views, &F.lightIdx, &F.lightCdf,
                                &F.lightMeta, &F.rInit, &F.rTemp, &F.resv[0], &F.resv[1], &F.surf[0], &F.surf[1],

@@ -105,6 +105,11 @@ struct nomad_ctx {
   // device memory
   DeviceBuf arena;      // pair nodes then triangle records
   DeviceBuf prims, materials;
+  // Compact shading records: one float4 per primitive (the geometric-or-shading normal the hit
+  // normal resolves to, or a sphere's center, and bits(material index | type << 30)) and the
+  // distinct 80-byte material records they index (nomad_build_shade_records).
+  DeviceBuf shadeRec, matTable;
+  uint32_t matCount = 0;
   DeviceBuf objHits, status, cursor;
   DeviceBuf stageIn, stageOut, stageAux;  // host-pointer staging
   DeviceBuf patchOffs, patchVals;
@@ -201,6 +206,7 @@ struct nomad_ctx {
 nomad_status nomad_residency_sync_host(nomad_ctx *ctx);
 // Per-object "rays tested" of n closest-hit rays (2 float4 each) and their hits (5 words each;
 // the count from lenDev when set), added to ctx->res.tests on the context's stream.
+nomad_status nomad_build_shade_records(nomad_ctx *ctx, const float *materials, uint32_t primCount);
 nomad_status nomad_count_object_tests(nomad_ctx *ctx, const float4 *rays, const int32_t *hits5, uint64_t n,
                                       const uint32_t *lenDev);
 constexpr int kPostWords = 9;

@@ -336,6 +336,10 @@ extern "C" nomad_status nomad_scene_upload(nomad_ctx *ctx, const float *bvh, uin
   NOMAD_CUDA(ctx, cudaMemcpy(ctx->materials.p, materials, (size_t)primCount * 80,
                              cudaMemcpyHostToDevice));
   NOMAD_CUDA(ctx, cudaMemset(ctx->objHits.p, 0, (size_t)objectCount * 4 + 16));
+  {
+    nomad_status ss = nomad_build_shade_records(ctx, materials, primCount);
+    if (ss != NOMAD_OK) return ss;
+  }
   ctx->pnodeWords = pnBytes / 4;
   DevScene &S = ctx->scene;
   S.pn = reinterpret_cast<const float4 *>(base);
