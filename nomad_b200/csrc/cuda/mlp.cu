@@ -1,13 +1,13 @@
 // Learned residency scorer: MLP 24 -> 128 -> 128 -> 1 (ReLU), BF16 weights and activations,
-// FP32 accumulation on the tensor cores, trained on the device with AdamW. Inference (every
-// residency step) runs on tcgen05 with tensor-memory accumulators; training uses mma.sync
-// m16n8k16 kernels.
+// FP32 accumulation on the tensor cores, trained on the device with AdamW. Every matrix product
+// runs on tcgen05 with tensor-memory accumulators: inference (every residency step) and the
+// training forward pass in one fused kernel (both hidden layers and the output dot product, the
+// weights staged by one bulk copy), and the backward products in a tiled GEMM kernel whose
+// operands the threads stage in the canonical shared-memory layout.
 //
-// The GEMMs are tiny (2,048 objects x 128 x 128 per frame), so the kernels are built for
-// latency: the forward pass is one fused kernel (both hidden layers and the output dot product
-// with the weights resident in shared memory); training uses one generic BF16 GEMM kernel for
-// the backward products, with split-K partial sums reduced in a fixed order so training is
-// bit-reproducible for a given seed.
+// The GEMMs are tiny (2,048 objects x 128 x 128 per frame; a 4,096-row training batch), so the
+// kernels are built for latency; the backward products use split-K partial sums reduced in a
+// fixed order, so training is bit-reproducible for a given seed.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -42,155 +42,6 @@ static_assert(kParams == NOMAD_MLP_PARAMS, "parameter blob layout");
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
   __nv_bfloat162 h = __floats2bfloat162_rn(a, b);  // a -> low half
   return *reinterpret_cast<uint32_t *>(&h);
-}
-
-__device__ __forceinline__ void mma_bf16(float c[4], const uint32_t a[4], const uint32_t b[2]) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};\n"
-      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
-
-// ---- fused forward ------------------------------------------------------------------------
-// Block: 4 warps, 64 rows (16 per warp). Shared: W1 [128][32], W2 [128][128], X [64][32],
-// H1 [64][128] in bf16 (row stride padded by 8 halves against bank conflicts).
-constexpr int kFwdRows = 64;
-constexpr int kS32 = kInPad + 8;   // row stride (halves) for 32-wide rows
-constexpr int kS128 = kHid + 8;    // row stride for 128-wide rows
-constexpr size_t kFwdSmem =
-    sizeof(__nv_bfloat16) * (kHid * kS32 + kHid * kS128 + kFwdRows * kS32 + kFwdRows * kS128) +
-    sizeof(float) * (3 * kHid + 1 + 2 * kIn);
-
-// X rows are raw features (fp32, n x 24); standardised with the blob's mean/istd on load.
-// Outputs: y[n]; when saving for backward also Z1 (pre-ReLU) and H2 (post-ReLU) as fp32 and
-// H1 (post-ReLU) and the standardised X as bf16.
-__global__ void __launch_bounds__(128) k_mlp_forward(const float *__restrict__ X, uint64_t n,
-                                                     const float *__restrict__ P,
-                                                     const __nv_bfloat16 *__restrict__ W1b,
-                                                     const __nv_bfloat16 *__restrict__ W2b,
-                                                     float *__restrict__ y, float *__restrict__ z1,
-                                                     __nv_bfloat16 *__restrict__ h1out,
-                                                     float *__restrict__ z2,
-                                                     __nv_bfloat16 *__restrict__ xout) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  __nv_bfloat16 *sW1 = reinterpret_cast<__nv_bfloat16 *>(smem);
-  __nv_bfloat16 *sW2 = sW1 + kHid * kS32;
-  __nv_bfloat16 *sX = sW2 + kHid * kS128;
-  __nv_bfloat16 *sH1 = sX + kFwdRows * kS32;
-  float *sB1 = reinterpret_cast<float *>(sH1 + kFwdRows * kS128);
-  float *sB2 = sB1 + kHid;
-  float *sW3 = sB2 + kHid;
-  float *sB3 = sW3 + kHid;
-  float *sMean = sB3 + 1;
-  float *sIstd = sMean + kIn;
-  const int tid = threadIdx.x;
-  for (int i = tid; i < kHid * kInPad; i += 128) sW1[(i / kInPad) * kS32 + i % kInPad] = W1b[i];
-  for (int i = tid; i < kHid * kHid; i += 128) sW2[(i / kHid) * kS128 + i % kHid] = W2b[i];
-  for (int i = tid; i < kHid; i += 128) {
-    sB1[i] = P[oB1 + i];
-    sB2[i] = P[oB2 + i];
-    sW3[i] = P[oW3 + i];
-  }
-  if (tid == 0) sB3[0] = P[oB3];
-  for (int i = tid; i < kIn; i += 128) {
-    sMean[i] = P[oMean + i];
-    sIstd[i] = P[oIstd + i];
-  }
-  __syncthreads();
-  const uint64_t row0 = (uint64_t)blockIdx.x * kFwdRows;
-  for (int i = tid; i < kFwdRows * kInPad; i += 128) {
-    int r = i / kInPad, f = i % kInPad;
-    float v = 0.0f;
-    if (f < kIn && row0 + r < n) v = (X[(row0 + r) * kIn + f] - sMean[f]) * sIstd[f];
-    __nv_bfloat16 b = __float2bfloat16_rn(v);
-    sX[r * kS32 + f] = b;
-    if (xout && row0 + r < n) xout[(row0 + r) * kInPad + f] = b;
-  }
-  __syncthreads();
-  const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, t4 = lane & 3;
-  const int wr = warp * 16;
-  // layer 1: [16 x 32] x [32 x 128]
-  float acc[16][4];
-#pragma unroll
-  for (int j = 0; j < 16; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
-#pragma unroll
-  for (int ks = 0; ks < kInPad; ks += 16) {
-    uint32_t a[4];
-    a[0] = *reinterpret_cast<const uint32_t *>(sX + (wr + g) * kS32 + ks + t4 * 2);
-    a[1] = *reinterpret_cast<const uint32_t *>(sX + (wr + g + 8) * kS32 + ks + t4 * 2);
-    a[2] = *reinterpret_cast<const uint32_t *>(sX + (wr + g) * kS32 + ks + 8 + t4 * 2);
-    a[3] = *reinterpret_cast<const uint32_t *>(sX + (wr + g + 8) * kS32 + ks + 8 + t4 * 2);
-#pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      uint32_t b[2];
-      b[0] = *reinterpret_cast<const uint32_t *>(sW1 + (j * 8 + g) * kS32 + ks + t4 * 2);
-      b[1] = *reinterpret_cast<const uint32_t *>(sW1 + (j * 8 + g) * kS32 + ks + 8 + t4 * 2);
-      mma_bf16(acc[j], a, b);
-    }
-  }
-#pragma unroll
-  for (int j = 0; j < 16; ++j) {
-    int c0 = j * 8 + t4 * 2;
-    float v0 = acc[j][0] + sB1[c0], v1 = acc[j][1] + sB1[c0 + 1];
-    float v2 = acc[j][2] + sB1[c0], v3 = acc[j][3] + sB1[c0 + 1];
-    uint64_t ra = row0 + wr + g, rb = ra + 8;
-    if (z1) {
-      if (ra < n) { z1[ra * kHid + c0] = v0; z1[ra * kHid + c0 + 1] = v1; }
-      if (rb < n) { z1[rb * kHid + c0] = v2; z1[rb * kHid + c0 + 1] = v3; }
-    }
-    uint32_t pa = pack_bf16(fmaxf(v0, 0.0f), fmaxf(v1, 0.0f));
-    uint32_t pb = pack_bf16(fmaxf(v2, 0.0f), fmaxf(v3, 0.0f));
-    *reinterpret_cast<uint32_t *>(sH1 + (wr + g) * kS128 + c0) = pa;
-    *reinterpret_cast<uint32_t *>(sH1 + (wr + g + 8) * kS128 + c0) = pb;
-    if (h1out) {
-      if (ra < n) *reinterpret_cast<uint32_t *>(h1out + ra * kHid + c0) = pa;
-      if (rb < n) *reinterpret_cast<uint32_t *>(h1out + rb * kHid + c0) = pb;
-    }
-  }
-  __syncwarp();
-  // layer 2: [16 x 128] x [128 x 128]
-#pragma unroll
-  for (int j = 0; j < 16; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
-#pragma unroll 2
-  for (int ks = 0; ks < kHid; ks += 16) {
-    uint32_t a[4];
-    a[0] = *reinterpret_cast<const uint32_t *>(sH1 + (wr + g) * kS128 + ks + t4 * 2);
-    a[1] = *reinterpret_cast<const uint32_t *>(sH1 + (wr + g + 8) * kS128 + ks + t4 * 2);
-    a[2] = *reinterpret_cast<const uint32_t *>(sH1 + (wr + g) * kS128 + ks + 8 + t4 * 2);
-    a[3] = *reinterpret_cast<const uint32_t *>(sH1 + (wr + g + 8) * kS128 + ks + 8 + t4 * 2);
-#pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      uint32_t b[2];
-      b[0] = *reinterpret_cast<const uint32_t *>(sW2 + (j * 8 + g) * kS128 + ks + t4 * 2);
-      b[1] = *reinterpret_cast<const uint32_t *>(sW2 + (j * 8 + g) * kS128 + ks + 8 + t4 * 2);
-      mma_bf16(acc[j], a, b);
-    }
-  }
-  // layer 3: relu(acc + b2) . w3 + b3
-  float sa = 0.0f, sb = 0.0f;
-#pragma unroll
-  for (int j = 0; j < 16; ++j) {
-    int c0 = j * 8 + t4 * 2;
-    float v0 = acc[j][0] + sB2[c0], v1 = acc[j][1] + sB2[c0 + 1];
-    float v2 = acc[j][2] + sB2[c0], v3 = acc[j][3] + sB2[c0 + 1];
-    uint64_t ra = row0 + wr + g, rb = ra + 8;
-    if (z2) {
-      if (ra < n) { z2[ra * kHid + c0] = v0; z2[ra * kHid + c0 + 1] = v1; }
-      if (rb < n) { z2[rb * kHid + c0] = v2; z2[rb * kHid + c0 + 1] = v3; }
-    }
-    sa += fmaxf(v0, 0.0f) * sW3[c0] + fmaxf(v1, 0.0f) * sW3[c0 + 1];
-    sb += fmaxf(v2, 0.0f) * sW3[c0] + fmaxf(v3, 0.0f) * sW3[c0 + 1];
-  }
-  sa += __shfl_xor_sync(0xffffffffu, sa, 1);
-  sa += __shfl_xor_sync(0xffffffffu, sa, 2);
-  sb += __shfl_xor_sync(0xffffffffu, sb, 1);
-  sb += __shfl_xor_sync(0xffffffffu, sb, 2);
-  if (t4 == 0) {
-    uint64_t ra = row0 + wr + g, rb = ra + 8;
-    if (ra < n) y[ra] = sa + sB3[0];
-    if (rb < n) y[rb] = sb + sB3[0];
-  }
 }
 
 // ---- inference on the 5th-generation tensor cores (tcgen05) ---------------------------------
@@ -271,11 +122,19 @@ __device__ __forceinline__ void tc_ld32(uint32_t taddr, float (&v)[32]) {
 // them whenever the weights change), so one bulk asynchronous copy stages both.
 // FEAT: the rows are the residency step's objects; each thread computes its object's features
 // (nomad_res::object_features, the same code as the feature kernel) instead of reading X.
-template <bool FEAT>
+// SAVE (training): also stores what the backward pass needs, row-major: the standardised inputs
+// (bf16, n x 32), Z1 = X W1^T + b1 (fp32), H1 = ReLU(Z1) (bf16) and Z2 = H1 W2^T + b2 (fp32).
+struct FwdSave {
+  __nv_bfloat16 *xbf, *h1;
+  float *z1, *z2;
+};
+
+template <bool FEAT, bool SAVE>
 __global__ void __launch_bounds__(128) k_mlp_forward_tc(const float *__restrict__ X, uint64_t n,
                                                         const float *__restrict__ P,
                                                         const unsigned char *__restrict__ Wc, float *__restrict__ y,
-                                                        uint32_t *__restrict__ status, nomad_res::FeatArgs fa) {
+                                                        uint32_t *__restrict__ status, nomad_res::FeatArgs fa,
+                                                        FwdSave sv) {
   extern __shared__ __align__(16) unsigned char smem[];
   const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
   float *sB1 = reinterpret_cast<float *>(smem + kTcF);
@@ -337,7 +196,9 @@ __global__ void __launch_bounds__(128) k_mlp_forward_tc(const float *__restrict_
       const int r = i / kInPad, f = i % kInPad;
       float v = 0.0f;
       if (f < kIn && row0 + r < n) v = (X[(row0 + r) * kIn + f] - sMean[f]) * sIstd[f];
-      *reinterpret_cast<__nv_bfloat16 *>(smem + kTcX + canon_off(r, f)) = __float2bfloat16_rn(v);
+      const __nv_bfloat16 b = __float2bfloat16_rn(v);
+      *reinterpret_cast<__nv_bfloat16 *>(smem + kTcX + canon_off(r, f)) = b;
+      if (SAVE && row0 + r < n) sv.xbf[(row0 + r) * kInPad + f] = b;
     }
   }
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -360,14 +221,22 @@ __global__ void __launch_bounds__(128) k_mlp_forward_tc(const float *__restrict_
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   // epilogue 1: bias, ReLU, BF16 into the layer-2 operand (row = this thread's lane)
   const int r = tid;
+  const bool rowLive = row0 + r < n;
 #pragma unroll
   for (int c0 = 0; c0 < kHid; c0 += 32) {
     float v[32];
     tc_ld32(lane_base + c0, v);
 #pragma unroll
     for (int j = 0; j < 32; j += 2) {
-      const float a = fmaxf(v[j] + sB1[c0 + j], 0.0f), b = fmaxf(v[j + 1] + sB1[c0 + j + 1], 0.0f);
-      *reinterpret_cast<uint32_t *>(smem + kTcH1 + canon_off(r, c0 + j)) = pack_bf16(a, b);
+      const float za = v[j] + sB1[c0 + j], zb = v[j + 1] + sB1[c0 + j + 1];
+      const uint32_t h = pack_bf16(fmaxf(za, 0.0f), fmaxf(zb, 0.0f));
+      *reinterpret_cast<uint32_t *>(smem + kTcH1 + canon_off(r, c0 + j)) = h;
+      if (SAVE && rowLive) {
+        const uint64_t o = (row0 + r) * kHid + c0 + j;
+        sv.z1[o] = za;
+        sv.z1[o + 1] = zb;
+        *reinterpret_cast<uint32_t *>(sv.h1 + o) = h;
+      }
     }
   }
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -391,7 +260,11 @@ __global__ void __launch_bounds__(128) k_mlp_forward_tc(const float *__restrict_
     float v[32];
     tc_ld32(lane_base + 128 + c0, v);
 #pragma unroll
-    for (int j = 0; j < 32; ++j) acc += fmaxf(v[j] + sB2[c0 + j], 0.0f) * sW3[c0 + j];
+    for (int j = 0; j < 32; ++j) {
+      const float z = v[j] + sB2[c0 + j];
+      if (SAVE && rowLive) sv.z2[(row0 + r) * kHid + c0 + j] = z;
+      acc += fmaxf(z, 0.0f) * sW3[c0 + j];
+    }
   }
   if (row0 + r < n) y[row0 + r] = ok ? acc + sB3[0] : 0.0f;
   if (!ok && tid == 0) atomicOr(status, kStatusWaitExpired);
@@ -403,70 +276,140 @@ __global__ void __launch_bounds__(128) k_mlp_forward_tc(const float *__restrict_
   }
 }
 
-// ---- generic BF16 GEMM for the backward pass ------------------------------------------------
-// C[z][M][N] (fp32) = sum over this split's K range of op(A)[M][K] * op(B)[K][N].
-// A is stored [M][K] (transA = 0) or [K][M] (transA = 1); B is stored [K][N] (transB = 0) or
-// [N][K] (transB = 1). Block tile 64 x 64, 4 warps of 32 x 32, K step 16.
-template <bool TA, bool TB>
-__global__ void __launch_bounds__(128) k_gemm_bf16(const __nv_bfloat16 *__restrict__ A,
-                                                   const __nv_bfloat16 *__restrict__ B,
-                                                   float *__restrict__ C, int M, int N, int K,
-                                                   int lda, int ldb, int kPerSplit) {
-  __shared__ __align__(16) __nv_bfloat16 As[64][24];
-  __shared__ __align__(16) __nv_bfloat16 Bs[64][24];  // [n][k]
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t4 = lane & 3;
-  const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
+// ---- backward GEMMs on the 5th-generation tensor cores (tcgen05) ---------------------------
+// C[z][M][N] (fp32) = sum over split z's K range of op(A)[M][K] op(B)[K][N], where A is stored
+// [M][K] (TA = 0) or [K][M] (TA = 1) and B [K][N] (TB = 0) or [N][K] (TB = 1), all bf16. One CTA
+// of 128 threads owns a 128-row tile of C and all NT (= N rounded up: 32 or 128) columns,
+// accumulated in tensor memory. K advances 64 at a time: the threads stage the A tile (128 x 64)
+// and the B tile (NT x 64) in shared memory in the canonical K-major layout (whatever the global
+// layout, so transposed operands cost nothing extra), then one thread issues four
+// tcgen05.mma (M = 128, N = NT, K = 16) and commits to an mbarrier that every thread waits on
+// before the tiles are overwritten. Elements past M, N or the split's K range are staged as zero.
+// Split-K partial tiles are summed afterwards in a fixed order (k_reduce_splits), so a gradient
+// is bit-reproducible.
+constexpr int kGemmK = 64;
+
+// Byte offset of element (r, k) of an R-row K-major operand tile in the canonical layout.
+template <int R>
+__device__ __forceinline__ uint32_t canon_off_r(int r, int k) {
+  return (uint32_t)((((k >> 3) * (R / 8) + (r >> 3)) << 7) + ((r & 7) << 4) + ((k & 7) << 1));
+}
+
+// Descriptor of an R-row operand: next K chunk (R / 8) * 128 B away, next row group 128 B away.
+template <int R>
+__device__ __forceinline__ uint64_t canon_desc_r(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3fffu) | ((uint64_t)((R / 8 * 128) >> 4) << 16) |
+         ((uint64_t)(128u >> 4) << 32) | (1ull << 46);
+}
+
+template <int NT>
+__device__ __forceinline__ void tc_mma_n(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  // kind::f16: FP32 accumulator, BF16 A and B, both K-major, N = NT, M = 128
+  constexpr uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NT >> 3) << 17) | ((128u >> 4) << 24);
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(dtmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+template <bool TA, bool TB, int NT>
+__global__ void __launch_bounds__(128) k_gemm_tc(const __nv_bfloat16 *__restrict__ A,
+                                                 const __nv_bfloat16 *__restrict__ B, float *__restrict__ C,
+                                                 int M, int N, int K, int lda, int ldb, int kPerSplit,
+                                                 uint32_t *__restrict__ status) {
+  static_assert(NT == 32 || NT == 64 || NT == 128, "tile width");
+  __shared__ __align__(1024) unsigned char sA[128 * kGemmK * 2];
+  __shared__ __align__(1024) unsigned char sB[NT * kGemmK * 2];
+  __shared__ __align__(8) unsigned long long sBar;
+  __shared__ uint32_t sTmem;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const uint32_t aBase = static_cast<uint32_t>(__cvta_generic_to_shared(sA));
+  const uint32_t bBase = static_cast<uint32_t>(__cvta_generic_to_shared(sB));
+  const uint32_t bar = static_cast<uint32_t>(__cvta_generic_to_shared(&sBar));
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     static_cast<uint32_t>(__cvta_generic_to_shared(&sTmem))),
+                 "r"((uint32_t)NT)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = sTmem;
+  const int m0 = blockIdx.y * 128;
   const int kBeg = blockIdx.z * kPerSplit, kEnd = min(K, kBeg + kPerSplit);
-  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-  float acc[2][4][4];
-#pragma unroll
-  for (int a = 0; a < 2; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = acc[a][b][2] = acc[a][b][3] = 0.0f;
   const __nv_bfloat16 zero = __float2bfloat16_rn(0.0f);
-  for (int k0 = kBeg; k0 < kEnd; k0 += 16) {
-    for (int i = tid; i < 64 * 16; i += 128) {
-      int r = i / 16, c = i % 16;
-      int m = m0 + r, k = k0 + c;
+  uint32_t phase = 0;
+  bool ok = true, issued = false;
+  for (int k0 = kBeg; k0 < kEnd && ok; k0 += kGemmK) {
+    for (int i = tid; i < 128 * kGemmK; i += 128) {
+      // consecutive threads read consecutive addresses of the stored layout
+      const int r = TA ? i % 128 : i / kGemmK, c = TA ? i / 128 : i % kGemmK;
+      const int m = m0 + r, k = k0 + c;
       __nv_bfloat16 v = zero;
       if (m < M && k < kEnd) v = TA ? A[(size_t)k * lda + m] : A[(size_t)m * lda + k];
-      As[r][c] = v;
-      int nn = n0 + r;
-      __nv_bfloat16 w = zero;
-      if (nn < N && k < kEnd) w = TB ? B[(size_t)nn * ldb + k] : B[(size_t)k * ldb + nn];
-      Bs[r][c] = w;
+      *reinterpret_cast<__nv_bfloat16 *>(sA + canon_off_r<128>(r, c)) = v;
     }
-    __syncthreads();
-#pragma unroll
-    for (int a = 0; a < 2; ++a) {
-      uint32_t af[4];
-      int r = wm + a * 16;
-      af[0] = *reinterpret_cast<const uint32_t *>(&As[r + g][t4 * 2]);
-      af[1] = *reinterpret_cast<const uint32_t *>(&As[r + g + 8][t4 * 2]);
-      af[2] = *reinterpret_cast<const uint32_t *>(&As[r + g][8 + t4 * 2]);
-      af[3] = *reinterpret_cast<const uint32_t *>(&As[r + g + 8][8 + t4 * 2]);
-#pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        uint32_t bf[2];
-        int c = wn + b * 8;
-        bf[0] = *reinterpret_cast<const uint32_t *>(&Bs[c + g][t4 * 2]);
-        bf[1] = *reinterpret_cast<const uint32_t *>(&Bs[c + g][8 + t4 * 2]);
-        mma_bf16(acc[a][b], af, bf);
-      }
+    for (int i = tid; i < NT * kGemmK; i += 128) {
+      const int r = TB ? i / kGemmK : i % NT, c = TB ? i % kGemmK : i / NT;
+      const int k = k0 + c;
+      __nv_bfloat16 v = zero;
+      if (r < N && k < kEnd) v = TB ? B[(size_t)r * ldb + k] : B[(size_t)k * ldb + r];
+      *reinterpret_cast<__nv_bfloat16 *>(sB + canon_off_r<NT>(r, c)) = v;
     }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (tid == 0) {
+#pragma unroll
+      for (int s = 0; s < kGemmK / 16; ++s)
+        tc_mma_n<NT>(tmem, canon_desc_r<128>(aBase + s * 2 * (128 / 8 * 128)),
+                     canon_desc_r<NT>(bBase + s * 2 * (NT / 8 * 128)), (k0 > kBeg || s > 0) ? 1u : 0u);
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                   : "memory");
+    }
+    issued = true;
+    ok = __syncthreads_and(tc_wait(bar, phase) ? 1 : 0) != 0;  // one outcome for the whole CTA
+    phase ^= 1u;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   }
+  if (!ok) {
+    // the last commit did not arrive in time: give the MMAs in flight one more bounded wait
+    // before the tensor memory is released, and report it
+    tc_wait(bar, phase ^ 1u);
+    if (tid == 0) atomicOr(status, kStatusWaitExpired);
+  }
+  const int row = m0 + tid;
   float *Cz = C + (size_t)blockIdx.z * M * N;
+  const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
 #pragma unroll
-  for (int a = 0; a < 2; ++a)
+  for (int c0 = 0; c0 < NT; c0 += 32) {
+    float v[32];
+    if (issued) {
+      tc_ld32(lane_base + c0, v);
+    } else {
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      int r = m0 + wm + a * 16 + g, c = n0 + wn + b * 8 + t4 * 2;
-      if (r < M && c < N) Cz[(size_t)r * N + c] = acc[a][b][0];
-      if (r < M && c + 1 < N) Cz[(size_t)r * N + c + 1] = acc[a][b][1];
-      if (r + 8 < M && c < N) Cz[(size_t)(r + 8) * N + c] = acc[a][b][2];
-      if (r + 8 < M && c + 1 < N) Cz[(size_t)(r + 8) * N + c + 1] = acc[a][b][3];
+      for (int j = 0; j < 32; ++j) v[j] = 0.0f;  // empty K range
     }
+    if (row < M) {
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        if (c0 + j < N) Cz[(size_t)row * N + c0 + j] = ok ? v[j] : 0.0f;
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)NT) : "memory");
+  }
 }
 
 // Sums split-K partials in fixed order: out[i] = sum_z part[z][i].
@@ -606,10 +549,11 @@ nomad_status ensure(nomad_ctx *ctx, MlpState &S) {
   NOMAD_CUDA(ctx, S.G.reserve(kParams * 4));
   static bool attr = false;
   if (!attr) {
-    NOMAD_CUDA(ctx, cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwdSmem));
-    NOMAD_CUDA(ctx, cudaFuncSetAttribute(k_mlp_forward_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    NOMAD_CUDA(ctx, cudaFuncSetAttribute(k_mlp_forward_tc<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)kTcSmem));
-    NOMAD_CUDA(ctx, cudaFuncSetAttribute(k_mlp_forward_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    NOMAD_CUDA(ctx, cudaFuncSetAttribute(k_mlp_forward_tc<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kTcSmem));
+    NOMAD_CUDA(ctx, cudaFuncSetAttribute(k_mlp_forward_tc<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)kTcSmem));
     attr = true;
   }
@@ -625,9 +569,10 @@ nomad_status nomad_mlp_infer_device(nomad_ctx *ctx, const float *X, uint64_t n, 
   if (!S.ready) return nomad_fail(ctx, NOMAD_ERR_NOT_READY, "MLP not initialised or trained");
   if (n == 0) return NOMAD_OK;
   const unsigned blocks = (unsigned)((n + kTcRows - 1) / kTcRows);
-  k_mlp_forward_tc<false><<<blocks, 128, kTcSmem, ctx->stream>>>(X, n, S.P.as<const float>(),
-                                                                 S.Wc.as<const unsigned char>(), y,
-                                                                 ctx->status.as<uint32_t>(), nomad_res::FeatArgs{});
+  k_mlp_forward_tc<false, false><<<blocks, 128, kTcSmem, ctx->stream>>>(X, n, S.P.as<const float>(),
+                                                                        S.Wc.as<const unsigned char>(), y,
+                                                                        ctx->status.as<uint32_t>(),
+                                                                        nomad_res::FeatArgs{}, FwdSave{});
   NOMAD_CUDA(ctx, cudaGetLastError());
   return NOMAD_OK;
 }
@@ -637,9 +582,9 @@ nomad_status nomad_mlp_score_objects(nomad_ctx *ctx, const nomad_res::FeatArgs *
   if (!S.ready) return nomad_fail(ctx, NOMAD_ERR_NOT_READY, "MLP not initialised or trained");
   if (fa->n == 0) return NOMAD_OK;
   const unsigned blocks = (fa->n + kTcRows - 1) / kTcRows;
-  k_mlp_forward_tc<true><<<blocks, 128, kTcSmem, ctx->stream>>>(nullptr, fa->n, S.P.as<const float>(),
-                                                                S.Wc.as<const unsigned char>(), keys,
-                                                                ctx->status.as<uint32_t>(), *fa);
+  k_mlp_forward_tc<true, false><<<blocks, 128, kTcSmem, ctx->stream>>>(nullptr, fa->n, S.P.as<const float>(),
+                                                                       S.Wc.as<const unsigned char>(), keys,
+                                                                       ctx->status.as<uint32_t>(), *fa, FwdSave{});
   NOMAD_CUDA(ctx, cudaGetLastError());
   return NOMAD_OK;
 }
@@ -845,10 +790,10 @@ nomad_status batch_gradient(nomad_ctx *ctx, MlpState &S, int B) {
   cudaStream_t s = ctx->stream;
   const int splits = batch_splits(B);
   float *Pm = S.P.as<float>(), *G = S.G.as<float>();
-  k_mlp_forward<<<B / kFwdRows, 128, kFwdSmem, s>>>(S.xb.as<const float>(), B, Pm, S.W1b.as<const __nv_bfloat16>(),
-                                                    S.W2b.as<const __nv_bfloat16>(), S.y.as<float>(), S.z1.as<float>(),
-                                                    S.h1.as<__nv_bfloat16>(), S.z2.as<float>(),
-                                                    S.xbf.as<__nv_bfloat16>());
+  uint32_t *status = ctx->status.as<uint32_t>();
+  k_mlp_forward_tc<false, true><<<(B + kTcRows - 1) / kTcRows, 128, kTcSmem, s>>>(
+      S.xb.as<const float>(), B, Pm, S.Wc.as<const unsigned char>(), S.y.as<float>(), status, nomad_res::FeatArgs{},
+      FwdSave{S.xbf.as<__nv_bfloat16>(), S.h1.as<__nv_bfloat16>(), S.z1.as<float>(), S.z2.as<float>()});
   k_mse_grad<<<(B + 255) / 256, 256, 0, s>>>(S.y.as<const float>(), S.tb.as<const float>(), B, S.dy.as<float>(),
                                              S.se.as<float>());
   k_dz2<<<(B * kHid + 255) / 256, 256, 0, s>>>(S.dy.as<const float>(), S.z2.as<const float>(), Pm, B,
@@ -866,29 +811,29 @@ nomad_status batch_gradient(nomad_ctx *ctx, MlpState &S, int B) {
   k_colsum<<<1, kHid, 0, s>>>(S.dz2f.as<const float>(), nullptr, B, kHid, G + oB2);
   // dW2[n][k] = sum_i dZ2[i][n] H1[i][k]: A = dZ2^T (stored [B][128]), B = H1 [B][128]
   {
-    int kPer = ((B / splits) + 15) / 16 * 16;
+    int kPer = ((B / splits) + kGemmK - 1) / kGemmK * kGemmK;
     int sp = (B + kPer - 1) / kPer;
-    dim3 grid(kHid / 64, kHid / 64, sp);
-    k_gemm_bf16<true, false><<<grid, 128, 0, s>>>(S.dz2b.as<const __nv_bfloat16>(), S.h1.as<const __nv_bfloat16>(),
-                                                  S.part.as<float>(), kHid, kHid, B, kHid, kHid, kPer);
+    dim3 grid(1, 1, sp);
+    k_gemm_tc<true, false, kHid><<<grid, 128, 0, s>>>(S.dz2b.as<const __nv_bfloat16>(), S.h1.as<const __nv_bfloat16>(),
+                                                      S.part.as<float>(), kHid, kHid, B, kHid, kHid, kPer, status);
     k_reduce_splits<<<64, 256, 0, s>>>(S.part.as<const float>(), sp, (size_t)kHid * kHid, G + oW2);
   }
   // dH1[i][k] = sum_n dZ2[i][n] W2[n][k]: A = dZ2 [B][128], B = W2 [128(n)][128(k)] row-major = [K][N]
   {
-    dim3 grid(kHid / 64, (B + 63) / 64, 1);
-    k_gemm_bf16<false, false><<<grid, 128, 0, s>>>(S.dz2b.as<const __nv_bfloat16>(), S.W2b.as<const __nv_bfloat16>(),
-                                                   S.dh1.as<float>(), B, kHid, kHid, kHid, kHid, kHid);
+    dim3 grid(1, (B + 127) / 128, 1);
+    k_gemm_tc<false, false, kHid><<<grid, 128, 0, s>>>(S.dz2b.as<const __nv_bfloat16>(), S.W2b.as<const __nv_bfloat16>(),
+                                                       S.dh1.as<float>(), B, kHid, kHid, kHid, kHid, kHid, status);
   }
   k_dz1<<<(B * kHid + 255) / 256, 256, 0, s>>>(S.dh1.as<const float>(), S.z1.as<const float>(), B,
                                                S.dz1b.as<__nv_bfloat16>(), S.dz1f.as<float>());
   k_colsum<<<1, kHid, 0, s>>>(S.dz1f.as<const float>(), nullptr, B, kHid, G + oB1);
   // dW1[n][k] = sum_i dZ1[i][n] X[i][k]: A = dZ1^T, B = Xbf [B][32]
   {
-    int kPer = ((B / splits) + 15) / 16 * 16;
+    int kPer = ((B / splits) + kGemmK - 1) / kGemmK * kGemmK;
     int sp = (B + kPer - 1) / kPer;
-    dim3 grid(1, kHid / 64, sp);
-    k_gemm_bf16<true, false><<<grid, 128, 0, s>>>(S.dz1b.as<const __nv_bfloat16>(), S.xbf.as<const __nv_bfloat16>(),
-                                                  S.part.as<float>(), kHid, kInPad, B, kHid, kInPad, kPer);
+    dim3 grid(1, 1, sp);
+    k_gemm_tc<true, false, kInPad><<<grid, 128, 0, s>>>(S.dz1b.as<const __nv_bfloat16>(), S.xbf.as<const __nv_bfloat16>(),
+                                                        S.part.as<float>(), kHid, kInPad, B, kHid, kInPad, kPer, status);
     k_reduce_splits<<<16, 256, 0, s>>>(S.part.as<const float>(), sp, (size_t)kHid * kInPad, G + oW1);
   }
   NOMAD_CUDA(ctx, cudaGetLastError());
