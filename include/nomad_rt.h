@@ -382,6 +382,13 @@ typedef struct nomad_residency_params {
   float energy_visibility_boost;     /* energyVisibilityBoost 1.75                             */
   float energy_smoothing;            /* energyImportanceSmoothing 0.85                         */
   uint32_t energy_use_average;       /* energyUseAverageImportance 1                           */
+  /* NOMAD_POLICY_RAYHIT_BUDGET and NOMAD_POLICY_LEARNED: hysteresis of the selection. A resident
+   * object's key k becomes k + resident_key_bonus * |k| before the sort, so it leaves the resident
+   * set only for an object that scores that much higher. Each re-entry of an evicted object costs
+   * an onload when geometry is paged, so this trades a little image error for fewer copies.
+   * No counterpart in the reference, whose ray-hit step has rebuild and state cooldowns instead;
+   * 0 = off. */
+  float resident_key_bonus;
 } nomad_residency_params;
 
 /* One residency step, all on the device: consumes the per-object closest-hit counts gathered

@@ -402,7 +402,7 @@ __global__ void __launch_bounds__(1024) k_select(uint32_t n, uint32_t npow2, uin
                                                  const float *__restrict__ keys, const uint8_t *__restrict__ visible,
                                                  const unsigned long long *__restrict__ bytes,
                                                  unsigned long long budget, uint32_t reserve, uint32_t minActive,
-                                                 uint32_t maxToggles, uint8_t *__restrict__ desired,
+                                                 uint32_t maxToggles, float resBonus, uint8_t *__restrict__ desired,
                                                  uint8_t *__restrict__ res, const long long *__restrict__ slot,
                                                  const int32_t *__restrict__ blasRef, int32_t *__restrict__ pnodeWords,
                                                  uint32_t *__restrict__ misc, WidePatch wp, LightArgs la) {
@@ -413,8 +413,14 @@ __global__ void __launch_bounds__(1024) k_select(uint32_t n, uint32_t npow2, uin
   __shared__ uint8_t on[4096];
   __shared__ float ltotal;
   __shared__ uint32_t lcount;
-  for (uint32_t i = threadIdx.x; i < npow2; i += blockDim.x)
-    sk[i] = i < n ? sort_key(policy == NOMAD_POLICY_ALWAYS ? 1.0f : keys[i], i) : ~0ull;
+  for (uint32_t i = threadIdx.x; i < npow2; i += blockDim.x) {
+    float k = 1.0f;
+    if (i < n && policy != NOMAD_POLICY_ALWAYS) {
+      k = keys[i];
+      if (resBonus != 0.0f && res[i]) k = k + resBonus * fabsf(k);  // hysteresis for resident objects
+    }
+    sk[i] = i < n ? sort_key(k, i) : ~0ull;
+  }
   if (threadIdx.x == 0) {
     sh.used4 = 0;
     misc[1] = 0;
@@ -2210,7 +2216,8 @@ extern "C" nomad_status nomad_residency_step(nomad_ctx *ctx, const nomad_residen
   // one kernel: selection, toggles, pair and wide layout patches, light CDF
   k_select<<<1, 1024, smem, s>>>(N, npow2, prm->policy, R.keys.as<const float>(), R.visible.as<const uint8_t>(),
                                  R.bytes.as<const unsigned long long>(), prm->budget_bytes, reserve, prm->min_active,
-                                 prm->max_toggles, R.desired.as<uint8_t>(), R.objRes.as<uint8_t>(),
+                                 prm->max_toggles, prm->resident_key_bonus, R.desired.as<uint8_t>(),
+                                 R.objRes.as<uint8_t>(),
                                  R.objSlot.as<const long long>(), R.objBlasRef.as<const int32_t>(),
                                  static_cast<int32_t *>(ctx->arena.p), R.misc.as<uint32_t>(), wp, la);
   NOMAD_CUDA(ctx, cudaGetLastError());

@@ -273,7 +273,7 @@ class ResidencyParams(C.Structure):
                 ("demotion_dwell_frames", C.c_uint32), ("env_escape_threshold", C.c_float),
                 ("env_high_escape", C.c_float), ("env_low_escape", C.c_float),
                 ("energy_visibility_boost", C.c_float), ("energy_smoothing", C.c_float),
-                ("energy_use_average", C.c_uint32)]
+                ("energy_use_average", C.c_uint32), ("resident_key_bonus", C.c_float)]
 
     @staticmethod
     def make(policy, budget_bytes=0, max_toggles=0, hit_decay=0.85, camera_motion=0.0,
@@ -285,7 +285,7 @@ class ResidencyParams(C.Structure):
              rayhit_prior_scale=0.0, uncertainty_boost=0.25, desired_hysteresis=0.02, visible_floor=0.0,
              recent_promotion_frames=4, demotion_dwell_frames=0, env_escape_threshold=0.4,
              env_high_escape=0.6, env_low_escape=0.3, energy_visibility_boost=1.75, energy_smoothing=0.85,
-             energy_use_average=1):
+             energy_use_average=1, resident_key_bonus=0.0):
         return ResidencyParams(policy, max_toggles, budget_bytes, hit_decay, camera_motion,
                                memory_pressure, reserve_base, reserve_motion, min_active, target_fraction,
                                rebuild_cooldown, state_cooldown, lod_enter_distance, lod_exit_distance,
@@ -294,7 +294,8 @@ class ResidencyParams(C.Structure):
                                probability_idle_decay, probability_threshold, rayhit_prior_scale,
                                uncertainty_boost, desired_hysteresis, visible_floor, recent_promotion_frames,
                                demotion_dwell_frames, env_escape_threshold, env_high_escape, env_low_escape,
-                               energy_visibility_boost, energy_smoothing, energy_use_average)
+                               energy_visibility_boost, energy_smoothing, energy_use_average,
+                               resident_key_bonus)
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

@@ -8,9 +8,11 @@ one residency step. The image judge is the same frame rendered with every object
 the headline error is the energy-weighted rel-MSE sum_f sum_px (I - I_AR)^2 / sum_f sum_px I_AR^2
 over the path, which near-black reference frames cannot dominate (also reported: the per-frame
 rel-MSE mean((I - I_AR)^2) / mean(I_AR^2), averaged over the frames whose reference is not black,
-and its median). ms/frame is device time: CUDA events recorded on the stream the context runs on,
-around the frame's render, residency step and (when paging) streaming update; each policy's path is
-run `repeats` times and reported as the mean with its spread (min, max of the per-run means).
+and its median; and the energy-weighted rel-MSE of the images clamped to [0, 1], the displayable
+range, which the few near-light fireflies of the HDR images cannot dominate). ms/frame is device
+time: CUDA events recorded on the stream the context runs on, around the frame's render,
+residency step and (when paging) streaming update; each policy's path is run `repeats` times
+and reported as the mean with its spread (min, max of the per-run means).
 
 The learned scorer is trained on the device on hit counts recorded along seeded training camera
 paths rendered with every object resident: features of frame f, target log1p(hits of frame
@@ -29,6 +31,7 @@ import numpy as np
 from . import native as nat
 
 HIST_FEATURES = list(range(3, 12)) + [19, 20]
+HYSTERESIS = 0.5  # resident_key_bonus of the hysteresis rows
 # the reference's host-side heuristics, which toggle through the residency interface
 HOST_POLICIES = (nat.POLICY_RAYHIT_PRIM, nat.POLICY_DISTANCE_LOD, nat.POLICY_SCREEN_SPACE,
                  nat.POLICY_PROBABILISTIC, nat.POLICY_ENVIRONMENT_HIT, nat.POLICY_PREDICTIVE, nat.POLICY_ENERGY)
@@ -205,7 +208,7 @@ class Workload:
         d_img = torch.empty(npix * 3, dtype=torch.float32, device="cuda")
         d_ref = torch.empty(npix * 3, dtype=torch.float32, device="cuda")
         mse, ms, resident_bytes = [], [], []
-        sum_num = sum_den = 0.0
+        sum_num = sum_den = sum_num_c = sum_den_c = 0.0
         # host-side policies step synchronously (the toggles come back to the host)
         host_step = prm.policy in HOST_POLICIES
         clock = FrameClock(ctx)
@@ -222,11 +225,14 @@ class Workload:
                 dt = clock.stop()
                 num = torch.mean((d_img - d_ref) ** 2).item()
                 den = torch.mean(d_ref ** 2).item()
+                ci, cr = torch.clamp(d_img, max=1.0), torch.clamp(d_ref, max=1.0)
                 if f >= warm:
                     if den > 0:  # a black reference frame (camera inside geometry) has no relative error
                         mse.append(num / den)
                     sum_num += num
                     sum_den += den
+                    sum_num_c += torch.mean((ci - cr) ** 2).item()
+                    sum_den_c += torch.mean(cr ** 2).item()
                     ms.append(dt)
                     flags = ctx.residency_flags().astype(bool)
                     resident_bytes.append(int(nbytes[flags].sum()))
@@ -234,6 +240,7 @@ class Workload:
             clock.close()
         return {"rel_mse": float(np.mean(mse)), "rel_mse_p50": float(np.median(mse)),
                 "rel_mse_energy": sum_num / sum_den if sum_den > 0 else None,
+                "rel_mse_energy_clamped": sum_num_c / sum_den_c if sum_den_c > 0 else None,
                 "ms_per_frame": float(np.mean(ms)),
                 "ms_per_frame_p50": float(np.median(ms)),
                 "resident_fraction": float(np.mean(resident_bytes) / nbytes.sum()),
@@ -241,13 +248,13 @@ class Workload:
 
 
     def evaluate_paged(self, ctx, judge, policy, path_seed=1, frames=None, warm=5, pool_slack=1.25,
-                       budget_fraction=None, mlp=None):
+                       budget_fraction=None, mlp=None, bonus=0.0):
         """The same run with geometry paging: a third context whose BLAS nodes (of the tuned
         traversal width) and triangle records live in a device pool of pool_slack x the budget's
         share of the paged bytes, streamed in by nomad_paging_update after every residency step
         (at most 32 onloads per frame). ms/frame includes the update; rel-MSE includes the frames
         where wanted objects are still streaming. The scorer is ctx's unless mlp (a weight blob)
-        is given."""
+        is given; bonus is the selection's hysteresis (resident_key_bonus)."""
         import torch
 
         frames = frames or self.frames
@@ -267,12 +274,13 @@ class Workload:
             pc.paging_enable(pool, width=trav["width"])
             nbytes = pc.object_bytes()
             budget = int(frac * nbytes.sum())
-            prm = nat.ResidencyParams.make(policy, budget_bytes=budget, camera_motion=0.3, min_active=0)
+            prm = nat.ResidencyParams.make(policy, budget_bytes=budget, camera_motion=0.3, min_active=0,
+                                           resident_key_bonus=bonus)
             npix = self.width * self.height
             d_img = torch.empty(npix * 3, dtype=torch.float32, device="cuda")
             d_ref = torch.empty(npix * 3, dtype=torch.float32, device="cuda")
             mse, ms, streamed, onl = [], [], [], []
-            sum_num = sum_den = 0.0
+            sum_num = sum_den = sum_num_c = sum_den_c = 0.0
             clock = FrameClock(pc)  # paging work must run on the context's stream: this one
             pc.reset_object_hits()
             prev = pc.paging_stats()
@@ -286,11 +294,14 @@ class Workload:
                 dt = clock.stop()
                 num = torch.mean((d_img - d_ref) ** 2).item()
                 den = torch.mean(d_ref ** 2).item()
+                ci, cr = torch.clamp(d_img, max=1.0), torch.clamp(d_ref, max=1.0)
                 st = pc.paging_stats()
                 if f >= warm:
                     mse.append(num / den if den > 0 else None)
                     sum_num += num
                     sum_den += den
+                    sum_num_c += torch.mean((ci - cr) ** 2).item()
+                    sum_den_c += torch.mean(cr ** 2).item()
                     ms.append(dt)
                     streamed.append(st["bytes_streamed"] - prev["bytes_streamed"])
                     onl.append(st["onloads"] - prev["onloads"])
@@ -301,6 +312,7 @@ class Workload:
             mse = [m for m in mse if m is not None]
             return {"rel_mse": float(np.mean(mse)), "rel_mse_p50": float(np.median(mse)),
                     "rel_mse_energy": sum_num / sum_den if sum_den > 0 else None,
+                    "rel_mse_energy_clamped": sum_num_c / sum_den_c if sum_den_c > 0 else None,
                     "rel_mse_from_frame_40": float(np.mean(late)) if late else None,
                     "ms_per_frame": float(np.mean(ms)),
                     "ms_per_frame_p50": float(np.median(ms)), "frames": len(mse),
@@ -359,11 +371,16 @@ def run(paths=200, frames_per_path=8, steps=1500, frames=300, repeats=3, log=pri
     out["learned_cost"] = with_model(blob_cost, lambda: repeat(
         lambda: w.evaluate(ctx, judge, nat.POLICY_LEARNED, frames=frames), repeats))
     log(f"learned_cost: {out['learned_cost']}")
-    for name, pol, blob in (("ray_hit_budget_paged", nat.POLICY_RAYHIT_BUDGET, None),
-                            ("learned_paged", nat.POLICY_LEARNED, blob_hits),
-                            ("learned_cost_paged", nat.POLICY_LEARNED, blob_cost)):
+    # paged runs; "_hysteresis" rows raise resident objects' keys by HYSTERESIS * |key|, so the
+    # selection changes less from frame to frame and fewer objects are streamed back in
+    for name, pol, blob, bonus in (("ray_hit_budget_paged", nat.POLICY_RAYHIT_BUDGET, None, 0.0),
+                                   ("learned_paged", nat.POLICY_LEARNED, blob_hits, 0.0),
+                                   ("learned_cost_paged", nat.POLICY_LEARNED, blob_cost, 0.0),
+                                   ("ray_hit_budget_paged_hysteresis", nat.POLICY_RAYHIT_BUDGET, None, HYSTERESIS),
+                                   ("learned_paged_hysteresis", nat.POLICY_LEARNED, blob_hits, HYSTERESIS)):
         try:
-            out[name] = repeat(lambda: w.evaluate_paged(ctx, judge, pol, frames=frames, mlp=blob), repeats)
+            out[name] = repeat(lambda: w.evaluate_paged(ctx, judge, pol, frames=frames, mlp=blob, bonus=bonus),
+                               repeats)
         except nat.NomadError as exc:  # a traversal width the paging cannot hold
             out[name] = {"error": str(exc)}
         log(f"{name}: {out[name]}")
@@ -424,18 +441,52 @@ def run(paths=200, frames_per_path=8, steps=1500, frames=300, repeats=3, log=pri
             out[f"{tag}_matching_rayhit"] = None
             continue
         frac = float(ok[0])
-        try:
-            paged = repeat(lambda: w.evaluate_paged(ctx, judge, nat.POLICY_LEARNED, frames=frames,
-                                                    budget_fraction=frac, mlp=blob), repeats)
-        except nat.NomadError as exc:
-            paged = {"error": str(exc)}
         rh = out["ray_hit_budget_paged"]
-        out[f"{tag}_matching_rayhit"] = {
-            "budget_fraction": frac, "unpaged": sweep[ok[0]], "paged": paged,
-            "ray_hit_paged_ms_per_frame_spread": rh.get("ms_per_frame_spread"),
-            "faster_outside_spread": bool("ms_per_frame_spread" in paged and "ms_per_frame_spread" in rh and
-                                          paged["ms_per_frame_spread"]["max"] < rh["ms_per_frame_spread"]["min"])}
+        rec = {"budget_fraction": frac, "unpaged": sweep[ok[0]],
+               "ray_hit_paged_ms_per_frame_spread": rh.get("ms_per_frame_spread")}
+        for key, bonus in (("paged", 0.0), ("paged_hysteresis", HYSTERESIS)):
+            try:
+                paged = repeat(lambda: w.evaluate_paged(ctx, judge, nat.POLICY_LEARNED, frames=frames,
+                                                        budget_fraction=frac, mlp=blob, bonus=bonus), repeats)
+            except nat.NomadError as exc:
+                paged = {"error": str(exc)}
+            rec[key] = paged
+            rec[f"{key}_faster_outside_spread"] = bool(
+                "ms_per_frame_spread" in paged and "ms_per_frame_spread" in rh and
+                paged["ms_per_frame_spread"]["max"] < rh["ms_per_frame_spread"]["min"])
+            rec[f"{key}_energy_within_5pct_of_ray_hit_paged"] = bool(
+                "rel_mse_energy" in paged and paged["rel_mse_energy"] <= 1.05 * rh["rel_mse_energy"])
+        out[f"{tag}_matching_rayhit"] = rec
         log(f"{tag} matching ray-hit at {frac}: {out[f'{tag}_matching_rayhit']}")
+    # With paging on (the budget then bounds device memory): the smallest budget at which the
+    # learned policy with hysteresis, paged, keeps its energy rel-MSE within 5 % of the paged
+    # ray-hit policy's at the full budget, and its ms/frame against that policy's.
+    rhp = out["ray_hit_budget_paged"]
+    if "rel_mse_energy" in rhp:
+        target_p = 1.05 * rhp["rel_mse_energy"]
+        psweep = {}
+        for frac in (0.15, 0.2, 0.25, 0.3, 0.35):
+            try:
+                psweep[f"{frac:.2f}"] = w.evaluate_paged(ctx, judge, nat.POLICY_LEARNED, frames=frames,
+                                                         budget_fraction=frac, mlp=blob_hits, bonus=HYSTERESIS)
+            except nat.NomadError as exc:
+                psweep[f"{frac:.2f}"] = {"error": str(exc)}
+        out["learned_paged_hysteresis_budget_sweep"] = psweep
+        log(f"learned paged (hysteresis) sweep: "
+            f"{ {k: (v.get('rel_mse_energy'), v.get('ms_per_frame')) for k, v in psweep.items()} }")
+        ok = [k for k, v in sorted(psweep.items()) if v.get("rel_mse_energy", 1e30) <= target_p]
+        if ok:
+            frac = float(ok[0])
+            rep = repeat(lambda: w.evaluate_paged(ctx, judge, nat.POLICY_LEARNED, frames=frames,
+                                                  budget_fraction=frac, mlp=blob_hits, bonus=HYSTERESIS), repeats)
+            out["learned_paged_matching_rayhit_paged"] = {
+                "budget_fraction": frac, "learned_paged_hysteresis": rep,
+                "ray_hit_paged_ms_per_frame_spread": rhp.get("ms_per_frame_spread"),
+                "ray_hit_paged_rel_mse_energy": rhp["rel_mse_energy"],
+                "faster_outside_spread": bool(rep["ms_per_frame_spread"]["max"] < rhp["ms_per_frame_spread"]["min"])}
+        else:
+            out["learned_paged_matching_rayhit_paged"] = None
+        log(f"learned paged matching ray-hit paged: {out['learned_paged_matching_rayhit_paged']}")
     rh, le = out["ray_hit_budget"]["rel_mse_energy"], out["learned"]["rel_mse_energy"]
     out["learned_vs_rayhit_energy_rel_mse_ratio"] = le / rh if rh else None
     out["learned_cost_vs_rayhit_energy_rel_mse_ratio"] = out["learned_cost"]["rel_mse_energy"] / rh if rh else None

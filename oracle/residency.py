@@ -25,9 +25,16 @@ def rayhit_keys(score, hits, visible, memory_pressure):
     return key
 
 
-def select(keys, visible, nbytes, budget, reserve, min_active, current, max_toggles=0, always=False):
+def select(keys, visible, nbytes, budget, reserve, min_active, current, max_toggles=0, always=False,
+           resident_bonus=0.0):
     n = keys.shape[0]
-    k = np.where(np.isfinite(keys), keys, 0.0).astype(np.float32)
+    kk = np.asarray(keys, np.float32).copy()
+    if resident_bonus:
+        # hysteresis: a resident object's key k becomes k + bonus * |k| (float32, no fused ops)
+        m = np.asarray(current).astype(bool)
+        with np.errstate(all="ignore"):
+            kk[m] = kk[m] + np.float32(resident_bonus) * np.abs(kk[m])
+    k = np.where(np.isfinite(kk), kk, 0.0).astype(np.float32)
     if always:
         k = np.ones(n, np.float32)
     order = sorted(range(n), key=lambda i: (-float(k[i]), i))

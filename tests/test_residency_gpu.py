@@ -72,10 +72,16 @@ def _residency_frame(nb, ctx, view):
     return ctx.object_hits().astype(np.int64)
 
 
+@pytest.mark.parametrize("bonus", [0.0, 0.5])
 @pytest.mark.parametrize("sync_toggles", [True, False])
 @pytest.mark.parametrize("policy", [0, 1, 2])
-def test_residency_step_against_oracle(nb, orc, ctx, small_city, policy, sync_toggles):
+def test_residency_step_against_oracle(nb, orc, ctx, small_city, policy, sync_toggles, bonus):
+    """The device step against the restatement over a moving camera; bonus > 0 is the selection's
+    hysteresis (resident keys raised by bonus * |key|)."""
     from oracle import residency as ores
+
+    if policy == 0 and bonus:
+        pytest.skip("AlwaysResident has no keys")
 
     scene, sb = small_city
     ctx.upload(sb)
@@ -84,7 +90,7 @@ def test_residency_step_against_oracle(nb, orc, ctx, small_city, policy, sync_to
     nbytes = ctx.object_bytes()
     budget = int(0.4 * nbytes.sum())
     prm = nb.ResidencyParams.make(policy, budget_bytes=budget, camera_motion=0.5, memory_pressure=0.25,
-                                  min_active=2)
+                                  min_active=2, resident_key_bonus=bonus)
     score = np.zeros(sb.object_count, np.float64)
     flags = np.ones(sb.object_count, np.uint8)
     for frame, pos in enumerate([(0, 60, -180), (20, 50, -150), (40, 45, -120)]):
@@ -102,7 +108,7 @@ def test_residency_step_against_oracle(nb, orc, ctx, small_city, policy, sync_to
             assert np.array_equal(keys, want_keys)
         reserve = ores.reserve_count(sb.object_count, 0.02, 0.06, 0.5)
         want, want_t = ores.select(keys, visible, nbytes, budget, reserve, 2, flags,
-                                   always=(policy == nb.POLICY_ALWAYS))
+                                   always=(policy == nb.POLICY_ALWAYS), resident_bonus=bonus)
         got = ctx.residency_flags()
         assert np.array_equal(got, want), (frame, np.nonzero(got != want)[0][:10])
         assert toggles == (want_t if sync_toggles else None)

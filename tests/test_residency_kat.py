@@ -150,3 +150,18 @@ def test_posterior_known_answers():
     s = f(1000.9)
     assert p.mass[4] == f(64) and p.alpha[4] == s * (f(64) / (s + f(0.9)))
     assert p.beta[4] == f(0.9) * (f(64) / (s + f(0.9)))
+
+
+def test_resident_key_bonus():
+    """The selection's hysteresis (no reference counterpart): a resident object's key k becomes
+    k + bonus * |k|. Keys [5, 4.5, 4, 1], 10 bytes each, budget 20, objects 1 and 2 resident, no
+    reserve: without a bonus objects 0 and 1 are wanted; with bonus 0.3 the resident keys become
+    5.85 and 5.2, both above 5, so 1 and 2 stay and 0 is not brought in."""
+    keys = np.array([5, 4.5, 4, 1], np.float32)
+    nbytes = np.full(4, 10)
+    vis = np.zeros(4, bool)
+    cur = np.array([0, 1, 1, 0], np.uint8)
+    res, t = ores.select(keys, vis, nbytes, 20, 0, 0, cur)
+    assert res.tolist() == [1, 1, 0, 0] and t == 2
+    res, t = ores.select(keys, vis, nbytes, 20, 0, 0, cur, resident_bonus=0.3)
+    assert res.tolist() == [0, 1, 1, 0] and t == 0
