@@ -530,6 +530,7 @@ nomad_status nomad_residency_init(nomad_ctx *ctx) {
   R.primHitsOn = false;
   R.primHitsHost.clear();
   R.primCooldown.clear();
+  R.primStep = 0;
   R.primScore.clear();
   R.primSphere.clear();
   R.primVisible.clear();
@@ -845,8 +846,7 @@ nomad_status rayhit_prim_step(nomad_ctx *ctx, const nomad_residency_params *prm,
   NOMAD_CUDA(ctx, cudaMemsetAsync(R.primHits.p, 0, (size_t)P * 4, ctx->stream));
   NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   for (uint32_t i = 0; i < P; ++i) R.primScore[i] = R.primScore[i] * prm->hit_decay + (float)R.primHitsHost[i];
-  for (uint32_t &c : R.primCooldown)
-    if (c > 0) --c;
+  ++R.primStep;  // every primitive cooldown counts down by one
   *toggled = 0;
   if (R.primRebuild > 0) {
     --R.primRebuild;
@@ -900,14 +900,14 @@ nomad_status rayhit_prim_step(nomad_ctx *ctx, const nomad_residency_params *prm,
     const bool want = desired[i] != 0;
     if (want == (ctx->primActive[i] != 0)) continue;
     if (!unlimited) {
-      if (R.primCooldown[i] > 0) continue;
+      if (R.primCooldown[i] > R.primStep) continue;
       if (toggles >= budget) break;
     }
     int32_t changed = 0;
     nomad_status st = nomad_residency_set_primitive_active(ctx, i, want ? 1 : 0, &changed);
     if (st != NOMAD_OK) return st;
     if (changed) {
-      R.primCooldown[i] = prm->state_cooldown;
+      R.primCooldown[i] = R.primStep + prm->state_cooldown;
       ++toggles;
     }
   }
@@ -918,7 +918,7 @@ nomad_status rayhit_prim_step(nomad_ctx *ctx, const nomad_residency_params *prm,
     nomad_status st = nomad_residency_set_primitive_active(ctx, order[0], 1, &changed);
     if (st != NOMAD_OK) return st;
     if (changed) {
-      R.primCooldown[order[0]] = prm->state_cooldown;
+      R.primCooldown[order[0]] = R.primStep + prm->state_cooldown;
       ++toggles;
     }
   }
@@ -1120,8 +1120,7 @@ nomad_status screen_space_step(nomad_ctx *ctx, const nomad_residency_params *prm
   if (R.primCooldown.size() != P) R.primCooldown.assign(P, 0);
   for (uint32_t &c : R.objCooldown)
     if (c > 0) --c;
-  for (uint32_t &c : R.primCooldown)
-    if (c > 0) --c;
+  ++R.primStep;  // every primitive cooldown counts down by one
   const float motion = clamp_unit(prm->camera_motion), pressure = clamp_unit(prm->memory_pressure);
   const float frac = std::min(std::max(prm->target_fraction + 0.08f * motion - 0.10f * pressure, 0.50f), 0.94f);
   const size_t budget = std::max<size_t>(
@@ -1175,10 +1174,10 @@ nomad_status screen_space_step(nomad_ctx *ctx, const nomad_residency_params *prm
     const nomad_instance_record &ir = ctx->instances[g];
     bool blocked = false;
     for (uint32_t p = ir.primitive_base; p < ir.primitive_base + ir.primitive_count && !blocked; ++p)
-      if ((ctx->primActive[p] != 0) != want && R.primCooldown[p] > 0) blocked = true;
+      if ((ctx->primActive[p] != 0) != want && R.primCooldown[p] > R.primStep) blocked = true;
     if (blocked) continue;
     for (uint32_t p = ir.primitive_base; p < ir.primitive_base + ir.primitive_count; ++p)
-      if ((ctx->primActive[p] != 0) != want) R.primCooldown[p] = prm->state_cooldown;
+      if ((ctx->primActive[p] != 0) != want) R.primCooldown[p] = R.primStep + prm->state_cooldown;
     uint32_t n = 0;
     nomad_status st = nomad_residency_set_object_active(ctx, g, want ? 1 : 0, &n);
     if (st != NOMAD_OK) return st;
@@ -1269,7 +1268,8 @@ extern "C" nomad_status nomad_residency_prim_state(nomad_ctx *ctx, uint32_t *hit
     NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }
   if (scores) std::memcpy(scores, R.primScore.data(), P * 4);
-  if (cooldowns) std::memcpy(cooldowns, R.primCooldown.data(), P * 4);
+  if (cooldowns)
+    for (size_t i = 0; i < P; ++i) cooldowns[i] = R.primCooldown[i] > R.primStep ? R.primCooldown[i] - R.primStep : 0u;
   if (visible) std::memcpy(visible, R.primVisible.data(), P);
   if (active) {
     nomad_status hs = nomad_residency_sync_host(ctx);

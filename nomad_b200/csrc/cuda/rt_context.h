@@ -109,6 +109,8 @@ struct nomad_ctx {
   // normal resolves to, or a sphere's center, and bits(material index | type << 30)) and the
   // distinct 80-byte material records they index (nomad_build_shade_records).
   DeviceBuf shadeRec, matTable;
+  DeviceBuf patchPrims;          // changed primitives of a flush (k_set_prim_act)
+  bool objTestsSmemSet = false;  // k_object_tests opted in to 64 KB of dynamic shared memory
   uint32_t matCount = 0;
   DeviceBuf objHits, status, cursor;
   DeviceBuf stageIn, stageOut, stageAux;  // host-pointer staging
@@ -150,7 +152,12 @@ struct nomad_ctx {
     // path tracer once enabled) and the host-side state of the reference's policy
     bool primHitsOn = false;
     DeviceBuf primHits;
-    std::vector<uint32_t> primHitsHost, primCooldown;
+    std::vector<uint32_t> primHitsHost;
+    // Per-primitive cooldowns of the per-primitive ray-hit and ScreenSpace policies, stored as the
+    // step at which they run out: a primitive is cooling while primCooldown[p] > primStep, and
+    // each step of either policy advances primStep instead of decrementing every counter.
+    std::vector<uint32_t> primCooldown;
+    uint32_t primStep = 0;
     std::vector<float> primScore;
     std::vector<float> primSphere;  // centre xyz, radius per primitive
     std::vector<uint8_t> primVisible;

@@ -113,41 +113,61 @@ __global__ void __launch_bounds__(kBlock) k_work(DevScene S, const float4 *__res
 // leaf left = -(object + 1)) the ray segment [1e-4, t of its closest hit] enters, infinite for a
 // miss. A node's box contains its children's, and the slab test is monotone under containment,
 // so walking the TLAS and pruning failed boxes finds exactly the leaves whose own box passes:
-// the count does not depend on any traversal order. One thread per ray; a warp's lanes that
-// count the same object add once.
+// the count does not depend on any traversal order. Each thread walks its rays in a grid-stride
+// loop.
 constexpr int kTlasStack = 64;
 
 __global__ void __launch_bounds__(kBlock) k_object_tests(const float4 *__restrict__ tlas, const float4 *__restrict__ rays,
                                                          const int32_t *__restrict__ hits5, uint64_t n,
                                                          const uint32_t *__restrict__ lenDev,
-                                                         const uint8_t *__restrict__ resident,
+                                                         const uint8_t *__restrict__ resident, uint32_t objects,
                                                          uint32_t *__restrict__ tests, uint32_t *__restrict__ status) {
+  // Counts go to a per-block histogram in shared memory when it fits (one bin per object), and the
+  // block adds its non-zero bins to the global counts once at the end: a ray enters a handful of
+  // object boxes, and the popular objects would otherwise serialise on global atomics.
+  extern __shared__ uint32_t hist[];
+  const bool local = objects > 0;
+  if (local) {
+    for (uint32_t o = threadIdx.x; o < objects; o += blockDim.x) hist[o] = 0;
+    __syncthreads();
+  }
   const uint64_t N = lenDev ? (uint64_t)*lenDev : n;
-  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
-  const float4 a = __ldg(rays + 2 * i), b = __ldg(rays + 2 * i + 1);
-  const RayP r = prep_ray(a, b);
-  const float bound = __int_as_float(hits5[5 * i + 2]);
-  int32_t stack[kTlasStack];
-  int sp = 0;
-  stack[sp++] = 0;
-  while (sp > 0) {
-    const int32_t node = stack[--sp];
-    const float4 lo = __ldg(tlas + 2 * node), hi = __ldg(tlas + 2 * node + 1);
-    float tn;
-    if (!slab(r, lo.x, lo.y, lo.z, hi.x, hi.y, hi.z, bound, tn)) continue;
-    const int32_t left = __float_as_int(lo.w), right = __float_as_int(hi.w);
-    if (left < 0) {
-      const int32_t obj = -(left + 1);
-      if (resident[obj]) atomicAdd(tests + obj, 1u);
-      continue;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
+    const float4 a = __ldg(rays + 2 * i), b = __ldg(rays + 2 * i + 1);
+    const RayP r = prep_ray(a, b);
+    const float bound = __int_as_float(hits5[5 * i + 2]);
+    int32_t stack[kTlasStack];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp > 0) {
+      const int32_t node = stack[--sp];
+      const float4 lo = __ldg(tlas + 2 * node), hi = __ldg(tlas + 2 * node + 1);
+      float tn;
+      if (!slab(r, lo.x, lo.y, lo.z, hi.x, hi.y, hi.z, bound, tn)) continue;
+      const int32_t left = __float_as_int(lo.w), right = __float_as_int(hi.w);
+      if (left < 0) {
+        const int32_t obj = -(left + 1);
+        if (resident[obj]) {
+          if (local)
+            atomicAdd(&hist[obj], 1u);
+          else
+            atomicAdd(&tests[obj], 1u);
+        }
+        continue;
+      }
+      if (sp + 2 > kTlasStack) {
+        atomicOr(status, kStatusStackOverflow);
+        continue;
+      }
+      stack[sp++] = right;
+      stack[sp++] = left;
     }
-    if (sp + 2 > kTlasStack) {
-      atomicOr(status, kStatusStackOverflow);
-      continue;
-    }
-    stack[sp++] = right;
-    stack[sp++] = left;
+  }
+  if (local) {
+    __syncthreads();
+    for (uint32_t o = threadIdx.x; o < objects; o += blockDim.x)
+      if (hist[o]) atomicAdd(tests + o, hist[o]);
   }
 }
 
@@ -163,6 +183,13 @@ __global__ void k_patch_wide(int32_t *__restrict__ arena, size_t base, uint32_t 
 }
 
 // Residency patches: word offsets into the layout arena and their new values.
+// Device primitive-activity flags from a list of changed primitives: bit 31 the new state, bits
+// 0-30 the primitive.
+__global__ void k_set_prim_act(uint8_t *__restrict__ act, const uint32_t *__restrict__ list, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) act[list[i] & 0x7fffffffu] = (uint8_t)(list[i] >> 31);
+}
+
 __global__ void k_patch(int32_t *__restrict__ arena, const int64_t *__restrict__ offs,
                         const int32_t *__restrict__ vals, uint32_t n) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -379,17 +406,11 @@ extern "C" nomad_status nomad_scene_upload(nomad_ctx *ctx, const float *bvh, uin
   return NOMAD_OK;
 }
 
-extern "C" nomad_status nomad_residency_set_primitive_active(nomad_ctx *ctx, uint32_t prim,
-                                                             int32_t active, int32_t *changed) {
-  if (!ctx || !ctx->sceneReady) return NOMAD_ERR_NOT_READY;
-  {
-    nomad_status hs = nomad_residency_sync_host(ctx);
-    if (hs != NOMAD_OK) return hs;
-  }
-  if (changed) *changed = 0;
-  if (prim >= ctx->primCount) return fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "primitive out of range");
-  uint8_t a = active ? 1 : 0;
-  if (ctx->primActive[prim] == a) return NOMAD_OK;
+namespace {
+// setPrimitiveActive's bookkeeping for one primitive (the host mirror is current, the index valid);
+// returns whether its state changed.
+bool toggle_primitive(nomad_ctx *ctx, uint32_t prim, uint8_t a) {
+  if (ctx->primActive[prim] == a) return false;
   ctx->primActive[prim] = a;
   uint32_t o = static_cast<uint32_t>(ctx->layout.primObject[prim]);
   if (a)
@@ -404,6 +425,20 @@ extern "C" nomad_status nomad_residency_set_primitive_active(nomad_ctx *ctx, uin
     ctx->objDirtyFlag[o] = 1;
     ctx->dirtyObjs.push_back(o);
   }
+  return true;
+}
+}  // namespace
+
+extern "C" nomad_status nomad_residency_set_primitive_active(nomad_ctx *ctx, uint32_t prim,
+                                                             int32_t active, int32_t *changed) {
+  if (!ctx || !ctx->sceneReady) return NOMAD_ERR_NOT_READY;
+  {
+    nomad_status hs = nomad_residency_sync_host(ctx);
+    if (hs != NOMAD_OK) return hs;
+  }
+  if (changed) *changed = 0;
+  if (prim >= ctx->primCount) return fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "primitive out of range");
+  if (!toggle_primitive(ctx, prim, active ? 1 : 0)) return NOMAD_OK;
   if (changed) *changed = 1;
   return NOMAD_OK;
 }
@@ -419,11 +454,8 @@ extern "C" nomad_status nomad_residency_set_object_active(nomad_ctx *ctx, uint32
   if (obj >= ctx->objectCount) return fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "object out of range");
   const nomad_instance_record &r = ctx->instances[obj];
   uint32_t n = 0;
-  for (uint32_t p = r.primitive_base; p < r.primitive_base + r.primitive_count; ++p) {
-    int32_t ch = 0;
-    nomad_residency_set_primitive_active(ctx, p, active, &ch);
-    n += ch;
-  }
+  for (uint32_t p = r.primitive_base; p < r.primitive_base + r.primitive_count; ++p)
+    n += toggle_primitive(ctx, p, active ? 1 : 0) ? 1u : 0u;
   // An object toggled with no primitive change still gets its instance record refreshed.
   if (!ctx->objDirtyFlag[obj]) {
     ctx->objDirtyFlag[obj] = 1;
@@ -446,8 +478,11 @@ extern "C" nomad_status nomad_residency_flush(nomad_ctx *ctx) {
     nomad_status ps = nomad_paging_order(ctx);
     if (ps != NOMAD_OK) return ps;
   }
+  std::vector<uint32_t> primList;  // changed primitives for the device activity flags
+  primList.reserve(ctx->dirtyPrims.size());
   for (uint32_t p : ctx->dirtyPrims) {
     ctx->primDirtyFlag[p] = 0;
+    primList.push_back(p | (ctx->primActive[p] ? 0x80000000u : 0u));
     int64_t pos = L.primPos[p];
     const int32_t word = ctx->primActive[p] ? (int32_t)p : ~(int32_t)p;
     if (ctx->paging) {
@@ -480,12 +515,35 @@ extern "C" nomad_status nomad_residency_flush(nomad_ctx *ctx) {
   ctx->dirtyPrims.clear();
   ctx->dirtyObjs.clear();
   if (mirror) {
-    nomad_status mst = nomad_residency_mirror(ctx);
+    nomad_status mst;
+    if ((uint64_t)primList.size() * 16 < ctx->primCount) {
+      // few changes: the object flags whole, the primitive flags by a scatter of the changed ones
+      // (a full copy moves one byte per primitive of the scene)
+      auto &R = ctx->res;
+      NOMAD_CUDA(ctx, cudaMemcpyAsync(R.objRes.p, ctx->objResident.data(), ctx->objectCount, cudaMemcpyHostToDevice,
+                                      ctx->stream));
+      if (!primList.empty()) {
+        NOMAD_CUDA(ctx, ctx->patchPrims.reserve(primList.size() * 4));
+        NOMAD_CUDA(ctx, cudaMemcpyAsync(ctx->patchPrims.p, primList.data(), primList.size() * 4,
+                                        cudaMemcpyHostToDevice, ctx->stream));
+        const uint32_t n = (uint32_t)primList.size();
+        k_set_prim_act<<<(n + 255) / 256, 256, 0, ctx->stream>>>(R.primAct.as<uint8_t>(),
+                                                                 ctx->patchPrims.as<const uint32_t>(), n);
+        NOMAD_CUDA(ctx, cudaGetLastError());
+      }
+      ctx->frame.lightsDirty = true;
+      mst = NOMAD_OK;
+    } else {
+      mst = nomad_residency_mirror(ctx);
+    }
     if (mst != NOMAD_OK) return mst;
     mst = nomad_patch_wide(ctx);
     if (mst != NOMAD_OK) return mst;
   }
-  if (offs.empty()) return NOMAD_OK;
+  if (offs.empty()) {
+    NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // primList leaves scope
+    return NOMAD_OK;
+  }
   NOMAD_CUDA(ctx, ctx->patchOffs.reserve(offs.size() * 8));
   NOMAD_CUDA(ctx, ctx->patchVals.reserve(vals.size() * 4));
   // Synchronous copies: the host vectors go out of scope at return.
@@ -864,10 +922,18 @@ nomad_status nomad_count_object_tests(nomad_ctx *ctx, const float4 *rays, const 
                                       const uint32_t *lenDev) {
   auto &R = ctx->res;
   if (!R.testsOn || n == 0 || R.tlasCount == 0) return NOMAD_OK;
-  const uint64_t blocks = (n + kBlock - 1) / kBlock;
-  k_object_tests<<<(unsigned)blocks, kBlock, 0, ctx->stream>>>(R.tlas.as<const float4>(), rays, hits5, n, lenDev,
-                                                               R.objRes.as<const uint8_t>(), R.tests.as<uint32_t>(),
-                                                               ctx->status.as<uint32_t>());
+  // a grid-stride launch of a few blocks per SM, each with a histogram of every object (at most
+  // 16,384 objects: 64 KB of shared memory; larger scenes count straight into global memory)
+  const uint32_t objects = ctx->objectCount <= 16384 ? ctx->objectCount : 0u;
+  const size_t smem = (size_t)objects * 4;
+  if (smem > 48 * 1024 && !ctx->objTestsSmemSet) {
+    NOMAD_CUDA(ctx, cudaFuncSetAttribute(k_object_tests, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+    ctx->objTestsSmemSet = true;
+  }
+  const uint64_t blocks = std::min<uint64_t>((n + kBlock - 1) / kBlock, (uint64_t)ctx->smCount * 8);
+  k_object_tests<<<(unsigned)std::max<uint64_t>(blocks, 1), kBlock, smem, ctx->stream>>>(
+      R.tlas.as<const float4>(), rays, hits5, n, lenDev, R.objRes.as<const uint8_t>(), objects,
+      R.tests.as<uint32_t>(), ctx->status.as<uint32_t>());
   NOMAD_CUDA(ctx, cudaGetLastError());
   return NOMAD_OK;
 }
