@@ -149,6 +149,17 @@ __device__ __forceinline__ Material decode_material(const float4 *__restrict__ m
   return o;
 }
 
+// The shading records and the material table, as the ReSTIR passes read them: a primitive's
+// material is the table entry its record names (bits 0-29 of the record's w).
+struct ShadeTables {
+  const float4 *__restrict__ rec;
+  const float4 *__restrict__ mat;
+};
+
+__device__ __forceinline__ Material prim_material(const ShadeTables &T, int32_t prim, float lod) {
+  return decode_material(T.mat, (int32_t)(__float_as_uint(__ldg(T.rec + prim).w) & 0x3fffffffu), lod);
+}
+
 // Geometric normal at a hit, as firstHitBVH sets intersection.normal before the front-face flip
 // (triangle :779-806, rectangle :853-863, sphere :766). For triangles and rectangles it does not
 // depend on the hit point: surface_normal computes it from the primitive record alone.
@@ -171,14 +182,6 @@ __device__ __forceinline__ V3 surface_normal(int type, float4 p0, float4 p1, flo
   fb = (fl > kRayEps && finite3(fb)) ? normalize(fb) : v3(0.0f, 1.0f, 0.0f);
   float sl = dot(sn, sn);
   return (sl > kRayEps && finite3(sn)) ? normalize(sn) : fb;
-}
-
-__device__ __forceinline__ V3 hit_normal(const float4 *__restrict__ prims, int32_t prim, V3 p) {
-  const float4 *g = prims + 7ll * prim;
-  float4 p0 = __ldg(g);
-  int type = (int)p0.w;
-  if (type == 1 || type == 2) return surface_normal(type, p0, __ldg(g + 1), __ldg(g + 2), __ldg(g + 6));
-  return normalize(p - ld3(p0));
 }
 
 // The compact shading record of a primitive: (normal, bits(material | type << 30)) for
@@ -964,7 +967,7 @@ __device__ __forceinline__ Resv resv_empty() {
 }
 
 // Unoccluded area-measure integrand at surface s for light point y; returns the target.
-__device__ __forceinline__ float restir_target(const float4 *__restrict__ mats, const Material &m, const Surf &s,
+__device__ __forceinline__ float restir_target(const ShadeTables mats, const Material &m, const Surf &s,
                                                V3 lpos, V3 lnrm, int32_t lp, V3 &fa, V3 &wi, float &dist) {
   fa = v3(0.0f, 0.0f, 0.0f);
   if (lp < 0 || lp == __float_as_int(s.n.w)) return 0.0f;
@@ -976,7 +979,7 @@ __device__ __forceinline__ float restir_target(const float4 *__restrict__ mats, 
   wi = toL / dist;
   float cosT = fmax_ref(dot(n, wi), 0.0f), cosL = fmax_ref(dot(lnrm, -wi), 0.0f);
   if (cosT <= 0.0f || cosL <= 0.0f) return 0.0f;
-  Material lm = decode_material(mats, lp, 1.0f);
+  Material lm = prim_material(mats, lp, 1.0f);
   V3 lrad = lm.emission * lm.power;
   V3 f = eval_bsdf(m, n, ld3(s.v), wi) * lrad * cosT;
   float g = cosL / fmax_ref(dist2, kRayEps);
@@ -1017,7 +1020,7 @@ __device__ __forceinline__ bool restir_gate(const Surf &s, const Surf &q) {
 
 // Adds a reused reservoir to `out` (the owner surface s, material m).
 __device__ __forceinline__ void restir_merge(Resv &out, const Resv &src, const Surf &s, const Material &m,
-                                             const float4 *__restrict__ mats, float capM, float u) {
+                                             const ShadeTables mats, float capM, float u) {
   int32_t lp = __float_as_int(src.a.w);
   if (lp < 0 || !(src.c.z > 0.0f) || !(src.c.y > 0.0f) || !(src.c.w > 0.0f)) return;
   float Mp = fmin_ref(src.c.z, capM);
@@ -1039,8 +1042,8 @@ __device__ __forceinline__ void restir_merge(Resv &out, const Resv &src, const S
 // every candidate binary-searches it, 32 per path.
 __global__ void __launch_bounds__(kPtBlock, NOMAD_PT_MINB) k_restir_initial(
     const ViewDev *__restrict__ views, uint32_t nviews, unsigned long long P, RestirDev cfg,
-    const float4 *__restrict__ rays, const int32_t *__restrict__ hits, const float4 *__restrict__ prims,
-    const float4 *__restrict__ mats, Lights L, Resv *__restrict__ rOut, Surf *__restrict__ sOut, uint32_t cdfCap) {
+    const float4 *__restrict__ rays, const int32_t *__restrict__ hits,
+    const ShadeTables mats, Lights L, Resv *__restrict__ rOut, Surf *__restrict__ sOut, uint32_t cdfCap) {
   extern __shared__ float sCdf[];
   const uint32_t lightCount = L.meta->count;
   const float lightTotal = L.meta->total;
@@ -1060,9 +1063,9 @@ __global__ void __launch_bounds__(kPtBlock, NOMAD_PT_MINB) k_restir_initial(
       float t = __int_as_float(h[2]);
       V3 o = ld3(rays[2 * pid]), d = ld3(rays[2 * pid + 1]);
       V3 p = v3(o.x + t * d.x, o.y + t * d.y, o.z + t * d.z);
-      V3 n = hit_normal(prims, prim, p);
+      V3 n = record_normal(__ldg(mats.rec + prim), p);
       if (!(dot(n, d) < 0.0f)) n = -n;
-      Material m = decode_material(mats, prim, v.lod);
+      Material m = prim_material(mats, prim, v.lod);
       if (luminance(m.diffuse * m.opacity) > 0.0f) {
         V3 vd = normalize(-d);
         s.p = make_float4(p.x, p.y, p.z, length(p - o));
@@ -1104,7 +1107,7 @@ __global__ void __launch_bounds__(kPtBlock, NOMAD_PT_MINB) k_restir_initial(
 
 __global__ void __launch_bounds__(kPtBlock) k_restir_temporal(
     const ViewDev *__restrict__ views, const ViewDev *__restrict__ prevViews, uint32_t nviews,
-    unsigned long long P, RestirDev cfg, const float4 *__restrict__ mats, const Resv *__restrict__ rIn,
+    unsigned long long P, RestirDev cfg, const ShadeTables mats, const Resv *__restrict__ rIn,
     const Surf *__restrict__ sCur, const Resv *__restrict__ rPrev, const Surf *__restrict__ sPrev,
     Resv *__restrict__ rOut, int usePrev) {
   for (unsigned long long pid = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; pid < P;
@@ -1132,7 +1135,7 @@ __global__ void __launch_bounds__(kPtBlock) k_restir_temporal(
             uint32_t pixel = (uint32_t)(local / v.spp), sample = (uint32_t)(local % v.spp);
             unsigned long long ppid = pv.pathOffset + ((unsigned long long)py * pv.w + px) * pv.spp + sample;
             if (restir_gate(s, sPrev[ppid])) {
-              Material m = decode_material(mats, __float_as_int(s.n.w), v.lod);
+              Material m = prim_material(mats, __float_as_int(s.n.w), v.lod);
               U4 rr = philox(U4{pixel, sample, 0x20000u, v.index}, v.k0, v.k1);
               restir_merge(out, rPrev[ppid], s, m, mats, cfg.capM * (float)cfg.candidates, u01(rr.x));
             }
@@ -1146,7 +1149,7 @@ __global__ void __launch_bounds__(kPtBlock) k_restir_temporal(
 
 __global__ void __launch_bounds__(kPtBlock, NOMAD_PT_MINB) k_restir_spatial(
     const ViewDev *__restrict__ views, uint32_t nviews, unsigned long long P, RestirDev cfg,
-    const float4 *__restrict__ mats, const Resv *__restrict__ rIn, const Surf *__restrict__ sCur,
+    const ShadeTables mats, const Resv *__restrict__ rIn, const Surf *__restrict__ sCur,
     Resv *__restrict__ rOut) {
   for (unsigned long long pid = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; pid < P;
        pid += (unsigned long long)gridDim.x * blockDim.x) {
@@ -1157,7 +1160,7 @@ __global__ void __launch_bounds__(kPtBlock, NOMAD_PT_MINB) k_restir_spatial(
       unsigned long long local = pid - v.pathOffset;
       uint32_t pixel = (uint32_t)(local / v.spp), sample = (uint32_t)(local % v.spp);
       int px = (int)(pixel % v.w), py = (int)(pixel / v.w);
-      Material m = decode_material(mats, __float_as_int(s.n.w), v.lod);
+      Material m = prim_material(mats, __float_as_int(s.n.w), v.lod);
       for (uint32_t k = 0; k < cfg.spatial; ++k) {
         U4 rr = philox(U4{pixel, sample, 0x30000u + k, v.index}, v.k0, v.k1);
         float rad = cfg.radius * sqrtf(u01(rr.x));
@@ -1175,7 +1178,7 @@ __global__ void __launch_bounds__(kPtBlock, NOMAD_PT_MINB) k_restir_spatial(
 }
 
 __global__ void __launch_bounds__(kPtBlock) k_restir_shade(
-    const ViewDev *__restrict__ views, uint32_t nviews, unsigned long long P, const float4 *__restrict__ mats,
+    const ViewDev *__restrict__ views, uint32_t nviews, unsigned long long P, const ShadeTables mats,
     const Resv *__restrict__ rIn, const Surf *__restrict__ sCur, float4 *__restrict__ sRays,
     uint32_t *__restrict__ sIds, float4 *__restrict__ sContrib, Counters *cnt) {
   unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
@@ -1190,7 +1193,7 @@ __global__ void __launch_bounds__(kPtBlock) k_restir_shade(
       int32_t lp = __float_as_int(r.a.w);
       if (s.v.w > 0.0f && lp >= 0 && r.c.z > 0.0f && r.c.y > 0.0f && r.c.w > 0.0f) {
         const ViewDev &v = find_view(views, nviews, pid);
-        Material m = decode_material(mats, __float_as_int(s.n.w), v.lod);
+        Material m = prim_material(mats, __float_as_int(s.n.w), v.lod);
         V3 fa, wi;
         float dist = 0.0f;
         float ph = restir_target(mats, m, s, ld3(r.a), ld3(r.b), lp, fa, wi, dist);
@@ -1289,11 +1292,11 @@ __device__ __forceinline__ bool ref_new_candidate(const Surf &s, const Material 
 }
 
 // A candidate rebuilt from a stored reservoir sample.
-__device__ __forceinline__ bool ref_stored_candidate(const Surf &s, const Material &m, const float4 *__restrict__ mats,
+__device__ __forceinline__ bool ref_stored_candidate(const Surf &s, const Material &m, const ShadeTables mats,
                                                      const RefArgs &ra, const Resv &src, RefCand &c) {
   const int32_t lp = __float_as_int(src.a.w);
   if (!(src.b.w > 0.0f) || lp == __float_as_int(s.n.w) || lp < 0 || (uint32_t)lp >= ra.primCount) return false;
-  const Material lm = decode_material(mats, lp, 1.0f);
+  const Material lm = prim_material(mats, lp, 1.0f);
   return ref_geometry(s, m, ld3(src.a), ld3(src.b), src.b.w, ra.lightPdf[lp], lm.emission * lm.power, lp, c);
 }
 
@@ -1354,7 +1357,7 @@ __device__ __forceinline__ long long ref_neighbour(const ViewDev &v, const ViewD
 
 // Reuse candidate k of a path: the prior reservoir it comes from and the rebuilt candidate.
 __device__ __forceinline__ bool ref_reuse_candidate(uint32_t k, const ViewDev &v, const ViewDev &pv, const Surf &s,
-                                                    const Material &m, const float4 *__restrict__ mats,
+                                                    const Material &m, const ShadeTables mats,
                                                     const RefArgs &ra, const Resv *__restrict__ rPrev,
                                                     const Surf *__restrict__ sPrev, uint32_t pixel, uint32_t sample,
                                                     Resv &q, long long &qid, bool &prevValid, RefCand &c) {
@@ -1369,8 +1372,8 @@ __device__ __forceinline__ bool ref_reuse_candidate(uint32_t k, const ViewDev &v
 
 __global__ void __launch_bounds__(kPtBlock, NOMAD_PT_MINB) k_restir_ref_cand(
     const ViewDev *__restrict__ views, uint32_t nviews, unsigned long long P, RestirDev cfg,
-    const float4 *__restrict__ rays, const int32_t *__restrict__ hits, const float4 *__restrict__ prims,
-    const float4 *__restrict__ mats, Lights L, Surf *__restrict__ sOut, uint32_t *__restrict__ mask, RefArgs ra,
+    const float4 *__restrict__ rays, const int32_t *__restrict__ hits,
+    const ShadeTables mats, Lights L, Surf *__restrict__ sOut, uint32_t *__restrict__ mask, RefArgs ra,
     float4 *__restrict__ qRays, uint32_t *__restrict__ qIds, Counters *cnt) {
   const uint32_t lightCount = L.meta->count;
   const float lightTotal = L.meta->total;
@@ -1392,9 +1395,9 @@ __global__ void __launch_bounds__(kPtBlock, NOMAD_PT_MINB) k_restir_ref_cand(
         float t = __int_as_float(h[2]);
         V3 o = ld3(rays[2 * pid]), d = ld3(rays[2 * pid + 1]);
         V3 p = v3(o.x + t * d.x, o.y + t * d.y, o.z + t * d.z);
-        V3 n = hit_normal(prims, prim, p);
+        V3 n = record_normal(__ldg(mats.rec + prim), p);
         if (!(dot(n, d) < 0.0f)) n = -n;
-        m = decode_material(mats, prim, v.lod);
+        m = prim_material(mats, prim, v.lod);
         if (luminance(m.diffuse * m.opacity) > 0.0f) {
           V3 vd = normalize(-d);
           s.p = make_float4(p.x, p.y, p.z, length(p - o));
@@ -1448,7 +1451,7 @@ __global__ void k_restir_ref_reset(Counters *cnt) {
 
 __global__ void __launch_bounds__(kPtBlock, NOMAD_PT_MINB) k_restir_ref_reuse(
     const ViewDev *__restrict__ views, const ViewDev *__restrict__ prevViews, uint32_t nviews, unsigned long long P,
-    RestirDev cfg, const float4 *__restrict__ mats, Lights L, const Surf *__restrict__ sCur,
+    RestirDev cfg, const ShadeTables mats, Lights L, const Surf *__restrict__ sCur,
     const uint32_t *__restrict__ candMask, RefArgs ra, const Resv *__restrict__ rPrev, const Surf *__restrict__ sPrev,
     int usePrev, Resv *__restrict__ rMid, float4 *__restrict__ midContrib, uint32_t *__restrict__ reuseMask,
     float4 *__restrict__ qRays, uint32_t *__restrict__ qIds, Counters *cnt) {
@@ -1473,7 +1476,7 @@ __global__ void __launch_bounds__(kPtBlock, NOMAD_PT_MINB) k_restir_ref_reuse(
       Resv r = resv_empty();
       V3 contrib = v3(0.0f, 0.0f, 0.0f);
       if (s.v.w > 0.0f) {
-        m = decode_material(mats, __float_as_int(s.n.w), v.lod);
+        m = prim_material(mats, __float_as_int(s.n.w), v.lod);
         for (uint32_t c = 0; c < cfg.candidates; ++c) {
           if (!((candMask[pid * ra.words + c / 32] >> (c % 32)) & 1u)) continue;
           const U4 u = philox(U4{pixel, sample, 0x10000u + c, v.index}, v.k0, v.k1);
@@ -1513,7 +1516,7 @@ __global__ void __launch_bounds__(kPtBlock, NOMAD_PT_MINB) k_restir_ref_reuse(
 
 __global__ void __launch_bounds__(kPtBlock, NOMAD_PT_MINB) k_restir_ref_final(
     const ViewDev *__restrict__ views, const ViewDev *__restrict__ prevViews, uint32_t nviews, unsigned long long P,
-    const float4 *__restrict__ mats, const Surf *__restrict__ sCur, RefArgs ra, const Resv *__restrict__ rPrev,
+    const ShadeTables mats, const Surf *__restrict__ sCur, RefArgs ra, const Resv *__restrict__ rPrev,
     const Surf *__restrict__ sPrev, int usePrev, const Resv *__restrict__ rMid, const float4 *__restrict__ midContrib,
     const uint32_t *__restrict__ reuseMask, Resv *__restrict__ rOut, float4 *__restrict__ sRays,
     uint32_t *__restrict__ sIds, float4 *__restrict__ sContrib, Counters *cnt) {
@@ -1530,7 +1533,7 @@ __global__ void __launch_bounds__(kPtBlock, NOMAD_PT_MINB) k_restir_ref_final(
         const ViewDev &v = find_view(views, nviews, pid);
         const unsigned long long local = pid - v.pathOffset;
         const uint32_t pixel = (uint32_t)(local / v.spp), sample = (uint32_t)(local % v.spp);
-        const Material m = decode_material(mats, __float_as_int(s.n.w), v.lod);
+        const Material m = prim_material(mats, __float_as_int(s.n.w), v.lod);
         const float4 mc = midContrib[pid];
         V3 contrib = v3(mc.x, mc.y, mc.z);
         const float currentM = r.c.z;
@@ -1692,8 +1695,8 @@ nomad_status restir_launch(nomad_ctx *ctx, uint32_t nviews, unsigned long long P
     const ViewDev *PV = F.prevViews.as<const ViewDev>();
     k_restir_ref_reset<<<1, 1, 0, s>>>(C);
     k_restir_ref_cand<<<grid, kPtBlock, 0, s>>>(V, nviews, P, cfg, F.qRays[0].as<const float4>(),
-                                               F.hits.as<const int32_t>(), ctx->prims.as<const float4>(),
-                                               ctx->materials.as<const float4>(), L, sCur, F.refMask.as<uint32_t>(), ra,
+                                               F.hits.as<const int32_t>(),
+                                               ShadeTables{ctx->shadeRec.as<const float4>(), ctx->matTable.as<const float4>()}, L, sCur, F.refMask.as<uint32_t>(), ra,
                                                F.refRays.as<float4>(), F.refIds.as<uint32_t>(), C);
     NOMAD_CUDA(ctx, cudaGetLastError());
     nomad_status ts = nomad_trace_variant(ctx, ctx->trav, true, F.refRays.as<const float4>(), P * cf.candidates,
@@ -1702,7 +1705,7 @@ nomad_status restir_launch(nomad_ctx *ctx, uint32_t nviews, unsigned long long P
     k_restir_ref_vis<<<grid, kPtBlock, 0, s>>>(F.refIds.as<const uint32_t>(), F.refOcc.as<const uint8_t>(),
                                               cf.candidates, ra.words, F.refMask.as<uint32_t>(), C);
     k_restir_ref_reset<<<1, 1, 0, s>>>(C);
-    k_restir_ref_reuse<<<grid, kPtBlock, 0, s>>>(V, PV, nviews, P, cfg, ctx->materials.as<const float4>(), L, sCur,
+    k_restir_ref_reuse<<<grid, kPtBlock, 0, s>>>(V, PV, nviews, P, cfg, ShadeTables{ctx->shadeRec.as<const float4>(), ctx->matTable.as<const float4>()}, L, sCur,
                                                 F.refMask.as<const uint32_t>(), ra, F.resv[cur ^ 1].as<const Resv>(),
                                                 F.surf[cur ^ 1].as<const Surf>(), plan.temporal, F.rInit.as<Resv>(),
                                                 F.refContrib.as<float4>(), F.reuseMask.as<uint32_t>(),
@@ -1714,7 +1717,7 @@ nomad_status restir_launch(nomad_ctx *ctx, uint32_t nviews, unsigned long long P
     k_restir_ref_vis5<<<grid, kPtBlock, 0, s>>>(F.refIds.as<const uint32_t>(), F.refOcc.as<const uint8_t>(),
                                                F.reuseMask.as<uint32_t>(), C);
     k_restir_ref_reset<<<1, 1, 0, s>>>(C);
-    k_restir_ref_final<<<grid, kPtBlock, 0, s>>>(V, PV, nviews, P, ctx->materials.as<const float4>(), sCur, ra,
+    k_restir_ref_final<<<grid, kPtBlock, 0, s>>>(V, PV, nviews, P, ShadeTables{ctx->shadeRec.as<const float4>(), ctx->matTable.as<const float4>()}, sCur, ra,
                                                 F.resv[cur ^ 1].as<const Resv>(), F.surf[cur ^ 1].as<const Surf>(),
                                                 plan.temporal, F.rInit.as<const Resv>(), F.refContrib.as<const float4>(),
                                                 F.reuseMask.as<const uint32_t>(), F.resv[cur].as<Resv>(),
@@ -1725,15 +1728,15 @@ nomad_status restir_launch(nomad_ctx *ctx, uint32_t nviews, unsigned long long P
   }
   const uint32_t cdfCap = std::min<uint32_t>(ctx->res.emissiveCount, 8192u);
   k_restir_initial<<<grid, kPtBlock, cdfCap * sizeof(float), s>>>(
-      V, nviews, P, cfg, F.qRays[0].as<const float4>(), F.hits.as<const int32_t>(), ctx->prims.as<const float4>(),
-      ctx->materials.as<const float4>(), L, F.rInit.as<Resv>(), sCur, cdfCap);
+      V, nviews, P, cfg, F.qRays[0].as<const float4>(), F.hits.as<const int32_t>(),
+      ShadeTables{ctx->shadeRec.as<const float4>(), ctx->matTable.as<const float4>()}, L, F.rInit.as<Resv>(), sCur, cdfCap);
   k_restir_temporal<<<grid, kPtBlock, 0, s>>>(V, F.prevViews.as<const ViewDev>(), nviews, P, cfg,
-                                             ctx->materials.as<const float4>(), F.rInit.as<const Resv>(), sCur,
+                                             ShadeTables{ctx->shadeRec.as<const float4>(), ctx->matTable.as<const float4>()}, F.rInit.as<const Resv>(), sCur,
                                              F.resv[cur ^ 1].as<const Resv>(), F.surf[cur ^ 1].as<const Surf>(),
                                              F.rTemp.as<Resv>(), plan.temporal);
-  k_restir_spatial<<<grid, kPtBlock, 0, s>>>(V, nviews, P, cfg, ctx->materials.as<const float4>(),
+  k_restir_spatial<<<grid, kPtBlock, 0, s>>>(V, nviews, P, cfg, ShadeTables{ctx->shadeRec.as<const float4>(), ctx->matTable.as<const float4>()},
                                             F.rTemp.as<const Resv>(), sCur, F.resv[cur].as<Resv>());
-  k_restir_shade<<<grid, kPtBlock, 0, s>>>(V, nviews, P, ctx->materials.as<const float4>(), F.resv[cur].as<const Resv>(),
+  k_restir_shade<<<grid, kPtBlock, 0, s>>>(V, nviews, P, ShadeTables{ctx->shadeRec.as<const float4>(), ctx->matTable.as<const float4>()}, F.resv[cur].as<const Resv>(),
                                           sCur, F.sRays.as<float4>(), F.sIds.as<uint32_t>(), F.sContrib.as<float4>(), C);
   NOMAD_CUDA(ctx, cudaGetLastError());
   NOMAD_CUDA(ctx, cudaMemcpyAsync(F.prevViews.p, F.views.p, nviews * sizeof(ViewDev), cudaMemcpyDeviceToDevice, s));
