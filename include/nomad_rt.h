@@ -210,6 +210,16 @@ nomad_status nomad_trace_work(nomad_ctx *ctx, const nomad_ray *rays, uint64_t n,
 /* Per-object closest-hit counts accumulated by NOMAD_TRACE_COUNT_HITS calls: out[object_count]. */
 nomad_status nomad_read_object_hits(nomad_ctx *ctx, uint32_t *out);
 nomad_status nomad_reset_object_hits(nomad_ctx *ctx);
+/* The same counts into `out[object_count]`, a host array (synchronous) or, with
+ * NOMAD_TRACE_DEVICE_POINTERS in flags, a device array (queued on the context's stream). */
+nomad_status nomad_read_object_hits_ex(nomad_ctx *ctx, uint32_t *out, uint32_t flags);
+/* Replaces the per-object closest-hit counts gathered since the last residency step with
+ * `counts[object_count]`, a host array or (NOMAD_TRACE_DEVICE_POINTERS) a device array; queued on
+ * the context's stream. No counterpart in the reference, which renders on one GPU: it is the one
+ * cross-GPU exchange of a frame split over ranks. Each rank renders its views or tiles with hit
+ * counting, the ranks sum the counts (an all-reduce of object_count words), and every rank writes
+ * the sum back before its residency step, so all ranks decide the same resident set. */
+nomad_status nomad_write_object_hits(nomad_ctx *ctx, const uint32_t *counts, uint32_t flags);
 
 /* ---- path tracing (replaces pathTraceKernel + rayColor, PathTraceKernel.metal:7-162 and
  *      PathTracing.h:1069-1881, as a wavefront loop; the reference's per-pixel seed hash is

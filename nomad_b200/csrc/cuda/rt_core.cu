@@ -798,6 +798,28 @@ extern "C" nomad_status nomad_read_object_hits(nomad_ctx *ctx, uint32_t *out) {
   return NOMAD_OK;
 }
 
+extern "C" nomad_status nomad_read_object_hits_ex(nomad_ctx *ctx, uint32_t *out, uint32_t flags) {
+  if (!(flags & NOMAD_TRACE_DEVICE_POINTERS)) return nomad_read_object_hits(ctx, out);
+  if (!ctx || !ctx->sceneReady) return NOMAD_ERR_NOT_READY;
+  if (!out) return NOMAD_ERR_INVALID_ARGUMENT;
+  NOMAD_DEVICE_SCOPE(ctx);
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(out, ctx->objHits.p, (size_t)ctx->objectCount * 4, cudaMemcpyDeviceToDevice,
+                                  ctx->stream));
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_write_object_hits(nomad_ctx *ctx, const uint32_t *counts, uint32_t flags) {
+  if (!ctx || !ctx->sceneReady) return NOMAD_ERR_NOT_READY;
+  if (!counts) return NOMAD_ERR_INVALID_ARGUMENT;
+  NOMAD_DEVICE_SCOPE(ctx);
+  const bool dev = (flags & NOMAD_TRACE_DEVICE_POINTERS) != 0;
+  NOMAD_CUDA(ctx, cudaMemcpyAsync(ctx->objHits.p, counts, (size_t)ctx->objectCount * 4,
+                                  dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
+  // a host source may go out of scope when the call returns
+  if (!dev) NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return NOMAD_OK;
+}
+
 extern "C" nomad_status nomad_reset_object_hits(nomad_ctx *ctx) {
   if (!ctx || !ctx->sceneReady) return NOMAD_ERR_NOT_READY;
   NOMAD_DEVICE_SCOPE(ctx);

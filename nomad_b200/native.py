@@ -190,6 +190,8 @@ SIGNATURES = {
     "nomad_residency_object_state": (C.c_int32, [_P, _P, _P, _P]),
     "nomad_mlp_init": (C.c_int32, [_P, C.c_uint64]),
     "nomad_mlp_gradient": (C.c_int32, [_P, _P, _P, C.c_uint64, _P, _P]),
+    "nomad_read_object_hits_ex": (C.c_int32, [_P, _P, C.c_uint32]),
+    "nomad_write_object_hits": (C.c_int32, [_P, _P, C.c_uint32]),
     "nomad_residency_posterior": (C.c_int32, [_P, _P]),
     "nomad_residency_count_tests": (C.c_int32, [_P, C.c_int32, _P]),
     "nomad_mlp_train": (C.c_int32, [_P, _P, _P, C.c_uint64, C.c_uint32, C.c_uint32, C.c_float,
@@ -919,6 +921,21 @@ class Context:
         out = np.zeros(self.object_count, np.uint32)
         self._ck(self.lib.nomad_read_object_hits(self.h, _ptr(out)))
         return out
+
+    def object_hits_dev(self, out_ptr: int):
+        """The per-object hit counts into a device array of object_count u32 words (queued on the
+        context's stream)."""
+        self._ck(self.lib.nomad_read_object_hits_ex(self.h, _P(out_ptr), TRACE_DEVICE_POINTERS))
+
+    def write_object_hits(self, counts=None, dev_ptr: int = 0):
+        """Replaces the hit counts gathered since the last residency step: a host array of
+        object_count u32, or a device array (dev_ptr) queued on the context's stream."""
+        if dev_ptr:
+            self._ck(self.lib.nomad_write_object_hits(self.h, _P(dev_ptr), TRACE_DEVICE_POINTERS))
+        else:
+            c = np.ascontiguousarray(counts, np.uint32)
+            assert c.size == self.object_count
+            self._ck(self.lib.nomad_write_object_hits(self.h, _ptr(c), 0))
 
     # geometry paging
     def paging_enable(self, pool_bytes: int, width: int = 4, max_onloads: int = 0):
