@@ -75,12 +75,44 @@ __device__ __forceinline__ void traverse_wide(const DevScene &S, const WideScene
   int sp = 0;
   bool done = (ref == kEmptyRef);
   constexpr int F4 = (W == 4) ? 8 : 16;
+  // With no axis parallel to the ray (r.par == 0), each axis's near plane is the box minimum
+  // when the ray runs up that axis (1/d > 0) and the maximum otherwise, for every box: the slab
+  // test's min((mn - o) / d, (mx - o) / d) is that plane's distance, since subtraction and
+  // multiplication round monotonically. Loading the near- and far-plane rows of a node by these
+  // row offsets leaves one 3-way max and one 3-way min per child instead of three pairwise
+  // min/max first; the distances, and so the hits, are the slab test's exactly.
+  constexpr int Q = W / 4;
+  const int nX = r.ix > 0.0f ? 0 : 3, nY = r.iy > 0.0f ? 1 : 4, nZ = r.iz > 0.0f ? 2 : 5;
+  const int fX = 3 - nX, fY = 5 - nY, fZ = 7 - nZ;
   while (!done) {
     if (ref >= 0) {
       const float4 *n = WS.wn + (long long)F4 * ref;
       float bound = ANY ? tmax : h.t * kPruneScale;
       float t[W];
       int32_t c[W];
+      if (r.par == 0) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+          const float4 px = ldg4(n + nX * Q + q), py = ldg4(n + nY * Q + q), pz = ldg4(n + nZ * Q + q);
+          const float4 gx = ldg4(n + fX * Q + q), gy = ldg4(n + fY * Q + q), gz = ldg4(n + fZ * Q + q);
+          const float4 rf = ldg4(n + 6 * Q + q);
+          const float ax[4] = {px.x, px.y, px.z, px.w}, ay[4] = {py.x, py.y, py.z, py.w};
+          const float az[4] = {pz.x, pz.y, pz.z, pz.w}, bx[4] = {gx.x, gx.y, gx.z, gx.w};
+          const float by[4] = {gy.x, gy.y, gy.z, gy.w}, bz[4] = {gz.x, gz.y, gz.z, gz.w};
+          const int32_t rr[4] = {__float_as_int(rf.x), __float_as_int(rf.y), __float_as_int(rf.z),
+                                 __float_as_int(rf.w)};
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const float tnx = (ax[k] - r.ox) * r.ix, tny = (ay[k] - r.oy) * r.iy, tnz = (az[k] - r.oz) * r.iz;
+            const float tfx = (bx[k] - r.ox) * r.ix, tfy = (by[k] - r.oy) * r.iy, tfz = (bz[k] - r.oz) * r.iz;
+            const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, kRayEps));
+            const float tf = fminf(fminf(tfx, tfy), fminf(tfz, bound));
+            const bool hk = rr[k] != kEmptyRef && !(tf < tn);
+            t[q * 4 + k] = hk ? tn : INFINITY;
+            c[q * 4 + k] = hk ? rr[k] : kEmptyRef;
+          }
+        }
+      } else
 #pragma unroll
       for (int q = 0; q < W / 4; ++q) {
         float4 mnx = ldg4(n + 0 * (W / 4) + q), mny = ldg4(n + 1 * (W / 4) + q), mnz = ldg4(n + 2 * (W / 4) + q);
