@@ -171,10 +171,39 @@ def cpu_leg(sb, rays, budget_s=12.0, use_reference=False):
             os_.closest(part, orc.MODE_REFERENCE_ORDER, threads=cores)
         done += part.shape[0]
     dt = time.perf_counter() - t0
-    return {"value": done / dt / 1e6, "unit": "Mrays/s", "cores": cores,
-            "kind": "reference" if use_reference else "port",
-            "sample": f"{done} rays drawn uniformly from the workload's primary+bounce batch "
-                      f"({dt:.1f} s of CPU work, {cores} threads)"}
+    out = {"value": done / dt / 1e6, "unit": "Mrays/s", "cores": cores,
+           "kind": "reference" if use_reference else "port",
+           "sample": f"{done} rays drawn uniformly from the workload's primary+bounce batch "
+                     f"({dt:.1f} s of CPU work, {cores} threads)"}
+    if not use_reference:
+        out.update(cpu_extra(os_, orc, sb, sample, cores))
+    return out
+
+
+def cpu_extra(os_, orc, sb, sample, cores, budget_s=4.0):
+    """The scalar port's any-hit rate over the same rays (tmax as given), and its path-traced
+    ms per C2 frame (1920x1080 x 4 spp, 3 bounces, NEE) extrapolated from a seeded sample of
+    pixels rendered in full (all samples and bounces of each)."""
+    done, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < budget_s and done < sample.shape[0]:
+        part = sample[done:done + 200_000]
+        os_.any(part, orc.MODE_REFERENCE_ORDER, threads=cores)
+        done += part.shape[0]
+    dt_any = time.perf_counter() - t0
+    import nomad_b200 as nb
+
+    v = nb.view_pinhole((0.0, 220.0, -620.0), (0.0, 0.0, 60.0), width=WIDTH, height=HEIGHT, spp=SPP,
+                        max_depth=3, seed=SEED)
+    px = np.random.default_rng(321).permutation(WIDTH * HEIGHT).astype(np.uint64)
+    n, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < budget_s and n < px.size:
+        orc.render(os_, sb.materials, v, pixels=px[n:n + 1024], threads=cores)
+        n += 1024
+    dt_pt = time.perf_counter() - t0
+    return {"any_hit_mrays_s": done / dt_any / 1e6,
+            "path_traced_ms_per_frame": dt_pt / n * WIDTH * HEIGHT * 1e3,
+            "path_traced_sample": f"{n} seeded pixels of the C2 frame, every sample and bounce "
+                                  f"({dt_pt:.1f} s, {cores} threads), scaled to {WIDTH * HEIGHT} pixels"}
 
 
 def frame_leg(nb, ctx, sb, frames=3):
