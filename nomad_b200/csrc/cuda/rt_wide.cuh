@@ -70,8 +70,7 @@ __device__ __forceinline__ void traverse_wide(const DevScene &S, const WideScene
     return;
   }
   int32_t ref = WS.root;
-  int32_t stk[STACK];
-  float stt[STACK];
+  int2 stk[STACK];  // (ref, bits of its entry distance): one 8-byte local store per push
   int sp = 0;
   bool done = (ref == kEmptyRef);
   constexpr int F4 = (W == 4) ? 8 : 16;
@@ -138,8 +137,7 @@ __device__ __forceinline__ void traverse_wide(const DevScene &S, const WideScene
         for (int k = W - 1; k >= 1; --k) {
           if (c[k] != kEmptyRef) {
             if (sp < STACK) {
-              stk[sp] = c[k];
-              stt[sp] = t[k];
+              stk[sp] = make_int2(c[k], __float_as_int(t[k]));
               ++sp;
             } else {
               atomicOr(S.status, kStatusStackOverflow);
@@ -157,8 +155,9 @@ __device__ __forceinline__ void traverse_wide(const DevScene &S, const WideScene
     ref = kEmptyRef;
     while (sp > 0) {
       --sp;
-      if (!ANY && stt[sp] > h.t * kPruneScale) continue;
-      ref = stk[sp];
+      const int2 e = stk[sp];
+      if (!ANY && __int_as_float(e.y) > h.t * kPruneScale) continue;
+      ref = e.x;
       break;
     }
     if (ref == kEmptyRef) break;
