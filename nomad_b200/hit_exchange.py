@@ -9,7 +9,9 @@ counters, so the residency steps that follow take the same decisions on every ra
 exchange between ranks on this path; geometry, rays and images never cross.
 
 With the NCCL backend the counts stay on the device (device-to-device copies around the
-all-reduce, over NVLink); with any other backend (gloo) they go through host memory.
+all-reduce, over NVLink) and are summed as 32-bit integers, so an object's summed count must stay
+below 2^31 in one frame (the rays of a frame are far fewer); with any other backend (gloo) they go
+through host memory and are summed as 64-bit integers, with an error if a sum exceeds 32 bits.
 """
 from __future__ import annotations
 
