@@ -59,3 +59,21 @@ def test_reference_arm_maps_no_product_library():
     out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, check=True).stdout
     mine = [line for line in out.split() if line.startswith(ROOT)]
     assert mine and all(line.startswith(os.path.join(ROOT, "oracle")) for line in mine), mine
+
+
+def test_cpu_baseline_extras(nb, orc):
+    """The CPU baseline's any-hit rate and path-traced frame estimate run on a small city: the
+    any-hit answers agree with the closest hits (a ray with a closest hit is occluded), and the
+    frame estimate is the sampled pixels' time scaled to the full frame."""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    sb = nb.SceneBVH(nb.synth_city(**CITY))
+    os_ = orc.OracleScene(sb)
+    cam = nb.Camera((0, 50, -150), (0, 0, 0), width=64, height=40)
+    rays = cam.primary_rays(1, seed=3)
+    hit = os_.closest(rays)["prim"] >= 0
+    assert np.array_equal(os_.any(rays).astype(bool), hit)
+    out = bench.cpu_extra(os_, orc, sb, rays, 2, budget_s=0.2)
+    assert out["any_hit_mrays_s"] > 0 and out["path_traced_ms_per_frame"] > 0
+    assert "seeded pixels of the C2 frame" in out["path_traced_sample"]
