@@ -525,6 +525,14 @@ nomad_status nomad_paging_enable(nomad_ctx *ctx, const nomad_paging_config *cfg)
 nomad_status nomad_paging_update(nomad_ctx *ctx);
 /* Waits for the copies in flight and publishes them (does not start new onloads). */
 nomad_status nomad_paging_wait(nomad_ctx *ctx);
+/* on != 0: every nomad_paging_update first waits for the copies the previous updates started and
+ * for the frames that unlinked released pool space, then publishes and reuses all of them, so
+ * which objects a frame traces depends only on the sequence of calls, not on how fast the copies
+ * ran: runs repeat exactly. It costs a host wait when a copy is still in flight (a frame loop that
+ * waits for its frame anyway loses nothing). on = 0 (the default): an update publishes what has
+ * completed, as the reference's streaming does, and runs can differ by copy timing. No
+ * counterpart in the reference. */
+nomad_status nomad_paging_set_sync(nomad_ctx *ctx, int32_t on);
 nomad_status nomad_paging_stats_get(nomad_ctx *ctx, nomad_paging_stats *out);
 /* Per-object NOMAD_PAGE_* state (object_count bytes). */
 nomad_status nomad_paging_states(nomad_ctx *ctx, uint8_t *out);

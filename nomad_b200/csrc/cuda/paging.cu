@@ -135,6 +135,7 @@ struct Paging {
   DeviceBuf descBuf;
   cudaEvent_t descFree = nullptr;    // the previous batch's descriptors have been copied
   bool descPending = false;
+  bool syncPublish = false;          // updates wait for the previous updates' copies and releases
   std::vector<ObjPage> obj;
   std::vector<int32_t> ref;     // host copy of the published ref table
   RangeAlloc nodeAlloc, recAlloc;
@@ -547,6 +548,15 @@ extern "C" nomad_status nomad_paging_update(nomad_ctx *ctx) {
   NOMAD_DEVICE_SCOPE(ctx);
   nomad_status hs = nomad_residency_sync_host(ctx);
   if (hs != NOMAD_OK) return hs;
+  if (pg->syncPublish) {
+    // everything started or released by earlier updates completes before this one looks at it
+    for (const ObjPage &op : pg->obj)
+      if (op.state == NOMAD_PAGE_STREAMING) NOMAD_CUDA(ctx, cudaEventSynchronize(op.copied));
+    for (const Retire &r : pg->retiring) {
+      NOMAD_CUDA(ctx, cudaEventSynchronize(r.after));
+      if (r.copy) NOMAD_CUDA(ctx, cudaEventSynchronize(r.copy));
+    }
+  }
   refresh_retired(pg);
   ++pg->tick;
   std::vector<PubItem> items;
@@ -679,6 +689,14 @@ extern "C" nomad_status nomad_paging_wait(nomad_ctx *ctx) {
   if (st != NOMAD_OK) return st;
   NOMAD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   refresh_retired(pg);
+  return NOMAD_OK;
+}
+
+extern "C" nomad_status nomad_paging_set_sync(nomad_ctx *ctx, int32_t on) {
+  if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
+  Paging *pg = pg_of(ctx);
+  if (!pg) return fail(ctx, NOMAD_ERR_NOT_READY, "paging is not enabled");
+  pg->syncPublish = on != 0;
   return NOMAD_OK;
 }
 

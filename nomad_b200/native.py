@@ -173,6 +173,7 @@ SIGNATURES = {
     "nomad_paging_enable": (C.c_int32, [_P, C.POINTER(PagingConfig)]),
     "nomad_paging_update": (C.c_int32, [_P]),
     "nomad_paging_wait": (C.c_int32, [_P]),
+    "nomad_paging_set_sync": (C.c_int32, [_P, C.c_int32]),
     "nomad_paging_stats_get": (C.c_int32, [_P, C.POINTER(PagingStats)]),
     "nomad_paging_states": (C.c_int32, [_P, _P]),
     "nomad_view_pinhole": (C.c_int32, [_P, _P, _P, C.c_float, C.c_uint32, C.c_uint32, _P]),
@@ -947,6 +948,10 @@ class Context:
 
     def paging_wait(self):
         self._ck(self.lib.nomad_paging_wait(self.h))
+
+    def paging_set_sync(self, on: bool = True):
+        """Updates wait for the previous updates' copies and releases, so runs repeat exactly."""
+        self._ck(self.lib.nomad_paging_set_sync(self.h, 1 if on else 0))
 
     def paging_stats(self) -> dict:
         st = PagingStats()

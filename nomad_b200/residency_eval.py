@@ -32,6 +32,10 @@ from . import native as nat
 
 HIST_FEATURES = list(range(3, 12)) + [19, 20]
 HYSTERESIS = 0.5  # resident_key_bonus of the hysteresis rows
+# the traversal of every context of the workload: 4-wide nodes, persistent warps, 10 blocks per SM
+# (the bench city's autotuned choice)
+TRAVERSAL = dict(width=4, persistent=1, short_stack=0, regroup=1, staged_nodes=0, block=128, postpone_leaves=0,
+                 min_blocks=10)
 VALIDATION_PATH = 2  # camera path on which the paged configuration is chosen (evaluation: path 1)
 # the reference's host-side heuristics, which toggle through the residency interface
 HOST_POLICIES = (nat.POLICY_RAYHIT_PRIM, nat.POLICY_DISTANCE_LOD, nat.POLICY_SCREEN_SPACE,
@@ -132,6 +136,15 @@ class Workload:
         self.seed = seed
         self.budget_fraction = budget_fraction
         self.setup_s = time.perf_counter() - t0
+
+    def fix_traversal(self, *ctxs):
+        """Sets the fixed traversal of this workload on every context. An autotuned choice can
+        differ between runs (the fastest variants are within a few percent), and the paged runs
+        page the node layout of the chosen width, whose bytes per object differ between widths:
+        with one fixed configuration the whole comparison repeats exactly."""
+        for c in ctxs:
+            c.set_traversal(**TRAVERSAL)
+        return "bvh4_persist_mb10"
 
     def tune(self, ctx, judge=None):
         """Autotunes the traversal on the primary rays of a path's first view; the judge context
@@ -253,8 +266,9 @@ class Workload:
         """The same run with geometry paging: a third context whose BLAS nodes (of the tuned
         traversal width) and triangle records live in a device pool of pool_slack x the budget's
         share of the paged bytes, streamed in by nomad_paging_update after every residency step
-        (at most 32 onloads per frame). ms/frame includes the update; rel-MSE includes the frames
-        where wanted objects are still streaming. The scorer is ctx's unless mlp (a weight blob)
+        (at most 32 onloads per frame), each update publishing the onloads the previous ones started
+        (nomad_paging_set_sync). ms/frame includes the update; rel-MSE includes the frames where
+        wanted objects are still streaming. The scorer is ctx's unless mlp (a weight blob)
         is given; bonus is the selection's hysteresis (resident_key_bonus)."""
         import torch
 
@@ -273,6 +287,10 @@ class Workload:
             frac = budget_fraction or self.budget_fraction
             pool = int(min(full, full * frac * pool_slack))
             pc.paging_enable(pool, width=trav["width"])
+            # every update publishes what the previous ones started: the resident set of a frame
+            # then follows from the calls alone, and runs and policies compare without the noise
+            # of copy timing (the loop waits for each frame anyway)
+            pc.paging_set_sync(True)
             nbytes = pc.object_bytes()
             budget = int(frac * nbytes.sum())
             prm = nat.ResidencyParams.make(policy, budget_bytes=budget, camera_motion=0.3, min_active=0,
@@ -335,7 +353,7 @@ def run(paths=200, frames_per_path=8, steps=1500, frames=300, repeats=3, log=pri
     log(f"residency workload: {w.sb.prim_count} prims, {w.sb.object_count} objects, set-up {w.setup_s:.1f}s")
     ctx = w.context()
     judge = w.context()
-    traversal = w.tune(ctx, judge)
+    traversal = w.fix_traversal(ctx, judge)
     log(f"traversal: {traversal}")
     t1 = time.perf_counter()
     x, t = w.record(ctx, paths=paths, frames_per_path=frames_per_path)

@@ -259,6 +259,44 @@ def test_device_residency_step_drives_paging(nb, small_city):
     assert np.array_equal(_bits(got), _bits(want))
 
 
+def test_sync_publish_repeats_exactly(nb, small_city):
+    """With nomad_paging_set_sync, each update publishes what the previous ones started, so two
+    contexts given the same calls go through the same paging states, statistics and images frame
+    by frame, however fast their copies ran. A small pool (35 % of the geometry bytes), a ray-hit
+    budget of 30 % and 8 onloads per update keep objects streaming, cached and evicted."""
+    _, sb = small_city
+    runs = []
+    for _ in range(2):
+        ctx = nb.Context()
+        ctx.upload(sb)
+        nbytes = ctx.object_bytes()
+        ctx.paging_enable(int(nbytes.sum() * 0.35), width=4, max_onloads=8)
+        ctx.paging_set_sync(True)
+        prm = nb.ResidencyParams.make(nb.POLICY_RAYHIT_BUDGET, budget_bytes=int(nbytes.sum() * 0.3),
+                                      camera_motion=0.5)
+        trace = []
+        try:
+            for frame in range(16):
+                ang = frame * 0.4
+                view = nb.view_pinhole((180 * np.sin(ang), 60, -180 * np.cos(ang)), (0, 0, 0), width=96,
+                                       height=54, spp=2, max_depth=2, seed=frame)
+                img = ctx.render(view, count_hits=True)[0]
+                ctx.residency_step(prm, view, toggles=False)
+                ctx.paging_update()
+                st = ctx.paging_stats()
+                trace.append((ctx.paging_states().copy(), img.copy(),
+                              tuple(st[k] for k in ("onloads", "evictions", "deferred", "relinks", "cached"))))
+        finally:
+            ctx.close()
+        runs.append(trace)
+    for f, (a, b) in enumerate(zip(*runs)):
+        assert np.array_equal(a[0], b[0]), f
+        assert np.array_equal(a[1], b[1]), f
+        assert a[2] == b[2], f
+    onloads, evictions, deferred = runs[0][-1][2][:3]
+    assert onloads > 0 and evictions + deferred > 0  # the pool was under pressure
+
+
 def test_paging_refuses_other_layouts(nb, small_city):
     _, sb = small_city
     ctx = _paged(nb, sb, 4, 1 << 40)
