@@ -111,6 +111,34 @@ def spread(runs, key):
     return {"mean": float(np.mean(vals)), "min": float(np.min(vals)), "max": float(np.max(vals)), "runs": vals}
 
 
+def smallest_budget_within(sweep, bound):
+    """Key of the smallest swept budget (keys are budget fractions as text) whose energy rel-MSE
+    is at most bound, or None."""
+    ok = sorted((float(k), k) for k, v in sweep.items() if v.get("rel_mse_energy", float("inf")) <= bound)
+    return ok[0][1] if ok else None
+
+
+def fastest_within(sweep, bound):
+    """Key of the swept configuration with the lowest ms/frame among those whose energy rel-MSE
+    is at most bound (ties go to the smaller key), or None."""
+    ok = sorted((v["ms_per_frame"], k) for k, v in sweep.items()
+                if v.get("rel_mse_energy", float("inf")) <= bound and "ms_per_frame" in v)
+    return ok[0][1] if ok else None
+
+
+def faster_outside_spread(a, b):
+    """True when every run of record a was faster than every run of record b (the slowest of a's
+    run means below the fastest of b's)."""
+    return bool("ms_per_frame_spread" in a and "ms_per_frame_spread" in b
+                and a["ms_per_frame_spread"]["max"] < b["ms_per_frame_spread"]["min"])
+
+
+def within_5pct(a, b):
+    """True when record a's energy rel-MSE is at most 1.05 x record b's."""
+    return bool("rel_mse_energy" in a and "rel_mse_energy" in b
+                and a["rel_mse_energy"] <= 1.05 * b["rel_mse_energy"])
+
+
 def repeat(fn, repeats):
     """Runs fn() `repeats` times; the first run's record with ms_per_frame replaced by its mean
     and spread over the runs."""
@@ -455,13 +483,13 @@ def run(paths=200, frames_per_path=8, steps=1500, frames=300, repeats=3, log=pri
                                                                       frames=frames, budget_fraction=frac))
         out[f"{tag}_budget_sweep"] = sweep
         log(f"{tag} budget sweep: { {k: (v['rel_mse_energy'], v['ms_per_frame']) for k, v in sweep.items()} }")
-        ok = [k for k, v in sorted(sweep.items()) if v["rel_mse_energy"] <= target]
-        if not ok:
+        key = smallest_budget_within(sweep, target)
+        if key is None:
             out[f"{tag}_matching_rayhit"] = None
             continue
-        frac = float(ok[0])
+        frac = float(key)
         rh = out["ray_hit_budget_paged"]
-        rec = {"budget_fraction": frac, "unpaged": sweep[ok[0]],
+        rec = {"budget_fraction": frac, "unpaged": sweep[key],
                "ray_hit_paged_ms_per_frame_spread": rh.get("ms_per_frame_spread")}
         for key, bonus in (("paged", 0.0), ("paged_hysteresis", HYSTERESIS)):
             try:
@@ -470,11 +498,8 @@ def run(paths=200, frames_per_path=8, steps=1500, frames=300, repeats=3, log=pri
             except nat.NomadError as exc:
                 paged = {"error": str(exc)}
             rec[key] = paged
-            rec[f"{key}_faster_outside_spread"] = bool(
-                "ms_per_frame_spread" in paged and "ms_per_frame_spread" in rh and
-                paged["ms_per_frame_spread"]["max"] < rh["ms_per_frame_spread"]["min"])
-            rec[f"{key}_energy_within_5pct_of_ray_hit_paged"] = bool(
-                "rel_mse_energy" in paged and paged["rel_mse_energy"] <= 1.05 * rh["rel_mse_energy"])
+            rec[f"{key}_faster_outside_spread"] = faster_outside_spread(paged, rh)
+            rec[f"{key}_energy_within_5pct_of_ray_hit_paged"] = within_5pct(paged, rh)
         out[f"{tag}_matching_rayhit"] = rec
         log(f"{tag} matching ray-hit at {frac}: {out[f'{tag}_matching_rayhit']}")
     # With paging on (the budget then bounds device memory): the budget and hysteresis of the
@@ -500,9 +525,8 @@ def run(paths=200, frames_per_path=8, steps=1500, frames=300, repeats=3, log=pri
         log(f"learned paged (hysteresis) sweep (budget/bonus): "
             f"{ {k: (v.get('rel_mse_energy'), v.get('ms_per_frame')) for k, v in psweep.items()} }")
         # the fastest swept configuration whose error meets the bound, then repeated
-        ok = sorted((v["ms_per_frame"], k) for k, v in psweep.items() if v.get("rel_mse_energy", 1e30) <= target_p)
-        if ok:
-            key = ok[0][1]
+        key = fastest_within(psweep, target_p)
+        if key is not None:
             frac, bonus = float(key.split("/")[0]), float(key.split("/")[1])
             rep = repeat(lambda: w.evaluate_paged(ctx, judge, nat.POLICY_LEARNED, frames=frames,
                                                   budget_fraction=frac, mlp=blob_hits, bonus=bonus), repeats)
@@ -511,8 +535,8 @@ def run(paths=200, frames_per_path=8, steps=1500, frames=300, repeats=3, log=pri
                 "budget_fraction": frac, "resident_key_bonus": bonus, "learned_paged_hysteresis": rep,
                 "ray_hit_paged_ms_per_frame_spread": rhp.get("ms_per_frame_spread"),
                 "ray_hit_paged_rel_mse_energy": rhp["rel_mse_energy"],
-                "energy_within_5pct": bool(rep["rel_mse_energy"] <= 1.05 * rhp["rel_mse_energy"]),
-                "faster_outside_spread": bool(rep["ms_per_frame_spread"]["max"] < rhp["ms_per_frame_spread"]["min"])}
+                "energy_within_5pct": within_5pct(rep, rhp),
+                "faster_outside_spread": faster_outside_spread(rep, rhp)}
         else:
             out["learned_paged_matching_rayhit_paged"] = None
         log(f"learned paged matching ray-hit paged: {out['learned_paged_matching_rayhit_paged']}")
