@@ -268,6 +268,26 @@ nomad_status nomad_view_pinhole(const float position[3], const float look_at[3],
 enum { NOMAD_RENDER_DIRECT = 1u << 2 };
 nomad_status nomad_render_frame(nomad_ctx *ctx, const nomad_view *views, uint32_t nviews,
                                 float *radiance_out, uint32_t flags);
+
+/* A rectangle of a view's pixels: the reference's TileDispatchRegion (Renderer.cpp:1261-1266),
+ * the region its path-tracing kernel renders per dispatch (tile, buffer 16, and
+ * pixel = gid + tile.origin, PathTraceKernel.metal:43-58). */
+typedef struct nomad_tile {
+  uint32_t origin_x, origin_y;
+  uint32_t width, height;
+} nomad_tile;
+
+/* nomad_render_frame restricted to tiles[i] of views[i] (one tile per view; the tiled dispatch
+ * of Renderer.cpp:7319-7581 renders a frame tile by tile). A tile's paths are the view's own
+ * paths: the same pixel indices key their random numbers and place their camera rays, so every
+ * tile pixel equals that pixel of nomad_render_frame for the same views bit for bit, and with
+ * NOMAD_TRACE_COUNT_HITS the per-object counts of tiles that cover a view once add up to the
+ * whole frame's. radiance_out receives each tile's pixels row-major, tiles concatenated (sum of
+ * width*height*3 floats). A tile must be non-empty and inside its view; a NOMAD_VIEW_RESTIR view
+ * must be rendered whole (its reuse reads neighbouring pixels). Same flags and graph caching as
+ * nomad_render_frame. */
+nomad_status nomad_render_tiles(nomad_ctx *ctx, const nomad_view *views, const nomad_tile *tiles,
+                                uint32_t nviews, float *radiance_out, uint32_t flags);
 /* out[0] frame graphs captured, [1] graph launches, [2] graphs cached now (at most 8). */
 nomad_status nomad_frame_graph_stats(nomad_ctx *ctx, uint64_t out[3]);
 

@@ -42,8 +42,16 @@ struct ViewDev {
   float cam[3], vu[3], vv[3], fp[3];
   float lod;
   uint32_t w, h, spp, maxDepth, k0, k1, flags, index;
+  uint32_t tx, ty, tw;  // the rendered tile: origin and width in the view's pixels (0, 0, w: all)
   unsigned long long pathOffset, pixelOffset;
 };
+
+// The view pixel of the tile's pixel lp (row-major in the tile): the index that keys the path's
+// random numbers and places its camera ray, so a tile's paths are the full view's paths.
+__device__ __forceinline__ uint32_t tile_pixel(const ViewDev &v, uint32_t lp) {
+  if (v.tw == v.w) return v.ty * v.w + lp;  // whole rows
+  return (v.ty + lp / v.tw) * v.w + v.tx + lp % v.tw;
+}
 
 struct Counters {
   uint32_t qlen[4];                 // 0, 1: bounce queues; 2: shadow queue
@@ -95,7 +103,7 @@ __global__ void __launch_bounds__(kPtBlock) k_raygen(const ViewDev *__restrict__
   for (unsigned long long pid = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; pid < P; pid += stride) {
     const ViewDev &v = find_view(views, nviews, pid);
     unsigned long long local = pid - v.pathOffset;
-    uint32_t pixel = (uint32_t)(local / v.spp), sample = (uint32_t)(local % v.spp);
+    uint32_t pixel = tile_pixel(v, (uint32_t)(local / v.spp)), sample = (uint32_t)(local % v.spp);
     uint32_t px = pixel % v.w, py = pixel / v.w;
     U4 r = philox(U4{pixel, sample, 255u * 4u, v.index}, v.k0, v.k1);
     float ux = ((float)px + 0.5f) / (float)v.w;
@@ -386,7 +394,7 @@ __global__ void __launch_bounds__(kPtBlock) k_shade(
         hit = true;
         inst = h[0];
         unsigned long long local = pid - v.pathOffset;
-        uint32_t pixel = (uint32_t)(local / v.spp), sample = (uint32_t)(local % v.spp);
+        uint32_t pixel = tile_pixel(v, (uint32_t)(local / v.spp)), sample = (uint32_t)(local % v.spp);
         U4 b0 = philox(U4{pixel, sample, depth * 4u + 0u, v.index}, v.k0, v.k1);
         U4 b1 = philox(U4{pixel, sample, depth * 4u + 1u, v.index}, v.k0, v.k1);
         V3 p = v3(o.x + t * d.x, o.y + t * d.y, o.z + t * d.z);
@@ -681,8 +689,25 @@ void key_put(std::vector<unsigned char> &k, const T &v) {
 }
 }  // namespace
 
+static nomad_status render_views(nomad_ctx *ctx, const nomad_view *views, const nomad_tile *tiles, uint32_t nviews,
+                                 float *out, uint32_t flags);
+
 extern "C" nomad_status nomad_render_frame(nomad_ctx *ctx, const nomad_view *views, uint32_t nviews,
                                            float *out, uint32_t flags) {
+  return render_views(ctx, views, nullptr, nviews, out, flags);
+}
+
+extern "C" nomad_status nomad_render_tiles(nomad_ctx *ctx, const nomad_view *views, const nomad_tile *tiles,
+                                           uint32_t nviews, float *out, uint32_t flags) {
+  if (ctx && !tiles) return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "no tiles");
+  return render_views(ctx, views, tiles, nviews, out, flags);
+}
+
+// One frame over the views, each restricted to its tile when tiles is given (the whole view
+// otherwise). Paths are numbered view by view and, in a view, by tile pixel and sample; the
+// output holds each tile's pixels row-major, tile after tile.
+static nomad_status render_views(nomad_ctx *ctx, const nomad_view *views, const nomad_tile *tiles, uint32_t nviews,
+                                 float *out, uint32_t flags) {
   if (!ctx) return NOMAD_ERR_INVALID_ARGUMENT;
   if (!ctx->sceneReady) return nomad_fail(ctx, NOMAD_ERR_NOT_READY, "no scene uploaded");
   if (!views || nviews == 0 || !out) return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT, "no views or output");
@@ -715,10 +740,28 @@ extern "C" nomad_status nomad_render_frame(nomad_ctx *ctx, const nomad_view *vie
     d.k1 = v.seed_hi + v.frame;
     d.flags = v.flags;
     d.index = i;
+    uint32_t tw = v.width, th = v.height;
+    d.tx = d.ty = 0;
+    if (tiles) {
+      const nomad_tile &t = tiles[i];
+      if (t.width == 0 || t.height == 0 || t.origin_x >= v.width || t.origin_y >= v.height ||
+          t.width > v.width - t.origin_x || t.height > v.height - t.origin_y)
+        return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT,
+                          "tile " + std::to_string(i) + " is empty or reaches outside its view");
+      // ReSTIR's temporal and spatial reuse read the reservoirs of neighbouring pixels
+      if ((v.flags & NOMAD_VIEW_RESTIR) && (t.width != v.width || t.height != v.height))
+        return nomad_fail(ctx, NOMAD_ERR_INVALID_ARGUMENT,
+                          "view " + std::to_string(i) + " uses ReSTIR: its tile must be the whole view");
+      d.tx = t.origin_x;
+      d.ty = t.origin_y;
+      tw = t.width;
+      th = t.height;
+    }
+    d.tw = tw;
     d.pathOffset = P;
     d.pixelOffset = pixels;
-    P += (unsigned long long)v.width * v.height * v.spp;
-    pixels += (unsigned long long)v.width * v.height;
+    P += (unsigned long long)tw * th * v.spp;
+    pixels += (unsigned long long)tw * th;
     maxDepth = std::max(maxDepth, v.max_depth);
   }
   if (P > 0xffffffffull) return nomad_fail(ctx, NOMAD_ERR_LIMIT, "more than 2^32 paths in one frame");

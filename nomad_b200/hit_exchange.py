@@ -5,8 +5,9 @@ a full scene replica: every rank renders its own views or pixel tiles with hit c
 residency step must then see the whole frame's counts, or the ranks would keep different
 resident sets. `allreduce_object_hits` sums the counts of all ranks (one all-reduce of
 object_count 32-bit words, 8 KB at 2,048 objects) and writes the sum back into every rank's
-counters, so the residency steps that follow take the same decisions on every rank. It is the one
-exchange between ranks on this path; geometry, rays and images never cross.
+counters, so the residency steps that follow take the same decisions on every rank. With the
+radiance bands of a frame split by rows (nomad_b200.split_frame) it is the only exchange between
+ranks on this path; geometry and rays never cross.
 
 With the NCCL backend the counts stay on the device (device-to-device copies around the
 all-reduce, over NVLink) and are summed as 32-bit integers, so an object's summed count must stay

@@ -178,6 +178,7 @@ SIGNATURES = {
     "nomad_paging_states": (C.c_int32, [_P, _P]),
     "nomad_view_pinhole": (C.c_int32, [_P, _P, _P, C.c_float, C.c_uint32, C.c_uint32, _P]),
     "nomad_render_frame": (C.c_int32, [_P, _P, C.c_uint32, _P, C.c_uint32]),
+    "nomad_render_tiles": (C.c_int32, [_P, _P, _P, C.c_uint32, _P, C.c_uint32]),
     "nomad_render_stats": (C.c_int32, [_P, _P]),
     "nomad_frame_graph_stats": (C.c_int32, [_P, _P]),
     "nomad_reset_render_stats": (C.c_int32, [_P]),
@@ -770,6 +771,38 @@ class Context:
         views = np.ascontiguousarray(views, VIEW_DTYPE).reshape(-1)
         self._keep_views = views
         self._ck(self.lib.nomad_render_frame(self.h, _ptr(views), views.shape[0], _P(out_ptr),
+                                             TRACE_DEVICE_POINTERS |
+                                             (TRACE_COUNT_HITS if count_hits else 0) |
+                                             (0 if graph else RENDER_DIRECT)))
+
+    def render_tiles(self, views: np.ndarray, tiles, count_hits: bool = False, graph: bool = True) -> list:
+        """Renders tiles[i] = (origin_x, origin_y, width, height) of views[i] in one batched frame;
+        returns one (height, width, 3) float32 image per tile, equal bit for bit to that region
+        of render() of the same views."""
+        views = np.ascontiguousarray(views, VIEW_DTYPE).reshape(-1)
+        tiles = np.ascontiguousarray(np.asarray(tiles, np.uint32).reshape(-1, 4))
+        if tiles.shape[0] != views.shape[0]:
+            raise ValueError("one tile per view")
+        total = int((tiles[:, 2].astype(np.int64) * tiles[:, 3]).sum())
+        out = np.empty(total * 3, np.float32)
+        flags = (TRACE_COUNT_HITS if count_hits else 0) | (0 if graph else RENDER_DIRECT)
+        self._ck(self.lib.nomad_render_tiles(self.h, _ptr(views), _ptr(tiles), views.shape[0], _ptr(out), flags))
+        imgs, off = [], 0
+        for t in tiles:
+            n = int(t[2]) * int(t[3])
+            imgs.append(out[3 * off:3 * (off + n)].reshape(int(t[3]), int(t[2]), 3))
+            off += n
+        return imgs
+
+    def render_tiles_dev(self, views: np.ndarray, tiles, out_ptr: int, count_hits: bool = False,
+                         graph: bool = True):
+        """render_tiles into device memory at out_ptr (the tiles' pixels, 3 floats each)."""
+        views = np.ascontiguousarray(views, VIEW_DTYPE).reshape(-1)
+        tiles = np.ascontiguousarray(np.asarray(tiles, np.uint32).reshape(-1, 4))
+        if tiles.shape[0] != views.shape[0]:
+            raise ValueError("one tile per view")
+        self._keep_views = (views, tiles)
+        self._ck(self.lib.nomad_render_tiles(self.h, _ptr(views), _ptr(tiles), views.shape[0], _P(out_ptr),
                                              TRACE_DEVICE_POINTERS |
                                              (TRACE_COUNT_HITS if count_hits else 0) |
                                              (0 if graph else RENDER_DIRECT)))

@@ -4,7 +4,8 @@ bench.py runs one replica per GPU (the views shard; there is no data-path collec
 crosses ranks is the timing: each rank's timed region is reduced to the slowest rank's
 (`ranks_max`), and the whole-job throughput counts every rank's units (`job_rate`). The reference
 arm does its work on rank 0 only; other ranks return at once. A frame split over ranks also sums
-the per-object hit counters before the residency step (`nomad_b200.hit_exchange`). These are
+the per-object hit counters before the residency step (`nomad_b200.hit_exchange`) and gathers the
+row bands each rank rendered (`nomad_b200.split_frame`). These are
 checked here with two processes on 127.0.0.1; the GPU box has one GPU, so the NCCL run of the
 same code is not tested on several GPUs.
 """
@@ -137,3 +138,102 @@ def test_two_gloo_ranks_sum_object_hits(tmp_path):
     assert want.max() > 2**31
     for r in range(world):
         assert np.array_equal(np.load(tmp_path / f"total{r}.npy"), want.astype(np.uint32))
+
+
+class _FakeTiles(_FakeCounters):
+    """Stands in for a Context's tile rendering: a pixel's value depends only on its view and its
+    place in the whole view, like the paths of nomad_render_tiles, and every rendered pixel
+    counts one hit on object (pixel index mod object count)."""
+
+    def __init__(self, objects):
+        super().__init__(np.zeros(objects, np.uint32))
+
+    def render_tiles(self, views, tiles, count_hits=False, graph=True):
+        out = []
+        for i, (v, (x0, y0, w, h)) in enumerate(zip(views, tiles)):
+            W = int(v["width"])
+            ys, xs = np.meshgrid(np.arange(y0, y0 + h), np.arange(x0, x0 + w), indexing="ij")
+            pix = ys * W + xs
+            img = np.stack([np.sin(pix * 0.37 + i + c).astype(np.float32) for c in range(3)], -1)
+            out.append(img)
+            if count_hits:
+                np.add.at(self.counts, pix.reshape(-1) % self.object_count, 1)
+        return out
+
+
+def _views(dims):
+    from nomad_b200.native import VIEW_DTYPE
+
+    v = np.zeros(len(dims), VIEW_DTYPE)
+    for i, (w, h) in enumerate(dims):
+        v[i]["width"], v[i]["height"], v[i]["spp"], v[i]["max_depth"] = w, h, 1, 1
+    return v
+
+
+SPLIT_VIEWS = [(13, 7), (5, 11), (8, 3)]
+
+
+def _split_rank_main(rank, world, port, out_dir):
+    sys.path.insert(0, ROOT)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    import datetime
+
+    import torch.distributed as dist
+
+    from nomad_b200.split_frame import render_split
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        ctx = _FakeTiles(17)
+        frames = render_split(ctx, _views(SPLIT_VIEWS), count_hits=True)
+        for i, f in enumerate(frames):
+            np.save(os.path.join(out_dir, f"frame{rank}_{i}.npy"), f)
+        np.save(os.path.join(out_dir, f"hits{rank}.npy"), ctx.counts)
+    finally:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(240)
+def test_three_gloo_ranks_split_a_frame_by_rows(tmp_path):
+    """Three ranks render uneven row bands (7 rows: 2 + 2 + 3; 3 rows: one each) of three views;
+    every rank ends with the whole frames, equal to one rank's render of the whole views, and
+    with the whole frame's per-object counts."""
+    world = 3
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    procs = [ctx.Process(target=_split_rank_main, args=(r, world, port, str(tmp_path))) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(200)
+    for p in procs:
+        if p.is_alive():
+            p.kill()
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    whole = _FakeTiles(17)
+    views = _views(SPLIT_VIEWS)
+    want = whole.render_tiles(views, [(0, 0, w, h) for w, h in SPLIT_VIEWS], count_hits=True)
+    for r in range(world):
+        for i in range(len(SPLIT_VIEWS)):
+            got = np.load(tmp_path / f"frame{r}_{i}.npy")
+            assert got.shape == want[i].shape and np.array_equal(got, want[i]), (r, i)
+        assert np.array_equal(np.load(tmp_path / f"hits{r}.npy"), whole.counts), r
+
+
+def test_row_bands_partition_the_rows():
+    from nomad_b200.split_frame import band_tiles, row_bands
+
+    for h in (1, 2, 7, 1080, 1081):
+        for world in (1, 2, 3, 8):
+            bands = row_bands(h, world)
+            assert len(bands) == world
+            assert bands[0][0] == 0 and sum(b[1] for b in bands) == h
+            assert all(bands[r][0] + bands[r][1] == bands[r + 1][0] for r in range(world - 1))
+            assert max(b[1] for b in bands) - min(b[1] for b in bands) <= 1
+    t = band_tiles(_views([(640, 360), (17, 9)]), 2, 4)
+    assert t.tolist() == [[0, 180, 640, 90], [0, 4, 17, 2]]
+    with pytest.raises(ValueError):
+        band_tiles(_views([(640, 3)]), 0, 4)  # a band per rank needs at least as many rows
+    with pytest.raises(ValueError):
+        row_bands(10, 0)
