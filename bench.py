@@ -228,6 +228,34 @@ def frame_leg(nb, ctx, sb, frames=3):
             "mrays_per_s_incl_shadow": (st[0] + st[2]) / dt / 1e6}
 
 
+def split_frame_leg(nb, ctx, world, frames=5):
+    """The path-traced city frame of frame_leg split over the ranks by row bands
+    (nomad_b200.split_frame: each rank renders its rows as a tile, the bands are all-gathered on
+    the device). Every rank runs it, with the same collectives in the same order; ms/frame is the
+    slowest rank's time from its first band's launch to the gathered frame."""
+    import torch
+    import torch.distributed as dist
+
+    from nomad_b200.split_frame import render_split, row_bands
+
+    v = nb.view_pinhole((0.0, 220.0, -620.0), (0.0, 0.0, 60.0), width=WIDTH, height=HEIGHT, spp=SPP,
+                        max_depth=3, seed=SEED)
+    render_split(ctx, v)  # captures the band's frame graph
+    torch.cuda.synchronize()
+    dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for f in range(frames):
+        v["frame"] = f
+        img = render_split(ctx, v)[0]
+    e1.record()
+    e1.synchronize()
+    ms = ranks_max(e0.elapsed_time(e1) / frames, world)
+    return {"config": f"city {WIDTH}x{HEIGHT} x {SPP} spp, 3 bounces, one-sample NEE, rows split over {world} ranks",
+            "ms_per_frame": ms, "rows_per_rank": [b[1] for b in row_bands(HEIGHT, world)],
+            "frame_shape": list(img.shape), "frames": frames}
+
+
 def multiview_views(nb, n=16, seed=404):
     rng = np.random.default_rng(seed)
     views = []
@@ -852,6 +880,12 @@ def main():
         cpu = cpu_leg(sb, np.concatenate([primary, bounce]))
 
     extras = {}
+    if world > 1 and not args.no_extras:
+        ctx.set_stream(0)
+        try:
+            extras["city_frame_split"] = split_frame_leg(nb, ctx, world)
+        except Exception as exc:  # reported, never hiding the headline line
+            extras["city_frame_split"] = {"error": repr(exc)}
     if rank == 0 and world == 1 and not args.no_extras:
         ctx.set_stream(0)
         for name, fn in (("city_frame", lambda: frame_leg(nb, ctx, sb)),

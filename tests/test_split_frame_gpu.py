@@ -95,3 +95,41 @@ def test_refused_tiles(nb, cctx):
     # the context stays usable
     img = cctx.render_tiles(v, [(0, 0, 64, 32)])[0]
     assert np.array_equal(_bits(img), _bits(cctx.render(v)[0]))
+
+
+def test_nccl_single_rank_split_frame(nb, small_city):
+    """The NCCL paths of render_split (device bands, row padding, all-gather) and of
+    allreduce_object_hits (device counts, all-reduce, write-back) in a one-rank group, which one
+    GPU can run: the frames equal the whole render bit for bit and the counts are kept."""
+    import datetime
+    import socket
+
+    import torch.distributed as dist
+
+    from nomad_b200.hit_exchange import allreduce_object_hits
+    from nomad_b200.split_frame import render_split
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60))
+    c = nb.Context(0)
+    try:
+        c.upload(small_city[1])
+        views = np.concatenate([_view(nb, (0, 60, -180), 120, 71, 4), _view(nb, (40, 45, -120), 96, 54, 5)])
+        c.reset_object_hits()
+        want = c.render(views, count_hits=True)
+        want_hits = c.object_hits().copy()
+        c.reset_object_hits()
+        got = render_split(c, views, count_hits=True)
+        assert len(got) == 2
+        for g, w in zip(got, want):
+            assert g.is_cuda and tuple(g.shape) == w.shape
+            assert np.array_equal(_bits(g.cpu().numpy()), _bits(w))
+        assert np.array_equal(c.object_hits(), want_hits)
+        assert allreduce_object_hits(c) is None
+        assert np.array_equal(c.object_hits(), want_hits)
+    finally:
+        c.close()
+        dist.destroy_process_group()
