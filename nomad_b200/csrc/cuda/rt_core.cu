@@ -694,7 +694,28 @@ nomad_status trace_host(nomad_ctx *ctx, Op op, const nomad_ray *rays, uint64_t n
                         size_t outStride, bool countHits) {
   NOMAD_CUDA(ctx, ctx->stageIn.reserve(n * sizeof(nomad_ray)));
   NOMAD_CUDA(ctx, ctx->stageOut.reserve(n * outStride));
+  // Chunks of a sixteenth of the batch (at least 2^19 rays). The last chunk's traversal and
+  // download run after every upload has landed, so a batch of more than two chunks ends with
+  // halving ones (1/2, 1/4, 1/8, 1/8 of a chunk): the part of the batch that no upload overlaps
+  // shrinks to an eighth of a chunk.
   const uint64_t chunk = std::max<uint64_t>(1 << 19, (n + 15) / 16);
+  std::vector<uint64_t> parts;
+  {
+    uint64_t rest = n;
+    const bool taper = n > 2 * chunk;
+    while (rest > (taper ? chunk : 0)) {
+      const uint64_t m = std::min(chunk, rest);
+      parts.push_back(m);
+      rest -= m;
+    }
+    const uint64_t last = std::max<uint64_t>(chunk / 8, 1 << 16);
+    while (rest > last) {
+      const uint64_t m = (rest + 1) / 2;
+      parts.push_back(m);
+      rest -= m;
+    }
+    if (rest > 0) parts.push_back(rest);
+  }
   cudaStream_t sIn = ctx->copyStreams[0], sOut = ctx->copyStreams[1], sK = ctx->stream;
   std::vector<cudaEvent_t> evs;
   auto event = [&](cudaEvent_t *e) -> cudaError_t {
@@ -713,8 +734,9 @@ nomad_status trace_host(nomad_ctx *ctx, Op op, const nomad_ray *rays, uint64_t n
   // Uploads and kernels first, downloads second: a copy to or from pageable host memory returns
   // only once it is done, so issuing a download before the next upload would serialise them.
   std::vector<cudaEvent_t> traced;
-  for (uint64_t off = 0; off < n && st == NOMAD_OK; off += chunk) {
-    const uint64_t m = std::min(chunk, n - off);
+  uint64_t off = 0;
+  for (size_t k = 0; k < parts.size() && st == NOMAD_OK; off += parts[k], ++k) {
+    const uint64_t m = parts[k];
     char *din = static_cast<char *>(ctx->stageIn.p) + off * sizeof(nomad_ray);
     char *dout = static_cast<char *>(ctx->stageOut.p) + off * outStride;
     cudaEvent_t up, done;
@@ -732,8 +754,9 @@ nomad_status trace_host(nomad_ctx *ctx, Op op, const nomad_ray *rays, uint64_t n
     }
     traced.push_back(done);
   }
-  for (size_t k = 0; k < traced.size() && st == NOMAD_OK; ++k) {
-    const uint64_t off = k * chunk, m = std::min(chunk, n - off);
+  off = 0;
+  for (size_t k = 0; k < traced.size() && st == NOMAD_OK; off += parts[k], ++k) {
+    const uint64_t m = parts[k];
     if (cudaStreamWaitEvent(sOut, traced[k], 0) != cudaSuccess ||
         cudaMemcpyAsync(static_cast<char *>(out) + off * outStride,
                         static_cast<char *>(ctx->stageOut.p) + off * outStride, m * outStride,
