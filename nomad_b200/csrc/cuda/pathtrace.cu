@@ -53,8 +53,11 @@ __device__ __forceinline__ uint32_t tile_pixel(const ViewDev &v, uint32_t lp) {
   return (v.ty + lp / v.tw) * v.w + v.tx + lp % v.tw;
 }
 
+// Queue lengths 128 bytes apart: every warp of k_shade appends to the next-bounce and the shadow
+// queue, and atomics to one cache line are serialised by one L2 slice.
+constexpr int kQ = 32;
 struct Counters {
-  uint32_t qlen[4];                 // 0, 1: bounce queues; 2: shadow queue
+  uint32_t qlen[4 * kQ];            // [kQ * k]: 0, 1 bounce queues; 2 shadow queue; 3 ReSTIR rays
   unsigned long long cursor[2];     // persistent-trace cursors (closest, any)
   unsigned long long stats[4];      // segments, escapes, shadow rays, hits
 };
@@ -77,10 +80,11 @@ __device__ __forceinline__ const ViewDev &find_view(const ViewDev *views, uint32
   return views[lo];
 }
 
-__device__ __forceinline__ void warp_add64(unsigned long long *p, bool pred) {
-  unsigned m = __ballot_sync(__activemask(), pred);
-  int lane = threadIdx.x & 31;
-  if (m && lane == __ffs(__activemask()) - 1) atomicAdd(p, (unsigned long long)__popc(m));
+// Adds the sum of v over the warp's active lanes to *p with one atomic.
+__device__ __forceinline__ void warp_sum64(unsigned long long *p, uint32_t v) {
+  const unsigned act = __activemask();
+  const uint32_t sum = __reduce_add_sync(act, v);
+  if (sum && (threadIdx.x & 31) == __ffs(act) - 1) atomicAdd(p, (unsigned long long)sum);
 }
 
 // Warp-aggregated append: returns the slot of this lane (only meaningful when want).
@@ -121,7 +125,7 @@ __global__ void __launch_bounds__(kPtBlock) k_raygen(const ViewDev *__restrict__
     thr[pid] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
     rad[pid] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) cnt->qlen[0] = (uint32_t)P;
+  if (blockIdx.x == 0 && threadIdx.x == 0) cnt->qlen[kQ * (0)] = (uint32_t)P;
 }
 
 struct Material {
@@ -358,13 +362,16 @@ __global__ void __launch_bounds__(kPtBlock) k_shade(
     float4 *__restrict__ sContrib, float4 *__restrict__ thr, float4 *__restrict__ rad,
     const float4 *__restrict__ shadeRec, const float4 *__restrict__ matTable, Lights L, Counters *cnt, int cur,
     uint32_t *__restrict__ objHits, int restirDepth0, uint32_t *__restrict__ primHits) {
-  const uint32_t n = cnt->qlen[cur];
+  const uint32_t n = cnt->qlen[kQ * (cur)];
   const uint32_t lightCount = L.meta->count;
   const float lightTotal = L.meta->total;
-  uint32_t *nextLen = &cnt->qlen[cur ^ 1];
-  uint32_t *shadowLen = &cnt->qlen[2];
+  uint32_t *nextLen = &cnt->qlen[kQ * (cur ^ 1)];
+  uint32_t *shadowLen = &cnt->qlen[kQ * (2)];
   uint32_t stride = gridDim.x * blockDim.x;
   uint32_t iters = (n + stride - 1) / stride;
+  // this thread's segments, escapes and hits, added to the frame's counters once at the end (one
+  // atomic per warp and launch instead of three per warp and iteration on one cache line)
+  uint32_t nSeg = 0, nEsc = 0, nHit = 0;
   for (uint32_t it = 0; it < iters; ++it) {
     uint32_t i = it * stride + blockIdx.x * blockDim.x + threadIdx.x;
     bool live = i < n;
@@ -478,10 +485,10 @@ __global__ void __launch_bounds__(kPtBlock) k_shade(
         }
       }
     }
-    // Counters (warp-aggregated): segments, escapes, hits, per-object hits.
-    warp_add64(&cnt->stats[0], live);
-    warp_add64(&cnt->stats[1], live && !hit);
-    warp_add64(&cnt->stats[3], hit);
+    nSeg += live;
+    nEsc += live && !hit;
+    nHit += hit;
+    // per-object (and per-primitive) closest hits, warp-aggregated by key
     if (objHits) {
       unsigned act = __activemask();
       int key = hit ? inst : -1;
@@ -506,13 +513,16 @@ __global__ void __launch_bounds__(kPtBlock) k_shade(
       nIds[ns] = pid;
     }
   }
+  warp_sum64(&cnt->stats[0], nSeg);
+  warp_sum64(&cnt->stats[1], nEsc);
+  warp_sum64(&cnt->stats[3], nHit);
 }
 
 __global__ void __launch_bounds__(kPtBlock) k_resolve(const uint32_t *__restrict__ sIds,
                                                        const float4 *__restrict__ sContrib,
                                                        const uint8_t *__restrict__ occ, float4 *__restrict__ rad,
                                                        Counters *cnt) {
-  uint32_t n = cnt->qlen[2];
+  uint32_t n = cnt->qlen[kQ * (2)];
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     if (occ[i]) continue;
     uint32_t pid = sIds[i];
@@ -524,8 +534,8 @@ __global__ void __launch_bounds__(kPtBlock) k_resolve(const uint32_t *__restrict
 
 // Clears the next-bounce and shadow queue lengths and the trace cursors before a bounce.
 __global__ void k_bounce_reset(Counters *cnt, int cur) {
-  cnt->qlen[cur ^ 1] = 0;
-  cnt->qlen[2] = 0;
+  cnt->qlen[kQ * (cur ^ 1)] = 0;
+  cnt->qlen[kQ * (2)] = 0;
   cnt->cursor[0] = 0;
   cnt->cursor[1] = 0;
 }
@@ -823,12 +833,12 @@ static nomad_status render_views(nomad_ctx *ctx, const nomad_view *views, const 
     int cur = 0;
     for (uint32_t depth = 0; depth < maxDepth; ++depth) {
       k_bounce_reset<<<1, 1, 0, s>>>(C, cur);
-      nomad_status rs = nomad_trace_variant(ctx, ctx->trav, false, F.qRays[cur].as<const float4>(), P, &C->qlen[cur],
+      nomad_status rs = nomad_trace_variant(ctx, ctx->trav, false, F.qRays[cur].as<const float4>(), P, &C->qlen[kQ * (cur)],
                                             &C->cursor[0], F.hits.as<int32_t>(), nullptr, nullptr, s);
       if (rs != NOMAD_OK) return rs;
       if (objHits && ctx->res.testsOn) {  // per-object "rays tested" for the hit posterior
         rs = nomad_count_object_tests(ctx, F.qRays[cur].as<const float4>(), F.hits.as<const int32_t>(), P,
-                                      &C->qlen[cur]);
+                                      &C->qlen[kQ * (cur)]);
         if (rs != NOMAD_OK) return rs;
       }
       if (depth == 0 && plan.on) {
@@ -842,7 +852,7 @@ static nomad_status render_views(nomad_ctx *ctx, const nomad_view *views, const 
                                          F.thr.as<float4>(), F.rad.as<float4>(), ctx->shadeRec.as<const float4>(),
                                          ctx->matTable.as<const float4>(), L, C, cur, objHits, plan.on ? 1 : 0,
                                          primHits);
-      rs = nomad_trace_variant(ctx, ctx->trav, true, F.sRays.as<const float4>(), P, &C->qlen[2], &C->cursor[1],
+      rs = nomad_trace_variant(ctx, ctx->trav, true, F.sRays.as<const float4>(), P, &C->qlen[kQ * (2)], &C->cursor[1],
                                nullptr, F.sOcc.as<uint8_t>(), nullptr, s);
       if (rs != NOMAD_OK) return rs;
       k_resolve<<<gridPT, kPtBlock, 0, s>>>(F.sIds.as<const uint32_t>(), F.sContrib.as<const float4>(),
@@ -1253,7 +1263,7 @@ __global__ void __launch_bounds__(kPtBlock) k_restir_shade(
         }
       }
     }
-    uint32_t slot = warp_append(&cnt->qlen[2], want);
+    uint32_t slot = warp_append(&cnt->qlen[kQ * (2)], want);
     if (want) {
       sRays[2 * slot] = A;
       sRays[2 * slot + 1] = B;
@@ -1461,7 +1471,7 @@ __global__ void __launch_bounds__(kPtBlock, NOMAD_PT_MINB) k_restir_ref_cand(
         const U4 u = philox(U4{pixel, sample, 0x10000u + c, vp->index}, vp->k0, vp->k1);
         want = ref_new_candidate(s, m, L, lightCount, lightTotal, u, cd);
       }
-      const uint32_t slot = warp_append(&cnt->qlen[3], want);
+      const uint32_t slot = warp_append(&cnt->qlen[kQ * (3)], want);
       if (want) {
         float4 A, B;
         ref_ray(s, cd, A, B);
@@ -1478,7 +1488,7 @@ __global__ void __launch_bounds__(kPtBlock) k_restir_ref_vis(const uint32_t *__r
                                                              const uint8_t *__restrict__ occ, uint32_t per,
                                                              uint32_t words, uint32_t *__restrict__ mask,
                                                              Counters *cnt) {
-  const uint32_t n = cnt->qlen[3];
+  const uint32_t n = cnt->qlen[kQ * (3)];
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     if (occ[i]) continue;
     const uint32_t id = ids[i], pid = id / per, c = id - pid * per;
@@ -1488,7 +1498,7 @@ __global__ void __launch_bounds__(kPtBlock) k_restir_ref_vis(const uint32_t *__r
 }
 
 __global__ void k_restir_ref_reset(Counters *cnt) {
-  cnt->qlen[3] = 0;
+  cnt->qlen[kQ * (3)] = 0;
   cnt->cursor[1] = 0;
 }
 
@@ -1545,7 +1555,7 @@ __global__ void __launch_bounds__(kPtBlock, NOMAD_PT_MINB) k_restir_ref_reuse(
         want = ref_reuse_candidate(k, *vp, prevViews[vp->index], s, m, mats, ra, rPrev, sPrev, pixel, sample, q, qid,
                                    pv, cd);
       }
-      const uint32_t slot = warp_append(&cnt->qlen[3], want);
+      const uint32_t slot = warp_append(&cnt->qlen[kQ * (3)], want);
       if (want) {
         float4 A, B;
         ref_ray(s, cd, A, B);
@@ -1658,7 +1668,7 @@ __global__ void __launch_bounds__(kPtBlock, NOMAD_PT_MINB) k_restir_ref_final(
       }
       rOut[pid] = r;
     }
-    const uint32_t slot = warp_append(&cnt->qlen[2], want);
+    const uint32_t slot = warp_append(&cnt->qlen[kQ * (2)], want);
     if (want) {
       sRays[2 * slot] = A;
       sRays[2 * slot + 1] = B;
@@ -1672,7 +1682,7 @@ __global__ void __launch_bounds__(kPtBlock, NOMAD_PT_MINB) k_restir_ref_final(
 __global__ void __launch_bounds__(kPtBlock) k_restir_ref_vis5(const uint32_t *__restrict__ ids,
                                                               const uint8_t *__restrict__ occ,
                                                               uint32_t *__restrict__ mask, Counters *cnt) {
-  const uint32_t n = cnt->qlen[3];
+  const uint32_t n = cnt->qlen[kQ * (3)];
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     if (occ[i]) continue;
     const uint32_t id = ids[i], pid = id / kRefReuse, k = id - pid * kRefReuse;
@@ -1743,7 +1753,7 @@ nomad_status restir_launch(nomad_ctx *ctx, uint32_t nviews, unsigned long long P
                                                F.refRays.as<float4>(), F.refIds.as<uint32_t>(), C);
     NOMAD_CUDA(ctx, cudaGetLastError());
     nomad_status ts = nomad_trace_variant(ctx, ctx->trav, true, F.refRays.as<const float4>(), P * cf.candidates,
-                                          &C->qlen[3], &C->cursor[1], nullptr, F.refOcc.as<uint8_t>(), nullptr, s);
+                                          &C->qlen[kQ * (3)], &C->cursor[1], nullptr, F.refOcc.as<uint8_t>(), nullptr, s);
     if (ts != NOMAD_OK) return ts;
     k_restir_ref_vis<<<grid, kPtBlock, 0, s>>>(F.refIds.as<const uint32_t>(), F.refOcc.as<const uint8_t>(),
                                               cf.candidates, ra.words, F.refMask.as<uint32_t>(), C);
@@ -1754,7 +1764,7 @@ nomad_status restir_launch(nomad_ctx *ctx, uint32_t nviews, unsigned long long P
                                                 F.refContrib.as<float4>(), F.reuseMask.as<uint32_t>(),
                                                 F.refRays.as<float4>(), F.refIds.as<uint32_t>(), C);
     NOMAD_CUDA(ctx, cudaGetLastError());
-    ts = nomad_trace_variant(ctx, ctx->trav, true, F.refRays.as<const float4>(), P * kRefReuse, &C->qlen[3],
+    ts = nomad_trace_variant(ctx, ctx->trav, true, F.refRays.as<const float4>(), P * kRefReuse, &C->qlen[kQ * (3)],
                              &C->cursor[1], nullptr, F.refOcc.as<uint8_t>(), nullptr, s);
     if (ts != NOMAD_OK) return ts;
     k_restir_ref_vis5<<<grid, kPtBlock, 0, s>>>(F.refIds.as<const uint32_t>(), F.refOcc.as<const uint8_t>(),
