@@ -56,6 +56,10 @@ __device__ __forceinline__ uint32_t tile_pixel(const ViewDev &v, uint32_t lp) {
 // Queue lengths 128 bytes apart: every warp of k_shade appends to the next-bounce and the shadow
 // queue, and atomics to one cache line are serialised by one L2 slice.
 constexpr int kQ = 32;
+// Resident blocks per SM the shading kernel is compiled for: 4 (64 registers, about 110 bytes
+// spilled) hides more of its dependent loads than 2 uncapped (105 registers) or 3 (80) did; the
+// images are the same.
+constexpr int kShadeMinBlocks = 4;
 struct Counters {
   uint32_t qlen[4 * kQ];            // [kQ * k]: 0, 1 bounce queues; 2 shadow queue; 3 ReSTIR rays
   unsigned long long cursor[2];     // persistent-trace cursors (closest, any)
@@ -355,7 +359,7 @@ __device__ __forceinline__ uint32_t select_light_cdf(float xi, const float *cdf,
   return lo < count - 1 ? lo : count - 1;
 }
 
-__global__ void __launch_bounds__(kPtBlock) k_shade(
+__global__ void __launch_bounds__(kPtBlock, kShadeMinBlocks) k_shade(
     uint32_t depth, const ViewDev *__restrict__ views, uint32_t nviews, const float4 *__restrict__ qRays,
     const uint32_t *__restrict__ qIds, const int32_t *__restrict__ hits, float4 *__restrict__ nRays,
     uint32_t *__restrict__ nIds, float4 *__restrict__ sRays, uint32_t *__restrict__ sIds,
