@@ -31,10 +31,10 @@ using namespace nomad_pt;
 namespace {
 
 constexpr int kPtBlock = 256;
-// Resident blocks per SM the ReSTIR candidate and spatial kernels are compiled for (a register
-// cap: measured faster than the uncapped build; the shading kernel is faster uncapped).
+// Resident blocks per SM the ReSTIR candidate, spatial and reference-mode kernels are compiled
+// for (a register cap): 4 was measured faster than 3, 5 and the uncapped build, same images.
 #ifndef NOMAD_PT_MINB
-#define NOMAD_PT_MINB 3
+#define NOMAD_PT_MINB 4
 #endif
 constexpr float kPi = 3.14159265358979323846f;
 
