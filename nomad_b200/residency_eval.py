@@ -118,12 +118,14 @@ def smallest_budget_within(sweep, bound):
     return ok[0][1] if ok else None
 
 
-def fastest_within(sweep, bound):
-    """Key of the swept configuration with the lowest ms/frame among those whose energy rel-MSE
-    is at most bound (ties go to the smaller key), or None."""
-    ok = sorted((v["ms_per_frame"], k) for k, v in sweep.items()
-                if v.get("rel_mse_energy", float("inf")) <= bound and "ms_per_frame" in v)
-    return ok[0][1] if ok else None
+def cheapest_within(sweep, bound):
+    """Key ("budget/bonus") of the swept configuration with the smallest budget among those whose
+    energy rel-MSE is at most bound, the lower error deciding between hysteresis settings of one
+    budget; None if none. Budgets and errors repeat exactly from run to run, so the choice does
+    too; a choice by ms/frame would not, between configurations within each other's timing spread."""
+    ok = sorted((float(k.split("/")[0]), v["rel_mse_energy"], k) for k, v in sweep.items()
+                if v.get("rel_mse_energy", float("inf")) <= bound)
+    return ok[0][2] if ok else None
 
 
 def faster_outside_spread(a, b):
@@ -503,9 +505,9 @@ def run(paths=200, frames_per_path=8, steps=1500, frames=300, repeats=3, log=pri
         out[f"{tag}_matching_rayhit"] = rec
         log(f"{tag} matching ray-hit at {frac}: {out[f'{tag}_matching_rayhit']}")
     # With paging on (the budget then bounds device memory): the budget and hysteresis of the
-    # learned policy are chosen on a second camera path (VALIDATION_PATH): the fastest swept
-    # configuration whose energy rel-MSE there is within 5 % of the paged ray-hit policy's at the
-    # full budget on that path. The chosen configuration is then run on the evaluation path, and
+    # learned policy are chosen on a second camera path (VALIDATION_PATH): the smallest swept
+    # budget whose energy rel-MSE there is within 5 % of the paged ray-hit policy's at the full
+    # budget on that path (the lower error between hysteresis settings). The chosen configuration is then run on the evaluation path, and
     # its error and ms/frame are compared with the paged ray-hit policy's there.
     rhp = out["ray_hit_budget_paged"]
     if "rel_mse_energy" in rhp:
@@ -524,8 +526,8 @@ def run(paths=200, frames_per_path=8, steps=1500, frames=300, repeats=3, log=pri
         out["learned_paged_hysteresis_budget_sweep"] = psweep
         log(f"learned paged (hysteresis) sweep (budget/bonus): "
             f"{ {k: (v.get('rel_mse_energy'), v.get('ms_per_frame')) for k, v in psweep.items()} }")
-        # the fastest swept configuration whose error meets the bound, then repeated
-        key = fastest_within(psweep, target_p)
+        # the smallest swept budget whose error meets the bound, then repeated
+        key = cheapest_within(psweep, target_p)
         if key is not None:
             frac, bonus = float(key.split("/")[0]), float(key.split("/")[1])
             rep = repeat(lambda: w.evaluate_paged(ctx, judge, nat.POLICY_LEARNED, frames=frames,

@@ -91,15 +91,20 @@ def test_smallest_budget_within_orders_budgets_numerically():
     assert rev.smallest_budget_within({"0.10": {"error": "x"}, "0.25": _rec(0.1, 1.0)}, 1.0) == "0.25"
 
 
-def test_fastest_within_takes_the_lowest_ms_among_those_meeting_the_bound():
-    sweep = {"0.150/0.5": _rec(0.50, 1.20), "0.150/1": _rec(0.37, 1.27), "0.200/0.5": _rec(0.40, 1.25),
-             "0.300/1": _rec(0.20, 1.40), "0.250/1": {"error": "pool too small"}}
-    assert rev.fastest_within(sweep, 0.45) == "0.200/0.5"
-    assert rev.fastest_within(sweep, 0.6) == "0.150/0.5"
-    assert rev.fastest_within(sweep, 0.1) is None
-    # equal times: the smaller key wins, so the choice does not depend on dict order
-    tie = {"b": _rec(0.1, 1.0), "a": _rec(0.1, 1.0)}
-    assert rev.fastest_within(tie, 1.0) == "a"
+def test_cheapest_within_takes_the_smallest_budget_then_the_lower_error():
+    sweep = {"0.150/0.5": _rec(0.69, 1.20), "0.150/1": _rec(0.59, 1.21), "0.200/0.5": _rec(0.40, 1.10),
+             "0.300/1": _rec(0.20, 1.40), "0.100/1": {"error": "pool too small"}}
+    # both 15 % settings meet the bound: the lower error wins, whatever their ms/frame
+    assert rev.cheapest_within(sweep, 0.79) == "0.150/1"
+    assert rev.cheapest_within(sweep, 0.65) == "0.150/1"
+    assert rev.cheapest_within(sweep, 0.5) == "0.200/0.5"
+    assert rev.cheapest_within(sweep, 0.1) is None
+    # the choice depends on budgets and errors only: other timings give the same key
+    retimed = {k: (dict(v, ms_per_frame=2.0 - v["ms_per_frame"]) if "ms_per_frame" in v else v)
+               for k, v in sweep.items()}
+    assert rev.cheapest_within(retimed, 0.79) == "0.150/1"
+    # budgets compare as numbers: 0.175 comes after 0.15
+    assert rev.cheapest_within({"0.175/1": _rec(0.1, 1.0), "0.150/1": _rec(0.2, 1.0)}, 1.0) == "0.150/1"
 
 
 def test_faster_outside_spread_and_within_5pct():
