@@ -284,8 +284,11 @@ typedef struct nomad_tile {
  * NOMAD_TRACE_COUNT_HITS the per-object counts of tiles that cover a view once add up to the
  * whole frame's. radiance_out receives each tile's pixels row-major, tiles concatenated (sum of
  * width*height*3 floats). A tile must be non-empty and inside its view; a NOMAD_VIEW_RESTIR view
- * must be rendered whole (its reuse reads neighbouring pixels). Same flags and graph caching as
- * nomad_render_frame. */
+ * must be rendered whole (its reuse reads neighbouring pixels). views[i] is view i of the batch
+ * and its index keys its random numbers, as in nomad_render_frame: to reproduce a frame, pass
+ * the frame's views in the same order, one tile each, and render further tiles of a view in
+ * further calls (a view repeated in one call is another view of the batch, with other samples).
+ * Same flags and graph caching as nomad_render_frame. */
 nomad_status nomad_render_tiles(nomad_ctx *ctx, const nomad_view *views, const nomad_tile *tiles,
                                 uint32_t nviews, float *radiance_out, uint32_t flags);
 /* out[0] frame graphs captured, [1] graph launches, [2] graphs cached now (at most 8). */
